@@ -1,0 +1,227 @@
+/*
+ * mose_b200.h -- C ABI of the B200 residual / stage-update engine for the multi-block structured
+ * compressible Euler / Navier-Stokes solver MOSE-GPU.
+ *
+ * The reference drives one explicit Runge-Kutta step from Explicit_Step
+ * (src/lib/numerics/time/explicit/Mod_Explicit.f90:52-397). Inside it, per stage, it calls
+ *   Fill_Ghost_Cell        (Mod_Explicit.f90:173 -> bc/Lib_Extrapolation.f90:1370-1528)
+ *   Refresh_Thermo_Cache   (Mod_Explicit.f90:179 -> physics/Mod_Thermo_Cache.f90:25-111)
+ *   Fluxes                 (Mod_Explicit.f90:187 -> numerics/fluxes/Mod_Fluxes.f90:10-98)
+ *   BC_Fluxes              (Mod_Explicit.f90:189 -> numerics/fluxes/bc/Mod_BC.f90:646-800)
+ *   RK_Newstate            (Mod_Explicit.f90:262 -> explicit/Lib_Newstate.f90:77-143)
+ * and once per step Compute_dt (Mod_Explicit.f90:123 -> numerics/time/Mod_dt.f90:15-243) and
+ * Copy_State (Mod_Explicit.f90:157 -> gpu/MOSE_Field_m.f90:321-330).
+ * The entry points below replace those calls. Every data pointer handed to an entry point that
+ * launches work is a DEVICE pointer borrowed from the caller (the reference's OpenACC-resident
+ * arrays, obtained with `host_data use_device`), in the reference's own layouts:
+ *   P_flat, PO_flat, R_flat : (ncell_total, nprim) FP64, column-major, var-last, one padded block
+ *                             after the other (gpu/MOSE_Field_m.f90:42-47,128-167); the row of the
+ *                             interior or ghost cell (i,j,k) of block b (i,j,k 1-based, ghosts 1-gc..n+gc) is
+ *                             boff(b) + (i+gc-1) + (j+gc-1)*pi + (k+gc-1)*pi*pj, 0-based,
+ *                             pi = n1+2gc, pj = n2+2gc (MOSE_Field_m.f90:78-109).
+ *   fm1/fm2/fm3             : face normal + area (4, 0:n1, n2, n3) etc. (Mod_Convective.f90:594-596)
+ *   dl, m, vol              : dl_f(3, padded), m_f(3,3, padded), vol(padded) (Mod_Fluxes.f90:222-227,
+ *                             Lib_Newstate.f90:266)
+ * Host-side descriptions (blocks, boundary records, connections, thermo tables) are read once by
+ * mb_init, which builds its own device tables from them (Setup_BC_Device, Mod_BC.f90:99-338).
+ *
+ * Error behaviour: the reference stops the process (`error stop`) on a bad scheme id, a
+ * non-physical state or an off-table temperature (Lib_Newstate.f90:234-246,
+ * Mod_Thermo_Cache.f90:509-536, Mod_Convective.f90:759-766). Here every call returns an int
+ * status (MB_OK = 0, negative on error) and device code never traps; mb_get_status reports the
+ * first bad cell so that a Fortran shim can print the reference's message and stop.
+ */
+#ifndef MOSE_B200_H
+#define MOSE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* compile-time dimensions of the reference build for the configurations served here:
+ * single-species air, laminar (nsc = 1, nrans = 0 -> nprim = 5), gc = 2
+ * (src/lib/base/Global_m.f90:8,15,18; src/lib/CMakeLists.txt:64-72) */
+#define MB_GC 2
+#define MB_NSC 1
+#define MB_NPRIM 5
+
+/* status codes */
+#define MB_OK 0
+#define MB_E_ARG (-1)          /* bad argument (null pointer, size, index) */
+#define MB_E_UNSUPPORTED (-2)  /* scheme id or boundary type not served (Convective_assert_scheme) */
+#define MB_E_CUDA (-3)         /* a CUDA runtime call failed */
+#define MB_E_STATE (-4)        /* state check: p < 0 or a non-finite primitive (State_Check_blk) */
+#define MB_E_THERMO (-5)       /* thermo guard: T outside (1, 9990) K in a viscous run */
+#define MB_E_BUDGET (-6)       /* serving: a case does not fit the HBM budget */
+#define MB_E_TIMEOUT (-7)      /* a bounded device wait gave up */
+#define MB_E_NOMEM (-8)        /* device allocation failed */
+#define MB_E_NODEV (-9)        /* no CUDA device */
+
+/* boundary record types after Setup_BC_Device (IO_BC_Open.f90:155-390 maps the bc.txt codes):
+ * 1 = 1:1 / periodic connection (101, 201), 4 = inflow/outflow (405 supersonic inflow),
+ * 5 = adiabatic no-slip wall (301), 11 = extrapolation (400) */
+#define MB_BC_CONNECTION 1
+#define MB_BC_INFLOW 4
+#define MB_BC_WALL 5
+#define MB_BC_EXTRAPOLATION 11
+
+/* limiter ids = lim_dev (numerics/space/Lib_Limiters.f90:21-61) */
+#define MB_LIM_MINMOD 1
+#define MB_LIM_VANLEER 2
+#define MB_LIM_VANALBADA 3
+#define MB_LIM_MC 4
+#define MB_LIM_SUPERBEE 5
+#define MB_LIM_FIRST_ORDER 6
+/* Riemann solver ids = rs_dev (numerics/fluxes/Lib_Riemann.f90:23-107) */
+#define MB_RS_HLLC 1
+#define MB_RS_AUSMP 4
+#define MB_RS_LMROE 12
+
+#define MB_PREC_FP64 0
+#define MB_PREC_MIXED 1 /* reconstruction + Riemann + viscous flux arithmetic in FP32; state,
+                           RK accumulation, T/p recovery and dt in FP64 */
+
+/* One block: interior extents, row offset in the arena, geometry (device pointers). */
+typedef struct mb_block {
+  int32_t n[3];      /* interior cells n1, n2, n3 (blk%dim) */
+  int32_t pad0;
+  int64_t boff;      /* 0-based first row of the padded block in P_flat (field_block_index_params) */
+  const double* fm1; /* (4, 0:n1, n2, n3): nx, ny, nz, area of the i-faces */
+  const double* fm2; /* (4, n1, 0:n2, n3) */
+  const double* fm3; /* (4, n1, n2, 0:n3) */
+  const double* dl;  /* dl_f(3, 1-gc:n1+gc, 1-gc:n2+gc, 1-gc:n3+gc) */
+  const double* m;   /* m_f(3, 3, padded): m(d, a) = d xi_d / d x_a */
+  const double* vol; /* vol(padded) */
+} mb_block;
+
+/* One boundary record (domain%bc_bi/bj/bk/bf/typ, Mod_BC.f90:400-437): the interior cell that
+ * owns a boundary face, the face 1..6 (odd = low side), and its type. */
+typedef struct mb_bc {
+  int32_t blk;   /* 0-based block */
+  int32_t i, j, k;
+  int32_t face;  /* 1..6 */
+  int32_t type;  /* MB_BC_* */
+  int32_t conn;  /* type 1: index into mb_mesh.conn; -1 otherwise */
+  int32_t pad0;
+  double q[MB_NPRIM]; /* type 4: the imposed primitive state (rho, u, v, w, p) */
+} mb_bc;
+
+/* One connection (domain%conn_*, Lib_Extrapolation.f90:1023-1134): the donor face cell of a
+ * type-1 record and the orientation of the two transverse axes (d11 d12 d21 d22 of bc.txt). */
+typedef struct mb_conn {
+  int32_t rec;               /* the receiving record (index into mb_mesh.rec) */
+  int32_t bs, is, js, ks, fs; /* donor block (0-based), donor face cell (1-based), donor face 1..6 */
+  int32_t d11, d12, d21, d22;
+} mb_conn;
+
+typedef struct mb_mesh {
+  int32_t nblk;
+  int32_t nrec;
+  int32_t nconn;
+  int32_t pad0;
+  int64_t ncell_total;   /* rows of P_flat */
+  const mb_block* blk;   /* host array [nblk] (the geometry pointers in it are device pointers) */
+  const mb_bc* rec;      /* host array [nrec], grouped per block and ordered by face within it */
+  const mb_conn* conn;   /* host array [nconn] */
+} mb_mesh;
+
+/* Single-species thermo and transport tables on the reference's 1 K grid
+ * (lib/FLINT/src/lib/Load_ThermoTransport.f90:82-97,173-188): rows tmin..tmax of h, cp, mu, k
+ * (host pointers; copied to the device by mb_init). */
+typedef struct mb_thermo {
+  int32_t tmin, tmax;
+  double wm;          /* molar mass [kg/kmol]; R = Runiv / wm */
+  const double* cp;
+  const double* h;
+  const double* mu;
+  const double* k;
+} mb_thermo;
+
+typedef struct mb_scheme {
+  int32_t limiter;    /* lim_dev */
+  int32_t riemann;    /* rs_dev */
+  int32_t visc;       /* 0 Euler, 1 laminar Navier-Stokes */
+  int32_t n_rk;       /* 1 euler, 2 RK2, 3 SSP-RK3 (Lib_RK.f90:6-9); 4 classical RK4 (no reference) */
+  int32_t precision;  /* MB_PREC_* */
+  int32_t ndir;       /* computational directions (Lib_Metrics.f90:152-172) */
+  int32_t time_clip;  /* clip the last step onto time_threshold (Mod_dt.f90:283-296) */
+  int32_t state_check;/* [MOSE-scheme] state-check (Lib_Newstate.f90:14) */
+  int32_t dt_additive;/* dt-rule = additive (dt_blk.inc:79-155; 3-D): the convective and diffusive rates of
+                         the three directions add up; 0 = the default min rule (dt_blk.inc:156-191) */
+  int32_t pad0;
+  double cfl;
+  double vnn;         /* default 0.3 (MOSE_Types_m.f90:268) */
+  double prandtl;     /* > 0: kl = mu cp / Pr (Mod_Diffusive.f90:303) */
+  double schmidt;     /* laminar Schmidt (Lib_RANS.f90:25), 0.7 */
+  double mco;         /* riemann-options-Mco (LMRoe low-Mach floor; 1 = plain Roe) */
+  double time_threshold;
+} mb_scheme;
+
+typedef struct mb_status {
+  int32_t code;        /* first error seen (MB_OK if none) */
+  int32_t n_bad_state; /* cells that failed the state check */
+  int32_t n_bad_thermo;/* cells that failed the thermo guard */
+  int32_t bad_blk, bad_i, bad_j, bad_k; /* first offender */
+  int32_t steps;       /* steps taken by mb_step since mb_init */
+  double time;         /* simulated time (sum of dt) */
+  double dt;           /* dt of the last step */
+} mb_status;
+
+typedef struct mb_ctx mb_ctx;
+
+/* Reads the mesh, scheme and tables, checks the scheme ids, builds the device tables (ghost
+ * gather lists, record maps, tile lists) and the scratch state buffer. Replaces the device part of
+ * MOSE_setup (Setup_BC_Device Mod_BC.f90:99, Setup_Device_Residency Mod_Explicit.f90:404-482,
+ * cuf_init_tables Mod_Convective.f90:57-75). */
+int mb_init(const mb_mesh* mesh, const mb_scheme* scheme, const mb_thermo* thermo, int device,
+            mb_ctx** out);
+void mb_destroy(mb_ctx* ctx);
+
+/* Fill_Ghost_Cell on P (device pointer): physical ghosts, connection / periodic copies and the
+ * transverse viscous stencil of the connection records (Lib_Extrapolation.f90:1370-1528). */
+int mb_fill_ghosts(mb_ctx* ctx, double* P, void* stream);
+
+/* Fluxes + BC_Fluxes: R = sum of the face fluxes of every interior cell, in the reference's order
+ * (pass2_body.inc, then the boundary records face 1..6), from P whose ghosts are filled
+ * (Mod_Fluxes.f90:10-98, Mod_BC.f90:646-800). The parity hook: nothing else is written. */
+int mb_residual(mb_ctx* ctx, const double* P, double* R, void* stream);
+
+/* RK_Newstate (conservative form) of stage irk (1-based) with residual R and time step dt:
+ * P <- update(P, PO, R) at every interior cell (Lib_Newstate.f90:77-143, newstate_cons_body.inc). */
+int mb_update(mb_ctx* ctx, double* P, const double* PO, const double* R, int irk, double dt,
+              void* stream);
+
+/* Compute_dt: the global minimum local step of P (interior cells), written to *dt_host
+ * (Mod_dt.f90:15-243, dt_blk.inc:11-222). Synchronises the stream. */
+int mb_dt(mb_ctx* ctx, const double* P, double* dt_host, void* stream);
+
+/* One fused stage: ghost fill of the stage input, then ONE sweep that computes every face flux once,
+ * accumulates the divergence in registers and applies the RK update (and on the last stage the next
+ * step's local dt). Stage input and output buffers are chosen by the engine so that, after the last
+ * stage of a step, P holds the new state; PO is used as the engine's second buffer. */
+int mb_stage(mb_ctx* ctx, double* P, double* PO, int irk, void* stream);
+
+/* nsteps whole time steps on P (dt + stages), the dt kept on the device between steps; with
+ * use_graph != 0 one step is captured once as a CUDA graph and replayed. */
+int mb_step(mb_ctx* ctx, double* P, double* PO, int nsteps, int use_graph, void* stream);
+
+/* Sets the step's dt on the device clock from the minimum of the local steps of P (Compute_dt +
+ * Set_Global_dt + Clip_dt_To_Timemax), without a host read. Called before the first mb_stage. */
+int mb_begin_step(mb_ctx* ctx, const double* P, void* stream);
+
+/* Status (state check, thermo guard, first offender, simulated time, last dt). Synchronises. */
+int mb_get_status(mb_ctx* ctx, mb_status* st);
+
+/* Number of kernel launches this context has issued (for launch accounting). */
+int64_t mb_launch_count(const mb_ctx* ctx);
+
+/* Version string of the built library. */
+const char* mb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MOSE_B200_H */

@@ -1,0 +1,1251 @@
+// mose_oracle.cpp -- CPU restatement (FP64) of MOSE-GPU's explicit residual evaluation and
+// Runge-Kutta stage update, used ONLY as the correctness checker of the B200 engine and as the
+// timed CPU baseline of bench.py. It is test infrastructure: nothing in the product links it.
+//
+// Parity status: the reference cannot be compiled or run here (Fortran/OpenACC/CUDA-Fortran with
+// nvfortran; the FiNeR submodule is missing) and its tests ship no value-level golden vectors
+// (test/reference_1it.md5 pins the md5 of ASCII output only). This restatement is therefore pinned
+// by physics known-answers (exact Riemann solution of the Sod problem, conservation on periodic
+// meshes, Taylor-Green kinetic-energy decay) -- PARITY WITH THE REFERENCE'S OWN OUTPUT IS UNPINNED.
+//
+// Each routine cites the reference statements it restates (paths relative to the reference root)
+// and keeps their operation order (compile with -ffp-contract=off: no FMA contraction), because
+// that order is what fixes the last bits of the result:
+//   convective face         src/lib/gpu/conv_physics.inc:1-179, Mod_Convective.f90:288-412
+//   limiter                 src/lib/numerics/space/Lib_Limiters.f90:65-97 (Mod_Convective.f90:161-191)
+//   AUSM+, LMRoe            src/lib/numerics/fluxes/riemann_open_body.inc:100-150, 679-730, 965-1091
+//   HLLC at boundary faces  src/lib/numerics/fluxes/Lib_Riemann_HLL.f90:21-134, 209-310
+//   face thermo + viscous   src/lib/numerics/fluxes/Mod_Diffusive.f90:248-373, gpu/diff_cuf_kernels.inc:11-87,
+//                           gpu/diff_physics.inc:1-161
+//   pass 2                  src/lib/gpu/pass2_body.inc:1-61
+//   boundary records        numerics/fluxes/bc/bc_record_body.inc, bc_record_apply.inc, Mod_BC.f90:400-572,
+//                           Lib_BC.f90:1770-1867 (connection, Euler), 2113-2178 (connection, viscous),
+//                           1119-1165 (extrapolation)
+//   ghost fill              bc/Lib_Extrapolation.f90:590-641 (ZG, cubic), 643-730, 859-879, 1023-1191
+//   thermo cache            src/lib/physics/Mod_Thermo_Cache.f90:291-425
+//   state update            src/lib/gpu/newstate_cons_body.inc:1-89, explicit/Lib_Newstate.f90:257-307
+//   RK coefficients         explicit/Lib_RK.f90:6-9
+//   local dt                src/lib/gpu/dt_blk.inc:11-222, numerics/time/Mod_dt.f90:15-106
+//   thermo leaves           lib/FLINT/src/lib/Lib_ThermoTransport_dev.f90:54-300
+//   the step                explicit/Mod_Explicit.f90:52-279
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#include "../include/mose_b200.h"
+
+namespace {
+
+constexpr int GC = MB_GC;
+constexpr int NP = MB_NPRIM;
+constexpr int IU = 1, IV = 2, IW = 3, IP = 4;  // 0-based nu, nv, nw, np (nsc = 1: species slot 0)
+constexpr double RUNIV = 8314.46261815324;     // Lib_ThermoTransport.f90:13
+
+struct Thermo {
+  int tmin, tmax;
+  double wm, ri;                    // Ri_tab = Runiv / wm_tab (Load_ThermoTransport.f90:54)
+  std::vector<double> cp_, h_, mu_, k_;
+  const double* cp;  // indexed by the table row (T index), tmin..tmax
+  const double* h;
+  const double* mu;
+  const double* k;
+};
+
+struct Blk {
+  int n1, n2, n3, pi, pj;
+  int64_t boff;
+  const double *fm1, *fm2, *fm3, *dl, *m, *vol;
+};
+
+struct Ctx {
+  std::vector<Blk> blk;
+  std::vector<mb_bc> rec;
+  std::vector<mb_conn> conn;
+  int64_t ncell;
+  mb_scheme sc;
+  Thermo th;
+  std::vector<double> pg;  // bc_pg(nprim, 6, nrec) of the connection records
+  mb_status st;
+};
+
+// ---- indexing (MOSE_Field_m.f90:78-109; geometry shapes Mod_Convective.f90:594-596) ----
+inline int64_t row(const Blk& b, int i, int j, int k) {
+  return b.boff + (int64_t)(i + GC - 1) + (int64_t)(j + GC - 1) * b.pi + (int64_t)(k + GC - 1) * b.pi * b.pj;
+}
+inline int64_t lin(const Blk& b, int i, int j, int k) {
+  return (int64_t)(i + GC - 1) + (int64_t)(j + GC - 1) * b.pi + (int64_t)(k + GC - 1) * b.pi * b.pj;
+}
+inline const double* fm1p(const Blk& b, int i, int j, int k) {  // fm1(1:4, i, j, k), i in 0..n1
+  return b.fm1 + 4 * ((int64_t)i + (int64_t)(b.n1 + 1) * ((j - 1) + (int64_t)b.n2 * (k - 1)));
+}
+inline const double* fm2p(const Blk& b, int i, int j, int k) {
+  return b.fm2 + 4 * ((int64_t)(i - 1) + (int64_t)b.n1 * (j + (int64_t)(b.n2 + 1) * (k - 1)));
+}
+inline const double* fm3p(const Blk& b, int i, int j, int k) {
+  return b.fm3 + 4 * ((int64_t)(i - 1) + (int64_t)b.n1 * ((j - 1) + (int64_t)b.n2 * k));
+}
+inline double dlv(const Blk& b, int d, int i, int j, int k) { return b.dl[d + 3 * lin(b, i, j, k)]; }
+inline double mv(const Blk& b, int a, int c, int i, int j, int k) { return b.m[a + 3 * c + 9 * lin(b, i, j, k)]; }
+
+// ---- FLINT leaves ----
+// f_tabT_expr: Vij + (Viij - Vij) * Tdiff (Lib_ThermoTransport_dev.f90:306-314)
+inline double tabT(const double* t, int ti, double td) { return t[ti] + (t[ti + 1] - t[ti]) * td; }
+
+// The table row of a temperature: int(T), kept inside [tmin, tmax-1]. The reference clamps at some
+// call sites and indexes unchecked at others; on the table the two agree, off it (a state the thermo
+// guard / state check rejects) the unchecked form reads outside the table, which the engine must
+// never do on the GPU, so both the engine and this restatement clamp everywhere (NaN -> tmin).
+inline int tidx(const Thermo& th, double T) {
+  if (!(T >= (double)th.tmin)) return th.tmin;
+  if (T >= (double)(th.tmax - 1)) return th.tmax - 1;
+  return (int)T;
+}
+
+// co_rotot_Rtot_dev (Lib_ThermoTransport_dev.f90:107-115): rho = sum(rhoi), R = sum(Ri rhoi / rho)
+inline void rotot_rtot(const Thermo& th, double rhoi, double& rho, double& R) {
+  rho = 0.0 + rhoi;
+  R = 0.0 + th.ri * rhoi / rho;
+}
+
+// f_cp_dev (Lib_ThermoTransport_dev.f90:280-300)
+inline double f_cp(const Thermo& th, double rhoi, int ti, double td, double rho) {
+  double cpi = tabT(th.cp, ti, td);
+  return 0.0 + rhoi / rho * cpi;
+}
+
+// f_ss_dev (Lib_ThermoTransport_dev.f90:76-90): no clamp of the T index
+inline double f_ss(const Thermo& th, double rhoi, double p, double rho, double Rtot) {
+  double T = p / (Rtot * rho);
+  int ti = tidx(th, T);
+  double td = T - ti;
+  double cp = f_cp(th, rhoi, ti, td, rho);
+  double gam = cp / (cp - Rtot);
+  return std::sqrt(gam * Rtot * T);
+}
+
+// H0_dev (Lib_ThermoTransport_dev.f90:54-73)
+inline double H0(const Thermo& th, double p, double rhoi, double u) {
+  double rho = 0.0 + rhoi;
+  double Rgas = 0.0 + th.ri * rhoi / rho;
+  double T = p / (Rgas * rho);
+  int ti = tidx(th, T);
+  double td = T - ti;
+  double e = 0.0 + tabT(th.h, ti, td) * rhoi / rho;
+  return e + 0.5 * u * u;
+}
+
+// f_molecularWeight + co_fiij_dev + co_k_mi_lam_Wilke_dev for one species
+// (Lib_ThermoTransport_dev.f90:118-184, 316-345)
+inline void wilke(const Thermo& th, double rhoi, double rho, int ti, double td, double& mil, double& kl) {
+  double rho_ = 0.0 + rhoi;
+  double wmt = 0.0 + (rhoi / rho_ / th.wm);
+  wmt = 1.0 / wmt;
+  double xi = rhoi * wmt / (rho * th.wm);
+  double mi = tabT(th.mu, ti, td);
+  double ki = tabT(th.k, ti, td);
+  // co_fiij_dev: Mi_Mj_pow_m025(1,1) = 1, inv_sqrt8_1p(1,1) = 1/sqrt(16)
+  double sq_num = std::sqrt(mi);
+  double inv_den = 1.0 / std::sqrt(mi + 1e-20);
+  const double pw = std::pow(th.wm / th.wm, -0.25);
+  const double is8 = 1.0 / std::sqrt(8.0 * (1.0 + th.wm / th.wm));
+  double ratio = sq_num * inv_den * pw;
+  double one_plus = 1.0 + ratio;
+  double fi = one_plus * one_plus * is8;
+  double lam_den = 0.0 + xi * fi;
+  double inv_ld = 1.0 / lam_den;
+  mil = 0.0 + xi * mi * inv_ld;
+  kl = 0.0 + xi * ki * inv_ld;
+}
+
+// ---- limiter (Lib_Limiters.f90:65-97) ----
+inline double rlimiter(int lim, double x, double y) {
+  double ru, phi;
+  switch (lim) {
+    case 1: {
+      if (x * y < 0.0) return 0.0;
+      double r = x;
+      if (std::fabs(x) > std::fabs(y)) r = y;
+      return r;
+    }
+    case 2:
+      ru = y / (x + 1e-30);
+      phi = (ru + std::fabs(ru)) / (1.0 + std::fabs(ru));
+      return phi * x;
+    case 3:
+      ru = y / (x + 1e-30);
+      phi = (ru * ru + ru) / (1.0 + ru * ru);
+      return phi * x;
+    case 4:
+      ru = y / (x + 1e-30);
+      phi = std::max(0.0, std::min(std::min(2.0 * ru, 0.5 * (1.0 + ru)), 2.0));
+      return phi * x;
+    case 5:
+      ru = y / (x + 1e-30);
+      phi = std::max(std::max(0.0, std::min(2.0 * ru, 1.0)), std::min(ru, 2.0));
+      return phi * x;
+    default:
+      return 0.0;
+  }
+}
+
+inline double fsign_half(double f) { return std::copysign(0.5, f); }
+
+// ---- the MOSE_open solvers of riemann_open_body.inc used here: AUSM+ (4), LMRoe (12) ----
+// Thermo as written there: T clamped to [tmin, tmax-1] before the table lookup (H / H0 of FLINT).
+inline double h_static(const Thermo& th, double rhoi, double p) {
+  double rho_ = 0.0 + rhoi;
+  double rg = 0.0 + th.ri * rhoi / rho_;
+  double T = p / (rg * rho_);
+  double Tc = std::max((double)th.tmin, std::min(T, (double)(th.tmax - 1)));
+  int ti = (int)Tc;
+  double td = Tc - ti;
+  int t1 = std::max(th.tmin, std::min(ti, th.tmax));
+  int t2 = std::max(th.tmin, std::min(ti + 1, th.tmax));
+  double hs = th.h[t1] + (th.h[t2] - th.h[t1]) * td;
+  return 0.0 + hs * rhoi / rho_;
+}
+
+void riemann_open(const Thermo& th, int rs, double mco, double dl, double ul, double vl, double wl,
+                  double pl, double al, double dltot, double dr, double ur, double vr, double wr, double pr,
+                  double ar, double drtot, double nx, double ny, double nz, double& F_r, double& F_u,
+                  double& F_v, double& F_w, double& F_E) {
+  double unl = ul * nx + vl * ny + wl * nz;
+  double unr = ur * nx + vr * ny + wr * nz;
+  if (rs == 4) {  // riemann_open_body.inc:100-150
+    const double ab = 0.125, aa = 0.1875;
+    double vel = std::sqrt(ul * ul + vl * vl + wl * wl);
+    double H_L = h_static(th, dl, pl) + 0.5 * vel * vel;
+    vel = std::sqrt(ur * ur + vr * vr + wr * wr);
+    double H_R = h_static(th, dr, pr) + 0.5 * vel * vel;
+    double a_half = std::sqrt(al * ar);
+    double ML = unl / a_half, MR = unr / a_half;
+    double MplusL, pplusL, MminusR, pminusR;
+    if (std::fabs(ML) < 1.0) {
+      MplusL = 0.25 * ((ML + 1.0) * (ML + 1.0)) + ab * ((ML * ML - 1.0) * (ML * ML - 1.0));
+      pplusL = 0.25 * ((ML + 1.0) * (ML + 1.0)) * (2.0 - ML) + aa * ML * ((ML * ML - 1.0) * (ML * ML - 1.0));
+    } else {
+      MplusL = 0.5 * (ML + std::fabs(ML));
+      pplusL = 0.5 * (1.0 + std::copysign(1.0, ML));
+    }
+    if (std::fabs(MR) < 1.0) {
+      MminusR = -0.25 * ((MR - 1.0) * (MR - 1.0)) - ab * ((MR * MR - 1.0) * (MR * MR - 1.0));
+      pminusR = 0.25 * ((MR - 1.0) * (MR - 1.0)) * (2.0 + MR) - aa * MR * ((MR * MR - 1.0) * (MR * MR - 1.0));
+    } else {
+      MminusR = 0.5 * (MR - std::fabs(MR));
+      pminusR = 0.5 * (1.0 - std::copysign(1.0, MR));
+    }
+    double Mhalf = MplusL + MminusR;
+    double phalf = pplusL * pl + pminusR * pr;
+    double mdotp = dltot * a_half * 0.5 * (Mhalf + std::fabs(Mhalf));
+    double mdotm = drtot * a_half * 0.5 * (Mhalf - std::fabs(Mhalf));
+    F_r = mdotp + mdotm;
+    F_u = mdotp * ul + mdotm * ur + nx * phalf;
+    F_v = mdotp * vl + mdotm * vr + ny * phalf;
+    F_w = mdotp * wl + mdotm * wr + nz * phalf;
+    F_E = mdotp * H_L + mdotm * H_R;
+    return;
+  }
+  // rs == 12: Roe averages (riemann_open_body.inc:679-730) then LMRoe (:965-1091)
+  double rho_ = 0.0 + dl;
+  double Rl = 0.0 + th.ri * dl / rho_;
+  rho_ = 0.0 + dr;
+  double Rr = 0.0 + th.ri * dr / rho_;
+  double inv_dltot = 1.0 / dltot, inv_drtot = 1.0 / drtot;
+  double Tl = pl * inv_dltot / Rl, Tr = pr * inv_drtot / Rr;
+  int Til = tidx(th, Tl);
+  int Tir = tidx(th, Tr);
+  double dTl = Tl - Til, dTr = Tr - Tir;
+  double srL = std::sqrt(dltot), srR = std::sqrt(drtot);
+  double inv_sr = 1.0 / (srL + srR);
+  double rho_roe = srL * srR;
+  double u_roe = (srR * ur + srL * ul) * inv_sr;
+  double v_roe = (srR * vr + srL * vl) * inv_sr;
+  double w_roe = (srR * wr + srL * wl) * inv_sr;
+  double R_roe = (srR * Rr + srL * Rl) * inv_sr;
+  double T_roe = (srR * Tr + srL * Tl) * inv_sr;
+  double h0l = 0.0, h0r = 0.0, cv_roe = 0.0, sum_ei = 0.0;
+  {
+    double invW = RUNIV / th.wm;
+    double hl = th.h[Til] + (th.h[Til + 1] - th.h[Til]) * dTl;
+    double hr = th.h[Tir] + (th.h[Tir + 1] - th.h[Tir]) * dTr;
+    double el = hl - invW * Tl, er = hr - invW * Tr;
+    h0l = h0l + hl * dl * inv_dltot;
+    h0r = h0r + hr * dr * inv_drtot;
+    double d_roe = (srR * dr * inv_drtot + srL * dl * inv_dltot) * inv_sr;
+    cv_roe = cv_roe + d_roe * (0.5 * (th.cp[Til] + (th.cp[Til + 1] - th.cp[Til]) * dTl + th.cp[Tir] +
+                                      (th.cp[Tir + 1] - th.cp[Tir]) * dTr) - invW);
+    sum_ei = sum_ei + d_roe * (srR * er + srL * el) * inv_sr;
+  }
+  h0l = h0l + 0.5 * (ul * ul + vl * vl + wl * wl);
+  h0r = h0r + 0.5 * (ur * ur + vr * vr + wr * wr);
+  double h0_roe = (srR * h0r + srL * h0l) * inv_sr;
+  double gam_roe = 1.0 + R_roe / cv_roe;
+  double vel2 = u_roe * u_roe + v_roe * v_roe + w_roe * w_roe;
+  double a_roe = std::sqrt((gam_roe - 1.0) * (h0_roe - 0.5 * vel2 + cv_roe * T_roe - sum_ei));
+  double nmag = std::sqrt(nx * nx + ny * ny + nz * nz);
+  if (nmag <= 0.0) { F_r = F_u = F_v = F_w = F_E = 0.0; return; }
+  double n1 = nx / nmag, n2 = ny / nmag, n3 = nz / nmag;
+  double tx, ty, tz;
+  if (std::fabs(n1) < 0.9) { tx = 1.0; ty = 0.0; tz = 0.0; } else { tx = 0.0; ty = 1.0; tz = 0.0; }
+  double t1x = tx - (tx * n1 + ty * n2 + tz * n3) * n1;
+  double t1y = ty - (tx * n1 + ty * n2 + tz * n3) * n2;
+  double t1z = tz - (tx * n1 + ty * n2 + tz * n3) * n3;
+  double tmag = std::sqrt(t1x * t1x + t1y * t1y + t1z * t1z);
+  if (tmag <= 0.0) { t1x = -n2; t1y = n1; t1z = 0.0; tmag = std::sqrt(t1x * t1x + t1y * t1y + t1z * t1z); }
+  t1x = t1x / tmag; t1y = t1y / tmag; t1z = t1z / tmag;
+  double t2x = n2 * t1z - n3 * t1y;
+  double t2y = n3 * t1x - n1 * t1z;
+  double t2z = n1 * t1y - n2 * t1x;
+  double unL = ul * n1 + vl * n2 + wl * n3, unR = ur * n1 + vr * n2 + wr * n3;
+  double ut1L = ul * t1x + vl * t1y + wl * t1z, ut1R = ur * t1x + vr * t1y + wr * t1z;
+  double ut2L = ul * t2x + vl * t2y + wl * t2z, ut2R = ur * t2x + vr * t2y + wr * t2z;
+  double hL = h_static(th, dl, pl), hR = h_static(th, dr, pr);
+  double H0L = hL + 0.5 * (ul * ul + vl * vl + wl * wl);
+  double H0R = hR + 0.5 * (ur * ur + vr * vr + wr * wr);
+  double FL1 = dltot * unL, FL2 = dltot * unL * ul + pl * n1, FL3 = dltot * unL * vl + pl * n2;
+  double FL4 = dltot * unL * wl + pl * n3, FL5 = dltot * unL * H0L;
+  double FR1 = drtot * unR, FR2 = drtot * unR * ur + pr * n1, FR3 = drtot * unR * vr + pr * n2;
+  double FR4 = drtot * unR * wr + pr * n3, FR5 = drtot * unR * H0R;
+  double unRoe = u_roe * n1 + v_roe * n2 + w_roe * n3;
+  double u2 = u_roe * u_roe + v_roe * v_roe + w_roe * w_roe;
+  double utmag = std::sqrt(std::max(0.0, u2 - unRoe * unRoe));
+  double Ma = (a_roe > 0.0) ? (std::fabs(unRoe) + utmag) / a_roe : 1.0;
+  double phi = std::max(mco, std::min(1.0, Ma));
+  double drho = drtot - dltot, dp = pr - pl, dun = unR - unL;
+  double dut1 = ut1R - ut1L, dut2 = ut2R - ut2L;
+  double dunmod = phi * dun;
+  double abs1 = std::fabs(unRoe - a_roe), abs2 = std::fabs(unRoe), abs3 = std::fabs(unRoe),
+         abs4 = std::fabs(unRoe), abs5 = std::fabs(unRoe + a_roe);
+  double a2 = a_roe * a_roe, inva = 1.0 / a_roe, inva2 = 1.0 / a2;
+  double al4 = drho - dp * inva2;
+  double al2 = rho_roe * dut1, al3 = rho_roe * dut2;
+  double al1 = 0.5 * (dp * inva2 - rho_roe * dunmod * inva);
+  double al5 = 0.5 * (dp * inva2 + rho_roe * dunmod * inva);
+  double r1[5] = {1.0, u_roe - a_roe * n1, v_roe - a_roe * n2, w_roe - a_roe * n3, h0_roe - a_roe * unRoe};
+  double r5[5] = {1.0, u_roe + a_roe * n1, v_roe + a_roe * n2, w_roe + a_roe * n3, h0_roe + a_roe * unRoe};
+  double r4[5] = {1.0, u_roe, v_roe, w_roe, 0.5 * u2};
+  double r2[5] = {0.0, t1x, t1y, t1z, u_roe * t1x + v_roe * t1y + w_roe * t1z};
+  double r3[5] = {0.0, t2x, t2y, t2z, u_roe * t2x + v_roe * t2y + w_roe * t2z};
+  double d[5];
+  for (int q = 0; q < 5; ++q)
+    d[q] = abs1 * al1 * r1[q] + abs2 * al2 * r2[q] + abs3 * al3 * r3[q] + abs4 * al4 * r4[q] + abs5 * al5 * r5[q];
+  F_r = 0.5 * (FL1 + FR1) - 0.5 * d[0];
+  F_u = 0.5 * (FL2 + FR2) - 0.5 * d[1];
+  F_v = 0.5 * (FL3 + FR3) - 0.5 * d[2];
+  F_w = 0.5 * (FL4 + FR4) - 0.5 * d[3];
+  F_E = 0.5 * (FL5 + FR5) - 0.5 * d[4];
+}
+
+// HLLC of Lib_Riemann_HLL.f90:21-134 with roe_averages :209-310 (boundary records; no T clamp)
+void riemann_hllc_bc(const Thermo& th, double dl, double ul, double vl, double wl, double pl, double al,
+                     double dltot, double dr, double ur, double vr, double wr, double pr, double ar, double drtot,
+                     double nx, double ny, double nz, double& F_r, double& F_u, double& F_v, double& F_w,
+                     double& F_E) {
+  double unl = ul * nx + vl * ny + wl * nz;
+  double unr = ur * nx + vr * ny + wr * nz;
+  double Rl = 0.0 + th.ri * dl / (0.0 + dl);
+  double Rr = 0.0 + th.ri * dr / (0.0 + dr);
+  double inv_dltot = 1.0 / dltot, inv_drtot = 1.0 / drtot;
+  double Tl = pl * inv_dltot / Rl, Tr = pr * inv_drtot / Rr;
+  int Til = tidx(th, Tl), Tir = tidx(th, Tr);
+  double dTl = Tl - Til, dTr = Tr - Tir;
+  double srL = std::sqrt(dltot), srR = std::sqrt(drtot);
+  double inv_sr = 1.0 / (srL + srR);
+  double u_roe = (srR * ur + srL * ul) * inv_sr;
+  double v_roe = (srR * vr + srL * vl) * inv_sr;
+  double w_roe = (srR * wr + srL * wl) * inv_sr;
+  double R_roe = (srR * Rr + srL * Rl) * inv_sr;
+  double T_roe = (srR * Tr + srL * Tl) * inv_sr;
+  double h0l = 0.0, h0r = 0.0, cv_roe = 0.0, sum_ei = 0.0;
+  {
+    double invW = RUNIV / th.wm;
+    double hl = th.h[Til] + (th.h[Til + 1] - th.h[Til]) * dTl;
+    double hr = th.h[Tir] + (th.h[Tir + 1] - th.h[Tir]) * dTr;
+    double el = hl - invW * Tl, er = hr - invW * Tr;
+    h0l = h0l + hl * dl * inv_dltot;
+    h0r = h0r + hr * dr * inv_drtot;
+    double d_roe = (srR * dr * inv_drtot + srL * dl * inv_dltot) * inv_sr;
+    cv_roe = cv_roe + d_roe * (0.5 * (th.cp[Til] + (th.cp[Til + 1] - th.cp[Til]) * dTl + th.cp[Tir] +
+                                      (th.cp[Tir + 1] - th.cp[Tir]) * dTr) - invW);
+    sum_ei = sum_ei + d_roe * (srR * er + srL * el) * inv_sr;
+  }
+  h0l = h0l + 0.5 * (ul * ul + vl * vl + wl * wl);
+  h0r = h0r + 0.5 * (ur * ur + vr * vr + wr * wr);
+  double h0_roe = (srR * h0r + srL * h0l) * inv_sr;
+  double gam_roe = 1.0 + R_roe / cv_roe;
+  double vel2 = u_roe * u_roe + v_roe * v_roe + w_roe * w_roe;
+  double a_roe = std::sqrt((gam_roe - 1.0) * (h0_roe - 0.5 * vel2 + cv_roe * T_roe - sum_ei));
+  double un_roe = u_roe * nx + v_roe * ny + w_roe * nz;
+  double e0l = h0l - pl / dltot, e0r = h0r - pr / drtot;
+  double S1 = std::min(std::min(0.0, unl - al), un_roe - a_roe);
+  double S4 = std::max(std::max(0.0, unr + ar), un_roe + a_roe);
+  double inv_denom = 1.0 / (dltot * (S1 - unl) - drtot * (S4 - unr));
+  double Sstar = (pr - pl + dltot * unl * (S1 - unl) - drtot * unr * (S4 - unr)) * inv_denom;
+  double pstar = dltot * (unl - S1) * (unl - Sstar) + pl;
+  if (S1 >= 0.0) {
+    F_r = dltot * unl; F_u = F_r * ul + pl * nx; F_v = F_r * vl + pl * ny; F_w = F_r * wl + pl * nz; F_E = F_r * h0l;
+  } else if (Sstar >= 0.0) {
+    F_r = dltot * unl; F_u = F_r * ul + pl * nx; F_v = F_r * vl + pl * ny; F_w = F_r * wl + pl * nz; F_E = F_r * h0l;
+    inv_denom = 1.0 / (S1 - Sstar);
+    double U1S = dltot * (S1 - unl) * inv_denom;
+    double U2S = ((S1 - unl) * dltot * ul + (pstar - pl) * nx) * inv_denom;
+    double U3S = ((S1 - unl) * dltot * vl + (pstar - pl) * ny) * inv_denom;
+    double U4S = ((S1 - unl) * dltot * wl + (pstar - pl) * nz) * inv_denom;
+    double U5S = ((S1 - unl) * dltot * e0l - pl * unl + pstar * Sstar) * inv_denom;
+    F_r = F_r + S1 * (U1S - dltot); F_u = F_u + S1 * (U2S - dltot * ul); F_v = F_v + S1 * (U3S - dltot * vl);
+    F_w = F_w + S1 * (U4S - dltot * wl); F_E = F_E + S1 * (U5S - dltot * e0l);
+  } else if (S4 > 0.0) {
+    F_r = drtot * unr; F_u = F_r * ur + pr * nx; F_v = F_r * vr + pr * ny; F_w = F_r * wr + pr * nz; F_E = F_r * h0r;
+    inv_denom = 1.0 / (S4 - Sstar);
+    double U1S = drtot * (S4 - unr) * inv_denom;
+    double U2S = ((S4 - unr) * drtot * ur + (pstar - pr) * nx) * inv_denom;
+    double U3S = ((S4 - unr) * drtot * vr + (pstar - pr) * ny) * inv_denom;
+    double U4S = ((S4 - unr) * drtot * wr + (pstar - pr) * nz) * inv_denom;
+    double U5S = ((S4 - unr) * drtot * e0r - pr * unr + pstar * Sstar) * inv_denom;
+    F_r = F_r + S4 * (U1S - drtot); F_u = F_u + S4 * (U2S - drtot * ur); F_v = F_v + S4 * (U3S - drtot * vr);
+    F_w = F_w + S4 * (U4S - drtot * wr); F_E = F_E + S4 * (U5S - drtot * e0r);
+  } else {
+    F_r = drtot * unr; F_u = F_r * ur + pr * nx; F_v = F_r * vr + pr * ny; F_w = F_r * wr + pr * nz; F_E = F_r * h0r;
+  }
+}
+
+// ---- one interior convective face: conv_physics.inc:1-179 ----
+void conv_face(const Ctx& c, const double* pm1, const double* p0, const double* pp1, const double* pp2,
+               const double* dlc, const double* nrm, double area, double* res0) {
+  const Thermo& th = c.th;
+  const int limv = c.sc.limiter, rsv = c.sc.riemann;
+  double l0 = 0.5 * (dlc[0] + dlc[1]), l1 = 0.5 * (dlc[1] + dlc[2]), l2 = 0.5 * (dlc[2] + dlc[3]);
+  double lm = 0.5 * dlc[1], lp = 0.5 * dlc[2];
+  const double beta_order = 1.0;
+  double idl0 = 1.0 / l0, idl1 = 1.0 / l1, idl2 = 1.0 / l2;
+  double P1[NP], P4[NP];
+  for (int s = 0; s < NP; ++s) {
+    double slope0 = (p0[s] - pm1[s]) * idl0;
+    double slope1 = (pp1[s] - p0[s]) * idl1;
+    double slope2 = (pp2[s] - pp1[s]) * idl2;
+    double slopel = rlimiter(limv, slope1, slope0);
+    double sloper = rlimiter(limv, slope2, slope1);
+    P1[s] = p0[s] + beta_order * slopel * lm;
+    P4[s] = pp1[s] - beta_order * sloper * lp;
+  }
+  P1[0] = std::max(P1[0], 1e-20);
+  P4[0] = std::max(P4[0], 1e-20);
+  double rotot1 = 0.0 + P1[0];
+  double Rtot1 = 0.0 + th.ri * P1[0] / rotot1;
+  double rotot4 = 0.0 + P4[0];
+  double Rtot4 = 0.0 + th.ri * P4[0] / rotot4;
+  double T1d = P1[IP] / (Rtot1 * rotot1);
+  int Ti1 = tidx(th, T1d);
+  double Tdiffd = T1d - Ti1;
+  double cpd = 0.0 + P1[0] / rotot1 * (th.cp[Ti1] + (th.cp[Ti1 + 1] - th.cp[Ti1]) * Tdiffd);
+  double gamd = cpd / (cpd - Rtot1);
+  double a1 = std::sqrt(gamd * Rtot1 * T1d);
+  double T4d = P4[IP] / (Rtot4 * rotot4);
+  int Ti4 = tidx(th, T4d);
+  Tdiffd = T4d - Ti4;
+  cpd = 0.0 + P4[0] / rotot4 * (th.cp[Ti4] + (th.cp[Ti4 + 1] - th.cp[Ti4]) * Tdiffd);
+  gamd = cpd / (cpd - Rtot4);
+  double a4 = std::sqrt(gamd * Rtot4 * T4d);
+  double dltot = rotot1, drtot = rotot4;
+  double ul = P1[IU], vl = P1[IV], wl = P1[IW], pl = P1[IP], al = a1;
+  double ur = P4[IU], vr = P4[IV], wr = P4[IW], pr = P4[IP], ar = a4;
+  double nx = nrm[0], ny = nrm[1], nz = nrm[2];
+  double F_r, F_u, F_v, F_w, F_E;
+  if (rsv == 1) {
+    double unl = ul * nx + vl * ny + wl * nz;
+    double unr = ur * nx + vr * ny + wr * nz;
+    double Rl = Rtot1, Rr = Rtot4;
+    double inv_dltot = 1.0 / dltot, inv_drtot = 1.0 / drtot;
+    double Tl = pl * inv_dltot / Rl, Tr = pr * inv_drtot / Rr;
+    int Til = tidx(th, Tl);
+    int Tir = tidx(th, Tr);
+    double dTl = Tl - Til, dTr = Tr - Tir;
+    double srL = std::sqrt(dltot), srR = std::sqrt(drtot), inv_sr = 1.0 / (srL + srR);
+    double u_roe = (srR * ur + srL * ul) * inv_sr, v_roe = (srR * vr + srL * vl) * inv_sr,
+           w_roe = (srR * wr + srL * wl) * inv_sr;
+    double R_roe = (srR * Rr + srL * Rl) * inv_sr, T_roe = (srR * Tr + srL * Tl) * inv_sr;
+    double h0l = 0.0, h0r = 0.0, cv_roe = 0.0, sum_ei = 0.0;
+    {
+      double invW = RUNIV / th.wm;
+      double hl = th.h[Til] + (th.h[Til + 1] - th.h[Til]) * dTl;
+      double hr = th.h[Tir] + (th.h[Tir + 1] - th.h[Tir]) * dTr;
+      double el = hl - invW * Tl, er = hr - invW * Tr;
+      h0l = h0l + hl * P1[0] * inv_dltot;
+      h0r = h0r + hr * P4[0] * inv_drtot;
+      double d_roe = (srR * P4[0] * inv_drtot + srL * P1[0] * inv_dltot) * inv_sr;
+      cv_roe = cv_roe + d_roe * (0.5 * (th.cp[Til] + (th.cp[Til + 1] - th.cp[Til]) * dTl + th.cp[Tir] +
+                                        (th.cp[Tir + 1] - th.cp[Tir]) * dTr) - invW);
+      sum_ei = sum_ei + d_roe * (srR * er + srL * el) * inv_sr;
+    }
+    h0l = h0l + 0.5 * (ul * ul + vl * vl + wl * wl);
+    h0r = h0r + 0.5 * (ur * ur + vr * vr + wr * wr);
+    double h0_roe = (srR * h0r + srL * h0l) * inv_sr;
+    double gam_roe = 1.0 + R_roe / cv_roe;
+    double vel2 = u_roe * u_roe + v_roe * v_roe + w_roe * w_roe;
+    double a_roe = std::sqrt((gam_roe - 1.0) * (h0_roe - 0.5 * vel2 + cv_roe * T_roe - sum_ei));
+    double un_roe = u_roe * nx + v_roe * ny + w_roe * nz;
+    double e0l = h0l - pl / dltot, e0r = h0r - pr / drtot;
+    double S1 = std::min(std::min(0.0, unl - al), un_roe - a_roe);
+    double S4 = std::max(std::max(0.0, unr + ar), un_roe + a_roe);
+    double inv_denom = 1.0 / (dltot * (S1 - unl) - drtot * (S4 - unr));
+    double Sstar = (pr - pl + dltot * unl * (S1 - unl) - drtot * unr * (S4 - unr)) * inv_denom;
+    double pstar = dltot * (unl - S1) * (unl - Sstar) + pl;
+    if (S1 >= 0.0) {
+      F_r = dltot * unl; F_u = F_r * ul + pl * nx; F_v = F_r * vl + pl * ny; F_w = F_r * wl + pl * nz; F_E = F_r * h0l;
+    } else if (Sstar >= 0.0) {
+      F_r = dltot * unl; F_u = F_r * ul + pl * nx; F_v = F_r * vl + pl * ny; F_w = F_r * wl + pl * nz; F_E = F_r * h0l;
+      inv_denom = 1.0 / (S1 - Sstar);
+      double U1S = dltot * (S1 - unl) * inv_denom;
+      double U2S = ((S1 - unl) * dltot * ul + (pstar - pl) * nx) * inv_denom;
+      double U3S = ((S1 - unl) * dltot * vl + (pstar - pl) * ny) * inv_denom;
+      double U4S = ((S1 - unl) * dltot * wl + (pstar - pl) * nz) * inv_denom;
+      double U5S = ((S1 - unl) * dltot * e0l - pl * unl + pstar * Sstar) * inv_denom;
+      F_r = F_r + S1 * (U1S - dltot); F_u = F_u + S1 * (U2S - dltot * ul); F_v = F_v + S1 * (U3S - dltot * vl);
+      F_w = F_w + S1 * (U4S - dltot * wl); F_E = F_E + S1 * (U5S - dltot * e0l);
+    } else if (S4 > 0.0) {
+      F_r = drtot * unr; F_u = F_r * ur + pr * nx; F_v = F_r * vr + pr * ny; F_w = F_r * wr + pr * nz; F_E = F_r * h0r;
+      inv_denom = 1.0 / (S4 - Sstar);
+      double U1S = drtot * (S4 - unr) * inv_denom;
+      double U2S = ((S4 - unr) * drtot * ur + (pstar - pr) * nx) * inv_denom;
+      double U3S = ((S4 - unr) * drtot * vr + (pstar - pr) * ny) * inv_denom;
+      double U4S = ((S4 - unr) * drtot * wr + (pstar - pr) * nz) * inv_denom;
+      double U5S = ((S4 - unr) * drtot * e0r - pr * unr + pstar * Sstar) * inv_denom;
+      F_r = F_r + S4 * (U1S - drtot); F_u = F_u + S4 * (U2S - drtot * ur); F_v = F_v + S4 * (U3S - drtot * vr);
+      F_w = F_w + S4 * (U4S - drtot * wr); F_E = F_E + S4 * (U5S - drtot * e0r);
+    } else {
+      F_r = drtot * unr; F_u = F_r * ur + pr * nx; F_v = F_r * vr + pr * ny; F_w = F_r * wr + pr * nz; F_E = F_r * h0r;
+    }
+  } else {
+    riemann_open(th, rsv, c.sc.mco, P1[0], ul, vl, wl, pl, al, dltot, P4[0], ur, vr, wr, pr, ar, drtot, nx, ny, nz,
+                 F_r, F_u, F_v, F_w, F_E);
+  }
+  double su = fsign_half(F_r), sp = 0.5 + su, sm = su - 0.5;
+  double irotot1 = 1.0 / rotot1, irotot4 = 1.0 / rotot4;
+  res0[0] = F_r * area * (sp * (P1[0] * irotot1) - sm * (P4[0] * irotot4));
+  res0[IU] = F_u * area; res0[IV] = F_v * area; res0[IW] = F_w * area; res0[IP] = F_E * area;
+}
+
+// face thermo of the diffusive flux: Diffusive_Face_Thermo_Fill (Mod_Diffusive.f90:311-325)
+// and Diffusive_Face_State (Mod_Diffusive.f90:748-776): the same statements
+void face_thermo(const Ctx& c, double rhoi, double p, double& rho, double& T, int& ti, double& td, double& cp,
+                 double& mil, double& kl) {
+  double Rgas;
+  rotot_rtot(c.th, rhoi, rho, Rgas);
+  T = p / (rho * Rgas);
+  ti = tidx(c.th, T);
+  td = T - ti;
+  cp = f_cp(c.th, rhoi, ti, td, rho);
+  wilke(c.th, rhoi, rho, ti, td, mil, kl);
+  if (c.sc.prandtl > 0.0) kl = mil * cp / c.sc.prandtl;
+}
+
+// the cell temperature / density of the thermo cache (Mod_Thermo_Cache.f90:327-330,378-380)
+inline void cell_rho_T(const Ctx& c, const double* P, int64_t nc, int64_t r, double& rho, double& T) {
+  double Rg;
+  rotot_rtot(c.th, P[r], rho, Rg);
+  T = P[r + IP * nc] / (rho * Rg);
+}
+
+// ---- one interior viscous face: diff_cuf_kernels.inc:11-87 + diff_physics.inc:1-161 (laminar) ----
+// cells: 1,2 the face pair; 3,4 (-/+ along axis ib) of cell 1; 5,6 of cell 2; 7,8 along ic of cell 1; 9,10 of cell 2
+void visc_face(const Ctx& c, const Blk& b, const double* P, int dir, int i, int j, int k, double* res0) {
+  const int64_t nc = c.ncell;
+  const Thermo& th = c.th;
+  int ia, ib, ic;
+  int o[3] = {0, 0, 0};
+  o[dir] = 1;
+  if (dir == 0) { ia = 0; ib = 1; ic = 2; } else if (dir == 1) { ia = 1; ib = 0; ic = 2; } else { ia = 2; ib = 0; ic = 1; }
+  int eb[3] = {0, 0, 0}, ec[3] = {0, 0, 0};
+  eb[ib] = 1; ec[ic] = 1;
+  int64_t cc[10];
+  cc[0] = row(b, i, j, k);
+  cc[1] = row(b, i + o[0], j + o[1], k + o[2]);
+  cc[2] = row(b, i - eb[0], j - eb[1], k - eb[2]);
+  cc[3] = row(b, i + eb[0], j + eb[1], k + eb[2]);
+  cc[4] = row(b, i + o[0] - eb[0], j + o[1] - eb[1], k + o[2] - eb[2]);
+  cc[5] = row(b, i + o[0] + eb[0], j + o[1] + eb[1], k + o[2] + eb[2]);
+  cc[6] = row(b, i - ec[0], j - ec[1], k - ec[2]);
+  cc[7] = row(b, i + ec[0], j + ec[1], k + ec[2]);
+  cc[8] = row(b, i + o[0] - ec[0], j + o[1] - ec[1], k + o[2] - ec[2]);
+  cc[9] = row(b, i + o[0] + ec[0], j + o[1] + ec[1], k + o[2] + ec[2]);
+  double rho_n[10], T_n[10];
+  for (int q = 0; q < 10; ++q) cell_rho_T(c, P, nc, cc[q], rho_n[q], T_n[q]);
+  auto w = [&](int q, int s) { return P[cc[q] + (int64_t)s * nc]; };
+  double G[NP][3];
+  double irho1 = 1.0 / rho_n[0], irho2 = 1.0 / rho_n[1];
+  G[0][ia] = w(1, 0) * irho2 - w(0, 0) * irho1;
+  G[IP][ia] = T_n[1] - T_n[0];
+  for (int s = IU; s <= IW; ++s) G[s][ia] = w(1, s) - w(0, s);
+  double irt1 = 1.0 / rho_n[2], irt2 = 1.0 / rho_n[3], irt3 = 1.0 / rho_n[4], irt4 = 1.0 / rho_n[5];
+  G[0][ib] = (w(3, 0) * irt2 - w(2, 0) * irt1 + w(5, 0) * irt4 - w(4, 0) * irt3) * 0.25;
+  G[IP][ib] = (T_n[3] - T_n[2] + T_n[5] - T_n[4]) * 0.25;
+  for (int s = IU; s <= IW; ++s) G[s][ib] = (w(3, s) - w(2, s) + w(5, s) - w(4, s)) * 0.25;
+  irt1 = 1.0 / rho_n[6]; irt2 = 1.0 / rho_n[7]; irt3 = 1.0 / rho_n[8]; irt4 = 1.0 / rho_n[9];
+  G[0][ic] = (w(7, 0) * irt2 - w(6, 0) * irt1 + w(9, 0) * irt4 - w(8, 0) * irt3) * 0.25;
+  G[IP][ic] = (T_n[7] - T_n[6] + T_n[9] - T_n[8]) * 0.25;
+  for (int s = IU; s <= IW; ++s) G[s][ic] = (w(7, s) - w(6, s) + w(9, s) - w(8, s)) * 0.25;
+  double Mav[3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int q = 0; q < 3; ++q)
+      Mav[a][q] = 0.5 * (mv(b, a, q, i, j, k) + mv(b, a, q, i + o[0], j + o[1], k + o[2]));
+  for (int iv = 0; iv < NP; ++iv) {
+    double g1 = G[iv][0], g2 = G[iv][1], g3 = G[iv][2];
+    G[iv][0] = g1 * Mav[0][0] + g2 * Mav[1][0] + g3 * Mav[2][0];
+    G[iv][1] = g1 * Mav[0][1] + g2 * Mav[1][1] + g3 * Mav[2][1];
+    G[iv][2] = g1 * Mav[0][2] + g2 * Mav[1][2] + g3 * Mav[2][2];
+  }
+  double Pf[NP];
+  for (int iv = 0; iv < NP; ++iv) Pf[iv] = 0.5 * (w(0, iv) + w(1, iv));
+  // face thermo from the face-averaged species density and pressure (tface)
+  double frs = 0.5 * (w(0, 0) + w(1, 0));
+  double fp = 0.5 * (w(0, IP) + w(1, IP));
+  double drho, dT, dcp, dmil, dkl;
+  int tint; double tdf0;
+  face_thermo(c, frs, fp, drho, dT, tint, tdf0, dcp, dmil, dkl);
+  const double* nrm;
+  if (dir == 0) nrm = fm1p(b, i, j, k); else if (dir == 1) nrm = fm2p(b, i, j, k); else nrm = fm3p(b, i, j, k);
+  double area = nrm[3];
+  int Ti = tidx(th, dT);
+  double Tdf = dT - Ti;
+  double Gv[3][3];
+  for (int dd = 0; dd < 3; ++dd) { Gv[0][dd] = G[IU][dd]; Gv[1][dd] = G[IV][dd]; Gv[2][dd] = G[IW][dd]; }
+  const double mie = 0.0;
+  const double sct = 0.9, prt = 0.85;
+  double Dm = (dmil / c.sc.schmidt + mie / sct) / drho;
+  double kappaf = dkl + mie * dcp / prt;
+  double dmi = dmil + mie;
+  const double ntt = -2.0 / 3.0;
+  double dlam = ntt * dmi;
+  double Diver = Gv[0][0] + Gv[1][1] + Gv[2][2];
+  double lamDiv = dlam * Diver;
+  const double rhokd = 0.0;
+  double Txx = lamDiv + 2.0 * dmi * Gv[0][0] + rhokd;
+  double Tyy = lamDiv + 2.0 * dmi * Gv[1][1] + rhokd;
+  double Tzz = lamDiv + 2.0 * dmi * Gv[2][2] + rhokd;
+  double Txy = dmi * (Gv[0][1] + Gv[1][0]), Txz = dmi * (Gv[0][2] + Gv[2][0]), Tyz = dmi * (Gv[1][2] + Gv[2][1]);
+  double S1 = Txx * nrm[0] + Txy * nrm[1] + Txz * nrm[2];
+  double S2 = Txy * nrm[0] + Tyy * nrm[1] + Tyz * nrm[2];
+  double S3 = Txz * nrm[0] + Tyz * nrm[1] + Tzz * nrm[2];
+  double DiffH = 0.0;
+  double Flx[NP] = {0, 0, 0, 0, 0};
+  double DmGY = Dm * (G[0][0] * nrm[0] + G[0][1] * nrm[1] + G[0][2] * nrm[2]);
+  Flx[0] = drho * area * DmGY;
+  double hh1 = th.h[Ti], hh2 = th.h[Ti + 1];
+  double hh = hh1 + Tdf * (hh2 - hh1);
+  DiffH = DiffH + DmGY * hh;
+  double sflx = 0.0 + Flx[0];
+  Flx[0] = Flx[0] - sflx * Pf[0] / drho;
+  Flx[IU] = area * S1; Flx[IV] = area * S2; Flx[IW] = area * S3;
+  Flx[IP] = area * ((S1 * Pf[IU] + S2 * Pf[IV] + S3 * Pf[IW]) +
+                    kappaf * (G[IP][0] * nrm[0] + G[IP][1] * nrm[1] + G[IP][2] * nrm[2]) + DiffH * drho);
+  for (int s = 0; s < NP; ++s) res0[s] = Flx[s];
+}
+
+// ---- boundary records (bc_record_body.inc + bc_record_apply.inc) ----
+// Compute_Diffusive_Flux_St (Mod_Diffusive.f90:781-867), laminar
+void diff_flux_st(const Ctx& c, const double* Pa, const double G[NP][3], double area, const double* nrm, double rho,
+                  int ti, double td, double cp, double mil, double kl, double* F) {
+  const double mie = 0.0, sct = 0.9, prt = 0.85;
+  double Gv[3][3];
+  for (int dd = 0; dd < 3; ++dd) { Gv[0][dd] = G[IU][dd]; Gv[1][dd] = G[IV][dd]; Gv[2][dd] = G[IW][dd]; }
+  double Dm = (mil / c.sc.schmidt + mie / sct) / rho;
+  double kappa = kl + mie * cp / prt;
+  // Stress_Vector_Std (physics/turbulence/Mod_Fluid.f90:20-44)
+  double mi = mil + mie;
+  double lam = (-2.0 / 3.0) * mi;
+  double Div = Gv[0][0] + Gv[1][1] + Gv[2][2];
+  double lamDiv = lam * Div;
+  double Txx = lamDiv + 2.0 * mi * Gv[0][0], Tyy = lamDiv + 2.0 * mi * Gv[1][1], Tzz = lamDiv + 2.0 * mi * Gv[2][2];
+  double Txy = mi * (Gv[0][1] + Gv[1][0]), Txz = mi * (Gv[0][2] + Gv[2][0]), Tyz = mi * (Gv[1][2] + Gv[2][1]);
+  double S[3];
+  S[0] = Txx * nrm[0] + Txy * nrm[1] + Txz * nrm[2];
+  S[1] = Txy * nrm[0] + Tyy * nrm[1] + Tyz * nrm[2];
+  S[2] = Txz * nrm[0] + Tyz * nrm[1] + Tzz * nrm[2];
+  double DiffH = 0.0;
+  for (int s = 0; s < NP; ++s) F[s] = 0.0;
+  double DmG = Dm * (G[0][0] * nrm[0] + G[0][1] * nrm[1] + G[0][2] * nrm[2]);
+  F[0] = rho * area * DmG;
+  double hh1 = c.th.h[ti], hh2 = c.th.h[ti + 1];
+  double hh = hh1 + td * (hh2 - hh1);
+  DiffH = DiffH + DmG * hh;
+  double sum = 0.0 + F[0];
+  F[0] = F[0] - sum * Pa[0] / rho;
+  F[IU] = area * S[0]; F[IV] = area * S[1]; F[IW] = area * S[2];
+  F[IP] = area * ((S[0] * Pa[IU] + S[1] * Pa[IV] + S[2] * Pa[IW]) +
+                  kappa * (G[IP][0] * nrm[0] + G[IP][1] * nrm[1] + G[IP][2] * nrm[2]) + DiffH * rho);
+}
+
+void bc_face_geom(const Blk& b, int Im, int Jm, int Km, int Fm, double* nrm, double& area) {
+  int dir = (Fm + 1) / 2, modfm = Fm % 2;
+  const double* f;
+  if (dir == 1) f = fm1p(b, Im - modfm, Jm, Km);
+  else if (dir == 2) f = fm2p(b, Im, Jm - modfm, Km);
+  else f = fm3p(b, Im, Jm, Km - modfm);
+  nrm[0] = f[0]; nrm[1] = f[1]; nrm[2] = f[2]; area = f[3];
+}
+
+// BC_Connection_Eul_lean (Lib_BC.f90:1770-1867)
+void bc_connection_eul(const Ctx& c, const Blk& b, const double* P, double* R, int Im, int Jm, int Km, int Fm) {
+  const int64_t nc = c.ncell;
+  const Thermo& th = c.th;
+  int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm1 = 1 - modfm, modfm2 = 1 - 2 * modfm, gstep = 2 * modfm - 1;
+  int o1 = modfm * (-gstep * GC) + modfm1 * (gstep), o2 = modfm * (-gstep), o3 = modfm1 * (-gstep),
+      o4 = modfm1 * (-gstep * GC) + modfm * (gstep);
+  int e[3] = {0, 0, 0};
+  e[dir - 1] = 1;
+  int64_t r1 = row(b, Im + o1 * e[0], Jm + o1 * e[1], Km + o1 * e[2]);
+  int64_t r2 = row(b, Im + o2 * e[0], Jm + o2 * e[1], Km + o2 * e[2]);
+  int64_t r3 = row(b, Im + o3 * e[0], Jm + o3 * e[1], Km + o3 * e[2]);
+  int64_t r4 = row(b, Im + o4 * e[0], Jm + o4 * e[1], Km + o4 * e[2]);
+  double dlc4[4];
+  dlc4[0] = dlv(b, dir - 1, Im + o1 * e[0], Jm + o1 * e[1], Km + o1 * e[2]);
+  dlc4[1] = dlv(b, dir - 1, Im + o2 * e[0], Jm + o2 * e[1], Km + o2 * e[2]);
+  dlc4[2] = dlv(b, dir - 1, Im + o3 * e[0], Jm + o3 * e[1], Km + o3 * e[2]);
+  dlc4[3] = dlv(b, dir - 1, Im + o4 * e[0], Jm + o4 * e[1], Km + o4 * e[2]);
+  double nrm[3], area;
+  bc_face_geom(b, Im, Jm, Km, Fm, nrm, area);
+  const double beta_ = 1.0;
+  double Dl1 = dlc4[0] * 0.5, Dl2 = dlc4[1] * 0.5, Dl3 = dlc4[2] * 0.5, Dl4 = dlc4[3] * 0.5;
+  double D12 = Dl1 + Dl2, D23 = Dl2 + Dl3, D34 = Dl3 + Dl4;
+  double PL[NP], PR[NP];
+  for (int s = 0; s < NP; ++s) {
+    double q1 = P[r1 + s * nc], q2 = P[r2 + s * nc], q3 = P[r3 + s * nc], q4 = P[r4 + s * nc];
+    double d21 = (q2 - q1) / D12, d32 = (q3 - q2) / D23, d43 = (q4 - q3) / D34;
+    PL[s] = q2 + beta_ * rlimiter(c.sc.limiter, d32, d21) * Dl2;
+    PR[s] = q3 - beta_ * rlimiter(c.sc.limiter, d43, d32) * Dl3;
+  }
+  double rhoL, RL, rhoR, RR;
+  rotot_rtot(th, PL[0], rhoL, RL);
+  double aL = f_ss(th, PL[0], PL[IP], rhoL, RL);
+  rotot_rtot(th, PR[0], rhoR, RR);
+  double aR = f_ss(th, PR[0], PR[IP], rhoR, RR);
+  double F_r, F_u, F_v, F_w, F_E;
+  if (c.sc.riemann == 1)
+    riemann_hllc_bc(th, PL[0], PL[IU], PL[IV], PL[IW], PL[IP], aL, rhoL, PR[0], PR[IU], PR[IV], PR[IW], PR[IP], aR, rhoR,
+                    nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E);
+  else
+    riemann_open(th, c.sc.riemann, c.sc.mco, PL[0], PL[IU], PL[IV], PL[IW], PL[IP], aL, rhoL, PR[0], PR[IU], PR[IV],
+                 PR[IW], PR[IP], aR, rhoR, nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E);
+  double su = fsign_half(F_r), selL = 0.5 + su, selR = su - 0.5;
+  double Fmass = F_r * area;
+  int64_t rm = row(b, Im, Jm, Km);
+  double sg = (double)modfm2;
+  R[rm] = R[rm] + sg * Fmass * (selL * PL[0] / rhoL - selR * PR[0] / rhoR);
+  R[rm + IU * nc] = R[rm + IU * nc] + sg * F_u * area;
+  R[rm + IV * nc] = R[rm + IV * nc] + sg * F_v * area;
+  R[rm + IW * nc] = R[rm + IW * nc] + sg * F_w * area;
+  R[rm + IP * nc] = R[rm + IP * nc] + sg * F_E * area;
+}
+
+// BC_Connection_Visc_lean (Lib_BC.f90:2113-2178): pg = bc_pg(:, 1:6) of the record
+void bc_connection_visc(const Ctx& c, const Blk& b, const double* P, double* R, int Im, int Jm, int Km, int Fm,
+                        const double* pg) {
+  const int64_t nc = c.ncell;
+  int dir = (Fm + 1) / 2, modfm2 = 1 - 2 * (Fm % 2), gstep = 2 * (Fm % 2) - 1;
+  int ia = dir - 1, ib, ic;
+  int bm[3] = {Im, Jm, Km}, bp[3] = {Im, Jm, Km}, cm[3] = {Im, Jm, Km}, cp[3] = {Im, Jm, Km};
+  if (dir == 1) { ib = 1; ic = 2; bm[1] = Jm - 1; bp[1] = Jm + 1; cm[2] = Km - 1; cp[2] = Km + 1; }
+  else if (dir == 2) { ib = 0; ic = 2; bm[0] = Im - 1; bp[0] = Im + 1; cm[2] = Km - 1; cp[2] = Km + 1; }
+  else { ib = 0; ic = 1; bm[0] = Im - 1; bp[0] = Im + 1; cm[1] = Jm - 1; cp[1] = Jm + 1; }
+  int g[3] = {Im, Jm, Km};
+  g[dir - 1] -= gstep;
+  double M[3][3];
+  for (int q = 0; q < 3; ++q)
+    for (int a = 0; a < 3; ++a) M[a][q] = 0.5 * (mv(b, a, q, Im, Jm, Km) + mv(b, a, q, g[0], g[1], g[2]));
+  int64_t r1 = row(b, Im, Jm, Km), r3 = row(b, bp[0], bp[1], bp[2]), r4 = row(b, bm[0], bm[1], bm[2]),
+          r5 = row(b, cp[0], cp[1], cp[2]), r6 = row(b, cm[0], cm[1], cm[2]);
+  auto pv = [&](int q, int s) -> double {
+    switch (q) {
+      case 0: return P[r1 + s * nc];
+      case 1: return pg[s + NP * 0];
+      case 2: return P[r3 + s * nc];
+      case 3: return P[r4 + s * nc];
+      case 4: return P[r5 + s * nc];
+      case 5: return P[r6 + s * nc];
+      default: return pg[s + NP * (q - 4)];  // q = 6..9 -> Pg(:,3..6)
+    }
+  };
+  double rh[10], rg[10];
+  for (int q = 0; q < 10; ++q) rotot_rtot(c.th, pv(q, 0), rh[q], rg[q]);
+  double G2l[NP][3], G2g[NP][3], Pa[NP];
+  for (int s = 0; s < NP; ++s) {
+    double vv[10];
+    for (int q = 0; q < 10; ++q) {
+      double x = pv(q, s);
+      if (s >= IU && s <= IW) vv[q] = x;
+      else if (s == IP) vv[q] = x / (rh[q] * rg[q]);
+      else vv[q] = x / rh[q];
+    }
+    double gl[3], gg[3];
+    gl[ia] = (vv[1] - vv[0]) * (double)modfm2;
+    gl[ib] = (vv[2] - vv[3]) * 0.5;
+    gl[ic] = (vv[4] - vv[5]) * 0.5;
+    gg[ia] = (vv[0] - vv[1]) * (double)(-modfm2);
+    gg[ib] = (vv[7] - vv[6]) * 0.5;
+    gg[ic] = (vv[9] - vv[8]) * 0.5;
+    for (int kk = 0; kk < 3; ++kk) {
+      G2l[s][kk] = gl[0] * M[0][kk] + gl[1] * M[1][kk] + gl[2] * M[2][kk];
+      G2g[s][kk] = gg[0] * M[0][kk] + gg[1] * M[1][kk] + gg[2] * M[2][kk];
+    }
+    Pa[s] = 0.5 * (pv(0, s) + pv(1, s));
+  }
+  double rho_f, T_f, td, cp_f, mil_f, kl_f;
+  int ti;
+  face_thermo(c, Pa[0], Pa[IP], rho_f, T_f, ti, td, cp_f, mil_f, kl_f);
+  double nrm[3], area;
+  bc_face_geom(b, Im, Jm, Km, Fm, nrm, area);
+  double Fl[NP], Fg[NP];
+  diff_flux_st(c, Pa, G2l, area, nrm, rho_f, ti, td, cp_f, mil_f, kl_f, Fl);
+  diff_flux_st(c, Pa, G2g, area, nrm, rho_f, ti, td, cp_f, mil_f, kl_f, Fg);
+  for (int s = 0; s < NP; ++s) R[r1 + s * nc] = R[r1 + s * nc] - 0.5 * (double)modfm2 * (Fl[s] + Fg[s]);
+}
+
+// BC_Extrapolation (Lib_BC.f90:1119-1165)
+void bc_extrapolation(const Ctx& c, const Blk& b, const double* P, double* R, int Im, int Jm, int Km, int Fm) {
+  const int64_t nc = c.ncell;
+  int64_t r = row(b, Im, Jm, Km);
+  double Pr[NP];
+  for (int s = 0; s < NP; ++s) Pr[s] = P[r + s * nc];
+  double nrm[3], area;
+  bc_face_geom(b, Im, Jm, Km, Fm, nrm, area);
+  double Un = Pr[IU] * nrm[0] + Pr[IV] * nrm[1] + Pr[IW] * nrm[2];
+  double F[NP];
+  double Fmass = 0.0;
+  F[0] = Pr[0] * Un * area;
+  Fmass = Fmass + F[0];
+  F[IU] = Fmass * Pr[IU] + Pr[IP] * area * nrm[0];
+  F[IV] = Fmass * Pr[IV] + Pr[IP] * area * nrm[1];
+  F[IW] = Fmass * Pr[IW] + Pr[IP] * area * nrm[2];
+  double vmag = std::sqrt(Pr[IU] * Pr[IU] + Pr[IV] * Pr[IV] + Pr[IW] * Pr[IW]);
+  F[IP] = Fmass * H0(c.th, Pr[IP], Pr[0], vmag);
+  double sg = (double)(1 - 2 * (Fm % 2));
+  for (int s = 0; s < NP; ++s) R[r + s * nc] = R[r + s * nc] + sg * F[s];
+}
+
+// ---- ghost fill ----
+inline int64_t rowg(const Ctx& c, int blk, int i, int j, int k) { return row(c.blk[blk], i, j, k); }
+
+void fill_ghosts(Ctx& c, double* P) {
+  const int64_t nc = c.ncell;
+  // Fill_Ghost_Cell_blk: zero-gradient for type 11 / 4, cubic extrapolation for walls (Lib_Extrapolation.f90:643-730)
+  for (const mb_bc& r : c.rec) {
+    const Blk& b = c.blk[r.blk];
+    int dir = (r.face + 1) / 2, gstep = 2 * (r.face % 2) - 1;
+    int e[3] = {0, 0, 0};
+    e[dir - 1] = 1;
+    if (r.type == MB_BC_EXTRAPOLATION || r.type == MB_BC_INFLOW) {
+      int64_t src = row(b, r.i, r.j, r.k);
+      for (int g = 1; g <= GC; ++g) {
+        int64_t dst = row(b, r.i - gstep * g * e[0], r.j - gstep * g * e[1], r.k - gstep * g * e[2]);
+        for (int s = 0; s < NP; ++s) P[dst + s * nc] = P[src + s * nc];
+      }
+    } else if (r.type == MB_BC_WALL) {
+      int step = -gstep;
+      for (int g = 1; g <= GC; ++g) {
+        int64_t d0 = row(b, r.i + g * step * e[0], r.j + g * step * e[1], r.k + g * step * e[2]);
+        int64_t a1 = row(b, r.i + (g - 1) * step * e[0], r.j + (g - 1) * step * e[1], r.k + (g - 1) * step * e[2]);
+        int64_t a2 = row(b, r.i + (g - 2) * step * e[0], r.j + (g - 2) * step * e[1], r.k + (g - 2) * step * e[2]);
+        int64_t a3 = row(b, r.i + (g - 3) * step * e[0], r.j + (g - 3) * step * e[1], r.k + (g - 3) * step * e[2]);
+        for (int s = 0; s < NP; ++s)
+          P[d0 + s * nc] = 3.0 * P[a1 + s * nc] - 3.0 * P[a2 + s * nc] + P[a3 + s * nc];
+      }
+    }
+  }
+  // extrapolation-ghost = cubic on the 400 faces (Fill_Ghost_Cubic_Extrapolation_blk, :859-879)
+  for (const mb_bc& r : c.rec) {
+    if (r.type != MB_BC_EXTRAPOLATION) continue;
+    const Blk& b = c.blk[r.blk];
+    int dir = (r.face + 1) / 2, gstep = 2 * (r.face % 2) - 1, step = -gstep;
+    int e[3] = {0, 0, 0};
+    e[dir - 1] = 1;
+    for (int g = 1; g <= GC; ++g) {
+      int64_t d0 = row(b, r.i + g * step * e[0], r.j + g * step * e[1], r.k + g * step * e[2]);
+      int64_t a1 = row(b, r.i + (g - 1) * step * e[0], r.j + (g - 1) * step * e[1], r.k + (g - 1) * step * e[2]);
+      int64_t a2 = row(b, r.i + (g - 2) * step * e[0], r.j + (g - 2) * step * e[1], r.k + (g - 2) * step * e[2]);
+      int64_t a3 = row(b, r.i + (g - 3) * step * e[0], r.j + (g - 3) * step * e[1], r.k + (g - 3) * step * e[2]);
+      for (int s = 0; s < NP; ++s) P[d0 + s * nc] = 3.0 * P[a1 + s * nc] - 3.0 * P[a2 + s * nc] + P[a3 + s * nc];
+    }
+  }
+  // connection / periodic copies (Ghost_Connection_pair, :1023-1134): receiver ghost layer g <- donor layer g
+  // guide(F) = the inward unit step of face F
+  auto guide = [](int F, int ax) { int d = (F + 1) / 2 - 1; return ax == d ? ((F % 2) ? 1 : -1) : 0; };
+  for (const mb_conn& cn : c.conn) {
+    const mb_bc& r = c.rec[cn.rec];
+    for (int g = 1; g <= GC; ++g) {
+      int64_t dst = rowg(c, r.blk, r.i - guide(r.face, 0) * g, r.j - guide(r.face, 1) * g, r.k - guide(r.face, 2) * g);
+      int64_t src = rowg(c, cn.bs, cn.is + guide(cn.fs, 0) * (g - 1), cn.js + guide(cn.fs, 1) * (g - 1),
+                         cn.ks + guide(cn.fs, 2) * (g - 1));
+      for (int s = 0; s < NP; ++s) P[dst + s * nc] = P[src + s * nc];
+    }
+  }
+  // bc_pg: layers 1-2 and the four transverse neighbours of the donor face cell, after every ghost write
+  // (Ghost_Connection_pairs_B, :1136-1191)
+  for (size_t q = 0; q < c.conn.size(); ++q) {
+    const mb_conn& cn = c.conn[q];
+    double* pg = &c.pg[(size_t)cn.rec * 6 * NP];
+    int64_t s1 = rowg(c, cn.bs, cn.is, cn.js, cn.ks);
+    int64_t s2 = rowg(c, cn.bs, cn.is + guide(cn.fs, 0), cn.js + guide(cn.fs, 1), cn.ks + guide(cn.fs, 2));
+    int I = cn.is, J = cn.js, K = cn.ks;
+    int t[4][3];
+    if (cn.fs <= 2) {
+      int a[4][3] = {{I, J - cn.d11, K - cn.d12}, {I, J + cn.d11, K + cn.d12}, {I, J - cn.d21, K - cn.d22}, {I, J + cn.d21, K + cn.d22}};
+      std::memcpy(t, a, sizeof(t));
+    } else if (cn.fs <= 4) {
+      int a[4][3] = {{I - cn.d11, J, K - cn.d12}, {I + cn.d11, J, K + cn.d12}, {I - cn.d21, J, K - cn.d22}, {I + cn.d21, J, K + cn.d22}};
+      std::memcpy(t, a, sizeof(t));
+    } else {
+      int a[4][3] = {{I - cn.d11, J - cn.d12, K}, {I + cn.d11, J + cn.d12, K}, {I - cn.d21, J - cn.d22, K}, {I + cn.d21, J + cn.d22, K}};
+      std::memcpy(t, a, sizeof(t));
+    }
+    for (int s = 0; s < NP; ++s) {
+      pg[s + NP * 0] = P[s1 + s * nc];
+      pg[s + NP * 1] = P[s2 + s * nc];
+      for (int m = 0; m < 4; ++m) pg[s + NP * (2 + m)] = P[rowg(c, cn.bs, t[m][0], t[m][1], t[m][2]) + s * nc];
+    }
+  }
+}
+
+// ---- residual: pass 1 + pass 2 (Mod_Fluxes.f90:188-390) + BC_Fluxes (Mod_BC.f90:646-800) ----
+void residual(Ctx& c, const double* P, double* R) {
+  const int64_t nc = c.ncell;
+  const bool visc = c.sc.visc != 0;
+  for (const Blk& b : c.blk) {
+    const int n1 = b.n1, n2 = b.n2, n3 = b.n3;
+    const int64_t nf1 = (int64_t)(n1 - 1) * n2 * n3, nf2 = (int64_t)n1 * (n2 - 1) * n3, nf3 = (int64_t)n1 * n2 * (n3 - 1);
+    std::vector<double> fh[3], dfh[3];
+    fh[0].assign(std::max<int64_t>(nf1, 0) * NP, 0.0);
+    fh[1].assign(std::max<int64_t>(nf2, 0) * NP, 0.0);
+    fh[2].assign(std::max<int64_t>(nf3, 0) * NP, 0.0);
+    if (visc) { dfh[0].assign(fh[0].size(), 0.0); dfh[1].assign(fh[1].size(), 0.0); dfh[2].assign(fh[2].size(), 0.0); }
+    // pass 1: the interior faces of each direction (conv_cuf_i/j/k, diff_cuf_i/j/k)
+    for (int d = 0; d < 3; ++d) {
+      int h1 = n1, h2 = n2, h3 = n3;
+      if (d == 0) h1 = n1 - 1; else if (d == 1) h2 = n2 - 1; else h3 = n3 - 1;
+      if (h1 < 1 || h2 < 1 || h3 < 1) continue;
+#pragma omp parallel for collapse(2) schedule(static)
+      for (int k = 1; k <= h3; ++k)
+        for (int j = 1; j <= h2; ++j)
+          for (int i = 1; i <= h1; ++i) {
+            int e[3] = {0, 0, 0};
+            e[d] = 1;
+            double pm1[NP], p0[NP], pp1[NP], pp2[NP], dlc[4], res0[NP];
+            int64_t r0 = row(b, i, j, k);
+            int64_t st = e[0] + (int64_t)e[1] * b.pi + (int64_t)e[2] * b.pi * b.pj;
+            for (int s = 0; s < NP; ++s) {
+              pm1[s] = P[r0 - st + s * nc]; p0[s] = P[r0 + s * nc];
+              pp1[s] = P[r0 + st + s * nc]; pp2[s] = P[r0 + 2 * st + s * nc];
+            }
+            for (int q = -1; q <= 2; ++q) dlc[q + 1] = dlv(b, d, i + q * e[0], j + q * e[1], k + q * e[2]);
+            const double* f = (d == 0) ? fm1p(b, i, j, k) : (d == 1) ? fm2p(b, i, j, k) : fm3p(b, i, j, k);
+            conv_face(c, pm1, p0, pp1, pp2, dlc, f, f[3], res0);
+            int64_t fi;
+            if (d == 0) fi = (i - 1) + (int64_t)(j - 1) * (n1 - 1) + (int64_t)(k - 1) * (n1 - 1) * n2;
+            else if (d == 1) fi = (i - 1) + (int64_t)(j - 1) * n1 + (int64_t)(k - 1) * n1 * (n2 - 1);
+            else fi = (i - 1) + (int64_t)(j - 1) * n1 + (int64_t)(k - 1) * n1 * n2;
+            for (int s = 0; s < NP; ++s) fh[d][fi * NP + s] = res0[s];
+            if (visc) {
+              visc_face(c, b, P, d, i, j, k, res0);
+              for (int s = 0; s < NP; ++s) dfh[d][fi * NP + s] = res0[s];
+            }
+          }
+    }
+    // pass 2 (pass2_body.inc): R of every interior cell, written once
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 1; k <= n3; ++k)
+      for (int j = 1; j <= n2; ++j)
+        for (int i = 1; i <= n1; ++i) {
+          double t[NP] = {0, 0, 0, 0, 0};
+          auto add = [&](const std::vector<double>& v, int64_t f, double sg) {
+            for (int s = 0; s < NP; ++s) t[s] = (sg > 0) ? t[s] + v[f * NP + s] : t[s] - v[f * NP + s];
+          };
+          auto f1 = [&](int ii) { return (ii - 1) + (int64_t)(j - 1) * (n1 - 1) + (int64_t)(k - 1) * (n1 - 1) * n2; };
+          auto f2 = [&](int jj) { return (i - 1) + (int64_t)(jj - 1) * n1 + (int64_t)(k - 1) * n1 * (n2 - 1); };
+          auto f3 = [&](int kk) { return (i - 1) + (int64_t)(j - 1) * n1 + (int64_t)(kk - 1) * n1 * n2; };
+          if (i < n1) add(fh[0], f1(i), 1); if (i > 1) add(fh[0], f1(i - 1), -1);
+          if (j < n2) add(fh[1], f2(j), 1); if (j > 1) add(fh[1], f2(j - 1), -1);
+          if (k < n3) add(fh[2], f3(k), 1); if (k > 1) add(fh[2], f3(k - 1), -1);
+          if (visc) {
+            if (i < n1) add(dfh[0], f1(i), -1); if (i > 1) add(dfh[0], f1(i - 1), 1);
+            if (j < n2) add(dfh[1], f2(j), -1); if (j > 1) add(dfh[1], f2(j - 1), 1);
+            if (k < n3) add(dfh[2], f3(k), -1); if (k > 1) add(dfh[2], f3(k - 1), 1);
+          }
+          int64_t r0 = row(b, i, j, k);
+          for (int s = 0; s < NP; ++s) R[r0 + s * nc] = t[s];
+        }
+  }
+  // boundary records, one face index at a time (the per-cell add order of Mod_BC.f90:449-485)
+  for (int f = 1; f <= 6; ++f) {
+    const int nr = (int)c.rec.size();
+#pragma omp parallel for schedule(static)
+    for (int q = 0; q < nr; ++q) {
+      const mb_bc& r = c.rec[q];
+      if (r.face != f) continue;
+      const Blk& b = c.blk[r.blk];
+      switch (r.type) {
+        case MB_BC_CONNECTION:
+          bc_connection_eul(c, b, P, R, r.i, r.j, r.k, r.face);
+          if (visc) bc_connection_visc(c, b, P, R, r.i, r.j, r.k, r.face, &c.pg[(size_t)q * 6 * NP]);
+          break;
+        case MB_BC_EXTRAPOLATION:
+          bc_extrapolation(c, b, P, R, r.i, r.j, r.k, r.face);
+          break;
+        default:
+          break;
+      }
+    }
+  }
+}
+
+// ---- state update: newstate_cons_body.inc ----
+static const double RKC[4][4] = {{1.0, 0.0, 0.0, 0.0}, {1.0, 0.50, 0.0, 0.0}, {1.0, 0.25, 2.0 / 3.0, 0.0}, {0, 0, 0, 0}};
+
+void update_cell(const Ctx& c, const double* po, double* p, const double* res, double vol, double dt, double rkc,
+                 double tc) {
+  const Thermo& th = c.th;
+  const double strang = 1.0;
+  double cons[NP], cold[NP], rl[NP];
+  auto prim2cons = [&](const double* q, double* u) {
+    double rho = 0.0 + q[0];
+    double Rg = 0.0 + th.ri * q[0] / rho;
+    double vmag = 0.0;
+    for (int s = IU; s <= IW; ++s) vmag = vmag + q[s] * q[s];
+    double Tl = q[IP] / (Rg * rho);
+    int ti = tidx(th, Tl);
+    double Td = Tl - ti;
+    double hs = th.h[ti] + Td * (th.h[ti + 1] - th.h[ti]);
+    double hmix = 0.0 + hs * q[0] / rho;
+    double E0 = hmix - q[IP] / rho + 0.5 * vmag;
+    u[0] = q[0];
+    for (int s = IU; s <= IW; ++s) u[s] = rho * q[s];
+    u[IP] = rho * E0;
+  };
+  prim2cons(po, cold);
+  prim2cons(p, cons);
+  for (int s = 0; s < NP; ++s) rl[s] = -res[s] / vol * dt * strang;
+  for (int s = 0; s < NP; ++s) cons[s] = cold[s] + (cons[s] - cold[s] + rl[s]) * rkc;
+  double rho = 0.0 + cons[0];
+  double Rg = 0.0 + th.ri * cons[0] / rho;
+  p[0] = cons[0];
+  for (int s = IU; s <= IW; ++s) p[s] = cons[s] / rho;
+  double vmag = 0.0;
+  for (int s = IU; s <= IW; ++s) vmag = vmag + (cons[s] / rho) * (cons[s] / rho);
+  double energy = cons[IP] / rho - 0.5 * vmag;
+  double diff_en = 1e3, T_it = tc;
+  int it = 1;
+  while ((std::fabs(diff_en / energy) >= 1e-6) && (it <= 20)) {
+    int ti = tidx(th, T_it);
+    double Td = T_it - ti;
+    double cv = -Rg, enth = 0.0;
+    double cps = th.cp[ti] + Td * (th.cp[ti + 1] - th.cp[ti]);
+    double hs = th.h[ti] + Td * (th.h[ti + 1] - th.h[ti]);
+    cv = cv + cons[0] / rho * cps;
+    enth = enth + cons[0] / rho * hs;
+    double p_it = rho * Rg * T_it;
+    diff_en = std::fabs((enth - p_it / rho) - energy);
+    T_it = T_it + (energy - (enth - p_it / rho)) / cv;
+    it = it + 1;
+  }
+  p[IP] = rho * Rg * T_it;
+  if (p[0] < 1e-20) p[0] = 1e-20;
+}
+
+void update(Ctx& c, double* P, const double* PO, const double* R, int irk, double dt) {
+  const int64_t nc = c.ncell;
+  const double rkc = RKC[c.sc.n_rk - 1][irk - 1];
+  const bool guard = c.sc.visc != 0;
+  int nbad = 0, nth = 0;
+  for (size_t bi = 0; bi < c.blk.size(); ++bi) {
+    const Blk& b = c.blk[bi];
+#pragma omp parallel for collapse(2) schedule(static) reduction(+ : nbad, nth)
+    for (int k = 1; k <= b.n3; ++k)
+      for (int j = 1; j <= b.n2; ++j)
+        for (int i = 1; i <= b.n1; ++i) {
+          int64_t r = row(b, i, j, k);
+          double p[NP], po[NP], res[NP];
+          for (int s = 0; s < NP; ++s) { p[s] = P[r + s * nc]; po[s] = PO[r + s * nc]; res[s] = R[r + s * nc]; }
+          double rho, T;
+          cell_rho_T(c, P, nc, r, rho, T);
+          if (guard && !(T > 1.0 && T < 9990.0)) {  // thermo guard (Mod_Thermo_Cache.f90:317-327)
+            ++nth;
+            if (T != T) T = 300.0;
+            T = std::min(std::max(T, 1.0), 9990.0);
+          }
+          update_cell(c, po, p, res, b.vol[lin(b, i, j, k)], dt, rkc, T);
+          bool bad = !(p[IP] >= 0.0);
+          for (int s = 0; s < NP; ++s) if (!std::isfinite(p[s])) bad = true;
+          if (bad) ++nbad;
+          for (int s = 0; s < NP; ++s) P[r + s * nc] = p[s];
+        }
+  }
+  c.st.n_bad_state += nbad;
+  c.st.n_bad_thermo += nth;
+  if (nth && c.st.code == MB_OK) c.st.code = MB_E_THERMO;
+  if (nbad && c.sc.state_check && c.st.code == MB_OK) c.st.code = MB_E_STATE;
+}
+
+// ---- local dt: dt_blk.inc (min rule) + Thermo_Cache_rrt_blk / _visc_blk ----
+double compute_dt(Ctx& c, const double* P) {
+  const int64_t nc = c.ncell;
+  const Thermo& th = c.th;
+  double dtglobal = 1e5;  // Mod_Explicit.f90:122
+  for (const Blk& b : c.blk) {
+#pragma omp parallel for collapse(2) schedule(static) reduction(min : dtglobal)
+    for (int k = 1; k <= b.n3; ++k)
+      for (int j = 1; j <= b.n2; ++j)
+        for (int i = 1; i <= b.n1; ++i) {
+          int64_t r = row(b, i, j, k);
+          double pl[NP];
+          for (int s = 0; s < NP; ++s) pl[s] = P[r + s * nc];
+          double rho, Rg;
+          rotot_rtot(th, pl[0], rho, Rg);
+          double Tc = pl[IP] / (rho * Rg);
+          double Sound = f_ss(th, pl[0], pl[IP], rho, Rg);
+          double dtc = 1e8;
+          if (c.sc.dt_additive) {  // dt-rule = additive (dt_blk.inc:79-155)
+            double ra_c = 0.0, ra_v = 0.0;
+            for (int d = 0; d < c.sc.ndir; ++d) {
+              double m0 = mv(b, d, 0, i, j, k), m1 = mv(b, d, 1, i, j, k), m2 = mv(b, d, 2, i, j, k);
+              double gn = std::sqrt(m0 * m0 + m1 * m1 + m2 * m2);
+              double vel_ = std::fabs(pl[IU] * m0 + pl[IV] * m1 + pl[IW] * m2) / gn;
+              double lambda = vel_ + Sound;
+              ra_c = ra_c + lambda * gn;
+              ra_v = ra_v + gn * gn;
+            }
+            if (c.sc.visc) {
+              if (c.sc.ndir == 3) {
+                double g[3][3];
+                for (int d = 0; d < 3; ++d) for (int a = 0; a < 3; ++a) g[d][a] = mv(b, d, a, i, j, k);
+                auto dot = [&](int p, int q) { return g[p][0] * g[q][0] + g[p][1] * g[q][1] + g[p][2] * g[q][2]; };
+                auto nr = [&](int p) { return std::sqrt(g[p][0] * g[p][0] + g[p][1] * g[p][1] + g[p][2] * g[p][2]); };
+                double c12 = dot(0, 1) / (nr(0) * nr(1)), c13 = dot(0, 2) / (nr(0) * nr(2)), c23 = dot(1, 2) / (nr(1) * nr(2));
+                double ss = c12 * c12 + c13 * c13 + c23 * c23;
+                double qp = c12 * c13 * c23;
+                if (ss + 2.0 * qp > 1.0) {
+                  double mr = 2.0 * std::sqrt(ss / 3.0) *
+                              std::cos(std::acos(std::max(-1.0, std::min(1.0, 3.0 * std::sqrt(3.0) * qp / std::pow(ss, 1.5)))) / 3.0);
+                  ra_v = ra_v * 0.25 * (2.0 + mr + 1.0 / mr);
+                }
+              }
+              double Ta = pl[IP] / (rho * Rg);
+              int ta = tidx(th, Ta);
+              double tda = Ta - ta;
+              double cpa = f_cp(th, pl[0], ta, tda, rho);
+              double cva = cpa - Rg;
+              double mila, kla;
+              wilke(th, pl[0], rho, ta, tda, mila, kla);
+              if (c.sc.prandtl > 0.0) kla = mila * cpa / c.sc.prandtl;
+              const double mie = 0.0, prt = 0.85;
+              double Dmx = std::max(4.0 / 3.0 * (mila + mie) / rho, (kla + mie * cpa / prt) / (rho * cva));
+              dtc = 1.0 / (ra_c / c.sc.cfl + Dmx * ra_v / c.sc.vnn);
+            } else {
+              dtc = c.sc.cfl / ra_c;
+            }
+          } else {
+          for (int d = 0; d < c.sc.ndir; ++d) {
+            double m0 = mv(b, d, 0, i, j, k), m1 = mv(b, d, 1, i, j, k), m2 = mv(b, d, 2, i, j, k);
+            double nrm = std::sqrt(m0 * m0 + m1 * m1 + m2 * m2);
+            double v0 = m0 / nrm, v1 = m1 / nrm, v2 = m2 / nrm;
+            double vel_ = std::fabs(pl[IU] * v0 + pl[IV] * v1 + pl[IW] * v2);
+            double lambda = vel_ + Sound;
+            double dtd = dlv(b, d, i, j, k) / lambda * c.sc.cfl;
+            dtc = std::min(dtd, dtc);
+          }
+          if (c.sc.visc) {
+            int ti = tidx(th, Tc);
+            double td = Tc - ti, mil, kl;
+            wilke(th, pl[0], rho, ti, td, mil, kl);
+            double mi = 0.0 + mil;
+            for (int d = 0; d < c.sc.ndir; ++d) {
+              double dl = dlv(b, d, i, j, k);
+              double dtd = (rho * (dl * dl) * c.sc.vnn) / mi;
+              dtc = std::min(dtd, dtc);
+            }
+          }
+          }
+          dtc = dtc * 1.0;
+          dtglobal = std::min(dtc, dtglobal);
+        }
+  }
+  return dtglobal;
+}
+
+}  // namespace
+
+extern "C" {
+
+struct orc_ctx { Ctx c; };
+
+int orc_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, orc_ctx** out) {
+  if (!mesh || !sc || !th || !out) return MB_E_ARG;
+  if (sc->riemann != 1 && sc->riemann != 4 && sc->riemann != 12) return MB_E_UNSUPPORTED;
+  if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
+  if (sc->n_rk < 1 || sc->n_rk > 3) return MB_E_UNSUPPORTED;
+  orc_ctx* o = new orc_ctx();
+  Ctx& c = o->c;
+  c.sc = *sc;
+  c.ncell = mesh->ncell_total;
+  for (int b = 0; b < mesh->nblk; ++b) {
+    const mb_block& q = mesh->blk[b];
+    Blk k;
+    k.n1 = q.n[0]; k.n2 = q.n[1]; k.n3 = q.n[2];
+    k.pi = q.n[0] + 2 * GC; k.pj = q.n[1] + 2 * GC;
+    k.boff = q.boff;
+    k.fm1 = q.fm1; k.fm2 = q.fm2; k.fm3 = q.fm3; k.dl = q.dl; k.m = q.m; k.vol = q.vol;
+    c.blk.push_back(k);
+  }
+  c.rec.assign(mesh->rec, mesh->rec + mesh->nrec);
+  c.conn.assign(mesh->conn, mesh->conn + mesh->nconn);
+  for (const mb_bc& r : c.rec)
+    if (r.type != MB_BC_CONNECTION && r.type != MB_BC_EXTRAPOLATION) { delete o; return MB_E_UNSUPPORTED; }
+  c.pg.assign((size_t)c.rec.size() * 6 * NP, 0.0);
+  Thermo& t = c.th;
+  t.tmin = th->tmin; t.tmax = th->tmax; t.wm = th->wm; t.ri = RUNIV / th->wm;
+  size_t nt = (size_t)(th->tmax - th->tmin + 1);
+  t.cp_.assign(th->cp, th->cp + nt); t.h_.assign(th->h, th->h + nt);
+  t.mu_.assign(th->mu, th->mu + nt); t.k_.assign(th->k, th->k + nt);
+  t.cp = t.cp_.data() - th->tmin; t.h = t.h_.data() - th->tmin;
+  t.mu = t.mu_.data() - th->tmin; t.k = t.k_.data() - th->tmin;
+  std::memset(&c.st, 0, sizeof(c.st));
+  *out = o;
+  return MB_OK;
+}
+
+void orc_destroy(orc_ctx* o) { delete o; }
+
+int orc_fill_ghosts(orc_ctx* o, double* P) { fill_ghosts(o->c, P); return MB_OK; }
+int orc_residual(orc_ctx* o, const double* P, double* R) { residual(o->c, P, R); return MB_OK; }
+int orc_update(orc_ctx* o, double* P, const double* PO, const double* R, int irk, double dt) {
+  update(o->c, P, PO, R, irk, dt);
+  return o->c.st.code;
+}
+int orc_dt(orc_ctx* o, const double* P, double* dt) { *dt = compute_dt(o->c, P); return MB_OK; }
+
+// nsteps explicit steps (Mod_Explicit.f90:52-279): dt, PO <- P, then per stage ghost fill, residual, update.
+int orc_step(orc_ctx* o, double* P, double* PO, double* R, int nsteps) {
+  Ctx& c = o->c;
+  const int64_t n = c.ncell * NP;
+  for (int st = 0; st < nsteps; ++st) {
+    double dt = compute_dt(c, P);
+    if (c.sc.time_clip) {  // Clip_dt_To_Timemax (Mod_dt.f90:283-296)
+      double rem = c.sc.time_threshold - c.st.time;
+      if (rem > 0.0 && dt > rem) dt = rem * (1.0 + 1e-12);
+    }
+    c.st.time += dt;
+    c.st.dt = dt;
+    std::memcpy(PO, P, sizeof(double) * n);
+    for (int irk = 1; irk <= c.sc.n_rk; ++irk) {
+      fill_ghosts(c, P);
+      residual(c, P, R);
+      update(c, P, PO, R, irk, dt);
+    }
+    c.st.steps += 1;
+    if (c.st.code != MB_OK) return c.st.code;
+  }
+  return MB_OK;
+}
+
+int orc_get_status(orc_ctx* o, mb_status* st) { *st = o->c.st; return MB_OK; }
+
+}  // extern "C"
