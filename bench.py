@@ -1,0 +1,305 @@
+"""Benchmark of the B200 engine on the 3-D compressible Navier-Stokes Taylor-Green vortex, 256^3 cells, one
+periodic block (Roe = LMRoe with Mco = 1, MUSCL van Albada, central viscous fluxes, SSP-RK3, CFL 0.8):
+cell-updates/s of the mixed form (FP32 flux arithmetic, FP64 state) beside the plain FP64 form, with the
+L2 error of the mixed density against the FP64 form after the same steps.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--n 256]
+
+One step = one time step (dt + 3 RK stages) of the whole 256^3 field. Under torchrun every rank runs its own
+replica (the path shards by blocks; this config is one block: replicas only, weak scaling), timed with CUDA
+events, max over ranks. --impl reference times the CPU restatement of the reference's path (the reference
+itself is Fortran/OpenACC/CUDA Fortran and cannot be built here) on the host cores, on a bounded sample.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "mose-gpu_b200"), os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "cell-updates/s (FP64 vs mixed at stated L2 error)"
+UNIT = "cell-updates/s"
+B_STAGE = 320            # algorithmic bytes per cell per stage, 3-D NS, FP64 (state read/read/write + geometry)
+N_STAGES = 3
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_launch(n):
+    """DRAM bytes (read + write) of one sweep launch from the committed ncu summary, scaled from its case."""
+    p = os.path.join(ROOT, "profiles", "sweep_traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return float(d["dram_bytes_per_launch"]) * (n ** 3) / float(d["cells"])
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, idx):
+        self.f = os.path.join("/tmp", "mose_clocks_%d.csv" % os.getpid())
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(idx), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=open(self.f, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        rows = []
+        for line in open(self.f):
+            c = [x.strip() for x in line.split(",")]
+            if len(c) >= 9:
+                rows.append(c)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower() == "active"})
+        load = [s for s in sm if s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(pg, x, dev):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, dev):
+    import torch
+    torch.cuda.synchronize(dev)
+    if pg is not None:
+        pg.barrier()
+        torch.cuda.synchronize(dev)
+
+
+def cpu_sample(case, min_seconds=10.0, max_steps=3):
+    """The CPU restatement on the host cores over a bounded sample of the same workload: whole steps of the
+    full field until min_seconds have passed (at most max_steps)."""
+    import oracle
+    o = oracle.Oracle(case)
+    P = case.P0.copy()
+    n, t0 = 0, time.perf_counter()
+    while n < max_steps:
+        rc = o.step(P, 1)
+        if rc != 0:
+            raise RuntimeError("oracle step failed: %d" % rc)
+        n += 1
+        if time.perf_counter() - t0 >= min_seconds:
+            break
+    dt = time.perf_counter() - t0
+    return case.n_interior * n / dt, n, dt
+
+
+def run_reference(args):
+    world, rank, local, pg = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0, None
+    if rank != 0:
+        return 0
+    from mosegpu import case as cs
+    case = cs.taylor_green(n=args.n)
+    cores = os.cpu_count()
+    vals = []
+    for _ in range(max(1, args.warmup)):
+        cpu_sample(case, min_seconds=0.0, max_steps=1)
+        break
+    total_n, total_t = 0, 0.0
+    for _ in range(max(1, args.steps)):
+        v, n, t = cpu_sample(case, min_seconds=0.0, max_steps=1)
+        vals.append(v)
+        total_n += n
+        total_t += t
+        if total_t > 120.0:
+            break
+    value = case.n_interior * total_n / total_t
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": total_n, "warmup": 1, "ms_per_step": 1e3 * total_t / total_n, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Taylor-Green field)",
+            "config": {"workload": "tgv%d_ns_roe_vanalbada_ssprk3" % args.n, "cells": case.n_interior,
+                       "steps_timed": total_n},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "%d whole time step(s) of the %d^3 field, %.1f s, OpenMP over %d threads "
+                                       "(the reference's own host build needs nvfortran + FiNeR: unavailable)"
+                                       % (total_n, args.n, total_t, cores)},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    args.warmup = max(3, args.warmup)
+
+    import torch
+    from mosegpu import abi
+    from mosegpu import case as cs
+    from mosegpu.engine import Engine
+    world, rank, local, pg = dist_setup()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    t0 = time.time()
+    case = cs.taylor_green(n=args.n)
+    setup_s = time.time() - t0
+    cells = case.n_interior
+    stream = torch.cuda.Stream(dev)
+    forms = {}
+    for name, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
+        eng = Engine(case, precision=prec, device=local, stream=stream)
+        with torch.cuda.stream(stream):
+            eng.step(args.warmup, graph=True)
+        barrier(pg, dev)
+        l0 = eng.launches
+        clk = Clocks(local) if name == "mixed" else None
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier(pg, dev)
+        e0.record(stream)
+        with torch.cuda.stream(stream):
+            eng.step(args.steps, graph=True)
+        e1.record(stream)
+        e1.synchronize()
+        barrier(pg, dev)
+        ms = max_over_ranks(pg, e0.elapsed_time(e1), dev)
+        clocks = clk.stop() if clk else None
+        st = eng.status()
+        if st.code != 0:
+            raise RuntimeError("%s form: %s" % (name, abi.status_message(st.code)))
+        # the dominant kernel alone: the fused sweep of a middle stage, CUDA events on its stream
+        with torch.cuda.stream(stream):
+            g_ms, s_ms = eng.profile_stage(2, 5)
+        forms[name] = dict(eng=eng, ms=ms, launches=eng.launches - l0, clocks=clocks, sweep_ms=s_ms, ghost_ms=g_ms)
+    # accuracy of the mixed form: both forms ran warmup + steps from the same initial field
+    torch.cuda.synchronize(dev)
+    a = forms["fp64"]["eng"].state()
+    b = forms["mixed"]["eng"].state()
+    m = case.interior_mask()
+    err = {}
+    for q, nm in enumerate(["rho", "u", "v", "w", "p"]):
+        x, y = b[q, m], a[q, m]
+        d = x - y
+        err[nm] = {"L1": float(np.abs(d).sum() / np.abs(y).sum()),
+                   "L2": float(np.sqrt((d * d).sum() / (y * y).sum())),
+                   "Linf": float(np.abs(d).max() / np.abs(y).max())}
+    l2_rho = err["rho"]["L2"]
+    head = "mixed" if l2_rho <= 1e-5 else "fp64"
+    f = forms[head]
+    value = world * cells * args.steps / (f["ms"] * 1e-3)
+    fp64_value = world * cells * args.steps / (forms["fp64"]["ms"] * 1e-3)
+    mixed_value = world * cells * args.steps / (forms["mixed"]["ms"] * 1e-3)
+
+    # e2e through the C ABI with host buffers: the initial field uploaded from pinned host memory, each step
+    # driven by the reference-facing calls (begin_step, stage 1..3) with the status (dt, time, checks) read
+    # back to the host, the final field downloaded to pinned host memory.
+    eng = forms[head]["eng"]
+    host_in = torch.from_numpy(case.P0).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    barrier(pg, dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    with torch.cuda.stream(stream):
+        eng.P.copy_(host_in, non_blocking=True)
+        for _ in range(args.steps):
+            eng.begin_step()
+            for irk in range(1, 4):
+                eng.stage(irk)
+            st = eng.status()
+        host_out.copy_(eng.P, non_blocking=True)
+    e1.record(stream)
+    e1.synchronize()
+    barrier(pg, dev)
+    e2e_ms = max_over_ranks(pg, e0.elapsed_time(e1), dev)
+    e2e_value = world * cells * args.steps / (e2e_ms * 1e-3)
+    state_bytes = case.P0.nbytes
+
+    peak, peak_kind = peaks()
+    bytes_launch = cells * B_STAGE
+    achieved = bytes_launch / (f["sweep_ms"] * 1e-3) / 1e9
+    tr = traffic_per_launch(args.n)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": f["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 flux / f64 state" if head == "mixed" else "f64",
+            "data": "synthetic (seeded Taylor-Green field, dimensional: T0 300 K, Mach 0.1, Re 1600)",
+            "config": {"workload": "tgv%d_ns_roe_vanalbada_ssprk3" % args.n, "cells": cells,
+                       "block": "1 periodic block", "parallelism": "replicas only (dp%d)" % world,
+                       "form": head, "l2_flush": "inputs larger than L2 (state 3 x %.0f MB + geometry)" %
+                       (state_bytes / 1e6), "dt_rule": "additive", "setup_s": round(setup_s, 1)},
+            "forms": {"fp64": {"value": fp64_value, "ms_per_step": forms["fp64"]["ms"] / args.steps,
+                               "sweep_ms": forms["fp64"]["sweep_ms"], "ghost_ms": forms["fp64"]["ghost_ms"]},
+                      "mixed": {"value": mixed_value, "ms_per_step": forms["mixed"]["ms"] / args.steps,
+                                "sweep_ms": forms["mixed"]["sweep_ms"], "ghost_ms": forms["mixed"]["ghost_ms"],
+                                "speedup_vs_fp64": mixed_value / fp64_value},
+                      "mixed_vs_fp64_error_after_%d_steps" % (args.steps + args.warmup): err},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": tr, "peak_source": peak_kind,
+                         "kernel": "k_sweep<%s> (stage 2)" % ("float" if head == "mixed" else "double"),
+                         "algorithmic_bytes_per_launch": bytes_launch},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
+                    "d2h_bytes_per_step": state_bytes / args.steps + 48,
+                    "path": "C ABI: upload once, per step mb_begin_step + 3 x mb_stage + mb_get_status, download"},
+            "gpu_launches": f["launches"], "clocks": forms["mixed"]["clocks"]}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, n, t = cpu_sample(case, min_seconds=10.0, max_steps=2)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                "sample": "%d whole time step(s) of the %d^3 field (%.1f s), OpenMP" % (n, args.n, t)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for fm in forms.values():
+        fm["eng"].close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,499 @@
+// mb_api.cu -- the C ABI of include/mose_b200.h: context set-up (device tables built once from the
+// host descriptions, as Setup_BC_Device / Setup_Device_Residency do), the per-call entry points
+// and the time loop with a device-side clock, optionally replayed as a CUDA graph.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#include "../../include/mose_b200.h"
+#include "mb_launch.h"
+
+using namespace mb;
+
+struct mb_ctx {
+  int device = 0;
+  mb_scheme sc;
+  Params p;
+  GhostLists g;
+  // device allocations
+  DBlk* d_blk = nullptr;
+  int* d_recmap = nullptr;
+  DRec* d_rec = nullptr;
+  GRec* d_grec = nullptr;
+  int* d_phys = nullptr;
+  int* d_cubic = nullptr;
+  long long* d_cdst = nullptr;
+  long long* d_csrc = nullptr;
+  long long* d_pgsrc = nullptr;
+  double* d_pg = nullptr;
+  double* d_tab = nullptr;
+  float* d_tabf = nullptr;
+  DevState* d_st = nullptr;
+  DTile* d_tiles_sweep = nullptr;
+  int ntiles_sweep = 0;
+  DTile* d_tiles_aux = nullptr;
+  int ntiles_aux = 0;
+  double* d_scratch = nullptr;  // the engine's own stage buffer (ncell x 5)
+  long long ncell = 0;
+  std::vector<int> blk_n;       // 3 per block
+  bool dt_valid = false;
+  long long launches = 0;
+  // graph of one step
+  cudaGraphExec_t gexec = nullptr;
+  cudaGraph_t graph = nullptr;
+  const double* gP = nullptr;
+  const double* gPO = nullptr;
+  cudaStream_t gstream = nullptr;
+  int graph_kernels = 0;
+};
+
+#define CK(x)                                    \
+  do {                                           \
+    cudaError_t e_ = (x);                        \
+    if (e_ != cudaSuccess) {                     \
+      fprintf(stderr, "[mose_b200] CUDA error %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return MB_E_CUDA;                          \
+    }                                            \
+  } while (0)
+
+template <typename T>
+static int upload(T** dst, const T* src, size_t n) {
+  if (n == 0) { *dst = nullptr; return MB_OK; }
+  if (cudaMalloc((void**)dst, n * sizeof(T)) != cudaSuccess) return MB_E_NOMEM;
+  CK(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  return MB_OK;
+}
+
+static void free_ctx(mb_ctx* c) {
+  if (!c) return;
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  if (c->graph) cudaGraphDestroy(c->graph);
+  void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
+                  c->d_pgsrc, c->d_pg, c->d_tab, c->d_tabf, c->d_st, c->d_tiles_sweep, c->d_tiles_aux, c->d_scratch};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  delete c;
+}
+
+static std::vector<DTile> make_tiles(const mb_mesh* mesh, int ty, int kc) {
+  std::vector<DTile> t;
+  for (int b = 0; b < mesh->nblk; ++b) {
+    const int* n = mesh->blk[b].n;
+    for (int k0 = 1; k0 <= n[2]; k0 += kc)
+      for (int j0 = 1; j0 <= n[1]; j0 += ty)
+        for (int i0 = 1; i0 <= n[0]; i0 += 32) t.push_back(DTile{b, i0, j0, k0, std::min(k0 + kc, n[2] + 1)});
+  }
+  return t;
+}
+
+static const double RKC[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0 / 3.0}};  // Lib_RK.f90:6-9
+
+extern "C" {
+
+const char* mb_version(void) { return "mose_b200 0.1 (sm_100a)"; }
+
+int64_t mb_launch_count(const mb_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int device, mb_ctx** out) {
+  if (!mesh || !sc || !th || !out || mesh->nblk <= 0 || mesh->ncell_total <= 0) return MB_E_ARG;
+  *out = nullptr;
+  if (sc->riemann != MB_RS_HLLC && sc->riemann != MB_RS_AUSMP && sc->riemann != MB_RS_LMROE) return MB_E_UNSUPPORTED;
+  if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
+  if (sc->n_rk < 1 || sc->n_rk > 3) return MB_E_UNSUPPORTED;
+  if (sc->precision != MB_PREC_FP64 && sc->precision != MB_PREC_MIXED) return MB_E_UNSUPPORTED;
+  if (sc->ndir < 1 || sc->ndir > 3) return MB_E_ARG;
+  if (th->tmax - th->tmin < 2 || !th->cp || !th->h || !th->mu || !th->k) return MB_E_ARG;
+  for (int q = 0; q < mesh->nrec; ++q) {
+    const mb_bc& r = mesh->rec[q];
+    if (r.type != MB_BC_CONNECTION && r.type != MB_BC_EXTRAPOLATION) return MB_E_UNSUPPORTED;
+    if (r.blk < 0 || r.blk >= mesh->nblk || r.face < 1 || r.face > 6) return MB_E_ARG;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return MB_E_NODEV;
+  if (device < 0 || device >= ndev) return MB_E_ARG;
+  CK(cudaSetDevice(device));
+  mb_ctx* c = new mb_ctx();
+  c->device = device;
+  c->sc = *sc;
+  c->ncell = mesh->ncell_total;
+  int rc;
+#define TRY(x)                 \
+  do {                         \
+    rc = (x);                  \
+    if (rc != MB_OK) {         \
+      free_ctx(c);             \
+      return rc;               \
+    }                          \
+  } while (0)
+  // ---- blocks and the per-face record maps
+  std::vector<DBlk> hb(mesh->nblk);
+  std::vector<int> recmap;
+  for (int b = 0; b < mesh->nblk; ++b) {
+    const mb_block& q = mesh->blk[b];
+    if (q.n[0] < 1 || q.n[1] < 1 || q.n[2] < 1 || !q.fm1 || !q.fm2 || !q.fm3 || !q.dl || !q.m || !q.vol) {
+      free_ctx(c);
+      return MB_E_ARG;
+    }
+    DBlk& d = hb[b];
+    d.n1 = q.n[0]; d.n2 = q.n[1]; d.n3 = q.n[2];
+    d.pi = q.n[0] + 2 * MB_GC; d.pj = q.n[1] + 2 * MB_GC;
+    d.boff = q.boff;
+    d.fm1 = q.fm1; d.fm2 = q.fm2; d.fm3 = q.fm3; d.dl = q.dl; d.m = q.m; d.vol = q.vol;
+    for (int f = 0; f < 6; ++f) d.rmap[f] = -1;
+    c->blk_n.push_back(q.n[0]); c->blk_n.push_back(q.n[1]); c->blk_n.push_back(q.n[2]);
+  }
+  for (int q = 0; q < mesh->nrec; ++q) {
+    const mb_bc& r = mesh->rec[q];
+    DBlk& d = hb[r.blk];
+    const int ax = (r.face - 1) / 2;
+    const int nt = (ax == 0) ? d.n2 * d.n3 : (ax == 1 ? d.n1 * d.n3 : d.n1 * d.n2);
+    if (d.rmap[r.face - 1] < 0) {
+      d.rmap[r.face - 1] = (int)recmap.size();
+      recmap.resize(recmap.size() + nt, -1);
+    }
+    const int n[3] = {d.n1, d.n2, d.n3};
+    const int cc[3] = {r.i, r.j, r.k};
+    if (r.i < 1 || r.i > d.n1 || r.j < 1 || r.j > d.n2 || r.k < 1 || r.k > d.n3 ||
+        cc[ax] != ((r.face & 1) ? 1 : n[ax])) {
+      free_ctx(c);
+      return MB_E_ARG;
+    }
+    int t = (ax == 0) ? (r.j - 1) + (r.k - 1) * d.n2 : (ax == 1 ? (r.i - 1) + (r.k - 1) * d.n1 : (r.i - 1) + (r.j - 1) * d.n1);
+    recmap[d.rmap[r.face - 1] + t] = q;
+  }
+  // ---- records
+  std::vector<DRec> hr(mesh->nrec);
+  std::vector<GRec> hg(mesh->nrec);
+  std::vector<int> phys, cubic;
+  for (int q = 0; q < mesh->nrec; ++q) {
+    const mb_bc& r = mesh->rec[q];
+    hr[q].type = r.type;
+    hr[q].pg = r.conn;
+    for (int s = 0; s < MB_NPRIM; ++s) hr[q].q[s] = r.q[s];
+    hg[q] = GRec{r.blk, r.i, r.j, r.k, r.face, r.type};
+    if (r.type == MB_BC_EXTRAPOLATION || r.type == MB_BC_INFLOW || r.type == MB_BC_WALL) phys.push_back(q);
+    if (r.type == MB_BC_EXTRAPOLATION) cubic.push_back(q);
+  }
+  // ---- connections: ghost copies (2 layers) and the bc_pg source rows
+  auto rowof = [&](int b, int i, int j, int k) -> long long {
+    const DBlk& d = hb[b];
+    return d.boff + (long long)(i + MB_GC - 1) + (long long)(j + MB_GC - 1) * d.pi + (long long)(k + MB_GC - 1) * d.pi * d.pj;
+  };
+  auto guide = [](int F, int ax) { int d = (F + 1) / 2 - 1; return ax == d ? ((F % 2) ? 1 : -1) : 0; };
+  std::vector<long long> cdst, csrc, pgsrc;
+  for (int q = 0; q < mesh->nconn; ++q) {
+    const mb_conn& cn = mesh->conn[q];
+    if (cn.rec < 0 || cn.rec >= mesh->nrec || cn.bs < 0 || cn.bs >= mesh->nblk || mesh->rec[cn.rec].conn != q) {
+      free_ctx(c);
+      return MB_E_ARG;
+    }
+    const mb_bc& r = mesh->rec[cn.rec];
+    for (int g = 1; g <= MB_GC; ++g) {
+      cdst.push_back(rowof(r.blk, r.i - guide(r.face, 0) * g, r.j - guide(r.face, 1) * g, r.k - guide(r.face, 2) * g));
+      csrc.push_back(rowof(cn.bs, cn.is + guide(cn.fs, 0) * (g - 1), cn.js + guide(cn.fs, 1) * (g - 1),
+                           cn.ks + guide(cn.fs, 2) * (g - 1)));
+    }
+    const int I = cn.is, J = cn.js, K = cn.ks;
+    int t[4][3];
+    if (cn.fs <= 2) {
+      int a[4][3] = {{I, J - cn.d11, K - cn.d12}, {I, J + cn.d11, K + cn.d12}, {I, J - cn.d21, K - cn.d22}, {I, J + cn.d21, K + cn.d22}};
+      memcpy(t, a, sizeof(t));
+    } else if (cn.fs <= 4) {
+      int a[4][3] = {{I - cn.d11, J, K - cn.d12}, {I + cn.d11, J, K + cn.d12}, {I - cn.d21, J, K - cn.d22}, {I + cn.d21, J, K + cn.d22}};
+      memcpy(t, a, sizeof(t));
+    } else {
+      int a[4][3] = {{I - cn.d11, J - cn.d12, K}, {I + cn.d11, J + cn.d12, K}, {I - cn.d21, J - cn.d22, K}, {I + cn.d21, J + cn.d22, K}};
+      memcpy(t, a, sizeof(t));
+    }
+    pgsrc.push_back(rowof(cn.bs, I, J, K));
+    pgsrc.push_back(rowof(cn.bs, I + guide(cn.fs, 0), J + guide(cn.fs, 1), K + guide(cn.fs, 2)));
+    for (int m = 0; m < 4; ++m) pgsrc.push_back(rowof(cn.bs, t[m][0], t[m][1], t[m][2]));
+  }
+  // every row must lie inside the arena
+  for (const auto* v : {&cdst, &csrc, &pgsrc})
+    for (long long x : *v)
+      if (x < 0 || x >= c->ncell) { free_ctx(c); return MB_E_ARG; }
+  // ---- thermo tables (FP64 and FP32 copies)
+  const int nt = th->tmax - th->tmin + 1;
+  std::vector<double> tab(4 * (size_t)nt);
+  std::vector<float> tabf(4 * (size_t)nt);
+  for (int q = 0; q < nt; ++q) {
+    tab[q] = th->cp[q]; tab[nt + q] = th->h[q]; tab[2 * nt + q] = th->mu[q]; tab[3 * nt + q] = th->k[q];
+  }
+  for (size_t q = 0; q < tab.size(); ++q) tabf[q] = (float)tab[q];
+  // ---- tiles
+  std::vector<DTile> ts = make_tiles(mesh, sc->precision == MB_PREC_MIXED ? TY_F32 : TY_F64, 16);
+  std::vector<DTile> ta = make_tiles(mesh, TY_AUX, 16);
+  TRY(upload(&c->d_blk, hb.data(), hb.size()));
+  TRY(upload(&c->d_recmap, recmap.data(), recmap.size()));
+  TRY(upload(&c->d_rec, hr.data(), hr.size()));
+  TRY(upload(&c->d_grec, hg.data(), hg.size()));
+  TRY(upload(&c->d_phys, phys.data(), phys.size()));
+  TRY(upload(&c->d_cubic, cubic.data(), cubic.size()));
+  TRY(upload(&c->d_cdst, cdst.data(), cdst.size()));
+  TRY(upload(&c->d_csrc, csrc.data(), csrc.size()));
+  TRY(upload(&c->d_pgsrc, pgsrc.data(), pgsrc.size()));
+  TRY(upload(&c->d_tab, tab.data(), tab.size()));
+  TRY(upload(&c->d_tabf, tabf.data(), tabf.size()));
+  TRY(upload(&c->d_tiles_sweep, ts.data(), ts.size()));
+  TRY(upload(&c->d_tiles_aux, ta.data(), ta.size()));
+  c->ntiles_sweep = (int)ts.size();
+  c->ntiles_aux = (int)ta.size();
+  if (mesh->nconn > 0 && cudaMalloc((void**)&c->d_pg, (size_t)mesh->nconn * 6 * MB_NPRIM * sizeof(double)) != cudaSuccess) {
+    free_ctx(c);
+    return MB_E_NOMEM;
+  }
+  if (cudaMalloc((void**)&c->d_st, sizeof(DevState)) != cudaSuccess) { free_ctx(c); return MB_E_NOMEM; }
+  DevState hs;
+  memset(&hs, 0, sizeof(hs));
+  double big = 1e300;
+  memcpy(&hs.dtmin_bits, &big, sizeof(double));
+  if (cudaMemcpy(c->d_st, &hs, sizeof(hs), cudaMemcpyHostToDevice) != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+  if (cudaMalloc((void**)&c->d_scratch, (size_t)c->ncell * MB_NPRIM * sizeof(double)) != cudaSuccess) {
+    free_ctx(c);
+    return MB_E_NOMEM;
+  }
+  if (cudaMemset(c->d_scratch, 0, (size_t)c->ncell * MB_NPRIM * sizeof(double)) != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+  if (sweep_setup_f64() != cudaSuccess || sweep_setup_f32() != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+  // ---- kernel parameters
+  Params& p = c->p;
+  memset(&p, 0, sizeof(p));
+  p.blk = c->d_blk; p.rec_map = c->d_recmap; p.rec = c->d_rec; p.pg = c->d_pg;
+  p.cp = c->d_tab - th->tmin; p.h = c->d_tab + nt - th->tmin; p.mu = c->d_tab + 2 * nt - th->tmin; p.k = c->d_tab + 3 * nt - th->tmin;
+  p.cpf = c->d_tabf - th->tmin; p.hf = c->d_tabf + nt - th->tmin; p.muf = c->d_tabf + 2 * nt - th->tmin; p.kf = c->d_tabf + 3 * nt - th->tmin;
+  p.st = c->d_st;
+  p.nc = c->ncell;
+  p.tmin = th->tmin; p.tmax = th->tmax;
+  p.wm = th->wm; p.ri = RUNIV / th->wm;
+  p.lim = sc->limiter; p.rs = sc->riemann; p.visc = sc->visc ? 1 : 0; p.ndir = sc->ndir; p.dt_additive = sc->dt_additive;
+  p.guard = sc->visc ? 1 : 0; p.state_check = sc->state_check;
+  p.cfl = sc->cfl; p.vnn = sc->vnn; p.prandtl = sc->prandtl; p.schmidt = sc->schmidt; p.mco = sc->mco;
+  GhostLists& g = c->g;
+  g.rec = c->d_grec; g.phys = c->d_phys; g.nphys = (int)phys.size(); g.cubic = c->d_cubic; g.ncubic = (int)cubic.size();
+  g.cdst = c->d_cdst; g.csrc = c->d_csrc; g.ncopy = (int)cdst.size(); g.pgsrc = c->d_pgsrc; g.nconn = mesh->nconn;
+  g.pg = c->d_pg;
+#undef TRY
+  *out = c;
+  return MB_OK;
+}
+
+void mb_destroy(mb_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  free_ctx(ctx);
+}
+
+static int sweep(mb_ctx* c, int mode, const double* Pin, const double* Pold, double* Pout, double* Rout, double rkc,
+                 int last, cudaStream_t s) {
+  cudaError_t e = (c->sc.precision == MB_PREC_MIXED)
+                      ? sweep_f32(c->p, c->d_tiles_sweep, c->ntiles_sweep, mode, Pin, Pold, Pout, Rout, rkc, last, s)
+                      : sweep_f64(c->p, c->d_tiles_sweep, c->ntiles_sweep, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+  c->launches += 1;
+  CK(e);
+  return MB_OK;
+}
+
+static int fill(mb_ctx* c, double* P, cudaStream_t s) {
+  int nl = 0;
+  cudaError_t e = ghost_fill(c->p, c->g, P, s, &nl);
+  c->launches += nl;
+  CK(e);
+  return MB_OK;
+}
+
+int mb_fill_ghosts(mb_ctx* ctx, double* P, void* stream) {
+  if (!ctx || !P) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  return fill(ctx, P, (cudaStream_t)stream);
+}
+
+int mb_residual(mb_ctx* ctx, const double* P, double* R, void* stream) {
+  if (!ctx || !P || !R) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  return sweep(ctx, MODE_RESIDUAL, P, nullptr, nullptr, R, 0.0, 0, (cudaStream_t)stream);
+}
+
+int mb_update(mb_ctx* ctx, double* P, const double* PO, const double* R, int irk, double dt, void* stream) {
+  if (!ctx || !P || !PO || !R || irk < 1 || irk > ctx->sc.n_rk) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  cudaError_t e = update_cells(ctx->p, ctx->d_tiles_aux, ctx->ntiles_aux, P, PO, R, RKC[ctx->sc.n_rk - 1][irk - 1], dt,
+                               (cudaStream_t)stream);
+  ctx->launches += 1;
+  CK(e);
+  return MB_OK;
+}
+
+static int dt_min(mb_ctx* c, const double* P, cudaStream_t s) {
+  CK(reset_dt(c->p, s));
+  CK(dt_cells(c->p, c->d_tiles_aux, c->ntiles_aux, P, s));
+  c->launches += 2;
+  return MB_OK;
+}
+
+int mb_dt(mb_ctx* ctx, const double* P, double* dt_host, void* stream) {
+  if (!ctx || !P || !dt_host) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = dt_min(ctx, P, s);
+  if (rc != MB_OK) return rc;
+  unsigned long long bits;
+  CK(cudaMemcpyAsync(&bits, &ctx->d_st->dtmin_bits, sizeof(bits), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  double dm;
+  memcpy(&dm, &bits, sizeof(dm));
+  *dt_host = std::min(dm, 1e5);
+  ctx->dt_valid = true;  // the device minimum now belongs to P
+  return MB_OK;
+}
+
+int mb_begin_step(mb_ctx* ctx, const double* P, void* stream) {
+  if (!ctx || !P) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = dt_min(ctx, P, s);
+  if (rc != MB_OK) return rc;
+  CK(clock_step(ctx->p, ctx->sc.time_clip, ctx->sc.time_threshold, s));
+  ctx->launches += 1;
+  return MB_OK;
+}
+
+// stage irk of the step: input / old / output buffers so that the state lands back in P after the last
+// stage (the old state u^n is only read at the updated cell itself, so the last stage updates P in place):
+//   RK3: P -> S, S -> PO, PO -> P      RK2: P -> S, S -> P      Euler: P -> S, then S copied to P
+static int stage(mb_ctx* c, double* P, double* PO, int irk, cudaStream_t s) {
+  const int n = c->sc.n_rk;
+  double* S = c->d_scratch;
+  const double* in;
+  double* outp;
+  if (irk == 1) { in = P; outp = S; }
+  else if (n == 2) { in = S; outp = P; }
+  else if (irk == 2) { in = S; outp = PO; }
+  else { in = PO; outp = P; }
+  int rc = fill(c, const_cast<double*>(in), s);
+  if (rc != MB_OK) return rc;
+  const int last = (irk == n) ? 1 : 0;
+  rc = sweep(c, MODE_UPDATE, in, P, outp, nullptr, RKC[n - 1][irk - 1], last, s);
+  if (rc != MB_OK) return rc;
+  if (n == 1) {
+    CK(cudaMemcpyAsync(P, S, (size_t)c->ncell * MB_NPRIM * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  }
+  return MB_OK;
+}
+
+int mb_stage(mb_ctx* ctx, double* P, double* PO, int irk, void* stream) {
+  if (!ctx || !P || !PO || irk < 1 || irk > ctx->sc.n_rk) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  return stage(ctx, P, PO, irk, (cudaStream_t)stream);
+}
+
+static int one_step(mb_ctx* c, double* P, double* PO, cudaStream_t s) {
+  CK(clock_step(c->p, c->sc.time_clip, c->sc.time_threshold, s));
+  c->launches += 1;
+  for (int irk = 1; irk <= c->sc.n_rk; ++irk) {
+    int rc = stage(c, P, PO, irk, s);
+    if (rc != MB_OK) return rc;
+  }
+  return MB_OK;
+}
+
+int mb_step(mb_ctx* ctx, double* P, double* PO, int nsteps, int use_graph, void* stream) {
+  if (!ctx || !P || !PO || nsteps < 0) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!ctx->dt_valid) {
+    int rc = dt_min(ctx, P, s);
+    if (rc != MB_OK) return rc;
+    ctx->dt_valid = true;
+  }
+  if (!use_graph) {
+    for (int q = 0; q < nsteps; ++q) {
+      int rc = one_step(ctx, P, PO, s);
+      if (rc != MB_OK) return rc;
+    }
+    return MB_OK;
+  }
+  if (!ctx->gexec || ctx->gP != P || ctx->gPO != PO) {
+    if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+    if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+    // capture on a private stream so the caller's stream may be the legacy default stream
+    cudaStream_t cs;
+    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    long long l0 = ctx->launches;
+    CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    int rc = one_step(ctx, P, PO, cs);
+    cudaGraph_t gr = nullptr;
+    cudaError_t e = cudaStreamEndCapture(cs, &gr);
+    cudaStreamDestroy(cs);
+    ctx->graph_kernels = (int)(ctx->launches - l0);
+    ctx->launches = l0;
+    if (rc != MB_OK) { if (gr) cudaGraphDestroy(gr); return rc; }
+    CK(e);
+    ctx->graph = gr;
+    CK(cudaGraphInstantiate(&ctx->gexec, gr, 0));
+    ctx->gP = P;
+    ctx->gPO = PO;
+  }
+  for (int q = 0; q < nsteps; ++q) {
+    CK(cudaGraphLaunch(ctx->gexec, s));
+    ctx->launches += ctx->graph_kernels;
+  }
+  return MB_OK;
+}
+
+int mb_profile_stage(mb_ctx* ctx, double* P, double* PO, int irk, int nrep, float* ms_ghost, float* ms_sweep,
+                     void* stream) {
+  if (!ctx || !P || !PO || irk < 1 || irk > ctx->sc.n_rk || nrep < 1 || !ms_ghost || !ms_sweep) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int n = ctx->sc.n_rk;
+  double* S = ctx->d_scratch;
+  const double* in = (irk == 1) ? P : ((n == 2 || irk == 2) ? S : PO);
+  double* outp = (irk == 1) ? S : ((n == 2 || irk == 3) ? P : PO);
+  cudaEvent_t e0, e1, e2;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventCreate(&e2));
+  float tg = 0.f, ts = 0.f;
+  int rc = MB_OK;
+  for (int q = 0; q < nrep && rc == MB_OK; ++q) {
+    cudaEventRecord(e0, s);
+    rc = fill(ctx, const_cast<double*>(in), s);
+    cudaEventRecord(e1, s);
+    if (rc == MB_OK) rc = sweep(ctx, MODE_UPDATE, in, P, outp, nullptr, RKC[n - 1][irk - 1], irk == n ? 1 : 0, s);
+    cudaEventRecord(e2, s);
+    cudaEventSynchronize(e2);
+    float a = 0.f, b = 0.f;
+    cudaEventElapsedTime(&a, e0, e1);
+    cudaEventElapsedTime(&b, e1, e2);
+    tg += a;
+    ts += b;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(e2);
+  *ms_ghost = tg / nrep;
+  *ms_sweep = ts / nrep;
+  return rc;
+}
+
+int mb_get_status(mb_ctx* ctx, mb_status* st) {
+  if (!ctx || !st) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaDeviceSynchronize());
+  DevState h;
+  CK(cudaMemcpy(&h, ctx->d_st, sizeof(h), cudaMemcpyDeviceToHost));
+  memset(st, 0, sizeof(*st));
+  st->n_bad_state = h.n_bad_state;
+  st->n_bad_thermo = h.n_bad_thermo;
+  st->bad_blk = h.bad_blk; st->bad_i = h.bad_i; st->bad_j = h.bad_j; st->bad_k = h.bad_k;
+  st->steps = h.steps;
+  st->time = h.time;
+  st->dt = h.dt;
+  st->code = MB_OK;
+  if (h.n_bad_thermo > 0) st->code = MB_E_THERMO;
+  else if (h.n_bad_state > 0 && ctx->sc.state_check) st->code = MB_E_STATE;
+  return MB_OK;
+}
+
+}  // extern "C"

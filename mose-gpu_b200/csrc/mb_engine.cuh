@@ -1,0 +1,573 @@
+// mb_engine.cuh -- kernels of the B200 engine.
+//
+//   k_sweep      the fused stage: every interior face flux of a tile computed ONCE (one thread per
+//                face), exchanged through shared memory, summed per cell in the reference's pass-2
+//                order (src/lib/gpu/pass2_body.inc), the boundary records of the cell added in face
+//                order 1..6 (numerics/fluxes/bc/Mod_BC.f90:449-485), then either the residual is
+//                written (parity hook, mode RESIDUAL) or the conservative RK update is applied
+//                (gpu/newstate_cons_body.inc) with, on the last stage, the local dt of the new state
+//                reduced into the device clock (gpu/dt_blk.inc; warp shuffles, one atomic per CTA).
+//   k_ghost_*    the ghost fill (numerics/fluxes/bc/Lib_Extrapolation.f90:1370-1528)
+//   k_dt         Compute_dt on its own (numerics/time/Mod_dt.f90:15-106)
+//   k_update     RK_Newstate on its own (explicit/Lib_Newstate.f90:257-307)
+//
+// Tiling: a CTA owns a tile of 32 (i) x TY (j) cells of one block and marches over a chunk of k
+// planes. Per plane it computes the (32+1) x TY i-faces, 32 x (TY+1) j-faces and the 32 x TY
+// k-faces above the plane (the k-face below is the previous plane's), so only the tile's left i-faces
+// and bottom j-faces are computed twice across CTAs. Warps run the face tasks through one call
+// site, which keeps a single copy of the flux code in the kernel.
+#pragma once
+#include "mb_physics.cuh"
+
+namespace mb {
+
+struct DTile {
+  int blk, i0, j0, k0, k1;  // cells i0..i0+31, j0..j0+TY-1, planes k0..k1-1 (1-based)
+};
+
+enum { MODE_RESIDUAL = 0, MODE_UPDATE = 1 };
+
+template <typename R> __device__ __forceinline__ R cvt(double x) { return (R)x; }
+
+// ---------------------------------------------------------------------------------------------
+// One interior face of direction d between cell (i,j,k) and its +d neighbour: the convective flux
+// (conv_physics.inc) into out[0..4] and, for Navier-Stokes, the viscous flux (diff_physics.inc)
+// into out[5..9].
+template <typename R, bool VISC>
+__device__ __forceinline__ void face_flux(const Params& p, const DBlk& b, const double* __restrict__ P, int d, int i,
+                                          int j, int k, R* out) {
+  const long long nc = p.nc;
+  const long long r0 = row(b, i, j, k);
+  const long long st = (d == 0) ? 1 : (d == 1 ? (long long)b.pi : (long long)b.pi * b.pj);
+  R pm1[MB_NP], p0[MB_NP], pp1[MB_NP], pp2[MB_NP], dlc[4];
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) {
+    pm1[s] = cvt<R>(ld(P + r0 - st + s * nc));
+    p0[s] = cvt<R>(ld(P + r0 + s * nc));
+    pp1[s] = cvt<R>(ld(P + r0 + st + s * nc));
+    pp2[s] = cvt<R>(ld(P + r0 + 2 * st + s * nc));
+  }
+  const long long l0 = r0 - b.boff;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) dlc[q] = cvt<R>(ld(b.dl + d + 3 * (l0 + (q - 1) * st)));
+  const double* f = fmp(b, d, i, j, k);
+  R nx = cvt<R>(ld(f)), ny = cvt<R>(ld(f + 1)), nz = cvt<R>(ld(f + 2)), area = cvt<R>(ld(f + 3));
+  conv_face<R>(p, pm1, p0, pp1, pp2, dlc, nx, ny, nz, area, out);
+  if (!VISC) return;
+  // ---- viscous face: cells 1,2 = (c, c+d); 3,4 = c -/+ b-axis; 5,6 = c+d -/+ b; 7,8 = c -/+ c-axis; 9,10 = c+d -/+ c
+  const long long sb = (d == 0) ? (long long)b.pi : 1;
+  const long long sc = (d == 2) ? (long long)b.pi : (long long)b.pi * b.pj;
+  const long long cc[10] = {r0, r0 + st, r0 - sb, r0 + sb, r0 + st - sb, r0 + st + sb,
+                            r0 - sc, r0 + sc, r0 + st - sc, r0 + st + sc};
+  const int ia = d, ib = (d == 0) ? 1 : 0, ic = (d == 2) ? 1 : 2;
+  R rho_n[10], T_n[10];
+#pragma unroll
+  for (int q = 0; q < 10; ++q) cell_rho_T<R>(p, cvt<R>(ld(P + cc[q])), cvt<R>(ld(P + cc[q] + MB_IPR * nc)), rho_n[q], T_n[q]);
+  auto w = [&](int q, int s) -> R { return cvt<R>(ld(P + cc[q] + s * nc)); };
+  R G[MB_NP][3];
+  R irho1 = (R)1 / rho_n[0], irho2 = (R)1 / rho_n[1];
+  G[0][ia] = w(1, 0) * irho2 - w(0, 0) * irho1;
+  G[MB_IPR][ia] = T_n[1] - T_n[0];
+#pragma unroll
+  for (int s = MB_IU; s <= MB_IW; ++s) G[s][ia] = w(1, s) - w(0, s);
+  R irt1 = (R)1 / rho_n[2], irt2 = (R)1 / rho_n[3], irt3 = (R)1 / rho_n[4], irt4 = (R)1 / rho_n[5];
+  G[0][ib] = (w(3, 0) * irt2 - w(2, 0) * irt1 + w(5, 0) * irt4 - w(4, 0) * irt3) * (R)0.25;
+  G[MB_IPR][ib] = (T_n[3] - T_n[2] + T_n[5] - T_n[4]) * (R)0.25;
+#pragma unroll
+  for (int s = MB_IU; s <= MB_IW; ++s) G[s][ib] = (w(3, s) - w(2, s) + w(5, s) - w(4, s)) * (R)0.25;
+  irt1 = (R)1 / rho_n[6]; irt2 = (R)1 / rho_n[7]; irt3 = (R)1 / rho_n[8]; irt4 = (R)1 / rho_n[9];
+  G[0][ic] = (w(7, 0) * irt2 - w(6, 0) * irt1 + w(9, 0) * irt4 - w(8, 0) * irt3) * (R)0.25;
+  G[MB_IPR][ic] = (T_n[7] - T_n[6] + T_n[9] - T_n[8]) * (R)0.25;
+#pragma unroll
+  for (int s = MB_IU; s <= MB_IW; ++s) G[s][ic] = (w(7, s) - w(6, s) + w(9, s) - w(8, s)) * (R)0.25;
+  R Mav[3][3];
+  const double* m1 = b.m + 9 * l0;
+  const double* m2 = b.m + 9 * (l0 + st);
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) Mav[a][q] = (R)0.5 * (cvt<R>(ld(m1 + a + 3 * q)) + cvt<R>(ld(m2 + a + 3 * q)));
+#pragma unroll
+  for (int iv = 0; iv < MB_NP; ++iv) {
+    R g1 = G[iv][0], g2 = G[iv][1], g3 = G[iv][2];
+    G[iv][0] = g1 * Mav[0][0] + g2 * Mav[1][0] + g3 * Mav[2][0];
+    G[iv][1] = g1 * Mav[0][1] + g2 * Mav[1][1] + g3 * Mav[2][1];
+    G[iv][2] = g1 * Mav[0][2] + g2 * Mav[1][2] + g3 * Mav[2][2];
+  }
+  R Pf[MB_NP];
+#pragma unroll
+  for (int iv = 0; iv < MB_NP; ++iv) Pf[iv] = (R)0.5 * (w(0, iv) + w(1, iv));
+  R frs = (R)0.5 * (w(0, 0) + w(1, 0));
+  R fp = (R)0.5 * (w(0, MB_IPR) + w(1, MB_IPR));
+  R drho, dT, dcp, dmil, dkl, tdf0;
+  int tint;
+  face_thermo<R>(p, frs, fp, drho, dT, tint, tdf0, dcp, dmil, dkl);
+  visc_flux<R>(p, G, Pf, nx, ny, nz, area, drho, dT, dcp, dmil, dkl, out + MB_NP);
+}
+
+// ---------------------------------------------------------------------------------------------
+// The boundary record of the cell (i,j,k) on face F, added into acc (the R_flat row of the cell).
+__device__ __forceinline__ void bc_face_geom(const DBlk& b, int Im, int Jm, int Km, int F, double* g) {
+  int dir = (F + 1) / 2, modfm = F % 2;
+  const double* f = (dir == 1) ? fm1p(b, Im - modfm, Jm, Km) : (dir == 2 ? fm2p(b, Im, Jm - modfm, Km) : fm3p(b, Im, Jm, Km - modfm));
+  g[0] = ld(f); g[1] = ld(f + 1); g[2] = ld(f + 2); g[3] = ld(f + 3);
+}
+
+// BC_Connection_Eul_lean (Lib_BC.f90:1770-1867)
+template <typename R>
+__device__ __noinline__ void bc_conn_eul(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
+                                         int Km, int Fm, double* acc) {
+  const long long nc = p.nc;
+  int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm1 = 1 - modfm, modfm2 = 1 - 2 * modfm, gstep = 2 * modfm - 1;
+  int o[4] = {modfm * (-gstep * GC) + modfm1 * gstep, modfm * (-gstep), modfm1 * (-gstep),
+              modfm1 * (-gstep * GC) + modfm * gstep};
+  const long long st = (dir == 1) ? 1 : (dir == 2 ? (long long)b.pi : (long long)b.pi * b.pj);
+  const long long rm = row(b, Im, Jm, Km);
+  const long long lm = rm - b.boff;
+  R dlc4[4];
+  long long rr[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    rr[q] = rm + o[q] * st;
+    dlc4[q] = cvt<R>(ld(b.dl + (dir - 1) + 3 * (lm + o[q] * st)));
+  }
+  double g[4];
+  bc_face_geom(b, Im, Jm, Km, Fm, g);
+  R nx = cvt<R>(g[0]), ny = cvt<R>(g[1]), nz = cvt<R>(g[2]), area = cvt<R>(g[3]);
+  const R beta_ = (R)1;
+  R Dl1 = dlc4[0] * (R)0.5, Dl2 = dlc4[1] * (R)0.5, Dl3 = dlc4[2] * (R)0.5, Dl4 = dlc4[3] * (R)0.5;
+  R D12 = Dl1 + Dl2, D23 = Dl2 + Dl3, D34 = Dl3 + Dl4;
+  R PL[MB_NP], PR[MB_NP];
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) {
+    R q1 = cvt<R>(ld(P + rr[0] + s * nc)), q2 = cvt<R>(ld(P + rr[1] + s * nc)), q3 = cvt<R>(ld(P + rr[2] + s * nc)),
+      q4 = cvt<R>(ld(P + rr[3] + s * nc));
+    R d21 = (q2 - q1) / D12, d32 = (q3 - q2) / D23, d43 = (q4 - q3) / D34;
+    PL[s] = q2 + beta_ * rlimiter(p.lim, d32, d21) * Dl2;
+    PR[s] = q3 - beta_ * rlimiter(p.lim, d43, d32) * Dl3;
+  }
+  R rhoL, RL, rhoR, RRr;
+  rotot_rtot(p, PL[0], rhoL, RL);
+  R aL = f_ss(p, PL[0], PL[MB_IPR], rhoL, RL);
+  rotot_rtot(p, PR[0], rhoR, RRr);
+  R aR = f_ss(p, PR[0], PR[MB_IPR], rhoR, RRr);
+  R F_r, F_u, F_v, F_w, F_E;
+  if (p.rs == 1)
+    hllc(p, PL[0], PL[MB_IU], PL[MB_IV], PL[MB_IW], PL[MB_IPR], aL, rhoL, RL, PR[0], PR[MB_IU], PR[MB_IV], PR[MB_IW],
+         PR[MB_IPR], aR, rhoR, RRr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
+  else
+    riemann_open(p, p.rs, PL[0], PL[MB_IU], PL[MB_IV], PL[MB_IW], PL[MB_IPR], aL, rhoL, PR[0], PR[MB_IU], PR[MB_IV],
+                 PR[MB_IW], PR[MB_IPR], aR, rhoR, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
+  R su = copysign((R)0.5, F_r), selL = (R)0.5 + su, selR = su - (R)0.5;
+  R Fmass = F_r * area;
+  R sg = (R)modfm2;
+  acc[0] = acc[0] + (double)(sg * Fmass * (selL * PL[0] / rhoL - selR * PR[0] / rhoR));
+  acc[MB_IU] = acc[MB_IU] + (double)(sg * F_u * area);
+  acc[MB_IV] = acc[MB_IV] + (double)(sg * F_v * area);
+  acc[MB_IW] = acc[MB_IW] + (double)(sg * F_w * area);
+  acc[MB_IPR] = acc[MB_IPR] + (double)(sg * F_E * area);
+}
+
+// BC_Connection_Visc_lean (Lib_BC.f90:2113-2178); pg = bc_pg(:,1:6) of the record
+template <typename R>
+__device__ __noinline__ void bc_conn_visc(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
+                                          int Km, int Fm, const double* __restrict__ pg, double* acc) {
+  const long long nc = p.nc;
+  int dir = (Fm + 1) / 2, modfm2 = 1 - 2 * (Fm % 2), gstep = 2 * (Fm % 2) - 1;
+  int ia = dir - 1, ib, ic;
+  long long sb, sc;
+  if (dir == 1) { ib = 1; ic = 2; sb = b.pi; sc = (long long)b.pi * b.pj; }
+  else if (dir == 2) { ib = 0; ic = 2; sb = 1; sc = (long long)b.pi * b.pj; }
+  else { ib = 0; ic = 1; sb = 1; sc = b.pi; }
+  const long long st = (dir == 1) ? 1 : (dir == 2 ? (long long)b.pi : (long long)b.pi * b.pj);
+  const long long r1 = row(b, Im, Jm, Km);
+  const long long l1 = r1 - b.boff;
+  const long long lg = l1 - gstep * st;  // the ghost cell Im - gstep along dir
+  R M[3][3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q)
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+      M[a][q] = (R)0.5 * (cvt<R>(ld(b.m + a + 3 * q + 9 * l1)) + cvt<R>(ld(b.m + a + 3 * q + 9 * lg)));
+  // cells: 0 loc, 1 ghost (Pg(:,1)), 2 b+, 3 b-, 4 c+, 5 c-, 6..9 Pg(:,3..6)
+  const long long rc[6] = {r1, 0, r1 + sb, r1 - sb, r1 + sc, r1 - sc};
+  auto pv = [&](int q, int s) -> R {
+    if (q == 1) return cvt<R>(ld(pg + s));
+    if (q >= 6) return cvt<R>(ld(pg + s + MB_NP * (q - 4)));
+    return cvt<R>(ld(P + rc[q] + s * nc));
+  };
+  R rh[10], rg[10];
+#pragma unroll
+  for (int q = 0; q < 10; ++q) rotot_rtot(p, pv(q, 0), rh[q], rg[q]);
+  R G2l[MB_NP][3], G2g[MB_NP][3], Pa[MB_NP];
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) {
+    R vv[10];
+#pragma unroll
+    for (int q = 0; q < 10; ++q) {
+      R x = pv(q, s);
+      if (s >= MB_IU && s <= MB_IW) vv[q] = x;
+      else if (s == MB_IPR) vv[q] = x / (rh[q] * rg[q]);
+      else vv[q] = x / rh[q];
+    }
+    R gl[3], gg[3];
+    gl[ia] = (vv[1] - vv[0]) * (R)modfm2;
+    gl[ib] = (vv[2] - vv[3]) * (R)0.5;
+    gl[ic] = (vv[4] - vv[5]) * (R)0.5;
+    gg[ia] = (vv[0] - vv[1]) * (R)(-modfm2);
+    gg[ib] = (vv[7] - vv[6]) * (R)0.5;
+    gg[ic] = (vv[9] - vv[8]) * (R)0.5;
+#pragma unroll
+    for (int kk = 0; kk < 3; ++kk) {
+      G2l[s][kk] = gl[0] * M[0][kk] + gl[1] * M[1][kk] + gl[2] * M[2][kk];
+      G2g[s][kk] = gg[0] * M[0][kk] + gg[1] * M[1][kk] + gg[2] * M[2][kk];
+    }
+    Pa[s] = (R)0.5 * (pv(0, s) + pv(1, s));
+  }
+  R rho_f, T_f, td, cp_f, mil_f, kl_f;
+  int ti;
+  face_thermo(p, Pa[0], Pa[MB_IPR], rho_f, T_f, ti, td, cp_f, mil_f, kl_f);
+  double g[4];
+  bc_face_geom(b, Im, Jm, Km, Fm, g);
+  R nx = cvt<R>(g[0]), ny = cvt<R>(g[1]), nz = cvt<R>(g[2]), area = cvt<R>(g[3]);
+  R Fl[MB_NP], Fg[MB_NP];
+  visc_flux(p, G2l, Pa, nx, ny, nz, area, rho_f, T_f, cp_f, mil_f, kl_f, Fl);
+  visc_flux(p, G2g, Pa, nx, ny, nz, area, rho_f, T_f, cp_f, mil_f, kl_f, Fg);
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) acc[s] = acc[s] - (double)((R)0.5 * (R)modfm2 * (Fl[s] + Fg[s]));
+}
+
+// BC_Extrapolation (Lib_BC.f90:1119-1165)
+template <typename R>
+__device__ __noinline__ void bc_extrap(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
+                                       int Km, int Fm, double* acc) {
+  const long long nc = p.nc;
+  const long long r = row(b, Im, Jm, Km);
+  R Pr[MB_NP];
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) Pr[s] = cvt<R>(ld(P + r + s * nc));
+  double g[4];
+  bc_face_geom(b, Im, Jm, Km, Fm, g);
+  R nx = cvt<R>(g[0]), ny = cvt<R>(g[1]), nz = cvt<R>(g[2]), area = cvt<R>(g[3]);
+  R Un = Pr[MB_IU] * nx + Pr[MB_IV] * ny + Pr[MB_IW] * nz;
+  R F[MB_NP];
+  R Fmass = (R)0;
+  F[0] = Pr[0] * Un * area;
+  Fmass = Fmass + F[0];
+  F[MB_IU] = Fmass * Pr[MB_IU] + Pr[MB_IPR] * area * nx;
+  F[MB_IV] = Fmass * Pr[MB_IV] + Pr[MB_IPR] * area * ny;
+  F[MB_IW] = Fmass * Pr[MB_IW] + Pr[MB_IPR] * area * nz;
+  R vmag = rsqrt_(Pr[MB_IU] * Pr[MB_IU] + Pr[MB_IV] * Pr[MB_IV] + Pr[MB_IW] * Pr[MB_IW]);
+  F[MB_IPR] = Fmass * H0(p, Pr[MB_IPR], Pr[0], vmag);
+  R sg = (R)face_sign(Fm);
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) acc[s] = acc[s] + (double)(sg * F[s]);
+}
+
+// the records of the faces 1..6 that the cell (i,j,k) lies on, in face order
+template <typename R, bool VISC>
+__device__ __forceinline__ void bc_cell(const Params& p, const DBlk& b, const double* __restrict__ P, int i, int j,
+                                        int k, double* acc) {
+  const int n[3] = {b.n1, b.n2, b.n3};
+  const int c[3] = {i, j, k};
+#pragma unroll 1
+  for (int F = 1; F <= 6; ++F) {
+    const int ax = (F - 1) >> 1;
+    const bool on = (F & 1) ? (c[ax] == 1) : (c[ax] == n[ax]);
+    if (!on || b.rmap[F - 1] < 0) continue;
+    int t;
+    if (ax == 0) t = (j - 1) + (k - 1) * b.n2;
+    else if (ax == 1) t = (i - 1) + (k - 1) * b.n1;
+    else t = (i - 1) + (j - 1) * b.n1;
+    const int rid = p.rec_map[b.rmap[F - 1] + t];
+    if (rid < 0) continue;
+    const DRec& rc = p.rec[rid];
+    if (rc.type == 1) {
+      bc_conn_eul<R>(p, b, P, i, j, k, F, acc);
+      if (VISC) bc_conn_visc<R>(p, b, P, i, j, k, F, p.pg + (long long)rc.pg * 6 * MB_NP, acc);
+    } else if (rc.type == 11) {
+      bc_extrap<R>(p, b, P, i, j, k, F, acc);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// The conservative state update of one cell (newstate_cons_body.inc), FP64. Returns the new
+// primitive state in pn.
+__device__ __forceinline__ void cons_update(const Params& p, const double* pc, const double* po, const double* res,
+                                            double vol, double dt, double rkc, double tc, double* pn) {
+  const double strang = 1.0;
+  double cons[MB_NP], cold[MB_NP], rl[MB_NP];
+  auto prim2cons = [&](const double* q, double* u) {
+    double rho = 0.0 + q[0];
+    double Rg = 0.0 + p.ri * q[0] / rho;
+    double vmag = 0.0;
+#pragma unroll
+    for (int s = MB_IU; s <= MB_IW; ++s) vmag = vmag + q[s] * q[s];
+    double Tl = q[MB_IPR] / (Rg * rho);
+    int ti = tidx(p, Tl);
+    double Td = Tl - (double)ti;
+    double hs = p.h[ti] + Td * (p.h[ti + 1] - p.h[ti]);
+    double hmix = 0.0 + hs * q[0] / rho;
+    double E0 = hmix - q[MB_IPR] / rho + 0.5 * vmag;
+    u[0] = q[0];
+#pragma unroll
+    for (int s = MB_IU; s <= MB_IW; ++s) u[s] = rho * q[s];
+    u[MB_IPR] = rho * E0;
+  };
+  prim2cons(po, cold);
+  prim2cons(pc, cons);
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) rl[s] = -res[s] / vol * dt * strang;
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) cons[s] = cold[s] + (cons[s] - cold[s] + rl[s]) * rkc;
+  double rho = 0.0 + cons[0];
+  double Rg = 0.0 + p.ri * cons[0] / rho;
+  pn[0] = cons[0];
+#pragma unroll
+  for (int s = MB_IU; s <= MB_IW; ++s) pn[s] = cons[s] / rho;
+  double vmag = 0.0;
+#pragma unroll
+  for (int s = MB_IU; s <= MB_IW; ++s) vmag = vmag + (cons[s] / rho) * (cons[s] / rho);
+  double energy = cons[MB_IPR] / rho - 0.5 * vmag;
+  double diff_en = 1e3, T_it = tc;
+  int it = 1;
+  while ((fabs(diff_en / energy) >= 1e-6) && (it <= 20)) {
+    int ti = tidx(p, T_it);
+    double Td = T_it - (double)ti;
+    double cv = -Rg, enth = 0.0;
+    double cps = p.cp[ti] + Td * (p.cp[ti + 1] - p.cp[ti]);
+    double hs = p.h[ti] + Td * (p.h[ti + 1] - p.h[ti]);
+    cv = cv + cons[0] / rho * cps;
+    enth = enth + cons[0] / rho * hs;
+    double p_it = rho * Rg * T_it;
+    diff_en = fabs((enth - p_it / rho) - energy);
+    T_it = T_it + (energy - (enth - p_it / rho)) / cv;
+    it = it + 1;
+  }
+  pn[MB_IPR] = rho * Rg * T_it;
+  if (pn[0] < 1e-20) pn[0] = 1e-20;
+}
+
+// local dt of one cell (dt_blk.inc: min rule :156-191, additive rule :79-155), FP64
+__device__ __forceinline__ double cell_dt(const Params& p, const DBlk& b, long long l, const double* pl) {
+  double rho, Rg;
+  rotot_rtot(p, pl[0], rho, Rg);
+  double Tc = pl[MB_IPR] / (rho * Rg);
+  double Sound = f_ss(p, pl[0], pl[MB_IPR], rho, Rg);
+  const double* m = b.m + 9 * l;
+  const double* dl = b.dl + 3 * l;
+  double dtc = 1e8;
+  if (p.dt_additive) {
+    double ra_c = 0.0, ra_v = 0.0;
+    for (int d = 0; d < p.ndir; ++d) {
+      double m0 = ld(m + d), m1 = ld(m + d + 3), m2 = ld(m + d + 6);
+      double gn = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
+      double vel_ = fabs(pl[MB_IU] * m0 + pl[MB_IV] * m1 + pl[MB_IW] * m2) / gn;
+      double lambda = vel_ + Sound;
+      ra_c = ra_c + lambda * gn;
+      ra_v = ra_v + gn * gn;
+    }
+    if (p.visc) {
+      if (p.ndir == 3) {
+        double g[3][3];
+        for (int d = 0; d < 3; ++d)
+          for (int a = 0; a < 3; ++a) g[d][a] = ld(m + d + 3 * a);
+        auto dot = [&](int x, int y) { return g[x][0] * g[y][0] + g[x][1] * g[y][1] + g[x][2] * g[y][2]; };
+        auto nr = [&](int x) { return sqrt(g[x][0] * g[x][0] + g[x][1] * g[x][1] + g[x][2] * g[x][2]); };
+        double c12 = dot(0, 1) / (nr(0) * nr(1)), c13 = dot(0, 2) / (nr(0) * nr(2)), c23 = dot(1, 2) / (nr(1) * nr(2));
+        double ss = c12 * c12 + c13 * c13 + c23 * c23;
+        double qp = c12 * c13 * c23;
+        if (ss + 2.0 * qp > 1.0) {
+          double mr = 2.0 * sqrt(ss / 3.0) * cos(acos(mx(-1.0, mn(1.0, 3.0 * sqrt(3.0) * qp / pow(ss, 1.5)))) / 3.0);
+          ra_v = ra_v * 0.25 * (2.0 + mr + 1.0 / mr);
+        }
+      }
+      int ta = tidx(p, Tc);
+      double tda = Tc - (double)ta;
+      double cpa = f_cp(p, pl[0], ta, tda, rho);
+      double cva = cpa - Rg;
+      double mila, kla;
+      wilke(p, pl[0], rho, ta, tda, mila, kla);
+      if (p.prandtl > 0.0) kla = mila * cpa / p.prandtl;
+      const double mie = 0.0, prt = 0.85;
+      double Dmx = mx(4.0 / 3.0 * (mila + mie) / rho, (kla + mie * cpa / prt) / (rho * cva));
+      dtc = 1.0 / (ra_c / p.cfl + Dmx * ra_v / p.vnn);
+    } else {
+      dtc = p.cfl / ra_c;
+    }
+  } else {
+    for (int d = 0; d < p.ndir; ++d) {
+      double m0 = ld(m + d), m1 = ld(m + d + 3), m2 = ld(m + d + 6);
+      double nrm = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
+      double v0 = m0 / nrm, v1 = m1 / nrm, v2 = m2 / nrm;
+      double vel_ = fabs(pl[MB_IU] * v0 + pl[MB_IV] * v1 + pl[MB_IW] * v2);
+      double lambda = vel_ + Sound;
+      double dtd = ld(dl + d) / lambda * p.cfl;
+      dtc = mn(dtd, dtc);
+    }
+    if (p.visc) {
+      int ti = tidx(p, Tc);
+      double td = Tc - (double)ti, mil, kl;
+      wilke(p, pl[0], rho, ti, td, mil, kl);
+      double mi = 0.0 + mil;
+      for (int d = 0; d < p.ndir; ++d) {
+        double dlv = ld(dl + d);
+        double dtd = (rho * (dlv * dlv) * p.vnn) / mi;
+        dtc = mn(dtd, dtc);
+      }
+    }
+  }
+  return dtc * 1.0;
+}
+
+// min over the CTA of a positive double, then one atomic into the device clock
+__device__ __forceinline__ void cta_min_dt(const Params& p, double v, double* sred) {
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = mn(v, __shfl_xor_sync(full, v, o));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (lane == 0) sred[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = (lane < nw) ? sred[lane] : 1e300;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = mn(v, __shfl_xor_sync(full, v, o));
+    if (lane == 0 && v < 1e300) atomicMin(&p.st->dtmin_bits, (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+__device__ __forceinline__ void report_bad_state(const Params& p, int blk, int i, int j, int k) {
+  atomicAdd(&p.st->n_bad_state, 1);
+  if (atomicCAS(&p.st->first_bad_claimed, 0, 1) == 0) {
+    p.st->bad_blk = blk; p.st->bad_i = i; p.st->bad_j = j; p.st->bad_k = k;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+template <typename R, int TY, bool VISC, int MODE>
+__global__ void __launch_bounds__(32 * TY, 1)
+k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pin, const double* Pold, double* Pout,
+        double* Rout, double rkc, int last) {
+  constexpr int NF = VISC ? 2 * MB_NP : MB_NP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  typedef R RowI[33][NF];
+  typedef R RowJ[32][NF];
+  RowI* sFi = reinterpret_cast<RowI*>(smem_raw);                         // [TY][33][NF]
+  RowJ* sFj = reinterpret_cast<RowJ*>(smem_raw + sizeof(R) * TY * 33 * NF); // [TY+1][32][NF]
+  RowJ* sFk0 = reinterpret_cast<RowJ*>(smem_raw + sizeof(R) * (TY * 33 + (TY + 1) * 32) * NF);  // [2][TY][32][NF]
+  __shared__ double sred[32];
+  const DTile t = tiles[blockIdx.x];
+  const DBlk b = p.blk[t.blk];
+  const int tid = threadIdx.x;
+  const int tx = tid & 31, ty = tid >> 5;
+  const int i = t.i0 + tx, j = t.j0 + ty;
+  const bool own = (i <= b.n1) && (j <= b.n2);
+  const double dt = (MODE == MODE_UPDATE) ? p.st->dt : 0.0;
+  double dtloc = 1e300;
+  int kb = 0;  // buffer of the k-face above the current plane
+  for (int k = t.k0; k < t.k1; ++k) {
+    // ---- face tasks: i-faces, j-faces, k-faces of this plane, one call site
+    // task list of this thread: 0 = i-face #tid, 1 = extra i-face (last warp, lanes < TY),
+    // 2 = j-face #tid, 3 = extra j-face row (warp 0), 4 = k-face below the first plane, 5 = k-face above
+#pragma unroll 1
+    for (int task = 0; task < 6; ++task) {
+      int d = -1, fi = 0, fj = 0, fk = k;
+      R* dst = nullptr;
+      if (task == 0 || task == 1) {
+        int f;
+        if (task == 0) f = tid;
+        else { if (ty != TY - 1 || tx >= TY) continue; f = 32 * TY + tx; }
+        const int rw = f / 33, cl = f - rw * 33;
+        fi = t.i0 + cl - 1; fj = t.j0 + rw;
+        if (fi >= 1 && fi <= b.n1 - 1 && fj <= b.n2) { d = 0; dst = &sFi[rw][cl][0]; }
+      } else if (task == 2 || task == 3) {
+        int f;
+        if (task == 2) f = tid;
+        else { if (ty != 0) continue; f = 32 * TY + tx; }
+        const int rw = f >> 5, cl = f & 31;
+        fi = t.i0 + cl; fj = t.j0 + rw - 1;
+        if (fj >= 1 && fj <= b.n2 - 1 && fi <= b.n1) { d = 1; dst = &sFj[rw][cl][0]; }
+      } else if (task == 4) {
+        if (k != t.k0 || !own || k <= 1) continue;
+        fi = i; fj = j; fk = k - 1; d = 2; dst = &sFk0[(kb ^ 1) * TY + ty][tx][0];
+      } else {
+        if (!own || k >= b.n3) continue;
+        fi = i; fj = j; fk = k; d = 2; dst = &sFk0[kb * TY + ty][tx][0];
+      }
+      if (d < 0) continue;
+      R out[NF];
+      face_flux<R, VISC>(p, b, Pin, d, fi, fj, fk, out);
+#pragma unroll
+      for (int q = 0; q < NF; ++q) dst[q] = out[q];
+    }
+    __syncthreads();
+    if (own) {
+      // ---- pass 2 (pass2_body.inc): convective i +,-, j +,-, k +,-, then viscous i -,+, j -,+, k -,+
+      double acc[MB_NP] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      const R* fr = (i < b.n1) ? &sFi[ty][tx + 1][0] : nullptr;
+      const R* fl = (i > 1) ? &sFi[ty][tx][0] : nullptr;
+      const R* gr = (j < b.n2) ? &sFj[ty + 1][tx][0] : nullptr;
+      const R* gl = (j > 1) ? &sFj[ty][tx][0] : nullptr;
+      const R* hr = (k < b.n3) ? &sFk0[kb * TY + ty][tx][0] : nullptr;
+      const R* hl = (k > 1) ? &sFk0[(kb ^ 1) * TY + ty][tx][0] : nullptr;
+#pragma unroll
+      for (int s = 0; s < MB_NP; ++s) {
+        double a = 0.0;
+        if (fr) a = a + (double)fr[s];
+        if (fl) a = a - (double)fl[s];
+        if (gr) a = a + (double)gr[s];
+        if (gl) a = a - (double)gl[s];
+        if (hr) a = a + (double)hr[s];
+        if (hl) a = a - (double)hl[s];
+        if (VISC) {
+          if (fr) a = a - (double)fr[MB_NP + s];
+          if (fl) a = a + (double)fl[MB_NP + s];
+          if (gr) a = a - (double)gr[MB_NP + s];
+          if (gl) a = a + (double)gl[MB_NP + s];
+          if (hr) a = a - (double)hr[MB_NP + s];
+          if (hl) a = a + (double)hl[MB_NP + s];
+        }
+        acc[s] = a;
+      }
+      // ---- boundary records of the cell, face order 1..6
+      if (i == 1 || i == b.n1 || j == 1 || j == b.n2 || k == 1 || k == b.n3)
+        bc_cell<R, VISC>(p, b, Pin, i, j, k, acc);
+      const long long r = row(b, i, j, k);
+      if (MODE == MODE_RESIDUAL) {
+#pragma unroll
+        for (int s = 0; s < MB_NP; ++s) Rout[r + s * p.nc] = acc[s];
+      } else {
+        double pc[MB_NP], po[MB_NP], pn[MB_NP];
+#pragma unroll
+        for (int s = 0; s < MB_NP; ++s) { pc[s] = ld(Pin + r + s * p.nc); po[s] = Pold[r + s * p.nc]; }
+        double rho, T;
+        cell_rho_T(p, pc[0], pc[MB_IPR], rho, T);
+        if (p.guard && !(T > 1.0 && T < 9990.0)) {  // thermo guard (Mod_Thermo_Cache.f90:317-327)
+          atomicAdd(&p.st->n_bad_thermo, 1);
+          if (T != T) T = 300.0;
+          T = mn(mx(T, 1.0), 9990.0);
+        }
+        const double vol = ld(b.vol + (r - b.boff));
+        cons_update(p, pc, po, acc, vol, dt, rkc, T, pn);
+        bool bad = !(pn[MB_IPR] >= 0.0);
+#pragma unroll
+        for (int s = 0; s < MB_NP; ++s) bad = bad || !isfinite(pn[s]);
+        if (bad) report_bad_state(p, t.blk, i, j, k);
+#pragma unroll
+        for (int s = 0; s < MB_NP; ++s) Pout[r + s * p.nc] = pn[s];
+        if (last) dtloc = mn(dtloc, cell_dt(p, b, r - b.boff, pn));
+      }
+    }
+    __syncthreads();
+    kb ^= 1;
+  }
+  if (MODE == MODE_UPDATE && last) cta_min_dt(p, dtloc, sred);
+}
+
+template <typename R, int TY, bool VISC>
+constexpr size_t sweep_smem() {
+  return sizeof(R) * (size_t)(TY * 33 + (TY + 1) * 32 + 2 * TY * 32) * (VISC ? 2 * MB_NP : MB_NP);
+}
+
+}  // namespace mb

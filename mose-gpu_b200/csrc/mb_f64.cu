@@ -1,0 +1,207 @@
+// mb_f64.cu -- the FP64 form of the engine: fused sweep instantiations and the per-cell / ghost
+// kernels. Built with --fmad=false so that every statement rounds as written (the operation order of
+// the reference statements is kept in mb_physics.cuh / mb_engine.cuh).
+#include "mb_launch.h"
+
+namespace mb {
+
+// ---- ghost fill (numerics/fluxes/bc/Lib_Extrapolation.f90) ----
+// Fill_Ghost_Cell_blk (:643-730): zero-gradient ghosts of types 4 / 11 (Ghost_ZG_Extrapolate :590-614),
+// the second-order extrapolation 3 x3 - 3 x2 + x1 of walls (Ghost_Extrapolate :616-641)
+__global__ void k_ghost_phys(Params p, const GRec* __restrict__ rec, const int* __restrict__ list, int n, double* P) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const GRec r = rec[list[q]];
+  const DBlk b = p.blk[r.blk];
+  const int dir = (r.face + 1) / 2, gstep = 2 * (r.face % 2) - 1;
+  const long long st = (dir == 1) ? 1 : (dir == 2 ? (long long)b.pi : (long long)b.pi * b.pj);
+  const long long src = row(b, r.i, r.j, r.k);
+  const long long nc = p.nc;
+  if (r.type == 5) {
+    const int step = -gstep;
+    for (int g = 1; g <= GC; ++g) {
+      long long d0 = src + (long long)(g * step) * st, a1 = src + (long long)((g - 1) * step) * st,
+                a2 = src + (long long)((g - 2) * step) * st, a3 = src + (long long)((g - 3) * step) * st;
+      for (int s = 0; s < MB_NP; ++s) P[d0 + s * nc] = 3.0 * P[a1 + s * nc] - 3.0 * P[a2 + s * nc] + P[a3 + s * nc];
+    }
+  } else {
+    for (int g = 1; g <= GC; ++g) {
+      long long dst = src - (long long)(gstep * g) * st;
+      for (int s = 0; s < MB_NP; ++s) P[dst + s * nc] = P[src + s * nc];
+    }
+  }
+}
+
+// extrapolation-ghost = cubic on the 400 faces (Fill_Ghost_Cubic_Extrapolation_blk, :859-879),
+// a separate launch after every zero-gradient ghost is written
+__global__ void k_ghost_cubic(Params p, const GRec* __restrict__ rec, const int* __restrict__ list, int n, double* P) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const GRec r = rec[list[q]];
+  const DBlk b = p.blk[r.blk];
+  const int dir = (r.face + 1) / 2, gstep = 2 * (r.face % 2) - 1, step = -gstep;
+  const long long st = (dir == 1) ? 1 : (dir == 2 ? (long long)b.pi : (long long)b.pi * b.pj);
+  const long long src = row(b, r.i, r.j, r.k);
+  const long long nc = p.nc;
+  for (int g = 1; g <= GC; ++g) {
+    long long d0 = src + (long long)(g * step) * st, a1 = src + (long long)((g - 1) * step) * st,
+              a2 = src + (long long)((g - 2) * step) * st, a3 = src + (long long)((g - 3) * step) * st;
+    for (int s = 0; s < MB_NP; ++s) P[d0 + s * nc] = 3.0 * P[a1 + s * nc] - 3.0 * P[a2 + s * nc] + P[a3 + s * nc];
+  }
+}
+
+// 1:1 and periodic connections (Ghost_Connection_pair, :1023-1134): receiver ghost layer g <- donor layer g.
+// The donor layers are interior cells, so the copies of one launch never read what another writes.
+__global__ void k_ghost_copy(const long long* __restrict__ dst, const long long* __restrict__ src, int n, long long nc,
+                             double* P) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long long)n * MB_NP) return;
+  const int e = (int)(q % n), s = (int)(q / n);
+  P[dst[e] + s * nc] = P[src[e] + s * nc];
+}
+
+// bc_pg(:,1:6) of every connection after all ghosts are written (Ghost_Connection_pairs_B, :1136-1191)
+__global__ void k_pg(const long long* __restrict__ src, int nconn, long long nc, const double* __restrict__ P,
+                     double* pg) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long long)nconn * 6 * MB_NP) return;
+  const long long e = q / MB_NP;  // (conn, slot)
+  const int s = (int)(q - e * MB_NP);
+  pg[q] = P[src[e] + s * nc];
+}
+
+// ---- Compute_dt alone: local dt of every interior cell, reduced into the device clock ----
+__global__ void __launch_bounds__(32 * TY_AUX) k_dt(Params p, const DTile* __restrict__ tiles, const double* P) {
+  __shared__ double sred[32];
+  const DTile t = tiles[blockIdx.x];
+  const DBlk b = p.blk[t.blk];
+  const int i = t.i0 + (threadIdx.x & 31), j = t.j0 + (threadIdx.x >> 5);
+  double v = 1e300;
+  if (i <= b.n1 && j <= b.n2) {
+    for (int k = t.k0; k < t.k1; ++k) {
+      const long long r = row(b, i, j, k);
+      double pl[MB_NP];
+      for (int s = 0; s < MB_NP; ++s) pl[s] = P[r + s * p.nc];
+      v = mn(v, cell_dt(p, b, r - b.boff, pl));
+    }
+  }
+  cta_min_dt(p, v, sred);
+}
+
+// ---- RK_Newstate alone: the conservative update of every interior cell from a given residual ----
+__global__ void __launch_bounds__(32 * TY_AUX) k_update(Params p, const DTile* __restrict__ tiles, double* P,
+                                                        const double* PO, const double* R, double rkc, double dt) {
+  const DTile t = tiles[blockIdx.x];
+  const DBlk b = p.blk[t.blk];
+  const int i = t.i0 + (threadIdx.x & 31), j = t.j0 + (threadIdx.x >> 5);
+  if (i > b.n1 || j > b.n2) return;
+  for (int k = t.k0; k < t.k1; ++k) {
+    const long long r = row(b, i, j, k);
+    double pc[MB_NP], po[MB_NP], res[MB_NP], pn[MB_NP];
+    for (int s = 0; s < MB_NP; ++s) { pc[s] = P[r + s * p.nc]; po[s] = PO[r + s * p.nc]; res[s] = R[r + s * p.nc]; }
+    double rho, T;
+    cell_rho_T(p, pc[0], pc[MB_IPR], rho, T);
+    if (p.guard && !(T > 1.0 && T < 9990.0)) {
+      atomicAdd(&p.st->n_bad_thermo, 1);
+      if (T != T) T = 300.0;
+      T = mn(mx(T, 1.0), 9990.0);
+    }
+    cons_update(p, pc, po, res, ld(b.vol + (r - b.boff)), dt, rkc, T, pn);
+    bool bad = !(pn[MB_IPR] >= 0.0);
+    for (int s = 0; s < MB_NP; ++s) bad = bad || !isfinite(pn[s]);
+    if (bad) report_bad_state(p, t.blk, i, j, k);
+    for (int s = 0; s < MB_NP; ++s) P[r + s * p.nc] = pn[s];
+  }
+}
+
+__global__ void k_reset_dt(Params p) { p.st->dtmin_bits = (unsigned long long)__double_as_longlong(1e300); }
+
+// the step's dt (Compute_dt's dtglobal = 1e5 then the cell minimum, Mod_Explicit.f90:122; Set_Global_dt;
+// Clip_dt_To_Timemax, Mod_dt.f90:283-296), the simulated time, and a fresh minimum for the next step
+__global__ void k_clock(Params p, int time_clip, double threshold) {
+  DevState* st = p.st;
+  double dtg = 1e5;
+  double dm = __longlong_as_double((long long)st->dtmin_bits);
+  dtg = mn(dm, dtg);
+  if (time_clip) {
+    double rem = threshold - st->time;
+    if (rem > 0.0 && dtg > rem) dtg = rem * (1.0 + 1e-12);
+  }
+  st->dt = dtg;
+  st->time = st->time + dtg;
+  st->steps = st->steps + 1;
+  st->dtmin_bits = (unsigned long long)__double_as_longlong(1e300);
+}
+
+// ---- launchers ----
+template <int TY, bool VISC, int MODE>
+static cudaError_t sweep_one(const Params& p, const DTile* tiles, int ntiles, const double* Pin, const double* Pold,
+                             double* Pout, double* Rout, double rkc, int last, cudaStream_t s) {
+  const size_t sm = sweep_smem<double, TY, VISC>();
+  k_sweep<double, TY, VISC, MODE><<<ntiles, 32 * TY, sm, s>>>(p, tiles, Pin, Pold, Pout, Rout, rkc, last);
+  return cudaGetLastError();
+}
+
+template <int TY, bool VISC, int MODE>
+static cudaError_t set_attr() {
+  return cudaFuncSetAttribute(k_sweep<double, TY, VISC, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sweep_smem<double, TY, VISC>());
+}
+
+cudaError_t sweep_setup_f64() {
+  cudaError_t e;
+  if ((e = set_attr<TY_F64, true, MODE_RESIDUAL>()) != cudaSuccess) return e;
+  if ((e = set_attr<TY_F64, true, MODE_UPDATE>()) != cudaSuccess) return e;
+  if ((e = set_attr<TY_F64, false, MODE_RESIDUAL>()) != cudaSuccess) return e;
+  return set_attr<TY_F64, false, MODE_UPDATE>();
+}
+
+cudaError_t sweep_f64(const Params& p, const DTile* tiles, int ntiles, int mode, const double* Pin, const double* Pold,
+                      double* Pout, double* Rout, double rkc, int last, cudaStream_t s) {
+  if (p.visc) {
+    if (mode == MODE_RESIDUAL) return sweep_one<TY_F64, true, MODE_RESIDUAL>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
+    return sweep_one<TY_F64, true, MODE_UPDATE>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
+  }
+  if (mode == MODE_RESIDUAL) return sweep_one<TY_F64, false, MODE_RESIDUAL>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
+  return sweep_one<TY_F64, false, MODE_UPDATE>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
+}
+
+static inline unsigned nblk_for(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+cudaError_t ghost_fill(const Params& p, const GhostLists& g, double* P, cudaStream_t s, int* nl) {
+  *nl = 0;
+  if (g.nphys > 0) { k_ghost_phys<<<nblk_for(g.nphys, 128), 128, 0, s>>>(p, g.rec, g.phys, g.nphys, P); ++*nl; }
+  if (g.ncubic > 0) { k_ghost_cubic<<<nblk_for(g.ncubic, 128), 128, 0, s>>>(p, g.rec, g.cubic, g.ncubic, P); ++*nl; }
+  if (g.ncopy > 0) {
+    k_ghost_copy<<<nblk_for((long long)g.ncopy * MB_NP, 256), 256, 0, s>>>(g.cdst, g.csrc, g.ncopy, p.nc, P);
+    ++*nl;
+  }
+  if (g.nconn > 0 && p.visc) {
+    k_pg<<<nblk_for((long long)g.nconn * 6 * MB_NP, 256), 256, 0, s>>>(g.pgsrc, g.nconn, p.nc, P, g.pg);
+    ++*nl;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t dt_cells(const Params& p, const DTile* tiles, int ntiles, const double* P, cudaStream_t s) {
+  k_dt<<<ntiles, 32 * TY_AUX, 0, s>>>(p, tiles, P);
+  return cudaGetLastError();
+}
+
+cudaError_t update_cells(const Params& p, const DTile* tiles, int ntiles, double* P, const double* PO, const double* R,
+                         double rkc, double dt, cudaStream_t s) {
+  k_update<<<ntiles, 32 * TY_AUX, 0, s>>>(p, tiles, P, PO, R, rkc, dt);
+  return cudaGetLastError();
+}
+
+cudaError_t reset_dt(const Params& p, cudaStream_t s) {
+  k_reset_dt<<<1, 1, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t clock_step(const Params& p, int time_clip, double threshold, cudaStream_t s) {
+  k_clock<<<1, 1, 0, s>>>(p, time_clip, threshold);
+  return cudaGetLastError();
+}
+
+}  // namespace mb

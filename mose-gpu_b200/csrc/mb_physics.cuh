@@ -1,0 +1,553 @@
+// mb_physics.cuh -- device arithmetic of the face fluxes, boundary records, state update and local
+// dt of the B200 engine. Templated on the flux arithmetic type R: double for the plain FP64 form,
+// float for the mixed form (reconstruction, Riemann and viscous flux arithmetic in FP32; state,
+// RK accumulation, T/p recovery and dt stay FP64 -- those routines are not templated).
+//
+// The FP64 instantiation keeps the reference's operation order statement by statement and is built
+// with --fmad=false, so it rounds exactly as written. Sources (paths relative to the reference root):
+//   convective face       src/lib/gpu/conv_physics.inc:1-179
+//   limiters              src/lib/numerics/space/Lib_Limiters.f90:65-97
+//   AUSM+ / LMRoe         src/lib/numerics/fluxes/riemann_open_body.inc:100-150, 679-730, 965-1091
+//   HLLC (records)        src/lib/numerics/fluxes/Lib_Riemann_HLL.f90:21-134, 209-310
+//   viscous face          src/lib/gpu/diff_cuf_kernels.inc:11-87, diff_physics.inc:1-161,
+//                         Mod_Diffusive.f90:311-325 (face thermo)
+//   connection records    src/lib/numerics/fluxes/bc/Lib_BC.f90:1770-1867, 2113-2178
+//   extrapolation record  src/lib/numerics/fluxes/bc/Lib_BC.f90:1119-1165
+//   state update          src/lib/gpu/newstate_cons_body.inc:1-89
+//   local dt              src/lib/gpu/dt_blk.inc:11-222
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define MB_NP 5
+#define MB_IU 1
+#define MB_IV 2
+#define MB_IW 3
+#define MB_IPR 4
+
+namespace mb {
+
+constexpr int GC = 2;
+constexpr double RUNIV = 8314.46261815324;  // lib/FLINT/src/lib/Lib_ThermoTransport.f90:13
+
+struct DBlk {
+  int n1, n2, n3, pi, pj;
+  int rmap[6];          // offset of each face's record map in Params::rec_map (-1: none)
+  long long boff;
+  const double *fm1, *fm2, *fm3, *dl, *m, *vol;
+};
+
+struct DRec {
+  int type;
+  int pg;               // row of the record in the transverse-stencil table (connections), -1 otherwise
+  double q[MB_NP];
+};
+
+// device status + clock of the time loop (one per context)
+struct DevState {
+  unsigned long long dtmin_bits;  // min of the local dt of the step being computed (positive doubles order as u64)
+  double dt;                      // dt of the current step
+  double time;
+  int steps;
+  int code;
+  int n_bad_state;
+  int n_bad_thermo;
+  int bad_blk, bad_i, bad_j, bad_k;
+  int first_bad_claimed;
+};
+
+struct Params {
+  const DBlk* blk;
+  const int* rec_map;
+  const DRec* rec;
+  const double* pg;        // [record][6][5]
+  const double *cp, *h, *mu, *k;      // FP64 tables, indexed by the table row (pointer shifted by -tmin)
+  const float *cpf, *hf, *muf, *kf;   // FP32 copies for the mixed form
+  DevState* st;
+  long long nc;
+  int tmin, tmax;
+  double wm, ri;
+  int lim, rs, visc, ndir, dt_additive, guard, state_check;
+  double cfl, vnn, prandtl, schmidt, mco;
+};
+
+template <typename R> struct Tab;
+template <> struct Tab<double> {
+  __device__ static const double* cp(const Params& p) { return p.cp; }
+  __device__ static const double* h(const Params& p) { return p.h; }
+  __device__ static const double* mu(const Params& p) { return p.mu; }
+  __device__ static const double* k(const Params& p) { return p.k; }
+};
+template <> struct Tab<float> {
+  __device__ static const float* cp(const Params& p) { return p.cpf; }
+  __device__ static const float* h(const Params& p) { return p.hf; }
+  __device__ static const float* mu(const Params& p) { return p.muf; }
+  __device__ static const float* k(const Params& p) { return p.kf; }
+};
+
+template <typename R> __device__ __forceinline__ R rsqrt_(R x);
+template <> __device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
+template <> __device__ __forceinline__ float rsqrt_(float x) { return sqrtf(x); }
+
+// ---- indexing (gpu/MOSE_Field_m.f90:78-109) ----
+__device__ __forceinline__ long long lin(const DBlk& b, int i, int j, int k) {
+  return (long long)(i + GC - 1) + (long long)(j + GC - 1) * b.pi + (long long)(k + GC - 1) * b.pi * b.pj;
+}
+__device__ __forceinline__ long long row(const DBlk& b, int i, int j, int k) { return b.boff + lin(b, i, j, k); }
+__device__ __forceinline__ const double* fm1p(const DBlk& b, int i, int j, int k) {
+  return b.fm1 + 4 * ((long long)i + (long long)(b.n1 + 1) * ((j - 1) + (long long)b.n2 * (k - 1)));
+}
+__device__ __forceinline__ const double* fm2p(const DBlk& b, int i, int j, int k) {
+  return b.fm2 + 4 * ((long long)(i - 1) + (long long)b.n1 * (j + (long long)(b.n2 + 1) * (k - 1)));
+}
+__device__ __forceinline__ const double* fm3p(const DBlk& b, int i, int j, int k) {
+  return b.fm3 + 4 * ((long long)(i - 1) + (long long)b.n1 * ((j - 1) + (long long)b.n2 * k));
+}
+__device__ __forceinline__ const double* fmp(const DBlk& b, int d, int i, int j, int k) {
+  return d == 0 ? fm1p(b, i, j, k) : (d == 1 ? fm2p(b, i, j, k) : fm3p(b, i, j, k));
+}
+__device__ __forceinline__ double ld(const double* p) { return __ldg(p); }
+
+// min / max with the semantics of std::min / std::max of the CPU restatement ((b < a) ? b : a and
+// (a < b) ? b : a): the same operand is returned for equal values, so signed zeros match as well
+template <typename R> __device__ __forceinline__ R mn(R a, R b) { return (b < a) ? b : a; }
+template <typename R> __device__ __forceinline__ R mx(R a, R b) { return (a < b) ? b : a; }
+
+// ---- table lookups ----
+// The table row of a temperature, kept inside [tmin, tmax-1] (NaN -> tmin): on the table this is
+// int(T) as in the reference; off it the reference would index outside the table, which must never
+// happen on the GPU (the thermo guard / state check report such a state).
+template <typename R>
+__device__ __forceinline__ int tidx(const Params& p, R T) {
+  if (!(T >= (R)p.tmin)) return p.tmin;
+  if (T >= (R)(p.tmax - 1)) return p.tmax - 1;
+  return (int)T;
+}
+template <typename R>
+__device__ __forceinline__ R tabT(const R* t, int ti, R td) {
+  R a = t[ti];
+  R b = t[ti + 1];
+  return a + (b - a) * td;
+}
+
+// ---- FLINT leaves (Lib_ThermoTransport_dev.f90) ----
+template <typename R>
+__device__ __forceinline__ void rotot_rtot(const Params& p, R rhoi, R& rho, R& Rg) {
+  rho = (R)0 + rhoi;
+  Rg = (R)0 + (R)p.ri * rhoi / rho;
+}
+template <typename R>
+__device__ __forceinline__ R f_cp(const Params& p, R rhoi, int ti, R td, R rho) {
+  R cpi = tabT(Tab<R>::cp(p), ti, td);
+  return (R)0 + rhoi / rho * cpi;
+}
+template <typename R>
+__device__ __forceinline__ R f_ss(const Params& p, R rhoi, R pr, R rho, R Rtot) {
+  R T = pr / (Rtot * rho);
+  int ti = tidx(p, T);
+  R td = T - (R)ti;
+  R cp = f_cp(p, rhoi, ti, td, rho);
+  R gam = cp / (cp - Rtot);
+  return rsqrt_(gam * Rtot * T);
+}
+template <typename R>
+__device__ __forceinline__ R H0(const Params& p, R pr, R rhoi, R u) {
+  R rho = (R)0 + rhoi;
+  R Rg = (R)0 + (R)p.ri * rhoi / rho;
+  R T = pr / (Rg * rho);
+  int ti = tidx(p, T);
+  R td = T - (R)ti;
+  R e = (R)0 + tabT(Tab<R>::h(p), ti, td) * rhoi / rho;
+  return e + (R)0.5 * u * u;
+}
+// f_molecularWeight + co_fiij_dev + co_k_mi_lam_Wilke_dev, one species
+template <typename R>
+__device__ __forceinline__ void wilke(const Params& p, R rhoi, R rho, int ti, R td, R& mil, R& kl) {
+  const R wm = (R)p.wm;
+  R rho_ = (R)0 + rhoi;
+  R wmt = (R)0 + (rhoi / rho_ / wm);
+  wmt = (R)1 / wmt;
+  R xi = rhoi * wmt / (rho * wm);
+  R mi = tabT(Tab<R>::mu(p), ti, td);
+  R ki = tabT(Tab<R>::k(p), ti, td);
+  R sq_num = rsqrt_(mi);
+  R inv_den = (R)1 / rsqrt_(mi + (R)1e-20);
+  const R pw = (R)1;     // Mi_Mj_pow_m025(1,1) = (wm/wm)**(-0.25) = 1
+  const R is8 = (R)0.25; // inv_sqrt8_1p(1,1) = 1/sqrt(8 (1 + 1))
+  R ratio = sq_num * inv_den * pw;
+  R one_plus = (R)1 + ratio;
+  R fi = one_plus * one_plus * is8;
+  R lam_den = (R)0 + xi * fi;
+  R inv_ld = (R)1 / lam_den;
+  mil = (R)0 + xi * mi * inv_ld;
+  kl = (R)0 + xi * ki * inv_ld;
+}
+
+// ---- limiter (Lib_Limiters.f90:65-97) ----
+template <typename R>
+__device__ __forceinline__ R rlimiter(int lim, R x, R y) {
+  R ru, phi;
+  switch (lim) {
+    case 1: {
+      if (x * y < (R)0) return (R)0;
+      R r = x;
+      if (fabs(x) > fabs(y)) r = y;
+      return r;
+    }
+    case 2:
+      ru = y / (x + (R)1e-30);
+      phi = (ru + fabs(ru)) / ((R)1 + fabs(ru));
+      return phi * x;
+    case 3:
+      ru = y / (x + (R)1e-30);
+      phi = (ru * ru + ru) / ((R)1 + ru * ru);
+      return phi * x;
+    case 4:
+      ru = y / (x + (R)1e-30);
+      phi = mx((R)0, mn(mn((R)2 * ru, (R)0.5 * ((R)1 + ru)), (R)2));
+      return phi * x;
+    case 5:
+      ru = y / (x + (R)1e-30);
+      phi = mx(mx((R)0, mn((R)2 * ru, (R)1)), mn(ru, (R)2));
+      return phi * x;
+    default:
+      return (R)0;
+  }
+}
+
+// ---- MOSE_open solvers of riemann_open_body.inc: AUSM+ (4), LMRoe (12) ----
+template <typename R>
+__device__ __forceinline__ R h_static(const Params& p, R rhoi, R pr) {
+  R rho_ = (R)0 + rhoi;
+  R rg = (R)0 + (R)p.ri * rhoi / rho_;
+  R T = pr / (rg * rho_);
+  R Tc = mx((R)p.tmin, mn(T, (R)(p.tmax - 1)));
+  if (Tc != Tc) Tc = (R)p.tmin;
+  int ti = (int)Tc;
+  R td = Tc - (R)ti;
+  int t1 = max(p.tmin, min(ti, p.tmax));
+  int t2 = max(p.tmin, min(ti + 1, p.tmax));
+  const R* h = Tab<R>::h(p);
+  R hs = h[t1] + (h[t2] - h[t1]) * td;
+  return (R)0 + hs * rhoi / rho_;
+}
+
+template <typename R>
+__device__ __forceinline__ void riemann_open(const Params& p, int rs, R dl, R ul, R vl, R wl, R pl, R al, R dltot,
+                                             R dr, R ur, R vr, R wr, R pr, R ar, R drtot, R nx, R ny, R nz,
+                                             R& F_r, R& F_u, R& F_v, R& F_w, R& F_E) {
+  R unl = ul * nx + vl * ny + wl * nz;
+  R unr = ur * nx + vr * ny + wr * nz;
+  if (rs == 4) {
+    const R ab = (R)0.125, aa = (R)0.1875;
+    R vel = rsqrt_(ul * ul + vl * vl + wl * wl);
+    R H_L = h_static(p, dl, pl) + (R)0.5 * vel * vel;
+    vel = rsqrt_(ur * ur + vr * vr + wr * wr);
+    R H_R = h_static(p, dr, pr) + (R)0.5 * vel * vel;
+    R a_half = rsqrt_(al * ar);
+    R ML = unl / a_half, MR = unr / a_half;
+    R MplusL, pplusL, MminusR, pminusR;
+    if (fabs(ML) < (R)1) {
+      MplusL = (R)0.25 * ((ML + (R)1) * (ML + (R)1)) + ab * ((ML * ML - (R)1) * (ML * ML - (R)1));
+      pplusL = (R)0.25 * ((ML + (R)1) * (ML + (R)1)) * ((R)2 - ML) + aa * ML * ((ML * ML - (R)1) * (ML * ML - (R)1));
+    } else {
+      MplusL = (R)0.5 * (ML + fabs(ML));
+      pplusL = (R)0.5 * ((R)1 + copysign((R)1, ML));
+    }
+    if (fabs(MR) < (R)1) {
+      MminusR = (R)(-0.25) * ((MR - (R)1) * (MR - (R)1)) - ab * ((MR * MR - (R)1) * (MR * MR - (R)1));
+      pminusR = (R)0.25 * ((MR - (R)1) * (MR - (R)1)) * ((R)2 + MR) - aa * MR * ((MR * MR - (R)1) * (MR * MR - (R)1));
+    } else {
+      MminusR = (R)0.5 * (MR - fabs(MR));
+      pminusR = (R)0.5 * ((R)1 - copysign((R)1, MR));
+    }
+    R Mhalf = MplusL + MminusR;
+    R phalf = pplusL * pl + pminusR * pr;
+    R mdotp = dltot * a_half * (R)0.5 * (Mhalf + fabs(Mhalf));
+    R mdotm = drtot * a_half * (R)0.5 * (Mhalf - fabs(Mhalf));
+    F_r = mdotp + mdotm;
+    F_u = mdotp * ul + mdotm * ur + nx * phalf;
+    F_v = mdotp * vl + mdotm * vr + ny * phalf;
+    F_w = mdotp * wl + mdotm * wr + nz * phalf;
+    F_E = mdotp * H_L + mdotm * H_R;
+    return;
+  }
+  const R* H = Tab<R>::h(p);
+  const R* CP = Tab<R>::cp(p);
+  R rho_ = (R)0 + dl;
+  R Rl = (R)0 + (R)p.ri * dl / rho_;
+  rho_ = (R)0 + dr;
+  R Rr = (R)0 + (R)p.ri * dr / rho_;
+  R inv_dltot = (R)1 / dltot, inv_drtot = (R)1 / drtot;
+  R Tl = pl * inv_dltot / Rl, Tr = pr * inv_drtot / Rr;
+  int Til = tidx(p, Tl);
+  int Tir = tidx(p, Tr);
+  R dTl = Tl - (R)Til, dTr = Tr - (R)Tir;
+  R srL = rsqrt_(dltot), srR = rsqrt_(drtot);
+  R inv_sr = (R)1 / (srL + srR);
+  R rho_roe = srL * srR;
+  R u_roe = (srR * ur + srL * ul) * inv_sr;
+  R v_roe = (srR * vr + srL * vl) * inv_sr;
+  R w_roe = (srR * wr + srL * wl) * inv_sr;
+  R R_roe = (srR * Rr + srL * Rl) * inv_sr;
+  R T_roe = (srR * Tr + srL * Tl) * inv_sr;
+  R h0l = (R)0, h0r = (R)0, cv_roe = (R)0, sum_ei = (R)0;
+  {
+    R invW = (R)(RUNIV / p.wm);
+    R hl = H[Til] + (H[Til + 1] - H[Til]) * dTl;
+    R hr = H[Tir] + (H[Tir + 1] - H[Tir]) * dTr;
+    R el = hl - invW * Tl, er = hr - invW * Tr;
+    h0l = h0l + hl * dl * inv_dltot;
+    h0r = h0r + hr * dr * inv_drtot;
+    R d_roe = (srR * dr * inv_drtot + srL * dl * inv_dltot) * inv_sr;
+    cv_roe = cv_roe + d_roe * ((R)0.5 * (CP[Til] + (CP[Til + 1] - CP[Til]) * dTl + CP[Tir] +
+                                         (CP[Tir + 1] - CP[Tir]) * dTr) - invW);
+    sum_ei = sum_ei + d_roe * (srR * er + srL * el) * inv_sr;
+  }
+  h0l = h0l + (R)0.5 * (ul * ul + vl * vl + wl * wl);
+  h0r = h0r + (R)0.5 * (ur * ur + vr * vr + wr * wr);
+  R h0_roe = (srR * h0r + srL * h0l) * inv_sr;
+  R gam_roe = (R)1 + R_roe / cv_roe;
+  R vel2 = u_roe * u_roe + v_roe * v_roe + w_roe * w_roe;
+  R a_roe = rsqrt_((gam_roe - (R)1) * (h0_roe - (R)0.5 * vel2 + cv_roe * T_roe - sum_ei));
+  R nmag = rsqrt_(nx * nx + ny * ny + nz * nz);
+  if (!(nmag > (R)0)) { F_r = F_u = F_v = F_w = F_E = (R)0; return; }
+  R n1 = nx / nmag, n2 = ny / nmag, n3 = nz / nmag;
+  R tx, ty, tz;
+  if (fabs(n1) < (R)0.9) { tx = (R)1; ty = (R)0; tz = (R)0; } else { tx = (R)0; ty = (R)1; tz = (R)0; }
+  R t1x = tx - (tx * n1 + ty * n2 + tz * n3) * n1;
+  R t1y = ty - (tx * n1 + ty * n2 + tz * n3) * n2;
+  R t1z = tz - (tx * n1 + ty * n2 + tz * n3) * n3;
+  R tmag = rsqrt_(t1x * t1x + t1y * t1y + t1z * t1z);
+  if (tmag <= (R)0) { t1x = -n2; t1y = n1; t1z = (R)0; tmag = rsqrt_(t1x * t1x + t1y * t1y + t1z * t1z); }
+  t1x = t1x / tmag; t1y = t1y / tmag; t1z = t1z / tmag;
+  R t2x = n2 * t1z - n3 * t1y;
+  R t2y = n3 * t1x - n1 * t1z;
+  R t2z = n1 * t1y - n2 * t1x;
+  R unL = ul * n1 + vl * n2 + wl * n3, unR = ur * n1 + vr * n2 + wr * n3;
+  R ut1L = ul * t1x + vl * t1y + wl * t1z, ut1R = ur * t1x + vr * t1y + wr * t1z;
+  R ut2L = ul * t2x + vl * t2y + wl * t2z, ut2R = ur * t2x + vr * t2y + wr * t2z;
+  R hL = h_static(p, dl, pl), hR = h_static(p, dr, pr);
+  R H0L = hL + (R)0.5 * (ul * ul + vl * vl + wl * wl);
+  R H0R = hR + (R)0.5 * (ur * ur + vr * vr + wr * wr);
+  R FL1 = dltot * unL, FL2 = dltot * unL * ul + pl * n1, FL3 = dltot * unL * vl + pl * n2;
+  R FL4 = dltot * unL * wl + pl * n3, FL5 = dltot * unL * H0L;
+  R FR1 = drtot * unR, FR2 = drtot * unR * ur + pr * n1, FR3 = drtot * unR * vr + pr * n2;
+  R FR4 = drtot * unR * wr + pr * n3, FR5 = drtot * unR * H0R;
+  R unRoe = u_roe * n1 + v_roe * n2 + w_roe * n3;
+  R u2 = u_roe * u_roe + v_roe * v_roe + w_roe * w_roe;
+  R utmag = rsqrt_(mx((R)0, u2 - unRoe * unRoe));
+  R Ma = (a_roe > (R)0) ? (fabs(unRoe) + utmag) / a_roe : (R)1;
+  R phi = mx((R)p.mco, mn((R)1, Ma));
+  R drho = drtot - dltot, dp = pr - pl, dun = unR - unL;
+  R dut1 = ut1R - ut1L, dut2 = ut2R - ut2L;
+  R dunmod = phi * dun;
+  R abs1 = fabs(unRoe - a_roe), abs2 = fabs(unRoe), abs5 = fabs(unRoe + a_roe);
+  R a2 = a_roe * a_roe, inva = (R)1 / a_roe, inva2 = (R)1 / a2;
+  R al4 = drho - dp * inva2;
+  R al2 = rho_roe * dut1, al3 = rho_roe * dut2;
+  R al1 = (R)0.5 * (dp * inva2 - rho_roe * dunmod * inva);
+  R al5 = (R)0.5 * (dp * inva2 + rho_roe * dunmod * inva);
+  R d1 = abs1 * al1 * (R)1 + abs2 * al2 * (R)0 + abs2 * al3 * (R)0 + abs2 * al4 * (R)1 + abs5 * al5 * (R)1;
+  R d2 = abs1 * al1 * (u_roe - a_roe * n1) + abs2 * al2 * t1x + abs2 * al3 * t2x + abs2 * al4 * u_roe +
+         abs5 * al5 * (u_roe + a_roe * n1);
+  R d3 = abs1 * al1 * (v_roe - a_roe * n2) + abs2 * al2 * t1y + abs2 * al3 * t2y + abs2 * al4 * v_roe +
+         abs5 * al5 * (v_roe + a_roe * n2);
+  R d4 = abs1 * al1 * (w_roe - a_roe * n3) + abs2 * al2 * t1z + abs2 * al3 * t2z + abs2 * al4 * w_roe +
+         abs5 * al5 * (w_roe + a_roe * n3);
+  R d5 = abs1 * al1 * (h0_roe - a_roe * unRoe) + abs2 * al2 * (u_roe * t1x + v_roe * t1y + w_roe * t1z) +
+         abs2 * al3 * (u_roe * t2x + v_roe * t2y + w_roe * t2z) + abs2 * al4 * ((R)0.5 * u2) +
+         abs5 * al5 * (h0_roe + a_roe * unRoe);
+  F_r = (R)0.5 * (FL1 + FR1) - (R)0.5 * d1;
+  F_u = (R)0.5 * (FL2 + FR2) - (R)0.5 * d2;
+  F_v = (R)0.5 * (FL3 + FR3) - (R)0.5 * d3;
+  F_w = (R)0.5 * (FL4 + FR4) - (R)0.5 * d4;
+  F_E = (R)0.5 * (FL5 + FR5) - (R)0.5 * d5;
+}
+
+// Roe averages shared by the two HLLC forms: the inline one of conv_physics.inc (clamped T row, Rl/Rr
+// taken from the caller) and riemann_HLLC / roe_averages of Lib_Riemann_HLL.f90 (boundary records).
+template <typename R>
+__device__ __forceinline__ void hllc(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R Rl, R dr, R ur,
+                                     R vr, R wr, R pr, R ar, R drtot, R Rr, R nx, R ny, R nz, R& F_r, R& F_u,
+                                     R& F_v, R& F_w, R& F_E) {
+  const R* H = Tab<R>::h(p);
+  const R* CP = Tab<R>::cp(p);
+  R unl = ul * nx + vl * ny + wl * nz;
+  R unr = ur * nx + vr * ny + wr * nz;
+  R inv_dltot = (R)1 / dltot, inv_drtot = (R)1 / drtot;
+  R Tl = pl * inv_dltot / Rl, Tr = pr * inv_drtot / Rr;
+  int Til = tidx(p, Tl);
+  int Tir = tidx(p, Tr);
+  R dTl = Tl - (R)Til, dTr = Tr - (R)Tir;
+  R srL = rsqrt_(dltot), srR = rsqrt_(drtot), inv_sr = (R)1 / (srL + srR);
+  R u_roe = (srR * ur + srL * ul) * inv_sr, v_roe = (srR * vr + srL * vl) * inv_sr,
+    w_roe = (srR * wr + srL * wl) * inv_sr;
+  R R_roe = (srR * Rr + srL * Rl) * inv_sr, T_roe = (srR * Tr + srL * Tl) * inv_sr;
+  R h0l = (R)0, h0r = (R)0, cv_roe = (R)0, sum_ei = (R)0;
+  {
+    R invW = (R)(RUNIV / p.wm);
+    R hl = H[Til] + (H[Til + 1] - H[Til]) * dTl;
+    R hr = H[Tir] + (H[Tir + 1] - H[Tir]) * dTr;
+    R el = hl - invW * Tl, er = hr - invW * Tr;
+    h0l = h0l + hl * dl * inv_dltot;
+    h0r = h0r + hr * dr * inv_drtot;
+    R d_roe = (srR * dr * inv_drtot + srL * dl * inv_dltot) * inv_sr;
+    cv_roe = cv_roe + d_roe * ((R)0.5 * (CP[Til] + (CP[Til + 1] - CP[Til]) * dTl + CP[Tir] +
+                                         (CP[Tir + 1] - CP[Tir]) * dTr) - invW);
+    sum_ei = sum_ei + d_roe * (srR * er + srL * el) * inv_sr;
+  }
+  h0l = h0l + (R)0.5 * (ul * ul + vl * vl + wl * wl);
+  h0r = h0r + (R)0.5 * (ur * ur + vr * vr + wr * wr);
+  R h0_roe = (srR * h0r + srL * h0l) * inv_sr;
+  R gam_roe = (R)1 + R_roe / cv_roe;
+  R vel2 = u_roe * u_roe + v_roe * v_roe + w_roe * w_roe;
+  R a_roe = rsqrt_((gam_roe - (R)1) * (h0_roe - (R)0.5 * vel2 + cv_roe * T_roe - sum_ei));
+  R un_roe = u_roe * nx + v_roe * ny + w_roe * nz;
+  R e0l = h0l - pl / dltot, e0r = h0r - pr / drtot;
+  R S1 = mn(mn((R)0, unl - al), un_roe - a_roe);
+  R S4 = mx(mx((R)0, unr + ar), un_roe + a_roe);
+  R inv_denom = (R)1 / (dltot * (S1 - unl) - drtot * (S4 - unr));
+  R Sstar = (pr - pl + dltot * unl * (S1 - unl) - drtot * unr * (S4 - unr)) * inv_denom;
+  R pstar = dltot * (unl - S1) * (unl - Sstar) + pl;
+  if (S1 >= (R)0) {
+    F_r = dltot * unl; F_u = F_r * ul + pl * nx; F_v = F_r * vl + pl * ny; F_w = F_r * wl + pl * nz; F_E = F_r * h0l;
+  } else if (Sstar >= (R)0) {
+    F_r = dltot * unl; F_u = F_r * ul + pl * nx; F_v = F_r * vl + pl * ny; F_w = F_r * wl + pl * nz; F_E = F_r * h0l;
+    inv_denom = (R)1 / (S1 - Sstar);
+    R U1S = dltot * (S1 - unl) * inv_denom;
+    R U2S = ((S1 - unl) * dltot * ul + (pstar - pl) * nx) * inv_denom;
+    R U3S = ((S1 - unl) * dltot * vl + (pstar - pl) * ny) * inv_denom;
+    R U4S = ((S1 - unl) * dltot * wl + (pstar - pl) * nz) * inv_denom;
+    R U5S = ((S1 - unl) * dltot * e0l - pl * unl + pstar * Sstar) * inv_denom;
+    F_r = F_r + S1 * (U1S - dltot); F_u = F_u + S1 * (U2S - dltot * ul); F_v = F_v + S1 * (U3S - dltot * vl);
+    F_w = F_w + S1 * (U4S - dltot * wl); F_E = F_E + S1 * (U5S - dltot * e0l);
+  } else if (S4 > (R)0) {
+    F_r = drtot * unr; F_u = F_r * ur + pr * nx; F_v = F_r * vr + pr * ny; F_w = F_r * wr + pr * nz; F_E = F_r * h0r;
+    inv_denom = (R)1 / (S4 - Sstar);
+    R U1S = drtot * (S4 - unr) * inv_denom;
+    R U2S = ((S4 - unr) * drtot * ur + (pstar - pr) * nx) * inv_denom;
+    R U3S = ((S4 - unr) * drtot * vr + (pstar - pr) * ny) * inv_denom;
+    R U4S = ((S4 - unr) * drtot * wr + (pstar - pr) * nz) * inv_denom;
+    R U5S = ((S4 - unr) * drtot * e0r - pr * unr + pstar * Sstar) * inv_denom;
+    F_r = F_r + S4 * (U1S - drtot); F_u = F_u + S4 * (U2S - drtot * ur); F_v = F_v + S4 * (U3S - drtot * vr);
+    F_w = F_w + S4 * (U4S - drtot * wr); F_E = F_E + S4 * (U5S - drtot * e0r);
+  } else {
+    F_r = drtot * unr; F_u = F_r * ur + pr * nx; F_v = F_r * vr + pr * ny; F_w = F_r * wr + pr * nz; F_E = F_r * h0r;
+  }
+}
+
+// ---- interior convective face from the 4-cell stencil (conv_physics.inc) ----
+template <typename R>
+__device__ __forceinline__ void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, const R* pp2,
+                                          const R* dlc, R nx, R ny, R nz, R area, R* res0) {
+  R l0 = (R)0.5 * (dlc[0] + dlc[1]), l1 = (R)0.5 * (dlc[1] + dlc[2]), l2 = (R)0.5 * (dlc[2] + dlc[3]);
+  R lm = (R)0.5 * dlc[1], lp = (R)0.5 * dlc[2];
+  const R beta_order = (R)1;
+  R idl0 = (R)1 / l0, idl1 = (R)1 / l1, idl2 = (R)1 / l2;
+  R P1[MB_NP], P4[MB_NP];
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) {
+    R slope0 = (p0[s] - pm1[s]) * idl0;
+    R slope1 = (pp1[s] - p0[s]) * idl1;
+    R slope2 = (pp2[s] - pp1[s]) * idl2;
+    R slopel = rlimiter(p.lim, slope1, slope0);
+    R sloper = rlimiter(p.lim, slope2, slope1);
+    P1[s] = p0[s] + beta_order * slopel * lm;
+    P4[s] = pp1[s] - beta_order * sloper * lp;
+  }
+  P1[0] = mx(P1[0], (R)1e-20);
+  P4[0] = mx(P4[0], (R)1e-20);
+  R rotot1 = (R)0 + P1[0];
+  R Rtot1 = (R)0 + (R)p.ri * P1[0] / rotot1;
+  R rotot4 = (R)0 + P4[0];
+  R Rtot4 = (R)0 + (R)p.ri * P4[0] / rotot4;
+  const R* CP = Tab<R>::cp(p);
+  R T1d = P1[MB_IPR] / (Rtot1 * rotot1);
+  int Ti1 = tidx(p, T1d);
+  R Tdiffd = T1d - (R)Ti1;
+  R cpd = (R)0 + P1[0] / rotot1 * (CP[Ti1] + (CP[Ti1 + 1] - CP[Ti1]) * Tdiffd);
+  R gamd = cpd / (cpd - Rtot1);
+  R a1 = rsqrt_(gamd * Rtot1 * T1d);
+  R T4d = P4[MB_IPR] / (Rtot4 * rotot4);
+  int Ti4 = tidx(p, T4d);
+  Tdiffd = T4d - (R)Ti4;
+  cpd = (R)0 + P4[0] / rotot4 * (CP[Ti4] + (CP[Ti4 + 1] - CP[Ti4]) * Tdiffd);
+  gamd = cpd / (cpd - Rtot4);
+  R a4 = rsqrt_(gamd * Rtot4 * T4d);
+  R F_r, F_u, F_v, F_w, F_E;
+  if (p.rs == 1)
+    hllc(p, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], a1, rotot1, Rtot1, P4[0], P4[MB_IU], P4[MB_IV],
+         P4[MB_IW], P4[MB_IPR], a4, rotot4, Rtot4, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
+  else
+    riemann_open(p, p.rs, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], a1, rotot1, P4[0], P4[MB_IU],
+                 P4[MB_IV], P4[MB_IW], P4[MB_IPR], a4, rotot4, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
+  R su = copysign((R)0.5, F_r), sp = (R)0.5 + su, sm = su - (R)0.5;
+  R irotot1 = (R)1 / rotot1, irotot4 = (R)1 / rotot4;
+  res0[0] = F_r * area * (sp * (P1[0] * irotot1) - sm * (P4[0] * irotot4));
+  res0[MB_IU] = F_u * area; res0[MB_IV] = F_v * area; res0[MB_IW] = F_w * area; res0[MB_IPR] = F_E * area;
+}
+
+// face thermo (Diffusive_Face_Thermo_Fill, Mod_Diffusive.f90:311-325 = Diffusive_Face_State :748-776)
+template <typename R>
+__device__ __forceinline__ void face_thermo(const Params& p, R rhoi, R pr, R& rho, R& T, int& ti, R& td, R& cp,
+                                            R& mil, R& kl) {
+  R Rgas;
+  rotot_rtot(p, rhoi, rho, Rgas);
+  T = pr / (rho * Rgas);
+  ti = tidx(p, T);
+  td = T - (R)ti;
+  cp = f_cp(p, rhoi, ti, td, rho);
+  wilke(p, rhoi, rho, ti, td, mil, kl);
+  if (p.prandtl > 0.0) kl = mil * cp / (R)p.prandtl;
+}
+
+// the laminar viscous flux of a face from its gradients (diff_physics.inc:88-161 with mie = 0);
+// Stress_Vector_Std (physics/turbulence/Mod_Fluid.f90:20-44) is the same arithmetic
+template <typename R>
+__device__ __forceinline__ void visc_flux(const Params& p, const R G[MB_NP][3], const R* Pf, R nx, R ny, R nz,
+                                          R area, R drho, R dT, R dcp, R dmil, R dkl, R* F) {
+  int Ti = tidx(p, dT);
+  R Tdf = dT - (R)Ti;
+  const R mie = (R)0, sct = (R)0.9, prt = (R)0.85;
+  R Dm = (dmil / (R)p.schmidt + mie / sct) / drho;
+  R kappaf = dkl + mie * dcp / prt;
+  R dmi = dmil + mie;
+  const R ntt = (R)(-2.0 / 3.0);
+  R dlam = ntt * dmi;
+  R Diver = G[MB_IU][0] + G[MB_IV][1] + G[MB_IW][2];
+  R lamDiv = dlam * Diver;
+  const R rhokd = (R)0;
+  R Txx = lamDiv + (R)2 * dmi * G[MB_IU][0] + rhokd;
+  R Tyy = lamDiv + (R)2 * dmi * G[MB_IV][1] + rhokd;
+  R Tzz = lamDiv + (R)2 * dmi * G[MB_IW][2] + rhokd;
+  R Txy = dmi * (G[MB_IU][1] + G[MB_IV][0]), Txz = dmi * (G[MB_IU][2] + G[MB_IW][0]),
+    Tyz = dmi * (G[MB_IV][2] + G[MB_IW][1]);
+  R S1 = Txx * nx + Txy * ny + Txz * nz;
+  R S2 = Txy * nx + Tyy * ny + Tyz * nz;
+  R S3 = Txz * nx + Tyz * ny + Tzz * nz;
+  R DiffH = (R)0;
+  R DmGY = Dm * (G[0][0] * nx + G[0][1] * ny + G[0][2] * nz);
+  R F0 = drho * area * DmGY;
+  const R* H = Tab<R>::h(p);
+  R hh1 = H[Ti], hh2 = H[Ti + 1];
+  R hh = hh1 + Tdf * (hh2 - hh1);
+  DiffH = DiffH + DmGY * hh;
+  R sflx = (R)0 + F0;
+  F[0] = F0 - sflx * Pf[0] / drho;
+  F[MB_IU] = area * S1; F[MB_IV] = area * S2; F[MB_IW] = area * S3;
+  F[MB_IPR] = area * ((S1 * Pf[MB_IU] + S2 * Pf[MB_IV] + S3 * Pf[MB_IW]) +
+                      kappaf * (G[MB_IPR][0] * nx + G[MB_IPR][1] * ny + G[MB_IPR][2] * nz) + DiffH * drho);
+}
+
+// the cell density / temperature of the thermo cache (Mod_Thermo_Cache.f90:327-330,378-380)
+template <typename R>
+__device__ __forceinline__ void cell_rho_T(const Params& p, R rhoi, R pr, R& rho, R& T) {
+  R Rg;
+  rotot_rtot(p, rhoi, rho, Rg);
+  T = pr / (rho * Rg);
+}
+
+__device__ __forceinline__ int face_sign(int F) { return 1 - 2 * (F % 2); }  // modfm2 / FluxSign
+
+}  // namespace mb

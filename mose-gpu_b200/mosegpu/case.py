@@ -239,15 +239,13 @@ def layout_case(name, cuts, node_fn, periodic, bc_faces, thermo, scheme, prim_fn
     # boundary records, grouped per block, face-ordered within a block; cells i fastest
     recs = []
     conns = []
+    nrec = 0
     for bi, b in enumerate(blocks):
         n = b["n"]
         pos = b["pos"]
         for face in range(1, 7):
             ax = (face - 1) // 2
             low = face % 2 == 1
-            t = [0, 1, 2]
-            t.remove(ax)
-            # neighbour block across this face
             npos = list(pos)
             npos[ax] += -1 if low else 1
             neighbour = None
@@ -256,31 +254,30 @@ def layout_case(name, cuts, node_fn, periodic, bc_faces, thermo, scheme, prim_fn
             elif periodic[ax]:
                 npos[ax] %= nb[ax]
                 neighbour = bid[tuple(npos)]
-            rng = [range(1, n[0] + 1), range(1, n[1] + 1), range(1, n[2] + 1)]
-            rng[ax] = [1] if low else [n[ax]]
-            for k in rng[2]:
-                for j in rng[1]:
-                    for i in rng[0]:
-                        r = np.zeros(1, dtype=abi.BC_DTYPE)[0]
-                        r["blk"] = bi; r["i"] = i; r["j"] = j; r["k"] = k; r["face"] = face
-                        r["conn"] = -1
-                        if neighbour is not None:
-                            r["type"] = abi.BC_CONNECTION
-                            nd = blocks[neighbour]["n"]
-                            src = [i, j, k]
-                            src[ax] = nd[ax] if low else 1
-                            cn = np.zeros(1, dtype=abi.CONN_DTYPE)[0]
-                            cn["rec"] = len(recs); cn["bs"] = neighbour
-                            cn["is"], cn["js"], cn["ks"] = src
-                            cn["fs"] = face + 1 if low else face - 1
-                            cn["d11"], cn["d12"], cn["d21"], cn["d22"] = 1, 0, 0, 1
-                            r["conn"] = len(conns)
-                            conns.append(cn)
-                        else:
-                            r["type"] = bc_faces[face]
-                        recs.append(r)
-    case.rec = np.array(recs, dtype=abi.BC_DTYPE) if recs else np.zeros(0, dtype=abi.BC_DTYPE)
-    case.conn = np.array(conns, dtype=abi.CONN_DTYPE) if conns else np.zeros(0, dtype=abi.CONN_DTYPE)
+            rng = [np.arange(1, n[0] + 1), np.arange(1, n[1] + 1), np.arange(1, n[2] + 1)]
+            rng[ax] = np.array([1 if low else n[ax]])
+            I, J, K = [a.ravel(order="F") for a in np.meshgrid(*rng, indexing="ij")]
+            m = I.size
+            r = np.zeros(m, dtype=abi.BC_DTYPE)
+            r["blk"] = bi; r["i"] = I; r["j"] = J; r["k"] = K; r["face"] = face; r["conn"] = -1
+            if neighbour is not None:
+                r["type"] = abi.BC_CONNECTION
+                nd = blocks[neighbour]["n"]
+                cn = np.zeros(m, dtype=abi.CONN_DTYPE)
+                cn["rec"] = nrec + np.arange(m); cn["bs"] = neighbour
+                src = [I.copy(), J.copy(), K.copy()]
+                src[ax][:] = nd[ax] if low else 1
+                cn["is"], cn["js"], cn["ks"] = src
+                cn["fs"] = face + 1 if low else face - 1
+                cn["d11"], cn["d12"], cn["d21"], cn["d22"] = 1, 0, 0, 1
+                r["conn"] = sum(len(x) for x in conns) + np.arange(m)
+                conns.append(cn)
+            else:
+                r["type"] = bc_faces[face]
+            recs.append(r)
+            nrec += m
+    case.rec = np.concatenate(recs) if recs else np.zeros(0, dtype=abi.BC_DTYPE)
+    case.conn = np.concatenate(conns) if conns else np.zeros(0, dtype=abi.CONN_DTYPE)
     # initial state (interior cells; ghosts are filled by the ghost fill)
     P = np.zeros((NPRIM, case.ncell), dtype=np.float64)
     for bi, b in enumerate(blocks):

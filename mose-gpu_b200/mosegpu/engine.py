@@ -1,0 +1,188 @@
+"""Host binding of the B200 engine through its C ABI (include/mose_b200.h).
+
+torch provides device memory and streams only; every computation runs in the CUDA kernels of
+libmose_b200.so. There is no CPU fallback: without the built library or a CUDA device the
+constructor raises.
+
+Engine mirrors the reference's per-stage calls (Mod_Explicit.f90:52-279): fill_ghosts
+(Fill_Ghost_Cell), residual (Fluxes + BC_Fluxes), update (RK_Newstate), dt (Compute_dt), and the
+fused forms stage / step.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmose_b200.so")
+
+_lib = None
+
+
+def load_library():
+    """Loads libmose_b200.so (built by mose-gpu_b200/build.py); raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libmose_b200.so is not built (run python mose-gpu_b200/build.py): the engine has no "
+                           "CPU fallback")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.mb_init.argtypes = [C.POINTER(abi.MBMesh), C.POINTER(abi.MBScheme), C.POINTER(abi.MBThermo), C.c_int,
+                          C.POINTER(vp)]
+    L.mb_init.restype = C.c_int
+    L.mb_destroy.argtypes = [vp]
+    L.mb_destroy.restype = None
+    L.mb_fill_ghosts.argtypes = [vp, vp, vp]
+    L.mb_residual.argtypes = [vp, vp, vp, vp]
+    L.mb_update.argtypes = [vp, vp, vp, vp, C.c_int, C.c_double, vp]
+    L.mb_dt.argtypes = [vp, vp, C.POINTER(C.c_double), vp]
+    L.mb_stage.argtypes = [vp, vp, vp, C.c_int, vp]
+    L.mb_step.argtypes = [vp, vp, vp, C.c_int, C.c_int, vp]
+    L.mb_begin_step.argtypes = [vp, vp, vp]
+    L.mb_get_status.argtypes = [vp, C.POINTER(abi.MBStatus)]
+    L.mb_profile_stage.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), vp]
+    L.mb_launch_count.argtypes = [vp]
+    L.mb_launch_count.restype = C.c_int64
+    L.mb_version.restype = C.c_char_p
+    for f in ("mb_fill_ghosts", "mb_residual", "mb_update", "mb_dt", "mb_stage", "mb_step", "mb_begin_step",
+              "mb_get_status", "mb_profile_stage"):
+        getattr(L, f).restype = C.c_int
+    _lib = L
+    return L
+
+
+def _check(rc, where):
+    if rc != abi.MB_OK:
+        raise abi.MoseError(rc, where)
+
+
+class Engine:
+    """One case resident on one GPU, driven through the C ABI."""
+
+    def __init__(self, case, precision=abi.PREC_FP64, device=0, stream=None):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("no CUDA device: the engine has no CPU fallback")
+        self.torch = torch
+        self.case = case
+        self.dev = torch.device("cuda", device)
+        L = load_library()
+        self.lib = L
+        nb = len(case.blocks)
+        self._geo = []
+        self._blk = (abi.MBBlock * nb)()
+        for q, b in enumerate(case.blocks):
+            B = self._blk[q]
+            B.n[0], B.n[1], B.n[2] = b["n"]
+            B.boff = b["boff"]
+            for f in ("fm1", "fm2", "fm3", "dl", "m", "vol"):
+                t = torch.from_numpy(np.ascontiguousarray(b[f], dtype=np.float64)).to(self.dev)
+                self._geo.append(t)
+                setattr(B, f, t.data_ptr())
+        self._rec = np.ascontiguousarray(case.rec)
+        self._conn = np.ascontiguousarray(case.conn)
+        mesh = abi.MBMesh()
+        mesh.nblk = nb
+        mesh.nrec = len(self._rec)
+        mesh.nconn = len(self._conn)
+        mesh.ncell_total = case.ncell
+        mesh.blk = self._blk
+        mesh.rec = self._rec.ctypes.data if len(self._rec) else None
+        mesh.conn = self._conn.ctypes.data if len(self._conn) else None
+        th = case.thermo
+        self._tabs = [np.ascontiguousarray(th[k], dtype=np.float64) for k in ("cp", "h", "mu", "k")]
+        T = abi.MBThermo()
+        T.tmin, T.tmax, T.wm = th["tmin"], th["tmax"], th["wm"]
+        T.cp, T.h, T.mu, T.k = [a.ctypes.data for a in self._tabs]
+        sc = case.scheme_struct()
+        sc.precision = precision
+        self.precision = precision
+        self.n_rk = sc.n_rk
+        h = C.c_void_p()
+        with torch.cuda.device(self.dev):
+            _check(L.mb_init(C.byref(mesh), C.byref(sc), C.byref(T), device, C.byref(h)), "mb_init")
+        self.ctx = h
+        self.stream = stream
+        self.P = torch.from_numpy(case.P0.copy()).to(self.dev)          # (5, ncell): P_flat(ncell, 5)
+        self.PO = torch.zeros_like(self.P)
+
+    # ------------------------------------------------------------------ plumbing
+    def _s(self):
+        s = self.stream if self.stream is not None else self.torch.cuda.current_stream(self.dev)
+        return C.c_void_p(s.cuda_stream)
+
+    def close(self):
+        if getattr(self, "ctx", None) is not None and self.ctx.value:
+            self.lib.mb_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, P_host):
+        self.P.copy_(self.torch.from_numpy(np.ascontiguousarray(P_host)))
+
+    def state(self):
+        return self.P.cpu().numpy()
+
+    @property
+    def launches(self):
+        return int(self.lib.mb_launch_count(self.ctx))
+
+    # ------------------------------------------------------------------ the reference's calls
+    def fill_ghosts(self, P=None):
+        P = self.P if P is None else P
+        _check(self.lib.mb_fill_ghosts(self.ctx, P.data_ptr(), self._s()), "mb_fill_ghosts")
+
+    def residual(self, P=None, R=None):
+        P = self.P if P is None else P
+        R = self.torch.zeros_like(P) if R is None else R
+        _check(self.lib.mb_residual(self.ctx, P.data_ptr(), R.data_ptr(), self._s()), "mb_residual")
+        return R
+
+    def update(self, P, PO, R, irk, dt):
+        _check(self.lib.mb_update(self.ctx, P.data_ptr(), PO.data_ptr(), R.data_ptr(), irk, dt, self._s()),
+               "mb_update")
+
+    def dt(self, P=None):
+        P = self.P if P is None else P
+        d = C.c_double()
+        _check(self.lib.mb_dt(self.ctx, P.data_ptr(), C.byref(d), self._s()), "mb_dt")
+        return d.value
+
+    def begin_step(self):
+        _check(self.lib.mb_begin_step(self.ctx, self.P.data_ptr(), self._s()), "mb_begin_step")
+
+    def stage(self, irk):
+        _check(self.lib.mb_stage(self.ctx, self.P.data_ptr(), self.PO.data_ptr(), irk, self._s()), "mb_stage")
+
+    def step(self, nsteps=1, graph=True):
+        _check(self.lib.mb_step(self.ctx, self.P.data_ptr(), self.PO.data_ptr(), nsteps, 1 if graph else 0,
+                                self._s()), "mb_step")
+
+    def profile_stage(self, irk, nrep):
+        """(ghost-fill ms, sweep ms) averaged over nrep runs of stage irk, CUDA events on the stream."""
+        g, w = C.c_float(), C.c_float()
+        _check(self.lib.mb_profile_stage(self.ctx, self.P.data_ptr(), self.PO.data_ptr(), irk, nrep, C.byref(g),
+                                         C.byref(w), self._s()), "mb_profile_stage")
+        return g.value, w.value
+
+    def status(self):
+        st = abi.MBStatus()
+        _check(self.lib.mb_get_status(self.ctx, C.byref(st)), "mb_get_status")
+        return st
+
+    def run_to(self, t_end, max_steps=10 ** 7, chunk=1):
+        """Steps until the simulated time reaches t_end (the reference's `time >= timemax` stop)."""
+        n = 0
+        while self.status().time < t_end and n < max_steps:
+            self.step(chunk, graph=False)
+            n += chunk
+        return n

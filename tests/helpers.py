@@ -1,0 +1,60 @@
+"""Shared helpers of the tests: small cases, conserved variables, error norms."""
+import numpy as np
+
+from mosegpu import abi
+from mosegpu import case as cs
+
+
+def conserved(case, P):
+    """Interior conserved variables (rho, rho u, rho v, rho w, rho E) of every block, concatenated
+    (E = h(T) - p / rho + |u|^2 / 2 with h from the case's table, as prim2cons of the state update)."""
+    th = case.thermo
+    out = []
+    for b in range(len(case.blocks)):
+        I = case.interior(P, b).reshape(5, -1)
+        rho, u, v, w, p = I
+        T = p / (rho * th["R"])
+        ti = np.clip(np.floor(T).astype(np.int64), th["tmin"], th["tmax"] - 1)
+        h = th["h"][ti - th["tmin"]] + (T - ti) * (th["h"][ti + 1 - th["tmin"]] - th["h"][ti - th["tmin"]])
+        E = h - p / rho + 0.5 * (u * u + v * v + w * w)
+        out.append(np.stack([rho, rho * u, rho * v, rho * w, rho * E]))
+    return np.concatenate(out, axis=1)
+
+
+def rel_err(a, b, floor=1e-300):
+    """Per conserved variable: max |a - b| / max |b| (relative to the field's magnitude)."""
+    a = np.asarray(a).reshape(a.shape[0], -1)
+    b = np.asarray(b).reshape(b.shape[0], -1)
+    return np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), floor)
+
+
+def norms(a, b):
+    """L1, L2, Linf of a - b relative to the same norms of b, per variable."""
+    a = np.asarray(a).reshape(a.shape[0], -1)
+    b = np.asarray(b).reshape(b.shape[0], -1)
+    d = a - b
+    l1 = np.abs(d).sum(axis=1) / np.maximum(np.abs(b).sum(axis=1), 1e-300)
+    l2 = np.sqrt((d * d).sum(axis=1)) / np.maximum(np.sqrt((b * b).sum(axis=1)), 1e-300)
+    li = np.abs(d).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-300)
+    return l1, l2, li
+
+
+def interior_rows(case, R):
+    """R (5, ncell) restricted to the interior rows."""
+    return R[:, case.interior_mask()]
+
+
+def small_cases():
+    """(id, builder) of the parity cases: every boundary type, Riemann solver and limiter served."""
+    return [
+        ("sod_hllc_minmod", lambda: cs.riemann_1d(n=64)),
+        ("sod_ausm_vanleer", lambda: cs.riemann_1d(n=64, riemann=abi.RS_AUSMP, limiter=abi.LIM_VANLEER)),
+        ("sod_roe_vanalbada", lambda: cs.riemann_1d(n=64, riemann=abi.RS_LMROE, limiter=abi.LIM_VANALBADA)),
+        ("quad2d_hllc_minmod", lambda: cs.riemann_2d(n=20)),
+        ("quad2d_ausm_mc", lambda: cs.riemann_2d(n=20, riemann=abi.RS_AUSMP, limiter=abi.LIM_MC)),
+        ("tgv_roe_vanalbada_1blk", lambda: cs.taylor_green(n=12)),
+        ("tgv_hllc_minmod_8blk", lambda: cs.taylor_green(n=12, blocks=2, riemann=abi.RS_HLLC,
+                                                         limiter=abi.LIM_MINMOD)),
+        ("tgv_ausm_superbee_noise", lambda: cs.taylor_green(n=12, riemann=abi.RS_AUSMP, limiter=abi.LIM_SUPERBEE,
+                                                            noise=1e-3)),
+    ]

@@ -1,0 +1,166 @@
+"""Parity of the B200 engine (through its C ABI) with the CPU oracle on the same seeded inputs.
+
+Tolerances (the north-star gates, per conserved variable, max-norm relative to the field): 1e-12 after
+one step, 1e-9 after the case's step count. The FP64 form is built without FMA contraction and keeps the
+oracle's operation order, so most comparisons are expected to be exact; the tolerance is the bar.
+"""
+import numpy as np
+import pytest
+
+import helpers as H
+from mosegpu import abi
+
+pytestmark = pytest.mark.gpu
+
+TOL_ONE = 1e-12
+TOL_MANY = 1e-9
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _pair(builder):
+    import oracle
+    from mosegpu.engine import Engine
+    case = builder()
+    return case, Engine(case), oracle.Oracle(case)
+
+
+@pytest.mark.parametrize("cid,builder", H.small_cases(), ids=[c[0] for c in H.small_cases()])
+def test_ghosts_and_residual(torch_cuda, cid, builder):
+    case, eng, orc = _pair(builder)
+    P = case.P0.copy()
+    orc.fill_ghosts(P)
+    eng.fill_ghosts()
+    Pg = eng.state()
+    assert np.array_equal(Pg, P), "ghost fill differs"
+    Ro = orc.residual(P)
+    Rg = eng.residual().cpu().numpy()
+    e = H.rel_err(H.interior_rows(case, Rg), H.interior_rows(case, Ro), floor=1e-30)
+    assert np.all(e <= TOL_ONE), (cid, e)
+
+
+@pytest.mark.parametrize("cid,builder", H.small_cases(), ids=[c[0] for c in H.small_cases()])
+def test_dt(torch_cuda, cid, builder):
+    case, eng, orc = _pair(builder)
+    d_o = orc.dt(case.P0)
+    d_g = eng.dt()
+    assert abs(d_g - d_o) <= 1e-14 * d_o, (d_g, d_o)
+
+
+@pytest.mark.parametrize("cid,builder", H.small_cases(), ids=[c[0] for c in H.small_cases()])
+def test_update_hook(torch_cuda, cid, builder):
+    """mb_update alone (RK_Newstate) on the oracle's residual, every stage coefficient."""
+    torch = torch_cuda
+    case, eng, orc = _pair(builder)
+    P = case.P0.copy()
+    orc.fill_ghosts(P)
+    R = orc.residual(P)
+    dt = orc.dt(P)
+    for irk in range(1, case.scheme["n_rk"] + 1):
+        Po = P.copy()
+        orc.update(Po, P, R, irk, dt)
+        Pg = torch.from_numpy(P.copy()).cuda()
+        eng.update(Pg, torch.from_numpy(P.copy()).cuda(), torch.from_numpy(R).cuda(), irk, dt)
+        e = H.rel_err(H.conserved(case, Pg.cpu().numpy()), H.conserved(case, Po))
+        assert np.all(e <= TOL_ONE), (irk, e)
+
+
+@pytest.mark.parametrize("cid,builder", H.small_cases(), ids=[c[0] for c in H.small_cases()])
+@pytest.mark.parametrize("graph", [False, True])
+def test_one_step_and_many(torch_cuda, cid, builder, graph):
+    case, eng, orc = _pair(builder)
+    P = case.P0.copy()
+    assert orc.step(P, 1) == 0
+    eng.step(1, graph=graph)
+    e1 = H.rel_err(H.conserved(case, eng.state()), H.conserved(case, P))
+    assert np.all(e1 <= TOL_ONE), ("one step", e1)
+    nmany = 15
+    assert orc.step(P, nmany) == 0
+    eng.step(nmany, graph=graph)
+    en = H.rel_err(H.conserved(case, eng.state()), H.conserved(case, P))
+    assert np.all(en <= TOL_MANY), ("%d steps" % (nmany + 1), en)
+    so, sg = orc.status(), eng.status()
+    assert sg.code == 0 and sg.steps == so.steps
+    assert abs(sg.time - so.time) <= 1e-12 * so.time
+
+
+def test_stage_by_stage_matches_fused(torch_cuda):
+    """begin_step + stage(1..n) (the reference's call sequence) equals the fused mb_step."""
+    from mosegpu import case as cs
+    from mosegpu.engine import Engine
+    case = cs.taylor_green(n=12, blocks=2)
+    a, b = Engine(case), Engine(case)
+    for _ in range(3):
+        a.begin_step()
+        for irk in range(1, 4):
+            a.stage(irk)
+    b.step(3, graph=False)
+    assert np.array_equal(a.state()[:, case.interior_mask()], b.state()[:, case.interior_mask()])
+
+
+def test_sod_to_t_end(torch_cuda):
+    """The 1-D Sod config (1000 cells, HLLC + minmod, SSP-RK3, CFL 0.5) to t = 0.2: GPU = oracle, and
+    both close to the exact solution."""
+    import oracle
+    from mosegpu import case as cs
+    from mosegpu.engine import Engine
+    case = cs.riemann_1d(n=1000)
+    eng, orc = Engine(case), oracle.Oracle(case)
+    P = case.P0.copy()
+    no = orc.run_to(P, 0.2)
+    ng = eng.run_to(0.2)
+    assert no == ng
+    e = H.rel_err(H.conserved(case, eng.state()), H.conserved(case, P))
+    assert np.all(e <= TOL_MANY), e
+    x = case.blocks[0]["centres"][:, 0, 0, 0]
+    r, u, p = cs.exact_riemann((1.0, 0.0, 1.0), (0.125, 0.0, 0.1), x, eng.status().time)
+    rho = case.interior(eng.state(), 0)[0, :, 0, 0]
+    assert np.abs(rho - r).mean() < 2e-3
+
+
+def test_mixed_precision_error(torch_cuda):
+    """The mixed form (FP32 flux arithmetic, FP64 state) against the FP64 form on a small TGV."""
+    from mosegpu import case as cs
+    from mosegpu.engine import Engine
+    case = cs.taylor_green(n=24)
+    a = Engine(case, precision=abi.PREC_FP64)
+    b = Engine(case, precision=abi.PREC_MIXED)
+    a.step(20, graph=True)
+    b.step(20, graph=True)
+    l1, l2, li = H.norms(H.conserved(case, b.state()), H.conserved(case, a.state()))
+    assert l2[0] < 1e-5, l2
+    assert np.all(l2 < 1e-4), l2
+
+
+def test_state_check_reports_injected_nan(torch_cuda):
+    """Failure detection with a host-injected bad input: a NaN cell is reported, nothing faults."""
+    from mosegpu import case as cs
+    from mosegpu.engine import Engine
+    case = cs.riemann_1d(n=64)
+    eng = Engine(case)
+    P = case.P0.copy()
+    case.interior(P, 0)[4, 10, 0, 0] = np.nan
+    eng.set_state(P)
+    eng.step(1, graph=False)
+    st = eng.status()
+    assert st.code == abi.MB_E_STATE and st.n_bad_state > 0
+    assert st.bad_blk == 0 and st.bad_j == 1 and st.bad_k == 1
+
+
+def test_thermo_guard_reports_off_table_temperature(torch_cuda):
+    from mosegpu import case as cs
+    from mosegpu.engine import Engine
+    case = cs.taylor_green(n=12)
+    eng = Engine(case)
+    P = case.P0.copy()
+    case.interior(P, 0)[4, 3, 3, 3] *= 60.0   # T ~ 18000 K, off the 10000 K table
+    eng.set_state(P)
+    eng.step(1, graph=False)
+    st = eng.status()
+    assert st.code == abi.MB_E_THERMO and st.n_bad_thermo > 0

@@ -1,0 +1,112 @@
+"""The CPU oracle against known answers (no GPU): the exact Riemann solution (published star states of
+Toro's test 1, Sod), conservation on periodic meshes, block-decomposition independence, the dt rules,
+and the committed golden vectors of the oracle itself (tests/golden/make_golden.py)."""
+import os
+
+import numpy as np
+import pytest
+
+import helpers as H
+import oracle
+from mosegpu import abi
+from mosegpu import case as cs
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_exact_riemann_star_state():
+    # Toro, Riemann Solvers and Numerical Methods for Fluid Dynamics, Table 4.3, test 1:
+    # p* = 0.30313, u* = 0.92745, rho*L = 0.42632, rho*R = 0.26557
+    x = np.array([0.5 + 0.05, 0.85])  # t = 0.25: left of the contact (0.732), between contact and shock (0.938)
+    r, u, p = cs.exact_riemann((1.0, 0.0, 1.0), (0.125, 0.0, 0.1), x, 0.25)
+    assert abs(p[0] - 0.30313) < 5e-5 and abs(u[0] - 0.92745) < 5e-5
+    assert abs(r[0] - 0.42632) < 5e-5 and abs(r[1] - 0.26557) < 5e-5
+
+
+def test_sod_converges_to_exact_solution():
+    errs = []
+    for n in (100, 200, 400):
+        c = cs.riemann_1d(n=n)
+        o = oracle.Oracle(c)
+        P = c.P0.copy()
+        o.run_to(P, 0.2)
+        st = o.status()
+        assert st.code == 0 and abs(st.time - 0.2) < 1e-9
+        x = c.blocks[0]["centres"][:, 0, 0, 0]
+        r, u, p = cs.exact_riemann((1.0, 0.0, 1.0), (0.125, 0.0, 0.1), x, st.time)
+        I = c.interior(P, 0)[:, :, 0, 0]
+        errs.append(np.abs(I[0] - r).mean())
+        assert np.abs(I[2]).max() == 0.0 and np.abs(I[3]).max() == 0.0   # no transverse motion
+    assert errs[0] < 1e-2 and errs[1] < 0.7 * errs[0] and errs[2] < 0.7 * errs[1], errs
+
+
+@pytest.mark.parametrize("riemann", [abi.RS_HLLC, abi.RS_AUSMP, abi.RS_LMROE])
+def test_tgv_conserves_mass_and_energy(riemann):
+    c = cs.taylor_green(n=12, riemann=riemann)
+    o = oracle.Oracle(c)
+    P = c.P0.copy()
+    q0 = H.conserved(c, P).sum(axis=1)
+    ke0 = (0.5 * q0[0])
+    assert o.step(P, 10) == 0
+    q1 = H.conserved(c, P).sum(axis=1)
+    # uniform volumes: the sums of rho and rho E are conserved to round-off
+    assert abs(q1[0] - q0[0]) <= 1e-13 * abs(q0[0])
+    assert abs(q1[4] - q0[4]) <= 1e-12 * abs(q0[4])
+    for s in (1, 2, 3):
+        assert abs(q1[s] - q0[s]) <= 1e-10 * abs(q0[4]) ** 0.5 * c.n_interior
+    del ke0
+
+
+def test_tgv_kinetic_energy_decays():
+    c = cs.taylor_green(n=16)
+    o = oracle.Oracle(c)
+    P = c.P0.copy()
+
+    def ke(P):
+        I = c.interior(P, 0)
+        return (0.5 * I[0] * (I[1] ** 2 + I[2] ** 2 + I[3] ** 2)).sum()
+    k = [ke(P)]
+    for _ in range(4):
+        assert o.step(P, 5) == 0
+        k.append(ke(P))
+    assert all(b < a for a, b in zip(k, k[1:])), k
+    assert k[-1] > 0.5 * k[0]
+
+
+def test_block_split_matches_single_block():
+    """8 blocks joined by 1:1 connections against one periodic block: the connection records use their
+    own arithmetic (Lib_BC.f90:1770-1867), so the two agree to round-off, not bit for bit."""
+    a = cs.taylor_green(n=12, blocks=1)
+    b = cs.taylor_green(n=12, blocks=2)
+    Pa, Pb = a.P0.copy(), b.P0.copy()
+    oracle.Oracle(a).step(Pa, 5)
+    oracle.Oracle(b).step(Pb, 5)
+    full = np.zeros_like(a.interior(Pa, 0))
+    for q, blk in enumerate(b.blocks):
+        lo, n = blk["lo"], blk["n"]
+        full[:, lo[0]:lo[0] + n[0], lo[1]:lo[1] + n[1], lo[2]:lo[2] + n[2]] = b.interior(Pb, q)
+    e = H.rel_err(full, a.interior(Pa, 0))
+    assert np.all(e < 1e-11), e
+
+
+def test_min_rule_unstable_additive_stable_at_cfl_08():
+    """CFL 0.8 per direction with the min dt rule (the reference default) diverges on the 3-D TGV;
+    the additive rule the TGV configs use is stable."""
+    c = cs.taylor_green(n=12)
+    c.scheme["dt_additive"] = 0
+    P = c.P0.copy()
+    assert oracle.Oracle(c).step(P, 30) != 0
+    c2 = cs.taylor_green(n=12)
+    P2 = c2.P0.copy()
+    assert oracle.Oracle(c2).step(P2, 30) == 0
+
+
+def test_golden_vectors():
+    """The oracle reproduces its committed golden vectors (regression pin of the restatement)."""
+    import make_golden
+    for name, builder, nsteps in make_golden.CASES:
+        ref = np.load(os.path.join(GOLDEN, name + ".npz"))
+        R, P, dt = make_golden.run(builder(), nsteps)
+        np.testing.assert_array_equal(R, ref["R"])
+        np.testing.assert_array_equal(P, ref["P"])
+        assert dt == float(ref["dt"])
