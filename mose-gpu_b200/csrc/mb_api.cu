@@ -32,6 +32,7 @@ struct mb_ctx {
   DevState* d_st = nullptr;
   DTile* d_tiles_sweep = nullptr;
   int ntiles_sweep = 0;
+  int ty_sweep = 4;
   DTile* d_tiles_aux = nullptr;
   int ntiles_aux = 0;
   double* d_scratch = nullptr;  // the engine's own stage buffer (ncell x 5)
@@ -223,7 +224,13 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   }
   for (size_t q = 0; q < tab.size(); ++q) tabf[q] = (float)tab[q];
   // ---- tiles
-  std::vector<DTile> ts = make_tiles(mesh, sc->precision == MB_PREC_MIXED ? TY_F32 : TY_F64, 16);
+  // tile rows of the sweep: the form's default, or MB_SWEEP_TY (4 or 8) to tune
+  c->ty_sweep = sc->precision == MB_PREC_MIXED ? TY_F32 : TY_F64;
+  if (const char* e = getenv("MB_SWEEP_TY")) {
+    int v = atoi(e);
+    if (v == 4 || v == 8) c->ty_sweep = v;
+  }
+  std::vector<DTile> ts = make_tiles(mesh, c->ty_sweep, 16);
   std::vector<DTile> ta = make_tiles(mesh, TY_AUX, 16);
   TRY(upload(&c->d_blk, hb.data(), hb.size()));
   TRY(upload(&c->d_recmap, recmap.data(), recmap.size()));
@@ -287,8 +294,8 @@ void mb_destroy(mb_ctx* ctx) {
 static int sweep(mb_ctx* c, int mode, const double* Pin, const double* Pold, double* Pout, double* Rout, double rkc,
                  int last, cudaStream_t s) {
   cudaError_t e = (c->sc.precision == MB_PREC_MIXED)
-                      ? sweep_f32(c->p, c->d_tiles_sweep, c->ntiles_sweep, mode, Pin, Pold, Pout, Rout, rkc, last, s)
-                      : sweep_f64(c->p, c->d_tiles_sweep, c->ntiles_sweep, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+                      ? sweep_f32(c->p, c->d_tiles_sweep, c->ntiles_sweep, c->ty_sweep, mode, Pin, Pold, Pout, Rout, rkc, last, s)
+                      : sweep_f64(c->p, c->d_tiles_sweep, c->ntiles_sweep, c->ty_sweep, mode, Pin, Pold, Pout, Rout, rkc, last, s);
   c->launches += 1;
   CK(e);
   return MB_OK;

@@ -27,14 +27,14 @@ struct DTile {
 
 enum { MODE_RESIDUAL = 0, MODE_UPDATE = 1 };
 
-template <typename R> __device__ __forceinline__ R cvt(double x) { return (R)x; }
+template <typename R> MB_HD R cvt(double x) { return (R)x; }
 
 // ---------------------------------------------------------------------------------------------
 // One interior face of direction d between cell (i,j,k) and its +d neighbour: the convective flux
 // (conv_physics.inc) into out[0..4] and, for Navier-Stokes, the viscous flux (diff_physics.inc)
 // into out[5..9].
 template <typename R, bool VISC>
-__device__ __forceinline__ void face_flux(const Params& p, const DBlk& b, const double* __restrict__ P, int d, int i,
+MB_HD void face_flux(const Params& p, const DBlk& b, const double* __restrict__ P, int d, int i,
                                           int j, int k, R* out) {
   const long long nc = p.nc;
   const long long r0 = row(b, i, j, k);
@@ -107,7 +107,7 @@ __device__ __forceinline__ void face_flux(const Params& p, const DBlk& b, const 
 
 // ---------------------------------------------------------------------------------------------
 // The boundary record of the cell (i,j,k) on face F, added into acc (the R_flat row of the cell).
-__device__ __forceinline__ void bc_face_geom(const DBlk& b, int Im, int Jm, int Km, int F, double* g) {
+MB_HD void bc_face_geom(const DBlk& b, int Im, int Jm, int Km, int F, double* g) {
   int dir = (F + 1) / 2, modfm = F % 2;
   const double* f = (dir == 1) ? fm1p(b, Im - modfm, Jm, Km) : (dir == 2 ? fm2p(b, Im, Jm - modfm, Km) : fm3p(b, Im, Jm, Km - modfm));
   g[0] = ld(f); g[1] = ld(f + 1); g[2] = ld(f + 2); g[3] = ld(f + 3);
@@ -115,7 +115,7 @@ __device__ __forceinline__ void bc_face_geom(const DBlk& b, int Im, int Jm, int 
 
 // BC_Connection_Eul_lean (Lib_BC.f90:1770-1867)
 template <typename R>
-__device__ __noinline__ void bc_conn_eul(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
+MB_HD_NOINLINE void bc_conn_eul(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
                                          int Km, int Fm, double* acc) {
   const long long nc = p.nc;
   int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm1 = 1 - modfm, modfm2 = 1 - 2 * modfm, gstep = 2 * modfm - 1;
@@ -170,7 +170,7 @@ __device__ __noinline__ void bc_conn_eul(const Params& p, const DBlk& b, const d
 
 // BC_Connection_Visc_lean (Lib_BC.f90:2113-2178); pg = bc_pg(:,1:6) of the record
 template <typename R>
-__device__ __noinline__ void bc_conn_visc(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
+MB_HD_NOINLINE void bc_conn_visc(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
                                           int Km, int Fm, const double* __restrict__ pg, double* acc) {
   const long long nc = p.nc;
   int dir = (Fm + 1) / 2, modfm2 = 1 - 2 * (Fm % 2), gstep = 2 * (Fm % 2) - 1;
@@ -239,7 +239,7 @@ __device__ __noinline__ void bc_conn_visc(const Params& p, const DBlk& b, const 
 
 // BC_Extrapolation (Lib_BC.f90:1119-1165)
 template <typename R>
-__device__ __noinline__ void bc_extrap(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
+MB_HD_NOINLINE void bc_extrap(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
                                        int Km, int Fm, double* acc) {
   const long long nc = p.nc;
   const long long r = row(b, Im, Jm, Km);
@@ -266,7 +266,7 @@ __device__ __noinline__ void bc_extrap(const Params& p, const DBlk& b, const dou
 
 // the records of the faces 1..6 that the cell (i,j,k) lies on, in face order
 template <typename R, bool VISC>
-__device__ __forceinline__ void bc_cell(const Params& p, const DBlk& b, const double* __restrict__ P, int i, int j,
+MB_HD void bc_cell(const Params& p, const DBlk& b, const double* __restrict__ P, int i, int j,
                                         int k, double* acc) {
   const int n[3] = {b.n1, b.n2, b.n3};
   const int c[3] = {i, j, k};
@@ -294,7 +294,7 @@ __device__ __forceinline__ void bc_cell(const Params& p, const DBlk& b, const do
 // ---------------------------------------------------------------------------------------------
 // The conservative state update of one cell (newstate_cons_body.inc), FP64. Returns the new
 // primitive state in pn.
-__device__ __forceinline__ void cons_update(const Params& p, const double* pc, const double* po, const double* res,
+MB_HD void cons_update(const Params& p, const double* pc, const double* po, const double* res,
                                             double vol, double dt, double rkc, double tc, double* pn) {
   const double strang = 1.0;
   double cons[MB_NP], cold[MB_NP], rl[MB_NP];
@@ -350,7 +350,7 @@ __device__ __forceinline__ void cons_update(const Params& p, const double* pc, c
 }
 
 // local dt of one cell (dt_blk.inc: min rule :156-191, additive rule :79-155), FP64
-__device__ __forceinline__ double cell_dt(const Params& p, const DBlk& b, long long l, const double* pl) {
+MB_HD double cell_dt(const Params& p, const DBlk& b, long long l, const double* pl) {
   double rho, Rg;
   rotot_rtot(p, pl[0], rho, Rg);
   double Tc = pl[MB_IPR] / (rho * Rg);

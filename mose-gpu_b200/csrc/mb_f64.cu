@@ -150,20 +150,32 @@ static cudaError_t set_attr() {
 
 cudaError_t sweep_setup_f64() {
   cudaError_t e;
-  if ((e = set_attr<TY_F64, true, MODE_RESIDUAL>()) != cudaSuccess) return e;
-  if ((e = set_attr<TY_F64, true, MODE_UPDATE>()) != cudaSuccess) return e;
-  if ((e = set_attr<TY_F64, false, MODE_RESIDUAL>()) != cudaSuccess) return e;
-  return set_attr<TY_F64, false, MODE_UPDATE>();
+  if ((e = set_attr<4, true, MODE_RESIDUAL>()) != cudaSuccess) return e;
+  if ((e = set_attr<4, true, MODE_UPDATE>()) != cudaSuccess) return e;
+  if ((e = set_attr<4, false, MODE_RESIDUAL>()) != cudaSuccess) return e;
+  if ((e = set_attr<4, false, MODE_UPDATE>()) != cudaSuccess) return e;
+  if ((e = set_attr<8, true, MODE_RESIDUAL>()) != cudaSuccess) return e;
+  if ((e = set_attr<8, true, MODE_UPDATE>()) != cudaSuccess) return e;
+  if ((e = set_attr<8, false, MODE_RESIDUAL>()) != cudaSuccess) return e;
+  return set_attr<8, false, MODE_UPDATE>();
 }
 
-cudaError_t sweep_f64(const Params& p, const DTile* tiles, int ntiles, int mode, const double* Pin, const double* Pold,
-                      double* Pout, double* Rout, double rkc, int last, cudaStream_t s) {
+template <int TY>
+static cudaError_t sweep_ty(const Params& p, const DTile* tiles, int ntiles, int mode, const double* Pin,
+                            const double* Pold, double* Pout, double* Rout, double rkc, int last, cudaStream_t s) {
   if (p.visc) {
-    if (mode == MODE_RESIDUAL) return sweep_one<TY_F64, true, MODE_RESIDUAL>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
-    return sweep_one<TY_F64, true, MODE_UPDATE>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
+    if (mode == MODE_RESIDUAL) return sweep_one<TY, true, MODE_RESIDUAL>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
+    return sweep_one<TY, true, MODE_UPDATE>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
   }
-  if (mode == MODE_RESIDUAL) return sweep_one<TY_F64, false, MODE_RESIDUAL>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
-  return sweep_one<TY_F64, false, MODE_UPDATE>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
+  if (mode == MODE_RESIDUAL) return sweep_one<TY, false, MODE_RESIDUAL>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
+  return sweep_one<TY, false, MODE_UPDATE>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
+}
+
+cudaError_t sweep_f64(const Params& p, const DTile* tiles, int ntiles, int ty, int mode, const double* Pin,
+                      const double* Pold, double* Pout, double* Rout, double rkc, int last, cudaStream_t s) {
+  if (ty == 8) return sweep_ty<8>(p, tiles, ntiles, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+  if (ty == 4) return sweep_ty<4>(p, tiles, ntiles, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+  return cudaErrorInvalidValue;
 }
 
 static inline unsigned nblk_for(long long n, int t) { return (unsigned)((n + t - 1) / t); }

@@ -27,13 +27,13 @@ struct GhostLists {
   double* pg;             // [nconn][6][5]
 };
 
-constexpr int TY_F64 = 4;    // tile rows of the FP64 sweep
-constexpr int TY_F32 = 8;    // tile rows of the mixed sweep
+constexpr int TY_F64 = 4;    // default tile rows of the FP64 sweep (4 or 8; MB_SWEEP_TY overrides)
+constexpr int TY_F32 = 8;    // default tile rows of the mixed sweep
 constexpr int TY_AUX = 8;    // tile rows of the per-cell kernels (dt, update)
 
-cudaError_t sweep_f64(const Params& p, const DTile* tiles, int ntiles, int mode, const double* Pin,
+cudaError_t sweep_f64(const Params& p, const DTile* tiles, int ntiles, int ty, int mode, const double* Pin,
                       const double* Pold, double* Pout, double* Rout, double rkc, int last, cudaStream_t s);
-cudaError_t sweep_f32(const Params& p, const DTile* tiles, int ntiles, int mode, const double* Pin,
+cudaError_t sweep_f32(const Params& p, const DTile* tiles, int ntiles, int ty, int mode, const double* Pin,
                       const double* Pold, double* Pout, double* Rout, double rkc, int last, cudaStream_t s);
 // ghost fill; *nl receives the number of kernels launched
 cudaError_t ghost_fill(const Params& p, const GhostLists& g, double* P, cudaStream_t s, int* nl);

@@ -25,6 +25,10 @@
 #define MB_IW 3
 #define MB_IPR 4
 
+// the arithmetic is callable from host code as well (host-side debugging of the device arithmetic)
+#define MB_HD __host__ __device__ __forceinline__
+#define MB_HD_NOINLINE __host__ __device__ __noinline__
+
 namespace mb {
 
 constexpr int GC = 2;
@@ -73,58 +77,64 @@ struct Params {
 
 template <typename R> struct Tab;
 template <> struct Tab<double> {
-  __device__ static const double* cp(const Params& p) { return p.cp; }
-  __device__ static const double* h(const Params& p) { return p.h; }
-  __device__ static const double* mu(const Params& p) { return p.mu; }
-  __device__ static const double* k(const Params& p) { return p.k; }
+  MB_HD static const double* cp(const Params& p) { return p.cp; }
+  MB_HD static const double* h(const Params& p) { return p.h; }
+  MB_HD static const double* mu(const Params& p) { return p.mu; }
+  MB_HD static const double* k(const Params& p) { return p.k; }
 };
 template <> struct Tab<float> {
-  __device__ static const float* cp(const Params& p) { return p.cpf; }
-  __device__ static const float* h(const Params& p) { return p.hf; }
-  __device__ static const float* mu(const Params& p) { return p.muf; }
-  __device__ static const float* k(const Params& p) { return p.kf; }
+  MB_HD static const float* cp(const Params& p) { return p.cpf; }
+  MB_HD static const float* h(const Params& p) { return p.hf; }
+  MB_HD static const float* mu(const Params& p) { return p.muf; }
+  MB_HD static const float* k(const Params& p) { return p.kf; }
 };
 
-template <typename R> __device__ __forceinline__ R rsqrt_(R x);
-template <> __device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
-template <> __device__ __forceinline__ float rsqrt_(float x) { return sqrtf(x); }
+template <typename R> MB_HD R rsqrt_(R x);
+template <> MB_HD double rsqrt_(double x) { return sqrt(x); }
+template <> MB_HD float rsqrt_(float x) { return sqrtf(x); }
 
 // ---- indexing (gpu/MOSE_Field_m.f90:78-109) ----
-__device__ __forceinline__ long long lin(const DBlk& b, int i, int j, int k) {
+MB_HD long long lin(const DBlk& b, int i, int j, int k) {
   return (long long)(i + GC - 1) + (long long)(j + GC - 1) * b.pi + (long long)(k + GC - 1) * b.pi * b.pj;
 }
-__device__ __forceinline__ long long row(const DBlk& b, int i, int j, int k) { return b.boff + lin(b, i, j, k); }
-__device__ __forceinline__ const double* fm1p(const DBlk& b, int i, int j, int k) {
+MB_HD long long row(const DBlk& b, int i, int j, int k) { return b.boff + lin(b, i, j, k); }
+MB_HD const double* fm1p(const DBlk& b, int i, int j, int k) {
   return b.fm1 + 4 * ((long long)i + (long long)(b.n1 + 1) * ((j - 1) + (long long)b.n2 * (k - 1)));
 }
-__device__ __forceinline__ const double* fm2p(const DBlk& b, int i, int j, int k) {
+MB_HD const double* fm2p(const DBlk& b, int i, int j, int k) {
   return b.fm2 + 4 * ((long long)(i - 1) + (long long)b.n1 * (j + (long long)(b.n2 + 1) * (k - 1)));
 }
-__device__ __forceinline__ const double* fm3p(const DBlk& b, int i, int j, int k) {
+MB_HD const double* fm3p(const DBlk& b, int i, int j, int k) {
   return b.fm3 + 4 * ((long long)(i - 1) + (long long)b.n1 * ((j - 1) + (long long)b.n2 * k));
 }
-__device__ __forceinline__ const double* fmp(const DBlk& b, int d, int i, int j, int k) {
+MB_HD const double* fmp(const DBlk& b, int d, int i, int j, int k) {
   return d == 0 ? fm1p(b, i, j, k) : (d == 1 ? fm2p(b, i, j, k) : fm3p(b, i, j, k));
 }
-__device__ __forceinline__ double ld(const double* p) { return __ldg(p); }
+MB_HD double ld(const double* p) {
+#ifdef __CUDA_ARCH__
+  return __ldg(p);
+#else
+  return *p;
+#endif
+}
 
 // min / max with the semantics of std::min / std::max of the CPU restatement ((b < a) ? b : a and
 // (a < b) ? b : a): the same operand is returned for equal values, so signed zeros match as well
-template <typename R> __device__ __forceinline__ R mn(R a, R b) { return (b < a) ? b : a; }
-template <typename R> __device__ __forceinline__ R mx(R a, R b) { return (a < b) ? b : a; }
+template <typename R> MB_HD R mn(R a, R b) { return (b < a) ? b : a; }
+template <typename R> MB_HD R mx(R a, R b) { return (a < b) ? b : a; }
 
 // ---- table lookups ----
 // The table row of a temperature, kept inside [tmin, tmax-1] (NaN -> tmin): on the table this is
 // int(T) as in the reference; off it the reference would index outside the table, which must never
 // happen on the GPU (the thermo guard / state check report such a state).
 template <typename R>
-__device__ __forceinline__ int tidx(const Params& p, R T) {
+MB_HD int tidx(const Params& p, R T) {
   if (!(T >= (R)p.tmin)) return p.tmin;
   if (T >= (R)(p.tmax - 1)) return p.tmax - 1;
   return (int)T;
 }
 template <typename R>
-__device__ __forceinline__ R tabT(const R* t, int ti, R td) {
+MB_HD R tabT(const R* t, int ti, R td) {
   R a = t[ti];
   R b = t[ti + 1];
   return a + (b - a) * td;
@@ -132,17 +142,17 @@ __device__ __forceinline__ R tabT(const R* t, int ti, R td) {
 
 // ---- FLINT leaves (Lib_ThermoTransport_dev.f90) ----
 template <typename R>
-__device__ __forceinline__ void rotot_rtot(const Params& p, R rhoi, R& rho, R& Rg) {
+MB_HD void rotot_rtot(const Params& p, R rhoi, R& rho, R& Rg) {
   rho = (R)0 + rhoi;
   Rg = (R)0 + (R)p.ri * rhoi / rho;
 }
 template <typename R>
-__device__ __forceinline__ R f_cp(const Params& p, R rhoi, int ti, R td, R rho) {
+MB_HD R f_cp(const Params& p, R rhoi, int ti, R td, R rho) {
   R cpi = tabT(Tab<R>::cp(p), ti, td);
   return (R)0 + rhoi / rho * cpi;
 }
 template <typename R>
-__device__ __forceinline__ R f_ss(const Params& p, R rhoi, R pr, R rho, R Rtot) {
+MB_HD R f_ss(const Params& p, R rhoi, R pr, R rho, R Rtot) {
   R T = pr / (Rtot * rho);
   int ti = tidx(p, T);
   R td = T - (R)ti;
@@ -151,7 +161,7 @@ __device__ __forceinline__ R f_ss(const Params& p, R rhoi, R pr, R rho, R Rtot) 
   return rsqrt_(gam * Rtot * T);
 }
 template <typename R>
-__device__ __forceinline__ R H0(const Params& p, R pr, R rhoi, R u) {
+MB_HD R H0(const Params& p, R pr, R rhoi, R u) {
   R rho = (R)0 + rhoi;
   R Rg = (R)0 + (R)p.ri * rhoi / rho;
   R T = pr / (Rg * rho);
@@ -162,7 +172,7 @@ __device__ __forceinline__ R H0(const Params& p, R pr, R rhoi, R u) {
 }
 // f_molecularWeight + co_fiij_dev + co_k_mi_lam_Wilke_dev, one species
 template <typename R>
-__device__ __forceinline__ void wilke(const Params& p, R rhoi, R rho, int ti, R td, R& mil, R& kl) {
+MB_HD void wilke(const Params& p, R rhoi, R rho, int ti, R td, R& mil, R& kl) {
   const R wm = (R)p.wm;
   R rho_ = (R)0 + rhoi;
   R wmt = (R)0 + (rhoi / rho_ / wm);
@@ -184,8 +194,16 @@ __device__ __forceinline__ void wilke(const Params& p, R rhoi, R rho, int ti, R 
 }
 
 // ---- limiter (Lib_Limiters.f90:65-97) ----
+// The ratio ru = y / (x + 1e-30) reaches ~1e27 where a slope is exactly zero (a velocity component
+// that is zero, a symmetry point); ru*ru then overflows FP32 and van Albada turns into inf/inf = NaN,
+// where FP64 gives phi = 1 (and the limited slope phi*x = 0). The FP32 form therefore holds |ru| to
+// 1e18, beyond which every limiter function below has reached its FP32 limit value; the FP64 form
+// is untouched.
+template <typename R> MB_HD R hold_ratio(R ru) { return ru; }
+template <> MB_HD float hold_ratio<float>(float ru) { return mx(mn(ru, 1e18f), -1e18f); }
+
 template <typename R>
-__device__ __forceinline__ R rlimiter(int lim, R x, R y) {
+MB_HD R rlimiter(int lim, R x, R y) {
   R ru, phi;
   switch (lim) {
     case 1: {
@@ -195,19 +213,19 @@ __device__ __forceinline__ R rlimiter(int lim, R x, R y) {
       return r;
     }
     case 2:
-      ru = y / (x + (R)1e-30);
+      ru = hold_ratio(y / (x + (R)1e-30));
       phi = (ru + fabs(ru)) / ((R)1 + fabs(ru));
       return phi * x;
     case 3:
-      ru = y / (x + (R)1e-30);
+      ru = hold_ratio(y / (x + (R)1e-30));
       phi = (ru * ru + ru) / ((R)1 + ru * ru);
       return phi * x;
     case 4:
-      ru = y / (x + (R)1e-30);
+      ru = hold_ratio(y / (x + (R)1e-30));
       phi = mx((R)0, mn(mn((R)2 * ru, (R)0.5 * ((R)1 + ru)), (R)2));
       return phi * x;
     case 5:
-      ru = y / (x + (R)1e-30);
+      ru = hold_ratio(y / (x + (R)1e-30));
       phi = mx(mx((R)0, mn((R)2 * ru, (R)1)), mn(ru, (R)2));
       return phi * x;
     default:
@@ -217,7 +235,7 @@ __device__ __forceinline__ R rlimiter(int lim, R x, R y) {
 
 // ---- MOSE_open solvers of riemann_open_body.inc: AUSM+ (4), LMRoe (12) ----
 template <typename R>
-__device__ __forceinline__ R h_static(const Params& p, R rhoi, R pr) {
+MB_HD R h_static(const Params& p, R rhoi, R pr) {
   R rho_ = (R)0 + rhoi;
   R rg = (R)0 + (R)p.ri * rhoi / rho_;
   R T = pr / (rg * rho_);
@@ -233,7 +251,7 @@ __device__ __forceinline__ R h_static(const Params& p, R rhoi, R pr) {
 }
 
 template <typename R>
-__device__ __forceinline__ void riemann_open(const Params& p, int rs, R dl, R ul, R vl, R wl, R pl, R al, R dltot,
+MB_HD void riemann_open(const Params& p, int rs, R dl, R ul, R vl, R wl, R pl, R al, R dltot,
                                              R dr, R ur, R vr, R wr, R pr, R ar, R drtot, R nx, R ny, R nz,
                                              R& F_r, R& F_u, R& F_v, R& F_w, R& F_E) {
   R unl = ul * nx + vl * ny + wl * nz;
@@ -368,7 +386,7 @@ __device__ __forceinline__ void riemann_open(const Params& p, int rs, R dl, R ul
 // Roe averages shared by the two HLLC forms: the inline one of conv_physics.inc (clamped T row, Rl/Rr
 // taken from the caller) and riemann_HLLC / roe_averages of Lib_Riemann_HLL.f90 (boundary records).
 template <typename R>
-__device__ __forceinline__ void hllc(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R Rl, R dr, R ur,
+MB_HD void hllc(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R Rl, R dr, R ur,
                                      R vr, R wr, R pr, R ar, R drtot, R Rr, R nx, R ny, R nz, R& F_r, R& F_u,
                                      R& F_v, R& F_w, R& F_E) {
   const R* H = Tab<R>::h(p);
@@ -439,7 +457,7 @@ __device__ __forceinline__ void hllc(const Params& p, R dl, R ul, R vl, R wl, R 
 
 // ---- interior convective face from the 4-cell stencil (conv_physics.inc) ----
 template <typename R>
-__device__ __forceinline__ void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, const R* pp2,
+MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, const R* pp2,
                                           const R* dlc, R nx, R ny, R nz, R area, R* res0) {
   R l0 = (R)0.5 * (dlc[0] + dlc[1]), l1 = (R)0.5 * (dlc[1] + dlc[2]), l2 = (R)0.5 * (dlc[2] + dlc[3]);
   R lm = (R)0.5 * dlc[1], lp = (R)0.5 * dlc[2];
@@ -490,7 +508,7 @@ __device__ __forceinline__ void conv_face(const Params& p, const R* pm1, const R
 
 // face thermo (Diffusive_Face_Thermo_Fill, Mod_Diffusive.f90:311-325 = Diffusive_Face_State :748-776)
 template <typename R>
-__device__ __forceinline__ void face_thermo(const Params& p, R rhoi, R pr, R& rho, R& T, int& ti, R& td, R& cp,
+MB_HD void face_thermo(const Params& p, R rhoi, R pr, R& rho, R& T, int& ti, R& td, R& cp,
                                             R& mil, R& kl) {
   R Rgas;
   rotot_rtot(p, rhoi, rho, Rgas);
@@ -505,7 +523,7 @@ __device__ __forceinline__ void face_thermo(const Params& p, R rhoi, R pr, R& rh
 // the laminar viscous flux of a face from its gradients (diff_physics.inc:88-161 with mie = 0);
 // Stress_Vector_Std (physics/turbulence/Mod_Fluid.f90:20-44) is the same arithmetic
 template <typename R>
-__device__ __forceinline__ void visc_flux(const Params& p, const R G[MB_NP][3], const R* Pf, R nx, R ny, R nz,
+MB_HD void visc_flux(const Params& p, const R G[MB_NP][3], const R* Pf, R nx, R ny, R nz,
                                           R area, R drho, R dT, R dcp, R dmil, R dkl, R* F) {
   int Ti = tidx(p, dT);
   R Tdf = dT - (R)Ti;
@@ -542,12 +560,12 @@ __device__ __forceinline__ void visc_flux(const Params& p, const R G[MB_NP][3], 
 
 // the cell density / temperature of the thermo cache (Mod_Thermo_Cache.f90:327-330,378-380)
 template <typename R>
-__device__ __forceinline__ void cell_rho_T(const Params& p, R rhoi, R pr, R& rho, R& T) {
+MB_HD void cell_rho_T(const Params& p, R rhoi, R pr, R& rho, R& T) {
   R Rg;
   rotot_rtot(p, rhoi, rho, Rg);
   T = pr / (rho * Rg);
 }
 
-__device__ __forceinline__ int face_sign(int F) { return 1 - 2 * (F % 2); }  // modfm2 / FluxSign
+MB_HD int face_sign(int F) { return 1 - 2 * (F % 2); }  // modfm2 / FluxSign
 
 }  // namespace mb
