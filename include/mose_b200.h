@@ -220,6 +220,23 @@ int mb_profile_stage(mb_ctx* ctx, double* P, double* PO, int irk, int nrep, floa
 /* Status (state check, thermo guard, first offender, simulated time, last dt). Synchronises. */
 int mb_get_status(mb_ctx* ctx, mb_status* st);
 
+/* Compute_dt of one block without allocating any device memory. No counterpart in the reference.
+ * For callers that cannot allocate device memory when they need a time step: a Fortran host whose device
+ * arrays belong to the OpenACC runtime, a serving loop already at its HBM budget, or code that must not
+ * synchronise the device or is capturing a CUDA graph (cudaMalloc / cudaFree synchronise and are not
+ * allowed during capture). Everything is caller-owned: P (the arena, ncell_total rows), the block's
+ * padded dl and m, the FP64 cp, mu and k tables (rows tmin..tmax) on the device, the scheme (host
+ * struct: cfl, vnn, prandtl, ndir, visc, dt_additive) and dt_out, one device double that receives
+ * min(1e5, min of the local dt) as mb_dt computes it. The only scratch is a file-scope device array of
+ * 65536 doubles (512 KB) of per-CTA partial minima, held by every GPU that loads the library until exit;
+ * a block whose 32 x 8-cell (i, j) tiles exceed 65536 is rejected with MB_E_ARG. The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress), so make that first call before
+ * any stream capture. Calls share the array: calls that overlap on the GPU (different streams, no
+ * ordering between them) race and must not be issued. */
+int mb_dt_block_noalloc(const double* P, int64_t ncell_total, int64_t boff, const int32_t n[3], const double* dl,
+                        const double* m, const double* cp, const double* mu, const double* k, int32_t tmin,
+                        int32_t tmax, double wm, const mb_scheme* sc, double* dt_out, void* stream);
+
 /* Number of kernel launches this context has issued (for launch accounting). */
 int64_t mb_launch_count(const mb_ctx* ctx);
 

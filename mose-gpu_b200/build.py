@@ -16,7 +16,8 @@ BUILD = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-lineinfo", "-Xptxas", "-v"]
-UNITS = [("mb_f64.cu", ["--fmad=false"]), ("mb_f32.cu", ["--fmad=true"]), ("mb_api.cu", ["--fmad=false"])]
+UNITS = [("mb_f64.cu", ["--fmad=false"]), ("mb_f32.cu", ["--fmad=true"]), ("mb_api.cu", ["--fmad=false"]),
+         ("mb_noalloc.cu", ["--fmad=false"])]
 DEPS = ["mb_physics.cuh", "mb_engine.cuh", "mb_launch.h", os.path.join("..", "..", "include", "mose_b200.h")]
 
 
