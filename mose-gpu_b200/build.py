@@ -1,13 +1,17 @@
 """Builds the engine's shared library in-tree: mose-gpu_b200/mosegpu/libmose_b200.so (sm_100a).
 
-  mb_f64.cu, mb_api.cu   --fmad=false  (the FP64 form rounds statement by statement as written)
-  mb_f32.cu              --fmad=true   (the mixed form: FP32 flux arithmetic with FMA)
+  mb_f64.cu, mb_api.cu, mb_noalloc.cu, mb_sweep_f64_*.cu   --fmad=false
+      (the FP64 form rounds statement by statement as written)
+  mb_sweep_f32_*.cu   --fmad=true -prec-div=false -prec-sqrt=false -ftz=true
+      (the mixed form: FP32 flux arithmetic with FMA and the fast FP32 divide / square root; the FP64 state
+       arithmetic in those units is unaffected by these single-precision options)
 
-Usage: python mose-gpu_b200/build.py [--force]
+Units compile in parallel. Usage: python mose-gpu_b200/build.py [--force] [-v]
 """
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -16,9 +20,13 @@ BUILD = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-lineinfo", "-Xptxas", "-v"]
-UNITS = [("mb_f64.cu", ["--fmad=false"]), ("mb_f32.cu", ["--fmad=true"]), ("mb_api.cu", ["--fmad=false"]),
-         ("mb_noalloc.cu", ["--fmad=false"])]
-DEPS = ["mb_physics.cuh", "mb_engine.cuh", "mb_launch.h", os.path.join("..", "..", "include", "mose_b200.h")]
+F64 = ["--fmad=false"]
+F32 = ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
+UNITS = [("mb_f64.cu", F64), ("mb_api.cu", F64), ("mb_noalloc.cu", F64)] + \
+        [("mb_sweep_f64_rs%d.cu" % r, F64) for r in (1, 4, 12)] + \
+        [("mb_sweep_f32_rs%d.cu" % r, F32) for r in (1, 4, 12)]
+DEPS = ["mb_physics.cuh", "mb_engine.cuh", "mb_launch.h", "mb_sweep_inst.inc",
+        os.path.join("..", "..", "include", "mose_b200.h")]
 
 
 def _mtime(p):
@@ -28,16 +36,24 @@ def _mtime(p):
 def build(force=False, verbose=False):
     os.makedirs(BUILD, exist_ok=True)
     dep_t = max(_mtime(os.path.join(CSRC, d)) for d in DEPS)
+    jobs = []
     objs = []
-    logs = []
     for src, flags in UNITS:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(o)
         if force or _mtime(o) < max(_mtime(s), dep_t):
-            cmd = [NVCC] + ARCH + COMMON + flags + ["-c", s, "-o", o]
-            r = subprocess.run(cmd, capture_output=True, text=True)
-            logs.append(r.stderr)
+            jobs.append((src, [NVCC] + ARCH + COMMON + flags + ["-c", s, "-o", o]))
+
+    def run(job):
+        src, cmd = job
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return src, r
+
+    logs = []
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 4))) as ex:
+        for src, r in ex.map(run, jobs):
+            logs.append((src, r.stderr))
             if r.returncode != 0:
                 sys.stderr.write(r.stderr)
                 raise RuntimeError("nvcc failed on %s" % src)
@@ -48,8 +64,8 @@ def build(force=False, verbose=False):
             sys.stderr.write(r.stderr)
             raise RuntimeError("link failed")
     if verbose:
-        for l in logs:
-            sys.stdout.write(l)
+        for src, l in logs:
+            sys.stdout.write("== %s\n%s" % (src, l))
     return OUT
 
 

@@ -224,12 +224,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   }
   for (size_t q = 0; q < tab.size(); ++q) tabf[q] = (float)tab[q];
   // ---- tiles
-  // tile rows of the sweep: the form's default, or MB_SWEEP_TY (4 or 8) to tune
   c->ty_sweep = sc->precision == MB_PREC_MIXED ? TY_F32 : TY_F64;
-  if (const char* e = getenv("MB_SWEEP_TY")) {
-    int v = atoi(e);
-    if (v == 4 || v == 8) c->ty_sweep = v;
-  }
   std::vector<DTile> ts = make_tiles(mesh, c->ty_sweep, 16);
   std::vector<DTile> ta = make_tiles(mesh, TY_AUX, 16);
   TRY(upload(&c->d_blk, hb.data(), hb.size()));
@@ -262,7 +257,12 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
     return MB_E_NOMEM;
   }
   if (cudaMemset(c->d_scratch, 0, (size_t)c->ncell * MB_NPRIM * sizeof(double)) != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
-  if (sweep_setup_f64() != cudaSuccess || sweep_setup_f32() != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+  {
+    cudaError_t e = (sc->precision == MB_PREC_MIXED)
+                        ? (sc->riemann == 1 ? sweep_f32_rs1_setup() : sc->riemann == 4 ? sweep_f32_rs4_setup() : sweep_f32_rs12_setup())
+                        : (sc->riemann == 1 ? sweep_f64_rs1_setup() : sc->riemann == 4 ? sweep_f64_rs4_setup() : sweep_f64_rs12_setup());
+    if (e != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+  }
   // ---- kernel parameters
   Params& p = c->p;
   memset(&p, 0, sizeof(p));
@@ -293,9 +293,18 @@ void mb_destroy(mb_ctx* ctx) {
 
 static int sweep(mb_ctx* c, int mode, const double* Pin, const double* Pold, double* Pout, double* Rout, double rkc,
                  int last, cudaStream_t s) {
-  cudaError_t e = (c->sc.precision == MB_PREC_MIXED)
-                      ? sweep_f32(c->p, c->d_tiles_sweep, c->ntiles_sweep, c->ty_sweep, mode, Pin, Pold, Pout, Rout, rkc, last, s)
-                      : sweep_f64(c->p, c->d_tiles_sweep, c->ntiles_sweep, c->ty_sweep, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+  const DTile* t = c->d_tiles_sweep;
+  const int n = c->ntiles_sweep;
+  cudaError_t e;
+  if (c->sc.precision == MB_PREC_MIXED) {
+    if (c->sc.riemann == 1) e = sweep_f32_rs1(c->p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+    else if (c->sc.riemann == 4) e = sweep_f32_rs4(c->p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+    else e = sweep_f32_rs12(c->p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+  } else {
+    if (c->sc.riemann == 1) e = sweep_f64_rs1(c->p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+    else if (c->sc.riemann == 4) e = sweep_f64_rs4(c->p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+    else e = sweep_f64_rs12(c->p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+  }
   c->launches += 1;
   CK(e);
   return MB_OK;

@@ -33,7 +33,7 @@ template <typename R> MB_HD R cvt(double x) { return (R)x; }
 // One interior face of direction d between cell (i,j,k) and its +d neighbour: the convective flux
 // (conv_physics.inc) into out[0..4] and, for Navier-Stokes, the viscous flux (diff_physics.inc)
 // into out[5..9].
-template <typename R, bool VISC>
+template <typename R, bool VISC, int RS = 0, int LIM = 0>
 MB_HD void face_flux(const Params& p, const DBlk& b, const double* __restrict__ P, int d, int i,
                                           int j, int k, R* out) {
   const long long nc = p.nc;
@@ -52,7 +52,7 @@ MB_HD void face_flux(const Params& p, const DBlk& b, const double* __restrict__ 
   for (int q = 0; q < 4; ++q) dlc[q] = cvt<R>(ld(b.dl + d + 3 * (l0 + (q - 1) * st)));
   const double* f = fmp(b, d, i, j, k);
   R nx = cvt<R>(ld(f)), ny = cvt<R>(ld(f + 1)), nz = cvt<R>(ld(f + 2)), area = cvt<R>(ld(f + 3));
-  conv_face<R>(p, pm1, p0, pp1, pp2, dlc, nx, ny, nz, area, out);
+  conv_face<R, RS, LIM>(p, pm1, p0, pp1, pp2, dlc, nx, ny, nz, area, out);
   if (!VISC) return;
   // ---- viscous face: cells 1,2 = (c, c+d); 3,4 = c -/+ b-axis; 5,6 = c+d -/+ b; 7,8 = c -/+ c-axis; 9,10 = c+d -/+ c
   const long long sb = (d == 0) ? (long long)b.pi : 1;
@@ -114,10 +114,12 @@ MB_HD void bc_face_geom(const DBlk& b, int Im, int Jm, int Km, int F, double* g)
 }
 
 // BC_Connection_Eul_lean (Lib_BC.f90:1770-1867)
-template <typename R>
+template <typename R, int RS = 0, int LIM = 0>
 MB_HD_NOINLINE void bc_conn_eul(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
                                          int Km, int Fm, double* acc) {
   const long long nc = p.nc;
+  const int rs = RS ? RS : p.rs;
+  const int lim = LIM ? LIM : p.lim;
   int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm1 = 1 - modfm, modfm2 = 1 - 2 * modfm, gstep = 2 * modfm - 1;
   int o[4] = {modfm * (-gstep * GC) + modfm1 * gstep, modfm * (-gstep), modfm1 * (-gstep),
               modfm1 * (-gstep * GC) + modfm * gstep};
@@ -143,8 +145,8 @@ MB_HD_NOINLINE void bc_conn_eul(const Params& p, const DBlk& b, const double* __
     R q1 = cvt<R>(ld(P + rr[0] + s * nc)), q2 = cvt<R>(ld(P + rr[1] + s * nc)), q3 = cvt<R>(ld(P + rr[2] + s * nc)),
       q4 = cvt<R>(ld(P + rr[3] + s * nc));
     R d21 = (q2 - q1) / D12, d32 = (q3 - q2) / D23, d43 = (q4 - q3) / D34;
-    PL[s] = q2 + beta_ * rlimiter(p.lim, d32, d21) * Dl2;
-    PR[s] = q3 - beta_ * rlimiter(p.lim, d43, d32) * Dl3;
+    PL[s] = q2 + beta_ * rlimiter(lim, d32, d21) * Dl2;
+    PR[s] = q3 - beta_ * rlimiter(lim, d43, d32) * Dl3;
   }
   R rhoL, RL, rhoR, RRr;
   rotot_rtot(p, PL[0], rhoL, RL);
@@ -152,11 +154,11 @@ MB_HD_NOINLINE void bc_conn_eul(const Params& p, const DBlk& b, const double* __
   rotot_rtot(p, PR[0], rhoR, RRr);
   R aR = f_ss(p, PR[0], PR[MB_IPR], rhoR, RRr);
   R F_r, F_u, F_v, F_w, F_E;
-  if (p.rs == 1)
+  if (rs == 1)
     hllc(p, PL[0], PL[MB_IU], PL[MB_IV], PL[MB_IW], PL[MB_IPR], aL, rhoL, RL, PR[0], PR[MB_IU], PR[MB_IV], PR[MB_IW],
          PR[MB_IPR], aR, rhoR, RRr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
   else
-    riemann_open(p, p.rs, PL[0], PL[MB_IU], PL[MB_IV], PL[MB_IW], PL[MB_IPR], aL, rhoL, PR[0], PR[MB_IU], PR[MB_IV],
+    riemann_open(p, rs, PL[0], PL[MB_IU], PL[MB_IV], PL[MB_IW], PL[MB_IPR], aL, rhoL, PR[0], PR[MB_IU], PR[MB_IV],
                  PR[MB_IW], PR[MB_IPR], aR, rhoR, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
   R su = copysign((R)0.5, F_r), selL = (R)0.5 + su, selR = su - (R)0.5;
   R Fmass = F_r * area;
@@ -265,7 +267,7 @@ MB_HD_NOINLINE void bc_extrap(const Params& p, const DBlk& b, const double* __re
 }
 
 // the records of the faces 1..6 that the cell (i,j,k) lies on, in face order
-template <typename R, bool VISC>
+template <typename R, bool VISC, int RS = 0, int LIM = 0>
 MB_HD void bc_cell(const Params& p, const DBlk& b, const double* __restrict__ P, int i, int j,
                                         int k, double* acc) {
   const int n[3] = {b.n1, b.n2, b.n3};
@@ -283,7 +285,7 @@ MB_HD void bc_cell(const Params& p, const DBlk& b, const double* __restrict__ P,
     if (rid < 0) continue;
     const DRec& rc = p.rec[rid];
     if (rc.type == 1) {
-      bc_conn_eul<R>(p, b, P, i, j, k, F, acc);
+      bc_conn_eul<R, RS, LIM>(p, b, P, i, j, k, F, acc);
       if (VISC) bc_conn_visc<R>(p, b, P, i, j, k, F, p.pg + (long long)rc.pg * 6 * MB_NP, acc);
     } else if (rc.type == 11) {
       bc_extrap<R>(p, b, P, i, j, k, F, acc);
@@ -445,8 +447,9 @@ __device__ __forceinline__ void report_bad_state(const Params& p, int blk, int i
 }
 
 // ---------------------------------------------------------------------------------------------
-template <typename R, int TY, bool VISC, int MODE>
-__global__ void __launch_bounds__(32 * TY, 1)
+// MINB: resident CTAs per SM the register allocation must allow (launch bounds)
+template <typename R, int TY, bool VISC, int MODE, int RS, int LIM, int MINB>
+__global__ void __launch_bounds__(32 * TY, MINB)
 k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pin, const double* Pold, double* Pout,
         double* Rout, double rkc, int last) {
   constexpr int NF = VISC ? 2 * MB_NP : MB_NP;
@@ -497,7 +500,7 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
       }
       if (d < 0) continue;
       R out[NF];
-      face_flux<R, VISC>(p, b, Pin, d, fi, fj, fk, out);
+      face_flux<R, VISC, RS, LIM>(p, b, Pin, d, fi, fj, fk, out);
 #pragma unroll
       for (int q = 0; q < NF; ++q) dst[q] = out[q];
     }
@@ -532,7 +535,7 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
       }
       // ---- boundary records of the cell, face order 1..6
       if (i == 1 || i == b.n1 || j == 1 || j == b.n2 || k == 1 || k == b.n3)
-        bc_cell<R, VISC>(p, b, Pin, i, j, k, acc);
+        bc_cell<R, VISC, RS, LIM>(p, b, Pin, i, j, k, acc);
       const long long r = row(b, i, j, k);
       if (MODE == MODE_RESIDUAL) {
 #pragma unroll

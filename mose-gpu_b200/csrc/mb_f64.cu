@@ -1,6 +1,6 @@
-// mb_f64.cu -- the FP64 form of the engine: fused sweep instantiations and the per-cell / ghost
-// kernels. Built with --fmad=false so that every statement rounds as written (the operation order of
-// the reference statements is kept in mb_physics.cuh / mb_engine.cuh).
+// mb_f64.cu -- the per-cell and ghost kernels of the engine (FP64). Built with --fmad=false so that every
+// statement rounds as written (the operation order of the reference statements is kept in
+// mb_physics.cuh / mb_engine.cuh). The fused sweep is instantiated in the mb_sweep_*.cu units.
 #include "mb_launch.h"
 
 namespace mb {
@@ -134,50 +134,6 @@ __global__ void k_clock(Params p, int time_clip, double threshold) {
 }
 
 // ---- launchers ----
-template <int TY, bool VISC, int MODE>
-static cudaError_t sweep_one(const Params& p, const DTile* tiles, int ntiles, const double* Pin, const double* Pold,
-                             double* Pout, double* Rout, double rkc, int last, cudaStream_t s) {
-  const size_t sm = sweep_smem<double, TY, VISC>();
-  k_sweep<double, TY, VISC, MODE><<<ntiles, 32 * TY, sm, s>>>(p, tiles, Pin, Pold, Pout, Rout, rkc, last);
-  return cudaGetLastError();
-}
-
-template <int TY, bool VISC, int MODE>
-static cudaError_t set_attr() {
-  return cudaFuncSetAttribute(k_sweep<double, TY, VISC, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)sweep_smem<double, TY, VISC>());
-}
-
-cudaError_t sweep_setup_f64() {
-  cudaError_t e;
-  if ((e = set_attr<4, true, MODE_RESIDUAL>()) != cudaSuccess) return e;
-  if ((e = set_attr<4, true, MODE_UPDATE>()) != cudaSuccess) return e;
-  if ((e = set_attr<4, false, MODE_RESIDUAL>()) != cudaSuccess) return e;
-  if ((e = set_attr<4, false, MODE_UPDATE>()) != cudaSuccess) return e;
-  if ((e = set_attr<8, true, MODE_RESIDUAL>()) != cudaSuccess) return e;
-  if ((e = set_attr<8, true, MODE_UPDATE>()) != cudaSuccess) return e;
-  if ((e = set_attr<8, false, MODE_RESIDUAL>()) != cudaSuccess) return e;
-  return set_attr<8, false, MODE_UPDATE>();
-}
-
-template <int TY>
-static cudaError_t sweep_ty(const Params& p, const DTile* tiles, int ntiles, int mode, const double* Pin,
-                            const double* Pold, double* Pout, double* Rout, double rkc, int last, cudaStream_t s) {
-  if (p.visc) {
-    if (mode == MODE_RESIDUAL) return sweep_one<TY, true, MODE_RESIDUAL>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
-    return sweep_one<TY, true, MODE_UPDATE>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
-  }
-  if (mode == MODE_RESIDUAL) return sweep_one<TY, false, MODE_RESIDUAL>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
-  return sweep_one<TY, false, MODE_UPDATE>(p, tiles, ntiles, Pin, Pold, Pout, Rout, rkc, last, s);
-}
-
-cudaError_t sweep_f64(const Params& p, const DTile* tiles, int ntiles, int ty, int mode, const double* Pin,
-                      const double* Pold, double* Pout, double* Rout, double rkc, int last, cudaStream_t s) {
-  if (ty == 8) return sweep_ty<8>(p, tiles, ntiles, mode, Pin, Pold, Pout, Rout, rkc, last, s);
-  if (ty == 4) return sweep_ty<4>(p, tiles, ntiles, mode, Pin, Pold, Pout, Rout, rkc, last, s);
-  return cudaErrorInvalidValue;
-}
-
 static inline unsigned nblk_for(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 cudaError_t ghost_fill(const Params& p, const GhostLists& g, double* P, cudaStream_t s, int* nl) {

@@ -27,14 +27,26 @@ struct GhostLists {
   double* pg;             // [nconn][6][5]
 };
 
-constexpr int TY_F64 = 4;    // default tile rows of the FP64 sweep (4 or 8; MB_SWEEP_TY overrides)
-constexpr int TY_F32 = 8;    // default tile rows of the mixed sweep
+constexpr int TY_F64 = 4;    // tile rows of the FP64 sweep (128 threads)
+constexpr int TY_F32 = 8;    // tile rows of the mixed sweep (256 threads)
+constexpr int MINB_F64 = 2;  // resident CTAs per SM the FP64 sweep's registers must allow
+constexpr int MINB_F32 = 2;  // resident CTAs per SM the mixed sweep's registers must allow
 constexpr int TY_AUX = 8;    // tile rows of the per-cell kernels (dt, update)
 
-cudaError_t sweep_f64(const Params& p, const DTile* tiles, int ntiles, int ty, int mode, const double* Pin,
-                      const double* Pold, double* Pout, double* Rout, double rkc, int last, cudaStream_t s);
-cudaError_t sweep_f32(const Params& p, const DTile* tiles, int ntiles, int ty, int mode, const double* Pin,
-                      const double* Pold, double* Pout, double* Rout, double rkc, int last, cudaStream_t s);
+#define MB_CAT2(a, b) a##b
+#define MB_CAT(a, b) MB_CAT2(a, b)
+
+#define MB_DECLARE_SWEEP(name)                                                                                    \
+  cudaError_t name(const Params& p, const DTile* tiles, int ntiles, int mode, const double* Pin, const double* Pold, \
+                   double* Pout, double* Rout, double rkc, int last, cudaStream_t s);                              \
+  cudaError_t name##_setup();
+MB_DECLARE_SWEEP(sweep_f64_rs1)
+MB_DECLARE_SWEEP(sweep_f64_rs4)
+MB_DECLARE_SWEEP(sweep_f64_rs12)
+MB_DECLARE_SWEEP(sweep_f32_rs1)
+MB_DECLARE_SWEEP(sweep_f32_rs4)
+MB_DECLARE_SWEEP(sweep_f32_rs12)
+
 // ghost fill; *nl receives the number of kernels launched
 cudaError_t ghost_fill(const Params& p, const GhostLists& g, double* P, cudaStream_t s, int* nl);
 cudaError_t dt_cells(const Params& p, const DTile* tiles, int ntiles, const double* P, cudaStream_t s);
@@ -42,7 +54,5 @@ cudaError_t update_cells(const Params& p, const DTile* tiles, int ntiles, double
                          const double* R, double rkc, double dt, cudaStream_t s);
 cudaError_t reset_dt(const Params& p, cudaStream_t s);
 cudaError_t clock_step(const Params& p, int time_clip, double threshold, cudaStream_t s);
-cudaError_t sweep_setup_f64();
-cudaError_t sweep_setup_f32();
 
 }  // namespace mb

@@ -456,9 +456,12 @@ MB_HD void hllc(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R 
 }
 
 // ---- interior convective face from the 4-cell stencil (conv_physics.inc) ----
-template <typename R>
+// RS / LIM: the Riemann solver and limiter ids fixed at compile time (0: read p.rs / p.lim at run time)
+template <typename R, int RS = 0, int LIM = 0>
 MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, const R* pp2,
                                           const R* dlc, R nx, R ny, R nz, R area, R* res0) {
+  const int rs = RS ? RS : p.rs;
+  const int lim = LIM ? LIM : p.lim;
   R l0 = (R)0.5 * (dlc[0] + dlc[1]), l1 = (R)0.5 * (dlc[1] + dlc[2]), l2 = (R)0.5 * (dlc[2] + dlc[3]);
   R lm = (R)0.5 * dlc[1], lp = (R)0.5 * dlc[2];
   const R beta_order = (R)1;
@@ -469,8 +472,8 @@ MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, c
     R slope0 = (p0[s] - pm1[s]) * idl0;
     R slope1 = (pp1[s] - p0[s]) * idl1;
     R slope2 = (pp2[s] - pp1[s]) * idl2;
-    R slopel = rlimiter(p.lim, slope1, slope0);
-    R sloper = rlimiter(p.lim, slope2, slope1);
+    R slopel = rlimiter(lim, slope1, slope0);
+    R sloper = rlimiter(lim, slope2, slope1);
     P1[s] = p0[s] + beta_order * slopel * lm;
     P4[s] = pp1[s] - beta_order * sloper * lp;
   }
@@ -494,11 +497,11 @@ MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, c
   gamd = cpd / (cpd - Rtot4);
   R a4 = rsqrt_(gamd * Rtot4 * T4d);
   R F_r, F_u, F_v, F_w, F_E;
-  if (p.rs == 1)
+  if (rs == 1)
     hllc(p, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], a1, rotot1, Rtot1, P4[0], P4[MB_IU], P4[MB_IV],
          P4[MB_IW], P4[MB_IPR], a4, rotot4, Rtot4, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
   else
-    riemann_open(p, p.rs, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], a1, rotot1, P4[0], P4[MB_IU],
+    riemann_open(p, rs, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], a1, rotot1, P4[0], P4[MB_IU],
                  P4[MB_IV], P4[MB_IW], P4[MB_IPR], a4, rotot4, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
   R su = copysign((R)0.5, F_r), sp = (R)0.5 + su, sm = su - (R)0.5;
   R irotot1 = (R)1 / rotot1, irotot4 = (R)1 / rotot4;
