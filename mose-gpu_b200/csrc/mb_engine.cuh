@@ -30,22 +30,44 @@ enum { MODE_RESIDUAL = 0, MODE_UPDATE = 1 };
 template <typename R> MB_HD R cvt(double x) { return (R)x; }
 
 // ---------------------------------------------------------------------------------------------
-// One interior face of direction d between cell (i,j,k) and its +d neighbour: the convective flux
-// (conv_physics.inc) into out[0..4] and, for Navier-Stokes, the viscous flux (diff_physics.inc)
-// into out[5..9].
-template <typename R, bool VISC, int RS = 0, int LIM = 0>
-MB_HD void face_flux(const Params& p, const DBlk& b, const double* __restrict__ P, int d, int i,
-                                          int j, int k, R* out) {
-  const long long nc = p.nc;
+// The state tile of a CTA in shared memory: 4 k-planes (a rolling window), each (32+4) x (TY+4) cells
+// (two halo cells on each side in i and j), NV values per cell: rho_s, u, v, w, p of P and the thermo-cache
+// temperature T = p / (rho Rg) (Mod_Thermo_Cache.f90:327-330), converted to the flux arithmetic type once
+// per cell. Layout [slot][value][jj][ii], ii fastest.
+constexpr int TXH = 36;
+constexpr int NV = 6;
+
+template <typename R, int TY>
+struct Tile {
+  R* base;
+  static constexpr int VS = (TY + 4) * TXH;          // stride between the values of one cell
+  MB_HD int off(int slot, int jj, int ii) const { return slot * NV * VS + jj * TXH + ii; }
+  MB_HD R v(int o, int var) const { return base[o + var * VS]; }
+};
+
+// the plane slot of plane kk (kk >= -1)
+MB_HD int slot_of(int kk) { return (kk + 8) & 3; }
+
+// One interior face of direction d between cell (i,j,k) and its +d neighbour, from the state tile: the
+// convective flux (conv_physics.inc) into out[0..4] and, for Navier-Stokes, the viscous flux
+// (diff_cuf_kernels.inc:11-87 + diff_physics.inc) into out[5..9]. (ii, jj) are the tile coordinates of the
+// cell, sk the slot of plane k. The gradients are built per variable in registers and placed on the
+// axes by d (ia = d; the two tangential axes in increasing order), as the reference's Grad(:, ia/ib/ic).
+template <typename R, int TY, bool VISC, int RS = 0, int LIM = 0>
+MB_HD void face_flux(const Params& p, const DBlk& b, const Tile<R, TY>& T, int d, int i, int j, int k, int ii,
+                     int jj, R* out) {
+  const int skm = slot_of(k - 1), sk = slot_of(k), sk1 = slot_of(k + 1), sk2 = slot_of(k + 2);
   const long long r0 = row(b, i, j, k);
   const long long st = (d == 0) ? 1 : (d == 1 ? (long long)b.pi : (long long)b.pi * b.pj);
+  // the 4-cell stencil along d
+  int o4[4];
+  if (d == 0) { o4[0] = T.off(sk, jj, ii - 1); o4[1] = T.off(sk, jj, ii); o4[2] = T.off(sk, jj, ii + 1); o4[3] = T.off(sk, jj, ii + 2); }
+  else if (d == 1) { o4[0] = T.off(sk, jj - 1, ii); o4[1] = T.off(sk, jj, ii); o4[2] = T.off(sk, jj + 1, ii); o4[3] = T.off(sk, jj + 2, ii); }
+  else { o4[0] = T.off(skm, jj, ii); o4[1] = T.off(sk, jj, ii); o4[2] = T.off(sk1, jj, ii); o4[3] = T.off(sk2, jj, ii); }
   R pm1[MB_NP], p0[MB_NP], pp1[MB_NP], pp2[MB_NP], dlc[4];
 #pragma unroll
   for (int s = 0; s < MB_NP; ++s) {
-    pm1[s] = cvt<R>(ld(P + r0 - st + s * nc));
-    p0[s] = cvt<R>(ld(P + r0 + s * nc));
-    pp1[s] = cvt<R>(ld(P + r0 + st + s * nc));
-    pp2[s] = cvt<R>(ld(P + r0 + 2 * st + s * nc));
+    pm1[s] = T.v(o4[0], s); p0[s] = T.v(o4[1], s); pp1[s] = T.v(o4[2], s); pp2[s] = T.v(o4[3], s);
   }
   const long long l0 = r0 - b.boff;
 #pragma unroll
@@ -55,31 +77,46 @@ MB_HD void face_flux(const Params& p, const DBlk& b, const double* __restrict__ 
   conv_face<R, RS, LIM>(p, pm1, p0, pp1, pp2, dlc, nx, ny, nz, area, out);
   if (!VISC) return;
   // ---- viscous face: cells 1,2 = (c, c+d); 3,4 = c -/+ b-axis; 5,6 = c+d -/+ b; 7,8 = c -/+ c-axis; 9,10 = c+d -/+ c
-  const long long sb = (d == 0) ? (long long)b.pi : 1;
-  const long long sc = (d == 2) ? (long long)b.pi : (long long)b.pi * b.pj;
-  const long long cc[10] = {r0, r0 + st, r0 - sb, r0 + sb, r0 + st - sb, r0 + st + sb,
-                            r0 - sc, r0 + sc, r0 + st - sc, r0 + st + sc};
-  const int ia = d, ib = (d == 0) ? 1 : 0, ic = (d == 2) ? 1 : 2;
-  R rho_n[10], T_n[10];
-#pragma unroll
-  for (int q = 0; q < 10; ++q) cell_rho_T<R>(p, cvt<R>(ld(P + cc[q])), cvt<R>(ld(P + cc[q] + MB_IPR * nc)), rho_n[q], T_n[q]);
-  auto w = [&](int q, int s) -> R { return cvt<R>(ld(P + cc[q] + s * nc)); };
+  int oc[10];
+  oc[0] = o4[1];
+  oc[1] = o4[2];
+  if (d == 0) {
+    oc[2] = T.off(sk, jj - 1, ii); oc[3] = T.off(sk, jj + 1, ii); oc[4] = T.off(sk, jj - 1, ii + 1); oc[5] = T.off(sk, jj + 1, ii + 1);
+    oc[6] = T.off(skm, jj, ii); oc[7] = T.off(sk1, jj, ii); oc[8] = T.off(skm, jj, ii + 1); oc[9] = T.off(sk1, jj, ii + 1);
+  } else if (d == 1) {
+    oc[2] = T.off(sk, jj, ii - 1); oc[3] = T.off(sk, jj, ii + 1); oc[4] = T.off(sk, jj + 1, ii - 1); oc[5] = T.off(sk, jj + 1, ii + 1);
+    oc[6] = T.off(skm, jj, ii); oc[7] = T.off(sk1, jj, ii); oc[8] = T.off(skm, jj + 1, ii); oc[9] = T.off(sk1, jj + 1, ii);
+  } else {
+    oc[2] = T.off(sk, jj, ii - 1); oc[3] = T.off(sk, jj, ii + 1); oc[4] = T.off(sk1, jj, ii - 1); oc[5] = T.off(sk1, jj, ii + 1);
+    oc[6] = T.off(sk, jj - 1, ii); oc[7] = T.off(sk, jj + 1, ii); oc[8] = T.off(sk1, jj - 1, ii); oc[9] = T.off(sk1, jj + 1, ii);
+  }
+  auto w = [&](int q, int s) -> R { return T.v(oc[q], s); };
+  // rho_c = sum(rho_s) = rho_s (one species); T_c from the tile
   R G[MB_NP][3];
-  R irho1 = (R)1 / rho_n[0], irho2 = (R)1 / rho_n[1];
-  G[0][ia] = w(1, 0) * irho2 - w(0, 0) * irho1;
-  G[MB_IPR][ia] = T_n[1] - T_n[0];
+  {
+    R irho1 = (R)1 / w(0, 0), irho2 = (R)1 / w(1, 0);
+    R irt1 = (R)1 / w(2, 0), irt2 = (R)1 / w(3, 0), irt3 = (R)1 / w(4, 0), irt4 = (R)1 / w(5, 0);
+    R jrt1 = (R)1 / w(6, 0), jrt2 = (R)1 / w(7, 0), jrt3 = (R)1 / w(8, 0), jrt4 = (R)1 / w(9, 0);
+    R ga[MB_NP], gb[MB_NP], gc[MB_NP];
+    ga[0] = w(1, 0) * irho2 - w(0, 0) * irho1;
+    ga[MB_IPR] = w(1, 5) - w(0, 5);
+    gb[0] = (w(3, 0) * irt2 - w(2, 0) * irt1 + w(5, 0) * irt4 - w(4, 0) * irt3) * (R)0.25;
+    gb[MB_IPR] = (w(3, 5) - w(2, 5) + w(5, 5) - w(4, 5)) * (R)0.25;
+    gc[0] = (w(7, 0) * jrt2 - w(6, 0) * jrt1 + w(9, 0) * jrt4 - w(8, 0) * jrt3) * (R)0.25;
+    gc[MB_IPR] = (w(7, 5) - w(6, 5) + w(9, 5) - w(8, 5)) * (R)0.25;
 #pragma unroll
-  for (int s = MB_IU; s <= MB_IW; ++s) G[s][ia] = w(1, s) - w(0, s);
-  R irt1 = (R)1 / rho_n[2], irt2 = (R)1 / rho_n[3], irt3 = (R)1 / rho_n[4], irt4 = (R)1 / rho_n[5];
-  G[0][ib] = (w(3, 0) * irt2 - w(2, 0) * irt1 + w(5, 0) * irt4 - w(4, 0) * irt3) * (R)0.25;
-  G[MB_IPR][ib] = (T_n[3] - T_n[2] + T_n[5] - T_n[4]) * (R)0.25;
+    for (int s = MB_IU; s <= MB_IW; ++s) {
+      ga[s] = w(1, s) - w(0, s);
+      gb[s] = (w(3, s) - w(2, s) + w(5, s) - w(4, s)) * (R)0.25;
+      gc[s] = (w(7, s) - w(6, s) + w(9, s) - w(8, s)) * (R)0.25;
+    }
 #pragma unroll
-  for (int s = MB_IU; s <= MB_IW; ++s) G[s][ib] = (w(3, s) - w(2, s) + w(5, s) - w(4, s)) * (R)0.25;
-  irt1 = (R)1 / rho_n[6]; irt2 = (R)1 / rho_n[7]; irt3 = (R)1 / rho_n[8]; irt4 = (R)1 / rho_n[9];
-  G[0][ic] = (w(7, 0) * irt2 - w(6, 0) * irt1 + w(9, 0) * irt4 - w(8, 0) * irt3) * (R)0.25;
-  G[MB_IPR][ic] = (T_n[7] - T_n[6] + T_n[9] - T_n[8]) * (R)0.25;
-#pragma unroll
-  for (int s = MB_IU; s <= MB_IW; ++s) G[s][ic] = (w(7, s) - w(6, s) + w(9, s) - w(8, s)) * (R)0.25;
+    for (int s = 0; s < MB_NP; ++s) {
+      G[s][0] = (d == 0) ? ga[s] : gb[s];
+      G[s][1] = (d == 0) ? gb[s] : (d == 1 ? ga[s] : gc[s]);
+      G[s][2] = (d == 2) ? ga[s] : gc[s];
+    }
+  }
   R Mav[3][3];
   const double* m1 = b.m + 9 * l0;
   const double* m2 = b.m + 9 * (l0 + st);
@@ -447,6 +484,30 @@ __device__ __forceinline__ void report_bad_state(const Params& p, int blk, int i
 }
 
 // ---------------------------------------------------------------------------------------------
+// Stage plane kk of the tile window: cells (i0-2 .. i0+33) x (j0-2 .. j0+TY+1), those inside the padded block.
+template <typename R, int TY>
+__device__ __forceinline__ void stage_plane(const Params& p, const DBlk& b, const double* __restrict__ P,
+                                            const Tile<R, TY>& T, int i0, int j0, int kk) {
+  const int sl = slot_of(kk);
+  const long long nc = p.nc;
+  for (int c = threadIdx.x; c < TXH * (TY + 4); c += blockDim.x) {
+    const int jj = c / TXH, ii = c - jj * TXH;
+    const int i = i0 - 2 + ii, j = j0 - 2 + jj;
+    R vals[NV] = {(R)0, (R)0, (R)0, (R)0, (R)0, (R)0};
+    if (i >= 1 - GC && i <= b.n1 + GC && j >= 1 - GC && j <= b.n2 + GC) {
+      const long long r = row(b, i, j, kk);
+#pragma unroll
+      for (int s = 0; s < MB_NP; ++s) vals[s] = cvt<R>(ld(P + r + s * nc));
+      R rho, Tc;
+      cell_rho_T<R>(p, vals[0], vals[MB_IPR], rho, Tc);
+      vals[5] = Tc;
+    }
+    const int o = T.off(sl, jj, ii);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) T.base[o + v * Tile<R, TY>::VS] = vals[v];
+  }
+}
+
 // MINB: resident CTAs per SM the register allocation must allow (launch bounds)
 template <typename R, int TY, bool VISC, int MODE, int RS, int LIM, int MINB>
 __global__ void __launch_bounds__(32 * TY, MINB)
@@ -456,9 +517,12 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
   extern __shared__ __align__(16) unsigned char smem_raw[];
   typedef R RowI[33][NF];
   typedef R RowJ[32][NF];
-  RowI* sFi = reinterpret_cast<RowI*>(smem_raw);                         // [TY][33][NF]
-  RowJ* sFj = reinterpret_cast<RowJ*>(smem_raw + sizeof(R) * TY * 33 * NF); // [TY+1][32][NF]
-  RowJ* sFk0 = reinterpret_cast<RowJ*>(smem_raw + sizeof(R) * (TY * 33 + (TY + 1) * 32) * NF);  // [2][TY][32][NF]
+  Tile<R, TY> T;
+  T.base = reinterpret_cast<R*>(smem_raw);                                       // [4][NV][TY+4][36]
+  unsigned char* fbase = smem_raw + sizeof(R) * 4 * NV * (TY + 4) * TXH;
+  RowI* sFi = reinterpret_cast<RowI*>(fbase);                                     // [TY][33][NF]
+  RowJ* sFj = reinterpret_cast<RowJ*>(fbase + sizeof(R) * TY * 33 * NF);          // [TY+1][32][NF]
+  RowJ* sFk0 = reinterpret_cast<RowJ*>(fbase + sizeof(R) * (TY * 33 + (TY + 1) * 32) * NF);  // [2][TY][32][NF]
   __shared__ double sred[32];
   const DTile t = tiles[blockIdx.x];
   const DBlk b = p.blk[t.blk];
@@ -469,45 +533,55 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
   const double dt = (MODE == MODE_UPDATE) ? p.st->dt : 0.0;
   double dtloc = 1e300;
   int kb = 0;  // buffer of the k-face above the current plane
+  // prologue: planes k0-2 .. k0+1, and the k-face below the first plane
+  for (int kk = t.k0 - 2; kk <= t.k0 + 1; ++kk)
+    if (kk >= 1 - GC && kk <= b.n3 + GC) stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, kk);
+  __syncthreads();
+  if (own && t.k0 > 1) {
+    R out[NF];
+    face_flux<R, TY, VISC, RS, LIM>(p, b, T, 2, i, j, t.k0 - 1, tx + 2, ty + 2, out);
+    R* dst = &sFk0[(kb ^ 1) * TY + ty][tx][0];
+#pragma unroll
+    for (int q = 0; q < NF; ++q) dst[q] = out[q];
+  }
   for (int k = t.k0; k < t.k1; ++k) {
-    // ---- face tasks: i-faces, j-faces, k-faces of this plane, one call site
-    // task list of this thread: 0 = i-face #tid, 1 = extra i-face (last warp, lanes < TY),
-    // 2 = j-face #tid, 3 = extra j-face row (warp 0), 4 = k-face below the first plane, 5 = k-face above
+    __syncthreads();  // the slot of plane k-2 is free
+    if (k + 2 <= b.n3 + GC) stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, k + 2);
+    __syncthreads();
+    // ---- face tasks of this plane through one call site: 0 = i-face #tid, 1 = extra i-faces (last warp,
+    // lanes < TY), 2 = j-face #tid, 3 = extra j-face row (warp 0), 4 = the k-face above
 #pragma unroll 1
-    for (int task = 0; task < 6; ++task) {
-      int d = -1, fi = 0, fj = 0, fk = k;
+    for (int task = 0; task < 5; ++task) {
+      int d = -1, fi = 0, fj = 0, ii = 0, jj = 0;
       R* dst = nullptr;
       if (task == 0 || task == 1) {
         int f;
         if (task == 0) f = tid;
         else { if (ty != TY - 1 || tx >= TY) continue; f = 32 * TY + tx; }
         const int rw = f / 33, cl = f - rw * 33;
-        fi = t.i0 + cl - 1; fj = t.j0 + rw;
+        fi = t.i0 + cl - 1; fj = t.j0 + rw; ii = cl + 1; jj = rw + 2;
         if (fi >= 1 && fi <= b.n1 - 1 && fj <= b.n2) { d = 0; dst = &sFi[rw][cl][0]; }
       } else if (task == 2 || task == 3) {
         int f;
         if (task == 2) f = tid;
         else { if (ty != 0) continue; f = 32 * TY + tx; }
         const int rw = f >> 5, cl = f & 31;
-        fi = t.i0 + cl; fj = t.j0 + rw - 1;
+        fi = t.i0 + cl; fj = t.j0 + rw - 1; ii = cl + 2; jj = rw + 1;
         if (fj >= 1 && fj <= b.n2 - 1 && fi <= b.n1) { d = 1; dst = &sFj[rw][cl][0]; }
-      } else if (task == 4) {
-        if (k != t.k0 || !own || k <= 1) continue;
-        fi = i; fj = j; fk = k - 1; d = 2; dst = &sFk0[(kb ^ 1) * TY + ty][tx][0];
       } else {
         if (!own || k >= b.n3) continue;
-        fi = i; fj = j; fk = k; d = 2; dst = &sFk0[kb * TY + ty][tx][0];
+        fi = i; fj = j; ii = tx + 2; jj = ty + 2; d = 2; dst = &sFk0[kb * TY + ty][tx][0];
       }
       if (d < 0) continue;
       R out[NF];
-      face_flux<R, VISC, RS, LIM>(p, b, Pin, d, fi, fj, fk, out);
+      face_flux<R, TY, VISC, RS, LIM>(p, b, T, d, fi, fj, k, ii, jj, out);
 #pragma unroll
       for (int q = 0; q < NF; ++q) dst[q] = out[q];
     }
     __syncthreads();
     if (own) {
       // ---- pass 2 (pass2_body.inc): convective i +,-, j +,-, k +,-, then viscous i -,+, j -,+, k -,+
-      double acc[MB_NP] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      double acc[MB_NP];
       const R* fr = (i < b.n1) ? &sFi[ty][tx + 1][0] : nullptr;
       const R* fl = (i > 1) ? &sFi[ty][tx][0] : nullptr;
       const R* gr = (j < b.n2) ? &sFj[ty + 1][tx][0] : nullptr;
@@ -544,15 +618,15 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
         double pc[MB_NP], po[MB_NP], pn[MB_NP];
 #pragma unroll
         for (int s = 0; s < MB_NP; ++s) { pc[s] = ld(Pin + r + s * p.nc); po[s] = Pold[r + s * p.nc]; }
-        double rho, T;
-        cell_rho_T(p, pc[0], pc[MB_IPR], rho, T);
-        if (p.guard && !(T > 1.0 && T < 9990.0)) {  // thermo guard (Mod_Thermo_Cache.f90:317-327)
+        double rho, Tc;
+        cell_rho_T(p, pc[0], pc[MB_IPR], rho, Tc);
+        if (p.guard && !(Tc > 1.0 && Tc < 9990.0)) {  // thermo guard (Mod_Thermo_Cache.f90:317-327)
           atomicAdd(&p.st->n_bad_thermo, 1);
-          if (T != T) T = 300.0;
-          T = mn(mx(T, 1.0), 9990.0);
+          if (Tc != Tc) Tc = 300.0;
+          Tc = mn(mx(Tc, 1.0), 9990.0);
         }
         const double vol = ld(b.vol + (r - b.boff));
-        cons_update(p, pc, po, acc, vol, dt, rkc, T, pn);
+        cons_update(p, pc, po, acc, vol, dt, rkc, Tc, pn);
         bool bad = !(pn[MB_IPR] >= 0.0);
 #pragma unroll
         for (int s = 0; s < MB_NP; ++s) bad = bad || !isfinite(pn[s]);
@@ -562,7 +636,6 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
         if (last) dtloc = mn(dtloc, cell_dt(p, b, r - b.boff, pn));
       }
     }
-    __syncthreads();
     kb ^= 1;
   }
   if (MODE == MODE_UPDATE && last) cta_min_dt(p, dtloc, sred);
@@ -570,7 +643,8 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
 
 template <typename R, int TY, bool VISC>
 constexpr size_t sweep_smem() {
-  return sizeof(R) * (size_t)(TY * 33 + (TY + 1) * 32 + 2 * TY * 32) * (VISC ? 2 * MB_NP : MB_NP);
+  return sizeof(R) * ((size_t)4 * NV * (TY + 4) * TXH +
+                      (size_t)(TY * 33 + (TY + 1) * 32 + 2 * TY * 32) * (VISC ? 2 * MB_NP : MB_NP));
 }
 
 }  // namespace mb
