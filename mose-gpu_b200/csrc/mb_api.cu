@@ -36,6 +36,7 @@ struct mb_ctx {
   DTile* d_tiles_aux = nullptr;
   int ntiles_aux = 0;
   double* d_scratch = nullptr;  // the engine's own stage buffer (ncell x 5)
+  std::vector<void*> geo32;     // FP32 geometry copies of the mixed form
   long long ncell = 0;
   std::vector<int> blk_n;       // 3 per block
   bool dt_valid = false;
@@ -73,6 +74,8 @@ static void free_ctx(mb_ctx* c) {
   void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
                   c->d_pgsrc, c->d_pg, c->d_tab, c->d_tabf, c->d_st, c->d_tiles_sweep, c->d_tiles_aux, c->d_scratch};
   for (void* q : ptrs)
+    if (q) cudaFree(q);
+  for (void* q : c->geo32)
     if (q) cudaFree(q);
   delete c;
 }
@@ -227,6 +230,24 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   c->ty_sweep = sc->precision == MB_PREC_MIXED ? TY_F32 : TY_F64;
   std::vector<DTile> ts = make_tiles(mesh, c->ty_sweep, 16);
   std::vector<DTile> ta = make_tiles(mesh, TY_AUX, 16);
+  // the mixed form reads its geometry in FP32: one conversion here instead of one per face per stage
+  if (sc->precision == MB_PREC_MIXED) {
+    for (auto& d : hb) {
+      const long long pk = d.n3 + 2 * MB_GC;
+      const long long npad = (long long)d.pi * d.pj * pk;
+      const long long n[5] = {4LL * (d.n1 + 1) * d.n2 * d.n3, 4LL * d.n1 * (d.n2 + 1) * d.n3, 4LL * d.n1 * d.n2 * (d.n3 + 1),
+                              3 * npad, 9 * npad};
+      const double* src[5] = {d.fm1, d.fm2, d.fm3, d.dl, d.m};
+      float* dst[5];
+      for (int q = 0; q < 5; ++q) {
+        if (cudaMalloc((void**)&dst[q], n[q] * sizeof(float)) != cudaSuccess) { free_ctx(c); return MB_E_NOMEM; }
+        c->geo32.push_back(dst[q]);
+        if (to_float(src[q], dst[q], n[q], 0) != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+      }
+      d.fm1f = dst[0]; d.fm2f = dst[1]; d.fm3f = dst[2]; d.dlf = dst[3]; d.mf = dst[4];
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+  }
   TRY(upload(&c->d_blk, hb.data(), hb.size()));
   TRY(upload(&c->d_recmap, recmap.data(), recmap.size()));
   TRY(upload(&c->d_rec, hr.data(), hr.size()));
@@ -262,6 +283,14 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
                         ? (sc->riemann == 1 ? sweep_f32_rs1_setup() : sc->riemann == 4 ? sweep_f32_rs4_setup() : sweep_f32_rs12_setup())
                         : (sc->riemann == 1 ? sweep_f64_rs1_setup() : sc->riemann == 4 ? sweep_f64_rs4_setup() : sweep_f64_rs12_setup());
     if (e != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+    if (getenv("MB_REPORT")) {
+      const int v = sc->visc ? 1 : 0;
+      int occ = (sc->precision == MB_PREC_MIXED)
+                    ? (sc->riemann == 1 ? sweep_f32_rs1_occupancy(v) : sc->riemann == 4 ? sweep_f32_rs4_occupancy(v) : sweep_f32_rs12_occupancy(v))
+                    : (sc->riemann == 1 ? sweep_f64_rs1_occupancy(v) : sc->riemann == 4 ? sweep_f64_rs4_occupancy(v) : sweep_f64_rs12_occupancy(v));
+      fprintf(stderr, "[mose_b200] sweep: %s, %d threads per CTA, %d CTAs per SM, %d tiles\n",
+              sc->precision == MB_PREC_MIXED ? "mixed" : "fp64", 32 * c->ty_sweep, occ, (int)ts.size());
+    }
   }
   // ---- kernel parameters
   Params& p = c->p;

@@ -70,10 +70,11 @@ MB_HD void face_flux(const Params& p, const DBlk& b, const Tile<R, TY>& T, int d
     pm1[s] = T.v(o4[0], s); p0[s] = T.v(o4[1], s); pp1[s] = T.v(o4[2], s); pp2[s] = T.v(o4[3], s);
   }
   const long long l0 = r0 - b.boff;
+  const auto* gdl = Geo<R>::dl(b);
 #pragma unroll
-  for (int q = 0; q < 4; ++q) dlc[q] = cvt<R>(ld(b.dl + d + 3 * (l0 + (q - 1) * st)));
-  const double* f = fmp(b, d, i, j, k);
-  R nx = cvt<R>(ld(f)), ny = cvt<R>(ld(f + 1)), nz = cvt<R>(ld(f + 2)), area = cvt<R>(ld(f + 3));
+  for (int q = 0; q < 4; ++q) dlc[q] = (R)ld(gdl + d + 3 * (l0 + (q - 1) * st));
+  const auto* f = Geo<R>::fm(b, d) + fmi(b, d, i, j, k);
+  R nx = (R)ld(f), ny = (R)ld(f + 1), nz = (R)ld(f + 2), area = (R)ld(f + 3);
   conv_face<R, RS, LIM>(p, pm1, p0, pp1, pp2, dlc, nx, ny, nz, area, out);
   if (!VISC) return;
   // ---- viscous face: cells 1,2 = (c, c+d); 3,4 = c -/+ b-axis; 5,6 = c+d -/+ b; 7,8 = c -/+ c-axis; 9,10 = c+d -/+ c
@@ -118,12 +119,12 @@ MB_HD void face_flux(const Params& p, const DBlk& b, const Tile<R, TY>& T, int d
     }
   }
   R Mav[3][3];
-  const double* m1 = b.m + 9 * l0;
-  const double* m2 = b.m + 9 * (l0 + st);
+  const auto* m1 = Geo<R>::m(b) + 9 * l0;
+  const auto* m2 = Geo<R>::m(b) + 9 * (l0 + st);
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
-    for (int q = 0; q < 3; ++q) Mav[a][q] = (R)0.5 * (cvt<R>(ld(m1 + a + 3 * q)) + cvt<R>(ld(m2 + a + 3 * q)));
+    for (int q = 0; q < 3; ++q) Mav[a][q] = (R)0.5 * ((R)ld(m1 + a + 3 * q) + (R)ld(m2 + a + 3 * q));
 #pragma unroll
   for (int iv = 0; iv < MB_NP; ++iv) {
     R g1 = G[iv][0], g2 = G[iv][1], g3 = G[iv][2];
@@ -588,24 +589,26 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
       const R* gl = (j > 1) ? &sFj[ty][tx][0] : nullptr;
       const R* hr = (k < b.n3) ? &sFk0[kb * TY + ty][tx][0] : nullptr;
       const R* hl = (k > 1) ? &sFk0[(kb ^ 1) * TY + ty][tx][0] : nullptr;
+      // the sum runs in the flux type (the FP64 form: FP64 as the reference; the mixed form: the twelve FP32
+      // face fluxes summed in FP32 and converted once), the boundary records and the update in FP64
 #pragma unroll
       for (int s = 0; s < MB_NP; ++s) {
-        double a = 0.0;
-        if (fr) a = a + (double)fr[s];
-        if (fl) a = a - (double)fl[s];
-        if (gr) a = a + (double)gr[s];
-        if (gl) a = a - (double)gl[s];
-        if (hr) a = a + (double)hr[s];
-        if (hl) a = a - (double)hl[s];
+        R a = (R)0;
+        if (fr) a = a + fr[s];
+        if (fl) a = a - fl[s];
+        if (gr) a = a + gr[s];
+        if (gl) a = a - gl[s];
+        if (hr) a = a + hr[s];
+        if (hl) a = a - hl[s];
         if (VISC) {
-          if (fr) a = a - (double)fr[MB_NP + s];
-          if (fl) a = a + (double)fl[MB_NP + s];
-          if (gr) a = a - (double)gr[MB_NP + s];
-          if (gl) a = a + (double)gl[MB_NP + s];
-          if (hr) a = a - (double)hr[MB_NP + s];
-          if (hl) a = a + (double)hl[MB_NP + s];
+          if (fr) a = a - fr[MB_NP + s];
+          if (fl) a = a + fl[MB_NP + s];
+          if (gr) a = a - gr[MB_NP + s];
+          if (gl) a = a + gl[MB_NP + s];
+          if (hr) a = a - hr[MB_NP + s];
+          if (hl) a = a + hl[MB_NP + s];
         }
-        acc[s] = a;
+        acc[s] = (double)a;
       }
       // ---- boundary records of the cell, face order 1..6
       if (i == 1 || i == b.n1 || j == 1 || j == b.n2 || k == 1 || k == b.n3)

@@ -114,6 +114,16 @@ __global__ void __launch_bounds__(32 * TY_AUX) k_update(Params p, const DTile* _
   }
 }
 
+__global__ void k_to_float(const double* __restrict__ src, float* __restrict__ dst, long long n) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    dst[q] = (float)src[q];
+}
+
+cudaError_t to_float(const double* src, float* dst, long long n, cudaStream_t s) {
+  k_to_float<<<1184, 256, 0, s>>>(src, dst, n);
+  return cudaGetLastError();
+}
+
 __global__ void k_reset_dt(Params p) { p.st->dtmin_bits = (unsigned long long)__double_as_longlong(1e300); }
 
 // the step's dt (Compute_dt's dtglobal = 1e5 then the cell minimum, Mod_Explicit.f90:122; Set_Global_dt;

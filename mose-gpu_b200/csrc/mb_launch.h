@@ -39,7 +39,8 @@ constexpr int TY_AUX = 8;    // tile rows of the per-cell kernels (dt, update)
 #define MB_DECLARE_SWEEP(name)                                                                                    \
   cudaError_t name(const Params& p, const DTile* tiles, int ntiles, int mode, const double* Pin, const double* Pold, \
                    double* Pout, double* Rout, double rkc, int last, cudaStream_t s);                              \
-  cudaError_t name##_setup();
+  cudaError_t name##_setup();                                                                                    \
+  int name##_occupancy(int visc);
 MB_DECLARE_SWEEP(sweep_f64_rs1)
 MB_DECLARE_SWEEP(sweep_f64_rs4)
 MB_DECLARE_SWEEP(sweep_f64_rs12)
@@ -53,6 +54,7 @@ cudaError_t dt_cells(const Params& p, const DTile* tiles, int ntiles, const doub
 cudaError_t update_cells(const Params& p, const DTile* tiles, int ntiles, double* P, const double* PO,
                          const double* R, double rkc, double dt, cudaStream_t s);
 cudaError_t reset_dt(const Params& p, cudaStream_t s);
+cudaError_t to_float(const double* src, float* dst, long long n, cudaStream_t s);
 cudaError_t clock_step(const Params& p, int time_clip, double threshold, cudaStream_t s);
 
 }  // namespace mb

@@ -39,6 +39,21 @@ struct DBlk {
   int rmap[6];          // offset of each face's record map in Params::rec_map (-1: none)
   long long boff;
   const double *fm1, *fm2, *fm3, *dl, *m, *vol;
+  // FP32 copies of the face and cell geometry, made once by mb_init for the mixed form (null otherwise)
+  const float *fm1f, *fm2f, *fm3f, *dlf, *mf;
+};
+
+// the geometry arrays in the flux arithmetic type
+template <typename R> struct Geo;
+template <> struct Geo<double> {
+  MB_HD static const double* fm(const DBlk& b, int d) { return d == 0 ? b.fm1 : (d == 1 ? b.fm2 : b.fm3); }
+  MB_HD static const double* dl(const DBlk& b) { return b.dl; }
+  MB_HD static const double* m(const DBlk& b) { return b.m; }
+};
+template <> struct Geo<float> {
+  MB_HD static const float* fm(const DBlk& b, int d) { return d == 0 ? b.fm1f : (d == 1 ? b.fm2f : b.fm3f); }
+  MB_HD static const float* dl(const DBlk& b) { return b.dlf; }
+  MB_HD static const float* m(const DBlk& b) { return b.mf; }
 };
 
 struct DRec {
@@ -110,7 +125,20 @@ MB_HD const double* fm3p(const DBlk& b, int i, int j, int k) {
 MB_HD const double* fmp(const DBlk& b, int d, int i, int j, int k) {
   return d == 0 ? fm1p(b, i, j, k) : (d == 1 ? fm2p(b, i, j, k) : fm3p(b, i, j, k));
 }
+// index (in values) of the face (i,j,k) of direction d in its fm array
+MB_HD long long fmi(const DBlk& b, int d, int i, int j, int k) {
+  if (d == 0) return 4 * ((long long)i + (long long)(b.n1 + 1) * ((j - 1) + (long long)b.n2 * (k - 1)));
+  if (d == 1) return 4 * ((long long)(i - 1) + (long long)b.n1 * (j + (long long)(b.n2 + 1) * (k - 1)));
+  return 4 * ((long long)(i - 1) + (long long)b.n1 * ((j - 1) + (long long)b.n2 * k));
+}
 MB_HD double ld(const double* p) {
+#ifdef __CUDA_ARCH__
+  return __ldg(p);
+#else
+  return *p;
+#endif
+}
+MB_HD float ld(const float* p) {
 #ifdef __CUDA_ARCH__
   return __ldg(p);
 #else
