@@ -95,15 +95,19 @@ MB_HD void face_flux(const Params& p, const DBlk& b, const Tile<R, TY>& T, int d
   // rho_c = sum(rho_s) = rho_s (one species); T_c from the tile
   R G[MB_NP][3];
   {
-    R irho1 = (R)1 / w(0, 0), irho2 = (R)1 / w(1, 0);
-    R irt1 = (R)1 / w(2, 0), irt2 = (R)1 / w(3, 0), irt3 = (R)1 / w(4, 0), irt4 = (R)1 / w(5, 0);
-    R jrt1 = (R)1 / w(6, 0), jrt2 = (R)1 / w(7, 0), jrt3 = (R)1 / w(8, 0), jrt4 = (R)1 / w(9, 0);
     R ga[MB_NP], gb[MB_NP], gc[MB_NP];
-    ga[0] = w(1, 0) * irho2 - w(0, 0) * irho1;
+    if (Fast<R>::on) {  // one species: the mass-fraction gradient is zero
+      ga[0] = gb[0] = gc[0] = (R)0;
+    } else {
+      R irho1 = (R)1 / w(0, 0), irho2 = (R)1 / w(1, 0);
+      R irt1 = (R)1 / w(2, 0), irt2 = (R)1 / w(3, 0), irt3 = (R)1 / w(4, 0), irt4 = (R)1 / w(5, 0);
+      R jrt1 = (R)1 / w(6, 0), jrt2 = (R)1 / w(7, 0), jrt3 = (R)1 / w(8, 0), jrt4 = (R)1 / w(9, 0);
+      ga[0] = w(1, 0) * irho2 - w(0, 0) * irho1;
+      gb[0] = (w(3, 0) * irt2 - w(2, 0) * irt1 + w(5, 0) * irt4 - w(4, 0) * irt3) * (R)0.25;
+      gc[0] = (w(7, 0) * jrt2 - w(6, 0) * jrt1 + w(9, 0) * jrt4 - w(8, 0) * jrt3) * (R)0.25;
+    }
     ga[MB_IPR] = w(1, 5) - w(0, 5);
-    gb[0] = (w(3, 0) * irt2 - w(2, 0) * irt1 + w(5, 0) * irt4 - w(4, 0) * irt3) * (R)0.25;
     gb[MB_IPR] = (w(3, 5) - w(2, 5) + w(5, 5) - w(4, 5)) * (R)0.25;
-    gc[0] = (w(7, 0) * jrt2 - w(6, 0) * jrt1 + w(9, 0) * jrt4 - w(8, 0) * jrt3) * (R)0.25;
     gc[MB_IPR] = (w(7, 5) - w(6, 5) + w(9, 5) - w(8, 5)) * (R)0.25;
 #pragma unroll
     for (int s = MB_IU; s <= MB_IW; ++s) {

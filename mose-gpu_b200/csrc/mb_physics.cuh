@@ -90,6 +90,12 @@ struct Params {
   double cfl, vnn, prandtl, schmidt, mco;
 };
 
+// The mixed form (R = float) applies the single-species identities of the reference's mixture formulas
+// exactly: rho = rho_s, Y = rho_s / rho = 1, R_mix = Ri, cp_mix = cp(T), h_mix = h(T), the Wilke mixture
+// viscosity / conductivity = the table values, and a zero species-diffusion flux. The FP64 form keeps the
+// literal statements (their rounding is what the parity gate compares).
+template <typename R> struct Fast { static constexpr bool on = sizeof(R) == 4; };
+
 template <typename R> struct Tab;
 template <> struct Tab<double> {
   MB_HD static const double* cp(const Params& p) { return p.cp; }
@@ -171,12 +177,14 @@ MB_HD R tabT(const R* t, int ti, R td) {
 // ---- FLINT leaves (Lib_ThermoTransport_dev.f90) ----
 template <typename R>
 MB_HD void rotot_rtot(const Params& p, R rhoi, R& rho, R& Rg) {
+  if (Fast<R>::on) { rho = rhoi; Rg = (R)p.ri; return; }
   rho = (R)0 + rhoi;
   Rg = (R)0 + (R)p.ri * rhoi / rho;
 }
 template <typename R>
 MB_HD R f_cp(const Params& p, R rhoi, int ti, R td, R rho) {
   R cpi = tabT(Tab<R>::cp(p), ti, td);
+  if (Fast<R>::on) return cpi;
   return (R)0 + rhoi / rho * cpi;
 }
 template <typename R>
@@ -190,17 +198,18 @@ MB_HD R f_ss(const Params& p, R rhoi, R pr, R rho, R Rtot) {
 }
 template <typename R>
 MB_HD R H0(const Params& p, R pr, R rhoi, R u) {
-  R rho = (R)0 + rhoi;
-  R Rg = (R)0 + (R)p.ri * rhoi / rho;
+  R rho, Rg;
+  rotot_rtot(p, rhoi, rho, Rg);
   R T = pr / (Rg * rho);
   int ti = tidx(p, T);
   R td = T - (R)ti;
-  R e = (R)0 + tabT(Tab<R>::h(p), ti, td) * rhoi / rho;
+  R e = Fast<R>::on ? tabT(Tab<R>::h(p), ti, td) : (R)0 + tabT(Tab<R>::h(p), ti, td) * rhoi / rho;
   return e + (R)0.5 * u * u;
 }
 // f_molecularWeight + co_fiij_dev + co_k_mi_lam_Wilke_dev, one species
 template <typename R>
 MB_HD void wilke(const Params& p, R rhoi, R rho, int ti, R td, R& mil, R& kl) {
+  if (Fast<R>::on) { mil = tabT(Tab<R>::mu(p), ti, td); kl = tabT(Tab<R>::k(p), ti, td); return; }
   const R wm = (R)p.wm;
   R rho_ = (R)0 + rhoi;
   R wmt = (R)0 + (rhoi / rho_ / wm);
@@ -264,8 +273,8 @@ MB_HD R rlimiter(int lim, R x, R y) {
 // ---- MOSE_open solvers of riemann_open_body.inc: AUSM+ (4), LMRoe (12) ----
 template <typename R>
 MB_HD R h_static(const Params& p, R rhoi, R pr) {
-  R rho_ = (R)0 + rhoi;
-  R rg = (R)0 + (R)p.ri * rhoi / rho_;
+  R rho_, rg;
+  rotot_rtot(p, rhoi, rho_, rg);
   R T = pr / (rg * rho_);
   R Tc = mx((R)p.tmin, mn(T, (R)(p.tmax - 1)));
   if (Tc != Tc) Tc = (R)p.tmin;
@@ -275,6 +284,7 @@ MB_HD R h_static(const Params& p, R rhoi, R pr) {
   int t2 = max(p.tmin, min(ti + 1, p.tmax));
   const R* h = Tab<R>::h(p);
   R hs = h[t1] + (h[t2] - h[t1]) * td;
+  if (Fast<R>::on) return hs;
   return (R)0 + hs * rhoi / rho_;
 }
 
@@ -320,10 +330,9 @@ MB_HD void riemann_open(const Params& p, int rs, R dl, R ul, R vl, R wl, R pl, R
   }
   const R* H = Tab<R>::h(p);
   const R* CP = Tab<R>::cp(p);
-  R rho_ = (R)0 + dl;
-  R Rl = (R)0 + (R)p.ri * dl / rho_;
-  rho_ = (R)0 + dr;
-  R Rr = (R)0 + (R)p.ri * dr / rho_;
+  R rho_, Rl, Rr;
+  rotot_rtot(p, dl, rho_, Rl);
+  rotot_rtot(p, dr, rho_, Rr);
   R inv_dltot = (R)1 / dltot, inv_drtot = (R)1 / drtot;
   R Tl = pl * inv_dltot / Rl, Tr = pr * inv_drtot / Rr;
   int Til = tidx(p, Tl);
@@ -343,12 +352,19 @@ MB_HD void riemann_open(const Params& p, int rs, R dl, R ul, R vl, R wl, R pl, R
     R hl = H[Til] + (H[Til + 1] - H[Til]) * dTl;
     R hr = H[Tir] + (H[Tir + 1] - H[Tir]) * dTr;
     R el = hl - invW * Tl, er = hr - invW * Tr;
+    if (Fast<R>::on) {  // one species: Y = 1, d_roe = 1
+      h0l = hl;
+      h0r = hr;
+      cv_roe = (R)0.5 * (CP[Til] + (CP[Til + 1] - CP[Til]) * dTl + CP[Tir] + (CP[Tir + 1] - CP[Tir]) * dTr) - invW;
+      sum_ei = (srR * er + srL * el) * inv_sr;
+    } else {
     h0l = h0l + hl * dl * inv_dltot;
     h0r = h0r + hr * dr * inv_drtot;
     R d_roe = (srR * dr * inv_drtot + srL * dl * inv_dltot) * inv_sr;
     cv_roe = cv_roe + d_roe * ((R)0.5 * (CP[Til] + (CP[Til + 1] - CP[Til]) * dTl + CP[Tir] +
                                          (CP[Tir + 1] - CP[Tir]) * dTr) - invW);
     sum_ei = sum_ei + d_roe * (srR * er + srL * el) * inv_sr;
+    }
   }
   h0l = h0l + (R)0.5 * (ul * ul + vl * vl + wl * wl);
   h0r = h0r + (R)0.5 * (ur * ur + vr * vr + wr * wr);
@@ -436,12 +452,19 @@ MB_HD void hllc(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R 
     R hl = H[Til] + (H[Til + 1] - H[Til]) * dTl;
     R hr = H[Tir] + (H[Tir + 1] - H[Tir]) * dTr;
     R el = hl - invW * Tl, er = hr - invW * Tr;
+    if (Fast<R>::on) {  // one species: Y = 1, d_roe = 1
+      h0l = hl;
+      h0r = hr;
+      cv_roe = (R)0.5 * (CP[Til] + (CP[Til + 1] - CP[Til]) * dTl + CP[Tir] + (CP[Tir + 1] - CP[Tir]) * dTr) - invW;
+      sum_ei = (srR * er + srL * el) * inv_sr;
+    } else {
     h0l = h0l + hl * dl * inv_dltot;
     h0r = h0r + hr * dr * inv_drtot;
     R d_roe = (srR * dr * inv_drtot + srL * dl * inv_dltot) * inv_sr;
     cv_roe = cv_roe + d_roe * ((R)0.5 * (CP[Til] + (CP[Til + 1] - CP[Til]) * dTl + CP[Tir] +
                                          (CP[Tir + 1] - CP[Tir]) * dTr) - invW);
     sum_ei = sum_ei + d_roe * (srR * er + srL * el) * inv_sr;
+    }
   }
   h0l = h0l + (R)0.5 * (ul * ul + vl * vl + wl * wl);
   h0r = h0r + (R)0.5 * (ur * ur + vr * vr + wr * wr);
@@ -507,21 +530,22 @@ MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, c
   }
   P1[0] = mx(P1[0], (R)1e-20);
   P4[0] = mx(P4[0], (R)1e-20);
-  R rotot1 = (R)0 + P1[0];
-  R Rtot1 = (R)0 + (R)p.ri * P1[0] / rotot1;
-  R rotot4 = (R)0 + P4[0];
-  R Rtot4 = (R)0 + (R)p.ri * P4[0] / rotot4;
+  R rotot1, Rtot1, rotot4, Rtot4;
+  rotot_rtot(p, P1[0], rotot1, Rtot1);
+  rotot_rtot(p, P4[0], rotot4, Rtot4);
   const R* CP = Tab<R>::cp(p);
   R T1d = P1[MB_IPR] / (Rtot1 * rotot1);
   int Ti1 = tidx(p, T1d);
   R Tdiffd = T1d - (R)Ti1;
-  R cpd = (R)0 + P1[0] / rotot1 * (CP[Ti1] + (CP[Ti1 + 1] - CP[Ti1]) * Tdiffd);
+  R cpd = Fast<R>::on ? CP[Ti1] + (CP[Ti1 + 1] - CP[Ti1]) * Tdiffd
+                       : (R)0 + P1[0] / rotot1 * (CP[Ti1] + (CP[Ti1 + 1] - CP[Ti1]) * Tdiffd);
   R gamd = cpd / (cpd - Rtot1);
   R a1 = rsqrt_(gamd * Rtot1 * T1d);
   R T4d = P4[MB_IPR] / (Rtot4 * rotot4);
   int Ti4 = tidx(p, T4d);
   Tdiffd = T4d - (R)Ti4;
-  cpd = (R)0 + P4[0] / rotot4 * (CP[Ti4] + (CP[Ti4 + 1] - CP[Ti4]) * Tdiffd);
+  cpd = Fast<R>::on ? CP[Ti4] + (CP[Ti4 + 1] - CP[Ti4]) * Tdiffd
+                   : (R)0 + P4[0] / rotot4 * (CP[Ti4] + (CP[Ti4 + 1] - CP[Ti4]) * Tdiffd);
   gamd = cpd / (cpd - Rtot4);
   R a4 = rsqrt_(gamd * Rtot4 * T4d);
   R F_r, F_u, F_v, F_w, F_E;
@@ -531,9 +555,13 @@ MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, c
   else
     riemann_open(p, rs, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], a1, rotot1, P4[0], P4[MB_IU],
                  P4[MB_IV], P4[MB_IW], P4[MB_IPR], a4, rotot4, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
-  R su = copysign((R)0.5, F_r), sp = (R)0.5 + su, sm = su - (R)0.5;
-  R irotot1 = (R)1 / rotot1, irotot4 = (R)1 / rotot4;
-  res0[0] = F_r * area * (sp * (P1[0] * irotot1) - sm * (P4[0] * irotot4));
+  if (Fast<R>::on) {
+    res0[0] = F_r * area;  // one species: the upwinded mass fraction is 1
+  } else {
+    R su = copysign((R)0.5, F_r), sp = (R)0.5 + su, sm = su - (R)0.5;
+    R irotot1 = (R)1 / rotot1, irotot4 = (R)1 / rotot4;
+    res0[0] = F_r * area * (sp * (P1[0] * irotot1) - sm * (P4[0] * irotot4));
+  }
   res0[MB_IU] = F_u * area; res0[MB_IV] = F_v * area; res0[MB_IW] = F_w * area; res0[MB_IPR] = F_E * area;
 }
 
@@ -576,6 +604,9 @@ MB_HD void visc_flux(const Params& p, const R G[MB_NP][3], const R* Pf, R nx, R 
   R S2 = Txy * nx + Tyy * ny + Tyz * nz;
   R S3 = Txz * nx + Tyz * ny + Tzz * nz;
   R DiffH = (R)0;
+  if (Fast<R>::on) {
+    F[0] = (R)0;  // one species: no species diffusion, no enthalpy diffusion
+  } else {
   R DmGY = Dm * (G[0][0] * nx + G[0][1] * ny + G[0][2] * nz);
   R F0 = drho * area * DmGY;
   const R* H = Tab<R>::h(p);
@@ -584,9 +615,14 @@ MB_HD void visc_flux(const Params& p, const R G[MB_NP][3], const R* Pf, R nx, R 
   DiffH = DiffH + DmGY * hh;
   R sflx = (R)0 + F0;
   F[0] = F0 - sflx * Pf[0] / drho;
+  }
   F[MB_IU] = area * S1; F[MB_IV] = area * S2; F[MB_IW] = area * S3;
-  F[MB_IPR] = area * ((S1 * Pf[MB_IU] + S2 * Pf[MB_IV] + S3 * Pf[MB_IW]) +
-                      kappaf * (G[MB_IPR][0] * nx + G[MB_IPR][1] * ny + G[MB_IPR][2] * nz) + DiffH * drho);
+  if (Fast<R>::on)
+    F[MB_IPR] = area * ((S1 * Pf[MB_IU] + S2 * Pf[MB_IV] + S3 * Pf[MB_IW]) +
+                        kappaf * (G[MB_IPR][0] * nx + G[MB_IPR][1] * ny + G[MB_IPR][2] * nz));
+  else
+    F[MB_IPR] = area * ((S1 * Pf[MB_IU] + S2 * Pf[MB_IV] + S3 * Pf[MB_IW]) +
+                        kappaf * (G[MB_IPR][0] * nx + G[MB_IPR][1] * ny + G[MB_IPR][2] * nz) + DiffH * drho);
 }
 
 // the cell density / temperature of the thermo cache (Mod_Thermo_Cache.f90:327-330,378-380)
