@@ -11,6 +11,7 @@ events, max over ranks. --impl reference times the CPU restatement of the refere
 itself is Fortran/OpenACC/CUDA Fortran and cannot be built here) on the host cores, on a bounded sample.
 """
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -39,32 +40,47 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_launch(n):
-    """DRAM bytes (read + write) of one sweep launch from the committed ncu summary, scaled from its case."""
+def traffic_per_launch(n, form):
+    """DRAM bytes (read + write) of one sweep launch of `form` from the committed ncu summary, scaled from the
+    captured case by the cells processed (the sweep's traffic grows in proportion to them)."""
     p = os.path.join(ROOT, "profiles", "sweep_traffic.json")
     if not os.path.exists(p):
         return None
-    d = json.load(open(p))
+    d = json.load(open(p)).get(form)
+    if not d:
+        return None
     return float(d["dram_bytes_per_launch"]) * (n ** 3) / float(d["cells"])
 
 
 class Clocks:
-    """nvidia-smi samples during the timed region."""
+    """nvidia-smi samples (every 100 ms) kept for the timed region only: the sampler starts before the warm-up,
+    mark() and stop() bracket the timed region by host wall-clock, and samples are selected by their own
+    timestamps."""
 
     def __init__(self, idx):
-        self.f = os.path.join("/tmp", "mose_clocks_%d.csv" % os.getpid())
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        self.f = os.path.join("/tmp", "mose_clocks_%d_%d.csv" % (os.getpid(), idx))
+        q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.t0 = self.t1 = None
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(idx), "--query-gpu=" + q, "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=open(self.f, "w"), stderr=subprocess.DEVNULL)
+                                       "-lms", "100"], stdout=open(self.f, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+            return
+        deadline = time.time() + 5.0            # wait for the first sample so the timed region is covered
+        while time.time() < deadline and os.path.getsize(self.f) == 0:
+            time.sleep(0.02)
+
+    def mark(self):
+        self.t0 = time.time()
 
     def stop(self):
+        self.t1 = time.time()
         if self.p is None:
             return None
+        time.sleep(0.25)                         # let the sample that covers the end of the region arrive
         self.p.terminate()
         try:
             self.p.wait(timeout=5)
@@ -73,17 +89,27 @@ class Clocks:
         rows = []
         for line in open(self.f):
             c = [x.strip() for x in line.split(",")]
-            if len(c) >= 9:
-                rows.append(c)
-        if not rows:
+            if len(c) < 10:
+                continue
+            try:
+                ts = datetime.datetime.strptime(c[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except ValueError:
+                continue
+            rows.append((ts, c[1:]))
+        inside = [r for t, r in rows if self.t0 - 0.1 <= t <= self.t1 + 0.1]
+        if not inside and rows:                  # region shorter than the sampling period: nearest sample
+            mid = 0.5 * (self.t0 + self.t1)
+            inside = [min(rows, key=lambda tr: abs(tr[0] - mid))[1]]
+        if not inside:
             return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = max(float(r[2]) for r in rows)
+        sm = [float(r[1]) for r in inside if r[1].replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in inside)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower() == "active"})
-        load = [s for s in sm if s > 0.5 * mx] or sm
+        reasons = sorted({names[q] for r in inside for q in range(4) if r[5 + q].lower() == "active"})
+        load = [v for v in sm if v > 0.5 * mx] or sm
+        pw = [float(r[3]) for r in inside if r[3].replace(".", "").isdigit()]
         return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(inside), "power_w_median": statistics.median(pw) if pw else None}
 
 
 def dist_setup():
@@ -172,7 +198,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--n", type=int, default=256)
@@ -197,13 +223,14 @@ def main():
     forms = {}
     for name, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
         eng = Engine(case, precision=prec, device=local, stream=stream)
+        clk = Clocks(local)
         with torch.cuda.stream(stream):
             eng.step(args.warmup, graph=True)
         barrier(pg, dev)
         l0 = eng.launches
-        clk = Clocks(local) if name == "mixed" else None
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier(pg, dev)
+        clk.mark()
         e0.record(stream)
         with torch.cuda.stream(stream):
             eng.step(args.steps, graph=True)
@@ -211,7 +238,7 @@ def main():
         e1.synchronize()
         barrier(pg, dev)
         ms = max_over_ranks(pg, e0.elapsed_time(e1), dev)
-        clocks = clk.stop() if clk else None
+        clocks = clk.stop()
         st = eng.status()
         if st.code != 0:
             raise RuntimeError("%s form: %s" % (name, abi.status_message(st.code)))
@@ -265,7 +292,7 @@ def main():
     peak, peak_kind = peaks()
     bytes_launch = cells * B_STAGE
     achieved = bytes_launch / (f["sweep_ms"] * 1e-3) / 1e9
-    tr = traffic_per_launch(args.n)
+    tr = traffic_per_launch(args.n, head)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": f["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 flux / f64 state" if head == "mixed" else "f64",
@@ -287,7 +314,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
                     "d2h_bytes_per_step": state_bytes / args.steps + 48,
                     "path": "C ABI: upload once, per step mb_begin_step + 3 x mb_stage + mb_get_status, download"},
-            "gpu_launches": f["launches"], "clocks": forms["mixed"]["clocks"]}
+            "gpu_launches": f["launches"], "clocks": f["clocks"]}
     if rank == 0 and world == 1 and not args.no_cpu:
         v, n, t = cpu_sample(case, min_seconds=10.0, max_steps=2)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
