@@ -60,12 +60,15 @@ extern "C" {
 #define MB_E_NODEV (-9)        /* no CUDA device */
 
 /* boundary record types after Setup_BC_Device (IO_BC_Open.f90:155-390 maps the bc.txt codes):
- * 1 = 1:1 / periodic connection (101, 201), 4 = inflow/outflow (405 supersonic inflow),
- * 5 = adiabatic no-slip wall (301), 11 = extrapolation (400) */
+ * 1 = 1:1 / periodic connection (101, 201), 4 = inflow/outflow as bc.txt 405 sets it up (the supersonic
+ * static-state inlet, pamb = PAMB_FORCE_SUPERSONIC, IO_BC_Open.f90:286-303: the supersonic closure
+ * whatever the Mach, the face closed to a symmetry face on outward flow), 5 = adiabatic no-slip wall
+ * (301 with q = 0), 11 = extrapolation (400) */
 #define MB_BC_CONNECTION 1
 #define MB_BC_INFLOW 4
 #define MB_BC_WALL 5
 #define MB_BC_EXTRAPOLATION 11
+#define MB_BC_NQ 6 /* parameters of a record (mb_bc.q) */
 
 /* limiter ids = lim_dev (numerics/space/Lib_Limiters.f90:21-61) */
 #define MB_LIM_MINMOD 1
@@ -105,7 +108,8 @@ typedef struct mb_bc {
   int32_t type;  /* MB_BC_* */
   int32_t conn;  /* type 1: index into mb_mesh.conn; -1 otherwise */
   int32_t pad0;
-  double q[MB_NPRIM]; /* type 4: the imposed primitive state (rho, u, v, w, p) */
+  double q[MB_BC_NQ]; /* type 4 (405): mach, T0, p0 (static T and p), alpha, beta (flow angles, radians),
+                         rel_fac (bc%mach, bc%T0, bc%p0, bc%alpha, bc%beta, bc%rel_fac); unused otherwise */
 } mb_bc;
 
 /* One connection (domain%conn_*, Lib_Extrapolation.f90:1023-1134): the donor face cell of a
@@ -143,7 +147,10 @@ typedef struct mb_scheme {
   int32_t limiter;    /* lim_dev */
   int32_t riemann;    /* rs_dev */
   int32_t visc;       /* 0 Euler, 1 laminar Navier-Stokes */
-  int32_t n_rk;       /* 1 euler, 2 RK2, 3 SSP-RK3 (Lib_RK.f90:6-9); 4 classical RK4 (no reference) */
+  int32_t n_rk;       /* 1 euler, 2 RK2, 3 SSP-RK3 (Lib_RK.f90:6-9); 4 classical RK4 (no reference: the
+                         reference's two-register update cannot express it; the engine keeps a conserved
+                         accumulator, U1 = Un + dt/2 k1, U2 = Un + dt/2 k2, U3 = Un + dt k3,
+                         Un+1 = Un + dt/6 (k1 + 2 k2 + 2 k3 + k4)) */
   int32_t precision;  /* MB_PREC_* */
   int32_t ndir;       /* computational directions (Lib_Metrics.f90:152-172) */
   int32_t time_clip;  /* clip the last step onto time_threshold (Mod_dt.f90:283-296) */

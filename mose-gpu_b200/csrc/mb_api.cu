@@ -1,6 +1,7 @@
 // mb_api.cu -- the C ABI of include/mose_b200.h: context set-up (device tables built once from the
 // host descriptions, as Setup_BC_Device / Setup_Device_Residency do), the per-call entry points
 // and the time loop with a device-side clock, optionally replayed as a CUDA graph.
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -36,6 +37,7 @@ struct mb_ctx {
   DTile* d_tiles_aux = nullptr;
   int ntiles_aux = 0;
   double* d_scratch = nullptr;  // the engine's own stage buffer (ncell x 5)
+  double* d_acc4 = nullptr;     // RK4: conserved accumulator (ncell x 5)
   std::vector<void*> geo32;     // FP32 geometry copies of the mixed form
   long long ncell = 0;
   std::vector<int> blk_n;       // 3 per block
@@ -72,7 +74,7 @@ static void free_ctx(mb_ctx* c) {
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   if (c->graph) cudaGraphDestroy(c->graph);
   void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
-                  c->d_pgsrc, c->d_pg, c->d_tab, c->d_tabf, c->d_st, c->d_tiles_sweep, c->d_tiles_aux, c->d_scratch};
+                  c->d_pgsrc, c->d_pg, c->d_tab, c->d_tabf, c->d_st, c->d_tiles_sweep, c->d_tiles_aux, c->d_scratch, c->d_acc4};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (void* q : c->geo32)
@@ -93,6 +95,25 @@ static std::vector<DTile> make_tiles(const mb_mesh* mesh, int ty, int kc) {
 
 static const double RKC[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0 / 3.0}};  // Lib_RK.f90:6-9
 
+// rk_coeff of stage irk (the SSP forms); RK4 carries its own weights in the update (cons_update)
+static double rkc_of(int n, int irk) { return n == 4 ? 0.0 : RKC[n - 1][irk - 1]; }
+
+// stage irk of the step: input / output buffers so that the state lands back in P after the last stage (the
+// old state u^n in P is only read at the updated cell itself, so the last stage updates P in place):
+//   RK4: P -> S, S -> PO, PO -> S, S -> P     RK3: P -> S, S -> PO, PO -> P
+//   RK2: P -> S, S -> P                       Euler: P -> S, then S copied to P
+static void stage_buffers(int n, int irk, double* P, double* PO, double* S, const double** in, double** out) {
+  if (irk == 1) { *in = P; *out = S; }
+  else if (n == 2) { *in = S; *out = P; }
+  else if (n == 3) { *in = (irk == 2) ? S : PO; *out = (irk == 2) ? PO : P; }
+  else {
+    const double* ins[4] = {P, S, PO, S};
+    double* outs[4] = {S, PO, S, P};
+    *in = ins[irk - 1];
+    *out = outs[irk - 1];
+  }
+}
+
 extern "C" {
 
 const char* mb_version(void) { return "mose_b200 0.1 (sm_100a)"; }
@@ -104,14 +125,17 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   *out = nullptr;
   if (sc->riemann != MB_RS_HLLC && sc->riemann != MB_RS_AUSMP && sc->riemann != MB_RS_LMROE) return MB_E_UNSUPPORTED;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
-  if (sc->n_rk < 1 || sc->n_rk > 3) return MB_E_UNSUPPORTED;
+  if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
   if (sc->precision != MB_PREC_FP64 && sc->precision != MB_PREC_MIXED) return MB_E_UNSUPPORTED;
   if (sc->ndir < 1 || sc->ndir > 3) return MB_E_ARG;
   if (th->tmax - th->tmin < 2 || !th->cp || !th->h || !th->mu || !th->k) return MB_E_ARG;
   for (int q = 0; q < mesh->nrec; ++q) {
     const mb_bc& r = mesh->rec[q];
-    if (r.type != MB_BC_CONNECTION && r.type != MB_BC_EXTRAPOLATION) return MB_E_UNSUPPORTED;
+    if (r.type != MB_BC_CONNECTION && r.type != MB_BC_EXTRAPOLATION && r.type != MB_BC_WALL &&
+        r.type != MB_BC_INFLOW)
+      return MB_E_UNSUPPORTED;
     if (r.blk < 0 || r.blk >= mesh->nblk || r.face < 1 || r.face > 6) return MB_E_ARG;
+    if (r.type == MB_BC_INFLOW && !(r.q[1] > 0.0 && r.q[2] > 0.0)) return MB_E_ARG;  // T0, p0
   }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return MB_E_NODEV;
@@ -174,7 +198,11 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
     const mb_bc& r = mesh->rec[q];
     hr[q].type = r.type;
     hr[q].pg = r.conn;
-    for (int s = 0; s < MB_NPRIM; ++s) hr[q].q[s] = r.q[s];
+    for (int s = 0; s < 8; ++s) hr[q].q[s] = 0.0;
+    if (r.type == MB_BC_INFLOW) {  // mach, T0, p0, rel_fac, cos / sin of alpha and beta
+      const double v[8] = {r.q[0], r.q[1], r.q[2], r.q[5], cos(r.q[3]), sin(r.q[3]), cos(r.q[4]), sin(r.q[4])};
+      for (int s = 0; s < 8; ++s) hr[q].q[s] = v[s];
+    }
     hg[q] = GRec{r.blk, r.i, r.j, r.k, r.face, r.type};
     if (r.type == MB_BC_EXTRAPOLATION || r.type == MB_BC_INFLOW || r.type == MB_BC_WALL) phys.push_back(q);
     if (r.type == MB_BC_EXTRAPOLATION) cubic.push_back(q);
@@ -232,6 +260,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   std::vector<DTile> ta = make_tiles(mesh, TY_AUX, 16);
   // the mixed form reads its geometry in FP32: one conversion here instead of one per face per stage
   if (sc->precision == MB_PREC_MIXED) {
+    std::vector<std::pair<const double*, float*>> made;  // blocks that share a geometry array share its copy
     for (auto& d : hb) {
       const long long pk = d.n3 + 2 * MB_GC;
       const long long npad = (long long)d.pi * d.pj * pk;
@@ -240,8 +269,13 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
       const double* src[5] = {d.fm1, d.fm2, d.fm3, d.dl, d.m};
       float* dst[5];
       for (int q = 0; q < 5; ++q) {
+        dst[q] = nullptr;
+        for (auto& m : made)
+          if (m.first == src[q]) dst[q] = m.second;
+        if (dst[q]) continue;
         if (cudaMalloc((void**)&dst[q], n[q] * sizeof(float)) != cudaSuccess) { free_ctx(c); return MB_E_NOMEM; }
         c->geo32.push_back(dst[q]);
+        made.push_back({src[q], dst[q]});
         if (to_float(src[q], dst[q], n[q], 0) != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
       }
       d.fm1f = dst[0]; d.fm2f = dst[1]; d.fm3f = dst[2]; d.dlf = dst[3]; d.mf = dst[4];
@@ -278,6 +312,13 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
     return MB_E_NOMEM;
   }
   if (cudaMemset(c->d_scratch, 0, (size_t)c->ncell * MB_NPRIM * sizeof(double)) != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+  if (sc->n_rk == 4) {
+    if (cudaMalloc((void**)&c->d_acc4, (size_t)c->ncell * MB_NPRIM * sizeof(double)) != cudaSuccess) {
+      free_ctx(c);
+      return MB_E_NOMEM;
+    }
+    if (cudaMemset(c->d_acc4, 0, (size_t)c->ncell * MB_NPRIM * sizeof(double)) != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+  }
   {
     cudaError_t e = (sc->precision == MB_PREC_MIXED)
                         ? (sc->riemann == 1 ? sweep_f32_rs1_setup() : sc->riemann == 4 ? sweep_f32_rs4_setup() : sweep_f32_rs12_setup())
@@ -305,6 +346,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   p.lim = sc->limiter; p.rs = sc->riemann; p.visc = sc->visc ? 1 : 0; p.ndir = sc->ndir; p.dt_additive = sc->dt_additive;
   p.guard = sc->visc ? 1 : 0; p.state_check = sc->state_check;
   p.cfl = sc->cfl; p.vnn = sc->vnn; p.prandtl = sc->prandtl; p.schmidt = sc->schmidt; p.mco = sc->mco;
+  p.n_rk = sc->n_rk; p.irk = 0; p.acc4 = c->d_acc4;
   GhostLists& g = c->g;
   g.rec = c->d_grec; g.phys = c->d_phys; g.nphys = (int)phys.size(); g.cubic = c->d_cubic; g.ncubic = (int)cubic.size();
   g.cdst = c->d_cdst; g.csrc = c->d_csrc; g.ncopy = (int)cdst.size(); g.pgsrc = c->d_pgsrc; g.nconn = mesh->nconn;
@@ -320,19 +362,22 @@ void mb_destroy(mb_ctx* ctx) {
   free_ctx(ctx);
 }
 
-static int sweep(mb_ctx* c, int mode, const double* Pin, const double* Pold, double* Pout, double* Rout, double rkc,
+static int sweep(mb_ctx* c, int mode, const double* Pin, const double* Pold, double* Pout, double* Rout, int irk,
                  int last, cudaStream_t s) {
   const DTile* t = c->d_tiles_sweep;
   const int n = c->ntiles_sweep;
+  Params p = c->p;
+  p.irk = irk;
+  const double rkc = irk > 0 ? rkc_of(c->sc.n_rk, irk) : 0.0;
   cudaError_t e;
   if (c->sc.precision == MB_PREC_MIXED) {
-    if (c->sc.riemann == 1) e = sweep_f32_rs1(c->p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
-    else if (c->sc.riemann == 4) e = sweep_f32_rs4(c->p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
-    else e = sweep_f32_rs12(c->p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+    if (c->sc.riemann == 1) e = sweep_f32_rs1(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+    else if (c->sc.riemann == 4) e = sweep_f32_rs4(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+    else e = sweep_f32_rs12(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
   } else {
-    if (c->sc.riemann == 1) e = sweep_f64_rs1(c->p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
-    else if (c->sc.riemann == 4) e = sweep_f64_rs4(c->p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
-    else e = sweep_f64_rs12(c->p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+    if (c->sc.riemann == 1) e = sweep_f64_rs1(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+    else if (c->sc.riemann == 4) e = sweep_f64_rs4(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+    else e = sweep_f64_rs12(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
   }
   c->launches += 1;
   CK(e);
@@ -356,13 +401,15 @@ int mb_fill_ghosts(mb_ctx* ctx, double* P, void* stream) {
 int mb_residual(mb_ctx* ctx, const double* P, double* R, void* stream) {
   if (!ctx || !P || !R) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
-  return sweep(ctx, MODE_RESIDUAL, P, nullptr, nullptr, R, 0.0, 0, (cudaStream_t)stream);
+  return sweep(ctx, MODE_RESIDUAL, P, nullptr, nullptr, R, 0, 0, (cudaStream_t)stream);
 }
 
 int mb_update(mb_ctx* ctx, double* P, const double* PO, const double* R, int irk, double dt, void* stream) {
   if (!ctx || !P || !PO || !R || irk < 1 || irk > ctx->sc.n_rk) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
-  cudaError_t e = update_cells(ctx->p, ctx->d_tiles_aux, ctx->ntiles_aux, P, PO, R, RKC[ctx->sc.n_rk - 1][irk - 1], dt,
+  Params p = ctx->p;
+  p.irk = irk;
+  cudaError_t e = update_cells(p, ctx->d_tiles_aux, ctx->ntiles_aux, P, PO, R, rkc_of(ctx->sc.n_rk, irk), dt,
                                (cudaStream_t)stream);
   ctx->launches += 1;
   CK(e);
@@ -403,22 +450,16 @@ int mb_begin_step(mb_ctx* ctx, const double* P, void* stream) {
   return MB_OK;
 }
 
-// stage irk of the step: input / old / output buffers so that the state lands back in P after the last
-// stage (the old state u^n is only read at the updated cell itself, so the last stage updates P in place):
-//   RK3: P -> S, S -> PO, PO -> P      RK2: P -> S, S -> P      Euler: P -> S, then S copied to P
 static int stage(mb_ctx* c, double* P, double* PO, int irk, cudaStream_t s) {
   const int n = c->sc.n_rk;
   double* S = c->d_scratch;
   const double* in;
   double* outp;
-  if (irk == 1) { in = P; outp = S; }
-  else if (n == 2) { in = S; outp = P; }
-  else if (irk == 2) { in = S; outp = PO; }
-  else { in = PO; outp = P; }
+  stage_buffers(n, irk, P, PO, S, &in, &outp);
   int rc = fill(c, const_cast<double*>(in), s);
   if (rc != MB_OK) return rc;
   const int last = (irk == n) ? 1 : 0;
-  rc = sweep(c, MODE_UPDATE, in, P, outp, nullptr, RKC[n - 1][irk - 1], last, s);
+  rc = sweep(c, MODE_UPDATE, in, P, outp, nullptr, irk, last, s);
   if (rc != MB_OK) return rc;
   if (n == 1) {
     CK(cudaMemcpyAsync(P, S, (size_t)c->ncell * MB_NPRIM * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -493,8 +534,9 @@ int mb_profile_stage(mb_ctx* ctx, double* P, double* PO, int irk, int nrep, floa
   cudaStream_t s = (cudaStream_t)stream;
   const int n = ctx->sc.n_rk;
   double* S = ctx->d_scratch;
-  const double* in = (irk == 1) ? P : ((n == 2 || irk == 2) ? S : PO);
-  double* outp = (irk == 1) ? S : ((n == 2 || irk == 3) ? P : PO);
+  const double* in;
+  double* outp;
+  stage_buffers(n, irk, P, PO, S, &in, &outp);
   cudaEvent_t e0, e1, e2;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -505,7 +547,7 @@ int mb_profile_stage(mb_ctx* ctx, double* P, double* PO, int irk, int nrep, floa
     cudaEventRecord(e0, s);
     rc = fill(ctx, const_cast<double*>(in), s);
     cudaEventRecord(e1, s);
-    if (rc == MB_OK) rc = sweep(ctx, MODE_UPDATE, in, P, outp, nullptr, RKC[n - 1][irk - 1], irk == n ? 1 : 0, s);
+    if (rc == MB_OK) rc = sweep(ctx, MODE_UPDATE, in, P, outp, nullptr, irk, irk == n ? 1 : 0, s);
     cudaEventRecord(e2, s);
     cudaEventSynchronize(e2);
     float a = 0.f, b = 0.f;

@@ -308,6 +308,195 @@ MB_HD_NOINLINE void bc_extrap(const Params& p, const DBlk& b, const double* __re
   for (int s = 0; s < MB_NP; ++s) acc[s] = acc[s] + (double)(sg * F[s]);
 }
 
+// the Riemann dispatch of the record routines (Lib_Riemann.f90:120-140): HLLC Batten for rs 1, the MOSE_open
+// solvers otherwise
+template <typename R, int RS = 0>
+MB_HD void riemann_rec(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R Rl, R dr, R ur, R vr, R wr,
+                       R pr, R ar, R drtot, R Rr, R nx, R ny, R nz, R& F_r, R& F_u, R& F_v, R& F_w, R& F_E) {
+  const int rs = RS ? RS : p.rs;
+  if (rs == 1)
+    hllc(p, dl, ul, vl, wl, pl, al, dltot, Rl, dr, ur, vr, wr, pr, ar, drtot, Rr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
+  else
+    riemann_open(p, rs, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r, F_u, F_v, F_w,
+                 F_E);
+}
+
+// BC_Symmetry_Eul (Lib_BC.f90:640-737): mirror of the boundary cell about the face, limited one-sided
+// reconstruction, Riemann problem between the face state and its mirror; momentum rows only. The Euler part of
+// the adiabatic wall and the closed-inlet fallback of the 405 record.
+template <typename R, int RS = 0, int LIM = 0>
+MB_HD_NOINLINE void bc_sym_eul(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km,
+                               int Fm, double* acc) {
+  const long long nc = p.nc;
+  const int lim = LIM ? LIM : p.lim;
+  int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm1 = 1 - modfm, modfm2 = 1 - 2 * modfm, gstep = 2 * modfm - 1;
+  const long long st = (dir == 1) ? 1 : (dir == 2 ? (long long)b.pi : (long long)b.pi * b.pj);
+  const long long rb = row(b, Im, Jm, Km), ri = rb + gstep * st;
+  double g[4];
+  bc_face_geom(b, Im, Jm, Km, Fm, g);
+  R nrm[3] = {cvt<R>(g[0]), cvt<R>(g[1]), cvt<R>(g[2])};
+  R area = cvt<R>(g[3]);
+  R Bound_Dl = (R)0.5 * cvt<R>(ld(b.dl + (dir - 1) + 3 * (rb - b.boff)));
+  R Int_Dl = (R)0.5 * cvt<R>(ld(b.dl + (dir - 1) + 3 * (ri - b.boff)));
+  R B[MB_NP], I[MB_NP], G[MB_NP], F[MB_NP];
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) { B[s] = cvt<R>(ld(P + rb + s * nc)); I[s] = cvt<R>(ld(P + ri + s * nc)); }
+  R Un = B[MB_IU] * nrm[0] + B[MB_IV] * nrm[1] + B[MB_IW] * nrm[2];
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) G[s] = B[s];
+  G[MB_IU] = B[MB_IU] - (R)2 * Un * nrm[0];
+  G[MB_IV] = B[MB_IV] - (R)2 * Un * nrm[1];
+  G[MB_IW] = B[MB_IW] - (R)2 * Un * nrm[2];
+  const R fm = (R)modfm, fm1 = (R)modfm1;
+  R Dist12 = (R)2 * Bound_Dl * fm + (Bound_Dl + Int_Dl) * fm1;
+  R Dist23 = (Bound_Dl + Int_Dl) * fm + (R)2 * Bound_Dl * fm1;
+  R Dist = Bound_Dl * (R)modfm2;
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) {
+    R P1 = fm * G[s] + fm1 * I[s];
+    R P3 = fm * I[s] + fm1 * G[s];
+    R s32 = (P3 - B[s]) / Dist23;
+    R s21 = (B[s] - P1) / Dist12;
+    F[s] = B[s] + rlimiter(lim, s32, s21) * Dist;
+  }
+  R rotot, Rtot;
+  rotot_rtot(p, F[0], rotot, Rtot);
+  R Sound = f_ss(p, F[0], F[MB_IPR], rotot, Rtot);
+  Un = F[MB_IU] * nrm[0] + F[MB_IV] * nrm[1] + F[MB_IW] * nrm[2];
+  R Vt[3] = {F[MB_IU] - Un * nrm[0], F[MB_IV] - Un * nrm[1], F[MB_IW] - Un * nrm[2]};
+  R Un1 = Un * (R)modfm2;
+  R U1[3], U4[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) { U1[a] = Un1 * nrm[a] + Vt[a]; U4[a] = -Un1 * nrm[a] + Vt[a]; }
+  R F_r, F_u, F_v, F_w, F_E;
+  riemann_rec<R, RS>(p, F[0], U1[0], U1[1], U1[2], F[MB_IPR], Sound, rotot, Rtot, F[0], U4[0], U4[1], U4[2],
+                     F[MB_IPR], Sound, rotot, Rtot, nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E);
+  acc[MB_IU] = acc[MB_IU] + (double)((R)modfm2 * F_u * area);
+  acc[MB_IV] = acc[MB_IV] + (double)((R)modfm2 * F_v * area);
+  acc[MB_IW] = acc[MB_IW] + (double)((R)modfm2 * F_w * area);
+}
+
+// BC_Wall_Heat_dev (Lib_BC.f90:879-982), laminar adiabatic no-slip wall: the wall-normal velocity gradient of the
+// boundary cell, Grad . M of the cell, Stress_Vector_Std (Mod_Fluid.f90:20-44) with mu_t = 0; momentum rows only.
+template <typename R>
+MB_HD_NOINLINE void bc_wall_heat(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km,
+                                 int Fm, double* acc) {
+  const long long nc = p.nc;
+  int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm2 = 1 - 2 * modfm, modfm3 = 2 * (2 * modfm - 1);
+  const long long rb = row(b, Im, Jm, Km), l = rb - b.boff;
+  R Pb[MB_NP];
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) Pb[s] = cvt<R>(ld(P + rb + s * nc));
+  R M[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) M[a][q] = cvt<R>(ld(b.m + a + 3 * q + 9 * l));
+  R rho, Rgas;
+  rotot_rtot(p, Pb[0], rho, Rgas);
+  R T = Pb[MB_IPR] / (rho * Rgas);
+  int ti = tidx(p, T);
+  R Tdiff = T - (R)ti;
+  R mil, kl;
+  wilke(p, Pb[0], rho, ti, Tdiff, mil, kl);
+  R Grad[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) Grad[a][d] = (d == dir - 1) ? Pb[MB_IU + a] * (R)modfm3 : (R)0;
+  R G2[3][3];
+#pragma unroll
+  for (int kk = 0; kk < 3; ++kk)
+#pragma unroll
+    for (int ii = 0; ii < 3; ++ii) G2[ii][kk] = Grad[ii][0] * M[0][kk] + Grad[ii][1] * M[1][kk] + Grad[ii][2] * M[2][kk];
+  double g[4];
+  bc_face_geom(b, Im, Jm, Km, Fm, g);
+  R nx = cvt<R>(g[0]), ny = cvt<R>(g[1]), nz = cvt<R>(g[2]), area = cvt<R>(g[3]);
+  const R ntt = (R)(-2.0 / 3.0);
+  R mi = mil + (R)0;
+  R lam = ntt * mi;
+  R Div = G2[0][0] + G2[1][1] + G2[2][2];
+  R lamDiv = lam * Div;
+  R txx = lamDiv + (R)2 * mi * G2[0][0], tyy = lamDiv + (R)2 * mi * G2[1][1], tzz = lamDiv + (R)2 * mi * G2[2][2];
+  R txy = mi * (G2[0][1] + G2[1][0]), txz = mi * (G2[0][2] + G2[2][0]), tyz = mi * (G2[1][2] + G2[2][1]);
+  R S1 = txx * nx + txy * ny + txz * nz;
+  R S2 = txy * nx + tyy * ny + tyz * nz;
+  R S3 = txz * nx + tyz * ny + tzz * nz;
+  acc[MB_IU] = acc[MB_IU] - (double)((R)modfm2 * area * S1);
+  acc[MB_IV] = acc[MB_IV] - (double)((R)modfm2 * area * S2);
+  acc[MB_IW] = acc[MB_IW] - (double)((R)modfm2 * area * S3);
+}
+
+// BC_Inflow_Outflow (Lib_BC.f90:1519-1597) of a 405 record: inward flow -> BC_Supersonic_Inflow (Lib_BC.f90:
+// 1247-1330), outward flow -> the face closes (BC_Symmetry_Eul).
+template <typename R, int RS = 0, int LIM = 0>
+MB_HD_NOINLINE void bc_inflow(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km,
+                              int Fm, const double* __restrict__ q, double* acc) {
+  const long long nc = p.nc;
+  const int lim = LIM ? LIM : p.lim;
+  int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm1 = 1 - modfm, modfm2 = 1 - 2 * modfm, gstep = 2 * modfm - 1;
+  const long long st = (dir == 1) ? 1 : (dir == 2 ? (long long)b.pi : (long long)b.pi * b.pj);
+  const long long rb = row(b, Im, Jm, Km), ri = rb + gstep * st;
+  R P2[MB_NP], Ip[MB_NP];
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) { P2[s] = cvt<R>(ld(P + rb + s * nc)); Ip[s] = cvt<R>(ld(P + ri + s * nc)); }
+  double g[4];
+  bc_face_geom(b, Im, Jm, Km, Fm, g);
+  R nx = cvt<R>(g[0]), ny = cvt<R>(g[1]), nz = cvt<R>(g[2]), area = cvt<R>(g[3]);
+  const R BC_Mach = cvt<R>(ld(q + 0)), BC_T0 = cvt<R>(ld(q + 1)), BC_p0 = cvt<R>(ld(q + 2)), rel = cvt<R>(ld(q + 3));
+  R Un = P2[MB_IU] * nx + P2[MB_IV] * ny + P2[MB_IW] * nz;
+  R InOut = (R)modfm2 * Un;
+  if (BC_Mach < (R)0) InOut = (R)-1;
+  if (InOut >= (R)0) {
+    bc_sym_eul<R, RS, LIM>(p, b, P, Im, Jm, Km, Fm, acc);
+    return;
+  }
+  R frho, fR;
+  rotot_rtot(p, P2[0], frho, fR);
+  R vmag2 = P2[MB_IU] * P2[MB_IU] + P2[MB_IV] * P2[MB_IV] + P2[MB_IW] * P2[MB_IW];
+  R fS = f_ss(p, P2[0], P2[MB_IPR], P2[0], fR);
+  R fM = rsqrt_(vmag2) / fS;
+  R Mach_l = rel * BC_Mach + ((R)1 - rel) * fM;
+  R p0_l = rel * BC_p0 + ((R)1 - rel) * P2[MB_IPR];
+  R Sup[MB_NP];
+  Sup[MB_IPR] = p0_l;
+  R Sup_Rgas = (R)0 + (R)1 * (R)p.ri;
+  R Sup_rho = Sup[MB_IPR] / (Sup_Rgas * BC_T0);
+  Sup[0] = Sup_rho * (R)1;
+  R Sup_Sound = f_ss(p, Sup[0], Sup[MB_IPR], Sup_rho, Sup_Rgas);
+  const R ca = cvt<R>(ld(q + 4)), sa = cvt<R>(ld(q + 5)), cb = cvt<R>(ld(q + 6)), sb = cvt<R>(ld(q + 7));
+  Sup[MB_IU] = Mach_l * Sup_Sound * ca * cb;
+  Sup[MB_IV] = Mach_l * Sup_Sound * sa * cb;
+  Sup[MB_IW] = Mach_l * Sup_Sound * sb;
+  const R fm = (R)modfm, fm1 = (R)modfm1;
+  R PL[MB_NP], PR[MB_NP];
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) {
+    R p1 = fm * Sup[s] + fm1 * Ip[s];
+    R p3 = fm * Ip[s] + fm1 * Sup[s];
+    R Slope = rlimiter(lim, p3 - P2[s], P2[s] - p1);
+    R Face = P2[s] + (R)0.5 * Slope * (R)modfm2;
+    PL[s] = fm * Sup[s] + fm1 * Face;
+    PR[s] = fm * Face + fm1 * Sup[s];
+  }
+  R rL, RL, rR, RRr;
+  rotot_rtot(p, PL[0], rL, RL);
+  R aL = f_ss(p, PL[0], PL[MB_IPR], rL, RL);
+  rotot_rtot(p, PR[0], rR, RRr);
+  R aR = f_ss(p, PR[0], PR[MB_IPR], rR, RRr);
+  R F_r, F_u, F_v, F_w, F_E;
+  riemann_rec<R, RS>(p, PL[0], PL[MB_IU], PL[MB_IV], PL[MB_IW], PL[MB_IPR], aL, rL, RL, PR[0], PR[MB_IU], PR[MB_IV],
+                     PR[MB_IW], PR[MB_IPR], aR, rR, RRr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
+  R su = copysign((R)1, F_r);
+  R selL = ((R)1 + su) / (R)2, selR = (su - (R)1) / (R)2;
+  R Fmass = F_r * area;
+  R Fl[MB_NP];
+  Fl[0] = Fmass * (selL * PL[0] / rL - selR * PR[0] / rR);
+  Fl[MB_IU] = F_u * area; Fl[MB_IV] = F_v * area; Fl[MB_IW] = F_w * area; Fl[MB_IPR] = F_E * area;
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) acc[s] = acc[s] + (double)((R)modfm2 * Fl[s]);
+}
+
 // the records of the faces 1..6 that the cell (i,j,k) lies on, in face order
 template <typename R, bool VISC, int RS = 0, int LIM = 0>
 MB_HD void bc_cell(const Params& p, const DBlk& b, const double* __restrict__ P, int i, int j,
@@ -331,6 +520,11 @@ MB_HD void bc_cell(const Params& p, const DBlk& b, const double* __restrict__ P,
       if (VISC) bc_conn_visc<R>(p, b, P, i, j, k, F, p.pg + (long long)rc.pg * 6 * MB_NP, acc);
     } else if (rc.type == 11) {
       bc_extrap<R>(p, b, P, i, j, k, F, acc);
+    } else if (rc.type == 5) {
+      bc_sym_eul<R, RS, LIM>(p, b, P, i, j, k, F, acc);
+      if (VISC) bc_wall_heat<R>(p, b, P, i, j, k, F, acc);
+    } else if (rc.type == 4) {
+      bc_inflow<R, RS, LIM>(p, b, P, i, j, k, F, rc.q, acc);
     }
   }
 }
@@ -338,8 +532,12 @@ MB_HD void bc_cell(const Params& p, const DBlk& b, const double* __restrict__ P,
 // ---------------------------------------------------------------------------------------------
 // The conservative state update of one cell (newstate_cons_body.inc), FP64. Returns the new
 // primitive state in pn.
+// RK4 (n_rk = 4, no reference): weight C of rl in the new state from Un (stages 1-3: 1/2, 1/2, 1) and weight W
+// of rl in the accumulator a4 (stage 1: a4 = Un + rl/6; 2-3: a4 += rl/3; 4: new state = a4 + rl/6), rl = -R/vol*dt
+
 MB_HD void cons_update(const Params& p, const double* pc, const double* po, const double* res,
-                                            double vol, double dt, double rkc, double tc, double* pn) {
+                                            double vol, double dt, double rkc, double tc, double* pn,
+                                            long long row_ = -1) {
   const double strang = 1.0;
   double cons[MB_NP], cold[MB_NP], rl[MB_NP];
   auto prim2cons = [&](const double* q, double* u) {
@@ -363,8 +561,26 @@ MB_HD void cons_update(const Params& p, const double* pc, const double* po, cons
   prim2cons(pc, cons);
 #pragma unroll
   for (int s = 0; s < MB_NP; ++s) rl[s] = -res[s] / vol * dt * strang;
+  if (p.n_rk != 4) {
 #pragma unroll
-  for (int s = 0; s < MB_NP; ++s) cons[s] = cold[s] + (cons[s] - cold[s] + rl[s]) * rkc;
+    for (int s = 0; s < MB_NP; ++s) cons[s] = cold[s] + (cons[s] - cold[s] + rl[s]) * rkc;
+  } else {
+    double* a4 = p.acc4 + row_;
+    const int q = p.irk - 1;
+    const double W = (q == 0 || q == 3) ? 1.0 / 6.0 : 1.0 / 3.0;
+    if (q < 3) {
+      const double Cq = (q == 2) ? 1.0 : 0.5;
+#pragma unroll
+      for (int s = 0; s < MB_NP; ++s) {
+        const double prev = (q == 0) ? cold[s] : a4[s * p.nc];
+        a4[s * p.nc] = prev + rl[s] * W;
+        cons[s] = cold[s] + rl[s] * Cq;
+      }
+    } else {
+#pragma unroll
+      for (int s = 0; s < MB_NP; ++s) cons[s] = a4[s * p.nc] + rl[s] * W;
+    }
+  }
   double rho = 0.0 + cons[0];
   double Rg = 0.0 + p.ri * cons[0] / rho;
   pn[0] = cons[0];
@@ -633,7 +849,7 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
           Tc = mn(mx(Tc, 1.0), 9990.0);
         }
         const double vol = ld(b.vol + (r - b.boff));
-        cons_update(p, pc, po, acc, vol, dt, rkc, Tc, pn);
+        cons_update(p, pc, po, acc, vol, dt, rkc, Tc, pn, r);
         bool bad = !(pn[MB_IPR] >= 0.0);
 #pragma unroll
         for (int s = 0; s < MB_NP; ++s) bad = bad || !isfinite(pn[s]);

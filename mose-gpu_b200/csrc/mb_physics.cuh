@@ -59,7 +59,9 @@ template <> struct Geo<float> {
 struct DRec {
   int type;
   int pg;               // row of the record in the transverse-stencil table (connections), -1 otherwise
-  double q[MB_NP];
+  // type 4 (405 inlet): mach, T0, p0, rel_fac, cos alpha, sin alpha, cos beta, sin beta (the angles' cos / sin
+  // taken once on the host, so that every form uses the same values)
+  double q[8];
 };
 
 // device status + clock of the time loop (one per context)
@@ -88,6 +90,9 @@ struct Params {
   double wm, ri;
   int lim, rs, visc, ndir, dt_additive, guard, state_check;
   double cfl, vnn, prandtl, schmidt, mco;
+  int n_rk;                // 4: classical RK4 through the accumulator acc4
+  int irk;                 // stage of the launch (1-based; set per launch)
+  double* acc4;            // RK4: conserved accumulator (nc, 5), null otherwise
 };
 
 // The mixed form (R = float) applies the single-species identities of the reference's mixture formulas

@@ -10,6 +10,7 @@ import numpy as np
 GC = 2
 NSC = 1
 NPRIM = 5
+BC_NQ = 6
 
 MB_OK = 0
 MB_E_ARG = -1
@@ -49,7 +50,7 @@ class MBBlock(C.Structure):
 class MBBc(C.Structure):
     _fields_ = [("blk", C.c_int32), ("i", C.c_int32), ("j", C.c_int32), ("k", C.c_int32),
                 ("face", C.c_int32), ("type", C.c_int32), ("conn", C.c_int32), ("pad0", C.c_int32),
-                ("q", C.c_double * NPRIM)]
+                ("q", C.c_double * BC_NQ)]
 
 
 class MBConn(C.Structure):
@@ -85,7 +86,7 @@ class MBStatus(C.Structure):
 
 
 BC_DTYPE = np.dtype([("blk", "<i4"), ("i", "<i4"), ("j", "<i4"), ("k", "<i4"), ("face", "<i4"),
-                     ("type", "<i4"), ("conn", "<i4"), ("pad0", "<i4"), ("q", "<f8", (NPRIM,))])
+                     ("type", "<i4"), ("conn", "<i4"), ("pad0", "<i4"), ("q", "<f8", (BC_NQ,))])
 CONN_DTYPE = np.dtype([("rec", "<i4"), ("bs", "<i4"), ("is", "<i4"), ("js", "<i4"), ("ks", "<i4"),
                        ("fs", "<i4"), ("d11", "<i4"), ("d12", "<i4"), ("d21", "<i4"), ("d22", "<i4")])
 assert BC_DTYPE.itemsize == C.sizeof(MBBc)

@@ -187,15 +187,19 @@ def _axis_nodes(N, L, x0=0.0):
     return x0 + nu * (L / N)
 
 
-def layout_case(name, cuts, node_fn, periodic, bc_faces, thermo, scheme, prim_fn):
+def layout_case(name, cuts, node_fn, periodic, bc_faces, thermo, scheme, prim_fn, share_geometry=False):
     """A structured layout of blocks.
 
     cuts      : per axis, the cell-index cut points of the blocks, e.g. [[0, 128, 256], [0, 256], [0, 256]]
     node_fn   : (iu, iv, iw) extended global node indices (3 float arrays, ghosts included)
                 -> node coordinates (..., 3)
     periodic  : per axis, True if the global domain is periodic along it
-    bc_faces  : {global face 1..6: boundary type} for the non-periodic global faces
+    bc_faces  : {global face 1..6: boundary type, or (type, q) with the record parameters q (mb_bc.q)} for the
+                non-periodic global faces
     prim_fn   : cell-centre coordinates (..., 3) -> primitive state (5, ...) (rho, u, v, w, p)
+    share_geometry : blocks of equal extents reuse the metric arrays of the first such block (exact for a
+                node_fn that is a translation from block to block, e.g. a uniform Cartesian grid; the
+                engine then holds one copy of the geometry on the device)
     Blocks are numbered i fastest over the layout; faces between blocks are 1:1 connections with
     identity orientation; periodic axes wrap onto the first / last block.
     """
@@ -217,20 +221,30 @@ def layout_case(name, cuts, node_fn, periodic, bc_faces, thermo, scheme, prim_fn
                 boff += (n[0] + 2 * GC) * (n[1] + 2 * GC) * (n[2] + 2 * GC)
     case.ncell = boff
     # geometry
+    shared = {}
     for b in blocks:
         n, lo = b["n"], b["lo"]
-        ax = [np.arange(lo[d] - GC, lo[d] + n[d] + GC + 1, dtype=np.float64) for d in range(3)]
-        IU, IV, IW = np.meshgrid(ax[0], ax[1], ax[2], indexing="ij")
-        X = node_fn(IU, IV, IW)                           # (n1+5, n2+5, n3+5, 3)
-        M, dl, vol = cell_metrics(X)                      # padded cells
-        Xi = X[GC:GC + n[0] + 1, GC:GC + n[1] + 1, GC:GC + n[2] + 1]
-        fm1, fm2, fm3 = face_metrics(Xi)
-        b["fm1"] = np.ascontiguousarray(np.moveaxis(fm1, -1, 0)).ravel(order="F")
-        b["fm2"] = np.ascontiguousarray(np.moveaxis(fm2, -1, 0)).ravel(order="F")
-        b["fm3"] = np.ascontiguousarray(np.moveaxis(fm3, -1, 0)).ravel(order="F")
-        b["dl"] = np.moveaxis(dl, -1, 0).ravel(order="F").copy()
-        b["m"] = np.moveaxis(np.moveaxis(M, -1, 0), -1, 0).ravel(order="F").copy()  # (h, c, ...) -> m(h,c)
-        b["vol"] = vol.ravel(order="F").copy()
+        if share_geometry and tuple(n) in shared:
+            b.update(shared[tuple(n)])
+            ax = [np.arange(lo[d], lo[d] + n[d] + 1, dtype=np.float64) for d in range(3)]
+            IU, IV, IW = np.meshgrid(ax[0], ax[1], ax[2], indexing="ij")
+            Xi = node_fn(IU, IV, IW)
+        else:
+            ax = [np.arange(lo[d] - GC, lo[d] + n[d] + GC + 1, dtype=np.float64) for d in range(3)]
+            IU, IV, IW = np.meshgrid(ax[0], ax[1], ax[2], indexing="ij")
+            X = node_fn(IU, IV, IW)                           # (n1+5, n2+5, n3+5, 3)
+            M, dl, vol = cell_metrics(X)                      # padded cells
+            Xi = X[GC:GC + n[0] + 1, GC:GC + n[1] + 1, GC:GC + n[2] + 1]
+            fm1, fm2, fm3 = face_metrics(Xi)
+            b["fm1"] = np.ascontiguousarray(np.moveaxis(fm1, -1, 0)).ravel(order="F")
+            b["fm2"] = np.ascontiguousarray(np.moveaxis(fm2, -1, 0)).ravel(order="F")
+            b["fm3"] = np.ascontiguousarray(np.moveaxis(fm3, -1, 0)).ravel(order="F")
+            b["dl"] = np.moveaxis(dl, -1, 0).ravel(order="F").copy()
+            b["m"] = np.moveaxis(np.moveaxis(M, -1, 0), -1, 0).ravel(order="F").copy()  # (h, c, ...) -> m(h,c)
+            b["vol"] = vol.ravel(order="F").copy()
+            del X, M, dl, vol
+            if share_geometry:
+                shared[tuple(n)] = {f: b[f] for f in ("fm1", "fm2", "fm3", "dl", "m", "vol")}
         # cell centres of the interior cells (mean of the 8 nodes)
         C8 = 0.125 * (Xi[:-1, :-1, :-1] + Xi[1:, :-1, :-1] + Xi[:-1, 1:, :-1] + Xi[1:, 1:, :-1] +
                       Xi[:-1, :-1, 1:] + Xi[1:, :-1, 1:] + Xi[:-1, 1:, 1:] + Xi[1:, 1:, 1:])
@@ -273,7 +287,12 @@ def layout_case(name, cuts, node_fn, periodic, bc_faces, thermo, scheme, prim_fn
                 r["conn"] = sum(len(x) for x in conns) + np.arange(m)
                 conns.append(cn)
             else:
-                r["type"] = bc_faces[face]
+                spec = bc_faces[face]
+                if isinstance(spec, tuple):
+                    r["type"] = spec[0]
+                    r["q"][:] = np.asarray(spec[1], dtype=np.float64)
+                else:
+                    r["type"] = spec
             recs.append(r)
             nrec += m
     case.rec = np.concatenate(recs) if recs else np.zeros(0, dtype=abi.BC_DTYPE)
@@ -288,7 +307,8 @@ def layout_case(name, cuts, node_fn, periodic, bc_faces, thermo, scheme, prim_fn
 
 # ----------------------------------------------------------------------------- configurations
 def taylor_green(n=256, mach=0.1, re=1600.0, prandtl=0.71, blocks=1, noise=0.0, seed=20261203,
-                 riemann=abi.RS_LMROE, limiter=abi.LIM_VANALBADA, cfl=0.8, steps=100, T0=300.0, rho0=1.0):
+                 riemann=abi.RS_LMROE, limiter=abi.LIM_VANALBADA, cfl=0.8, steps=100, T0=300.0, rho0=1.0,
+                 share_geometry=None):
     """3-D compressible Navier-Stokes Taylor-Green vortex on the periodic box [0, 2 pi]^3, n^3 cells
     (split into blocks^3 equal blocks). Dimensional so that T stays on the table and inside the
     viscous thermo guard: T0 = 300 K, p0 = rho0 R T0, V0 = Mach sqrt(gamma R T0), L = 1,
@@ -324,9 +344,77 @@ def taylor_green(n=256, mach=0.1, re=1600.0, prandtl=0.71, blocks=1, noise=0.0, 
     # multi-dimensional CFL near 2.4 in 3-D and the SSP-RK3 step diverges within ten steps
     scheme = dict(limiter=limiter, riemann=riemann, visc=1, n_rk=3, ndir=3, cfl=cfl, vnn=0.3,
                   prandtl=prandtl, schmidt=0.7, mco=1.0, dt_additive=1)
-    case = layout_case("tgv%d" % n, cuts, nodes, (True, True, True), {}, th, scheme, prim)
+    if share_geometry is None:
+        share_geometry = blocks > 1 and n % blocks == 0
+    case = layout_case("tgv%d" % n, cuts, nodes, (True, True, True), {}, th, scheme, prim,
+                       share_geometry=share_geometry)
     case.steps = steps
     case.meta = dict(V0=V0, p0=p0, T0=T0, rho0=rho0, mu=mu, L=L)
+    return case
+
+
+def taylor_green_blocks(nb=4, nblk=128, steps=50, seed=20261203, **kw):
+    """The large multi-block Taylor-Green case: nb^3 blocks of nblk^3 cells on the periodic [0, 2 pi]^3, Mach 0.3,
+    Re 1600, seeded uniform velocity noise of amplitude 1e-3 V0, HLLC + MUSCL van Albada, central viscous fluxes,
+    SSP-RK3. The blocks share one copy of the (uniform) geometry."""
+    args = dict(n=nb * nblk, blocks=nb, mach=0.3, noise=1e-3, seed=seed, riemann=abi.RS_HLLC,
+                limiter=abi.LIM_VANALBADA, steps=steps, share_geometry=True)
+    args.update(kw)
+    case = taylor_green(**args)
+    case.name = "tgv_%dx%dx%d_%d" % (nb, nb, nb, nblk)
+    return case
+
+
+def multiblock_2d(cols=8, rows=6, lo=64, hi=512, seed=20261203, mach=2.0, T=300.0, p=1.0e5, re=1.0e5,
+                  amp=0.05, steps=200, cfl=0.5, n_rk=4, riemann=abi.RS_AUSMP, limiter=abi.LIM_VANLEER,
+                  prandtl=0.71, widths=None, heights=None, visc=1, bc=None, velocity=None):
+    """2-D laminar Navier-Stokes batch: a cols x rows layout of blocks whose column widths and row heights are
+    drawn from the seed uniformly in [lo, hi] cells (1:1 interfaces), one k layer, on the global (xi, eta) in
+    [0, 1]^2 mapped by x = xi + amp sin(2 pi eta), y = eta + amp sin(2 pi xi). Uniform supersonic inflow
+    (405: Mach, static T and p, flow along +x) at i = 1, extrapolation outflow (400) at i = max, adiabatic
+    no-slip walls (301) at j = 1 and j = max, extrapolation on the k faces. Re on the domain length 1 with a
+    constant viscosity, kl = mu cp / Pr. AUSM+, MUSCL van Leer, classical RK4 (no reference), min dt rule."""
+    rng = np.random.default_rng(seed)
+    if widths is None:
+        widths = rng.integers(lo, hi + 1, size=cols)
+    if heights is None:
+        heights = rng.integers(lo, hi + 1, size=rows)
+    cx = [0] + list(np.cumsum(widths).astype(int))
+    cy = [0] + list(np.cumsum(heights).astype(int))
+    NI, NJ = cx[-1], cy[-1]
+    th = ideal_gas_tables(prandtl=prandtl)
+    R, gam = th["R"], th["gamma"]
+    rho = p / (R * T)
+    a = math.sqrt(gam * R * T)
+    V = mach * a
+    mu = rho * V * 1.0 / re
+    th = ideal_gas_tables(mu=mu, prandtl=prandtl)
+    dz = 1.0 / max(NI, NJ)
+
+    def nodes(iu, iv, iw):
+        xi, eta = iu / NI, iv / NJ
+        x = xi + amp * np.sin(2.0 * np.pi * eta)
+        y = eta + amp * np.sin(2.0 * np.pi * xi)
+        return np.stack([x, y, iw * dz], axis=-1)
+
+    u0 = V if velocity is None else velocity
+
+    def prim(c):
+        shp = c.shape[:-1]
+        return np.stack([np.full(shp, rho), np.full(shp, u0), np.zeros(shp), np.zeros(shp), np.full(shp, p)])
+
+    inflow = (abi.BC_INFLOW, (mach, T, p, 0.0, 0.0, 1.0))   # mach, T0, p0, alpha, beta, rel_fac
+    if bc is None:
+        bc = {1: inflow, 2: abi.BC_EXTRAPOLATION, 3: abi.BC_WALL, 4: abi.BC_WALL, 5: abi.BC_EXTRAPOLATION,
+              6: abi.BC_EXTRAPOLATION}
+    else:
+        bc = {f: (inflow if t == abi.BC_INFLOW else t) for f, t in bc.items()}
+    scheme = dict(limiter=limiter, riemann=riemann, visc=visc, n_rk=n_rk, ndir=2, cfl=cfl, vnn=0.3,
+                  prandtl=prandtl, schmidt=0.7, mco=1.0, dt_additive=0)
+    case = layout_case("mb2d_%dx%d" % (cols, rows), [cx, cy, [0, 1]], nodes, (False, False, False), bc, th,
+                       scheme, prim)
+    case.steps = steps
+    case.meta = dict(widths=[int(w) for w in widths], heights=[int(h) for h in heights], rho=rho, V=V, mu=mu)
     return case
 
 

@@ -73,16 +73,17 @@ class Engine:
         L = load_library()
         self.lib = L
         nb = len(case.blocks)
-        self._geo = []
+        self._geo = {}                     # one device copy per geometry array (blocks may share arrays)
         self._blk = (abi.MBBlock * nb)()
         for q, b in enumerate(case.blocks):
             B = self._blk[q]
             B.n[0], B.n[1], B.n[2] = b["n"]
             B.boff = b["boff"]
             for f in ("fm1", "fm2", "fm3", "dl", "m", "vol"):
-                t = torch.from_numpy(np.ascontiguousarray(b[f], dtype=np.float64)).to(self.dev)
-                self._geo.append(t)
-                setattr(B, f, t.data_ptr())
+                key = id(b[f])
+                if key not in self._geo:
+                    self._geo[key] = (b[f], torch.from_numpy(np.ascontiguousarray(b[f], dtype=np.float64)).to(self.dev))
+                setattr(B, f, self._geo[key][1].data_ptr())
         self._rec = np.ascontiguousarray(case.rec)
         self._conn = np.ascontiguousarray(case.conn)
         mesh = abi.MBMesh()

@@ -20,11 +20,13 @@
 //   pass 2                  src/lib/gpu/pass2_body.inc:1-61
 //   boundary records        numerics/fluxes/bc/bc_record_body.inc, bc_record_apply.inc, Mod_BC.f90:400-572,
 //                           Lib_BC.f90:1770-1867 (connection, Euler), 2113-2178 (connection, viscous),
-//                           1119-1165 (extrapolation)
+//                           1119-1165 (extrapolation), 640-737 (symmetry, Euler part of the adiabatic wall),
+//                           879-982 (adiabatic wall, viscous), 1519-1597 + 1247-1330 (405 supersonic inlet),
+//                           physics/turbulence/Mod_Fluid.f90:20-44 (wall stress)
 //   ghost fill              bc/Lib_Extrapolation.f90:590-641 (ZG, cubic), 643-730, 859-879, 1023-1191
 //   thermo cache            src/lib/physics/Mod_Thermo_Cache.f90:291-425
 //   state update            src/lib/gpu/newstate_cons_body.inc:1-89, explicit/Lib_Newstate.f90:257-307
-//   RK coefficients         explicit/Lib_RK.f90:6-9
+//   RK coefficients         explicit/Lib_RK.f90:6-9; classical RK4 with a conserved accumulator (no reference)
 //   local dt                src/lib/gpu/dt_blk.inc:11-222, numerics/time/Mod_dt.f90:15-106
 //   thermo leaves           lib/FLINT/src/lib/Lib_ThermoTransport_dev.f90:54-300
 //   the step                explicit/Mod_Explicit.f90:52-279
@@ -67,6 +69,7 @@ struct Ctx {
   mb_scheme sc;
   Thermo th;
   std::vector<double> pg;  // bc_pg(nprim, 6, nrec) of the connection records
+  std::vector<double> acc4; // RK4: the conserved accumulator Un + dt (k1/6 + k2/3 + ...), (ncell, nprim)
   mb_status st;
 };
 
@@ -824,6 +827,179 @@ void bc_extrapolation(const Ctx& c, const Blk& b, const double* P, double* R, in
   for (int s = 0; s < NP; ++s) R[r + s * nc] = R[r + s * nc] + sg * F[s];
 }
 
+// The Riemann dispatch of the record routines (Lib_Riemann.f90:120-140, `Riemann`): HLLC Batten for rs 1,
+// the MOSE_open solvers for rs 4..14 (the face sensor argument is 1 at these records)
+void riemann_rec(const Ctx& c, double dl, double ul, double vl, double wl, double pl, double al, double dltot,
+                 double dr, double ur, double vr, double wr, double pr, double ar, double drtot, double nx, double ny,
+                 double nz, double& F_r, double& F_u, double& F_v, double& F_w, double& F_E) {
+  if (c.sc.riemann == 1)
+    riemann_hllc_bc(c.th, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r, F_u, F_v, F_w,
+                    F_E);
+  else
+    riemann_open(c.th, c.sc.riemann, c.sc.mco, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz,
+                 F_r, F_u, F_v, F_w, F_E);
+}
+
+// BC_Symmetry_Eul (Lib_BC.f90:640-737): the boundary cell mirrored about the face (Un_wall = 0), a limited
+// one-sided reconstruction to the face, and the Riemann problem between the face state and its mirror;
+// only the momentum rows change. Also the Euler part of the adiabatic wall (bc_record_apply.inc, case 5).
+void bc_symmetry_eul(const Ctx& c, const Blk& b, const double* P, double* R, int Im, int Jm, int Km, int Fm) {
+  const int64_t nc = c.ncell;
+  const Thermo& th = c.th;
+  int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm1 = 1 - modfm, modfm2 = 1 - 2 * modfm, gstep = 2 * modfm - 1;
+  int In[3] = {Im, Jm, Km};
+  In[dir - 1] += gstep;
+  int64_t rb = row(b, Im, Jm, Km), ri = row(b, In[0], In[1], In[2]);
+  double nrm[3], area;
+  bc_face_geom(b, Im, Jm, Km, Fm, nrm, area);
+  double Bound_Dl = 0.5 * dlv(b, dir - 1, Im, Jm, Km);
+  double Int_Dl = 0.5 * dlv(b, dir - 1, In[0], In[1], In[2]);
+  double B[NP], I[NP], G[NP], P1[NP], P3[NP], F[NP], Sl[NP];
+  for (int s = 0; s < NP; ++s) { B[s] = P[rb + s * nc]; I[s] = P[ri + s * nc]; }
+  double Un = B[IU] * nrm[0] + B[IV] * nrm[1] + B[IW] * nrm[2];
+  for (int s = 0; s < NP; ++s) G[s] = B[s];
+  G[IU] = B[IU] - 2.0 * Un * nrm[0];
+  G[IV] = B[IV] - 2.0 * Un * nrm[1];
+  G[IW] = B[IW] - 2.0 * Un * nrm[2];
+  for (int s = 0; s < NP; ++s) {
+    P1[s] = (double)modfm * G[s] + (double)modfm1 * I[s];
+    P3[s] = (double)modfm * I[s] + (double)modfm1 * G[s];
+  }
+  double Dist12 = 2.0 * Bound_Dl * (double)modfm + (Bound_Dl + Int_Dl) * (double)modfm1;
+  double Dist23 = (Bound_Dl + Int_Dl) * (double)modfm + 2.0 * Bound_Dl * (double)modfm1;
+  for (int s = 0; s < NP; ++s) {
+    double s32 = (P3[s] - B[s]) / Dist23;
+    double s21 = (B[s] - P1[s]) / Dist12;
+    Sl[s] = rlimiter(c.sc.limiter, s32, s21);
+  }
+  double Dist = Bound_Dl * (double)modfm2;
+  for (int s = 0; s < NP; ++s) F[s] = B[s] + Sl[s] * Dist;
+  double rotot, Rtot;
+  rotot_rtot(th, F[0], rotot, Rtot);
+  double Sound = f_ss(th, F[0], F[IP], rotot, Rtot);
+  Un = F[IU] * nrm[0] + F[IV] * nrm[1] + F[IW] * nrm[2];
+  double Vt[3] = {F[IU] - Un * nrm[0], F[IV] - Un * nrm[1], F[IW] - Un * nrm[2]};
+  double Un1 = Un * (double)modfm2;
+  double U1[3], U4[3];
+  for (int a = 0; a < 3; ++a) { U1[a] = Un1 * nrm[a] + Vt[a]; U4[a] = -Un1 * nrm[a] + Vt[a]; }
+  double F_r, F_u, F_v, F_w, F_E;
+  riemann_rec(c, F[0], U1[0], U1[1], U1[2], F[IP], Sound, rotot, F[0], U4[0], U4[1], U4[2], F[IP], Sound, rotot,
+              nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E);
+  R[rb + IU * nc] = R[rb + IU * nc] + (double)modfm2 * F_u * area;
+  R[rb + IV * nc] = R[rb + IV * nc] + (double)modfm2 * F_v * area;
+  R[rb + IW * nc] = R[rb + IW * nc] + (double)modfm2 * F_w * area;
+}
+
+// BC_Wall_Heat_dev (Lib_BC.f90:879-982), laminar: the wall-normal velocity gradient of the boundary cell
+// (wall velocity 0), Grad . M of the cell, the stress vector of Stress_Vector_Std (Mod_Fluid.f90:20-44) with
+// mu_t = 0; adiabatic, so the energy row is untouched.
+void bc_wall_heat(const Ctx& c, const Blk& b, const double* P, double* R, int Im, int Jm, int Km, int Fm) {
+  const int64_t nc = c.ncell;
+  int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm2 = 1 - 2 * modfm, modfm3 = 2 * (2 * modfm - 1);
+  int64_t rb = row(b, Im, Jm, Km);
+  double Pb[NP];
+  for (int s = 0; s < NP; ++s) Pb[s] = P[rb + s * nc];
+  double M[3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int q = 0; q < 3; ++q) M[a][q] = mv(b, a, q, Im, Jm, Km);
+  double rho, Rgas;
+  rotot_rtot(c.th, Pb[0], rho, Rgas);
+  double T = Pb[IP] / (rho * Rgas);
+  int ti = tidx(c.th, T);
+  double Tdiff = T - ti;
+  double mil, kl;
+  wilke(c.th, Pb[0], rho, ti, Tdiff, mil, kl);
+  double Grad[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (int a = 0; a < 3; ++a) Grad[a][dir - 1] = Pb[IU + a] * (double)modfm3;
+  double G2[3][3];
+  for (int kk = 0; kk < 3; ++kk)
+    for (int ii = 0; ii < 3; ++ii)
+      G2[ii][kk] = Grad[ii][0] * M[0][kk] + Grad[ii][1] * M[1][kk] + Grad[ii][2] * M[2][kk];
+  double nrm[3], area;
+  bc_face_geom(b, Im, Jm, Km, Fm, nrm, area);
+  const double ntt = -2.0 / 3.0;  // negativetwothird (Mod_Fluid.f90:4)
+  double mi = mil + 0.0;
+  double lam = ntt * mi;
+  double Div = G2[0][0] + G2[1][1] + G2[2][2];
+  double lamDiv = lam * Div;
+  double txx = lamDiv + 2.0 * mi * G2[0][0], tyy = lamDiv + 2.0 * mi * G2[1][1], tzz = lamDiv + 2.0 * mi * G2[2][2];
+  double txy = mi * (G2[0][1] + G2[1][0]), txz = mi * (G2[0][2] + G2[2][0]), tyz = mi * (G2[1][2] + G2[2][1]);
+  double S1 = txx * nrm[0] + txy * nrm[1] + txz * nrm[2];
+  double S2 = txy * nrm[0] + tyy * nrm[1] + tyz * nrm[2];
+  double S3 = txz * nrm[0] + tyz * nrm[1] + tzz * nrm[2];
+  R[rb + IU * nc] = R[rb + IU * nc] - (double)modfm2 * area * S1;
+  R[rb + IV * nc] = R[rb + IV * nc] - (double)modfm2 * area * S2;
+  R[rb + IW * nc] = R[rb + IW * nc] - (double)modfm2 * area * S3;
+}
+
+// BC_Inflow_Outflow (Lib_BC.f90:1519-1597) for a 405 record (pamb = PAMB_FORCE_SUPERSONIC): inward flow ->
+// BC_Supersonic_Inflow (Lib_BC.f90:1247-1330), outward flow -> the face closes (BC_Symmetry_Eul).
+// q = mach, T0, p0, alpha, beta, rel_fac; the angles enter through cos / sin taken on the host.
+void bc_inflow_405(const Ctx& c, const Blk& b, const double* P, double* R, int Im, int Jm, int Km, int Fm,
+                   const double* q) {
+  const int64_t nc = c.ncell;
+  const Thermo& th = c.th;
+  int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm1 = 1 - modfm, modfm2 = 1 - 2 * modfm, gstep = 2 * modfm - 1;
+  int In[3] = {Im, Jm, Km};
+  In[dir - 1] += gstep;
+  int64_t rb = row(b, Im, Jm, Km), ri = row(b, In[0], In[1], In[2]);
+  double P2[NP], Ip[NP];
+  for (int s = 0; s < NP; ++s) { P2[s] = P[rb + s * nc]; Ip[s] = P[ri + s * nc]; }
+  double nrm[3], area;
+  bc_face_geom(b, Im, Jm, Km, Fm, nrm, area);
+  const double BC_Mach = q[0], BC_T0 = q[1], BC_p0 = q[2], rel = q[5];
+  double Un = P2[IU] * nrm[0] + P2[IV] * nrm[1] + P2[IW] * nrm[2];
+  double InOut = (double)modfm2 * Un;
+  if (BC_Mach < 0.0) InOut = -1.0;
+  if (InOut >= 0.0) {  // error = 1: the caller applies the symmetry flux
+    bc_symmetry_eul(c, b, P, R, Im, Jm, Km, Fm);
+    return;
+  }
+  // BC_Supersonic_Inflow
+  double fR, frho;
+  rotot_rtot(th, P2[0], frho, fR);  // f_Rtot
+  double vmag2 = P2[IU] * P2[IU] + P2[IV] * P2[IV] + P2[IW] * P2[IW];
+  double fS = f_ss(th, P2[0], P2[IP], P2[0], fR);
+  double fM = std::sqrt(vmag2) / fS;
+  double Mach_l = rel * BC_Mach + (1.0 - rel) * fM;
+  double p0_l = rel * BC_p0 + (1.0 - rel) * P2[IP];
+  double Sup[NP];
+  Sup[IP] = p0_l;
+  double Sup_T = BC_T0;
+  double Sup_Rgas = 0.0 + 1.0 * th.ri;
+  double Sup_rho = Sup[IP] / (Sup_Rgas * Sup_T);
+  Sup[0] = Sup_rho * 1.0;
+  double Sup_Sound = f_ss(th, Sup[0], Sup[IP], Sup_rho, Sup_Rgas);
+  const double ca = std::cos(q[3]), sa = std::sin(q[3]), cb = std::cos(q[4]), sb = std::sin(q[4]);
+  Sup[IU] = Mach_l * Sup_Sound * ca * cb;
+  Sup[IV] = Mach_l * Sup_Sound * sa * cb;
+  Sup[IW] = Mach_l * Sup_Sound * sb;
+  double PL[NP], PR[NP];
+  for (int s = 0; s < NP; ++s) {
+    double p1 = (double)modfm * Sup[s] + (double)modfm1 * Ip[s];
+    double p3 = (double)modfm * Ip[s] + (double)modfm1 * Sup[s];
+    double Slope = rlimiter(c.sc.limiter, p3 - P2[s], P2[s] - p1);
+    double Face = P2[s] + 0.5 * Slope * (double)modfm2;
+    PL[s] = (double)modfm * Sup[s] + (double)modfm1 * Face;
+    PR[s] = (double)modfm * Face + (double)modfm1 * Sup[s];
+  }
+  double rL, RL, rR, RR;
+  rotot_rtot(th, PL[0], rL, RL);
+  double aL = f_ss(th, PL[0], PL[IP], rL, RL);
+  rotot_rtot(th, PR[0], rR, RR);
+  double aR = f_ss(th, PR[0], PR[IP], rR, RR);
+  double F_r, F_u, F_v, F_w, F_E;
+  riemann_rec(c, PL[0], PL[IU], PL[IV], PL[IW], PL[IP], aL, rL, PR[0], PR[IU], PR[IV], PR[IW], PR[IP], aR, rR, nrm[0],
+              nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E);
+  double su = std::copysign(1.0, F_r);
+  double selL = (1.0 + su) / 2.0, selR = (su - 1.0) / 2.0;
+  double Fmass = F_r * area;
+  double Fl[NP];
+  Fl[0] = Fmass * (selL * PL[0] / rL - selR * PR[0] / rR);
+  Fl[IU] = F_u * area; Fl[IV] = F_v * area; Fl[IW] = F_w * area; Fl[IP] = F_E * area;
+  for (int s = 0; s < NP; ++s) R[rb + s * nc] = R[rb + s * nc] + (double)modfm2 * Fl[s];
+}
+
 // ---- ghost fill ----
 inline int64_t rowg(const Ctx& c, int blk, int i, int j, int k) { return row(c.blk[blk], i, j, k); }
 
@@ -991,6 +1167,13 @@ void residual(Ctx& c, const double* P, double* R) {
         case MB_BC_EXTRAPOLATION:
           bc_extrapolation(c, b, P, R, r.i, r.j, r.k, r.face);
           break;
+        case MB_BC_WALL:
+          bc_symmetry_eul(c, b, P, R, r.i, r.j, r.k, r.face);
+          if (visc) bc_wall_heat(c, b, P, R, r.i, r.j, r.k, r.face);
+          break;
+        case MB_BC_INFLOW:
+          bc_inflow_405(c, b, P, R, r.i, r.j, r.k, r.face, r.q);
+          break;
         default:
           break;
       }
@@ -1001,8 +1184,15 @@ void residual(Ctx& c, const double* P, double* R) {
 // ---- state update: newstate_cons_body.inc ----
 static const double RKC[4][4] = {{1.0, 0.0, 0.0, 0.0}, {1.0, 0.50, 0.0, 0.0}, {1.0, 0.25, 2.0 / 3.0, 0.0}, {0, 0, 0, 0}};
 
+// RK4 (n_rk = 4, no reference): stage weights of the new state from Un and of the accumulator
+static const double RK4_C[4] = {0.5, 0.5, 1.0, 0.0};
+static const double RK4_W[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+
+// rk4 = 0: the SSP form of the reference, cons = cold + (cons - cold + rl) * rkc. rk4 = stage 1..4 of RK4 with
+// the cell's accumulator a4: stage 1 a4 = cold + rl/6, stages 2-3 a4 += rl/3, new = cold + C rl; stage 4
+// new = a4 + rl/6 (rl = -R / vol * dt).
 void update_cell(const Ctx& c, const double* po, double* p, const double* res, double vol, double dt, double rkc,
-                 double tc) {
+                 double tc, int rk4 = 0, double* a4 = nullptr) {
   const Thermo& th = c.th;
   const double strang = 1.0;
   double cons[NP], cold[NP], rl[NP];
@@ -1024,7 +1214,16 @@ void update_cell(const Ctx& c, const double* po, double* p, const double* res, d
   prim2cons(po, cold);
   prim2cons(p, cons);
   for (int s = 0; s < NP; ++s) rl[s] = -res[s] / vol * dt * strang;
-  for (int s = 0; s < NP; ++s) cons[s] = cold[s] + (cons[s] - cold[s] + rl[s]) * rkc;
+  if (rk4 == 0) {
+    for (int s = 0; s < NP; ++s) cons[s] = cold[s] + (cons[s] - cold[s] + rl[s]) * rkc;
+  } else if (rk4 < 4) {
+    for (int s = 0; s < NP; ++s) {
+      a4[s] = (rk4 == 1) ? cold[s] + rl[s] * RK4_W[0] : a4[s] + rl[s] * RK4_W[rk4 - 1];
+      cons[s] = cold[s] + rl[s] * RK4_C[rk4 - 1];
+    }
+  } else {
+    for (int s = 0; s < NP; ++s) cons[s] = a4[s] + rl[s] * RK4_W[3];
+  }
   double rho = 0.0 + cons[0];
   double Rg = 0.0 + th.ri * cons[0] / rho;
   p[0] = cons[0];
@@ -1053,7 +1252,7 @@ void update_cell(const Ctx& c, const double* po, double* p, const double* res, d
 
 void update(Ctx& c, double* P, const double* PO, const double* R, int irk, double dt) {
   const int64_t nc = c.ncell;
-  const double rkc = RKC[c.sc.n_rk - 1][irk - 1];
+  const double rkc = c.sc.n_rk == 4 ? 0.0 : RKC[c.sc.n_rk - 1][irk - 1];
   const bool guard = c.sc.visc != 0;
   int nbad = 0, nth = 0;
   for (size_t bi = 0; bi < c.blk.size(); ++bi) {
@@ -1072,7 +1271,10 @@ void update(Ctx& c, double* P, const double* PO, const double* R, int irk, doubl
             if (T != T) T = 300.0;
             T = std::min(std::max(T, 1.0), 9990.0);
           }
-          update_cell(c, po, p, res, b.vol[lin(b, i, j, k)], dt, rkc, T);
+          if (c.sc.n_rk == 4)
+            update_cell(c, po, p, res, b.vol[lin(b, i, j, k)], dt, rkc, T, irk, &c.acc4[(size_t)r * NP]);
+          else
+            update_cell(c, po, p, res, b.vol[lin(b, i, j, k)], dt, rkc, T);
           bool bad = !(p[IP] >= 0.0);
           for (int s = 0; s < NP; ++s) if (!std::isfinite(p[s])) bad = true;
           if (bad) ++nbad;
@@ -1181,7 +1383,7 @@ int orc_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, orc_
   if (!mesh || !sc || !th || !out) return MB_E_ARG;
   if (sc->riemann != 1 && sc->riemann != 4 && sc->riemann != 12) return MB_E_UNSUPPORTED;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
-  if (sc->n_rk < 1 || sc->n_rk > 3) return MB_E_UNSUPPORTED;
+  if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
   orc_ctx* o = new orc_ctx();
   Ctx& c = o->c;
   c.sc = *sc;
@@ -1198,8 +1400,10 @@ int orc_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, orc_
   c.rec.assign(mesh->rec, mesh->rec + mesh->nrec);
   c.conn.assign(mesh->conn, mesh->conn + mesh->nconn);
   for (const mb_bc& r : c.rec)
-    if (r.type != MB_BC_CONNECTION && r.type != MB_BC_EXTRAPOLATION) { delete o; return MB_E_UNSUPPORTED; }
+    if (r.type != MB_BC_CONNECTION && r.type != MB_BC_EXTRAPOLATION && r.type != MB_BC_WALL &&
+        r.type != MB_BC_INFLOW) { delete o; return MB_E_UNSUPPORTED; }
   c.pg.assign((size_t)c.rec.size() * 6 * NP, 0.0);
+  if (sc->n_rk == 4) c.acc4.assign((size_t)c.ncell * NP, 0.0);
   Thermo& t = c.th;
   t.tmin = th->tmin; t.tmax = th->tmax; t.wm = th->wm; t.ri = RUNIV / th->wm;
   size_t nt = (size_t)(th->tmax - th->tmin + 1);

@@ -57,4 +57,10 @@ def small_cases():
                                                          limiter=abi.LIM_MINMOD)),
         ("tgv_ausm_superbee_noise", lambda: cs.taylor_green(n=12, riemann=abi.RS_AUSMP, limiter=abi.LIM_SUPERBEE,
                                                             noise=1e-3)),
+        ("tgv_blocks_hllc_vanalbada_m03", lambda: cs.taylor_green_blocks(nb=2, nblk=6)),
+        ("mb2d_ausm_vanleer_rk4", lambda: cs.multiblock_2d(cols=2, rows=2, lo=6, hi=14, seed=7)),
+        ("mb2d_hllc_minmod_rk3", lambda: cs.multiblock_2d(cols=3, rows=2, lo=5, hi=12, seed=11, riemann=abi.RS_HLLC,
+                                                          limiter=abi.LIM_MINMOD, n_rk=3)),
+        ("mb2d_roe_mc_euler_rk4", lambda: cs.multiblock_2d(cols=2, rows=3, lo=5, hi=11, seed=5, riemann=abi.RS_LMROE,
+                                                           limiter=abi.LIM_MC, visc=0)),
     ]
