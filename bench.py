@@ -161,6 +161,110 @@ def cpu_sample(case, min_seconds=10.0, max_steps=3):
     return case.n_interior * n / dt, n, dt
 
 
+def _err_norms(case, a, b):
+    """L1 / L2 / Linf of the mixed state b against the FP64 state a, per primitive, relative to a's norms."""
+    m = case.interior_mask()
+    err = {}
+    for q, nm in enumerate(["rho", "u", "v", "w", "p"]):
+        x, y = b[q, m], a[q, m]
+        d = x - y
+        ny = np.abs(y).sum()
+        err[nm] = {"L1": float(np.abs(d).sum() / ny) if ny > 0 else float(np.abs(d).sum()),
+                   "L2": float(np.sqrt((d * d).sum() / max((y * y).sum(), 1e-300))) if ny > 0 else float(np.sqrt((d * d).sum())),
+                   "Linf": float(np.abs(d).max() / max(np.abs(y).max(), 1e-300)) if ny > 0 else float(np.abs(d).max())}
+    return err
+
+
+def run_fixed_steps(case, steps, warmup, dev, stream):
+    """Both forms of one case for warmup + steps graph-replayed steps; device time of the timed steps
+    (CUDA events on the launching stream), cell-updates/s, launches and the mixed-vs-FP64 error."""
+    import torch
+    from mosegpu import abi
+    from mosegpu.engine import Engine
+    out = {}
+    states = {}
+    for name, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
+        eng = Engine(case, precision=prec, device=dev.index, stream=stream)
+        with torch.cuda.stream(stream):
+            eng.step(warmup, graph=True)
+        torch.cuda.synchronize(dev)
+        l0 = eng.launches
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        with torch.cuda.stream(stream):
+            eng.step(steps, graph=True)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        st = eng.status()
+        if st.code != 0:
+            raise RuntimeError("%s %s form: %s" % (case.name, name, abi.status_message(st.code)))
+        out[name] = {"value": case.n_interior * steps / (ms * 1e-3), "ms_per_step": ms / steps,
+                     "gpu_launches": eng.launches - l0, "time": st.time}
+        states[name] = eng.state()
+        eng.close()
+        del eng
+        torch.cuda.empty_cache()
+    out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["mixed_vs_fp64_error_after_%d_steps" % (steps + warmup)] = _err_norms(case, states["fp64"], states["mixed"])
+    return out
+
+
+def run_c3(args, dev, stream):
+    """The 2-D multi-block laminar batch: 8 x 6 blocks of seeded widths / heights in [64, 512], 405 inlet M 2,
+    400 outlet, 301 walls, AUSM+ / van Leer, RK4, 200 steps, all 48 blocks in one sweep per stage."""
+    from mosegpu import case as cs
+    t0 = time.time()
+    case = cs.multiblock_2d()
+    setup = time.time() - t0
+    r = run_fixed_steps(case, case.steps - 3, 3, dev, stream)
+    r["config"] = {"workload": "mb2d_8x6_ns_ausm_vanleer_rk4", "cells": case.n_interior, "blocks": len(case.blocks),
+                   "widths": case.meta["widths"], "heights": case.meta["heights"], "steps": case.steps,
+                   "setup_s": round(setup, 1)}
+    return r
+
+
+def run_c5(args, dev, stream):
+    """The large multi-block 3-D case: 4 x 4 x 4 blocks of 128^3 (134 M cells), TGV at Mach 0.3 with 1e-3 noise,
+    HLLC / van Albada, SSP-RK3, 50 steps; the 64 blocks share one device copy of their (equal) geometry."""
+    from mosegpu import case as cs
+    t0 = time.time()
+    case = cs.taylor_green_blocks(nb=4, nblk=128, steps=50)
+    setup = time.time() - t0
+    r = run_fixed_steps(case, case.steps - 3, 3, dev, stream)
+    r["config"] = {"workload": "tgv_4x4x4_128_ns_hllc_vanalbada_ssprk3", "cells": case.n_interior,
+                   "blocks": len(case.blocks), "steps": case.steps, "setup_s": round(setup, 1)}
+    return r
+
+
+def run_serving(args, dev):
+    """A bounded sample of the seeded serving stream (1-D and 2-D Riemann cases, HLLC + minmod, SSP-RK3,
+    CFL 0.5, mixed precision) through the continuous-batching server: p50 / p99 time-to-solution (arrival to
+    result on the host), cases/s over the run, and the cell-updates/s the batch sustained."""
+    from mosegpu import abi
+    from mosegpu import serving as sv
+    t0 = time.time()
+    stream = sv.request_stream(n_cases=args.serve_cases, rate=args.serve_rate, seed=20261203)
+    reqs = [sv.riemann_request(q, d, n, st, te, arrival=t) for q, (t, d, n, st, te) in enumerate(stream)]
+    setup = time.time() - t0
+    srv = sv.Server(reqs[0].case.scheme, reqs[0].case.thermo, budget_bytes=int(args.serve_budget_gb * 2 ** 30),
+                    max_cases=256, precision=abi.PREC_MIXED, device=dev.index, poll_steps=args.serve_poll)
+    done = srv.serve(reqs, max_wall=args.serve_max_s)
+    srv.close()
+    lat = np.array(sorted(r.finish - r.arrival for r in done))
+    span = max(r.finish for r in done) - min(r.arrival for r in reqs) if done else float("nan")
+    work = sum(r.case.n_interior * r.steps for r in done)
+    bad = [r.rid for r in done if r.status.code != abi.MB_OK]
+    return {"cases_submitted": len(reqs), "cases_completed": len(done), "failed": bad,
+            "arrival_rate_per_s": args.serve_rate, "cases_per_s": len(done) / span if done else 0.0,
+            "p50_s": float(np.percentile(lat, 50)) if done else None,
+            "p99_s": float(np.percentile(lat, 99)) if done else None,
+            "cell_updates_per_s": work / span if done else 0.0, "makespan_s": span, "poll_steps": args.serve_poll,
+            "budget_gb": args.serve_budget_gb, "precision": "mixed", "setup_s": round(setup, 1),
+            "sample": "the first %d cases of the seeded 4096-case stream (half 1-D N in [256, 8192], half 2-D N^2 "
+                      "with N in [128, 1024], log-uniform), Poisson arrivals" % len(reqs)}
+
+
 def run_reference(args):
     world, rank, local, pg = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0, None
     if rank != 0:
@@ -203,6 +307,14 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", default="default", choices=["default", "c2", "c3", "c5", "serving"],
+                    help="default: the 256^3 Taylor-Green headline plus the serving sample and the 2-D batch; "
+                         "c2 / c3 / c5 / serving: that workload alone")
+    ap.add_argument("--serve-cases", type=int, default=48)
+    ap.add_argument("--serve-rate", type=float, default=1.0, help="Poisson arrivals per second")
+    ap.add_argument("--serve-budget-gb", type=float, default=32.0)
+    ap.add_argument("--serve-poll", type=int, default=16, help="steps between reads of the case clocks")
+    ap.add_argument("--serve-max-s", type=float, default=240.0)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -215,6 +327,15 @@ def main():
     world, rank, local, pg = dist_setup()
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if args.workload in ("c3", "c5", "serving"):
+        stream = torch.cuda.Stream(dev)
+        r = {"c3": lambda: run_c3(args, dev, stream), "c5": lambda: run_c5(args, dev, stream),
+             "serving": lambda: run_serving(args, dev)}[args.workload]()
+        if rank == 0:
+            print(json.dumps({"workload": args.workload, "n_gpus": world, **r}), flush=True)
+        if pg is not None:
+            pg.destroy_process_group()
+        return 0
     t0 = time.time()
     case = cs.taylor_green(n=args.n)
     setup_s = time.time() - t0
@@ -315,14 +436,18 @@ def main():
                     "d2h_bytes_per_step": state_bytes / args.steps + 48,
                     "path": "C ABI: upload once, per step mb_begin_step + 3 x mb_stage + mb_get_status, download"},
             "gpu_launches": f["launches"], "clocks": f["clocks"]}
+    for fm in forms.values():
+        fm["eng"].close()
+    forms.clear()
+    torch.cuda.empty_cache()
+    if args.workload == "default":
+        line["workloads"] = {"serving": run_serving(args, dev), "mb2d": run_c3(args, dev, torch.cuda.Stream(dev))}
     if rank == 0 and world == 1 and not args.no_cpu:
         v, n, t = cpu_sample(case, min_seconds=10.0, max_steps=2)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                                 "sample": "%d whole time step(s) of the %d^3 field (%.1f s), OpenMP" % (n, args.n, t)}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    for fm in forms.values():
-        fm["eng"].close()
     if pg is not None:
         pg.destroy_process_group()
     return 0

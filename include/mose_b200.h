@@ -89,7 +89,7 @@ extern "C" {
 /* One block: interior extents, row offset in the arena, geometry (device pointers). */
 typedef struct mb_block {
   int32_t n[3];      /* interior cells n1, n2, n3 (blk%dim) */
-  int32_t pad0;
+  int32_t group;     /* the independent case (time step, clock, status) the block belongs to: 0 .. ngroups-1 */
   int64_t boff;      /* 0-based first row of the padded block in P_flat (field_block_index_params) */
   const double* fm1; /* (4, 0:n1, n2, n3): nx, ny, nz, area of the i-faces */
   const double* fm2; /* (4, n1, 0:n2, n3) */
@@ -124,7 +124,10 @@ typedef struct mb_mesh {
   int32_t nblk;
   int32_t nrec;
   int32_t nconn;
-  int32_t pad0;
+  int32_t ngroups;       /* independent cases in the context (0 or 1: one case). Each case has its own dt (the
+                            minimum over its own cells), clock, stop time and status, so a batch of cases advances
+                            exactly as each case alone; mb_init reserves this many clocks for later
+                            mb_reconfigure calls */
   int64_t ncell_total;   /* rows of P_flat */
   const mb_block* blk;   /* host array [nblk] (the geometry pointers in it are device pointers) */
   const mb_bc* rec;      /* host array [nrec], grouped per block and ordered by face within it */
@@ -171,10 +174,20 @@ typedef struct mb_status {
   int32_t n_bad_state; /* cells that failed the state check */
   int32_t n_bad_thermo;/* cells that failed the thermo guard */
   int32_t bad_blk, bad_i, bad_j, bad_k; /* first offender */
-  int32_t steps;       /* steps taken by mb_step since mb_init */
+  int32_t steps;       /* steps taken by mb_step since mb_init (or the case's mb_group_reset) */
   double time;         /* simulated time (sum of dt) */
   double dt;           /* dt of the last step */
+  int32_t done;        /* the case reached its stop time (t_end) and no longer advances */
+  int32_t pad0;
 } mb_status;
+
+/* The stop rule of one case of a batch (mb_group_reset): the reference's time loop stops at time >= timemax
+ * (Mod_Explicit.f90:52-397) and Clip_dt_To_Timemax (Mod_dt.f90:283-296) clips the last step onto it. */
+typedef struct mb_group {
+  int32_t time_clip;  /* clip the last step onto t_end */
+  int32_t pad0;
+  double t_end;       /* the case stops advancing once its time reaches t_end (0: never) */
+} mb_group;
 
 typedef struct mb_ctx mb_ctx;
 
@@ -224,7 +237,7 @@ int mb_begin_step(mb_ctx* ctx, const double* P, void* stream);
 int mb_profile_stage(mb_ctx* ctx, double* P, double* PO, int irk, int nrep, float* ms_ghost, float* ms_sweep,
                      void* stream);
 
-/* Status (state check, thermo guard, first offender, simulated time, last dt). Synchronises. */
+/* Status of case 0 (state check, thermo guard, first offender, simulated time, last dt). Synchronises. */
 int mb_get_status(mb_ctx* ctx, mb_status* st);
 
 /* Compute_dt of one block without allocating any device memory. No counterpart in the reference.
@@ -243,6 +256,35 @@ int mb_get_status(mb_ctx* ctx, mb_status* st);
 int mb_dt_block_noalloc(const double* P, int64_t ncell_total, int64_t boff, const int32_t n[3], const double* dl,
                         const double* m, const double* cp, const double* mu, const double* k, int32_t tmin,
                         int32_t tmax, double wm, const mb_scheme* sc, double* dt_out, void* stream);
+
+/* Batched cases (no counterpart in the reference, whose process runs one case): mb_init with
+ * mesh->ngroups = G reserves G case clocks; the blocks of every case sit in one arena of ncell_total rows and
+ * every fused stage is ONE sweep over the tiles of all of them, each case with its own dt. */
+
+/* Replaces the blocks, records and connections of the context (cases admitted or retired) while keeping its
+ * buffers, the state arena layout rules (ncell_total may not grow) and the clocks of the cases that stay.
+ * Synchronises the device; invalidates the captured step graph. */
+int mb_reconfigure(mb_ctx* ctx, const mb_mesh* mesh);
+
+/* Starts case g afresh: time 0, no steps, cleared status, its stop rule, and its first dt from the cells of P
+ * that belong to it (the other cases' clocks are untouched). */
+int mb_group_reset(mb_ctx* ctx, int g, const mb_group* spec, const double* P, void* stream);
+
+/* Status of cases g0 .. g0+n-1 (one device read). Synchronises. */
+int mb_get_group_status(mb_ctx* ctx, int g0, int n, mb_status* out);
+
+/* The sweep's autotuner (no counterpart in the reference): times, on the state P and the current mesh, the
+ * k-chunk of the tiles of 3-D blocks (8 / 16 / 32 / 64 planes) and a plain grid (one CTA per tile) against the
+ * persistent work queue (one wave of CTAs taking the largest tiles first from a counter), and keeps the
+ * fastest for every later sweep. Does not change P or the clocks; call between steps. */
+int mb_autotune(mb_ctx* ctx, const double* P, void* stream);
+
+/* Sets the sweep configuration by hand: the k-chunk of 3-D tiles and the persistent work queue (1) or the plain
+ * grid (0). Synchronises; invalidates the captured step graph. */
+int mb_set_tuning(mb_ctx* ctx, int kchunk, int persistent);
+
+/* The configuration chosen by mb_autotune (k-chunk 16 and the plain grid before any call) and its sweep time. */
+int mb_get_tuning(const mb_ctx* ctx, int* kchunk, int* persistent, float* ms);
 
 /* Number of kernel launches this context has issued (for launch accounting). */
 int64_t mb_launch_count(const mb_ctx* ctx);

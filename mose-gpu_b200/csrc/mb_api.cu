@@ -33,14 +33,20 @@ struct mb_ctx {
   DevState* d_st = nullptr;
   DTile* d_tiles_sweep = nullptr;
   int ntiles_sweep = 0;
+  std::vector<int> hdims;       // 3 per block of the current mesh (interior extents)
+  int kc3 = 16;                 // k-chunk of the sweep tiles of blocks deeper than one cell (autotuned)
+  int persistent = 0;           // persistent work-queue sweep (autotuned)
+  float tuned_ms = 0.f;         // sweep time of the chosen configuration
+  int* d_queue = nullptr;       // tile counter of the persistent sweep
   int ty_sweep = 4;
   DTile* d_tiles_aux = nullptr;
   int ntiles_aux = 0;
   double* d_scratch = nullptr;  // the engine's own stage buffer (ncell x 5)
   double* d_acc4 = nullptr;     // RK4: conserved accumulator (ncell x 5)
-  std::vector<void*> geo32;     // FP32 geometry copies of the mixed form
+  struct Geo32 { const double* src; float* buf; long long n; };
+  std::vector<Geo32> geo32;     // FP32 geometry copies of the mixed form (source array, copy, elements)
+  int ngroups = 1;              // case clocks
   long long ncell = 0;
-  std::vector<int> blk_n;       // 3 per block
   bool dt_valid = false;
   long long launches = 0;
   // graph of one step
@@ -74,23 +80,37 @@ static void free_ctx(mb_ctx* c) {
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   if (c->graph) cudaGraphDestroy(c->graph);
   void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
-                  c->d_pgsrc, c->d_pg, c->d_tab, c->d_tabf, c->d_st, c->d_tiles_sweep, c->d_tiles_aux, c->d_scratch, c->d_acc4};
+                  c->d_pgsrc, c->d_pg, c->d_tab, c->d_tabf, c->d_st, c->d_tiles_sweep, c->d_tiles_aux, c->d_scratch, c->d_acc4, c->d_queue};
   for (void* q : ptrs)
     if (q) cudaFree(q);
-  for (void* q : c->geo32)
-    if (q) cudaFree(q);
+  for (auto& q : c->geo32)
+    if (q.buf) cudaFree(q.buf);
   delete c;
 }
 
-static std::vector<DTile> make_tiles(const mb_mesh* mesh, int ty, int kc) {
+// the tiles (32 x ty cells, kc planes) of the blocks whose class (3: deeper than one cell in k, 2: one k plane,
+// 1: one cell deep in j and k) is in mask (bit cls), block-major
+static std::vector<DTile> make_tiles(const std::vector<int>& dims, int ty, int kc, int mask = 0xe) {
   std::vector<DTile> t;
-  for (int b = 0; b < mesh->nblk; ++b) {
-    const int* n = mesh->blk[b].n;
+  const int nb = (int)dims.size() / 3;
+  for (int b = 0; b < nb; ++b) {
+    const int* n = &dims[3 * b];
+    const int cls = n[2] > 1 ? 3 : (n[1] > 1 ? 2 : 1);
+    if (!(mask & (1 << cls))) continue;
     for (int k0 = 1; k0 <= n[2]; k0 += kc)
       for (int j0 = 1; j0 <= n[1]; j0 += ty)
         for (int i0 = 1; i0 <= n[0]; i0 += 32) t.push_back(DTile{b, i0, j0, k0, std::min(k0 + kc, n[2] + 1)});
   }
   return t;
+}
+
+// the tile order of a persistent sweep: the largest tiles first, so that the queue ends on small ones
+static void sort_by_work(std::vector<DTile>& t, const std::vector<int>& dims, int ty) {
+  auto w = [&](const DTile& d) {
+    const int* n = &dims[3 * d.blk];
+    return (long long)(d.k1 - d.k0) * std::min(32, n[0] - d.i0 + 1) * std::min(ty, n[1] - d.j0 + 1);
+  };
+  std::stable_sort(t.begin(), t.end(), [&](const DTile& a, const DTile& b) { return w(a) > w(b); });
 }
 
 static const double RKC[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0 / 3.0}};  // Lib_RK.f90:6-9
@@ -120,15 +140,18 @@ const char* mb_version(void) { return "mose_b200 0.1 (sm_100a)"; }
 
 int64_t mb_launch_count(const mb_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
-int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int device, mb_ctx** out) {
-  if (!mesh || !sc || !th || !out || mesh->nblk <= 0 || mesh->ncell_total <= 0) return MB_E_ARG;
-  *out = nullptr;
-  if (sc->riemann != MB_RS_HLLC && sc->riemann != MB_RS_AUSMP && sc->riemann != MB_RS_LMROE) return MB_E_UNSUPPORTED;
-  if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
-  if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
-  if (sc->precision != MB_PREC_FP64 && sc->precision != MB_PREC_MIXED) return MB_E_UNSUPPORTED;
-  if (sc->ndir < 1 || sc->ndir > 3) return MB_E_ARG;
-  if (th->tmax - th->tmin < 2 || !th->cp || !th->h || !th->mu || !th->k) return MB_E_ARG;
+// the checks of a mesh description that mb_init and mb_reconfigure share
+static int check_mesh(const mb_mesh* mesh, int ngroups) {
+  if (!mesh || mesh->nblk <= 0 || mesh->ncell_total <= 0 || !mesh->blk) return MB_E_ARG;
+  if (mesh->nrec > 0 && !mesh->rec) return MB_E_ARG;
+  if (mesh->nconn > 0 && !mesh->conn) return MB_E_ARG;
+  for (int b = 0; b < mesh->nblk; ++b) {
+    const mb_block& q = mesh->blk[b];
+    if (q.n[0] < 1 || q.n[1] < 1 || q.n[2] < 1 || !q.fm1 || !q.fm2 || !q.fm3 || !q.dl || !q.m || !q.vol) return MB_E_ARG;
+    if (q.group < 0 || q.group >= ngroups) return MB_E_ARG;
+    const long long np = (long long)(q.n[0] + 2 * MB_GC) * (q.n[1] + 2 * MB_GC) * (q.n[2] + 2 * MB_GC);
+    if (q.boff < 0 || q.boff + np > mesh->ncell_total) return MB_E_ARG;
+  }
   for (int q = 0; q < mesh->nrec; ++q) {
     const mb_bc& r = mesh->rec[q];
     if (r.type != MB_BC_CONNECTION && r.type != MB_BC_EXTRAPOLATION && r.type != MB_BC_WALL &&
@@ -137,39 +160,46 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
     if (r.blk < 0 || r.blk >= mesh->nblk || r.face < 1 || r.face > 6) return MB_E_ARG;
     if (r.type == MB_BC_INFLOW && !(r.q[1] > 0.0 && r.q[2] > 0.0)) return MB_E_ARG;  // T0, p0
   }
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return MB_E_NODEV;
-  if (device < 0 || device >= ndev) return MB_E_ARG;
-  CK(cudaSetDevice(device));
-  mb_ctx* c = new mb_ctx();
-  c->device = device;
-  c->sc = *sc;
-  c->ncell = mesh->ncell_total;
+  return MB_OK;
+}
+
+// frees the mesh-dependent device tables (blocks, record maps, records, ghost lists, tiles, FP32 geometry)
+static void free_tables(mb_ctx* c) {
+  void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
+                  c->d_pgsrc, c->d_pg, c->d_tiles_sweep, c->d_tiles_aux};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  c->d_blk = nullptr; c->d_recmap = nullptr; c->d_rec = nullptr; c->d_grec = nullptr; c->d_phys = nullptr;
+  c->d_cubic = nullptr; c->d_cdst = nullptr; c->d_csrc = nullptr; c->d_pgsrc = nullptr; c->d_pg = nullptr;
+  c->d_tiles_sweep = nullptr; c->d_tiles_aux = nullptr;
+}
+
+// builds the mesh-dependent device tables from the host description (Setup_BC_Device, Mod_BC.f90:99-338) and
+// points the kernel parameters and ghost lists at them
+static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
+  const mb_scheme* sc = &c->sc;
   int rc;
-#define TRY(x)                 \
-  do {                         \
-    rc = (x);                  \
-    if (rc != MB_OK) {         \
-      free_ctx(c);             \
-      return rc;               \
-    }                          \
-  } while (0)
   // ---- blocks and the per-face record maps
   std::vector<DBlk> hb(mesh->nblk);
   std::vector<int> recmap;
+  // ndir: the scheme's for one case; per case, from the dimensions of its first block as the reference sets it
+  // for its one case (Lib_Metrics.f90:150-172: nk > 1 -> 3, nj = nk = 1 -> 1, else 2)
+  std::vector<int> gndir(c->ngroups, 0);
   for (int b = 0; b < mesh->nblk; ++b) {
     const mb_block& q = mesh->blk[b];
-    if (q.n[0] < 1 || q.n[1] < 1 || q.n[2] < 1 || !q.fm1 || !q.fm2 || !q.fm3 || !q.dl || !q.m || !q.vol) {
-      free_ctx(c);
-      return MB_E_ARG;
-    }
+    if (gndir[q.group] == 0) gndir[q.group] = (q.n[2] > 1) ? 3 : ((q.n[1] == 1 && q.n[2] == 1) ? 1 : 2);
+  }
+  for (int b = 0; b < mesh->nblk; ++b) {
+    const mb_block& q = mesh->blk[b];
     DBlk& d = hb[b];
+    memset(&d, 0, sizeof(d));
     d.n1 = q.n[0]; d.n2 = q.n[1]; d.n3 = q.n[2];
     d.pi = q.n[0] + 2 * MB_GC; d.pj = q.n[1] + 2 * MB_GC;
+    d.grp = q.group;
+    d.ndir = (c->ngroups > 1) ? gndir[q.group] : sc->ndir;
     d.boff = q.boff;
     d.fm1 = q.fm1; d.fm2 = q.fm2; d.fm3 = q.fm3; d.dl = q.dl; d.m = q.m; d.vol = q.vol;
     for (int f = 0; f < 6; ++f) d.rmap[f] = -1;
-    c->blk_n.push_back(q.n[0]); c->blk_n.push_back(q.n[1]); c->blk_n.push_back(q.n[2]);
   }
   for (int q = 0; q < mesh->nrec; ++q) {
     const mb_bc& r = mesh->rec[q];
@@ -183,10 +213,8 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
     const int n[3] = {d.n1, d.n2, d.n3};
     const int cc[3] = {r.i, r.j, r.k};
     if (r.i < 1 || r.i > d.n1 || r.j < 1 || r.j > d.n2 || r.k < 1 || r.k > d.n3 ||
-        cc[ax] != ((r.face & 1) ? 1 : n[ax])) {
-      free_ctx(c);
+        cc[ax] != ((r.face & 1) ? 1 : n[ax]))
       return MB_E_ARG;
-    }
     int t = (ax == 0) ? (r.j - 1) + (r.k - 1) * d.n2 : (ax == 1 ? (r.i - 1) + (r.k - 1) * d.n1 : (r.i - 1) + (r.j - 1) * d.n1);
     recmap[d.rmap[r.face - 1] + t] = q;
   }
@@ -216,10 +244,8 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   std::vector<long long> cdst, csrc, pgsrc;
   for (int q = 0; q < mesh->nconn; ++q) {
     const mb_conn& cn = mesh->conn[q];
-    if (cn.rec < 0 || cn.rec >= mesh->nrec || cn.bs < 0 || cn.bs >= mesh->nblk || mesh->rec[cn.rec].conn != q) {
-      free_ctx(c);
+    if (cn.rec < 0 || cn.rec >= mesh->nrec || cn.bs < 0 || cn.bs >= mesh->nblk || mesh->rec[cn.rec].conn != q)
       return MB_E_ARG;
-    }
     const mb_bc& r = mesh->rec[cn.rec];
     for (int g = 1; g <= MB_GC; ++g) {
       cdst.push_back(rowof(r.blk, r.i - guide(r.face, 0) * g, r.j - guide(r.face, 1) * g, r.k - guide(r.face, 2) * g));
@@ -245,22 +271,19 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   // every row must lie inside the arena
   for (const auto* v : {&cdst, &csrc, &pgsrc})
     for (long long x : *v)
-      if (x < 0 || x >= c->ncell) { free_ctx(c); return MB_E_ARG; }
-  // ---- thermo tables (FP64 and FP32 copies)
-  const int nt = th->tmax - th->tmin + 1;
-  std::vector<double> tab(4 * (size_t)nt);
-  std::vector<float> tabf(4 * (size_t)nt);
-  for (int q = 0; q < nt; ++q) {
-    tab[q] = th->cp[q]; tab[nt + q] = th->h[q]; tab[2 * nt + q] = th->mu[q]; tab[3 * nt + q] = th->k[q];
-  }
-  for (size_t q = 0; q < tab.size(); ++q) tabf[q] = (float)tab[q];
+      if (x < 0 || x >= c->ncell) return MB_E_ARG;
   // ---- tiles
-  c->ty_sweep = sc->precision == MB_PREC_MIXED ? TY_F32 : TY_F64;
-  std::vector<DTile> ts = make_tiles(mesh, c->ty_sweep, 16);
-  std::vector<DTile> ta = make_tiles(mesh, TY_AUX, 16);
-  // the mixed form reads its geometry in FP32: one conversion here instead of one per face per stage
+  c->hdims.assign(3 * (size_t)mesh->nblk, 0);
+  for (int b = 0; b < mesh->nblk; ++b)
+    for (int a = 0; a < 3; ++a) c->hdims[3 * b + a] = mesh->blk[b].n[a];
+  std::vector<DTile> ts = make_tiles(c->hdims, c->ty_sweep, c->kc3);
+  if (c->persistent) sort_by_work(ts, c->hdims, c->ty_sweep);
+  std::vector<DTile> ta = make_tiles(c->hdims, TY_AUX, 16);
+  // ---- the mixed form reads its geometry in FP32: one conversion per distinct array of this mesh (blocks may
+  // share arrays). Every copy is converted afresh (a caller may have replaced an array at the same address);
+  // the buffers of the previous mesh are reused where the size matches.
   if (sc->precision == MB_PREC_MIXED) {
-    std::vector<std::pair<const double*, float*>> made;  // blocks that share a geometry array share its copy
+    std::vector<mb_ctx::Geo32> keep, pool = c->geo32;
     for (auto& d : hb) {
       const long long pk = d.n3 + 2 * MB_GC;
       const long long npad = (long long)d.pi * d.pj * pk;
@@ -270,43 +293,114 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
       float* dst[5];
       for (int q = 0; q < 5; ++q) {
         dst[q] = nullptr;
-        for (auto& m : made)
-          if (m.first == src[q]) dst[q] = m.second;
+        for (auto& m : keep)
+          if (m.src == src[q]) dst[q] = m.buf;
         if (dst[q]) continue;
-        if (cudaMalloc((void**)&dst[q], n[q] * sizeof(float)) != cudaSuccess) { free_ctx(c); return MB_E_NOMEM; }
-        c->geo32.push_back(dst[q]);
-        made.push_back({src[q], dst[q]});
-        if (to_float(src[q], dst[q], n[q], 0) != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+        for (auto& m : pool)
+          if (m.buf && m.n == n[q]) { dst[q] = m.buf; m.buf = nullptr; break; }
+        if (!dst[q] && cudaMalloc((void**)&dst[q], n[q] * sizeof(float)) != cudaSuccess) {
+          for (auto& m : keep) cudaFree(m.buf);
+          for (auto& m : pool) if (m.buf) cudaFree(m.buf);
+          c->geo32.clear();
+          return MB_E_NOMEM;
+        }
+        keep.push_back({src[q], dst[q], n[q]});
+        if (to_float(src[q], dst[q], n[q], 0) != cudaSuccess) {
+          c->geo32 = keep;  // every buffer stays owned by the context
+          for (auto& m : pool)
+            if (m.buf) c->geo32.push_back(m);
+          return MB_E_CUDA;
+        }
       }
       d.fm1f = dst[0]; d.fm2f = dst[1]; d.fm3f = dst[2]; d.dlf = dst[3]; d.mf = dst[4];
     }
-    if (cudaDeviceSynchronize() != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+    for (auto& m : pool)
+      if (m.buf) cudaFree(m.buf);
+    c->geo32 = keep;
+    CK(cudaDeviceSynchronize());
   }
-  TRY(upload(&c->d_blk, hb.data(), hb.size()));
-  TRY(upload(&c->d_recmap, recmap.data(), recmap.size()));
-  TRY(upload(&c->d_rec, hr.data(), hr.size()));
-  TRY(upload(&c->d_grec, hg.data(), hg.size()));
-  TRY(upload(&c->d_phys, phys.data(), phys.size()));
-  TRY(upload(&c->d_cubic, cubic.data(), cubic.size()));
-  TRY(upload(&c->d_cdst, cdst.data(), cdst.size()));
-  TRY(upload(&c->d_csrc, csrc.data(), csrc.size()));
-  TRY(upload(&c->d_pgsrc, pgsrc.data(), pgsrc.size()));
-  TRY(upload(&c->d_tab, tab.data(), tab.size()));
-  TRY(upload(&c->d_tabf, tabf.data(), tabf.size()));
-  TRY(upload(&c->d_tiles_sweep, ts.data(), ts.size()));
-  TRY(upload(&c->d_tiles_aux, ta.data(), ta.size()));
+  free_tables(c);
+  if ((rc = upload(&c->d_blk, hb.data(), hb.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_recmap, recmap.data(), recmap.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_rec, hr.data(), hr.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_grec, hg.data(), hg.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_phys, phys.data(), phys.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_cubic, cubic.data(), cubic.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_cdst, cdst.data(), cdst.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_csrc, csrc.data(), csrc.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_pgsrc, pgsrc.data(), pgsrc.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_tiles_sweep, ts.data(), ts.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_tiles_aux, ta.data(), ta.size())) != MB_OK) return rc;
   c->ntiles_sweep = (int)ts.size();
   c->ntiles_aux = (int)ta.size();
-  if (mesh->nconn > 0 && cudaMalloc((void**)&c->d_pg, (size_t)mesh->nconn * 6 * MB_NPRIM * sizeof(double)) != cudaSuccess) {
-    free_ctx(c);
+  if (mesh->nconn > 0 && cudaMalloc((void**)&c->d_pg, (size_t)mesh->nconn * 6 * MB_NPRIM * sizeof(double)) != cudaSuccess)
     return MB_E_NOMEM;
+  Params& p = c->p;
+  p.blk = c->d_blk; p.rec_map = c->d_recmap; p.rec = c->d_rec; p.pg = c->d_pg;
+  GhostLists& g = c->g;
+  g.rec = c->d_grec; g.phys = c->d_phys; g.nphys = (int)phys.size(); g.cubic = c->d_cubic; g.ncubic = (int)cubic.size();
+  g.cdst = c->d_cdst; g.csrc = c->d_csrc; g.ncopy = (int)cdst.size(); g.pgsrc = c->d_pgsrc; g.nconn = mesh->nconn;
+  g.pg = c->d_pg;
+  return MB_OK;
+}
+
+int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int device, mb_ctx** out) {
+  if (!mesh || !sc || !th || !out) return MB_E_ARG;
+  *out = nullptr;
+  if (sc->riemann != MB_RS_HLLC && sc->riemann != MB_RS_AUSMP && sc->riemann != MB_RS_LMROE) return MB_E_UNSUPPORTED;
+  if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
+  if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
+  if (sc->precision != MB_PREC_FP64 && sc->precision != MB_PREC_MIXED) return MB_E_UNSUPPORTED;
+  if (sc->ndir < 1 || sc->ndir > 3) return MB_E_ARG;
+  if (th->tmax - th->tmin < 2 || !th->cp || !th->h || !th->mu || !th->k) return MB_E_ARG;
+  const int ngroups = mesh->ngroups > 0 ? mesh->ngroups : 1;
+  int rc = check_mesh(mesh, ngroups);
+  if (rc != MB_OK) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return MB_E_NODEV;
+  if (device < 0 || device >= ndev) return MB_E_ARG;
+  CK(cudaSetDevice(device));
+  mb_ctx* c = new mb_ctx();
+  c->device = device;
+  c->sc = *sc;
+  c->ncell = mesh->ncell_total;
+  c->ngroups = ngroups;
+  c->ty_sweep = sc->precision == MB_PREC_MIXED ? TY_F32 : TY_F64;
+#define TRY(x)                 \
+  do {                         \
+    rc = (x);                  \
+    if (rc != MB_OK) {         \
+      free_ctx(c);             \
+      return rc;               \
+    }                          \
+  } while (0)
+  // ---- thermo tables (FP64 and FP32 copies)
+  const int nt = th->tmax - th->tmin + 1;
+  std::vector<double> tab(4 * (size_t)nt);
+  std::vector<float> tabf(4 * (size_t)nt);
+  for (int q = 0; q < nt; ++q) {
+    tab[q] = th->cp[q]; tab[nt + q] = th->h[q]; tab[2 * nt + q] = th->mu[q]; tab[3 * nt + q] = th->k[q];
   }
-  if (cudaMalloc((void**)&c->d_st, sizeof(DevState)) != cudaSuccess) { free_ctx(c); return MB_E_NOMEM; }
-  DevState hs;
-  memset(&hs, 0, sizeof(hs));
-  double big = 1e300;
-  memcpy(&hs.dtmin_bits, &big, sizeof(double));
-  if (cudaMemcpy(c->d_st, &hs, sizeof(hs), cudaMemcpyHostToDevice) != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+  for (size_t q = 0; q < tab.size(); ++q) tabf[q] = (float)tab[q];
+  TRY(upload(&c->d_tab, tab.data(), tab.size()));
+  TRY(upload(&c->d_tabf, tabf.data(), tabf.size()));
+  // ---- one clock per case; every case starts with the scheme's stop rule
+  if (cudaMalloc((void**)&c->d_st, ngroups * sizeof(DevState)) != cudaSuccess) { free_ctx(c); return MB_E_NOMEM; }
+  {
+    std::vector<DevState> hs(ngroups);
+    for (auto& h : hs) {
+      memset(&h, 0, sizeof(h));
+      double big = 1e300;
+      memcpy(&h.dtmin_bits, &big, sizeof(double));
+      h.time_clip = sc->time_clip;
+      h.t_end = sc->time_clip ? sc->time_threshold : 0.0;
+    }
+    if (cudaMemcpy(c->d_st, hs.data(), ngroups * sizeof(DevState), cudaMemcpyHostToDevice) != cudaSuccess) {
+      free_ctx(c);
+      return MB_E_CUDA;
+    }
+  }
+  // ---- the engine's stage buffer (and the RK4 accumulator) over the whole arena
   if (cudaMalloc((void**)&c->d_scratch, (size_t)c->ncell * MB_NPRIM * sizeof(double)) != cudaSuccess) {
     free_ctx(c);
     return MB_E_NOMEM;
@@ -324,22 +418,14 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
                         ? (sc->riemann == 1 ? sweep_f32_rs1_setup() : sc->riemann == 4 ? sweep_f32_rs4_setup() : sweep_f32_rs12_setup())
                         : (sc->riemann == 1 ? sweep_f64_rs1_setup() : sc->riemann == 4 ? sweep_f64_rs4_setup() : sweep_f64_rs12_setup());
     if (e != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
-    if (getenv("MB_REPORT")) {
-      const int v = sc->visc ? 1 : 0;
-      int occ = (sc->precision == MB_PREC_MIXED)
-                    ? (sc->riemann == 1 ? sweep_f32_rs1_occupancy(v) : sc->riemann == 4 ? sweep_f32_rs4_occupancy(v) : sweep_f32_rs12_occupancy(v))
-                    : (sc->riemann == 1 ? sweep_f64_rs1_occupancy(v) : sc->riemann == 4 ? sweep_f64_rs4_occupancy(v) : sweep_f64_rs12_occupancy(v));
-      fprintf(stderr, "[mose_b200] sweep: %s, %d threads per CTA, %d CTAs per SM, %d tiles\n",
-              sc->precision == MB_PREC_MIXED ? "mixed" : "fp64", 32 * c->ty_sweep, occ, (int)ts.size());
-    }
   }
   // ---- kernel parameters
   Params& p = c->p;
   memset(&p, 0, sizeof(p));
-  p.blk = c->d_blk; p.rec_map = c->d_recmap; p.rec = c->d_rec; p.pg = c->d_pg;
   p.cp = c->d_tab - th->tmin; p.h = c->d_tab + nt - th->tmin; p.mu = c->d_tab + 2 * nt - th->tmin; p.k = c->d_tab + 3 * nt - th->tmin;
   p.cpf = c->d_tabf - th->tmin; p.hf = c->d_tabf + nt - th->tmin; p.muf = c->d_tabf + 2 * nt - th->tmin; p.kf = c->d_tabf + 3 * nt - th->tmin;
   p.st = c->d_st;
+  p.ngroups = ngroups;
   p.nc = c->ncell;
   p.tmin = th->tmin; p.tmax = th->tmax;
   p.wm = th->wm; p.ri = RUNIV / th->wm;
@@ -347,12 +433,79 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   p.guard = sc->visc ? 1 : 0; p.state_check = sc->state_check;
   p.cfl = sc->cfl; p.vnn = sc->vnn; p.prandtl = sc->prandtl; p.schmidt = sc->schmidt; p.mco = sc->mco;
   p.n_rk = sc->n_rk; p.irk = 0; p.acc4 = c->d_acc4;
-  GhostLists& g = c->g;
-  g.rec = c->d_grec; g.phys = c->d_phys; g.nphys = (int)phys.size(); g.cubic = c->d_cubic; g.ncubic = (int)cubic.size();
-  g.cdst = c->d_cdst; g.csrc = c->d_csrc; g.ncopy = (int)cdst.size(); g.pgsrc = c->d_pgsrc; g.nconn = mesh->nconn;
-  g.pg = c->d_pg;
+  if (cudaMalloc((void**)&c->d_queue, sizeof(int)) != cudaSuccess) { free_ctx(c); return MB_E_NOMEM; }
+  {
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    const int v = sc->visc ? 1 : 0;
+    int occ = (sc->precision == MB_PREC_MIXED)
+                  ? (sc->riemann == 1 ? sweep_f32_rs1_occupancy(v) : sc->riemann == 4 ? sweep_f32_rs4_occupancy(v) : sweep_f32_rs12_occupancy(v))
+                  : (sc->riemann == 1 ? sweep_f64_rs1_occupancy(v) : sc->riemann == 4 ? sweep_f64_rs4_occupancy(v) : sweep_f64_rs12_occupancy(v));
+    p.pgrid = std::max(1, occ) * std::max(1, nsm);
+  }
+  p.queue = nullptr;
+  // ---- the mesh tables
+  TRY(build_tables(c, mesh));
+  if (getenv("MB_REPORT")) {
+    const int v = sc->visc ? 1 : 0;
+    int occ = (sc->precision == MB_PREC_MIXED)
+                  ? (sc->riemann == 1 ? sweep_f32_rs1_occupancy(v) : sc->riemann == 4 ? sweep_f32_rs4_occupancy(v) : sweep_f32_rs12_occupancy(v))
+                  : (sc->riemann == 1 ? sweep_f64_rs1_occupancy(v) : sc->riemann == 4 ? sweep_f64_rs4_occupancy(v) : sweep_f64_rs12_occupancy(v));
+    fprintf(stderr, "[mose_b200] sweep: %s, %d threads per CTA, %d CTAs per SM, %d tiles\n",
+            sc->precision == MB_PREC_MIXED ? "mixed" : "fp64", 32 * c->ty_sweep, occ, c->ntiles_sweep);
+  }
 #undef TRY
   *out = c;
+  return MB_OK;
+}
+
+int mb_reconfigure(mb_ctx* ctx, const mb_mesh* mesh) {
+  if (!ctx || !mesh) return MB_E_ARG;
+  if (mesh->ncell_total > ctx->ncell) return MB_E_ARG;
+  const int ng = mesh->ngroups > 0 ? mesh->ngroups : 1;
+  if (ng > ctx->ngroups) return MB_E_ARG;
+  int rc = check_mesh(mesh, ctx->ngroups);
+  if (rc != MB_OK) return rc;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaDeviceSynchronize());  // the old tables may still be read by queued work
+  if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+  if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+  ctx->gP = nullptr;
+  ctx->gPO = nullptr;
+  return build_tables(ctx, mesh);
+}
+
+int mb_group_reset(mb_ctx* ctx, int g, const mb_group* spec, const double* P, void* stream) {
+  if (!ctx || !spec || !P || g < 0 || g >= ctx->ngroups || spec->t_end < 0.0) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(group_reset(ctx->p, g, spec->time_clip, spec->t_end, s));
+  CK(dt_cells(ctx->p, ctx->d_tiles_aux, ctx->ntiles_aux, P, s, g));
+  ctx->launches += 2;
+  return MB_OK;
+}
+
+static void to_status(const DevState& h, int state_check, mb_status* st) {
+  memset(st, 0, sizeof(*st));
+  st->n_bad_state = h.n_bad_state;
+  st->n_bad_thermo = h.n_bad_thermo;
+  st->bad_blk = h.bad_blk; st->bad_i = h.bad_i; st->bad_j = h.bad_j; st->bad_k = h.bad_k;
+  st->steps = h.steps;
+  st->time = h.time;
+  st->dt = h.dt;
+  st->done = h.done;
+  st->code = MB_OK;
+  if (h.n_bad_thermo > 0) st->code = MB_E_THERMO;
+  else if (h.n_bad_state > 0 && state_check) st->code = MB_E_STATE;
+}
+
+int mb_get_group_status(mb_ctx* ctx, int g0, int n, mb_status* out) {
+  if (!ctx || !out || g0 < 0 || n < 1 || g0 + n > ctx->ngroups) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaDeviceSynchronize());
+  std::vector<DevState> h(n);
+  CK(cudaMemcpy(h.data(), ctx->d_st + g0, n * sizeof(DevState), cudaMemcpyDeviceToHost));
+  for (int q = 0; q < n; ++q) to_status(h[q], ctx->sc.state_check, out + q);
   return MB_OK;
 }
 
@@ -362,12 +515,12 @@ void mb_destroy(mb_ctx* ctx) {
   free_ctx(ctx);
 }
 
-static int sweep(mb_ctx* c, int mode, const double* Pin, const double* Pold, double* Pout, double* Rout, int irk,
-                 int last, cudaStream_t s) {
-  const DTile* t = c->d_tiles_sweep;
-  const int n = c->ntiles_sweep;
+static int sweep_on(mb_ctx* c, const DTile* t, int n, int persistent, int mode, const double* Pin,
+                    const double* Pold, double* Pout, double* Rout, int irk, int last, cudaStream_t s) {
+  if (n <= 0) return MB_OK;
   Params p = c->p;
   p.irk = irk;
+  p.queue = persistent ? c->d_queue : nullptr;
   const double rkc = irk > 0 ? rkc_of(c->sc.n_rk, irk) : 0.0;
   cudaError_t e;
   if (c->sc.precision == MB_PREC_MIXED) {
@@ -382,6 +535,37 @@ static int sweep(mb_ctx* c, int mode, const double* Pin, const double* Pold, dou
   c->launches += 1;
   CK(e);
   return MB_OK;
+}
+
+static int sweep(mb_ctx* c, int mode, const double* Pin, const double* Pold, double* Pout, double* Rout, int irk,
+                 int last, cudaStream_t s) {
+  return sweep_on(c, c->d_tiles_sweep, c->ntiles_sweep, c->persistent, mode, Pin, Pold, Pout, Rout, irk, last, s);
+}
+
+// average device time of nrep sweeps (MODE_UPDATE of stage 1 from P into the stage buffer, no dt) over a tile
+// list, after one untimed sweep; the state P and the clocks are not changed
+static int time_sweep(mb_ctx* c, const std::vector<DTile>& tl, int persistent, const double* P, int nrep,
+                      cudaStream_t s, float* ms) {
+  DTile* d = nullptr;
+  int rc = upload(&d, tl.data(), tl.size());
+  if (rc != MB_OK) return rc;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  rc = sweep_on(c, d, (int)tl.size(), persistent, MODE_UPDATE, P, P, c->d_scratch, nullptr, 1, 0, s);
+  cudaEventRecord(e0, s);
+  for (int q = 0; q < nrep && rc == MB_OK; ++q)
+    rc = sweep_on(c, d, (int)tl.size(), persistent, MODE_UPDATE, P, P, c->d_scratch, nullptr, 1, 0, s);
+  cudaEventRecord(e1, s);
+  cudaEventSynchronize(e1);
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  *ms = t / nrep;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamSynchronize(s);
+  cudaFree(d);
+  return rc;
 }
 
 static int fill(mb_ctx* c, double* P, cudaStream_t s) {
@@ -445,7 +629,7 @@ int mb_begin_step(mb_ctx* ctx, const double* P, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   int rc = dt_min(ctx, P, s);
   if (rc != MB_OK) return rc;
-  CK(clock_step(ctx->p, ctx->sc.time_clip, ctx->sc.time_threshold, s));
+  CK(clock_step(ctx->p, s));
   ctx->launches += 1;
   return MB_OK;
 }
@@ -474,7 +658,7 @@ int mb_stage(mb_ctx* ctx, double* P, double* PO, int irk, void* stream) {
 }
 
 static int one_step(mb_ctx* c, double* P, double* PO, cudaStream_t s) {
-  CK(clock_step(c->p, c->sc.time_clip, c->sc.time_threshold, s));
+  CK(clock_step(c->p, s));
   c->launches += 1;
   for (int irk = 1; irk <= c->sc.n_rk; ++irk) {
     int rc = stage(c, P, PO, irk, s);
@@ -564,22 +748,80 @@ int mb_profile_stage(mb_ctx* ctx, double* P, double* PO, int irk, int nrep, floa
   return rc;
 }
 
-int mb_get_status(mb_ctx* ctx, mb_status* st) {
-  if (!ctx || !st) return MB_E_ARG;
+int mb_get_status(mb_ctx* ctx, mb_status* st) { return mb_get_group_status(ctx, 0, 1, st); }
+
+// The sweep's project-written autotuner: per block-size class, the k-chunk of the tiles of blocks deeper than
+// one cell (8, 16, 32 or 64 planes; blocks one plane deep have one chunk), then a plain grid of one CTA per tile
+// against the persistent work queue (about one wave of CTAs taking tiles, largest first, from a counter), each
+// candidate timed on the caller's state over the current mesh. Call between steps (it uses the stage buffer).
+int mb_autotune(mb_ctx* ctx, const double* P, void* stream) {
+  if (!ctx || !P) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int ty = ctx->ty_sweep;
+  int maxk = 1;
+  for (size_t b = 0; b < ctx->hdims.size() / 3; ++b) maxk = std::max(maxk, ctx->hdims[3 * b + 2]);
+  int rc;
+  float best = 1e30f;
+  int kbest = ctx->kc3;
+  if (maxk > 1) {
+    for (int kc : {8, 16, 32, 64}) {
+      if (kc > 16 && kc / 2 >= maxk) break;
+      std::vector<DTile> tl = make_tiles(ctx->hdims, ty, kc, 1 << 3);
+      float ms = 0.f;
+      if ((rc = time_sweep(ctx, tl, 0, P, 3, s, &ms)) != MB_OK) return rc;
+      if (ms < best) { best = ms; kbest = kc; }
+    }
+  }
+  ctx->kc3 = kbest;
+  std::vector<DTile> all = make_tiles(ctx->hdims, ty, kbest);
+  std::vector<DTile> sorted = all;
+  sort_by_work(sorted, ctx->hdims, ty);
+  float ms_plain = 0.f, ms_pers = 0.f;
+  if ((rc = time_sweep(ctx, all, 0, P, 3, s, &ms_plain)) != MB_OK) return rc;
+  if ((rc = time_sweep(ctx, sorted, 1, P, 3, s, &ms_pers)) != MB_OK) return rc;
+  ctx->persistent = ms_pers < ms_plain ? 1 : 0;
+  ctx->tuned_ms = std::min(ms_plain, ms_pers);
+  const std::vector<DTile>& use = ctx->persistent ? sorted : all;
+  if (ctx->d_tiles_sweep) cudaFree(ctx->d_tiles_sweep);
+  ctx->d_tiles_sweep = nullptr;
+  if ((rc = upload(&ctx->d_tiles_sweep, use.data(), use.size())) != MB_OK) return rc;
+  ctx->ntiles_sweep = (int)use.size();
+  if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+  if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+  ctx->gP = nullptr;
+  ctx->gPO = nullptr;
+  if (getenv("MB_REPORT"))
+    fprintf(stderr, "[mose_b200] autotune: k-chunk %d, %s sweep (plain %.3f ms, persistent %.3f ms), %d tiles\n",
+            ctx->kc3, ctx->persistent ? "persistent" : "plain", ms_plain, ms_pers, ctx->ntiles_sweep);
+  return MB_OK;
+}
+
+int mb_set_tuning(mb_ctx* ctx, int kchunk, int persistent) {
+  if (!ctx || kchunk < 1 || persistent < 0 || persistent > 1) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
   CK(cudaDeviceSynchronize());
-  DevState h;
-  CK(cudaMemcpy(&h, ctx->d_st, sizeof(h), cudaMemcpyDeviceToHost));
-  memset(st, 0, sizeof(*st));
-  st->n_bad_state = h.n_bad_state;
-  st->n_bad_thermo = h.n_bad_thermo;
-  st->bad_blk = h.bad_blk; st->bad_i = h.bad_i; st->bad_j = h.bad_j; st->bad_k = h.bad_k;
-  st->steps = h.steps;
-  st->time = h.time;
-  st->dt = h.dt;
-  st->code = MB_OK;
-  if (h.n_bad_thermo > 0) st->code = MB_E_THERMO;
-  else if (h.n_bad_state > 0 && ctx->sc.state_check) st->code = MB_E_STATE;
+  ctx->kc3 = kchunk;
+  ctx->persistent = persistent;
+  std::vector<DTile> use = make_tiles(ctx->hdims, ctx->ty_sweep, kchunk);
+  if (persistent) sort_by_work(use, ctx->hdims, ctx->ty_sweep);
+  if (ctx->d_tiles_sweep) cudaFree(ctx->d_tiles_sweep);
+  ctx->d_tiles_sweep = nullptr;
+  int rc = upload(&ctx->d_tiles_sweep, use.data(), use.size());
+  if (rc != MB_OK) return rc;
+  ctx->ntiles_sweep = (int)use.size();
+  if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+  if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+  ctx->gP = nullptr;
+  ctx->gPO = nullptr;
+  return MB_OK;
+}
+
+int mb_get_tuning(const mb_ctx* ctx, int* kchunk, int* persistent, float* ms) {
+  if (!ctx || !kchunk || !persistent || !ms) return MB_E_ARG;
+  *kchunk = ctx->kc3;
+  *persistent = ctx->persistent;
+  *ms = ctx->tuned_ms;
   return MB_OK;
 }
 

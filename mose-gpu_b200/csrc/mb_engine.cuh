@@ -620,7 +620,7 @@ MB_HD double cell_dt(const Params& p, const DBlk& b, long long l, const double* 
   double dtc = 1e8;
   if (p.dt_additive) {
     double ra_c = 0.0, ra_v = 0.0;
-    for (int d = 0; d < p.ndir; ++d) {
+    for (int d = 0; d < b.ndir; ++d) {
       double m0 = ld(m + d), m1 = ld(m + d + 3), m2 = ld(m + d + 6);
       double gn = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
       double vel_ = fabs(pl[MB_IU] * m0 + pl[MB_IV] * m1 + pl[MB_IW] * m2) / gn;
@@ -629,7 +629,7 @@ MB_HD double cell_dt(const Params& p, const DBlk& b, long long l, const double* 
       ra_v = ra_v + gn * gn;
     }
     if (p.visc) {
-      if (p.ndir == 3) {
+      if (b.ndir == 3) {
         double g[3][3];
         for (int d = 0; d < 3; ++d)
           for (int a = 0; a < 3; ++a) g[d][a] = ld(m + d + 3 * a);
@@ -657,7 +657,7 @@ MB_HD double cell_dt(const Params& p, const DBlk& b, long long l, const double* 
       dtc = p.cfl / ra_c;
     }
   } else {
-    for (int d = 0; d < p.ndir; ++d) {
+    for (int d = 0; d < b.ndir; ++d) {
       double m0 = ld(m + d), m1 = ld(m + d + 3), m2 = ld(m + d + 6);
       double nrm = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
       double v0 = m0 / nrm, v1 = m1 / nrm, v2 = m2 / nrm;
@@ -671,7 +671,7 @@ MB_HD double cell_dt(const Params& p, const DBlk& b, long long l, const double* 
       double td = Tc - (double)ti, mil, kl;
       wilke(p, pl[0], rho, ti, td, mil, kl);
       double mi = 0.0 + mil;
-      for (int d = 0; d < p.ndir; ++d) {
+      for (int d = 0; d < b.ndir; ++d) {
         double dlv = ld(dl + d);
         double dtd = (rho * (dlv * dlv) * p.vnn) / mi;
         dtc = mn(dtd, dtc);
@@ -682,7 +682,7 @@ MB_HD double cell_dt(const Params& p, const DBlk& b, long long l, const double* 
 }
 
 // min over the CTA of a positive double, then one atomic into the device clock
-__device__ __forceinline__ void cta_min_dt(const Params& p, double v, double* sred) {
+__device__ __forceinline__ void cta_min_dt(DevState* st, double v, double* sred) {
   const unsigned full = 0xffffffffu;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = mn(v, __shfl_xor_sync(full, v, o));
@@ -693,29 +693,31 @@ __device__ __forceinline__ void cta_min_dt(const Params& p, double v, double* sr
     v = (lane < nw) ? sred[lane] : 1e300;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = mn(v, __shfl_xor_sync(full, v, o));
-    if (lane == 0 && v < 1e300) atomicMin(&p.st->dtmin_bits, (unsigned long long)__double_as_longlong(v));
+    if (lane == 0 && v < 1e300) atomicMin(&st->dtmin_bits, (unsigned long long)__double_as_longlong(v));
   }
 }
 
-__device__ __forceinline__ void report_bad_state(const Params& p, int blk, int i, int j, int k) {
-  atomicAdd(&p.st->n_bad_state, 1);
-  if (atomicCAS(&p.st->first_bad_claimed, 0, 1) == 0) {
-    p.st->bad_blk = blk; p.st->bad_i = i; p.st->bad_j = j; p.st->bad_k = k;
+__device__ __forceinline__ void report_bad_state(DevState* st, int blk, int i, int j, int k) {
+  atomicAdd(&st->n_bad_state, 1);
+  if (atomicCAS(&st->first_bad_claimed, 0, 1) == 0) {
+    st->bad_blk = blk; st->bad_i = i; st->bad_j = j; st->bad_k = k;
   }
 }
 
 // ---------------------------------------------------------------------------------------------
-// Stage plane kk of the tile window: cells (i0-2 .. i0+33) x (j0-2 .. j0+TY+1), those inside the padded block.
+// Stage plane kk of the tile window: cells (i0-2 .. i0+33) x (j0-2 .. j0+TY+1), those inside the padded block and
+// within jext rows of the interior (jext < 2 for a block one cell deep in j: no j-faces, so only the viscous
+// transverse stencil reads the ghost rows).
 template <typename R, int TY>
 __device__ __forceinline__ void stage_plane(const Params& p, const DBlk& b, const double* __restrict__ P,
-                                            const Tile<R, TY>& T, int i0, int j0, int kk) {
+                                            const Tile<R, TY>& T, int i0, int j0, int kk, int jext) {
   const int sl = slot_of(kk);
   const long long nc = p.nc;
   for (int c = threadIdx.x; c < TXH * (TY + 4); c += blockDim.x) {
     const int jj = c / TXH, ii = c - jj * TXH;
     const int i = i0 - 2 + ii, j = j0 - 2 + jj;
     R vals[NV] = {(R)0, (R)0, (R)0, (R)0, (R)0, (R)0};
-    if (i >= 1 - GC && i <= b.n1 + GC && j >= 1 - GC && j <= b.n2 + GC) {
+    if (i >= 1 - GC && i <= b.n1 + GC && j >= 1 - jext && j <= b.n2 + jext) {
       const long long r = row(b, i, j, kk);
 #pragma unroll
       for (int s = 0; s < MB_NP; ++s) vals[s] = cvt<R>(ld(P + r + s * nc));
@@ -729,13 +731,12 @@ __device__ __forceinline__ void stage_plane(const Params& p, const DBlk& b, cons
   }
 }
 
-// MINB: resident CTAs per SM the register allocation must allow (launch bounds)
-template <typename R, int TY, bool VISC, int MODE, int RS, int LIM, int MINB>
-__global__ void __launch_bounds__(32 * TY, MINB)
-k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pin, const double* Pold, double* Pout,
-        double* Rout, double rkc, int last) {
+// One tile of the fused stage (the body of k_sweep).
+template <typename R, int TY, bool VISC, int MODE, int RS, int LIM>
+__device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const double* __restrict__ Pin,
+                                           const double* Pold, double* Pout, double* Rout, double rkc, int last,
+                                           unsigned char* smem_raw, double* sred) {
   constexpr int NF = VISC ? 2 * MB_NP : MB_NP;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   typedef R RowI[33][NF];
   typedef R RowJ[32][NF];
   Tile<R, TY> T;
@@ -744,19 +745,23 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
   RowI* sFi = reinterpret_cast<RowI*>(fbase);                                     // [TY][33][NF]
   RowJ* sFj = reinterpret_cast<RowJ*>(fbase + sizeof(R) * TY * 33 * NF);          // [TY+1][32][NF]
   RowJ* sFk0 = reinterpret_cast<RowJ*>(fbase + sizeof(R) * (TY * 33 + (TY + 1) * 32) * NF);  // [2][TY][32][NF]
-  __shared__ double sred[32];
-  const DTile t = tiles[blockIdx.x];
   const DBlk b = p.blk[t.blk];
+  DevState* st = p.st + b.grp;
+  if (MODE == MODE_UPDATE && st->done) return;  // the case has reached its stop time (uniform over the CTA)
   const int tid = threadIdx.x;
   const int tx = tid & 31, ty = tid >> 5;
   const int i = t.i0 + tx, j = t.j0 + ty;
   const bool own = (i <= b.n1) && (j <= b.n2);
-  const double dt = (MODE == MODE_UPDATE) ? p.st->dt : 0.0;
+  const double dt = (MODE == MODE_UPDATE) ? st->dt : 0.0;
   double dtloc = 1e300;
   int kb = 0;  // buffer of the k-face above the current plane
+  // ghost layers the stencils read: 2 along an axis with faces; for a block one cell deep along j or k (2-D,
+  // 1-D) no face of that axis exists and only the viscous transverse gradient reads one ghost layer
+  const int jext = (b.n2 > 1) ? GC : (VISC ? 1 : 0);
+  const int kext = (b.n3 > 1) ? GC : (VISC ? 1 : 0);
   // prologue: planes k0-2 .. k0+1, and the k-face below the first plane
   for (int kk = t.k0 - 2; kk <= t.k0 + 1; ++kk)
-    if (kk >= 1 - GC && kk <= b.n3 + GC) stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, kk);
+    if (kk >= 1 - kext && kk <= b.n3 + kext) stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, kk, jext);
   __syncthreads();
   if (own && t.k0 > 1) {
     R out[NF];
@@ -767,7 +772,7 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
   }
   for (int k = t.k0; k < t.k1; ++k) {
     __syncthreads();  // the slot of plane k-2 is free
-    if (k + 2 <= b.n3 + GC) stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, k + 2);
+    if (k + 2 <= b.n3 + kext) stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, k + 2, jext);
     __syncthreads();
     // ---- face tasks of this plane through one call site: 0 = i-face #tid, 1 = extra i-faces (last warp,
     // lanes < TY), 2 = j-face #tid, 3 = extra j-face row (warp 0), 4 = the k-face above
@@ -844,7 +849,7 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
         double rho, Tc;
         cell_rho_T(p, pc[0], pc[MB_IPR], rho, Tc);
         if (p.guard && !(Tc > 1.0 && Tc < 9990.0)) {  // thermo guard (Mod_Thermo_Cache.f90:317-327)
-          atomicAdd(&p.st->n_bad_thermo, 1);
+          atomicAdd(&st->n_bad_thermo, 1);
           if (Tc != Tc) Tc = 300.0;
           Tc = mn(mx(Tc, 1.0), 9990.0);
         }
@@ -853,7 +858,7 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
         bool bad = !(pn[MB_IPR] >= 0.0);
 #pragma unroll
         for (int s = 0; s < MB_NP; ++s) bad = bad || !isfinite(pn[s]);
-        if (bad) report_bad_state(p, t.blk, i, j, k);
+        if (bad) report_bad_state(st, t.blk, i, j, k);
 #pragma unroll
         for (int s = 0; s < MB_NP; ++s) Pout[r + s * p.nc] = pn[s];
         if (last) dtloc = mn(dtloc, cell_dt(p, b, r - b.boff, pn));
@@ -861,7 +866,32 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
     }
     kb ^= 1;
   }
-  if (MODE == MODE_UPDATE && last) cta_min_dt(p, dtloc, sred);
+  if (MODE == MODE_UPDATE && last) cta_min_dt(st, dtloc, sred);
+}
+
+// The fused stage over a tile list. p.queue == null: one CTA per tile (grid = ntiles). Otherwise a persistent
+// work queue: a grid of about one wave of CTAs, each taking the next tile from the counter p.queue (zeroed
+// before the launch) until the list is exhausted. MINB: resident CTAs per SM the register allocation must
+// allow (launch bounds).
+template <typename R, int TY, bool VISC, int MODE, int RS, int LIM, int MINB>
+__global__ void __launch_bounds__(32 * TY, MINB)
+k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pin, const double* Pold, double* Pout,
+        double* Rout, double rkc, int last) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double sred[32];
+  __shared__ int s_next;
+  if (!p.queue) {
+    sweep_tile<R, TY, VISC, MODE, RS, LIM>(p, tiles[blockIdx.x], Pin, Pold, Pout, Rout, rkc, last, smem_raw, sred);
+    return;
+  }
+  for (;;) {
+    if (threadIdx.x == 0) s_next = atomicAdd(p.queue, 1);
+    __syncthreads();
+    const int tix = s_next;
+    if (tix >= p.ntiles_run) break;
+    sweep_tile<R, TY, VISC, MODE, RS, LIM>(p, tiles[tix], Pin, Pold, Pout, Rout, rkc, last, smem_raw, sred);
+    __syncthreads();  // the tile's shared memory is free and s_next may be overwritten
+  }
 }
 
 template <typename R, int TY, bool VISC>

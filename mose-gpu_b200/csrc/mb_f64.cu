@@ -71,10 +71,13 @@ __global__ void k_pg(const long long* __restrict__ src, int nconn, long long nc,
 }
 
 // ---- Compute_dt alone: local dt of every interior cell, reduced into the device clock ----
-__global__ void __launch_bounds__(32 * TY_AUX) k_dt(Params p, const DTile* __restrict__ tiles, const double* P) {
+// only_group >= 0: the cells of that case only (its first dt after mb_group_reset)
+__global__ void __launch_bounds__(32 * TY_AUX) k_dt(Params p, const DTile* __restrict__ tiles, const double* P,
+                                                    int only_group) {
   __shared__ double sred[32];
   const DTile t = tiles[blockIdx.x];
   const DBlk b = p.blk[t.blk];
+  if (only_group >= 0 && b.grp != only_group) return;
   const int i = t.i0 + (threadIdx.x & 31), j = t.j0 + (threadIdx.x >> 5);
   double v = 1e300;
   if (i <= b.n1 && j <= b.n2) {
@@ -85,7 +88,7 @@ __global__ void __launch_bounds__(32 * TY_AUX) k_dt(Params p, const DTile* __res
       v = mn(v, cell_dt(p, b, r - b.boff, pl));
     }
   }
-  cta_min_dt(p, v, sred);
+  cta_min_dt(p.st + b.grp, v, sred);
 }
 
 // ---- RK_Newstate alone: the conservative update of every interior cell from a given residual ----
@@ -93,6 +96,7 @@ __global__ void __launch_bounds__(32 * TY_AUX) k_update(Params p, const DTile* _
                                                         const double* PO, const double* R, double rkc, double dt) {
   const DTile t = tiles[blockIdx.x];
   const DBlk b = p.blk[t.blk];
+  DevState* st = p.st + b.grp;
   const int i = t.i0 + (threadIdx.x & 31), j = t.j0 + (threadIdx.x >> 5);
   if (i > b.n1 || j > b.n2) return;
   for (int k = t.k0; k < t.k1; ++k) {
@@ -102,14 +106,14 @@ __global__ void __launch_bounds__(32 * TY_AUX) k_update(Params p, const DTile* _
     double rho, T;
     cell_rho_T(p, pc[0], pc[MB_IPR], rho, T);
     if (p.guard && !(T > 1.0 && T < 9990.0)) {
-      atomicAdd(&p.st->n_bad_thermo, 1);
+      atomicAdd(&st->n_bad_thermo, 1);
       if (T != T) T = 300.0;
       T = mn(mx(T, 1.0), 9990.0);
     }
     cons_update(p, pc, po, res, ld(b.vol + (r - b.boff)), dt, rkc, T, pn, r);
     bool bad = !(pn[MB_IPR] >= 0.0);
     for (int s = 0; s < MB_NP; ++s) bad = bad || !isfinite(pn[s]);
-    if (bad) report_bad_state(p, t.blk, i, j, k);
+    if (bad) report_bad_state(st, t.blk, i, j, k);
     for (int s = 0; s < MB_NP; ++s) P[r + s * p.nc] = pn[s];
   }
 }
@@ -124,23 +128,45 @@ cudaError_t to_float(const double* src, float* dst, long long n, cudaStream_t s)
   return cudaGetLastError();
 }
 
-__global__ void k_reset_dt(Params p) { p.st->dtmin_bits = (unsigned long long)__double_as_longlong(1e300); }
+__global__ void k_reset_dt(Params p, int only_group) {
+  for (int g = threadIdx.x; g < p.ngroups; g += blockDim.x)
+    if (only_group < 0 || g == only_group) p.st[g].dtmin_bits = (unsigned long long)__double_as_longlong(1e300);
+}
 
-// the step's dt (Compute_dt's dtglobal = 1e5 then the cell minimum, Mod_Explicit.f90:122; Set_Global_dt;
-// Clip_dt_To_Timemax, Mod_dt.f90:283-296), the simulated time, and a fresh minimum for the next step
-__global__ void k_clock(Params p, int time_clip, double threshold) {
-  DevState* st = p.st;
-  double dtg = 1e5;
-  double dm = __longlong_as_double((long long)st->dtmin_bits);
-  dtg = mn(dm, dtg);
-  if (time_clip) {
-    double rem = threshold - st->time;
-    if (rem > 0.0 && dtg > rem) dtg = rem * (1.0 + 1e-12);
+// the step's dt of every case (Compute_dt's dtglobal = 1e5 then the cell minimum, Mod_Explicit.f90:122;
+// Set_Global_dt; Clip_dt_To_Timemax, Mod_dt.f90:283-296), its simulated time, and a fresh minimum for the
+// next step. A case whose time has reached its stop time (the reference's time-loop exit) is marked done and
+// no longer advances.
+__global__ void k_clock(Params p) {
+  for (int g = threadIdx.x; g < p.ngroups; g += blockDim.x) {
+    DevState* st = p.st + g;
+    if (st->done) continue;
+    if (st->t_end > 0.0 && st->time >= st->t_end) {
+      st->done = 1;
+      continue;
+    }
+    double dtg = 1e5;
+    double dm = __longlong_as_double((long long)st->dtmin_bits);
+    dtg = mn(dm, dtg);
+    if (st->time_clip) {
+      double rem = st->t_end - st->time;
+      if (rem > 0.0 && dtg > rem) dtg = rem * (1.0 + 1e-12);
+    }
+    st->dt = dtg;
+    st->time = st->time + dtg;
+    st->steps = st->steps + 1;
+    st->dtmin_bits = (unsigned long long)__double_as_longlong(1e300);
   }
-  st->dt = dtg;
-  st->time = st->time + dtg;
-  st->steps = st->steps + 1;
+}
+
+// mb_group_reset: case g starts afresh with its stop rule
+__global__ void k_group_reset(Params p, int g, int time_clip, double t_end) {
+  DevState* st = p.st + g;
   st->dtmin_bits = (unsigned long long)__double_as_longlong(1e300);
+  st->dt = 0.0; st->time = 0.0; st->steps = 0; st->code = 0;
+  st->n_bad_state = 0; st->n_bad_thermo = 0;
+  st->bad_blk = 0; st->bad_i = 0; st->bad_j = 0; st->bad_k = 0; st->first_bad_claimed = 0;
+  st->time_clip = time_clip; st->done = 0; st->t_end = t_end;
 }
 
 // ---- launchers ----
@@ -161,8 +187,9 @@ cudaError_t ghost_fill(const Params& p, const GhostLists& g, double* P, cudaStre
   return cudaGetLastError();
 }
 
-cudaError_t dt_cells(const Params& p, const DTile* tiles, int ntiles, const double* P, cudaStream_t s) {
-  k_dt<<<ntiles, 32 * TY_AUX, 0, s>>>(p, tiles, P);
+cudaError_t dt_cells(const Params& p, const DTile* tiles, int ntiles, const double* P, cudaStream_t s,
+                     int only_group) {
+  k_dt<<<ntiles, 32 * TY_AUX, 0, s>>>(p, tiles, P, only_group);
   return cudaGetLastError();
 }
 
@@ -172,13 +199,18 @@ cudaError_t update_cells(const Params& p, const DTile* tiles, int ntiles, double
   return cudaGetLastError();
 }
 
-cudaError_t reset_dt(const Params& p, cudaStream_t s) {
-  k_reset_dt<<<1, 1, 0, s>>>(p);
+cudaError_t reset_dt(const Params& p, cudaStream_t s, int only_group) {
+  k_reset_dt<<<1, 256, 0, s>>>(p, only_group);
   return cudaGetLastError();
 }
 
-cudaError_t clock_step(const Params& p, int time_clip, double threshold, cudaStream_t s) {
-  k_clock<<<1, 1, 0, s>>>(p, time_clip, threshold);
+cudaError_t clock_step(const Params& p, cudaStream_t s) {
+  k_clock<<<1, 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t group_reset(const Params& p, int g, int time_clip, double t_end, cudaStream_t s) {
+  k_group_reset<<<1, 1, 0, s>>>(p, g, time_clip, t_end);
   return cudaGetLastError();
 }
 

@@ -50,11 +50,13 @@ MB_DECLARE_SWEEP(sweep_f32_rs12)
 
 // ghost fill; *nl receives the number of kernels launched
 cudaError_t ghost_fill(const Params& p, const GhostLists& g, double* P, cudaStream_t s, int* nl);
-cudaError_t dt_cells(const Params& p, const DTile* tiles, int ntiles, const double* P, cudaStream_t s);
+cudaError_t dt_cells(const Params& p, const DTile* tiles, int ntiles, const double* P, cudaStream_t s,
+                     int only_group = -1);
 cudaError_t update_cells(const Params& p, const DTile* tiles, int ntiles, double* P, const double* PO,
                          const double* R, double rkc, double dt, cudaStream_t s);
-cudaError_t reset_dt(const Params& p, cudaStream_t s);
+cudaError_t reset_dt(const Params& p, cudaStream_t s, int only_group = -1);
 cudaError_t to_float(const double* src, float* dst, long long n, cudaStream_t s);
-cudaError_t clock_step(const Params& p, int time_clip, double threshold, cudaStream_t s);
+cudaError_t clock_step(const Params& p, cudaStream_t s);
+cudaError_t group_reset(const Params& p, int g, int time_clip, double t_end, cudaStream_t s);
 
 }  // namespace mb

@@ -129,6 +129,7 @@ extern "C" int mb_dt_block_noalloc(const double* P, int64_t ncell_total, int64_t
   memset(&b, 0, sizeof(b));
   b.n1 = n[0]; b.n2 = n[1]; b.n3 = n[2];
   b.pi = (int)pi; b.pj = (int)pj;
+  b.grp = 0; b.ndir = sc->ndir;
   b.boff = boff;
   b.dl = dl;
   b.m = m;

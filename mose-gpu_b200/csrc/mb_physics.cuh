@@ -36,6 +36,8 @@ constexpr double RUNIV = 8314.46261815324;  // lib/FLINT/src/lib/Lib_ThermoTrans
 
 struct DBlk {
   int n1, n2, n3, pi, pj;
+  int grp;              // the case of the block (its clock: Params::st[grp])
+  int ndir;             // computational directions of the case (the dt rule)
   int rmap[6];          // offset of each face's record map in Params::rec_map (-1: none)
   long long boff;
   const double *fm1, *fm2, *fm3, *dl, *m, *vol;
@@ -75,6 +77,9 @@ struct DevState {
   int n_bad_thermo;
   int bad_blk, bad_i, bad_j, bad_k;
   int first_bad_claimed;
+  int time_clip;                  // the case's stop rule: clip the last step onto t_end
+  int done;                       // the case reached t_end: its tiles are skipped
+  double t_end;                   // 0: no stop
 };
 
 struct Params {
@@ -84,12 +89,16 @@ struct Params {
   const double* pg;        // [record][6][5]
   const double *cp, *h, *mu, *k;      // FP64 tables, indexed by the table row (pointer shifted by -tmin)
   const float *cpf, *hf, *muf, *kf;   // FP32 copies for the mixed form
-  DevState* st;
+  DevState* st;            // one clock per case: st[DBlk::grp]
+  int ngroups;
   long long nc;
   int tmin, tmax;
   double wm, ri;
   int lim, rs, visc, ndir, dt_additive, guard, state_check;
   double cfl, vnn, prandtl, schmidt, mco;
+  int* queue;              // persistent sweep: the tile counter (null: one CTA per tile)
+  int ntiles_run;          // tiles of the launch (persistent sweep)
+  int pgrid;               // CTAs of a persistent launch (resident CTAs per SM x SMs)
   int n_rk;                // 4: classical RK4 through the accumulator acc4
   int irk;                 // stage of the launch (1-based; set per launch)
   double* acc4;            // RK4: conserved accumulator (nc, 5), null otherwise

@@ -42,7 +42,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 
 
 class MBBlock(C.Structure):
-    _fields_ = [("n", C.c_int32 * 3), ("pad0", C.c_int32), ("boff", C.c_int64),
+    _fields_ = [("n", C.c_int32 * 3), ("group", C.c_int32), ("boff", C.c_int64),
                 ("fm1", C.c_void_p), ("fm2", C.c_void_p), ("fm3", C.c_void_p),
                 ("dl", C.c_void_p), ("m", C.c_void_p), ("vol", C.c_void_p)]
 
@@ -60,7 +60,7 @@ class MBConn(C.Structure):
 
 
 class MBMesh(C.Structure):
-    _fields_ = [("nblk", C.c_int32), ("nrec", C.c_int32), ("nconn", C.c_int32), ("pad0", C.c_int32),
+    _fields_ = [("nblk", C.c_int32), ("nrec", C.c_int32), ("nconn", C.c_int32), ("ngroups", C.c_int32),
                 ("ncell_total", C.c_int64), ("blk", C.POINTER(MBBlock)), ("rec", C.c_void_p),
                 ("conn", C.c_void_p)]
 
@@ -82,7 +82,12 @@ class MBScheme(C.Structure):
 class MBStatus(C.Structure):
     _fields_ = [("code", C.c_int32), ("n_bad_state", C.c_int32), ("n_bad_thermo", C.c_int32),
                 ("bad_blk", C.c_int32), ("bad_i", C.c_int32), ("bad_j", C.c_int32), ("bad_k", C.c_int32),
-                ("steps", C.c_int32), ("time", C.c_double), ("dt", C.c_double)]
+                ("steps", C.c_int32), ("time", C.c_double), ("dt", C.c_double), ("done", C.c_int32),
+                ("pad0", C.c_int32)]
+
+
+class MBGroup(C.Structure):
+    _fields_ = [("time_clip", C.c_int32), ("pad0", C.c_int32), ("t_end", C.c_double)]
 
 
 BC_DTYPE = np.dtype([("blk", "<i4"), ("i", "<i4"), ("j", "<i4"), ("k", "<i4"), ("face", "<i4"),

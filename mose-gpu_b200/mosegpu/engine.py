@@ -45,11 +45,18 @@ def load_library():
     L.mb_begin_step.argtypes = [vp, vp, vp]
     L.mb_get_status.argtypes = [vp, C.POINTER(abi.MBStatus)]
     L.mb_profile_stage.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), vp]
+    L.mb_reconfigure.argtypes = [vp, C.POINTER(abi.MBMesh)]
+    L.mb_group_reset.argtypes = [vp, C.c_int, C.POINTER(abi.MBGroup), vp, vp]
+    L.mb_get_group_status.argtypes = [vp, C.c_int, C.c_int, C.POINTER(abi.MBStatus)]
+    L.mb_autotune.argtypes = [vp, vp, vp]
+    L.mb_set_tuning.argtypes = [vp, C.c_int, C.c_int]
+    L.mb_get_tuning.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)]
     L.mb_launch_count.argtypes = [vp]
     L.mb_launch_count.restype = C.c_int64
     L.mb_version.restype = C.c_char_p
     for f in ("mb_fill_ghosts", "mb_residual", "mb_update", "mb_dt", "mb_stage", "mb_step", "mb_begin_step",
-              "mb_get_status", "mb_profile_stage"):
+              "mb_get_status", "mb_profile_stage", "mb_reconfigure", "mb_group_reset", "mb_get_group_status",
+              "mb_autotune", "mb_set_tuning", "mb_get_tuning"):
         getattr(L, f).restype = C.c_int
     _lib = L
     return L
@@ -174,6 +181,19 @@ class Engine:
         _check(self.lib.mb_profile_stage(self.ctx, self.P.data_ptr(), self.PO.data_ptr(), irk, nrep, C.byref(g),
                                          C.byref(w), self._s()), "mb_profile_stage")
         return g.value, w.value
+
+    def autotune(self):
+        """Runs the sweep autotuner on the current state; returns (k-chunk, persistent, sweep ms)."""
+        _check(self.lib.mb_autotune(self.ctx, self.P.data_ptr(), self._s()), "mb_autotune")
+        return self.tuning()
+
+    def set_tuning(self, kchunk, persistent):
+        _check(self.lib.mb_set_tuning(self.ctx, kchunk, 1 if persistent else 0), "mb_set_tuning")
+
+    def tuning(self):
+        k, q, ms = C.c_int(), C.c_int(), C.c_float()
+        _check(self.lib.mb_get_tuning(self.ctx, C.byref(k), C.byref(q), C.byref(ms)), "mb_get_tuning")
+        return k.value, q.value, ms.value
 
     def status(self):
         st = abi.MBStatus()

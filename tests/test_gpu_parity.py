@@ -164,3 +164,47 @@ def test_thermo_guard_reports_off_table_temperature(torch_cuda):
     eng.step(1, graph=False)
     st = eng.status()
     assert st.code == abi.MB_E_THERMO and st.n_bad_thermo > 0
+
+
+@pytest.mark.parametrize("kchunk,persistent", [(8, 0), (32, 1), (5, 1)])
+def test_tile_configuration_does_not_change_results(torch_cuda, kchunk, persistent):
+    """The k-chunk of the tiles and the persistent work queue change only which CTA computes a face: the state
+    after several steps is bit-identical to the default configuration, on a 3-D multi-block case and on the
+    2-D wall / inlet batch; the autotuner's choice likewise."""
+    from mosegpu import case as cs
+    from mosegpu.engine import Engine
+    for case in (cs.taylor_green(n=24, blocks=2, riemann=abi.RS_HLLC), cs.multiblock_2d(cols=2, rows=2, lo=9, hi=20,
+                                                                                      seed=2)):
+        a, b = Engine(case), Engine(case)
+        b.set_tuning(kchunk, persistent)
+        assert b.tuning()[:2] == (kchunk, persistent)
+        a.step(4, graph=True)
+        b.step(4, graph=True)
+        m = case.interior_mask()
+        assert np.array_equal(a.state()[:, m], b.state()[:, m])
+        c = Engine(case)
+        k, q, ms = c.autotune()
+        assert k in (8, 16, 32, 64) and q in (0, 1) and ms > 0
+        c.step(4, graph=True)
+        assert np.array_equal(a.state()[:, m], c.state()[:, m])
+        assert a.status().time == b.status().time == c.status().time
+
+
+def test_multiblock_2d_many_steps_fp64_and_mixed(torch_cuda):
+    """The 2-D wall / inlet batch (RK4, AUSM+, van Leer) for 30 steps: FP64 = oracle within the many-step gate,
+    the mixed form within L2(rho) 1e-5 of FP64."""
+    import oracle
+    from mosegpu import case as cs
+    from mosegpu.engine import Engine
+    case = cs.multiblock_2d(cols=3, rows=2, lo=16, hi=40, seed=9)
+    orc = oracle.Oracle(case)
+    P = case.P0.copy()
+    assert orc.step(P, 30) == 0
+    a = Engine(case, precision=abi.PREC_FP64)
+    b = Engine(case, precision=abi.PREC_MIXED)
+    a.step(30, graph=True)
+    b.step(30, graph=True)
+    e = H.rel_err(H.conserved(case, a.state()), H.conserved(case, P))
+    assert np.all(e <= TOL_MANY), e
+    l1, l2, li = H.norms(H.conserved(case, b.state()), H.conserved(case, a.state()))
+    assert l2[0] < 1e-5, l2
