@@ -231,9 +231,10 @@ int mb_step(mb_ctx* ctx, double* P, double* PO, int nsteps, int use_graph, void*
  * Set_Global_dt + Clip_dt_To_Timemax), without a host read. Called before the first mb_stage. */
 int mb_begin_step(mb_ctx* ctx, const double* P, void* stream);
 
-/* Measurement hook: runs stage irk (ghost fill + fused sweep, as mb_stage) nrep times on the stream and
- * returns the average device time of the ghost fill and of the sweep kernel in milliseconds, each taken
- * with CUDA events recorded around the launches on that stream. Advances the state like mb_stage. */
+/* Measurement hook: runs stage irk (ghost fill + boundary records + fused sweep, as mb_stage) nrep times on the
+ * stream and returns the average device time of the surface work (ghost fill and boundary records) and of the
+ * sweep kernel in milliseconds, each taken with CUDA events recorded around the launches on that stream.
+ * Advances the state like mb_stage. */
 int mb_profile_stage(mb_ctx* ctx, double* P, double* PO, int irk, int nrep, float* ms_ghost, float* ms_sweep,
                      void* stream);
 

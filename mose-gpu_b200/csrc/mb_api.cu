@@ -28,6 +28,10 @@ struct mb_ctx {
   long long* d_csrc = nullptr;
   long long* d_pgsrc = nullptr;
   double* d_pg = nullptr;
+  double* d_recflux = nullptr;  // boundary-record contributions [nrec][10] (flux type)
+  int* d_brec = nullptr;        // records in type order (the record kernel's work list)
+  int* d_bcell = nullptr;       // their blk, i, j, k, face
+  int nrec = 0;
   double* d_tab = nullptr;
   float* d_tabf = nullptr;
   DevState* d_st = nullptr;
@@ -80,7 +84,7 @@ static void free_ctx(mb_ctx* c) {
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   if (c->graph) cudaGraphDestroy(c->graph);
   void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
-                  c->d_pgsrc, c->d_pg, c->d_tab, c->d_tabf, c->d_st, c->d_tiles_sweep, c->d_tiles_aux, c->d_scratch, c->d_acc4, c->d_queue};
+                  c->d_pgsrc, c->d_pg, c->d_tab, c->d_tabf, c->d_st, c->d_tiles_sweep, c->d_tiles_aux, c->d_scratch, c->d_acc4, c->d_queue, c->d_recflux, c->d_brec, c->d_bcell};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& q : c->geo32)
@@ -166,9 +170,10 @@ static int check_mesh(const mb_mesh* mesh, int ngroups) {
 // frees the mesh-dependent device tables (blocks, record maps, records, ghost lists, tiles, FP32 geometry)
 static void free_tables(mb_ctx* c) {
   void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
-                  c->d_pgsrc, c->d_pg, c->d_tiles_sweep, c->d_tiles_aux};
+                  c->d_pgsrc, c->d_pg, c->d_tiles_sweep, c->d_tiles_aux, c->d_recflux, c->d_brec, c->d_bcell};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  c->d_recflux = nullptr; c->d_brec = nullptr; c->d_bcell = nullptr; c->nrec = 0;
   c->d_blk = nullptr; c->d_recmap = nullptr; c->d_rec = nullptr; c->d_grec = nullptr; c->d_phys = nullptr;
   c->d_cubic = nullptr; c->d_cdst = nullptr; c->d_csrc = nullptr; c->d_pgsrc = nullptr; c->d_pg = nullptr;
   c->d_tiles_sweep = nullptr; c->d_tiles_aux = nullptr;
@@ -234,6 +239,15 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
     hg[q] = GRec{r.blk, r.i, r.j, r.k, r.face, r.type};
     if (r.type == MB_BC_EXTRAPOLATION || r.type == MB_BC_INFLOW || r.type == MB_BC_WALL) phys.push_back(q);
     if (r.type == MB_BC_EXTRAPOLATION) cubic.push_back(q);
+  }
+  // the record kernel's work list: records grouped by type (one code path per warp where possible)
+  std::vector<int> brec(mesh->nrec), bcell(5 * (size_t)mesh->nrec);
+  for (int q = 0; q < mesh->nrec; ++q) brec[q] = q;
+  std::stable_sort(brec.begin(), brec.end(), [&](int a, int b) { return mesh->rec[a].type < mesh->rec[b].type; });
+  for (int q = 0; q < mesh->nrec; ++q) {
+    const mb_bc& r = mesh->rec[brec[q]];
+    const int v[5] = {r.blk, r.i, r.j, r.k, r.face};
+    for (int a = 0; a < 5; ++a) bcell[5 * q + a] = v[a];
   }
   // ---- connections: ghost copies (2 layers) and the bc_pg source rows
   auto rowof = [&](int b, int i, int j, int k) -> long long {
@@ -331,12 +345,19 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   if ((rc = upload(&c->d_pgsrc, pgsrc.data(), pgsrc.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_tiles_sweep, ts.data(), ts.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_tiles_aux, ta.data(), ta.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_brec, brec.data(), brec.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_bcell, bcell.data(), bcell.size())) != MB_OK) return rc;
+  c->nrec = mesh->nrec;
+  if (mesh->nrec > 0 &&
+      cudaMalloc((void**)&c->d_recflux, (size_t)mesh->nrec * 2 * MB_NPRIM * sizeof(double)) != cudaSuccess)
+    return MB_E_NOMEM;
   c->ntiles_sweep = (int)ts.size();
   c->ntiles_aux = (int)ta.size();
   if (mesh->nconn > 0 && cudaMalloc((void**)&c->d_pg, (size_t)mesh->nconn * 6 * MB_NPRIM * sizeof(double)) != cudaSuccess)
     return MB_E_NOMEM;
   Params& p = c->p;
   p.blk = c->d_blk; p.rec_map = c->d_recmap; p.rec = c->d_rec; p.pg = c->d_pg;
+  p.recflux = c->d_recflux;
   GhostLists& g = c->g;
   g.rec = c->d_grec; g.phys = c->d_phys; g.nphys = (int)phys.size(); g.cubic = c->d_cubic; g.ncubic = (int)cubic.size();
   g.cdst = c->d_cdst; g.csrc = c->d_csrc; g.ncopy = (int)cdst.size(); g.pgsrc = c->d_pgsrc; g.nconn = mesh->nconn;
@@ -537,6 +558,25 @@ static int sweep_on(mb_ctx* c, const DTile* t, int n, int persistent, int mode, 
   return MB_OK;
 }
 
+// the boundary records of the stage input (BC_Fluxes), before the sweep that adds them
+static int records(mb_ctx* c, const double* Pin, cudaStream_t s) {
+  if (c->nrec <= 0) return MB_OK;
+  const Params& p = c->p;
+  cudaError_t e;
+  if (c->sc.precision == MB_PREC_MIXED) {
+    if (c->sc.riemann == 1) e = sweep_f32_rs1_records(p, c->d_brec, c->d_bcell, c->nrec, Pin, s);
+    else if (c->sc.riemann == 4) e = sweep_f32_rs4_records(p, c->d_brec, c->d_bcell, c->nrec, Pin, s);
+    else e = sweep_f32_rs12_records(p, c->d_brec, c->d_bcell, c->nrec, Pin, s);
+  } else {
+    if (c->sc.riemann == 1) e = sweep_f64_rs1_records(p, c->d_brec, c->d_bcell, c->nrec, Pin, s);
+    else if (c->sc.riemann == 4) e = sweep_f64_rs4_records(p, c->d_brec, c->d_bcell, c->nrec, Pin, s);
+    else e = sweep_f64_rs12_records(p, c->d_brec, c->d_bcell, c->nrec, Pin, s);
+  }
+  c->launches += 1;
+  CK(e);
+  return MB_OK;
+}
+
 static int sweep(mb_ctx* c, int mode, const double* Pin, const double* Pold, double* Pout, double* Rout, int irk,
                  int last, cudaStream_t s) {
   return sweep_on(c, c->d_tiles_sweep, c->ntiles_sweep, c->persistent, mode, Pin, Pold, Pout, Rout, irk, last, s);
@@ -552,7 +592,8 @@ static int time_sweep(mb_ctx* c, const std::vector<DTile>& tl, int persistent, c
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  rc = sweep_on(c, d, (int)tl.size(), persistent, MODE_UPDATE, P, P, c->d_scratch, nullptr, 1, 0, s);
+  rc = records(c, P, s);
+  if (rc == MB_OK) rc = sweep_on(c, d, (int)tl.size(), persistent, MODE_UPDATE, P, P, c->d_scratch, nullptr, 1, 0, s);
   cudaEventRecord(e0, s);
   for (int q = 0; q < nrep && rc == MB_OK; ++q)
     rc = sweep_on(c, d, (int)tl.size(), persistent, MODE_UPDATE, P, P, c->d_scratch, nullptr, 1, 0, s);
@@ -585,6 +626,8 @@ int mb_fill_ghosts(mb_ctx* ctx, double* P, void* stream) {
 int mb_residual(mb_ctx* ctx, const double* P, double* R, void* stream) {
   if (!ctx || !P || !R) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
+  int rc = records(ctx, P, (cudaStream_t)stream);
+  if (rc != MB_OK) return rc;
   return sweep(ctx, MODE_RESIDUAL, P, nullptr, nullptr, R, 0, 0, (cudaStream_t)stream);
 }
 
@@ -641,6 +684,8 @@ static int stage(mb_ctx* c, double* P, double* PO, int irk, cudaStream_t s) {
   double* outp;
   stage_buffers(n, irk, P, PO, S, &in, &outp);
   int rc = fill(c, const_cast<double*>(in), s);
+  if (rc != MB_OK) return rc;
+  rc = records(c, in, s);
   if (rc != MB_OK) return rc;
   const int last = (irk == n) ? 1 : 0;
   rc = sweep(c, MODE_UPDATE, in, P, outp, nullptr, irk, last, s);
@@ -730,6 +775,7 @@ int mb_profile_stage(mb_ctx* ctx, double* P, double* PO, int irk, int nrep, floa
   for (int q = 0; q < nrep && rc == MB_OK; ++q) {
     cudaEventRecord(e0, s);
     rc = fill(ctx, const_cast<double*>(in), s);
+    if (rc == MB_OK) rc = records(ctx, in, s);
     cudaEventRecord(e1, s);
     if (rc == MB_OK) rc = sweep(ctx, MODE_UPDATE, in, P, outp, nullptr, irk, irk == n ? 1 : 0, s);
     cudaEventRecord(e2, s);

@@ -158,7 +158,7 @@ MB_HD void bc_face_geom(const DBlk& b, int Im, int Jm, int Km, int F, double* g)
 // BC_Connection_Eul_lean (Lib_BC.f90:1770-1867)
 template <typename R, int RS = 0, int LIM = 0>
 MB_HD_NOINLINE void bc_conn_eul(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
-                                         int Km, int Fm, double* acc) {
+                                         int Km, int Fm, R* A) {
   const long long nc = p.nc;
   const int rs = RS ? RS : p.rs;
   const int lim = LIM ? LIM : p.lim;
@@ -205,17 +205,17 @@ MB_HD_NOINLINE void bc_conn_eul(const Params& p, const DBlk& b, const double* __
   R su = copysign((R)0.5, F_r), selL = (R)0.5 + su, selR = su - (R)0.5;
   R Fmass = F_r * area;
   R sg = (R)modfm2;
-  acc[0] = acc[0] + (double)(sg * Fmass * (selL * PL[0] / rhoL - selR * PR[0] / rhoR));
-  acc[MB_IU] = acc[MB_IU] + (double)(sg * F_u * area);
-  acc[MB_IV] = acc[MB_IV] + (double)(sg * F_v * area);
-  acc[MB_IW] = acc[MB_IW] + (double)(sg * F_w * area);
-  acc[MB_IPR] = acc[MB_IPR] + (double)(sg * F_E * area);
+  A[0] = sg * Fmass * (selL * PL[0] / rhoL - selR * PR[0] / rhoR);
+  A[MB_IU] = sg * F_u * area;
+  A[MB_IV] = sg * F_v * area;
+  A[MB_IW] = sg * F_w * area;
+  A[MB_IPR] = sg * F_E * area;
 }
 
 // BC_Connection_Visc_lean (Lib_BC.f90:2113-2178); pg = bc_pg(:,1:6) of the record
 template <typename R>
 MB_HD_NOINLINE void bc_conn_visc(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
-                                          int Km, int Fm, const double* __restrict__ pg, double* acc) {
+                                          int Km, int Fm, const double* __restrict__ pg, R* S) {
   const long long nc = p.nc;
   int dir = (Fm + 1) / 2, modfm2 = 1 - 2 * (Fm % 2), gstep = 2 * (Fm % 2) - 1;
   int ia = dir - 1, ib, ic;
@@ -278,13 +278,13 @@ MB_HD_NOINLINE void bc_conn_visc(const Params& p, const DBlk& b, const double* _
   visc_flux(p, G2l, Pa, nx, ny, nz, area, rho_f, T_f, cp_f, mil_f, kl_f, Fl);
   visc_flux(p, G2g, Pa, nx, ny, nz, area, rho_f, T_f, cp_f, mil_f, kl_f, Fg);
 #pragma unroll
-  for (int s = 0; s < MB_NP; ++s) acc[s] = acc[s] - (double)((R)0.5 * (R)modfm2 * (Fl[s] + Fg[s]));
+  for (int s = 0; s < MB_NP; ++s) S[s] = (R)0.5 * (R)modfm2 * (Fl[s] + Fg[s]);
 }
 
 // BC_Extrapolation (Lib_BC.f90:1119-1165)
 template <typename R>
 MB_HD_NOINLINE void bc_extrap(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
-                                       int Km, int Fm, double* acc) {
+                                       int Km, int Fm, R* A) {
   const long long nc = p.nc;
   const long long r = row(b, Im, Jm, Km);
   R Pr[MB_NP];
@@ -305,7 +305,7 @@ MB_HD_NOINLINE void bc_extrap(const Params& p, const DBlk& b, const double* __re
   F[MB_IPR] = Fmass * H0(p, Pr[MB_IPR], Pr[0], vmag);
   R sg = (R)face_sign(Fm);
 #pragma unroll
-  for (int s = 0; s < MB_NP; ++s) acc[s] = acc[s] + (double)(sg * F[s]);
+  for (int s = 0; s < MB_NP; ++s) A[s] = sg * F[s];
 }
 
 // the Riemann dispatch of the record routines (Lib_Riemann.f90:120-140): HLLC Batten for rs 1, the MOSE_open
@@ -326,7 +326,7 @@ MB_HD void riemann_rec(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dl
 // the adiabatic wall and the closed-inlet fallback of the 405 record.
 template <typename R, int RS = 0, int LIM = 0>
 MB_HD_NOINLINE void bc_sym_eul(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km,
-                               int Fm, double* acc) {
+                               int Fm, R* A) {
   const long long nc = p.nc;
   const int lim = LIM ? LIM : p.lim;
   int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm1 = 1 - modfm, modfm2 = 1 - 2 * modfm, gstep = 2 * modfm - 1;
@@ -371,16 +371,18 @@ MB_HD_NOINLINE void bc_sym_eul(const Params& p, const DBlk& b, const double* __r
   R F_r, F_u, F_v, F_w, F_E;
   riemann_rec<R, RS>(p, F[0], U1[0], U1[1], U1[2], F[MB_IPR], Sound, rotot, Rtot, F[0], U4[0], U4[1], U4[2],
                      F[MB_IPR], Sound, rotot, Rtot, nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E);
-  acc[MB_IU] = acc[MB_IU] + (double)((R)modfm2 * F_u * area);
-  acc[MB_IV] = acc[MB_IV] + (double)((R)modfm2 * F_v * area);
-  acc[MB_IW] = acc[MB_IW] + (double)((R)modfm2 * F_w * area);
+  A[0] = (R)-0.0;  // an exact no-op when added: only the momentum rows change
+  A[MB_IU] = (R)modfm2 * F_u * area;
+  A[MB_IV] = (R)modfm2 * F_v * area;
+  A[MB_IW] = (R)modfm2 * F_w * area;
+  A[MB_IPR] = (R)-0.0;
 }
 
 // BC_Wall_Heat_dev (Lib_BC.f90:879-982), laminar adiabatic no-slip wall: the wall-normal velocity gradient of the
 // boundary cell, Grad . M of the cell, Stress_Vector_Std (Mod_Fluid.f90:20-44) with mu_t = 0; momentum rows only.
 template <typename R>
 MB_HD_NOINLINE void bc_wall_heat(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km,
-                                 int Fm, double* acc) {
+                                 int Fm, R* S) {
   const long long nc = p.nc;
   int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm2 = 1 - 2 * modfm, modfm3 = 2 * (2 * modfm - 1);
   const long long rb = row(b, Im, Jm, Km), l = rb - b.boff;
@@ -422,16 +424,18 @@ MB_HD_NOINLINE void bc_wall_heat(const Params& p, const DBlk& b, const double* _
   R S1 = txx * nx + txy * ny + txz * nz;
   R S2 = txy * nx + tyy * ny + tyz * nz;
   R S3 = txz * nx + tyz * ny + tzz * nz;
-  acc[MB_IU] = acc[MB_IU] - (double)((R)modfm2 * area * S1);
-  acc[MB_IV] = acc[MB_IV] - (double)((R)modfm2 * area * S2);
-  acc[MB_IW] = acc[MB_IW] - (double)((R)modfm2 * area * S3);
+  S[0] = (R)0;  // an exact no-op when subtracted: only the momentum rows change
+  S[MB_IU] = (R)modfm2 * area * S1;
+  S[MB_IV] = (R)modfm2 * area * S2;
+  S[MB_IW] = (R)modfm2 * area * S3;
+  S[MB_IPR] = (R)0;
 }
 
 // BC_Inflow_Outflow (Lib_BC.f90:1519-1597) of a 405 record: inward flow -> BC_Supersonic_Inflow (Lib_BC.f90:
 // 1247-1330), outward flow -> the face closes (BC_Symmetry_Eul).
 template <typename R, int RS = 0, int LIM = 0>
 MB_HD_NOINLINE void bc_inflow(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km,
-                              int Fm, const double* __restrict__ q, double* acc) {
+                              int Fm, const double* __restrict__ q, R* A) {
   const long long nc = p.nc;
   const int lim = LIM ? LIM : p.lim;
   int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm1 = 1 - modfm, modfm2 = 1 - 2 * modfm, gstep = 2 * modfm - 1;
@@ -448,7 +452,7 @@ MB_HD_NOINLINE void bc_inflow(const Params& p, const DBlk& b, const double* __re
   R InOut = (R)modfm2 * Un;
   if (BC_Mach < (R)0) InOut = (R)-1;
   if (InOut >= (R)0) {
-    bc_sym_eul<R, RS, LIM>(p, b, P, Im, Jm, Km, Fm, acc);
+    bc_sym_eul<R, RS, LIM>(p, b, P, Im, Jm, Km, Fm, A);
     return;
   }
   R frho, fR;
@@ -494,38 +498,68 @@ MB_HD_NOINLINE void bc_inflow(const Params& p, const DBlk& b, const double* __re
   Fl[0] = Fmass * (selL * PL[0] / rL - selR * PR[0] / rR);
   Fl[MB_IU] = F_u * area; Fl[MB_IV] = F_v * area; Fl[MB_IW] = F_w * area; Fl[MB_IPR] = F_E * area;
 #pragma unroll
-  for (int s = 0; s < MB_NP; ++s) acc[s] = acc[s] + (double)((R)modfm2 * Fl[s]);
+  for (int s = 0; s < MB_NP; ++s) A[s] = (R)modfm2 * Fl[s];
 }
 
-// the records of the faces 1..6 that the cell (i,j,k) lies on, in face order
+// The record (type, id) of the cell (i,j,k) on face F, -1 if none.
+MB_HD int record_of(const Params& p, const DBlk& b, int F, int i, int j, int k) {
+  if (b.rmap[F - 1] < 0) return -1;
+  const int ax = (F - 1) >> 1;
+  const int t = (ax == 0) ? (j - 1) + (k - 1) * b.n2 : (ax == 1 ? (i - 1) + (k - 1) * b.n1 : (i - 1) + (j - 1) * b.n1);
+  return p.rec_map[b.rmap[F - 1] + t];
+}
+
+// One boundary record (bc_record_apply.inc): its contributions to the cell's R row, in the flux type. A is added
+// and then, in Navier-Stokes, S is subtracted (the order of the reference's statements); components a record leaves
+// alone hold exact no-ops (-0 in A, +0 in S).
 template <typename R, bool VISC, int RS = 0, int LIM = 0>
-MB_HD void bc_cell(const Params& p, const DBlk& b, const double* __restrict__ P, int i, int j,
-                                        int k, double* acc) {
-  const int n[3] = {b.n1, b.n2, b.n3};
-  const int c[3] = {i, j, k};
-#pragma unroll 1
-  for (int F = 1; F <= 6; ++F) {
-    const int ax = (F - 1) >> 1;
-    const bool on = (F & 1) ? (c[ax] == 1) : (c[ax] == n[ax]);
-    if (!on || b.rmap[F - 1] < 0) continue;
-    int t;
-    if (ax == 0) t = (j - 1) + (k - 1) * b.n2;
-    else if (ax == 1) t = (i - 1) + (k - 1) * b.n1;
-    else t = (i - 1) + (j - 1) * b.n1;
-    const int rid = p.rec_map[b.rmap[F - 1] + t];
-    if (rid < 0) continue;
-    const DRec& rc = p.rec[rid];
-    if (rc.type == 1) {
-      bc_conn_eul<R, RS, LIM>(p, b, P, i, j, k, F, acc);
-      if (VISC) bc_conn_visc<R>(p, b, P, i, j, k, F, p.pg + (long long)rc.pg * 6 * MB_NP, acc);
-    } else if (rc.type == 11) {
-      bc_extrap<R>(p, b, P, i, j, k, F, acc);
-    } else if (rc.type == 5) {
-      bc_sym_eul<R, RS, LIM>(p, b, P, i, j, k, F, acc);
-      if (VISC) bc_wall_heat<R>(p, b, P, i, j, k, F, acc);
-    } else if (rc.type == 4) {
-      bc_inflow<R, RS, LIM>(p, b, P, i, j, k, F, rc.q, acc);
-    }
+MB_HD void bc_record(const Params& p, const DBlk& b, const double* __restrict__ P, int rid, int i, int j, int k, int F,
+                     R* A, R* S) {
+  const DRec& rc = p.rec[rid];
+  if (VISC)
+    for (int s = 0; s < MB_NP; ++s) S[s] = (R)0;
+  if (rc.type == 1) {
+    bc_conn_eul<R, RS, LIM>(p, b, P, i, j, k, F, A);
+    if (VISC) bc_conn_visc<R>(p, b, P, i, j, k, F, p.pg + (long long)rc.pg * 6 * MB_NP, S);
+  } else if (rc.type == 11) {
+    bc_extrap<R>(p, b, P, i, j, k, F, A);
+  } else if (rc.type == 5) {
+    bc_sym_eul<R, RS, LIM>(p, b, P, i, j, k, F, A);
+    if (VISC) bc_wall_heat<R>(p, b, P, i, j, k, F, S);
+  } else if (rc.type == 4) {
+    bc_inflow<R, RS, LIM>(p, b, P, i, j, k, F, rc.q, A);
+  } else {
+    for (int s = 0; s < MB_NP; ++s) A[s] = (R)-0.0;
+  }
+}
+
+// Every boundary record of the mesh, one thread each, from the stage input P (ghosts filled): the contributions
+// (A, S) of record q go to recflux[q][0..9] in the flux type; the sweep adds them in face order after the interior
+// sum (BC_Fluxes after Fluxes, Mod_Explicit.f90:187-189).
+template <typename R, bool VISC, int RS, int LIM>
+__global__ void __launch_bounds__(128) k_records(Params p, const int* __restrict__ brec, const int* __restrict__ bcell,
+                                               int nrec, const double* __restrict__ P) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nrec) return;
+  const int rid = brec[q];
+  const int* c = bcell + 5 * q;  // blk, i, j, k, face
+  const DBlk b = p.blk[c[0]];
+  if (p.st[b.grp].done) return;
+  R v[2 * MB_NP];
+  bc_record<R, VISC, RS, LIM>(p, b, P, rid, c[1], c[2], c[3], c[4], v, v + MB_NP);
+  R* out = reinterpret_cast<R*>(p.recflux) + (long long)rid * 2 * MB_NP;
+#pragma unroll
+  for (int s = 0; s < 2 * MB_NP; ++s) out[s] = (VISC || s < MB_NP) ? v[s] : (R)0;
+}
+
+// adds the record contributions of slot v (A = v[0..4], S = v[5..9]) into acc
+template <typename R, bool VISC>
+MB_HD void bc_apply(const R* v, double* acc) {
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) acc[s] = acc[s] + (double)v[s];
+  if (VISC) {
+#pragma unroll
+    for (int s = 0; s < MB_NP; ++s) acc[s] = acc[s] - (double)v[MB_NP + s];
   }
 }
 
@@ -835,9 +869,17 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
         }
         acc[s] = (double)a;
       }
-      // ---- boundary records of the cell, face order 1..6
-      if (i == 1 || i == b.n1 || j == 1 || j == b.n2 || k == 1 || k == b.n3)
-        bc_cell<R, VISC, RS, LIM>(p, b, Pin, i, j, k, acc);
+      // ---- boundary records of the cell, face order 1..6 (computed before the sweep by k_records)
+      if (i == 1 || i == b.n1 || j == 1 || j == b.n2 || k == 1 || k == b.n3) {
+        const R* rf = reinterpret_cast<const R*>(p.recflux);
+        const int on = (i == 1) | (i == b.n1) << 1 | (j == 1) << 2 | (j == b.n2) << 3 | (k == 1) << 4 | (k == b.n3) << 5;
+#pragma unroll 1
+        for (int F = 1; F <= 6; ++F) {
+          if (!((on >> (F - 1)) & 1)) continue;
+          const int rid = record_of(p, b, F, i, j, k);
+          if (rid >= 0) bc_apply<R, VISC>(rf + (long long)rid * 2 * MB_NP, acc);
+        }
+      }
       const long long r = row(b, i, j, k);
       if (MODE == MODE_RESIDUAL) {
 #pragma unroll

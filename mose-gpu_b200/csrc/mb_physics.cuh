@@ -96,6 +96,7 @@ struct Params {
   double wm, ri;
   int lim, rs, visc, ndir, dt_additive, guard, state_check;
   double cfl, vnn, prandtl, schmidt, mco;
+  void* recflux;           // boundary-record contributions [record][10] in the flux type (k_records)
   int* queue;              // persistent sweep: the tile counter (null: one CTA per tile)
   int ntiles_run;          // tiles of the launch (persistent sweep)
   int pgrid;               // CTAs of a persistent launch (resident CTAs per SM x SMs)
