@@ -643,76 +643,82 @@ MB_HD void cons_update(const Params& p, const double* pc, const double* po, cons
   if (pn[0] < 1e-20) pn[0] = 1e-20;
 }
 
-// local dt of one cell (dt_blk.inc: min rule :156-191, additive rule :79-155), FP64
-MB_HD double cell_dt(const Params& p, const DBlk& b, long long l, const double* pl) {
-  double rho, Rg;
+// local dt of one cell (dt_blk.inc: min rule :156-191, additive rule :79-155) in the arithmetic type R: FP64 for the
+// parity form and the standalone Compute_dt, FP32 (geometry and tables in FP32) for the fused dt of the mixed form
+template <typename R>
+MB_HD R cell_dt_t(const Params& p, const DBlk& b, long long l, const R* pl) {
+  R rho, Rg;
   rotot_rtot(p, pl[0], rho, Rg);
-  double Tc = pl[MB_IPR] / (rho * Rg);
-  double Sound = f_ss(p, pl[0], pl[MB_IPR], rho, Rg);
-  const double* m = b.m + 9 * l;
-  const double* dl = b.dl + 3 * l;
-  double dtc = 1e8;
+  R Tc = pl[MB_IPR] / (rho * Rg);
+  R Sound = f_ss(p, pl[0], pl[MB_IPR], rho, Rg);
+  const auto* m = Geo<R>::m(b) + 9 * l;
+  const auto* dl = Geo<R>::dl(b) + 3 * l;
+  R dtc = (R)1e8;
   if (p.dt_additive) {
-    double ra_c = 0.0, ra_v = 0.0;
+    R ra_c = (R)0, ra_v = (R)0;
     for (int d = 0; d < b.ndir; ++d) {
-      double m0 = ld(m + d), m1 = ld(m + d + 3), m2 = ld(m + d + 6);
-      double gn = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
-      double vel_ = fabs(pl[MB_IU] * m0 + pl[MB_IV] * m1 + pl[MB_IW] * m2) / gn;
-      double lambda = vel_ + Sound;
+      R m0 = cvt<R>(ld(m + d)), m1 = cvt<R>(ld(m + d + 3)), m2 = cvt<R>(ld(m + d + 6));
+      R gn = rsqrt_(m0 * m0 + m1 * m1 + m2 * m2);
+      R vel_ = fabs(pl[MB_IU] * m0 + pl[MB_IV] * m1 + pl[MB_IW] * m2) / gn;
+      R lambda = vel_ + Sound;
       ra_c = ra_c + lambda * gn;
       ra_v = ra_v + gn * gn;
     }
     if (p.visc) {
       if (b.ndir == 3) {
-        double g[3][3];
+        R g[3][3];
         for (int d = 0; d < 3; ++d)
-          for (int a = 0; a < 3; ++a) g[d][a] = ld(m + d + 3 * a);
+          for (int a = 0; a < 3; ++a) g[d][a] = cvt<R>(ld(m + d + 3 * a));
         auto dot = [&](int x, int y) { return g[x][0] * g[y][0] + g[x][1] * g[y][1] + g[x][2] * g[y][2]; };
-        auto nr = [&](int x) { return sqrt(g[x][0] * g[x][0] + g[x][1] * g[x][1] + g[x][2] * g[x][2]); };
-        double c12 = dot(0, 1) / (nr(0) * nr(1)), c13 = dot(0, 2) / (nr(0) * nr(2)), c23 = dot(1, 2) / (nr(1) * nr(2));
-        double ss = c12 * c12 + c13 * c13 + c23 * c23;
-        double qp = c12 * c13 * c23;
-        if (ss + 2.0 * qp > 1.0) {
-          double mr = 2.0 * sqrt(ss / 3.0) * cos(acos(mx(-1.0, mn(1.0, 3.0 * sqrt(3.0) * qp / pow(ss, 1.5)))) / 3.0);
-          ra_v = ra_v * 0.25 * (2.0 + mr + 1.0 / mr);
+        auto nr = [&](int x) { return rsqrt_(g[x][0] * g[x][0] + g[x][1] * g[x][1] + g[x][2] * g[x][2]); };
+        R c12 = dot(0, 1) / (nr(0) * nr(1)), c13 = dot(0, 2) / (nr(0) * nr(2)), c23 = dot(1, 2) / (nr(1) * nr(2));
+        R ss = c12 * c12 + c13 * c13 + c23 * c23;
+        R qp = c12 * c13 * c23;
+        if (ss + (R)2.0 * qp > (R)1.0) {
+          R mr = (R)2.0 * rsqrt_(ss / (R)3.0) *
+                 cos(acos(mx((R)-1.0, mn((R)1.0, (R)3.0 * rsqrt_((R)3.0) * qp / pow(ss, (R)1.5)))) / (R)3.0);
+          ra_v = ra_v * (R)0.25 * ((R)2.0 + mr + (R)1.0 / mr);
         }
       }
       int ta = tidx(p, Tc);
-      double tda = Tc - (double)ta;
-      double cpa = f_cp(p, pl[0], ta, tda, rho);
-      double cva = cpa - Rg;
-      double mila, kla;
+      R tda = Tc - (R)ta;
+      R cpa = f_cp(p, pl[0], ta, tda, rho);
+      R cva = cpa - Rg;
+      R mila, kla;
       wilke(p, pl[0], rho, ta, tda, mila, kla);
-      if (p.prandtl > 0.0) kla = mila * cpa / p.prandtl;
-      const double mie = 0.0, prt = 0.85;
-      double Dmx = mx(4.0 / 3.0 * (mila + mie) / rho, (kla + mie * cpa / prt) / (rho * cva));
-      dtc = 1.0 / (ra_c / p.cfl + Dmx * ra_v / p.vnn);
+      if (p.prandtl > 0.0) kla = mila * cpa / (R)p.prandtl;
+      const R mie = (R)0.0, prt = (R)0.85;
+      R Dmx = mx((R)4.0 / (R)3.0 * (mila + mie) / rho, (kla + mie * cpa / prt) / (rho * cva));
+      dtc = (R)1.0 / (ra_c / (R)p.cfl + Dmx * ra_v / (R)p.vnn);
     } else {
-      dtc = p.cfl / ra_c;
+      dtc = (R)p.cfl / ra_c;
     }
   } else {
     for (int d = 0; d < b.ndir; ++d) {
-      double m0 = ld(m + d), m1 = ld(m + d + 3), m2 = ld(m + d + 6);
-      double nrm = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
-      double v0 = m0 / nrm, v1 = m1 / nrm, v2 = m2 / nrm;
-      double vel_ = fabs(pl[MB_IU] * v0 + pl[MB_IV] * v1 + pl[MB_IW] * v2);
-      double lambda = vel_ + Sound;
-      double dtd = ld(dl + d) / lambda * p.cfl;
+      R m0 = cvt<R>(ld(m + d)), m1 = cvt<R>(ld(m + d + 3)), m2 = cvt<R>(ld(m + d + 6));
+      R nrm = rsqrt_(m0 * m0 + m1 * m1 + m2 * m2);
+      R v0 = m0 / nrm, v1 = m1 / nrm, v2 = m2 / nrm;
+      R vel_ = fabs(pl[MB_IU] * v0 + pl[MB_IV] * v1 + pl[MB_IW] * v2);
+      R lambda = vel_ + Sound;
+      R dtd = cvt<R>(ld(dl + d)) / lambda * (R)p.cfl;
       dtc = mn(dtd, dtc);
     }
     if (p.visc) {
       int ti = tidx(p, Tc);
-      double td = Tc - (double)ti, mil, kl;
+      R td = Tc - (R)ti, mil, kl;
       wilke(p, pl[0], rho, ti, td, mil, kl);
-      double mi = 0.0 + mil;
+      R mi = (R)0.0 + mil;
       for (int d = 0; d < b.ndir; ++d) {
-        double dlv = ld(dl + d);
-        double dtd = (rho * (dlv * dlv) * p.vnn) / mi;
+        R dlv = cvt<R>(ld(dl + d));
+        R dtd = (rho * (dlv * dlv) * (R)p.vnn) / mi;
         dtc = mn(dtd, dtc);
       }
     }
   }
-  return dtc * 1.0;
+  return dtc * (R)1.0;
+}
+MB_HD double cell_dt(const Params& p, const DBlk& b, long long l, const double* pl) {
+  return cell_dt_t<double>(p, b, l, pl);
 }
 
 // min over the CTA of a positive double, then one atomic into the device clock
@@ -903,7 +909,12 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
         if (bad) report_bad_state(st, t.blk, i, j, k);
 #pragma unroll
         for (int s = 0; s < MB_NP; ++s) Pout[r + s * p.nc] = pn[s];
-        if (last) dtloc = mn(dtloc, cell_dt(p, b, r - b.boff, pn));
+        if (last) {  // the new state's local dt, in the flux type (FP64 in the parity form)
+          R pr[MB_NP];
+#pragma unroll
+          for (int s = 0; s < MB_NP; ++s) pr[s] = cvt<R>(pn[s]);
+          dtloc = mn(dtloc, (double)cell_dt_t<R>(p, b, r - b.boff, pr));
+        }
       }
     }
     kb ^= 1;
