@@ -776,15 +776,19 @@ template <typename R, int TY, bool VISC, int MODE, int RS, int LIM>
 __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const double* __restrict__ Pin,
                                            const double* Pold, double* Pout, double* Rout, double rkc, int last,
                                            unsigned char* smem_raw, double* sred) {
-  constexpr int NF = VISC ? 2 * MB_NP : MB_NP;
-  typedef R RowI[33][NF];
-  typedef R RowJ[32][NF];
+  constexpr int NF = VISC ? 2 * MB_NP : MB_NP;  // values a face task computes (convective, viscous)
+  // values a face keeps in shared memory: both fluxes in the FP64 form (pass 2 sums them in the reference's
+  // order); the net flux (convective - viscous) in the mixed form
+  constexpr bool NET = VISC && Fast<R>::on;
+  constexpr int NS = NET ? MB_NP : NF;
+  typedef R RowI[33][NS];
+  typedef R RowJ[32][NS];
   Tile<R, TY> T;
   T.base = reinterpret_cast<R*>(smem_raw);                                       // [4][NV][TY+4][36]
   unsigned char* fbase = smem_raw + sizeof(R) * 4 * NV * (TY + 4) * TXH;
-  RowI* sFi = reinterpret_cast<RowI*>(fbase);                                     // [TY][33][NF]
-  RowJ* sFj = reinterpret_cast<RowJ*>(fbase + sizeof(R) * TY * 33 * NF);          // [TY+1][32][NF]
-  RowJ* sFk0 = reinterpret_cast<RowJ*>(fbase + sizeof(R) * (TY * 33 + (TY + 1) * 32) * NF);  // [2][TY][32][NF]
+  RowI* sFi = reinterpret_cast<RowI*>(fbase);                                     // [TY][33][NS]
+  RowJ* sFj = reinterpret_cast<RowJ*>(fbase + sizeof(R) * TY * 33 * NS);          // [TY+1][32][NS]
+  RowJ* sFk0 = reinterpret_cast<RowJ*>(fbase + sizeof(R) * (TY * 33 + (TY + 1) * 32) * NS);  // [2][TY][32][NS]
   const DBlk b = p.blk[t.blk];
   DevState* st = p.st + b.grp;
   if (MODE == MODE_UPDATE && st->done) return;  // the case has reached its stop time (uniform over the CTA)
@@ -808,7 +812,7 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
     face_flux<R, TY, VISC, RS, LIM>(p, b, T, 2, i, j, t.k0 - 1, tx + 2, ty + 2, out);
     R* dst = &sFk0[(kb ^ 1) * TY + ty][tx][0];
 #pragma unroll
-    for (int q = 0; q < NF; ++q) dst[q] = out[q];
+    for (int q = 0; q < NS; ++q) dst[q] = NET ? out[q] - out[MB_NP + q] : out[q];
   }
   for (int k = t.k0; k < t.k1; ++k) {
     __syncthreads();  // the slot of plane k-2 is free
@@ -842,7 +846,7 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
       R out[NF];
       face_flux<R, TY, VISC, RS, LIM>(p, b, T, d, fi, fj, k, ii, jj, out);
 #pragma unroll
-      for (int q = 0; q < NF; ++q) dst[q] = out[q];
+      for (int q = 0; q < NS; ++q) dst[q] = NET ? out[q] - out[MB_NP + q] : out[q];
     }
     __syncthreads();
     if (own) {
@@ -854,8 +858,8 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
       const R* gl = (j > 1) ? &sFj[ty][tx][0] : nullptr;
       const R* hr = (k < b.n3) ? &sFk0[kb * TY + ty][tx][0] : nullptr;
       const R* hl = (k > 1) ? &sFk0[(kb ^ 1) * TY + ty][tx][0] : nullptr;
-      // the sum runs in the flux type (the FP64 form: FP64 as the reference; the mixed form: the twelve FP32
-      // face fluxes summed in FP32 and converted once), the boundary records and the update in FP64
+      // the sum runs in the flux type (the FP64 form: FP64 in the reference's order; the mixed form: the six FP32
+      // net face fluxes summed in FP32 and converted once), the boundary records and the update in FP64
 #pragma unroll
       for (int s = 0; s < MB_NP; ++s) {
         R a = (R)0;
@@ -865,7 +869,7 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
         if (gl) a = a - gl[s];
         if (hr) a = a + hr[s];
         if (hl) a = a - hl[s];
-        if (VISC) {
+        if (VISC && !NET) {
           if (fr) a = a - fr[MB_NP + s];
           if (fl) a = a + fl[MB_NP + s];
           if (gr) a = a - gr[MB_NP + s];
@@ -950,7 +954,7 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
 template <typename R, int TY, bool VISC>
 constexpr size_t sweep_smem() {
   return sizeof(R) * ((size_t)4 * NV * (TY + 4) * TXH +
-                      (size_t)(TY * 33 + (TY + 1) * 32 + 2 * TY * 32) * (VISC ? 2 * MB_NP : MB_NP));
+                      (size_t)(TY * 33 + (TY + 1) * 32 + 2 * TY * 32) * ((VISC && !Fast<R>::on) ? 2 * MB_NP : MB_NP));
 }
 
 }  // namespace mb

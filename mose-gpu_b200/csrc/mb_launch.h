@@ -30,7 +30,7 @@ struct GhostLists {
 constexpr int TY_F64 = 4;    // tile rows of the FP64 sweep (128 threads)
 constexpr int TY_F32 = 8;    // tile rows of the mixed sweep (256 threads)
 constexpr int MINB_F64 = 2;  // resident CTAs per SM the FP64 sweep's registers must allow
-constexpr int MINB_F32 = 2;  // resident CTAs per SM the mixed sweep's registers must allow
+constexpr int MINB_F32 = 3;  // resident CTAs per SM the mixed sweep's registers must allow (80 registers)
 constexpr int TY_AUX = 8;    // tile rows of the per-cell kernels (dt, update)
 
 #define MB_CAT2(a, b) a##b
