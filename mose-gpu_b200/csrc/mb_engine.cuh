@@ -815,9 +815,10 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
     for (int q = 0; q < NS; ++q) dst[q] = NET ? out[q] - out[MB_NP + q] : out[q];
   }
   for (int k = t.k0; k < t.k1; ++k) {
-    __syncthreads();  // the slot of plane k-2 is free
+    // the slot of plane k-2 is free: its last readers, the faces of plane k-1, finished before the barrier that
+    // preceded pass 2 of plane k-1; so a thread stages plane k+2 as soon as its own pass 2 of plane k-1 is done
     if (k + 2 <= b.n3 + kext) stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, k + 2, jext);
-    __syncthreads();
+    __syncthreads();  // plane k+2 staged, and every pass 2 of plane k-1 done (the flux buffers are free)
     // ---- face tasks of this plane through one call site: 0 = i-face #tid, 1 = extra i-faces (last warp,
     // lanes < TY), 2 = j-face #tid, 3 = extra j-face row (warp 0), 4 = the k-face above
 #pragma unroll 1
