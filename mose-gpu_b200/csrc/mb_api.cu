@@ -153,6 +153,9 @@ static int check_mesh(const mb_mesh* mesh, int ngroups) {
     const mb_block& q = mesh->blk[b];
     if (q.n[0] < 1 || q.n[1] < 1 || q.n[2] < 1 || !q.fm1 || !q.fm2 || !q.fm3 || !q.dl || !q.m || !q.vol) return MB_E_ARG;
     if (q.group < 0 || q.group >= ngroups) return MB_E_ARG;
+    // intra-block offsets of the sweep are 32-bit: 9 metric values per padded cell, 4 per face
+    const long long npad = (long long)(q.n[0] + 2 * MB_GC) * (q.n[1] + 2 * MB_GC) * (q.n[2] + 2 * MB_GC);
+    if (9 * npad >= (1LL << 31)) return MB_E_ARG;
     const long long np = (long long)(q.n[0] + 2 * MB_GC) * (q.n[1] + 2 * MB_GC) * (q.n[2] + 2 * MB_GC);
     if (q.boff < 0 || q.boff + np > mesh->ncell_total) return MB_E_ARG;
   }

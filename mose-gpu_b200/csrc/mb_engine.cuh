@@ -57,8 +57,8 @@ template <typename R, int TY, bool VISC, int RS = 0, int LIM = 0>
 MB_HD void face_flux(const Params& p, const DBlk& b, const Tile<R, TY>& T, int d, int i, int j, int k, int ii,
                      int jj, R* out) {
   const int skm = slot_of(k - 1), sk = slot_of(k), sk1 = slot_of(k + 1), sk2 = slot_of(k + 2);
-  const long long r0 = row(b, i, j, k);
-  const long long st = (d == 0) ? 1 : (d == 1 ? (long long)b.pi : (long long)b.pi * b.pj);
+  const int l0 = lin32(b, i, j, k);
+  const int st = (d == 0) ? 1 : (d == 1 ? b.pi : b.pi * b.pj);
   // the 4-cell stencil along d
   int o4[4];
   if (d == 0) { o4[0] = T.off(sk, jj, ii - 1); o4[1] = T.off(sk, jj, ii); o4[2] = T.off(sk, jj, ii + 1); o4[3] = T.off(sk, jj, ii + 2); }
@@ -69,11 +69,10 @@ MB_HD void face_flux(const Params& p, const DBlk& b, const Tile<R, TY>& T, int d
   for (int s = 0; s < MB_NP; ++s) {
     pm1[s] = T.v(o4[0], s); p0[s] = T.v(o4[1], s); pp1[s] = T.v(o4[2], s); pp2[s] = T.v(o4[3], s);
   }
-  const long long l0 = r0 - b.boff;
   const auto* gdl = Geo<R>::dl(b);
 #pragma unroll
   for (int q = 0; q < 4; ++q) dlc[q] = (R)ld(gdl + d + 3 * (l0 + (q - 1) * st));
-  const auto* f = Geo<R>::fm(b, d) + fmi(b, d, i, j, k);
+  const auto* f = Geo<R>::fm(b, d) + fmi32(b, d, i, j, k);
   R nx = (R)ld(f), ny = (R)ld(f + 1), nz = (R)ld(f + 2), area = (R)ld(f + 3);
   conv_face<R, RS, LIM>(p, pm1, p0, pp1, pp2, dlc, nx, ny, nz, area, out);
   if (!VISC) return;

@@ -152,6 +152,16 @@ MB_HD long long fmi(const DBlk& b, int d, int i, int j, int k) {
   if (d == 1) return 4 * ((long long)(i - 1) + (long long)b.n1 * (j + (long long)(b.n2 + 1) * (k - 1)));
   return 4 * ((long long)(i - 1) + (long long)b.n1 * ((j - 1) + (long long)b.n2 * k));
 }
+// 32-bit forms of lin and fmi for the sweep's hot path: mb_init rejects a block whose padded cells x 9 or face
+// values reach 2^31, so every intra-block offset fits an int
+MB_HD int lin32(const DBlk& b, int i, int j, int k) {
+  return (i + GC - 1) + (j + GC - 1) * b.pi + (k + GC - 1) * b.pi * b.pj;
+}
+MB_HD int fmi32(const DBlk& b, int d, int i, int j, int k) {
+  if (d == 0) return 4 * (i + (b.n1 + 1) * ((j - 1) + b.n2 * (k - 1)));
+  if (d == 1) return 4 * ((i - 1) + b.n1 * (j + (b.n2 + 1) * (k - 1)));
+  return 4 * ((i - 1) + b.n1 * ((j - 1) + b.n2 * k));
+}
 MB_HD double ld(const double* p) {
 #ifdef __CUDA_ARCH__
   return __ldg(p);
