@@ -24,6 +24,9 @@ struct mb_ctx {
   GRec* d_grec = nullptr;
   int* d_phys = nullptr;
   int* d_cubic = nullptr;
+  int* d_physf = nullptr;       // the fused stage's ghost lists: only the layers some computation reads
+  int* d_cubicf = nullptr;
+  GhostLists gf;
   long long* d_cdst = nullptr;
   long long* d_csrc = nullptr;
   long long* d_pgsrc = nullptr;
@@ -84,7 +87,8 @@ static void free_ctx(mb_ctx* c) {
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   if (c->graph) cudaGraphDestroy(c->graph);
   void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
-                  c->d_pgsrc, c->d_pg, c->d_tab, c->d_tabf, c->d_st, c->d_tiles_sweep, c->d_tiles_aux, c->d_scratch, c->d_acc4, c->d_queue, c->d_recflux, c->d_brec, c->d_bcell};
+                  c->d_pgsrc, c->d_pg, c->d_tab, c->d_tabf, c->d_st, c->d_tiles_sweep, c->d_tiles_aux, c->d_scratch, c->d_acc4, c->d_queue, c->d_recflux, c->d_brec, c->d_bcell,
+                  c->d_physf, c->d_cubicf};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& q : c->geo32)
@@ -148,6 +152,7 @@ int64_t mb_launch_count(const mb_ctx* ctx) { return ctx ? ctx->launches : 0; }
 static int check_mesh(const mb_mesh* mesh, int ngroups) {
   if (!mesh || mesh->nblk <= 0 || mesh->ncell_total <= 0 || !mesh->blk) return MB_E_ARG;
   if (mesh->nrec > 0 && !mesh->rec) return MB_E_ARG;
+  if (mesh->nrec >= (1 << 28)) return MB_E_ARG;  // record ids share a 32-bit word with a layer count
   if (mesh->nconn > 0 && !mesh->conn) return MB_E_ARG;
   for (int b = 0; b < mesh->nblk; ++b) {
     const mb_block& q = mesh->blk[b];
@@ -173,9 +178,11 @@ static int check_mesh(const mb_mesh* mesh, int ngroups) {
 // frees the mesh-dependent device tables (blocks, record maps, records, ghost lists, tiles, FP32 geometry)
 static void free_tables(mb_ctx* c) {
   void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
-                  c->d_pgsrc, c->d_pg, c->d_tiles_sweep, c->d_tiles_aux, c->d_recflux, c->d_brec, c->d_bcell};
+                  c->d_pgsrc, c->d_pg, c->d_tiles_sweep, c->d_tiles_aux, c->d_recflux, c->d_brec, c->d_bcell,
+                  c->d_physf, c->d_cubicf};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  c->d_physf = nullptr; c->d_cubicf = nullptr;
   c->d_recflux = nullptr; c->d_brec = nullptr; c->d_bcell = nullptr; c->nrec = 0;
   c->d_blk = nullptr; c->d_recmap = nullptr; c->d_rec = nullptr; c->d_grec = nullptr; c->d_phys = nullptr;
   c->d_cubic = nullptr; c->d_cdst = nullptr; c->d_csrc = nullptr; c->d_pgsrc = nullptr; c->d_pg = nullptr;
@@ -242,6 +249,33 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
     hg[q] = GRec{r.blk, r.i, r.j, r.k, r.face, r.type};
     if (r.type == MB_BC_EXTRAPOLATION || r.type == MB_BC_INFLOW || r.type == MB_BC_WALL) phys.push_back(q);
     if (r.type == MB_BC_EXTRAPOLATION) cubic.push_back(q);
+  }
+  // The fused stage fills only the ghost layers that some computation of the stage reads (entries carry their
+  // layer count in bits 28-29; mb_fill_ghosts keeps the reference's full fill):
+  //  - along an axis of two or more cells, a type 11 / 4 / 5 face's second layer is read by nothing (interior
+  //    faces read one layer, these records read the boundary cell and its interior neighbour): one layer;
+  //  - along an axis one cell deep whose two faces are both type 11, an Euler stage reads no ghost there (no
+  //    faces along it, no viscous stencil, extrapolation records read the cell): no layer;
+  //  - otherwise both layers (the cubic ghost of a one-cell-deep axis reads the opposite face's layers).
+  std::vector<int> physf, cubicf;
+  {
+    std::vector<int> all11(3 * (size_t)mesh->nblk, 1);
+    for (int q = 0; q < mesh->nrec; ++q) {
+      const mb_bc& r = mesh->rec[q];
+      if (r.type != MB_BC_EXTRAPOLATION) all11[3 * r.blk + (r.face - 1) / 2] = 0;
+    }
+    for (int q = 0; q < mesh->nrec; ++q) {
+      const mb_bc& r = mesh->rec[q];
+      if (r.type != MB_BC_EXTRAPOLATION && r.type != MB_BC_INFLOW && r.type != MB_BC_WALL) continue;
+      const int ax = (r.face - 1) / 2;
+      const int nax = mesh->blk[r.blk].n[ax];
+      int layers = 2;
+      if (nax >= 2) layers = 1;
+      else if (!sc->visc && all11[3 * r.blk + ax]) layers = 0;
+      if (layers == 0) continue;
+      physf.push_back(q | (layers << 28));
+      if (r.type == MB_BC_EXTRAPOLATION) cubicf.push_back(q | (layers << 28));
+    }
   }
   // the record kernel's work list: records grouped by type (one code path per warp where possible)
   std::vector<int> brec(mesh->nrec), bcell(5 * (size_t)mesh->nrec);
@@ -343,6 +377,8 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   if ((rc = upload(&c->d_grec, hg.data(), hg.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_phys, phys.data(), phys.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_cubic, cubic.data(), cubic.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_physf, physf.data(), physf.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_cubicf, cubicf.data(), cubicf.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_cdst, cdst.data(), cdst.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_csrc, csrc.data(), csrc.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_pgsrc, pgsrc.data(), pgsrc.size())) != MB_OK) return rc;
@@ -365,6 +401,8 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   g.rec = c->d_grec; g.phys = c->d_phys; g.nphys = (int)phys.size(); g.cubic = c->d_cubic; g.ncubic = (int)cubic.size();
   g.cdst = c->d_cdst; g.csrc = c->d_csrc; g.ncopy = (int)cdst.size(); g.pgsrc = c->d_pgsrc; g.nconn = mesh->nconn;
   g.pg = c->d_pg;
+  c->gf = g;
+  c->gf.phys = c->d_physf; c->gf.nphys = (int)physf.size(); c->gf.cubic = c->d_cubicf; c->gf.ncubic = (int)cubicf.size();
   return MB_OK;
 }
 
@@ -504,7 +542,8 @@ int mb_group_reset(mb_ctx* ctx, int g, const mb_group* spec, const double* P, vo
   CK(cudaSetDevice(ctx->device));
   cudaStream_t s = (cudaStream_t)stream;
   CK(group_reset(ctx->p, g, spec->time_clip, spec->t_end, s));
-  CK(dt_cells(ctx->p, ctx->d_tiles_aux, ctx->ntiles_aux, P, s, g));
+  CK(ctx->sc.precision == MB_PREC_MIXED ? sweep_f32_rs1_dt(ctx->p, ctx->d_tiles_aux, ctx->ntiles_aux, P, g, s)
+                                         : dt_cells(ctx->p, ctx->d_tiles_aux, ctx->ntiles_aux, P, s, g));
   ctx->launches += 2;
   return MB_OK;
 }
@@ -612,9 +651,9 @@ static int time_sweep(mb_ctx* c, const std::vector<DTile>& tl, int persistent, c
   return rc;
 }
 
-static int fill(mb_ctx* c, double* P, cudaStream_t s) {
+static int fill(mb_ctx* c, double* P, cudaStream_t s, bool fused = true) {
   int nl = 0;
-  cudaError_t e = ghost_fill(c->p, c->g, P, s, &nl);
+  cudaError_t e = ghost_fill(c->p, fused ? c->gf : c->g, P, s, &nl);
   c->launches += nl;
   CK(e);
   return MB_OK;
@@ -623,7 +662,7 @@ static int fill(mb_ctx* c, double* P, cudaStream_t s) {
 int mb_fill_ghosts(mb_ctx* ctx, double* P, void* stream) {
   if (!ctx || !P) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
-  return fill(ctx, P, (cudaStream_t)stream);
+  return fill(ctx, P, (cudaStream_t)stream, false);
 }
 
 int mb_residual(mb_ctx* ctx, const double* P, double* R, void* stream) {
@@ -648,7 +687,8 @@ int mb_update(mb_ctx* ctx, double* P, const double* PO, const double* R, int irk
 
 static int dt_min(mb_ctx* c, const double* P, cudaStream_t s) {
   CK(reset_dt(c->p, s));
-  CK(dt_cells(c->p, c->d_tiles_aux, c->ntiles_aux, P, s));
+  CK(c->sc.precision == MB_PREC_MIXED ? sweep_f32_rs1_dt(c->p, c->d_tiles_aux, c->ntiles_aux, P, -1, s)
+                                       : dt_cells(c->p, c->d_tiles_aux, c->ntiles_aux, P, s));
   c->launches += 2;
   return MB_OK;
 }

@@ -156,7 +156,7 @@ MB_HD void bc_face_geom(const DBlk& b, int Im, int Jm, int Km, int F, double* g)
 
 // BC_Connection_Eul_lean (Lib_BC.f90:1770-1867)
 template <typename R, int RS = 0, int LIM = 0>
-MB_HD_NOINLINE void bc_conn_eul(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
+MB_HD void bc_conn_eul(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
                                          int Km, int Fm, R* A) {
   const long long nc = p.nc;
   const int rs = RS ? RS : p.rs;
@@ -213,7 +213,7 @@ MB_HD_NOINLINE void bc_conn_eul(const Params& p, const DBlk& b, const double* __
 
 // BC_Connection_Visc_lean (Lib_BC.f90:2113-2178); pg = bc_pg(:,1:6) of the record
 template <typename R>
-MB_HD_NOINLINE void bc_conn_visc(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
+MB_HD void bc_conn_visc(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
                                           int Km, int Fm, const double* __restrict__ pg, R* S) {
   const long long nc = p.nc;
   int dir = (Fm + 1) / 2, modfm2 = 1 - 2 * (Fm % 2), gstep = 2 * (Fm % 2) - 1;
@@ -282,7 +282,7 @@ MB_HD_NOINLINE void bc_conn_visc(const Params& p, const DBlk& b, const double* _
 
 // BC_Extrapolation (Lib_BC.f90:1119-1165)
 template <typename R>
-MB_HD_NOINLINE void bc_extrap(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
+MB_HD void bc_extrap(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
                                        int Km, int Fm, R* A) {
   const long long nc = p.nc;
   const long long r = row(b, Im, Jm, Km);
@@ -324,7 +324,7 @@ MB_HD void riemann_rec(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dl
 // reconstruction, Riemann problem between the face state and its mirror; momentum rows only. The Euler part of
 // the adiabatic wall and the closed-inlet fallback of the 405 record.
 template <typename R, int RS = 0, int LIM = 0>
-MB_HD_NOINLINE void bc_sym_eul(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km,
+MB_HD void bc_sym_eul(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km,
                                int Fm, R* A) {
   const long long nc = p.nc;
   const int lim = LIM ? LIM : p.lim;
@@ -380,7 +380,7 @@ MB_HD_NOINLINE void bc_sym_eul(const Params& p, const DBlk& b, const double* __r
 // BC_Wall_Heat_dev (Lib_BC.f90:879-982), laminar adiabatic no-slip wall: the wall-normal velocity gradient of the
 // boundary cell, Grad . M of the cell, Stress_Vector_Std (Mod_Fluid.f90:20-44) with mu_t = 0; momentum rows only.
 template <typename R>
-MB_HD_NOINLINE void bc_wall_heat(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km,
+MB_HD void bc_wall_heat(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km,
                                  int Fm, R* S) {
   const long long nc = p.nc;
   int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm2 = 1 - 2 * modfm, modfm3 = 2 * (2 * modfm - 1);
@@ -433,7 +433,7 @@ MB_HD_NOINLINE void bc_wall_heat(const Params& p, const DBlk& b, const double* _
 // BC_Inflow_Outflow (Lib_BC.f90:1519-1597) of a 405 record: inward flow -> BC_Supersonic_Inflow (Lib_BC.f90:
 // 1247-1330), outward flow -> the face closes (BC_Symmetry_Eul).
 template <typename R, int RS = 0, int LIM = 0>
-MB_HD_NOINLINE void bc_inflow(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km,
+MB_HD void bc_inflow(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km,
                               int Fm, const double* __restrict__ q, R* A) {
   const long long nc = p.nc;
   const int lim = LIM ? LIM : p.lim;
@@ -734,6 +734,29 @@ __device__ __forceinline__ void cta_min_dt(DevState* st, double v, double* sred)
     for (int o = 16; o > 0; o >>= 1) v = mn(v, __shfl_xor_sync(full, v, o));
     if (lane == 0 && v < 1e300) atomicMin(&st->dtmin_bits, (unsigned long long)__double_as_longlong(v));
   }
+}
+
+// ---- Compute_dt alone: the local dt of every interior cell in the form's arithmetic (FP64; FP32 for the mixed
+// form, as its fused dt), reduced into the case's clock. only_group >= 0: the cells of that case only (its first
+// dt after mb_group_reset). Tiles of 32 x TY_AUX cells (8 rows).
+template <typename R>
+__global__ void __launch_bounds__(256) k_dt_t(Params p, const DTile* __restrict__ tiles, const double* P,
+                                             int only_group) {
+  __shared__ double sred[32];
+  const DTile t = tiles[blockIdx.x];
+  const DBlk b = p.blk[t.blk];
+  if (only_group >= 0 && b.grp != only_group) return;
+  const int i = t.i0 + (threadIdx.x & 31), j = t.j0 + (threadIdx.x >> 5);
+  double v = 1e300;
+  if (i <= b.n1 && j <= b.n2) {
+    for (int k = t.k0; k < t.k1; ++k) {
+      const long long r = row(b, i, j, k);
+      R pl[MB_NP];
+      for (int s = 0; s < MB_NP; ++s) pl[s] = cvt<R>(P[r + s * p.nc]);
+      v = mn(v, (double)cell_dt_t<R>(p, b, r - b.boff, pl));
+    }
+  }
+  cta_min_dt(p.st + b.grp, v, sred);
 }
 
 __device__ __forceinline__ void report_bad_state(DevState* st, int blk, int i, int j, int k) {

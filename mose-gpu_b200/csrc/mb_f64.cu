@@ -11,7 +11,9 @@ namespace mb {
 __global__ void k_ghost_phys(Params p, const GRec* __restrict__ rec, const int* __restrict__ list, int n, double* P) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
-  const GRec r = rec[list[q]];
+  const int e = list[q];
+  const int nl = (e >> 28) ? (e >> 28) : GC;  // ghost layers to fill (entries of the fused lists carry theirs)
+  const GRec r = rec[e & 0x0fffffff];
   const DBlk b = p.blk[r.blk];
   const int dir = (r.face + 1) / 2, gstep = 2 * (r.face % 2) - 1;
   const long long st = (dir == 1) ? 1 : (dir == 2 ? (long long)b.pi : (long long)b.pi * b.pj);
@@ -19,13 +21,13 @@ __global__ void k_ghost_phys(Params p, const GRec* __restrict__ rec, const int* 
   const long long nc = p.nc;
   if (r.type == 5) {
     const int step = -gstep;
-    for (int g = 1; g <= GC; ++g) {
+    for (int g = 1; g <= nl; ++g) {
       long long d0 = src + (long long)(g * step) * st, a1 = src + (long long)((g - 1) * step) * st,
                 a2 = src + (long long)((g - 2) * step) * st, a3 = src + (long long)((g - 3) * step) * st;
       for (int s = 0; s < MB_NP; ++s) P[d0 + s * nc] = 3.0 * P[a1 + s * nc] - 3.0 * P[a2 + s * nc] + P[a3 + s * nc];
     }
   } else {
-    for (int g = 1; g <= GC; ++g) {
+    for (int g = 1; g <= nl; ++g) {
       long long dst = src - (long long)(gstep * g) * st;
       for (int s = 0; s < MB_NP; ++s) P[dst + s * nc] = P[src + s * nc];
     }
@@ -37,13 +39,15 @@ __global__ void k_ghost_phys(Params p, const GRec* __restrict__ rec, const int* 
 __global__ void k_ghost_cubic(Params p, const GRec* __restrict__ rec, const int* __restrict__ list, int n, double* P) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
-  const GRec r = rec[list[q]];
+  const int e = list[q];
+  const int nl = (e >> 28) ? (e >> 28) : GC;
+  const GRec r = rec[e & 0x0fffffff];
   const DBlk b = p.blk[r.blk];
   const int dir = (r.face + 1) / 2, gstep = 2 * (r.face % 2) - 1, step = -gstep;
   const long long st = (dir == 1) ? 1 : (dir == 2 ? (long long)b.pi : (long long)b.pi * b.pj);
   const long long src = row(b, r.i, r.j, r.k);
   const long long nc = p.nc;
-  for (int g = 1; g <= GC; ++g) {
+  for (int g = 1; g <= nl; ++g) {
     long long d0 = src + (long long)(g * step) * st, a1 = src + (long long)((g - 1) * step) * st,
               a2 = src + (long long)((g - 2) * step) * st, a3 = src + (long long)((g - 3) * step) * st;
     for (int s = 0; s < MB_NP; ++s) P[d0 + s * nc] = 3.0 * P[a1 + s * nc] - 3.0 * P[a2 + s * nc] + P[a3 + s * nc];
@@ -70,26 +74,7 @@ __global__ void k_pg(const long long* __restrict__ src, int nconn, long long nc,
   pg[q] = P[src[e] + s * nc];
 }
 
-// ---- Compute_dt alone: local dt of every interior cell, reduced into the device clock ----
-// only_group >= 0: the cells of that case only (its first dt after mb_group_reset)
-__global__ void __launch_bounds__(32 * TY_AUX) k_dt(Params p, const DTile* __restrict__ tiles, const double* P,
-                                                    int only_group) {
-  __shared__ double sred[32];
-  const DTile t = tiles[blockIdx.x];
-  const DBlk b = p.blk[t.blk];
-  if (only_group >= 0 && b.grp != only_group) return;
-  const int i = t.i0 + (threadIdx.x & 31), j = t.j0 + (threadIdx.x >> 5);
-  double v = 1e300;
-  if (i <= b.n1 && j <= b.n2) {
-    for (int k = t.k0; k < t.k1; ++k) {
-      const long long r = row(b, i, j, k);
-      double pl[MB_NP];
-      for (int s = 0; s < MB_NP; ++s) pl[s] = P[r + s * p.nc];
-      v = mn(v, cell_dt(p, b, r - b.boff, pl));
-    }
-  }
-  cta_min_dt(p.st + b.grp, v, sred);
-}
+// ---- Compute_dt alone: k_dt_t<double> of mb_engine.cuh ----
 
 // ---- RK_Newstate alone: the conservative update of every interior cell from a given residual ----
 __global__ void __launch_bounds__(32 * TY_AUX) k_update(Params p, const DTile* __restrict__ tiles, double* P,
@@ -189,7 +174,7 @@ cudaError_t ghost_fill(const Params& p, const GhostLists& g, double* P, cudaStre
 
 cudaError_t dt_cells(const Params& p, const DTile* tiles, int ntiles, const double* P, cudaStream_t s,
                      int only_group) {
-  k_dt<<<ntiles, 32 * TY_AUX, 0, s>>>(p, tiles, P, only_group);
+  k_dt_t<double><<<ntiles, 32 * TY_AUX, 0, s>>>(p, tiles, P, only_group);
   return cudaGetLastError();
 }
 
