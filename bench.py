@@ -247,10 +247,15 @@ def run_serving(args, dev):
     stream = sv.request_stream(n_cases=args.serve_cases, rate=args.serve_rate, seed=20261203)
     reqs = [sv.riemann_request(q, d, n, st, te, arrival=t) for q, (t, d, n, st, te) in enumerate(stream)]
     setup = time.time() - t0
-    srv = sv.Server(reqs[0].case.scheme, reqs[0].case.thermo, budget_bytes=int(args.serve_budget_gb * 2 ** 30),
-                    max_cases=256, precision=abi.PREC_MIXED, device=dev.index, poll_steps=args.serve_poll)
-    done = srv.serve(reqs, max_wall=args.serve_max_s)
-    srv.close()
+    # two lanes: 1-D cases (cheap steps, many of them) and 2-D cases, each its own context and stream
+    budget = int(args.serve_budget_gb * 2 ** 30)
+    lanes = [sv.Server(reqs[0].case.scheme, reqs[0].case.thermo, budget_bytes=min(2 << 30, budget // 4),
+                       max_cases=128, precision=abi.PREC_MIXED, device=dev.index, poll_steps=args.serve_poll),
+             sv.Server(reqs[0].case.scheme, reqs[0].case.thermo, budget_bytes=budget - min(2 << 30, budget // 4),
+                       max_cases=128, precision=abi.PREC_MIXED, device=dev.index, poll_steps=args.serve_poll)]
+    done = sv.serve_lanes(lanes, lambda r: 0 if r.case.blocks[0]["n"][1] == 1 else 1, reqs, max_wall=args.serve_max_s)
+    for lane in lanes:
+        lane.close()
     lat = np.array(sorted(r.finish - r.arrival for r in done))
     span = max(r.finish for r in done) - min(r.arrival for r in reqs) if done else float("nan")
     work = sum(r.case.n_interior * r.steps for r in done)
@@ -260,6 +265,7 @@ def run_serving(args, dev):
             "p50_s": float(np.percentile(lat, 50)) if done else None,
             "p99_s": float(np.percentile(lat, 99)) if done else None,
             "cell_updates_per_s": work / span if done else 0.0, "makespan_s": span, "poll_steps": args.serve_poll,
+            "lanes": "2 (1-D cases | 2-D cases), one context and stream each",
             "budget_gb": args.serve_budget_gb, "precision": "mixed", "setup_s": round(setup, 1),
             "sample": "the first %d cases of the seeded 4096-case stream (half 1-D N in [256, 8192], half 2-D N^2 "
                       "with N in [128, 1024], log-uniform), Poisson arrivals" % len(reqs)}

@@ -274,6 +274,10 @@ int mb_group_reset(mb_ctx* ctx, int g, const mb_group* spec, const double* P, vo
 /* Status of cases g0 .. g0+n-1 (one device read). Synchronises. */
 int mb_get_group_status(mb_ctx* ctx, int g0, int n, mb_status* out);
 
+/* The same, ordered on `stream` (the stream the context's steps run on): waits for that stream only, so that
+ * several contexts on their own streams keep running. */
+int mb_read_group_status(mb_ctx* ctx, int g0, int n, mb_status* out, void* stream);
+
 /* The sweep's autotuner (no counterpart in the reference): times, on the state P and the current mesh, the
  * k-chunk of the tiles of 3-D blocks (8 / 16 / 32 / 64 planes) and a plain grid (one CTA per tile) against the
  * persistent work queue (one wave of CTAs taking the largest tiles first from a counter), and keeps the

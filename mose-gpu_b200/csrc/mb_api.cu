@@ -562,6 +562,17 @@ static void to_status(const DevState& h, int state_check, mb_status* st) {
   else if (h.n_bad_state > 0 && state_check) st->code = MB_E_STATE;
 }
 
+int mb_read_group_status(mb_ctx* ctx, int g0, int n, mb_status* out, void* stream) {
+  if (!ctx || !out || g0 < 0 || n < 1 || g0 + n > ctx->ngroups) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<DevState> h(n);
+  CK(cudaMemcpyAsync(h.data(), ctx->d_st + g0, n * sizeof(DevState), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (int q = 0; q < n; ++q) to_status(h[q], ctx->sc.state_check, out + q);
+  return MB_OK;
+}
+
 int mb_get_group_status(mb_ctx* ctx, int g0, int n, mb_status* out) {
   if (!ctx || !out || g0 < 0 || n < 1 || g0 + n > ctx->ngroups) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));

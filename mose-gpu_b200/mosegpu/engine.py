@@ -48,6 +48,7 @@ def load_library():
     L.mb_reconfigure.argtypes = [vp, C.POINTER(abi.MBMesh)]
     L.mb_group_reset.argtypes = [vp, C.c_int, C.POINTER(abi.MBGroup), vp, vp]
     L.mb_get_group_status.argtypes = [vp, C.c_int, C.c_int, C.POINTER(abi.MBStatus)]
+    L.mb_read_group_status.argtypes = [vp, C.c_int, C.c_int, C.POINTER(abi.MBStatus), vp]
     L.mb_autotune.argtypes = [vp, vp, vp]
     L.mb_set_tuning.argtypes = [vp, C.c_int, C.c_int]
     L.mb_get_tuning.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)]
@@ -56,7 +57,7 @@ def load_library():
     L.mb_version.restype = C.c_char_p
     for f in ("mb_fill_ghosts", "mb_residual", "mb_update", "mb_dt", "mb_stage", "mb_step", "mb_begin_step",
               "mb_get_status", "mb_profile_stage", "mb_reconfigure", "mb_group_reset", "mb_get_group_status",
-              "mb_autotune", "mb_set_tuning", "mb_get_tuning"):
+              "mb_read_group_status", "mb_autotune", "mb_set_tuning", "mb_get_tuning"):
         getattr(L, f).restype = C.c_int
     _lib = L
     return L

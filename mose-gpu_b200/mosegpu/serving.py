@@ -247,13 +247,14 @@ class Server:
         if self.ctx is None or not self.active:
             return []
         st = (abi.MBStatus * self.max_cases)()
-        _check(self.L.mb_get_group_status(self.ctx, 0, self.max_cases, st), "mb_get_group_status")
+        _check(self.L.mb_read_group_status(self.ctx, 0, self.max_cases, st, self._s()), "mb_read_group_status")
         out = []
         for grp in list(self.active):
             s = st[grp]
             if s.done or s.code != abi.MB_OK:
                 req, boff, _ = self.active.pop(grp)
-                req.result = self.P[:, boff:boff + req.npad].cpu().numpy()
+                with self.torch.cuda.stream(self.stream):
+                    req.result = self.P[:, boff:boff + req.npad].cpu().numpy()
                 req.finish = now_fn()
                 req.status = s
                 req.steps = s.steps
@@ -273,45 +274,68 @@ class Server:
             self.ctx = None
 
     # ------------------------------------------------------------------ the request loop
-    def serve(self, requests, clock="wall", max_wall=None):
-        """Serves `requests` (sorted by arrival time, seconds from the start). Returns them with start / finish.
+    def serve(self, requests, max_wall=None):
+        """Serves `requests` (arrival times in seconds from the start) on this server alone; returns them with
+        their start / finish times (see serve_lanes)."""
+        return serve_lanes([self], lambda r: 0, requests, max_wall=max_wall)
 
-        The loop admits every arrived request that fits, advances all running cases poll_steps steps, then
-        retires finished ones; when nothing runs it waits for the next arrival."""
-        pending = sorted(requests, key=lambda r: r.arrival)
-        t0 = time.perf_counter()
-        now = lambda: time.perf_counter() - t0  # noqa: E731
-        qi = 0
-        waiting = []
-        finished = []
-        while qi < len(pending) or waiting or self.active:
-            if max_wall is not None and now() > max_wall:
-                break
-            while qi < len(pending) and pending[qi].arrival <= now():
-                waiting.append(pending[qi])
-                qi += 1
+
+def serve_lanes(lanes, route, requests, max_wall=None):
+    """The request loop over one or more servers ("lanes", each an engine context with its own arena, clocks and
+    stream). route(request) picks a request's lane: cases whose steps cost about the same share a lane, so that a
+    cheap case with many steps is not held to the step time of an expensive one. The lanes run independently on
+    their streams: whenever a lane's last burst of poll_steps steps has finished on the GPU, the loop reads its
+    clocks (waiting for that stream only), retires its finished cases, admits what fits of its queue (a request
+    that cannot fit its empty lane is rejected with MB_E_BUDGET) and launches its next burst. With nothing running
+    it waits for the next arrival. Returns the finished requests."""
+    import torch
+    pending = sorted(requests, key=lambda r: r.arrival)
+    t0 = time.perf_counter()
+    now = lambda: time.perf_counter() - t0  # noqa: E731
+    qi = 0
+    waiting = [[] for _ in lanes]
+    events = [None for _ in lanes]       # the event after a lane's burst in flight
+    finished = []
+    while qi < len(pending) or any(waiting) or any(l.active for l in lanes):
+        if max_wall is not None and now() > max_wall:
+            break
+        while qi < len(pending) and pending[qi].arrival <= now():
+            waiting[route(pending[qi])].append(pending[qi])
+            qi += 1
+        progressed = False
+        for li, (lane, wq) in enumerate(zip(lanes, waiting)):
+            if events[li] is not None:
+                if not events[li].query():
+                    continue
+                events[li] = None
+                finished += lane.poll(now)
             new = []
-            while waiting:
-                if self.try_admit(waiting[0], now()):
-                    new.append(waiting.pop(0).group)
-                elif not self.active and not new:
-                    # nothing runs and it still does not fit: it never will (rows or HBM budget)
-                    r = waiting.pop(0)
+            while wq:
+                if lane.try_admit(wq[0], now()):
+                    new.append(wq.pop(0).group)
+                elif not lane.active and not new:
+                    # nothing runs in the lane and it still does not fit: it never will (rows or HBM budget)
+                    r = wq.pop(0)
                     r.error = abi.MB_E_BUDGET
                     r.finish = now()
                     finished.append(r)
                 else:
                     break
             if new:
-                self.commit_admissions(new)
-            if not self.active:
-                if qi < len(pending):
-                    time.sleep(max(0.0, pending[qi].arrival - now()))
-                continue
-            self.advance(self.poll_steps)
-            finished += self.poll(now)
-        self.stream.synchronize()
-        return finished
+                lane.commit_admissions(new)
+            if lane.active:
+                lane.advance(lane.poll_steps)
+                events[li] = torch.cuda.Event()
+                events[li].record(lane.stream)
+                progressed = True
+        if not progressed:
+            if all(e is None for e in events) and qi < len(pending):
+                time.sleep(max(0.0, min(pending[qi].arrival - now(), 0.01)))
+            else:
+                time.sleep(5e-5)
+    for lane in lanes:
+        lane.stream.synchronize()
+    return finished
 
 
 # ---------------------------------------------------------------------- the serving request stream

@@ -102,3 +102,25 @@ def test_admission_waits_for_budget_and_overlaps_running_cases():
         want, _ = _alone(r, abi.PREC_FP64)
         m = r.case.interior_mask()
         assert np.array_equal(r.result[:, m], want[:, m]), r.rid
+
+
+@pytest.mark.gpu
+def test_two_lanes_run_independently_and_match_alone():
+    """1-D cases in one lane, 2-D cases in another (each its own context and stream): every case ends
+    bit-identical to itself alone."""
+    reqs = [sv.riemann_request(0, 1, 300, [(1.0, 0.0, 1.0), (0.125, 0.0, 0.1)], 0.15, arrival=0.0),
+            sv.riemann_request(1, 2, 40, [(1.5, 0, 0, 1.5), (0.53, 1.2, 0, 0.3), (0.14, 1.2, 1.2, 0.03),
+                                          (0.53, 0, 1.2, 0.3)], 0.25, arrival=0.0),
+            sv.riemann_request(2, 1, 120, [(0.4, 0.5, 3.0), (1.7, -0.8, 0.7)], 0.15, arrival=0.005)]
+    mk = lambda: sv.Server(reqs[0].case.scheme, reqs[0].case.thermo, budget_bytes=1 << 29, max_cases=4,  # noqa
+                           precision=abi.PREC_FP64, poll_steps=9)
+    lanes = [mk(), mk()]
+    done = sv.serve_lanes(lanes, lambda r: 0 if r.case.blocks[0]["n"][1] == 1 else 1, reqs, max_wall=120.0)
+    for lane in lanes:
+        lane.close()
+    assert sorted(r.rid for r in done) == [0, 1, 2]
+    for r in done:
+        want, st = _alone(r, abi.PREC_FP64)
+        assert r.status.done == 1 and r.status.steps == st.steps
+        m = r.case.interior_mask()
+        assert np.array_equal(r.result[:, m], want[:, m]), r.rid
