@@ -260,13 +260,21 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   std::vector<int> physf, cubicf;
   {
     std::vector<int> all11(3 * (size_t)mesh->nblk, 1);
+    std::vector<long long> nface(6 * (size_t)mesh->nblk, 0);
     for (int q = 0; q < mesh->nrec; ++q) {
       const mb_bc& r = mesh->rec[q];
       if (r.type != MB_BC_EXTRAPOLATION) all11[3 * r.blk + (r.face - 1) / 2] = 0;
+      nface[6 * r.blk + r.face - 1] += 1;
+    }
+    for (int b = 0; b < mesh->nblk; ++b) {
+      DBlk& d = hb[b];
+      const long long nk = (long long)d.n1 * d.n2;
+      d.kmirror = (d.n3 == 1 && all11[3 * b + 2] && nface[6 * b + 4] == nk && nface[6 * b + 5] == nk) ? 1 : 0;
     }
     for (int q = 0; q < mesh->nrec; ++q) {
       const mb_bc& r = mesh->rec[q];
       if (r.type != MB_BC_EXTRAPOLATION && r.type != MB_BC_INFLOW && r.type != MB_BC_WALL) continue;
+      if (hb[r.blk].kmirror && r.face >= 5) continue;  // the k ghosts of a mirrored block are never read
       const int ax = (r.face - 1) / 2;
       const int nax = mesh->blk[r.blk].n[ax];
       int layers = 2;
@@ -317,7 +325,8 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
     }
     pgsrc.push_back(rowof(cn.bs, I, J, K));
     pgsrc.push_back(rowof(cn.bs, I + guide(cn.fs, 0), J + guide(cn.fs, 1), K + guide(cn.fs, 2)));
-    for (int m = 0; m < 4; ++m) pgsrc.push_back(rowof(cn.bs, t[m][0], t[m][1], t[m][2]));
+    for (int m = 0; m < 4; ++m)  // a mirrored donor's k ghosts are its k = 1 cells
+      pgsrc.push_back(rowof(cn.bs, t[m][0], t[m][1], hb[cn.bs].kmirror ? 1 : t[m][2]));
   }
   // every row must lie inside the arena
   for (const auto* v : {&cdst, &csrc, &pgsrc})

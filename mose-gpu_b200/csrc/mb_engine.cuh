@@ -56,7 +56,9 @@ MB_HD int slot_of(int kk) { return (kk + 8) & 3; }
 template <typename R, int TY, bool VISC, int RS = 0, int LIM = 0>
 MB_HD void face_flux(const Params& p, const DBlk& b, const Tile<R, TY>& T, int d, int i, int j, int k, int ii,
                      int jj, R* out) {
-  const int skm = slot_of(k - 1), sk = slot_of(k), sk1 = slot_of(k + 1), sk2 = slot_of(k + 2);
+  // a mirrored block (one cell deep in k, extrapolated k faces) reads its k = 1 plane for the k ghosts
+  const int skm = slot_of(b.kmirror ? k : k - 1), sk = slot_of(k), sk1 = slot_of(b.kmirror ? k : k + 1),
+            sk2 = slot_of(k + 2);
   const int l0 = lin32(b, i, j, k);
   const int st = (d == 0) ? 1 : (d == 1 ? b.pi : b.pi * b.pj);
   // the 4-cell stencil along d
@@ -233,7 +235,8 @@ MB_HD void bc_conn_visc(const Params& p, const DBlk& b, const double* __restrict
     for (int a = 0; a < 3; ++a)
       M[a][q] = (R)0.5 * (cvt<R>(ld(b.m + a + 3 * q + 9 * l1)) + cvt<R>(ld(b.m + a + 3 * q + 9 * lg)));
   // cells: 0 loc, 1 ghost (Pg(:,1)), 2 b+, 3 b-, 4 c+, 5 c-, 6..9 Pg(:,3..6)
-  const long long rc[6] = {r1, 0, r1 + sb, r1 - sb, r1 + sc, r1 - sc};
+  const long long scm = (b.kmirror && ic == 2) ? 0 : sc;  // a mirrored block's k ghosts are its k = 1 cells
+  const long long rc[6] = {r1, 0, r1 + sb, r1 - sb, r1 + scm, r1 - scm};
   auto pv = [&](int q, int s) -> R {
     if (q == 1) return cvt<R>(ld(pg + s));
     if (q >= 6) return cvt<R>(ld(pg + s + MB_NP * (q - 4)));
@@ -824,7 +827,7 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
   // ghost layers the stencils read: 2 along an axis with faces; for a block one cell deep along j or k (2-D,
   // 1-D) no face of that axis exists and only the viscous transverse gradient reads one ghost layer
   const int jext = (b.n2 > 1) ? GC : (VISC ? 1 : 0);
-  const int kext = (b.n3 > 1) ? GC : (VISC ? 1 : 0);
+  const int kext = (b.n3 > 1) ? GC : ((VISC && !b.kmirror) ? 1 : 0);
   // prologue: planes k0-2 .. k0+1, and the k-face below the first plane
   for (int kk = t.k0 - 2; kk <= t.k0 + 1; ++kk)
     if (kk >= 1 - kext && kk <= b.n3 + kext) stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, kk, jext);
