@@ -40,6 +40,9 @@ struct mb_ctx {
   DevState* d_st = nullptr;
   DTile* d_tiles_sweep = nullptr;
   int ntiles_sweep = 0;
+  DTile* d_tiles_km = nullptr;  // tiles of the mirrored one-plane blocks (their own sweep instantiation)
+  int ntiles_km = 0;
+  std::vector<int> hkm;         // mirrored-block flag per block
   std::vector<int> hdims;       // 3 per block of the current mesh (interior extents)
   int kc3 = 16;                 // k-chunk of the sweep tiles of blocks deeper than one cell (autotuned)
   int persistent = 0;           // persistent work-queue sweep (autotuned)
@@ -88,7 +91,7 @@ static void free_ctx(mb_ctx* c) {
   if (c->graph) cudaGraphDestroy(c->graph);
   void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
                   c->d_pgsrc, c->d_pg, c->d_tab, c->d_tabf, c->d_st, c->d_tiles_sweep, c->d_tiles_aux, c->d_scratch, c->d_acc4, c->d_queue, c->d_recflux, c->d_brec, c->d_bcell,
-                  c->d_physf, c->d_cubicf};
+                  c->d_physf, c->d_cubicf, c->d_tiles_km};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& q : c->geo32)
@@ -98,13 +101,16 @@ static void free_ctx(mb_ctx* c) {
 
 // the tiles (32 x ty cells, kc planes) of the blocks whose class (3: deeper than one cell in k, 2: one k plane,
 // 1: one cell deep in j and k) is in mask (bit cls), block-major
-static std::vector<DTile> make_tiles(const std::vector<int>& dims, int ty, int kc, int mask = 0xe) {
+// km: the mirrored-block flag per block; km_sel 0 / 1 keeps only the blocks with that flag (-1: all)
+static std::vector<DTile> make_tiles(const std::vector<int>& dims, int ty, int kc, int mask = 0xe,
+                                     const std::vector<int>* km = nullptr, int km_sel = -1) {
   std::vector<DTile> t;
   const int nb = (int)dims.size() / 3;
   for (int b = 0; b < nb; ++b) {
     const int* n = &dims[3 * b];
     const int cls = n[2] > 1 ? 3 : (n[1] > 1 ? 2 : 1);
     if (!(mask & (1 << cls))) continue;
+    if (km && km_sel >= 0 && (*km)[b] != km_sel) continue;
     for (int k0 = 1; k0 <= n[2]; k0 += kc)
       for (int j0 = 1; j0 <= n[1]; j0 += ty)
         for (int i0 = 1; i0 <= n[0]; i0 += 32) t.push_back(DTile{b, i0, j0, k0, std::min(k0 + kc, n[2] + 1)});
@@ -179,10 +185,10 @@ static int check_mesh(const mb_mesh* mesh, int ngroups) {
 static void free_tables(mb_ctx* c) {
   void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
                   c->d_pgsrc, c->d_pg, c->d_tiles_sweep, c->d_tiles_aux, c->d_recflux, c->d_brec, c->d_bcell,
-                  c->d_physf, c->d_cubicf};
+                  c->d_physf, c->d_cubicf, c->d_tiles_km};
   for (void* q : ptrs)
     if (q) cudaFree(q);
-  c->d_physf = nullptr; c->d_cubicf = nullptr;
+  c->d_physf = nullptr; c->d_cubicf = nullptr; c->d_tiles_km = nullptr; c->ntiles_km = 0;
   c->d_recflux = nullptr; c->d_brec = nullptr; c->d_bcell = nullptr; c->nrec = 0;
   c->d_blk = nullptr; c->d_recmap = nullptr; c->d_rec = nullptr; c->d_grec = nullptr; c->d_phys = nullptr;
   c->d_cubic = nullptr; c->d_cdst = nullptr; c->d_csrc = nullptr; c->d_pgsrc = nullptr; c->d_pg = nullptr;
@@ -285,11 +291,14 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
       if (r.type == MB_BC_EXTRAPOLATION) cubicf.push_back(q | (layers << 28));
     }
   }
-  // the record kernel's work list: records grouped by type (one code path per warp where possible)
-  std::vector<int> brec(mesh->nrec), bcell(5 * (size_t)mesh->nrec);
-  for (int q = 0; q < mesh->nrec; ++q) brec[q] = q;
+  // the record kernel's work list: records grouped by type (one code path per warp where possible), without the
+  // k-face records of mirrored blocks (their sweep computes those)
+  std::vector<int> brec;
+  for (int q = 0; q < mesh->nrec; ++q)
+    if (!(hb[mesh->rec[q].blk].kmirror && mesh->rec[q].face >= 5)) brec.push_back(q);
   std::stable_sort(brec.begin(), brec.end(), [&](int a, int b) { return mesh->rec[a].type < mesh->rec[b].type; });
-  for (int q = 0; q < mesh->nrec; ++q) {
+  std::vector<int> bcell(5 * brec.size());
+  for (size_t q = 0; q < brec.size(); ++q) {
     const mb_bc& r = mesh->rec[brec[q]];
     const int v[5] = {r.blk, r.i, r.j, r.k, r.face};
     for (int a = 0; a < 5; ++a) bcell[5 * q + a] = v[a];
@@ -336,7 +345,10 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   c->hdims.assign(3 * (size_t)mesh->nblk, 0);
   for (int b = 0; b < mesh->nblk; ++b)
     for (int a = 0; a < 3; ++a) c->hdims[3 * b + a] = mesh->blk[b].n[a];
-  std::vector<DTile> ts = make_tiles(c->hdims, c->ty_sweep, c->kc3);
+  c->hkm.assign(mesh->nblk, 0);
+  for (int b = 0; b < mesh->nblk; ++b) c->hkm[b] = hb[b].kmirror;
+  std::vector<DTile> ts = make_tiles(c->hdims, c->ty_sweep, c->kc3, 0xe, &c->hkm, 0);
+  std::vector<DTile> tk = make_tiles(c->hdims, c->ty_sweep, c->kc3, 0xe, &c->hkm, 1);
   if (c->persistent) sort_by_work(ts, c->hdims, c->ty_sweep);
   std::vector<DTile> ta = make_tiles(c->hdims, TY_AUX, 16);
   // ---- the mixed form reads its geometry in FP32: one conversion per distinct array of this mesh (blocks may
@@ -393,9 +405,11 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   if ((rc = upload(&c->d_pgsrc, pgsrc.data(), pgsrc.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_tiles_sweep, ts.data(), ts.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_tiles_aux, ta.data(), ta.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_tiles_km, tk.data(), tk.size())) != MB_OK) return rc;
+  c->ntiles_km = (int)tk.size();
   if ((rc = upload(&c->d_brec, brec.data(), brec.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_bcell, bcell.data(), bcell.size())) != MB_OK) return rc;
-  c->nrec = mesh->nrec;
+  c->nrec = (int)brec.size();
   if (mesh->nrec > 0 &&
       cudaMalloc((void**)&c->d_recflux, (size_t)mesh->nrec * 2 * MB_NPRIM * sizeof(double)) != cudaSuccess)
     return MB_E_NOMEM;
@@ -599,7 +613,7 @@ void mb_destroy(mb_ctx* ctx) {
 }
 
 static int sweep_on(mb_ctx* c, const DTile* t, int n, int persistent, int mode, const double* Pin,
-                    const double* Pold, double* Pout, double* Rout, int irk, int last, cudaStream_t s) {
+                    const double* Pold, double* Pout, double* Rout, int irk, int last, cudaStream_t s, int km = 0) {
   if (n <= 0) return MB_OK;
   Params p = c->p;
   p.irk = irk;
@@ -607,13 +621,13 @@ static int sweep_on(mb_ctx* c, const DTile* t, int n, int persistent, int mode, 
   const double rkc = irk > 0 ? rkc_of(c->sc.n_rk, irk) : 0.0;
   cudaError_t e;
   if (c->sc.precision == MB_PREC_MIXED) {
-    if (c->sc.riemann == 1) e = sweep_f32_rs1(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
-    else if (c->sc.riemann == 4) e = sweep_f32_rs4(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
-    else e = sweep_f32_rs12(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+    if (c->sc.riemann == 1) e = sweep_f32_rs1(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s);
+    else if (c->sc.riemann == 4) e = sweep_f32_rs4(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s);
+    else e = sweep_f32_rs12(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s);
   } else {
-    if (c->sc.riemann == 1) e = sweep_f64_rs1(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
-    else if (c->sc.riemann == 4) e = sweep_f64_rs4(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
-    else e = sweep_f64_rs12(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, s);
+    if (c->sc.riemann == 1) e = sweep_f64_rs1(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s);
+    else if (c->sc.riemann == 4) e = sweep_f64_rs4(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s);
+    else e = sweep_f64_rs12(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s);
   }
   c->launches += 1;
   CK(e);
@@ -641,7 +655,9 @@ static int records(mb_ctx* c, const double* Pin, cudaStream_t s) {
 
 static int sweep(mb_ctx* c, int mode, const double* Pin, const double* Pold, double* Pout, double* Rout, int irk,
                  int last, cudaStream_t s) {
-  return sweep_on(c, c->d_tiles_sweep, c->ntiles_sweep, c->persistent, mode, Pin, Pold, Pout, Rout, irk, last, s);
+  int rc = sweep_on(c, c->d_tiles_sweep, c->ntiles_sweep, c->persistent, mode, Pin, Pold, Pout, Rout, irk, last, s);
+  if (rc == MB_OK) rc = sweep_on(c, c->d_tiles_km, c->ntiles_km, 0, mode, Pin, Pold, Pout, Rout, irk, last, s, 1);
+  return rc;
 }
 
 // average device time of nrep sweeps (MODE_UPDATE of stage 1 from P into the stage buffer, no dt) over a tile
@@ -876,14 +892,14 @@ int mb_autotune(mb_ctx* ctx, const double* P, void* stream) {
   if (maxk > 1) {
     for (int kc : {8, 16, 32, 64}) {
       if (kc > 16 && kc / 2 >= maxk) break;
-      std::vector<DTile> tl = make_tiles(ctx->hdims, ty, kc, 1 << 3);
+      std::vector<DTile> tl = make_tiles(ctx->hdims, ty, kc, 1 << 3, &ctx->hkm, 0);
       float ms = 0.f;
       if ((rc = time_sweep(ctx, tl, 0, P, 3, s, &ms)) != MB_OK) return rc;
       if (ms < best) { best = ms; kbest = kc; }
     }
   }
   ctx->kc3 = kbest;
-  std::vector<DTile> all = make_tiles(ctx->hdims, ty, kbest);
+  std::vector<DTile> all = make_tiles(ctx->hdims, ty, kbest, 0xe, &ctx->hkm, 0);
   std::vector<DTile> sorted = all;
   sort_by_work(sorted, ctx->hdims, ty);
   float ms_plain = 0.f, ms_pers = 0.f;
@@ -912,7 +928,7 @@ int mb_set_tuning(mb_ctx* ctx, int kchunk, int persistent) {
   CK(cudaDeviceSynchronize());
   ctx->kc3 = kchunk;
   ctx->persistent = persistent;
-  std::vector<DTile> use = make_tiles(ctx->hdims, ctx->ty_sweep, kchunk);
+  std::vector<DTile> use = make_tiles(ctx->hdims, ctx->ty_sweep, kchunk, 0xe, &ctx->hkm, 0);
   if (persistent) sort_by_work(use, ctx->hdims, ctx->ty_sweep);
   if (ctx->d_tiles_sweep) cudaFree(ctx->d_tiles_sweep);
   ctx->d_tiles_sweep = nullptr;

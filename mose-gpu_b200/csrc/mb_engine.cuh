@@ -53,11 +53,11 @@ MB_HD int slot_of(int kk) { return (kk + 8) & 3; }
 // (diff_cuf_kernels.inc:11-87 + diff_physics.inc) into out[5..9]. (ii, jj) are the tile coordinates of the
 // cell, sk the slot of plane k. The gradients are built per variable in registers and placed on the
 // axes by d (ia = d; the two tangential axes in increasing order), as the reference's Grad(:, ia/ib/ic).
-template <typename R, int TY, bool VISC, int RS = 0, int LIM = 0>
+template <typename R, int TY, bool VISC, int RS = 0, int LIM = 0, bool KM = false>
 MB_HD void face_flux(const Params& p, const DBlk& b, const Tile<R, TY>& T, int d, int i, int j, int k, int ii,
                      int jj, R* out) {
   // a mirrored block (one cell deep in k, extrapolated k faces) reads its k = 1 plane for the k ghosts
-  const int skm = slot_of(b.kmirror ? k : k - 1), sk = slot_of(k), sk1 = slot_of(b.kmirror ? k : k + 1),
+  const int skm = slot_of(KM ? k : k - 1), sk = slot_of(k), sk1 = slot_of(KM ? k : k + 1),
             sk2 = slot_of(k + 2);
   const int l0 = lin32(b, i, j, k);
   const int st = (d == 0) ? 1 : (d == 1 ? b.pi : b.pi * b.pj);
@@ -797,7 +797,7 @@ __device__ __forceinline__ void stage_plane(const Params& p, const DBlk& b, cons
 }
 
 // One tile of the fused stage (the body of k_sweep).
-template <typename R, int TY, bool VISC, int MODE, int RS, int LIM>
+template <typename R, int TY, bool VISC, int MODE, int RS, int LIM, bool KM>
 __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const double* __restrict__ Pin,
                                            const double* Pold, double* Pout, double* Rout, double rkc, int last,
                                            unsigned char* smem_raw, double* sred) {
@@ -827,14 +827,14 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
   // ghost layers the stencils read: 2 along an axis with faces; for a block one cell deep along j or k (2-D,
   // 1-D) no face of that axis exists and only the viscous transverse gradient reads one ghost layer
   const int jext = (b.n2 > 1) ? GC : (VISC ? 1 : 0);
-  const int kext = (b.n3 > 1) ? GC : ((VISC && !b.kmirror) ? 1 : 0);
+  const int kext = (b.n3 > 1) ? GC : ((VISC && !KM) ? 1 : 0);
   // prologue: planes k0-2 .. k0+1, and the k-face below the first plane
   for (int kk = t.k0 - 2; kk <= t.k0 + 1; ++kk)
     if (kk >= 1 - kext && kk <= b.n3 + kext) stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, kk, jext);
   __syncthreads();
   if (own && t.k0 > 1) {
     R out[NF];
-    face_flux<R, TY, VISC, RS, LIM>(p, b, T, 2, i, j, t.k0 - 1, tx + 2, ty + 2, out);
+    face_flux<R, TY, VISC, RS, LIM, KM>(p, b, T, 2, i, j, t.k0 - 1, tx + 2, ty + 2, out);
     R* dst = &sFk0[(kb ^ 1) * TY + ty][tx][0];
 #pragma unroll
     for (int q = 0; q < NS; ++q) dst[q] = NET ? out[q] - out[MB_NP + q] : out[q];
@@ -870,7 +870,7 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
       }
       if (d < 0) continue;
       R out[NF];
-      face_flux<R, TY, VISC, RS, LIM>(p, b, T, d, fi, fj, k, ii, jj, out);
+      face_flux<R, TY, VISC, RS, LIM, KM>(p, b, T, d, fi, fj, k, ii, jj, out);
 #pragma unroll
       for (int q = 0; q < NS; ++q) dst[q] = NET ? out[q] - out[MB_NP + q] : out[q];
     }
@@ -909,11 +909,21 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
       if (i == 1 || i == b.n1 || j == 1 || j == b.n2 || k == 1 || k == b.n3) {
         const R* rf = reinterpret_cast<const R*>(p.recflux);
         const int on = (i == 1) | (i == b.n1) << 1 | (j == 1) << 2 | (j == b.n2) << 3 | (k == 1) << 4 | (k == b.n3) << 5;
+        constexpr int nF = KM ? 4 : 6;  // a mirrored block's k-face records follow below
 #pragma unroll 1
-        for (int F = 1; F <= 6; ++F) {
+        for (int F = 1; F <= nF; ++F) {
           if (!((on >> (F - 1)) & 1)) continue;
           const int rid = record_of(p, b, F, i, j, k);
           if (rid >= 0) bc_apply<R, VISC>(rf + (long long)rid * 2 * MB_NP, acc);
+        }
+        if (KM) {  // faces 5 and 6 of a mirrored block: the extrapolation records of every cell, computed here
+          R A[MB_NP];
+#pragma unroll 1
+          for (int F = 5; F <= 6; ++F) {
+            bc_extrap<R>(p, b, Pin, i, j, k, F, A);
+#pragma unroll
+            for (int s = 0; s < MB_NP; ++s) acc[s] = acc[s] + (double)A[s];
+          }
         }
       }
       const long long r = row(b, i, j, k);
@@ -952,11 +962,13 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
   if (MODE == MODE_UPDATE && last) cta_min_dt(st, dtloc, sred);
 }
 
-// The fused stage over a tile list. p.queue == null: one CTA per tile (grid = ntiles). Otherwise a persistent
+// The fused stage over a tile list (KM: the tiles of mirrored one-plane blocks, a separate instantiation so that
+// the other blocks' code carries none of their special cases). p.queue == null: one CTA per tile (grid = ntiles).
+// Otherwise a persistent
 // work queue: a grid of about one wave of CTAs, each taking the next tile from the counter p.queue (zeroed
 // before the launch) until the list is exhausted. MINB: resident CTAs per SM the register allocation must
 // allow (launch bounds).
-template <typename R, int TY, bool VISC, int MODE, int RS, int LIM, int MINB>
+template <typename R, int TY, bool VISC, int MODE, int RS, int LIM, int MINB, bool KM = false>
 __global__ void __launch_bounds__(32 * TY, MINB)
 k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pin, const double* Pold, double* Pout,
         double* Rout, double rkc, int last) {
@@ -964,7 +976,7 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
   __shared__ double sred[32];
   __shared__ int s_next;
   if (!p.queue) {
-    sweep_tile<R, TY, VISC, MODE, RS, LIM>(p, tiles[blockIdx.x], Pin, Pold, Pout, Rout, rkc, last, smem_raw, sred);
+    sweep_tile<R, TY, VISC, MODE, RS, LIM, KM>(p, tiles[blockIdx.x], Pin, Pold, Pout, Rout, rkc, last, smem_raw, sred);
     return;
   }
   for (;;) {
@@ -972,7 +984,7 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
     __syncthreads();
     const int tix = s_next;
     if (tix >= p.ntiles_run) break;
-    sweep_tile<R, TY, VISC, MODE, RS, LIM>(p, tiles[tix], Pin, Pold, Pout, Rout, rkc, last, smem_raw, sred);
+    sweep_tile<R, TY, VISC, MODE, RS, LIM, KM>(p, tiles[tix], Pin, Pold, Pout, Rout, rkc, last, smem_raw, sred);
     __syncthreads();  // the tile's shared memory is free and s_next may be overwritten
   }
 }

@@ -38,7 +38,7 @@ constexpr int TY_AUX = 8;    // tile rows of the per-cell kernels (dt, update)
 
 #define MB_DECLARE_SWEEP(name)                                                                                    \
   cudaError_t name(const Params& p, const DTile* tiles, int ntiles, int mode, const double* Pin, const double* Pold, \
-                   double* Pout, double* Rout, double rkc, int last, cudaStream_t s);                              \
+                   double* Pout, double* Rout, double rkc, int last, int km, cudaStream_t s);                      \
   cudaError_t name##_setup();                                                                                    \
   cudaError_t name##_records(const Params& p, const int* brec, const int* bcell, int nrec, const double* P,      \
                              cudaStream_t s);                                                                    \
