@@ -112,7 +112,9 @@ class Clocks:
                 "samples": len(inside), "power_w_median": statistics.median(pw) if pw else None}
 
 
-def dist_setup():
+def dist_setup(backend=None, timeout_s=600):
+    """One process per GPU under torchrun (RANK / LOCAL_RANK / WORLD_SIZE / MASTER_* from the environment): the
+    replicas share only the timing reductions. NCCL on GPUs; gloo where there is no GPU (the CPU tests)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -120,13 +122,17 @@ def dist_setup():
     if world > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
         pg = dist
     return world, rank, local, pg
 
 
 def max_over_ranks(pg, x, dev):
+    """The maximum of x over the ranks (a device time of every rank -> the job's time)."""
     if pg is None:
         return x
     import torch
@@ -137,10 +143,12 @@ def max_over_ranks(pg, x, dev):
 
 def barrier(pg, dev):
     import torch
-    torch.cuda.synchronize(dev)
+    if dev.type == "cuda":
+        torch.cuda.synchronize(dev)
     if pg is not None:
         pg.barrier()
-        torch.cuda.synchronize(dev)
+        if dev.type == "cuda":
+            torch.cuda.synchronize(dev)
 
 
 def cpu_sample(case, min_seconds=10.0, max_steps=3):
