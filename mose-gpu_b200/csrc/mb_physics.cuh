@@ -490,6 +490,61 @@ MB_HD void riemann_open(const Params& p, int rs, R dl, R ul, R vl, R wl, R pl, R
   F_E = (R)0.5 * (FL5 + FR5) - (R)0.5 * d5;
 }
 
+// The mixed form's LMRoe (Mco floor) from the states' thermo already evaluated by the caller (T, its table row and
+// fraction, cp): the Roe averages of riemann_open_body.inc:679-730 with the single-species identities, then the
+// dissipation of the fast path of riemann_open.
+template <typename R>
+MB_HD void lmroe_fast(const Params& p, R dl, R ul, R vl, R wl, R pl, R Tl, int Til, R dTl, R cpl, R dr, R ur, R vr,
+                      R wr, R pr, R Tr, int Tir, R dTr, R cpr, R nx, R ny, R nz, R& F_r, R& F_u, R& F_v, R& F_w,
+                      R& F_E) {
+  const R* H = Tab<R>::h(p);
+  const R Rg = (R)p.ri;
+  const R srL = rsqrt_(dl), srR = rsqrt_(dr);
+  const R inv_sr = (R)1 / (srL + srR);
+  const R rho_roe = srL * srR;
+  const R u_roe = (srR * ur + srL * ul) * inv_sr;
+  const R v_roe = (srR * vr + srL * vl) * inv_sr;
+  const R w_roe = (srR * wr + srL * wl) * inv_sr;
+  const R T_roe = (srR * Tr + srL * Tl) * inv_sr;
+  const R hl = H[Til] + (H[Til + 1] - H[Til]) * dTl;
+  const R hr = H[Tir] + (H[Tir + 1] - H[Tir]) * dTr;
+  const R el = hl - Rg * Tl, er = hr - Rg * Tr;
+  const R cv_roe = (R)0.5 * (cpl + cpr) - Rg;
+  const R sum_ei = (srR * er + srL * el) * inv_sr;
+  const R h0l = hl + (R)0.5 * (ul * ul + vl * vl + wl * wl);
+  const R h0r = hr + (R)0.5 * (ur * ur + vr * vr + wr * wr);
+  const R h0_roe = (srR * h0r + srL * h0l) * inv_sr;
+  const R gam_roe = (R)1 + Rg / cv_roe;
+  const R u2 = u_roe * u_roe + v_roe * v_roe + w_roe * w_roe;
+  const R a_roe = rsqrt_((gam_roe - (R)1) * (h0_roe - (R)0.5 * u2 + cv_roe * T_roe - sum_ei));
+  if (nx == (R)0 && ny == (R)0 && nz == (R)0) { F_r = F_u = F_v = F_w = F_E = (R)0; return; }
+  const R unL = ul * nx + vl * ny + wl * nz, unR = ur * nx + vr * ny + wr * nz;
+  const R FL1 = dl * unL, FR1 = dr * unR;
+  const R unRoe = u_roe * nx + v_roe * ny + w_roe * nz;
+  const R utmag = rsqrt_(mx((R)0, u2 - unRoe * unRoe));
+  const R Ma = (a_roe > (R)0) ? (fabs(unRoe) + utmag) / a_roe : (R)1;
+  const R phi = mx((R)p.mco, mn((R)1, Ma));
+  const R drho = dr - dl, dp = pr - pl, dun = unR - unL;
+  const R abs1 = fabs(unRoe - a_roe), abs2 = fabs(unRoe), abs5 = fabs(unRoe + a_roe);
+  const R inva = (R)1 / a_roe, inva2 = inva * inva;
+  const R al4 = drho - dp * inva2;
+  const R al1 = (R)0.5 * (dp * inva2 - rho_roe * phi * dun * inva);
+  const R al5 = (R)0.5 * (dp * inva2 + rho_roe * phi * dun * inva);
+  const R k1 = abs1 * al1, k5 = abs5 * al5, k4 = abs2 * al4, kt = abs2 * rho_roe;
+  const R dtx = (ur - ul) - dun * nx, dty = (vr - vl) - dun * ny, dtz = (wr - wl) - dun * nz;
+  const R d1 = k1 + k4 + k5;
+  const R d2 = k1 * (u_roe - a_roe * nx) + kt * dtx + k4 * u_roe + k5 * (u_roe + a_roe * nx);
+  const R d3 = k1 * (v_roe - a_roe * ny) + kt * dty + k4 * v_roe + k5 * (v_roe + a_roe * ny);
+  const R d4 = k1 * (w_roe - a_roe * nz) + kt * dtz + k4 * w_roe + k5 * (w_roe + a_roe * nz);
+  const R d5 = k1 * (h0_roe - a_roe * unRoe) + kt * (u_roe * dtx + v_roe * dty + w_roe * dtz) +
+               k4 * ((R)0.5 * u2) + k5 * (h0_roe + a_roe * unRoe);
+  F_r = (R)0.5 * (FL1 + FR1) - (R)0.5 * d1;
+  F_u = (R)0.5 * (FL1 * ul + pl * nx + FR1 * ur + pr * nx) - (R)0.5 * d2;
+  F_v = (R)0.5 * (FL1 * vl + pl * ny + FR1 * vr + pr * ny) - (R)0.5 * d3;
+  F_w = (R)0.5 * (FL1 * wl + pl * nz + FR1 * wr + pr * nz) - (R)0.5 * d4;
+  F_E = (R)0.5 * (FL1 * h0l + FR1 * h0r) - (R)0.5 * d5;
+}
+
 // Roe averages shared by the two HLLC forms: the inline one of conv_physics.inc (clamped T row, Rl/Rr
 // taken from the caller) and riemann_HLLC / roe_averages of Lib_Riemann_HLL.f90 (boundary records).
 template <typename R>
@@ -600,6 +655,7 @@ MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, c
   R T1d = P1[MB_IPR] / (Rtot1 * rotot1);
   int Ti1 = tidx(p, T1d);
   R Tdiffd = T1d - (R)Ti1;
+  const R Td1 = Tdiffd;
   R cpd = Fast<R>::on ? CP[Ti1] + (CP[Ti1 + 1] - CP[Ti1]) * Tdiffd
                        : (R)0 + P1[0] / rotot1 * (CP[Ti1] + (CP[Ti1 + 1] - CP[Ti1]) * Tdiffd);
   R gamd = cpd / (cpd - Rtot1);
@@ -612,7 +668,11 @@ MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, c
   gamd = cpd / (cpd - Rtot4);
   R a4 = rsqrt_(gamd * Rtot4 * T4d);
   R F_r, F_u, F_v, F_w, F_E;
-  if (rs == 1)
+  if (Fast<R>::on && rs == 12) {  // the mixed form's LMRoe takes the thermo of the two states evaluated above
+    const R cp1 = CP[Ti1] + (CP[Ti1 + 1] - CP[Ti1]) * Td1;
+    lmroe_fast(p, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], T1d, Ti1, Td1, cp1, P4[0], P4[MB_IU],
+               P4[MB_IV], P4[MB_IW], P4[MB_IPR], T4d, Ti4, Tdiffd, cpd, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
+  } else if (rs == 1)
     hllc(p, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], a1, rotot1, Rtot1, P4[0], P4[MB_IU], P4[MB_IV],
          P4[MB_IW], P4[MB_IPR], a4, rotot4, Rtot4, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
   else
