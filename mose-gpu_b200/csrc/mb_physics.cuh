@@ -550,16 +550,19 @@ MB_HD void lmroe_fast(const Params& p, R dl, R ul, R vl, R wl, R pl, R Tl, int T
 template <typename R>
 MB_HD void hllc(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R Rl, R dr, R ur,
                                      R vr, R wr, R pr, R ar, R drtot, R Rr, R nx, R ny, R nz, R& F_r, R& F_u,
-                                     R& F_v, R& F_w, R& F_E) {
+                                     R& F_v, R& F_w, R& F_E, const R* thL = nullptr, const R* thR = nullptr,
+                                     int tiL = 0, int tiR = 0) {
+  // thL / thR (the mixed form, from the caller's reconstruction): T, its table fraction and cp of each state
   const R* H = Tab<R>::h(p);
   const R* CP = Tab<R>::cp(p);
+  const bool given = Fast<R>::on && thL != nullptr;
   R unl = ul * nx + vl * ny + wl * nz;
   R unr = ur * nx + vr * ny + wr * nz;
-  R inv_dltot = (R)1 / dltot, inv_drtot = (R)1 / drtot;
-  R Tl = pl * inv_dltot / Rl, Tr = pr * inv_drtot / Rr;
-  int Til = tidx(p, Tl);
-  int Tir = tidx(p, Tr);
-  R dTl = Tl - (R)Til, dTr = Tr - (R)Tir;
+  R inv_dltot = given ? (R)0 : (R)1 / dltot, inv_drtot = given ? (R)0 : (R)1 / drtot;
+  R Tl = given ? thL[0] : pl * inv_dltot / Rl, Tr = given ? thR[0] : pr * inv_drtot / Rr;
+  int Til = given ? tiL : tidx(p, Tl);
+  int Tir = given ? tiR : tidx(p, Tr);
+  R dTl = given ? thL[1] : Tl - (R)Til, dTr = given ? thR[1] : Tr - (R)Tir;
   R srL = rsqrt_(dltot), srR = rsqrt_(drtot), inv_sr = (R)1 / (srL + srR);
   R u_roe = (srR * ur + srL * ul) * inv_sr, v_roe = (srR * vr + srL * vl) * inv_sr,
     w_roe = (srR * wr + srL * wl) * inv_sr;
@@ -573,7 +576,8 @@ MB_HD void hllc(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R 
     if (Fast<R>::on) {  // one species: Y = 1, d_roe = 1
       h0l = hl;
       h0r = hr;
-      cv_roe = (R)0.5 * (CP[Til] + (CP[Til + 1] - CP[Til]) * dTl + CP[Tir] + (CP[Tir + 1] - CP[Tir]) * dTr) - invW;
+      cv_roe = given ? (R)0.5 * (thL[2] + thR[2]) - invW
+                     : (R)0.5 * (CP[Til] + (CP[Til + 1] - CP[Til]) * dTl + CP[Tir] + (CP[Tir + 1] - CP[Tir]) * dTr) - invW;
       sum_ei = (srR * er + srL * el) * inv_sr;
     } else {
     h0l = h0l + hl * dl * inv_dltot;
@@ -672,9 +676,12 @@ MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, c
     const R cp1 = CP[Ti1] + (CP[Ti1 + 1] - CP[Ti1]) * Td1;
     lmroe_fast(p, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], T1d, Ti1, Td1, cp1, P4[0], P4[MB_IU],
                P4[MB_IV], P4[MB_IW], P4[MB_IPR], T4d, Ti4, Tdiffd, cpd, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
-  } else if (rs == 1)
+  } else if (rs == 1) {
+    const R th1[3] = {T1d, Td1, CP[Ti1] + (CP[Ti1 + 1] - CP[Ti1]) * Td1}, th4[3] = {T4d, Tdiffd, cpd};
     hllc(p, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], a1, rotot1, Rtot1, P4[0], P4[MB_IU], P4[MB_IV],
-         P4[MB_IW], P4[MB_IPR], a4, rotot4, Rtot4, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
+         P4[MB_IW], P4[MB_IPR], a4, rotot4, Rtot4, nx, ny, nz, F_r, F_u, F_v, F_w, F_E,
+         Fast<R>::on ? th1 : nullptr, Fast<R>::on ? th4 : nullptr, Ti1, Ti4);
+  }
   else
     riemann_open(p, rs, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], a1, rotot1, P4[0], P4[MB_IU],
                  P4[MB_IV], P4[MB_IW], P4[MB_IPR], a4, rotot4, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
