@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <vector>
+#include <unordered_map>
 #include <algorithm>
 #include "../../include/mose_b200.h"
 #include "mb_launch.h"
@@ -396,6 +397,55 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   if ((rc = upload(&c->d_recmap, recmap.data(), recmap.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_rec, hr.data(), hr.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_grec, hg.data(), hg.size())) != MB_OK) return rc;
+  // Ghost passes in two halves where the record order changes values. The extrapolating ghosts of a face (walls in
+  // the first pass, type 11 in the second) read the opposite face's ghost layers when the axis has at most two
+  // cells, so of two records on opposite faces of one column the later one in record order must see the earlier
+  // one's ghosts (the reference fills them in one sequential record loop). Every record goes into the first half
+  // unless its opposite partner on the same column comes earlier in record order; only pairs interact, so two
+  // launches per pass reproduce the sequential order exactly. An axis of one cell with type 11 on both faces is
+  // order-free (every ghost equals the cell), as are axes of three or more cells.
+  int ordered = 0;
+  std::vector<char> late_phys(mesh->nrec, 0), late_cubic(mesh->nrec, 0);
+  {
+    std::vector<int> ax11(3 * (size_t)mesh->nblk, 1);
+    for (int q = 0; q < mesh->nrec; ++q)
+      if (mesh->rec[q].type != MB_BC_EXTRAPOLATION) ax11[3 * mesh->rec[q].blk + (mesh->rec[q].face - 1) / 2] = 0;
+    for (int q = 0; q < mesh->nrec; ++q) {
+      const mb_bc& r = mesh->rec[q];
+      const int ax = (r.face - 1) / 2, nax = mesh->blk[r.blk].n[ax];
+      if (r.type != MB_BC_EXTRAPOLATION && r.type != MB_BC_WALL) continue;
+      if (nax == 2 || (nax == 1 && !ax11[3 * r.blk + ax])) ordered = 1;
+    }
+    if (ordered) {
+      std::unordered_map<unsigned long long, int> seen_phys, seen_cubic;  // column -> face of its first record
+      for (int q = 0; q < mesh->nrec; ++q) {
+        const mb_bc& r = mesh->rec[q];
+        const bool ph = r.type == MB_BC_EXTRAPOLATION || r.type == MB_BC_INFLOW || r.type == MB_BC_WALL;
+        if (!ph) continue;
+        const int ax = (r.face - 1) / 2;
+        const int t1 = ax == 0 ? r.j : r.i, t2 = ax == 2 ? r.j : r.k;
+        const unsigned long long key = ((unsigned long long)(3 * (unsigned long long)r.blk + ax) << 40) |
+                                       ((unsigned long long)(unsigned)t1 << 20) | (unsigned long long)(unsigned)t2;
+        auto mark = [&](std::unordered_map<unsigned long long, int>& seen, std::vector<char>& late) {
+          auto it = seen.find(key);
+          if (it == seen.end()) seen.emplace(key, r.face);
+          else if (it->second != r.face) late[q] = 1;
+        };
+        mark(seen_phys, late_phys);
+        if (r.type == MB_BC_EXTRAPOLATION) mark(seen_cubic, late_cubic);
+      }
+    }
+  }
+  auto split = [&](std::vector<int>& v, const std::vector<char>& late, int* off) {
+    std::stable_partition(v.begin(), v.end(), [&](int e) { return !late[e & 0x0fffffff]; });
+    off[0] = 0; off[2] = (int)v.size(); off[1] = 0;
+    for (int e : v) off[1] += !late[e & 0x0fffffff];
+  };
+  int po[3], co[3], pof[3], cof[3];
+  split(phys, late_phys, po);
+  split(cubic, late_cubic, co);
+  split(physf, late_phys, pof);
+  split(cubicf, late_cubic, cof);
   if ((rc = upload(&c->d_phys, phys.data(), phys.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_cubic, cubic.data(), cubic.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_physf, physf.data(), physf.size())) != MB_OK) return rc;
@@ -424,8 +474,11 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   g.rec = c->d_grec; g.phys = c->d_phys; g.nphys = (int)phys.size(); g.cubic = c->d_cubic; g.ncubic = (int)cubic.size();
   g.cdst = c->d_cdst; g.csrc = c->d_csrc; g.ncopy = (int)cdst.size(); g.pgsrc = c->d_pgsrc; g.nconn = mesh->nconn;
   g.pg = c->d_pg;
+  g.ordered = ordered;
+  for (int f = 0; f < 3; ++f) { g.phys_off[f] = po[f]; g.cubic_off[f] = co[f]; }
   c->gf = g;
   c->gf.phys = c->d_physf; c->gf.nphys = (int)physf.size(); c->gf.cubic = c->d_cubicf; c->gf.ncubic = (int)cubicf.size();
+  for (int f = 0; f < 3; ++f) { c->gf.phys_off[f] = pof[f]; c->gf.cubic_off[f] = cof[f]; }
   return MB_OK;
 }
 

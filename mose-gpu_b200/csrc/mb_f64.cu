@@ -159,8 +159,19 @@ static inline unsigned nblk_for(long long n, int t) { return (unsigned)((n + t -
 
 cudaError_t ghost_fill(const Params& p, const GhostLists& g, double* P, cudaStream_t s, int* nl) {
   *nl = 0;
-  if (g.nphys > 0) { k_ghost_phys<<<nblk_for(g.nphys, 128), 128, 0, s>>>(p, g.rec, g.phys, g.nphys, P); ++*nl; }
-  if (g.ncubic > 0) { k_ghost_cubic<<<nblk_for(g.ncubic, 128), 128, 0, s>>>(p, g.rec, g.cubic, g.ncubic, P); ++*nl; }
+  if (!g.ordered) {
+    if (g.nphys > 0) { k_ghost_phys<<<nblk_for(g.nphys, 128), 128, 0, s>>>(p, g.rec, g.phys, g.nphys, P); ++*nl; }
+    if (g.ncubic > 0) { k_ghost_cubic<<<nblk_for(g.ncubic, 128), 128, 0, s>>>(p, g.rec, g.cubic, g.ncubic, P); ++*nl; }
+  } else {
+    for (int f = 0; f < 2; ++f) {
+      const int n = g.phys_off[f + 1] - g.phys_off[f];
+      if (n > 0) { k_ghost_phys<<<nblk_for(n, 128), 128, 0, s>>>(p, g.rec, g.phys + g.phys_off[f], n, P); ++*nl; }
+    }
+    for (int f = 0; f < 2; ++f) {
+      const int n = g.cubic_off[f + 1] - g.cubic_off[f];
+      if (n > 0) { k_ghost_cubic<<<nblk_for(n, 128), 128, 0, s>>>(p, g.rec, g.cubic + g.cubic_off[f], n, P); ++*nl; }
+    }
+  }
   if (g.ncopy > 0) {
     k_ghost_copy<<<nblk_for((long long)g.ncopy * MB_NP, 256), 256, 0, s>>>(g.cdst, g.csrc, g.ncopy, p.nc, P);
     ++*nl;

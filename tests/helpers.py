@@ -44,6 +44,14 @@ def interior_rows(case, R):
     return R[:, case.interior_mask()]
 
 
+def reversed_records(case):
+    """The same case with its boundary records in reverse order (a case without connections: the connection
+    table refers to records by index). The ghost fill of the reference runs its record loop in this order."""
+    assert len(case.conn) == 0
+    case.rec = case.rec[::-1].copy()
+    return case
+
+
 def small_cases():
     """(id, builder) of the parity cases: every boundary type, Riemann solver and limiter served."""
     return [
@@ -63,4 +71,13 @@ def small_cases():
                                                           limiter=abi.LIM_MINMOD, n_rk=3)),
         ("mb2d_roe_mc_euler_rk4", lambda: cs.multiblock_2d(cols=2, rows=3, lo=5, hi=11, seed=5, riemann=abi.RS_LMROE,
                                                            limiter=abi.LIM_MC, visc=0)),
+        # blocks two cells and one cell high between walls: a wall's cubic ghosts read the opposite face's ghosts,
+        # so the fill must follow the record order
+        # (Euler slip walls: no-slip walls two cells apart diverge in the oracle itself)
+        ("mb2d_thin_walls_hllc", lambda: cs.multiblock_2d(cols=2, rows=1, widths=[6, 7], heights=[2], visc=0,
+                                                          riemann=abi.RS_HLLC, limiter=abi.LIM_MINMOD)),
+        ("mb2d_thin_walls_reversed", lambda: reversed_records(cs.multiblock_2d(cols=1, rows=1, widths=[8],
+                                                                               heights=[2], visc=0, mach=0.5))),
+        ("mb2d_one_row_walls_reversed", lambda: reversed_records(cs.multiblock_2d(cols=1, rows=1, widths=[7],
+                                                                                  heights=[1], visc=0))),
     ]
