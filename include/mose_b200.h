@@ -79,7 +79,11 @@ extern "C" {
 #define MB_LIM_FIRST_ORDER 6
 /* Riemann solver ids = rs_dev (numerics/fluxes/Lib_Riemann.f90:23-107) */
 #define MB_RS_HLLC 1
+#define MB_RS_HLLE 2
+#define MB_RS_SLAU 3
 #define MB_RS_AUSMP 4
+#define MB_RS_LLF 8
+#define MB_RS_SLAU2 9
 #define MB_RS_LMROE 12
 
 #define MB_PREC_FP64 0

@@ -23,8 +23,8 @@ COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-lineinfo", "-Xptxas", "-
 F64 = ["--fmad=false"]
 F32 = ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
 UNITS = [("mb_f64.cu", F64), ("mb_api.cu", F64), ("mb_noalloc.cu", F64)] + \
-        [("mb_sweep_f64_rs%d.cu" % r, F64) for r in (1, 4, 12)] + \
-        [("mb_sweep_f32_rs%d.cu" % r, F32) for r in (1, 4, 12)]
+        [("mb_sweep_f64_rs%d.cu" % r, F64) for r in (0, 1, 4, 12)] + \
+        [("mb_sweep_f32_rs%d.cu" % r, F32) for r in (0, 1, 4, 12)]
 DEPS = ["mb_physics.cuh", "mb_engine.cuh", "mb_launch.h", "mb_sweep_inst.inc",
         os.path.join("..", "..", "include", "mose_b200.h")]
 

@@ -485,7 +485,9 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
 int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int device, mb_ctx** out) {
   if (!mesh || !sc || !th || !out) return MB_E_ARG;
   *out = nullptr;
-  if (sc->riemann != MB_RS_HLLC && sc->riemann != MB_RS_AUSMP && sc->riemann != MB_RS_LMROE) return MB_E_UNSUPPORTED;
+  if (sc->riemann != MB_RS_HLLC && sc->riemann != MB_RS_HLLE && sc->riemann != MB_RS_SLAU && sc->riemann != MB_RS_AUSMP &&
+      sc->riemann != MB_RS_LLF && sc->riemann != MB_RS_SLAU2 && sc->riemann != MB_RS_LMROE)
+    return MB_E_UNSUPPORTED;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
   if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
   if (sc->precision != MB_PREC_FP64 && sc->precision != MB_PREC_MIXED) return MB_E_UNSUPPORTED;
@@ -553,8 +555,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   }
   {
     cudaError_t e = (sc->precision == MB_PREC_MIXED)
-                        ? (sc->riemann == 1 ? sweep_f32_rs1_setup() : sc->riemann == 4 ? sweep_f32_rs4_setup() : sweep_f32_rs12_setup())
-                        : (sc->riemann == 1 ? sweep_f64_rs1_setup() : sc->riemann == 4 ? sweep_f64_rs4_setup() : sweep_f64_rs12_setup());
+                        ? MB_BY_RS(f32, sc->riemann, _setup, ()) : MB_BY_RS(f64, sc->riemann, _setup, ());
     if (e != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
   }
   // ---- kernel parameters
@@ -577,8 +578,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
     const int v = sc->visc ? 1 : 0;
     int occ = (sc->precision == MB_PREC_MIXED)
-                  ? (sc->riemann == 1 ? sweep_f32_rs1_occupancy(v) : sc->riemann == 4 ? sweep_f32_rs4_occupancy(v) : sweep_f32_rs12_occupancy(v))
-                  : (sc->riemann == 1 ? sweep_f64_rs1_occupancy(v) : sc->riemann == 4 ? sweep_f64_rs4_occupancy(v) : sweep_f64_rs12_occupancy(v));
+                  ? MB_BY_RS(f32, sc->riemann, _occupancy, (v)) : MB_BY_RS(f64, sc->riemann, _occupancy, (v));
     p.pgrid = std::max(1, occ) * std::max(1, nsm);
   }
   p.queue = nullptr;
@@ -587,8 +587,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   if (getenv("MB_REPORT")) {
     const int v = sc->visc ? 1 : 0;
     int occ = (sc->precision == MB_PREC_MIXED)
-                  ? (sc->riemann == 1 ? sweep_f32_rs1_occupancy(v) : sc->riemann == 4 ? sweep_f32_rs4_occupancy(v) : sweep_f32_rs12_occupancy(v))
-                  : (sc->riemann == 1 ? sweep_f64_rs1_occupancy(v) : sc->riemann == 4 ? sweep_f64_rs4_occupancy(v) : sweep_f64_rs12_occupancy(v));
+                  ? MB_BY_RS(f32, sc->riemann, _occupancy, (v)) : MB_BY_RS(f64, sc->riemann, _occupancy, (v));
     fprintf(stderr, "[mose_b200] sweep: %s, %d threads per CTA, %d CTAs per SM, %d tiles\n",
             sc->precision == MB_PREC_MIXED ? "mixed" : "fp64", 32 * c->ty_sweep, occ, c->ntiles_sweep);
   }
@@ -674,13 +673,9 @@ static int sweep_on(mb_ctx* c, const DTile* t, int n, int persistent, int mode, 
   const double rkc = irk > 0 ? rkc_of(c->sc.n_rk, irk) : 0.0;
   cudaError_t e;
   if (c->sc.precision == MB_PREC_MIXED) {
-    if (c->sc.riemann == 1) e = sweep_f32_rs1(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s);
-    else if (c->sc.riemann == 4) e = sweep_f32_rs4(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s);
-    else e = sweep_f32_rs12(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s);
+    e = MB_BY_RS(f32, c->sc.riemann, , (p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s));
   } else {
-    if (c->sc.riemann == 1) e = sweep_f64_rs1(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s);
-    else if (c->sc.riemann == 4) e = sweep_f64_rs4(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s);
-    else e = sweep_f64_rs12(p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s);
+    e = MB_BY_RS(f64, c->sc.riemann, , (p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s));
   }
   c->launches += 1;
   CK(e);
@@ -693,13 +688,9 @@ static int records(mb_ctx* c, const double* Pin, cudaStream_t s) {
   const Params& p = c->p;
   cudaError_t e;
   if (c->sc.precision == MB_PREC_MIXED) {
-    if (c->sc.riemann == 1) e = sweep_f32_rs1_records(p, c->d_brec, c->d_bcell, c->nrec, Pin, s);
-    else if (c->sc.riemann == 4) e = sweep_f32_rs4_records(p, c->d_brec, c->d_bcell, c->nrec, Pin, s);
-    else e = sweep_f32_rs12_records(p, c->d_brec, c->d_bcell, c->nrec, Pin, s);
+    e = MB_BY_RS(f32, c->sc.riemann, _records, (p, c->d_brec, c->d_bcell, c->nrec, Pin, s));
   } else {
-    if (c->sc.riemann == 1) e = sweep_f64_rs1_records(p, c->d_brec, c->d_bcell, c->nrec, Pin, s);
-    else if (c->sc.riemann == 4) e = sweep_f64_rs4_records(p, c->d_brec, c->d_bcell, c->nrec, Pin, s);
-    else e = sweep_f64_rs12_records(p, c->d_brec, c->d_bcell, c->nrec, Pin, s);
+    e = MB_BY_RS(f64, c->sc.riemann, _records, (p, c->d_brec, c->d_bcell, c->nrec, Pin, s));
   }
   c->launches += 1;
   CK(e);

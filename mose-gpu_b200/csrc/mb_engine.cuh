@@ -197,12 +197,8 @@ MB_HD void bc_conn_eul(const Params& p, const DBlk& b, const double* __restrict_
   rotot_rtot(p, PR[0], rhoR, RRr);
   R aR = f_ss(p, PR[0], PR[MB_IPR], rhoR, RRr);
   R F_r, F_u, F_v, F_w, F_E;
-  if (rs == 1)
-    hllc(p, PL[0], PL[MB_IU], PL[MB_IV], PL[MB_IW], PL[MB_IPR], aL, rhoL, RL, PR[0], PR[MB_IU], PR[MB_IV], PR[MB_IW],
-         PR[MB_IPR], aR, rhoR, RRr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
-  else
-    riemann_open(p, rs, PL[0], PL[MB_IU], PL[MB_IV], PL[MB_IW], PL[MB_IPR], aL, rhoL, PR[0], PR[MB_IU], PR[MB_IV],
-                 PR[MB_IW], PR[MB_IPR], aR, rhoR, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
+  riemann_rec<R, RS>(p, PL[0], PL[MB_IU], PL[MB_IV], PL[MB_IW], PL[MB_IPR], aL, rhoL, RL, PR[0], PR[MB_IU], PR[MB_IV],
+                     PR[MB_IW], PR[MB_IPR], aR, rhoR, RRr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
   R su = copysign((R)0.5, F_r), selL = (R)0.5 + su, selR = su - (R)0.5;
   R Fmass = F_r * area;
   R sg = (R)modfm2;
@@ -308,19 +304,6 @@ MB_HD void bc_extrap(const Params& p, const DBlk& b, const double* __restrict__ 
   R sg = (R)face_sign(Fm);
 #pragma unroll
   for (int s = 0; s < MB_NP; ++s) A[s] = sg * F[s];
-}
-
-// the Riemann dispatch of the record routines (Lib_Riemann.f90:120-140): HLLC Batten for rs 1, the MOSE_open
-// solvers otherwise
-template <typename R, int RS = 0>
-MB_HD void riemann_rec(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R Rl, R dr, R ur, R vr, R wr,
-                       R pr, R ar, R drtot, R Rr, R nx, R ny, R nz, R& F_r, R& F_u, R& F_v, R& F_w, R& F_E) {
-  const int rs = RS ? RS : p.rs;
-  if (rs == 1)
-    hllc(p, dl, ul, vl, wl, pl, al, dltot, Rl, dr, ur, vr, wr, pr, ar, drtot, Rr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
-  else
-    riemann_open(p, rs, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r, F_u, F_v, F_w,
-                 F_E);
 }
 
 // BC_Symmetry_Eul (Lib_BC.f90:640-737): mirror of the boundary cell about the face, limited one-sided

@@ -57,6 +57,13 @@ MB_DECLARE_SWEEP(sweep_f64_rs12)
 MB_DECLARE_SWEEP(sweep_f32_rs1)
 MB_DECLARE_SWEEP(sweep_f32_rs4)
 MB_DECLARE_SWEEP(sweep_f32_rs12)
+MB_DECLARE_SWEEP(sweep_f64_rs0)
+MB_DECLARE_SWEEP(sweep_f32_rs0)
+// the sweep unit of a Riemann solver id: one unit per benchmarked solver (the id a compile-time constant there), the
+// rs0 units (the id read at run time) for the others
+#define MB_BY_RS(form, rs, fn, args)                                                                        \
+  ((rs) == 1 ? sweep_##form##_rs1##fn args                                                                  \
+             : (rs) == 4 ? sweep_##form##_rs4##fn args : (rs) == 12 ? sweep_##form##_rs12##fn args : sweep_##form##_rs0##fn args)
 
 // ghost fill; *nl receives the number of kernels launched
 cudaError_t ghost_fill(const Params& p, const GhostLists& g, double* P, cudaStream_t s, int* nl);

@@ -358,6 +358,67 @@ MB_HD void riemann_open(const Params& p, int rs, R dl, R ul, R vl, R wl, R pl, R
     F_E = mdotp * H_L + mdotm * H_R;
     return;
   }
+  if (rs == 8) {  // LLF / Rusanov (riemann_open_body.inc:244-278)
+    R lf_a = mx(mx(fabs(unl - al), fabs(unr - ar)), mx(fabs(unl + al), fabs(unr + ar)));
+    R rho_ = (R)0 + dr;
+    R Hs_R = h_static(p, dr, pr);
+    R vel_ = rsqrt_(ur * ur + vr * vr + wr * wr);
+    R FrR = rho_ * (ur * nx + vr * ny + wr * nz);
+    R Fur = FrR * ur + pr * nx, Fvr = FrR * vr + pr * ny, Fwr = FrR * wr + pr * nz;
+    R Fer = FrR * (Hs_R + (R)0.5 * vel_ * vel_);
+    R e0r_ = (Hs_R - pr / rho_) + (R)0.5 * vel_ * vel_;
+    rho_ = (R)0 + dl;
+    R Hs_L = h_static(p, dl, pl);
+    vel_ = rsqrt_(ul * ul + vl * vl + wl * wl);
+    R FrL = rho_ * (ul * nx + vl * ny + wl * nz);
+    R Ful = FrL * ul + pl * nx, Fvl = FrL * vl + pl * ny, Fwl = FrL * wl + pl * nz;
+    R Fel = FrL * (Hs_L + (R)0.5 * vel_ * vel_);
+    R e0l_ = (Hs_L - pl / rho_) + (R)0.5 * vel_ * vel_;
+    F_r = (R)0.5 * (FrL + FrR - lf_a * (drtot - dltot));
+    F_u = (R)0.5 * (Fur + Ful - lf_a * (drtot * ur - dltot * ul));
+    F_v = (R)0.5 * (Fvr + Fvl - lf_a * (drtot * vr - dltot * vl));
+    F_w = (R)0.5 * (Fwr + Fwl - lf_a * (drtot * wr - dltot * wl));
+    F_E = (R)0.5 * (Fel + Fer - lf_a * (drtot * e0r_ - dltot * e0l_));
+    return;
+  }
+  if (rs == 9) {  // SLAU2 (riemann_open_body.inc:280-347): SLAU with the Kitamura-Shima 2013 pressure flux
+    // the reference holds F_r, the pressure flux and H to +-1e150; FP32 holds them to +-3e38 (1e150 is inf there)
+    const R big = (R)(sizeof(R) == 4 ? 3.0e38 : 1.0e150);
+    R Vl2 = ul * ul + vl * vl + wl * wl;
+    R Vr2 = ur * ur + vr * vr + wr * wr;
+    R af = (R)0.5 * (al + ar);
+    R ml = unl / af, mr = unr / af;
+    R mt = mn((R)1, rsqrt_((R)0.5 * (Vl2 + Vr2)) / af);
+    R chi = ((R)1 - mt) * ((R)1 - mt);
+    R vnm = (dltot * fabs(unl) + drtot * fabs(unr)) / (dltot + drtot);
+    R frho = -mx(mn(ml, (R)0), (R)(-1)) * mn(mx(mr, (R)0), (R)1);
+    R vnl = ((R)1 - frho) * vnm + frho * fabs(unl);
+    R vnr = ((R)1 - frho) * vnm + frho * fabs(unr);
+    F_r = (R)0.5 * (dltot * (unl + vnl) + drtot * (unr - vnr) - (chi / af) * (pr - pl));
+    F_r = mx(-big, mn(F_r, big));
+    R bl, br;
+    if (fabs(ml) < (R)1) bl = (R)0.25 * ((R)2 - ml) * ((ml + (R)1) * (ml + (R)1));
+    else if (ml >= (R)0) bl = (R)1;
+    else bl = (R)0;
+    if (fabs(mr) < (R)1) br = (R)0.25 * ((R)2 + mr) * ((mr - (R)1) * (mr - (R)1));
+    else if (mr >= (R)0) br = (R)0;
+    else br = (R)1;
+    R ph = (R)0.5 * (pl + pr) + (R)0.5 * (bl - br) * (pl - pr) +
+           rsqrt_((R)0.5 * (Vl2 + Vr2)) * (bl + br - (R)1) * af * (R)0.5 * (dltot + drtot);
+    ph = mx(-big, mn(ph, big));
+    R Hs_L = h_static(p, dl, pl);
+    R Hs_R = h_static(p, dr, pr);
+    R H_L = Hs_L + (R)0.5 * rsqrt_(Vl2) * rsqrt_(Vl2);
+    R H_R = Hs_R + (R)0.5 * rsqrt_(Vr2) * rsqrt_(Vr2);
+    H_L = mx(-big, mn(H_L, big));
+    H_R = mx(-big, mn(H_R, big));
+    if (F_r >= (R)0) {
+      F_u = F_r * ul + nx * ph; F_v = F_r * vl + ny * ph; F_w = F_r * wl + nz * ph; F_E = F_r * H_L;
+    } else {
+      F_u = F_r * ur + nx * ph; F_v = F_r * vr + ny * ph; F_w = F_r * wr + nz * ph; F_E = F_r * H_R;
+    }
+    return;
+  }
   const R* H = Tab<R>::h(p);
   const R* CP = Tab<R>::cp(p);
   R rho_, Rl, Rr;
@@ -547,11 +608,76 @@ MB_HD void lmroe_fast(const Params& p, R dl, R ul, R vl, R wl, R pl, R Tl, int T
 
 // Roe averages shared by the two HLLC forms: the inline one of conv_physics.inc (clamped T row, Rl/Rr
 // taken from the caller) and riemann_HLLC / roe_averages of Lib_Riemann_HLL.f90 (boundary records).
+// SLAU flux from the two states and their total enthalpies (riemann_SLAU_base + riemann_SLAU: conv_physics.inc:125-159
+// = Lib_Riemann.f90:167-196, the same statements)
+template <typename R>
+MB_HD void slau_flux(R ul, R vl, R wl, R pl, R al, R dltot, R h0l, R ur, R vr, R wr, R pr, R ar, R drtot, R h0r, R unl,
+                     R unr, R nx, R ny, R nz, R& F_r, R& F_u, R& F_v, R& F_w, R& F_E) {
+  R af_ = (R)0.5 * (al + ar);
+  R ml_ = unl / af_, mr_ = unr / af_;
+  R mt_ = mn((R)1, rsqrt_((R)0.5 * ((ul * ul + vl * vl + wl * wl) + (ur * ur + vr * vr + wr * wr))) / af_);
+  R chi_ = ((R)1 - mt_) * ((R)1 - mt_);
+  R vnm_ = (dltot * fabs(unl) + drtot * fabs(unr)) / (dltot + drtot);
+  R frho_ = -mx(mn(ml_, (R)0), (R)(-1)) * mn(mx(mr_, (R)0), (R)1);
+  R vnl_ = ((R)1 - frho_) * vnm_ + frho_ * fabs(unl);
+  R vnr_ = ((R)1 - frho_) * vnm_ + frho_ * fabs(unr);
+  F_r = (R)0.5 * (dltot * (unl + vnl_) + drtot * (unr - vnr_) - (chi_ / af_) * (pr - pl));
+  R bl_, br_;
+  if (fabs(ml_) < (R)1) bl_ = (R)0.25 * ((R)2 - ml_) * ((ml_ + (R)1) * (ml_ + (R)1));
+  else if (ml_ >= (R)0) bl_ = (R)1;
+  else bl_ = (R)0;
+  if (fabs(mr_) < (R)1) br_ = (R)0.25 * ((R)2 + mr_) * ((mr_ - (R)1) * (mr_ - (R)1));
+  else if (mr_ >= (R)0) br_ = (R)0;
+  else br_ = (R)1;
+  R ph_ = (R)0.5 * (pl + pr) + (R)0.5 * (bl_ - br_) * (pl - pr) + ((R)1 - chi_) * (bl_ + br_ - (R)1) * (R)0.5 * (pl + pr);
+  if (F_r >= (R)0) {
+    F_u = F_r * ul + nx * ph_; F_v = F_r * vl + ny * ph_; F_w = F_r * wl + nz * ph_; F_E = F_r * h0l;
+  } else {
+    F_u = F_r * ur + nx * ph_; F_v = F_r * vr + ny * ph_; F_w = F_r * wr + nz * ph_; F_E = F_r * h0r;
+  }
+}
+
+// HLLE two-wave flux with the Batten signal speeds (Lib_Riemann_HLL.f90:176-196 = conv_physics.inc:116-124)
+template <typename R>
+MB_HD void hlle_flux(R ul, R vl, R wl, R pl, R dltot, R h0l, R ur, R vr, R wr, R pr, R drtot, R h0r, R unl, R unr, R S1,
+                     R S4, R nx, R ny, R nz, R& F_r, R& F_u, R& F_v, R& F_w, R& F_E) {
+  R inv_denom = (R)1 / (S4 - S1);
+  R FrL = dltot * unl, FrR = drtot * unr;
+  F_r = (S4 * FrL - S1 * FrR + S1 * S4 * (drtot - dltot)) * inv_denom;
+  F_u = (S4 * (FrL * ul + pl * nx) - S1 * (FrR * ur + pr * nx) + S1 * S4 * (drtot * ur - dltot * ul)) * inv_denom;
+  F_v = (S4 * (FrL * vl + pl * ny) - S1 * (FrR * vr + pr * ny) + S1 * S4 * (drtot * vr - dltot * vl)) * inv_denom;
+  F_w = (S4 * (FrL * wl + pl * nz) - S1 * (FrR * wr + pr * nz) + S1 * S4 * (drtot * wr - dltot * wl)) * inv_denom;
+  F_E = (S4 * (FrL * h0l) - S1 * (FrR * h0r) + S1 * S4 * (drtot * (h0r - pr / drtot) - dltot * (h0l - pl / dltot))) *
+        inv_denom;
+}
+
+// SLAU at the boundary records (Lib_Riemann.f90:140-197): T = p / (rho R) and H0 = h(T) + V^2/2 of each state from
+// the tables (no T clamp), then the SLAU flux
+template <typename R>
+MB_HD void slau_rec(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R dr, R ur, R vr, R wr, R pr, R ar,
+                    R drtot, R nx, R ny, R nz, R& F_r, R& F_u, R& F_v, R& F_w, R& F_E) {
+  const R* H = Tab<R>::h(p);
+  const R ri = (R)(RUNIV / p.wm);
+  R unl = ul * nx + vl * ny + wl * nz;
+  R unr = ur * nx + vr * ny + wr * nz;
+  R Rl = (R)0 + ri * dl / dltot;
+  R Rr = (R)0 + ri * dr / drtot;
+  R Tl = pl / (dltot * Rl), Tr = pr / (drtot * Rr);
+  int Til = (int)Tl, Tir = (int)Tr;
+  R dTl = Tl - (R)Til, dTr = Tr - (R)Tir;
+  R h0l = (R)0 + (H[Til] + (H[Til + 1] - H[Til]) * dTl) * dl / dltot;
+  R h0r = (R)0 + (H[Tir] + (H[Tir + 1] - H[Tir]) * dTr) * dr / drtot;
+  h0l = h0l + (R)0.5 * (ul * ul + vl * vl + wl * wl);
+  h0r = h0r + (R)0.5 * (ur * ur + vr * vr + wr * wr);
+  slau_flux(ul, vl, wl, pl, al, dltot, h0l, ur, vr, wr, pr, ar, drtot, h0r, unl, unr, nx, ny, nz, F_r, F_u, F_v, F_w,
+            F_E);
+}
+
 template <typename R>
 MB_HD void hllc(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R Rl, R dr, R ur,
                                      R vr, R wr, R pr, R ar, R drtot, R Rr, R nx, R ny, R nz, R& F_r, R& F_u,
                                      R& F_v, R& F_w, R& F_E, const R* thL = nullptr, const R* thR = nullptr,
-                                     int tiL = 0, int tiR = 0) {
+                                     int tiL = 0, int tiR = 0, int tail = 1) {
   // thL / thR (the mixed form, from the caller's reconstruction): T, its table fraction and cp of each state
   const R* H = Tab<R>::h(p);
   const R* CP = Tab<R>::cp(p);
@@ -598,6 +724,16 @@ MB_HD void hllc(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R 
   R e0l = h0l - pl / dltot, e0r = h0r - pr / drtot;
   R S1 = mn(mn((R)0, unl - al), un_roe - a_roe);
   R S4 = mx(mx((R)0, unr + ar), un_roe + a_roe);
+  if (tail == 2) {  // HLLE
+    hlle_flux(ul, vl, wl, pl, dltot, h0l, ur, vr, wr, pr, drtot, h0r, unl, unr, S1, S4, nx, ny, nz, F_r, F_u, F_v, F_w,
+              F_E);
+    return;
+  }
+  if (tail == 3) {  // SLAU (the interior face: the total enthalpies of this prologue)
+    slau_flux(ul, vl, wl, pl, al, dltot, h0l, ur, vr, wr, pr, ar, drtot, h0r, unl, unr, nx, ny, nz, F_r, F_u, F_v, F_w,
+              F_E);
+    return;
+  }
   R inv_denom = (R)1 / (dltot * (S1 - unl) - drtot * (S4 - unr));
   R Sstar = (pr - pl + dltot * unl * (S1 - unl) - drtot * unr * (S4 - unr)) * inv_denom;
   R pstar = dltot * (unl - S1) * (unl - Sstar) + pl;
@@ -676,11 +812,11 @@ MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, c
     const R cp1 = CP[Ti1] + (CP[Ti1 + 1] - CP[Ti1]) * Td1;
     lmroe_fast(p, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], T1d, Ti1, Td1, cp1, P4[0], P4[MB_IU],
                P4[MB_IV], P4[MB_IW], P4[MB_IPR], T4d, Ti4, Tdiffd, cpd, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
-  } else if (rs == 1) {
+  } else if (rs == 1 || rs == 2 || rs == 3) {  // HLLC, HLLE, SLAU after the Roe-average prologue of conv_physics.inc
     const R th1[3] = {T1d, Td1, CP[Ti1] + (CP[Ti1 + 1] - CP[Ti1]) * Td1}, th4[3] = {T4d, Tdiffd, cpd};
     hllc(p, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], a1, rotot1, Rtot1, P4[0], P4[MB_IU], P4[MB_IV],
          P4[MB_IW], P4[MB_IPR], a4, rotot4, Rtot4, nx, ny, nz, F_r, F_u, F_v, F_w, F_E,
-         Fast<R>::on ? th1 : nullptr, Fast<R>::on ? th4 : nullptr, Ti1, Ti4);
+         Fast<R>::on ? th1 : nullptr, Fast<R>::on ? th4 : nullptr, Ti1, Ti4, rs);
   }
   else
     riemann_open(p, rs, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], a1, rotot1, P4[0], P4[MB_IU],
@@ -693,6 +829,22 @@ MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, c
     res0[0] = F_r * area * (sp * (P1[0] * irotot1) - sm * (P4[0] * irotot4));
   }
   res0[MB_IU] = F_u * area; res0[MB_IV] = F_v * area; res0[MB_IW] = F_w * area; res0[MB_IPR] = F_E * area;
+}
+
+// the Riemann dispatch of the record routines (Lib_Riemann.f90:114-136, `Riemann`): HLLC Batten for rs 1, HLLE for
+// 2 (both after roe_averages), SLAU for 3, the MOSE_open solvers otherwise
+template <typename R, int RS = 0>
+MB_HD void riemann_rec(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R Rl, R dr, R ur, R vr, R wr,
+                       R pr, R ar, R drtot, R Rr, R nx, R ny, R nz, R& F_r, R& F_u, R& F_v, R& F_w, R& F_E) {
+  const int rs = RS ? RS : p.rs;
+  if (rs == 1 || rs == 2)
+    hllc(p, dl, ul, vl, wl, pl, al, dltot, Rl, dr, ur, vr, wr, pr, ar, drtot, Rr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E,
+         (const R*)nullptr, (const R*)nullptr, 0, 0, rs);
+  else if (rs == 3)
+    slau_rec(p, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
+  else
+    riemann_open(p, rs, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r, F_u, F_v, F_w,
+                 F_E);
 }
 
 // face thermo (Diffusive_Face_Thermo_Fill, Mod_Diffusive.f90:311-325 = Diffusive_Face_State :748-776)

@@ -14,7 +14,10 @@
 //   convective face         src/lib/gpu/conv_physics.inc:1-179, Mod_Convective.f90:288-412
 //   limiter                 src/lib/numerics/space/Lib_Limiters.f90:65-97 (Mod_Convective.f90:161-191)
 //   AUSM+, LMRoe            src/lib/numerics/fluxes/riemann_open_body.inc:100-150, 679-730, 965-1091
-//   HLLC at boundary faces  src/lib/numerics/fluxes/Lib_Riemann_HLL.f90:21-134, 209-310
+//   LLF, SLAU2              src/lib/numerics/fluxes/riemann_open_body.inc:244-347
+//   HLLC, HLLE at records   src/lib/numerics/fluxes/Lib_Riemann_HLL.f90:21-198, 209-310
+//   HLLE, SLAU interior     src/lib/gpu/conv_physics.inc:116-159
+//   SLAU at records         src/lib/numerics/fluxes/Lib_Riemann.f90:138-197
 //   face thermo + viscous   src/lib/numerics/fluxes/Mod_Diffusive.f90:248-373, gpu/diff_cuf_kernels.inc:11-87,
 //                           gpu/diff_physics.inc:1-161
 //   pass 2                  src/lib/gpu/pass2_body.inc:1-61
@@ -195,7 +198,50 @@ inline double rlimiter(int lim, double x, double y) {
 
 inline double fsign_half(double f) { return std::copysign(0.5, f); }
 
-// ---- the MOSE_open solvers of riemann_open_body.inc used here: AUSM+ (4), LMRoe (12) ----
+// SLAU flux from the two states and their total enthalpies h0l / h0r (Liou-Shima: riemann_SLAU_base +
+// riemann_SLAU; the statements of conv_physics.inc:125-159 and Lib_Riemann.f90:167-196, which are the same)
+void slau_flux(double ul, double vl, double wl, double pl, double al, double dltot, double h0l, double ur, double vr,
+               double wr, double pr, double ar, double drtot, double h0r, double unl, double unr, double nx, double ny,
+               double nz, double& F_r, double& F_u, double& F_v, double& F_w, double& F_E) {
+  double af_ = 0.5 * (al + ar);
+  double ml_ = unl / af_, mr_ = unr / af_;
+  double mt_ = std::min(1.0, std::sqrt(0.5 * ((ul * ul + vl * vl + wl * wl) + (ur * ur + vr * vr + wr * wr))) / af_);
+  double chi_ = (1.0 - mt_) * (1.0 - mt_);
+  double vnm_ = (dltot * std::fabs(unl) + drtot * std::fabs(unr)) / (dltot + drtot);
+  double frho_ = -std::max(std::min(ml_, 0.0), -1.0) * std::min(std::max(mr_, 0.0), 1.0);
+  double vnl_ = (1.0 - frho_) * vnm_ + frho_ * std::fabs(unl);
+  double vnr_ = (1.0 - frho_) * vnm_ + frho_ * std::fabs(unr);
+  F_r = 0.5 * (dltot * (unl + vnl_) + drtot * (unr - vnr_) - (chi_ / af_) * (pr - pl));
+  double bl_, br_;
+  if (std::fabs(ml_) < 1.0) bl_ = 0.25 * (2.0 - ml_) * ((ml_ + 1.0) * (ml_ + 1.0));
+  else if (ml_ >= 0.0) bl_ = 1.0;
+  else bl_ = 0.0;
+  if (std::fabs(mr_) < 1.0) br_ = 0.25 * (2.0 + mr_) * ((mr_ - 1.0) * (mr_ - 1.0));
+  else if (mr_ >= 0.0) br_ = 0.0;
+  else br_ = 1.0;
+  double ph_ = 0.5 * (pl + pr) + 0.5 * (bl_ - br_) * (pl - pr) + (1.0 - chi_) * (bl_ + br_ - 1.0) * 0.5 * (pl + pr);
+  if (F_r >= 0.0) {
+    F_u = F_r * ul + nx * ph_; F_v = F_r * vl + ny * ph_; F_w = F_r * wl + nz * ph_; F_E = F_r * h0l;
+  } else {
+    F_u = F_r * ur + nx * ph_; F_v = F_r * vr + ny * ph_; F_w = F_r * wr + nz * ph_; F_E = F_r * h0r;
+  }
+}
+
+// HLLE two-wave flux with the Batten signal speeds S1, S4 (Lib_Riemann_HLL.f90:176-196 = conv_physics.inc:116-124)
+void hlle_flux(double ul, double vl, double wl, double pl, double dltot, double h0l, double ur, double vr, double wr,
+               double pr, double drtot, double h0r, double unl, double unr, double S1, double S4, double nx, double ny,
+               double nz, double& F_r, double& F_u, double& F_v, double& F_w, double& F_E) {
+  double inv_denom = 1.0 / (S4 - S1);
+  double FrL = dltot * unl, FrR = drtot * unr;
+  F_r = (S4 * FrL - S1 * FrR + S1 * S4 * (drtot - dltot)) * inv_denom;
+  F_u = (S4 * (FrL * ul + pl * nx) - S1 * (FrR * ur + pr * nx) + S1 * S4 * (drtot * ur - dltot * ul)) * inv_denom;
+  F_v = (S4 * (FrL * vl + pl * ny) - S1 * (FrR * vr + pr * ny) + S1 * S4 * (drtot * vr - dltot * vl)) * inv_denom;
+  F_w = (S4 * (FrL * wl + pl * nz) - S1 * (FrR * wr + pr * nz) + S1 * S4 * (drtot * wr - dltot * wl)) * inv_denom;
+  F_E = (S4 * (FrL * h0l) - S1 * (FrR * h0r) + S1 * S4 * (drtot * (h0r - pr / drtot) - dltot * (h0l - pl / dltot))) *
+        inv_denom;
+}
+
+// ---- the MOSE_open solvers of riemann_open_body.inc used here: AUSM+ (4), LLF (8), SLAU2 (9), LMRoe (12) ----
 // Thermo as written there: T clamped to [tmin, tmax-1] before the table lookup (H / H0 of FLINT).
 inline double h_static(const Thermo& th, double rhoi, double p) {
   double rho_ = 0.0 + rhoi;
@@ -248,6 +294,66 @@ void riemann_open(const Thermo& th, int rs, double mco, double dl, double ul, do
     F_v = mdotp * vl + mdotm * vr + ny * phalf;
     F_w = mdotp * wl + mdotm * wr + nz * phalf;
     F_E = mdotp * H_L + mdotm * H_R;
+    return;
+  }
+  if (rs == 8) {  // LLF / Rusanov (riemann_open_body.inc:244-278)
+    double lf_a = std::max(std::max(std::fabs(unl - al), std::fabs(unr - ar)),
+                           std::max(std::fabs(unl + al), std::fabs(unr + ar)));
+    double rho_ = 0.0 + dr;
+    double Hs_R = h_static(th, dr, pr);
+    double vel_ = std::sqrt(ur * ur + vr * vr + wr * wr);
+    double FrR = rho_ * (ur * nx + vr * ny + wr * nz);
+    double Fur = FrR * ur + pr * nx, Fvr = FrR * vr + pr * ny, Fwr = FrR * wr + pr * nz;
+    double Fer = FrR * (Hs_R + 0.5 * vel_ * vel_);
+    double e0r_ = (Hs_R - pr / rho_) + 0.5 * vel_ * vel_;
+    rho_ = 0.0 + dl;
+    double Hs_L = h_static(th, dl, pl);
+    vel_ = std::sqrt(ul * ul + vl * vl + wl * wl);
+    double FrL = rho_ * (ul * nx + vl * ny + wl * nz);
+    double Ful = FrL * ul + pl * nx, Fvl = FrL * vl + pl * ny, Fwl = FrL * wl + pl * nz;
+    double Fel = FrL * (Hs_L + 0.5 * vel_ * vel_);
+    double e0l_ = (Hs_L - pl / rho_) + 0.5 * vel_ * vel_;
+    F_r = 0.5 * (FrL + FrR - lf_a * (drtot - dltot));
+    F_u = 0.5 * (Fur + Ful - lf_a * (drtot * ur - dltot * ul));
+    F_v = 0.5 * (Fvr + Fvl - lf_a * (drtot * vr - dltot * vl));
+    F_w = 0.5 * (Fwr + Fwl - lf_a * (drtot * wr - dltot * wl));
+    F_E = 0.5 * (Fel + Fer - lf_a * (drtot * e0r_ - dltot * e0l_));
+    return;
+  }
+  if (rs == 9) {  // SLAU2 (riemann_open_body.inc:280-347): SLAU with the Kitamura-Shima 2013 pressure flux
+    double Vl2 = ul * ul + vl * vl + wl * wl;
+    double Vr2 = ur * ur + vr * vr + wr * wr;
+    double af = 0.5 * (al + ar);
+    double ml = unl / af, mr = unr / af;
+    double mt = std::min(1.0, std::sqrt(0.5 * (Vl2 + Vr2)) / af);
+    double chi = (1.0 - mt) * (1.0 - mt);
+    double vnm = (dltot * std::fabs(unl) + drtot * std::fabs(unr)) / (dltot + drtot);
+    double frho = -std::max(std::min(ml, 0.0), -1.0) * std::min(std::max(mr, 0.0), 1.0);
+    double vnl = (1.0 - frho) * vnm + frho * std::fabs(unl);
+    double vnr = (1.0 - frho) * vnm + frho * std::fabs(unr);
+    F_r = 0.5 * (dltot * (unl + vnl) + drtot * (unr - vnr) - (chi / af) * (pr - pl));
+    F_r = std::max(-1.0e150, std::min(F_r, 1.0e150));
+    double bl, br;
+    if (std::fabs(ml) < 1.0) bl = 0.25 * (2.0 - ml) * ((ml + 1.0) * (ml + 1.0));
+    else if (ml >= 0.0) bl = 1.0;
+    else bl = 0.0;
+    if (std::fabs(mr) < 1.0) br = 0.25 * (2.0 + mr) * ((mr - 1.0) * (mr - 1.0));
+    else if (mr >= 0.0) br = 0.0;
+    else br = 1.0;
+    double ph = 0.5 * (pl + pr) + 0.5 * (bl - br) * (pl - pr) +
+                std::sqrt(0.5 * (Vl2 + Vr2)) * (bl + br - 1.0) * af * 0.5 * (dltot + drtot);
+    ph = std::max(-1.0e150, std::min(ph, 1.0e150));
+    double Hs_L = h_static(th, dl, pl);
+    double Hs_R = h_static(th, dr, pr);
+    double H_L = Hs_L + 0.5 * std::sqrt(Vl2) * std::sqrt(Vl2);
+    double H_R = Hs_R + 0.5 * std::sqrt(Vr2) * std::sqrt(Vr2);
+    H_L = std::max(-1.0e150, std::min(H_L, 1.0e150));
+    H_R = std::max(-1.0e150, std::min(H_R, 1.0e150));
+    if (F_r >= 0.0) {
+      F_u = F_r * ul + nx * ph; F_v = F_r * vl + ny * ph; F_w = F_r * wl + nz * ph; F_E = F_r * H_L;
+    } else {
+      F_u = F_r * ur + nx * ph; F_v = F_r * vr + ny * ph; F_w = F_r * wr + nz * ph; F_E = F_r * H_R;
+    }
     return;
   }
   // rs == 12: Roe averages (riemann_open_body.inc:679-730) then LMRoe (:965-1091)
@@ -341,8 +447,9 @@ void riemann_open(const Thermo& th, int rs, double mco, double dl, double ul, do
   F_E = 0.5 * (FL5 + FR5) - 0.5 * d[4];
 }
 
-// HLLC of Lib_Riemann_HLL.f90:21-134 with roe_averages :209-310 (boundary records; no T clamp)
-void riemann_hllc_bc(const Thermo& th, double dl, double ul, double vl, double wl, double pl, double al,
+// HLLC (rs 1) / HLLE (rs 2) of Lib_Riemann_HLL.f90:21-134 / 137-198 with roe_averages :209-310 (boundary records;
+// no T clamp)
+void riemann_hllc_bc(const Thermo& th, int rs, double dl, double ul, double vl, double wl, double pl, double al,
                      double dltot, double dr, double ur, double vr, double wr, double pr, double ar, double drtot,
                      double nx, double ny, double nz, double& F_r, double& F_u, double& F_v, double& F_w,
                      double& F_E) {
@@ -384,6 +491,11 @@ void riemann_hllc_bc(const Thermo& th, double dl, double ul, double vl, double w
   double e0l = h0l - pl / dltot, e0r = h0r - pr / drtot;
   double S1 = std::min(std::min(0.0, unl - al), un_roe - a_roe);
   double S4 = std::max(std::max(0.0, unr + ar), un_roe + a_roe);
+  if (rs == 2) {
+    hlle_flux(ul, vl, wl, pl, dltot, h0l, ur, vr, wr, pr, drtot, h0r, unl, unr, S1, S4, nx, ny, nz, F_r, F_u, F_v, F_w,
+              F_E);
+    return;
+  }
   double inv_denom = 1.0 / (dltot * (S1 - unl) - drtot * (S4 - unr));
   double Sstar = (pr - pl + dltot * unl * (S1 - unl) - drtot * unr * (S4 - unr)) * inv_denom;
   double pstar = dltot * (unl - S1) * (unl - Sstar) + pl;
@@ -412,6 +524,26 @@ void riemann_hllc_bc(const Thermo& th, double dl, double ul, double vl, double w
   } else {
     F_r = drtot * unr; F_u = F_r * ur + pr * nx; F_v = F_r * vr + pr * ny; F_w = F_r * wr + pr * nz; F_E = F_r * h0r;
   }
+}
+
+// SLAU at the records (Lib_Riemann.f90:140-197): T = p / (rho R) and H0 = h(T) + V^2/2 of each state from the
+// tables (no T clamp), then the SLAU flux
+void riemann_slau_bc(const Thermo& th, double dl, double ul, double vl, double wl, double pl, double al, double dltot,
+                     double dr, double ur, double vr, double wr, double pr, double ar, double drtot, double nx,
+                     double ny, double nz, double& F_r, double& F_u, double& F_v, double& F_w, double& F_E) {
+  double unl = ul * nx + vl * ny + wl * nz;
+  double unr = ur * nx + vr * ny + wr * nz;
+  double Rl = 0.0 + th.ri * dl / dltot;
+  double Rr = 0.0 + th.ri * dr / drtot;
+  double Tl = pl / (dltot * Rl), Tr = pr / (drtot * Rr);
+  int Til = (int)Tl, Tir = (int)Tr;
+  double dTl = Tl - Til, dTr = Tr - Tir;
+  double h0l = 0.0 + (th.h[Til] + (th.h[Til + 1] - th.h[Til]) * dTl) * dl / dltot;
+  double h0r = 0.0 + (th.h[Tir] + (th.h[Tir + 1] - th.h[Tir]) * dTr) * dr / drtot;
+  h0l = h0l + 0.5 * (ul * ul + vl * vl + wl * wl);
+  h0r = h0r + 0.5 * (ur * ur + vr * vr + wr * wr);
+  slau_flux(ul, vl, wl, pl, al, dltot, h0l, ur, vr, wr, pr, ar, drtot, h0r, unl, unr, nx, ny, nz, F_r, F_u, F_v, F_w,
+            F_E);
 }
 
 // ---- one interior convective face: conv_physics.inc:1-179 ----
@@ -456,7 +588,7 @@ void conv_face(const Ctx& c, const double* pm1, const double* p0, const double* 
   double ur = P4[IU], vr = P4[IV], wr = P4[IW], pr = P4[IP], ar = a4;
   double nx = nrm[0], ny = nrm[1], nz = nrm[2];
   double F_r, F_u, F_v, F_w, F_E;
-  if (rsv == 1) {
+  if (rsv == 1 || rsv == 2 || rsv == 3) {  // the prologue of conv_physics.inc:49-86, then the solver's flux
     double unl = ul * nx + vl * ny + wl * nz;
     double unr = ur * nx + vr * ny + wr * nz;
     double Rl = Rtot1, Rr = Rtot4;
@@ -495,7 +627,13 @@ void conv_face(const Ctx& c, const double* pm1, const double* p0, const double* 
     double inv_denom = 1.0 / (dltot * (S1 - unl) - drtot * (S4 - unr));
     double Sstar = (pr - pl + dltot * unl * (S1 - unl) - drtot * unr * (S4 - unr)) * inv_denom;
     double pstar = dltot * (unl - S1) * (unl - Sstar) + pl;
-    if (S1 >= 0.0) {
+    if (rsv == 2) {
+      hlle_flux(ul, vl, wl, pl, dltot, h0l, ur, vr, wr, pr, drtot, h0r, unl, unr, S1, S4, nx, ny, nz, F_r, F_u, F_v,
+                F_w, F_E);
+    } else if (rsv == 3) {
+      slau_flux(ul, vl, wl, pl, al, dltot, h0l, ur, vr, wr, pr, ar, drtot, h0r, unl, unr, nx, ny, nz, F_r, F_u, F_v,
+                F_w, F_E);
+    } else if (S1 >= 0.0) {
       F_r = dltot * unl; F_u = F_r * ul + pl * nx; F_v = F_r * vl + pl * ny; F_w = F_r * wl + pl * nz; F_E = F_r * h0l;
     } else if (Sstar >= 0.0) {
       F_r = dltot * unl; F_u = F_r * ul + pl * nx; F_v = F_r * vl + pl * ny; F_w = F_r * wl + pl * nz; F_E = F_r * h0l;
@@ -689,6 +827,10 @@ void bc_face_geom(const Blk& b, int Im, int Jm, int Km, int Fm, double* nrm, dou
   nrm[0] = f[0]; nrm[1] = f[1]; nrm[2] = f[2]; area = f[3];
 }
 
+void riemann_rec(const Ctx& c, double dl, double ul, double vl, double wl, double pl, double al, double dltot,
+                 double dr, double ur, double vr, double wr, double pr, double ar, double drtot, double nx, double ny,
+                 double nz, double& F_r, double& F_u, double& F_v, double& F_w, double& F_E);
+
 // BC_Connection_Eul_lean (Lib_BC.f90:1770-1867)
 void bc_connection_eul(const Ctx& c, const Blk& b, const double* P, double* R, int Im, int Jm, int Km, int Fm) {
   const int64_t nc = c.ncell;
@@ -725,12 +867,8 @@ void bc_connection_eul(const Ctx& c, const Blk& b, const double* P, double* R, i
   rotot_rtot(th, PR[0], rhoR, RR);
   double aR = f_ss(th, PR[0], PR[IP], rhoR, RR);
   double F_r, F_u, F_v, F_w, F_E;
-  if (c.sc.riemann == 1)
-    riemann_hllc_bc(th, PL[0], PL[IU], PL[IV], PL[IW], PL[IP], aL, rhoL, PR[0], PR[IU], PR[IV], PR[IW], PR[IP], aR, rhoR,
-                    nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E);
-  else
-    riemann_open(th, c.sc.riemann, c.sc.mco, PL[0], PL[IU], PL[IV], PL[IW], PL[IP], aL, rhoL, PR[0], PR[IU], PR[IV],
-                 PR[IW], PR[IP], aR, rhoR, nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E);
+  riemann_rec(c, PL[0], PL[IU], PL[IV], PL[IW], PL[IP], aL, rhoL, PR[0], PR[IU], PR[IV], PR[IW], PR[IP], aR, rhoR,
+              nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E);
   double su = fsign_half(F_r), selL = 0.5 + su, selR = su - 0.5;
   double Fmass = F_r * area;
   int64_t rm = row(b, Im, Jm, Km);
@@ -827,13 +965,16 @@ void bc_extrapolation(const Ctx& c, const Blk& b, const double* P, double* R, in
   for (int s = 0; s < NP; ++s) R[r + s * nc] = R[r + s * nc] + sg * F[s];
 }
 
-// The Riemann dispatch of the record routines (Lib_Riemann.f90:120-140, `Riemann`): HLLC Batten for rs 1,
-// the MOSE_open solvers for rs 4..14 (the face sensor argument is 1 at these records)
+// The Riemann dispatch of the record routines (Lib_Riemann.f90:114-136, `Riemann`): HLLC Batten for rs 1, HLLE for
+// 2, SLAU for 3, the MOSE_open solvers for rs 4..14 (the face sensor argument is 1 at these records)
 void riemann_rec(const Ctx& c, double dl, double ul, double vl, double wl, double pl, double al, double dltot,
                  double dr, double ur, double vr, double wr, double pr, double ar, double drtot, double nx, double ny,
                  double nz, double& F_r, double& F_u, double& F_v, double& F_w, double& F_E) {
-  if (c.sc.riemann == 1)
-    riemann_hllc_bc(c.th, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r, F_u, F_v, F_w,
+  if (c.sc.riemann == 1 || c.sc.riemann == 2)
+    riemann_hllc_bc(c.th, c.sc.riemann, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r,
+                    F_u, F_v, F_w, F_E);
+  else if (c.sc.riemann == 3)
+    riemann_slau_bc(c.th, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r, F_u, F_v, F_w,
                     F_E);
   else
     riemann_open(c.th, c.sc.riemann, c.sc.mco, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz,
@@ -1381,7 +1522,9 @@ struct orc_ctx { Ctx c; };
 
 int orc_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, orc_ctx** out) {
   if (!mesh || !sc || !th || !out) return MB_E_ARG;
-  if (sc->riemann != 1 && sc->riemann != 4 && sc->riemann != 12) return MB_E_UNSUPPORTED;
+  if (sc->riemann != 1 && sc->riemann != 2 && sc->riemann != 3 && sc->riemann != 4 && sc->riemann != 8 &&
+      sc->riemann != 9 && sc->riemann != 12)
+    return MB_E_UNSUPPORTED;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
   if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
   orc_ctx* o = new orc_ctx();

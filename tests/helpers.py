@@ -71,6 +71,20 @@ def small_cases():
                                                           limiter=abi.LIM_MINMOD, n_rk=3)),
         ("mb2d_roe_mc_euler_rk4", lambda: cs.multiblock_2d(cols=2, rows=3, lo=5, hi=11, seed=5, riemann=abi.RS_LMROE,
                                                            limiter=abi.LIM_MC, visc=0)),
+        # the solvers of no benchmarked case (the run-time solver unit): interior faces, connections, walls, inlet
+        ("sod_hlle_minmod", lambda: cs.riemann_1d(n=64, riemann=abi.RS_HLLE)),
+        ("sod79_slau_mc_cfl09", lambda: cs.riemann_1d(n=64, riemann=abi.RS_SLAU, limiter=abi.LIM_MC, cfl=0.9)),
+        ("sod_llf_vanleer", lambda: cs.riemann_1d(n=64, riemann=abi.RS_LLF, limiter=abi.LIM_VANLEER)),
+        ("sod_slau2_superbee", lambda: cs.riemann_1d(n=64, riemann=abi.RS_SLAU2, limiter=abi.LIM_SUPERBEE)),
+        ("quad2d_hlle_vanalbada", lambda: cs.riemann_2d(n=20, riemann=abi.RS_HLLE, limiter=abi.LIM_VANALBADA)),
+        ("tgv_slau2_vanalbada_8blk", lambda: cs.taylor_green(n=12, blocks=2, riemann=abi.RS_SLAU2)),
+        ("tgv_llf_mc", lambda: cs.taylor_green(n=12, riemann=abi.RS_LLF, limiter=abi.LIM_MC)),
+        ("mb2d_slau_vanleer_rk3", lambda: cs.multiblock_2d(cols=2, rows=2, lo=5, hi=10, seed=3, riemann=abi.RS_SLAU,
+                                                           n_rk=3)),
+        ("mb2d_llf_minmod_rk4", lambda: cs.multiblock_2d(cols=2, rows=2, lo=5, hi=10, seed=9, riemann=abi.RS_LLF,
+                                                         limiter=abi.LIM_MINMOD)),
+        ("mb2d_hlle_mc_euler", lambda: cs.multiblock_2d(cols=2, rows=2, lo=5, hi=10, seed=4, riemann=abi.RS_HLLE,
+                                                        limiter=abi.LIM_MC, visc=0)),
         # blocks two cells and one cell high between walls: a wall's cubic ghosts read the opposite face's ghosts,
         # so the fill must follow the record order
         # (Euler slip walls: no-slip walls two cells apart diverge in the oracle itself)

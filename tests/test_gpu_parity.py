@@ -124,11 +124,13 @@ def test_sod_to_t_end(torch_cuda):
     assert np.abs(rho - r).mean() < 2e-3
 
 
-def test_mixed_precision_error(torch_cuda):
-    """The mixed form (FP32 flux arithmetic, FP64 state) against the FP64 form on a small TGV."""
+@pytest.mark.parametrize("riemann", [abi.RS_LMROE, abi.RS_HLLC, abi.RS_HLLE, abi.RS_SLAU, abi.RS_AUSMP, abi.RS_LLF,
+                                     abi.RS_SLAU2])
+def test_mixed_precision_error(torch_cuda, riemann):
+    """The mixed form (FP32 flux arithmetic, FP64 state) against the FP64 form on a small TGV, every solver."""
     from mosegpu import case as cs
     from mosegpu.engine import Engine
-    case = cs.taylor_green(n=24)
+    case = cs.taylor_green(n=24, riemann=riemann)
     a = Engine(case, precision=abi.PREC_FP64)
     b = Engine(case, precision=abi.PREC_MIXED)
     a.step(20, graph=True)
