@@ -63,11 +63,15 @@ extern "C" {
  * 1 = 1:1 / periodic connection (101, 201), 4 = inflow/outflow as bc.txt 405 sets it up (the supersonic
  * static-state inlet, pamb = PAMB_FORCE_SUPERSONIC, IO_BC_Open.f90:286-303: the supersonic closure
  * whatever the Mach, the face closed to a symmetry face on outward flow), 5 = adiabatic no-slip wall
- * (301 with q = 0), 11 = extrapolation (400) */
+ * (301 with q = 0), 11 = extrapolation (400), 3 = symmetry (300), 6 = no-slip wall at a prescribed temperature
+ * (302; q[0] = T_wall), 24 = back-pressure outlet (406; q[0] = exit pressure, q[1] = relaxation factor) */
 #define MB_BC_CONNECTION 1
+#define MB_BC_SYMMETRY 3
 #define MB_BC_INFLOW 4
 #define MB_BC_WALL 5
+#define MB_BC_WALL_T 6
 #define MB_BC_EXTRAPOLATION 11
+#define MB_BC_OUTLET 24
 #define MB_BC_NQ 6 /* parameters of a record (mb_bc.q) */
 
 /* limiter ids = lim_dev (numerics/space/Lib_Limiters.f90:21-61) */

@@ -174,10 +174,12 @@ static int check_mesh(const mb_mesh* mesh, int ngroups) {
   for (int q = 0; q < mesh->nrec; ++q) {
     const mb_bc& r = mesh->rec[q];
     if (r.type != MB_BC_CONNECTION && r.type != MB_BC_EXTRAPOLATION && r.type != MB_BC_WALL &&
-        r.type != MB_BC_INFLOW)
+        r.type != MB_BC_INFLOW && r.type != MB_BC_SYMMETRY && r.type != MB_BC_WALL_T && r.type != MB_BC_OUTLET)
       return MB_E_UNSUPPORTED;
     if (r.blk < 0 || r.blk >= mesh->nblk || r.face < 1 || r.face > 6) return MB_E_ARG;
     if (r.type == MB_BC_INFLOW && !(r.q[1] > 0.0 && r.q[2] > 0.0)) return MB_E_ARG;  // T0, p0
+    if (r.type == MB_BC_WALL_T && !(r.q[0] > 0.0)) return MB_E_ARG;                   // T_wall
+    if (r.type == MB_BC_OUTLET && !(r.q[0] >= 0.0 && r.q[1] >= 0.0 && r.q[1] <= 1.0)) return MB_E_ARG;
   }
   return MB_OK;
 }
@@ -194,6 +196,12 @@ static void free_tables(mb_ctx* c) {
   c->d_blk = nullptr; c->d_recmap = nullptr; c->d_rec = nullptr; c->d_grec = nullptr; c->d_phys = nullptr;
   c->d_cubic = nullptr; c->d_cdst = nullptr; c->d_csrc = nullptr; c->d_pgsrc = nullptr; c->d_pg = nullptr;
   c->d_tiles_sweep = nullptr; c->d_tiles_aux = nullptr;
+}
+
+// record types with physical ghosts (Fill_Ghost_Cell_blk, Lib_Extrapolation.f90:643-730)
+static bool phys_type(int t) {
+  return t == MB_BC_EXTRAPOLATION || t == MB_BC_INFLOW || t == MB_BC_WALL || t == MB_BC_SYMMETRY ||
+         t == MB_BC_WALL_T || t == MB_BC_OUTLET;
 }
 
 // builds the mesh-dependent device tables from the host description (Setup_BC_Device, Mod_BC.f90:99-338) and
@@ -253,14 +261,17 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
       const double v[8] = {r.q[0], r.q[1], r.q[2], r.q[5], cos(r.q[3]), sin(r.q[3]), cos(r.q[4]), sin(r.q[4])};
       for (int s = 0; s < 8; ++s) hr[q].q[s] = v[s];
     }
+    if (r.type == MB_BC_WALL_T) hr[q].q[0] = r.q[0];                                  // T_wall
+    if (r.type == MB_BC_OUTLET) { hr[q].q[0] = r.q[0]; hr[q].q[1] = r.q[1]; }        // exit pressure, relaxation
     hg[q] = GRec{r.blk, r.i, r.j, r.k, r.face, r.type};
-    if (r.type == MB_BC_EXTRAPOLATION || r.type == MB_BC_INFLOW || r.type == MB_BC_WALL) phys.push_back(q);
+    if (phys_type(r.type)) phys.push_back(q);
     if (r.type == MB_BC_EXTRAPOLATION) cubic.push_back(q);
   }
   // The fused stage fills only the ghost layers that some computation of the stage reads (entries carry their
   // layer count in bits 28-29; mb_fill_ghosts keeps the reference's full fill):
-  //  - along an axis of two or more cells, a type 11 / 4 / 5 face's second layer is read by nothing (interior
-  //    faces read one layer, these records read the boundary cell and its interior neighbour): one layer;
+  //  - along an axis of two or more cells, the second layer of a type 11 / 4 / 5 / 6 / 24 face is read by nothing
+  //    (interior faces read one layer, these records read the boundary cell and its neighbours): one layer (a
+  //    symmetry face fills its first layer only, in both fills);
   //  - along an axis one cell deep whose two faces are both type 11, an Euler stage reads no ghost there (no
   //    faces along it, no viscous stencil, extrapolation records read the cell): no layer;
   //  - otherwise both layers (the cubic ghost of a one-cell-deep axis reads the opposite face's layers).
@@ -280,7 +291,7 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
     }
     for (int q = 0; q < mesh->nrec; ++q) {
       const mb_bc& r = mesh->rec[q];
-      if (r.type != MB_BC_EXTRAPOLATION && r.type != MB_BC_INFLOW && r.type != MB_BC_WALL) continue;
+      if (!phys_type(r.type)) continue;
       if (hb[r.blk].kmirror && r.face >= 5) continue;  // the k ghosts of a mirrored block are never read
       const int ax = (r.face - 1) / 2;
       const int nax = mesh->blk[r.blk].n[ax];
@@ -413,15 +424,14 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
     for (int q = 0; q < mesh->nrec; ++q) {
       const mb_bc& r = mesh->rec[q];
       const int ax = (r.face - 1) / 2, nax = mesh->blk[r.blk].n[ax];
-      if (r.type != MB_BC_EXTRAPOLATION && r.type != MB_BC_WALL) continue;
+      if (r.type != MB_BC_EXTRAPOLATION && r.type != MB_BC_WALL && r.type != MB_BC_WALL_T) continue;
       if (nax == 2 || (nax == 1 && !ax11[3 * r.blk + ax])) ordered = 1;
     }
     if (ordered) {
       std::unordered_map<unsigned long long, int> seen_phys, seen_cubic;  // column -> face of its first record
       for (int q = 0; q < mesh->nrec; ++q) {
         const mb_bc& r = mesh->rec[q];
-        const bool ph = r.type == MB_BC_EXTRAPOLATION || r.type == MB_BC_INFLOW || r.type == MB_BC_WALL;
-        if (!ph) continue;
+        if (!phys_type(r.type)) continue;
         const int ax = (r.face - 1) / 2;
         const int t1 = ax == 0 ? r.j : r.i, t2 = ax == 2 ? r.j : r.k;
         const unsigned long long key = ((unsigned long long)(3 * (unsigned long long)r.blk + ax) << 40) |

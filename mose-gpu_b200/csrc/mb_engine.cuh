@@ -416,6 +416,148 @@ MB_HD void bc_wall_heat(const Params& p, const DBlk& b, const double* __restrict
   S[MB_IPR] = (R)0;
 }
 
+// Stress_Vector_Std (Mod_Fluid.f90:20-44) with mu_t = 0: the stress vector tau . n of the gradient G2 (Grad . M)
+template <typename R>
+MB_HD void stress_std(const R G2[3][3], R nx, R ny, R nz, R mil, R* S) {
+  const R ntt = (R)(-2.0 / 3.0);
+  R mi = mil + (R)0;
+  R lam = ntt * mi;
+  R Div = G2[0][0] + G2[1][1] + G2[2][2];
+  R lamDiv = lam * Div;
+  R txx = lamDiv + (R)2 * mi * G2[0][0], tyy = lamDiv + (R)2 * mi * G2[1][1], tzz = lamDiv + (R)2 * mi * G2[2][2];
+  R txy = mi * (G2[0][1] + G2[1][0]), txz = mi * (G2[0][2] + G2[2][0]), tyz = mi * (G2[1][2] + G2[2][1]);
+  S[0] = txx * nx + txy * ny + txz * nz;
+  S[1] = txy * nx + tyy * ny + tyz * nz;
+  S[2] = txz * nx + tyz * ny + tzz * nz;
+}
+
+// BC_Symmetry_Visc (Lib_BC.f90:741-861), laminar: the boundary cell and its four transverse neighbours mirrored about
+// the face give the normal and transverse velocity gradients; the stress of Grad . M (momentum rows) and its work on
+// the face-mean velocity (energy row), subtracted.
+template <typename R>
+MB_HD void bc_sym_visc(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km, int Fm,
+                       R* S) {
+  const long long nc = p.nc;
+  const int modfm = Fm % 2, modfm2 = 1 - 2 * modfm;
+  const long long rb = row(b, Im, Jm, Km), l = rb - b.boff;
+  R Pb[MB_NP];
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) Pb[s] = cvt<R>(ld(P + rb + s * nc));
+  R M[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) M[a][q] = cvt<R>(ld(b.m + a + 3 * q + 9 * l));
+  R rho, Rgas;
+  rotot_rtot(p, Pb[0], rho, Rgas);
+  R T = Pb[MB_IPR] / (rho * Rgas);
+  int ti = tidx(p, T);
+  R Tdiff = T - (R)ti;
+  R mil, kl;
+  wilke(p, Pb[0], rho, ti, Tdiff, mil, kl);
+  // transverse strides: b then c axis of the face (Fm 1-2: j, k; 3-4: i, k; 5-6: i, j); a = the face axis
+  const long long sj = b.pi, sk = (long long)b.pi * b.pj;
+  const long long sb = (Fm <= 2) ? sj : 1, sc = (Fm <= 4) ? sk : sj;
+  const int a = (Fm - 1) >> 1, bb = (Fm <= 2) ? 1 : 0, cc = (Fm <= 4) ? 2 : 1;
+  R V1[3] = {Pb[MB_IU], Pb[MB_IV], Pb[MB_IW]}, V3[3], V4[3], V7[3], V8[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    V3[q] = cvt<R>(ld(P + rb - sb + (MB_IU + q) * nc));
+    V4[q] = cvt<R>(ld(P + rb + sb + (MB_IU + q) * nc));
+    V7[q] = cvt<R>(ld(P + rb - sc + (MB_IU + q) * nc));
+    V8[q] = cvt<R>(ld(P + rb + sc + (MB_IU + q) * nc));
+  }
+  double g[4];
+  bc_face_geom(b, Im, Jm, Km, Fm, g);
+  const R nrm[3] = {cvt<R>(g[0]), cvt<R>(g[1]), cvt<R>(g[2])};
+  const R area = cvt<R>(g[3]);
+  R d1 = V1[0] * nrm[0] + V1[1] * nrm[1] + V1[2] * nrm[2];
+  R d3 = V3[0] * nrm[0] + V3[1] * nrm[1] + V3[2] * nrm[2];
+  R d4 = V4[0] * nrm[0] + V4[1] * nrm[1] + V4[2] * nrm[2];
+  R d7 = V7[0] * nrm[0] + V7[1] * nrm[1] + V7[2] * nrm[2];
+  R d8 = V8[0] * nrm[0] + V8[1] * nrm[1] + V8[2] * nrm[2];
+  R V2[3], Grad[3][3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    V2[q] = V1[q] - (R)2 * d1 * nrm[q];
+    R V5 = V3[q] - (R)2 * d3 * nrm[q], V6 = V4[q] - (R)2 * d4 * nrm[q];
+    R V9 = V7[q] - (R)2 * d7 * nrm[q], V10 = V8[q] - (R)2 * d8 * nrm[q];
+    R ga = (V2[q] - V1[q]) * (R)modfm2;
+    R gb = (V4[q] - V3[q] + V6 - V5) * (R)0.25;
+    R gc = (V8[q] - V7[q] + V10 - V9) * (R)0.25;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) Grad[q][d] = (d == a) ? ga : ((d == bb) ? gb : gc);
+    (void)cc;
+  }
+  R G2[3][3];
+#pragma unroll
+  for (int kk = 0; kk < 3; ++kk)
+#pragma unroll
+    for (int ii = 0; ii < 3; ++ii) G2[ii][kk] = Grad[ii][0] * M[0][kk] + Grad[ii][1] * M[1][kk] + Grad[ii][2] * M[2][kk];
+  R St[3];
+  stress_std(G2, nrm[0], nrm[1], nrm[2], mil, St);
+  R Vf[3] = {(R)0.5 * (V1[0] + V2[0]), (R)0.5 * (V1[1] + V2[1]), (R)0.5 * (V1[2] + V2[2])};
+  S[0] = (R)0;
+  S[MB_IU] = (R)modfm2 * area * St[0];
+  S[MB_IV] = (R)modfm2 * area * St[1];
+  S[MB_IW] = (R)modfm2 * area * St[2];
+  S[MB_IPR] = (R)modfm2 * area * (Vf[0] * St[0] + Vf[1] * St[1] + Vf[2] * St[2]);
+}
+
+// BC_Wall_Temperature_dev (Lib_BC.f90:997-1115), laminar no-slip wall at T_wall: mu and k of the wall state
+// (p of the cell at T_wall; k = mu cp / Pr when Pr > 0), the wall-normal velocity and temperature gradients of the
+// boundary cell: stress (momentum rows) and conducted heat (energy row), subtracted.
+template <typename R>
+MB_HD void bc_wall_temp(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km, int Fm,
+                        double Tw_, R* S) {
+  const long long nc = p.nc;
+  int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm2 = 1 - 2 * modfm, modfm3 = 2 * (2 * modfm - 1);
+  const long long rb = row(b, Im, Jm, Km), l = rb - b.boff;
+  const R Tw = cvt<R>(Tw_);
+  R Pb[MB_NP];
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) Pb[s] = cvt<R>(ld(P + rb + s * nc));
+  R M[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) M[a][q] = cvt<R>(ld(b.m + a + 3 * q + 9 * l));
+  R rho, Rgas;
+  rotot_rtot(p, Pb[0], rho, Rgas);
+  R T = Pb[MB_IPR] / (rho * Rgas);
+  R rho_wall = Pb[MB_IPR] / (Rgas * Tw);
+  R Pw0 = Pb[0] * rho_wall / rho;
+  int ti = tidx(p, Tw);
+  R Tdiff = Tw - (R)ti;
+  R mil, kl;
+  wilke(p, Pw0, rho_wall, ti, Tdiff, mil, kl);
+  if (p.prandtl > 0.0) kl = mil * f_cp(p, Pw0, ti, Tdiff, rho_wall) / (R)p.prandtl;
+  R G2[3][3];
+#pragma unroll
+  for (int kk = 0; kk < 3; ++kk)
+#pragma unroll
+    for (int ii = 0; ii < 3; ++ii) {
+      R g1 = (dir == 1) ? Pb[MB_IU + ii] * (R)modfm3 : (R)0, g2 = (dir == 2) ? Pb[MB_IU + ii] * (R)modfm3 : (R)0,
+        g3 = (dir == 3) ? Pb[MB_IU + ii] * (R)modfm3 : (R)0;
+      G2[ii][kk] = g1 * M[0][kk] + g2 * M[1][kk] + g3 * M[2][kk];
+    }
+  double g[4];
+  bc_face_geom(b, Im, Jm, Km, Fm, g);
+  R nx = cvt<R>(g[0]), ny = cvt<R>(g[1]), nz = cvt<R>(g[2]), area = cvt<R>(g[3]);
+  R St[3];
+  stress_std(G2, nx, ny, nz, mil, St);
+  R Gnp_dir = (T - Tw) * (R)modfm3;
+  R Gnp[3];
+#pragma unroll
+  for (int kk = 0; kk < 3; ++kk) Gnp[kk] = Gnp_dir * M[dir - 1][kk];
+  R Flux_np = area * kl * (Gnp[0] * nx + Gnp[1] * ny + Gnp[2] * nz);
+  S[0] = (R)0;
+  S[MB_IU] = (R)modfm2 * area * St[0];
+  S[MB_IV] = (R)modfm2 * area * St[1];
+  S[MB_IW] = (R)modfm2 * area * St[2];
+  S[MB_IPR] = (R)modfm2 * Flux_np;
+}
+
 // BC_Inflow_Outflow (Lib_BC.f90:1519-1597) of a 405 record: inward flow -> BC_Supersonic_Inflow (Lib_BC.f90:
 // 1247-1330), outward flow -> the face closes (BC_Symmetry_Eul).
 template <typename R, int RS = 0, int LIM = 0>
@@ -486,6 +628,84 @@ MB_HD void bc_inflow(const Params& p, const DBlk& b, const double* __restrict__ 
   for (int s = 0; s < MB_NP; ++s) A[s] = (R)modfm2 * Fl[s];
 }
 
+template <typename R> MB_HD R pw_(R x, R y);
+template <> MB_HD double pw_(double x, double y) { return pow(x, y); }
+template <> MB_HD float pw_(float x, float y) { return powf(x, y); }
+
+// BC_Outlet (Lib_BC.f90:1604-1658) of a 406 record (q = exit pressure, relaxation factor): inward flow closes the face
+// (BC_Symmetry_Eul); otherwise the face state of BC_Outflow (Lib_BC.f90:1166-1240) from the Riemann invariant towards
+// the face and the relaxed exit pressure (isentropic when the normal Mach number is below 1 and p_exit > 0).
+template <typename R, int RS = 0, int LIM = 0>
+MB_HD void bc_outlet(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km, int Fm,
+                     const double* __restrict__ q, R* A) {
+  const long long nc = p.nc;
+  const int modfm = Fm % 2, modfm2 = 1 - 2 * modfm;
+  const long long rb = row(b, Im, Jm, Km);
+  R Bp[MB_NP];
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) Bp[s] = cvt<R>(ld(P + rb + s * nc));
+  double g[4];
+  bc_face_geom(b, Im, Jm, Km, Fm, g);
+  const R nrm[3] = {cvt<R>(g[0]), cvt<R>(g[1]), cvt<R>(g[2])};
+  const R area = cvt<R>(g[3]);
+  const R pExit = cvt<R>(ld(q + 0)), rel = cvt<R>(ld(q + 1));
+  const R BC_Sign = (R)modfm2;
+  R Un = Bp[MB_IU] * nrm[0] + Bp[MB_IV] * nrm[1] + Bp[MB_IW] * nrm[2];
+  if (BC_Sign * Un < (R)0) {
+    bc_sym_eul<R, RS, LIM>(p, b, P, Im, Jm, Km, Fm, A);
+    return;
+  }
+  R Brho, BRgas;
+  rotot_rtot(p, Bp[0], Brho, BRgas);
+  R BSound = f_ss(p, Bp[0], Bp[MB_IPR], Brho, BRgas);
+  R T = Bp[MB_IPR] / (Brho * BRgas);
+  int ti = tidx(p, T);
+  R Tdiff = T - (R)ti;
+  R cp = f_cp(p, Bp[0], ti, Tdiff, Brho);
+  R BGamma = cp / (cp - BRgas);
+  R Riem = BSound + BC_Sign * (R)0.5 * (BGamma - (R)1) * Un;
+  R p_Amb = rel * pExit + ((R)1 - rel) * Bp[MB_IPR];
+  R VT[3] = {Bp[MB_IU] - Un * nrm[0], Bp[MB_IV] - Un * nrm[1], Bp[MB_IW] - Un * nrm[2]};
+  R Mach_N = fabs(Un / BSound);
+  R pe = p_Amb;
+  R Fp[MB_NP], Fun, Frho, FRgas;
+  if (Mach_N < (R)1 && p_Amb > (R)0) {
+    R delta = (R)0.5 * (BGamma - (R)1);
+    R denom = (R)1 / pw_((R)1 + delta, BGamma / (BGamma - (R)1));
+    R pstar = Bp[MB_IPR] * denom * pw_((R)1 + delta * (Mach_N * Mach_N), BGamma / (BGamma - (R)1));
+    if (pstar >= p_Amb) pe = pstar;
+    R Isentropic = (BGamma - (R)1) / ((R)2 * BGamma);
+    R FSound = BSound * pw_(pe / Bp[MB_IPR], Isentropic);
+    Fun = (Riem - FSound) / (BC_Sign * (R)0.5 * (BGamma - (R)1));
+    Fp[MB_IPR] = pe;
+    Frho = BGamma * Fp[MB_IPR] / (FSound * FSound);
+    Fp[0] = Bp[0] / Brho * Frho;
+    Fp[MB_IU] = VT[0] + Fun * nrm[0];
+    Fp[MB_IV] = VT[1] + Fun * nrm[1];
+    Fp[MB_IW] = VT[2] + Fun * nrm[2];
+    FRgas = BRgas;
+  } else {
+#pragma unroll
+    for (int s = 0; s < MB_NP; ++s) Fp[s] = Bp[s];
+    Fun = Un; Frho = Brho; FRgas = BRgas;
+  }
+  R FT = Fp[MB_IPR] / (FRgas * Frho);
+  int Ti = tidx(p, FT);
+  R Td = FT - (R)Ti;
+  const R* H = Tab<R>::h(p);
+  R FEnth = (R)0 + Fp[0] / Frho * (H[Ti] + (H[Ti + 1] - H[Ti]) * Td);
+  R Fl[MB_NP];
+  Fl[0] = Fp[0] * area * Fun;
+  R Fmass = Frho * area * Fun;
+  Fl[MB_IU] = Fp[MB_IU] * Fmass + Fp[MB_IPR] * area * nrm[0];
+  Fl[MB_IV] = Fp[MB_IV] * Fmass + Fp[MB_IPR] * area * nrm[1];
+  Fl[MB_IW] = Fp[MB_IW] * Fmass + Fp[MB_IPR] * area * nrm[2];
+  R vt2 = Fp[MB_IU] * Fp[MB_IU] + Fp[MB_IV] * Fp[MB_IV] + Fp[MB_IW] * Fp[MB_IW];
+  Fl[MB_IPR] = Fmass * ((R)0.5 * vt2 + FEnth);
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) A[s] = (R)modfm2 * Fl[s];
+}
+
 // The record (type, id) of the cell (i,j,k) on face F, -1 if none.
 MB_HD int record_of(const Params& p, const DBlk& b, int F, int i, int j, int k) {
   if (b.rmap[F - 1] < 0) return -1;
@@ -513,6 +733,14 @@ MB_HD void bc_record(const Params& p, const DBlk& b, const double* __restrict__ 
     if (VISC) bc_wall_heat<R>(p, b, P, i, j, k, F, S);
   } else if (rc.type == 4) {
     bc_inflow<R, RS, LIM>(p, b, P, i, j, k, F, rc.q, A);
+  } else if (rc.type == 3) {
+    bc_sym_eul<R, RS, LIM>(p, b, P, i, j, k, F, A);
+    if (VISC) bc_sym_visc<R>(p, b, P, i, j, k, F, S);
+  } else if (rc.type == 6) {
+    bc_sym_eul<R, RS, LIM>(p, b, P, i, j, k, F, A);
+    if (VISC) bc_wall_temp<R>(p, b, P, i, j, k, F, rc.q[0], S);
+  } else if (rc.type == 24) {
+    bc_outlet<R, RS, LIM>(p, b, P, i, j, k, F, rc.q, A);
   } else {
     for (int s = 0; s < MB_NP; ++s) A[s] = (R)-0.0;
   }

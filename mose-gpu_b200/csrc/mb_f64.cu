@@ -6,8 +6,9 @@
 namespace mb {
 
 // ---- ghost fill (numerics/fluxes/bc/Lib_Extrapolation.f90) ----
-// Fill_Ghost_Cell_blk (:643-730): zero-gradient ghosts of types 4 / 11 (Ghost_ZG_Extrapolate :590-614),
-// the second-order extrapolation 3 x3 - 3 x2 + x1 of walls (Ghost_Extrapolate :616-641)
+// Fill_Ghost_Cell_blk (:643-730): the mirrored first layer of symmetry faces (type 3, Ghost_Symmetry :558-587),
+// zero-gradient ghosts of types 4 / 11 / 24 (Ghost_ZG_Extrapolate :590-614), the second-order extrapolation
+// 3 x3 - 3 x2 + x1 of the walls 5 / 6 (Ghost_Extrapolate :616-641)
 __global__ void k_ghost_phys(Params p, const GRec* __restrict__ rec, const int* __restrict__ list, int n, double* P) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
@@ -19,7 +20,17 @@ __global__ void k_ghost_phys(Params p, const GRec* __restrict__ rec, const int* 
   const long long st = (dir == 1) ? 1 : (dir == 2 ? (long long)b.pi : (long long)b.pi * b.pj);
   const long long src = row(b, r.i, r.j, r.k);
   const long long nc = p.nc;
-  if (r.type == 5) {
+  if (r.type == 3) {  // Ghost_Symmetry (Lib_Extrapolation.f90:558-587): the first layer, normal velocity reversed
+    double g[4];
+    bc_face_geom(b, r.i, r.j, r.k, r.face, g);
+    const long long dst = src - (long long)gstep * st;
+    double vel[3] = {P[src + MB_IU * nc], P[src + MB_IV * nc], P[src + MB_IW * nc]};
+    const double udotn = vel[0] * g[0] + vel[1] * g[1] + vel[2] * g[2];
+    for (int a = 0; a < 3; ++a) vel[a] = vel[a] - 2.0 * udotn * g[a];
+    P[dst] = P[src];
+    P[dst + MB_IU * nc] = vel[0]; P[dst + MB_IV * nc] = vel[1]; P[dst + MB_IW * nc] = vel[2];
+    P[dst + MB_IPR * nc] = P[src + MB_IPR * nc];
+  } else if (r.type == 5 || r.type == 6) {
     const int step = -gstep;
     for (int g = 1; g <= nl; ++g) {
       long long d0 = src + (long long)(g * step) * st, a1 = src + (long long)((g - 1) * step) * st,

@@ -35,6 +35,9 @@ BC_CONNECTION = 1
 BC_INFLOW = 4
 BC_WALL = 5
 BC_EXTRAPOLATION = 11
+BC_SYMMETRY = 3
+BC_WALL_T = 6       # q = (T_wall,)
+BC_OUTLET = 24      # q = (exit pressure, relaxation factor)
 
 LIM_MINMOD, LIM_VANLEER, LIM_VANALBADA, LIM_MC, LIM_SUPERBEE, LIM_FIRST = 1, 2, 3, 4, 5, 6
 RS_HLLC, RS_HLLE, RS_SLAU, RS_AUSMP, RS_LLF, RS_SLAU2, RS_LMROE = 1, 2, 3, 4, 8, 9, 12

@@ -290,7 +290,8 @@ def layout_case(name, cuts, node_fn, periodic, bc_faces, thermo, scheme, prim_fn
                 spec = bc_faces[face]
                 if isinstance(spec, tuple):
                     r["type"] = spec[0]
-                    r["q"][:] = np.asarray(spec[1], dtype=np.float64)
+                    qv = np.asarray(spec[1], dtype=np.float64)
+                    r["q"][:, :qv.size] = qv
                 else:
                     r["type"] = spec
             recs.append(r)
@@ -415,6 +416,53 @@ def multiblock_2d(cols=8, rows=6, lo=64, hi=512, seed=20261203, mach=2.0, T=300.
                        scheme, prim)
     case.steps = steps
     case.meta = dict(widths=[int(w) for w in widths], heights=[int(h) for h in heights], rho=rho, V=V, mu=mu)
+    return case
+
+
+def duct_3d(widths=(6, 5), heights=(5,), depths=(3, 4), mach=0.5, T=300.0, p=1.0e5, re=2.0e3, amp=0.05,
+            cfl=0.5, n_rk=3, riemann=abi.RS_HLLC, limiter=abi.LIM_VANLEER, prandtl=0.71, visc=1, bc=None,
+            velocity=None, steps=20):
+    """3-D laminar duct: blocks of the given column widths (i), row heights (j) and slab depths (k) in cells, 1:1
+    interfaces, on (xi, eta, zeta) in [0, 1] x [0, 1] x [0, 0.5] mapped by x = xi + amp sin(2 pi eta),
+    y = eta + amp sin(2 pi xi), z = zeta + amp sin(2 pi xi) sin(2 pi eta) (curvilinear in all three directions).
+    Uniform flow along +x at the given Mach number; by default the 405 static inlet at i = 1, the 406 outlet at
+    i = max (exit pressure 0.95 p, relaxation 0.5), isothermal no-slip walls (302) at 320 K and 290 K on the j faces,
+    symmetry (300) on the k faces. bc overrides {global face: type or (type, q)}."""
+    cx = [0] + list(np.cumsum(widths).astype(int))
+    cy = [0] + list(np.cumsum(heights).astype(int))
+    cz = [0] + list(np.cumsum(depths).astype(int))
+    NI, NJ, NK = cx[-1], cy[-1], cz[-1]
+    th = ideal_gas_tables(prandtl=prandtl)
+    R, gam = th["R"], th["gamma"]
+    rho = p / (R * T)
+    V = mach * math.sqrt(gam * R * T)
+    mu = rho * V * 1.0 / re
+    th = ideal_gas_tables(mu=mu, prandtl=prandtl)
+
+    def nodes(iu, iv, iw):
+        xi, eta, zeta = iu / NI, iv / NJ, 0.5 * iw / NK
+        x = xi + amp * np.sin(2.0 * np.pi * eta)
+        y = eta + amp * np.sin(2.0 * np.pi * xi)
+        z = zeta + amp * np.sin(2.0 * np.pi * xi) * np.sin(2.0 * np.pi * eta)
+        return np.stack([x, y, z], axis=-1)
+
+    u0 = V if velocity is None else velocity
+
+    def prim(c):
+        shp = c.shape[:-1]
+        return np.stack([np.full(shp, rho), np.full(shp, u0), np.zeros(shp), np.zeros(shp), np.full(shp, p)])
+
+    inflow = (abi.BC_INFLOW, (mach, T, p, 0.0, 0.0, 1.0))
+    faces = {1: inflow, 2: (abi.BC_OUTLET, (0.95 * p, 0.5)), 3: (abi.BC_WALL_T, (320.0,)),
+             4: (abi.BC_WALL_T, (290.0,)), 5: abi.BC_SYMMETRY, 6: abi.BC_SYMMETRY}
+    if bc is not None:
+        faces.update({f: (inflow if t == abi.BC_INFLOW else t) for f, t in bc.items()})
+    scheme = dict(limiter=limiter, riemann=riemann, visc=visc, n_rk=n_rk, ndir=3, cfl=cfl, vnn=0.3,
+                  prandtl=prandtl, schmidt=0.7, mco=1.0, dt_additive=0)
+    case = layout_case("duct3d_%dx%dx%d" % (len(widths), len(heights), len(depths)), [cx, cy, cz], nodes,
+                       (False, False, False), faces, th, scheme, prim)
+    case.steps = steps
+    case.meta = dict(rho=rho, V=V, mu=mu)
     return case
 
 

@@ -25,8 +25,10 @@
 //                           Lib_BC.f90:1770-1867 (connection, Euler), 2113-2178 (connection, viscous),
 //                           1119-1165 (extrapolation), 640-737 (symmetry, Euler part of the adiabatic wall),
 //                           879-982 (adiabatic wall, viscous), 1519-1597 + 1247-1330 (405 supersonic inlet),
+//                           741-861 (symmetry, viscous), 997-1115 (isothermal wall), 1604-1658 + 1166-1240
+//                           (406 outlet),
 //                           physics/turbulence/Mod_Fluid.f90:20-44 (wall stress)
-//   ghost fill              bc/Lib_Extrapolation.f90:590-641 (ZG, cubic), 643-730, 859-879, 1023-1191
+//   ghost fill              bc/Lib_Extrapolation.f90:558-641 (symmetry, ZG, cubic), 643-730, 859-879, 1023-1191
 //   thermo cache            src/lib/physics/Mod_Thermo_Cache.f90:291-425
 //   state update            src/lib/gpu/newstate_cons_body.inc:1-89, explicit/Lib_Newstate.f90:257-307
 //   RK coefficients         explicit/Lib_RK.f90:6-9; classical RK4 with a conserved accumulator (no reference)
@@ -1073,6 +1075,127 @@ void bc_wall_heat(const Ctx& c, const Blk& b, const double* P, double* R, int Im
   R[rb + IW * nc] = R[rb + IW * nc] - (double)modfm2 * area * S3;
 }
 
+// Stress_Vector_Std (Mod_Fluid.f90:20-44) with mu_t = 0: the stress vector tau . n of the gradient G2 (Grad . M)
+void stress_std(const double G2[3][3], const double* nrm, double mil, double* S) {
+  const double ntt = -2.0 / 3.0;
+  double mi = mil + 0.0;
+  double lam = ntt * mi;
+  double Div = G2[0][0] + G2[1][1] + G2[2][2];
+  double lamDiv = lam * Div;
+  double txx = lamDiv + 2.0 * mi * G2[0][0], tyy = lamDiv + 2.0 * mi * G2[1][1], tzz = lamDiv + 2.0 * mi * G2[2][2];
+  double txy = mi * (G2[0][1] + G2[1][0]), txz = mi * (G2[0][2] + G2[2][0]), tyz = mi * (G2[1][2] + G2[2][1]);
+  S[0] = txx * nrm[0] + txy * nrm[1] + txz * nrm[2];
+  S[1] = txy * nrm[0] + tyy * nrm[1] + tyz * nrm[2];
+  S[2] = txz * nrm[0] + tyz * nrm[1] + tzz * nrm[2];
+}
+
+// BC_Symmetry_Visc (Lib_BC.f90:741-861), laminar: the boundary cell and its four transverse neighbours mirrored
+// about the face give the normal and the two transverse velocity gradients; the stress of Grad . M and its work on
+// the face-mean velocity leave the momentum and energy rows.
+void bc_symmetry_visc(const Ctx& c, const Blk& b, const double* P, double* R, int Im, int Jm, int Km, int Fm) {
+  const int64_t nc = c.ncell;
+  int modfm = Fm % 2, modfm2 = 1 - 2 * modfm;
+  int64_t rb = row(b, Im, Jm, Km);
+  double Pb[NP];
+  for (int s = 0; s < NP; ++s) Pb[s] = P[rb + s * nc];
+  double M[3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int q = 0; q < 3; ++q) M[a][q] = mv(b, a, q, Im, Jm, Km);
+  double rho, Rgas;
+  rotot_rtot(c.th, Pb[0], rho, Rgas);
+  double T = Pb[IP] / (rho * Rgas);
+  int ti = tidx(c.th, T);
+  double Tdiff = T - ti;
+  double mil, kl;
+  wilke(c.th, Pb[0], rho, ti, Tdiff, mil, kl);
+  int o3[3] = {0, 0, 0}, o4[3] = {0, 0, 0}, o7[3] = {0, 0, 0}, o8[3] = {0, 0, 0};
+  int a, bb, cc;
+  if (Fm <= 2) { o3[1] = -1; o4[1] = 1; o7[2] = -1; o8[2] = 1; a = 0; bb = 1; cc = 2; }
+  else if (Fm <= 4) { o3[0] = -1; o4[0] = 1; o7[2] = -1; o8[2] = 1; a = 1; bb = 0; cc = 2; }
+  else { o3[0] = -1; o4[0] = 1; o7[1] = -1; o8[1] = 1; a = 2; bb = 0; cc = 1; }
+  auto vel = [&](const int* o, double* v) {
+    int64_t r = row(b, Im + o[0], Jm + o[1], Km + o[2]);
+    v[0] = P[r + IU * nc]; v[1] = P[r + IV * nc]; v[2] = P[r + IW * nc];
+  };
+  double V1[3] = {Pb[IU], Pb[IV], Pb[IW]}, V3[3], V4[3], V7[3], V8[3];
+  vel(o3, V3); vel(o4, V4); vel(o7, V7); vel(o8, V8);
+  double nrm[3], area;
+  bc_face_geom(b, Im, Jm, Km, Fm, nrm, area);
+  double d1 = V1[0] * nrm[0] + V1[1] * nrm[1] + V1[2] * nrm[2];
+  double d3 = V3[0] * nrm[0] + V3[1] * nrm[1] + V3[2] * nrm[2];
+  double d4 = V4[0] * nrm[0] + V4[1] * nrm[1] + V4[2] * nrm[2];
+  double d7 = V7[0] * nrm[0] + V7[1] * nrm[1] + V7[2] * nrm[2];
+  double d8 = V8[0] * nrm[0] + V8[1] * nrm[1] + V8[2] * nrm[2];
+  double V2[3], V5[3], V6[3], V9[3], V10[3];
+  for (int s = 0; s < 3; ++s) {
+    V2[s] = V1[s] - 2.0 * d1 * nrm[s];
+    V5[s] = V3[s] - 2.0 * d3 * nrm[s];
+    V6[s] = V4[s] - 2.0 * d4 * nrm[s];
+    V9[s] = V7[s] - 2.0 * d7 * nrm[s];
+    V10[s] = V8[s] - 2.0 * d8 * nrm[s];
+  }
+  double Grad[3][3];
+  for (int s = 0; s < 3; ++s) {
+    Grad[s][a] = (V2[s] - V1[s]) * (double)modfm2;
+    Grad[s][bb] = (V4[s] - V3[s] + V6[s] - V5[s]) * 0.25;
+    Grad[s][cc] = (V8[s] - V7[s] + V10[s] - V9[s]) * 0.25;
+  }
+  double G2[3][3];
+  for (int kk = 0; kk < 3; ++kk)
+    for (int ii = 0; ii < 3; ++ii)
+      G2[ii][kk] = Grad[ii][0] * M[0][kk] + Grad[ii][1] * M[1][kk] + Grad[ii][2] * M[2][kk];
+  double S[3];
+  stress_std(G2, nrm, mil, S);
+  double Vf[3] = {0.5 * (V1[0] + V2[0]), 0.5 * (V1[1] + V2[1]), 0.5 * (V1[2] + V2[2])};
+  R[rb + IU * nc] = R[rb + IU * nc] - (double)modfm2 * area * S[0];
+  R[rb + IV * nc] = R[rb + IV * nc] - (double)modfm2 * area * S[1];
+  R[rb + IW * nc] = R[rb + IW * nc] - (double)modfm2 * area * S[2];
+  R[rb + IP * nc] = R[rb + IP * nc] - (double)modfm2 * area * (Vf[0] * S[0] + Vf[1] * S[1] + Vf[2] * S[2]);
+}
+
+// BC_Wall_Temperature_dev (Lib_BC.f90:997-1115), laminar no-slip wall at T_wall: the wall state p(wall) = p(cell)
+// at T_wall gives mu and k (k = mu cp / Pr when Pr > 0), the wall-normal velocity and temperature gradients of the
+// boundary cell give the stress (momentum rows) and the conducted heat (energy row).
+void bc_wall_temperature(const Ctx& c, const Blk& b, const double* P, double* R, int Im, int Jm, int Km, int Fm,
+                         double Tw) {
+  const int64_t nc = c.ncell;
+  int dir = (Fm + 1) / 2, modfm = Fm % 2, modfm2 = 1 - 2 * modfm, modfm3 = 2 * (2 * modfm - 1);
+  int64_t rb = row(b, Im, Jm, Km);
+  double Pb[NP];
+  for (int s = 0; s < NP; ++s) Pb[s] = P[rb + s * nc];
+  double M[3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int q = 0; q < 3; ++q) M[a][q] = mv(b, a, q, Im, Jm, Km);
+  double rho, Rgas;
+  rotot_rtot(c.th, Pb[0], rho, Rgas);
+  double T = Pb[IP] / (rho * Rgas);
+  double rho_wall = Pb[IP] / (Rgas * Tw);
+  double Pw0 = Pb[0] * rho_wall / rho;
+  int ti = tidx(c.th, Tw);
+  double Tdiff = Tw - ti;
+  double mil, kl;
+  wilke(c.th, Pw0, rho_wall, ti, Tdiff, mil, kl);
+  if (c.sc.prandtl > 0.0) kl = mil * f_cp(c.th, Pw0, ti, Tdiff, rho_wall) / c.sc.prandtl;
+  double Grad[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (int a = 0; a < 3; ++a) Grad[a][dir - 1] = Pb[IU + a] * (double)modfm3;
+  double G2[3][3];
+  for (int kk = 0; kk < 3; ++kk)
+    for (int ii = 0; ii < 3; ++ii)
+      G2[ii][kk] = Grad[ii][0] * M[0][kk] + Grad[ii][1] * M[1][kk] + Grad[ii][2] * M[2][kk];
+  double nrm[3], area;
+  bc_face_geom(b, Im, Jm, Km, Fm, nrm, area);
+  double S[3];
+  stress_std(G2, nrm, mil, S);
+  double Gnp_dir = (T - Tw) * (double)modfm3;
+  double Gnp[3];
+  for (int kk = 0; kk < 3; ++kk) Gnp[kk] = Gnp_dir * M[dir - 1][kk];
+  double Flux_np = area * kl * (Gnp[0] * nrm[0] + Gnp[1] * nrm[1] + Gnp[2] * nrm[2]);
+  R[rb + IU * nc] = R[rb + IU * nc] - (double)modfm2 * area * S[0];
+  R[rb + IV * nc] = R[rb + IV * nc] - (double)modfm2 * area * S[1];
+  R[rb + IW * nc] = R[rb + IW * nc] - (double)modfm2 * area * S[2];
+  R[rb + IP * nc] = R[rb + IP * nc] - (double)modfm2 * Flux_np;
+}
+
 // BC_Inflow_Outflow (Lib_BC.f90:1519-1597) for a 405 record (pamb = PAMB_FORCE_SUPERSONIC): inward flow ->
 // BC_Supersonic_Inflow (Lib_BC.f90:1247-1330), outward flow -> the face closes (BC_Symmetry_Eul).
 // q = mach, T0, p0, alpha, beta, rel_fac; the angles enter through cos / sin taken on the host.
@@ -1141,24 +1264,111 @@ void bc_inflow_405(const Ctx& c, const Blk& b, const double* P, double* R, int I
   for (int s = 0; s < NP; ++s) R[rb + s * nc] = R[rb + s * nc] + (double)modfm2 * Fl[s];
 }
 
+// BC_Outlet (Lib_BC.f90:1604-1658) of a 406 record, q = exit pressure, relaxation factor: inward flow closes the
+// face (BC_Symmetry_Eul); otherwise the Riemann invariant towards the face and the relaxed exit pressure give the
+// face state of BC_Outflow (Lib_BC.f90:1166-1240): isentropic to p_exit when the normal Mach number is below 1 and
+// p_exit > 0, the boundary cell itself otherwise.
+void bc_outlet(const Ctx& c, const Blk& b, const double* P, double* R, int Im, int Jm, int Km, int Fm,
+               const double* q) {
+  const int64_t nc = c.ncell;
+  const Thermo& th = c.th;
+  int modfm = Fm % 2, modfm2 = 1 - 2 * modfm;
+  int64_t rb = row(b, Im, Jm, Km);
+  double Bp[NP];
+  for (int s = 0; s < NP; ++s) Bp[s] = P[rb + s * nc];
+  double nrm[3], area;
+  bc_face_geom(b, Im, Jm, Km, Fm, nrm, area);
+  const double BC_pExit = q[0], BC_rel_fac = q[1];
+  double BC_Sign = (double)modfm2;
+  double Un = Bp[IU] * nrm[0] + Bp[IV] * nrm[1] + Bp[IW] * nrm[2];
+  if (BC_Sign * Un < 0.0) {
+    bc_symmetry_eul(c, b, P, R, Im, Jm, Km, Fm);
+    return;
+  }
+  double Brho, BRgas;
+  rotot_rtot(th, Bp[0], Brho, BRgas);
+  double BSound = f_ss(th, Bp[0], Bp[IP], Brho, BRgas);
+  double T = Bp[IP] / (Brho * BRgas);
+  int ti = tidx(th, T);
+  double Tdiff = T - ti;
+  double cp = f_cp(th, Bp[0], ti, Tdiff, Brho);
+  double BGamma = cp / (cp - BRgas);
+  double Riem = BSound + BC_Sign * 0.5 * (BGamma - 1.0) * Un;
+  double p_exit = BC_rel_fac * BC_pExit + (1.0 - BC_rel_fac) * Bp[IP];
+  // BC_Outflow
+  const double p_Amb = p_exit;
+  double vmag = std::sqrt(Bp[IU] * Bp[IU] + Bp[IV] * Bp[IV] + Bp[IW] * Bp[IW]);
+  double VT[3] = {Bp[IU] - Un * nrm[0], Bp[IV] - Un * nrm[1], Bp[IW] - Un * nrm[2]};
+  double Mach_abs = vmag / BSound;
+  (void)Mach_abs;
+  double Mach_N = std::fabs(Un / BSound);
+  double pe = p_Amb;
+  double Fp[NP], Fun, Frho, FRgas;
+  if (Mach_N < 1.0 && p_Amb > 0.0) {
+    double delta = 0.5 * (BGamma - 1.0);
+    double denom = 1.0 / std::pow(1.0 + delta, BGamma / (BGamma - 1.0));
+    double pstar = Bp[IP] * denom * std::pow(1.0 + delta * (Mach_N * Mach_N), BGamma / (BGamma - 1.0));
+    if (pstar >= p_Amb) pe = pstar;
+    double Isentropic = (BGamma - 1.0) / (2.0 * BGamma);
+    double FSound = BSound * std::pow(pe / Bp[IP], Isentropic);
+    Fun = (Riem - FSound) / (BC_Sign * 0.5 * (BGamma - 1.0));
+    Fp[IP] = pe;
+    Frho = BGamma * Fp[IP] / (FSound * FSound);
+    Fp[0] = Bp[0] / Brho * Frho;
+    Fp[IU] = VT[0] + Fun * nrm[0];
+    Fp[IV] = VT[1] + Fun * nrm[1];
+    Fp[IW] = VT[2] + Fun * nrm[2];
+    FRgas = BRgas;
+  } else {
+    for (int s = 0; s < NP; ++s) Fp[s] = Bp[s];
+    Fun = Un; Frho = Brho; FRgas = BRgas;
+  }
+  double FEnth = 0.0;
+  double FT = Fp[IP] / (FRgas * Frho);
+  int Ti = tidx(th, FT);
+  double Td = FT - Ti;
+  double Flux[NP];
+  FEnth = FEnth + Fp[0] / Frho * tabT(th.h, Ti, Td);
+  Flux[0] = Fp[0] * area * Fun;
+  double Fmass = Frho * area * Fun;
+  Flux[IU] = Fp[IU] * Fmass + Fp[IP] * area * nrm[0];
+  Flux[IV] = Fp[IV] * Fmass + Fp[IP] * area * nrm[1];
+  Flux[IW] = Fp[IW] * Fmass + Fp[IP] * area * nrm[2];
+  double vt2 = Fp[IU] * Fp[IU] + Fp[IV] * Fp[IV] + Fp[IW] * Fp[IW];
+  Flux[IP] = Fmass * (0.5 * vt2 + FEnth);
+  for (int s = 0; s < NP; ++s) R[rb + s * nc] = R[rb + s * nc] + (double)modfm2 * Flux[s];
+}
+
 // ---- ghost fill ----
 inline int64_t rowg(const Ctx& c, int blk, int i, int j, int k) { return row(c.blk[blk], i, j, k); }
 
 void fill_ghosts(Ctx& c, double* P) {
   const int64_t nc = c.ncell;
-  // Fill_Ghost_Cell_blk: zero-gradient for type 11 / 4, cubic extrapolation for walls (Lib_Extrapolation.f90:643-730)
+  // Fill_Ghost_Cell_blk: symmetry for type 3, zero-gradient for types 11 / 4 / 24, cubic extrapolation for the walls
+  // 5 / 6 (Lib_Extrapolation.f90:643-730)
   for (const mb_bc& r : c.rec) {
     const Blk& b = c.blk[r.blk];
     int dir = (r.face + 1) / 2, gstep = 2 * (r.face % 2) - 1;
     int e[3] = {0, 0, 0};
     e[dir - 1] = 1;
-    if (r.type == MB_BC_EXTRAPOLATION || r.type == MB_BC_INFLOW) {
+    if (r.type == MB_BC_SYMMETRY) {  // Ghost_Symmetry (:558-587): the first layer only, normal velocity reversed
+      double nrm[3], area;
+      bc_face_geom(b, r.i, r.j, r.k, r.face, nrm, area);
+      int64_t src = row(b, r.i, r.j, r.k);
+      int64_t dst = row(b, r.i - gstep * e[0], r.j - gstep * e[1], r.k - gstep * e[2]);
+      double vel[3] = {P[src + IU * nc], P[src + IV * nc], P[src + IW * nc]};
+      double udotn = vel[0] * nrm[0] + vel[1] * nrm[1] + vel[2] * nrm[2];
+      for (int a = 0; a < 3; ++a) vel[a] = vel[a] - 2.0 * udotn * nrm[a];
+      P[dst] = P[src];
+      P[dst + IU * nc] = vel[0]; P[dst + IV * nc] = vel[1]; P[dst + IW * nc] = vel[2];
+      P[dst + IP * nc] = P[src + IP * nc];
+    } else if (r.type == MB_BC_EXTRAPOLATION || r.type == MB_BC_INFLOW || r.type == MB_BC_OUTLET) {
       int64_t src = row(b, r.i, r.j, r.k);
       for (int g = 1; g <= GC; ++g) {
         int64_t dst = row(b, r.i - gstep * g * e[0], r.j - gstep * g * e[1], r.k - gstep * g * e[2]);
         for (int s = 0; s < NP; ++s) P[dst + s * nc] = P[src + s * nc];
       }
-    } else if (r.type == MB_BC_WALL) {
+    } else if (r.type == MB_BC_WALL || r.type == MB_BC_WALL_T) {
       int step = -gstep;
       for (int g = 1; g <= GC; ++g) {
         int64_t d0 = row(b, r.i + g * step * e[0], r.j + g * step * e[1], r.k + g * step * e[2]);
@@ -1314,6 +1524,17 @@ void residual(Ctx& c, const double* P, double* R) {
           break;
         case MB_BC_INFLOW:
           bc_inflow_405(c, b, P, R, r.i, r.j, r.k, r.face, r.q);
+          break;
+        case MB_BC_SYMMETRY:
+          bc_symmetry_eul(c, b, P, R, r.i, r.j, r.k, r.face);
+          if (visc) bc_symmetry_visc(c, b, P, R, r.i, r.j, r.k, r.face);
+          break;
+        case MB_BC_WALL_T:
+          bc_symmetry_eul(c, b, P, R, r.i, r.j, r.k, r.face);
+          if (visc) bc_wall_temperature(c, b, P, R, r.i, r.j, r.k, r.face, r.q[0]);
+          break;
+        case MB_BC_OUTLET:
+          bc_outlet(c, b, P, R, r.i, r.j, r.k, r.face, r.q);
           break;
         default:
           break;
@@ -1544,7 +1765,10 @@ int orc_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, orc_
   c.conn.assign(mesh->conn, mesh->conn + mesh->nconn);
   for (const mb_bc& r : c.rec)
     if (r.type != MB_BC_CONNECTION && r.type != MB_BC_EXTRAPOLATION && r.type != MB_BC_WALL &&
-        r.type != MB_BC_INFLOW) { delete o; return MB_E_UNSUPPORTED; }
+        r.type != MB_BC_INFLOW && r.type != MB_BC_SYMMETRY && r.type != MB_BC_WALL_T && r.type != MB_BC_OUTLET) {
+      delete o;
+      return MB_E_UNSUPPORTED;
+    }
   c.pg.assign((size_t)c.rec.size() * 6 * NP, 0.0);
   if (sc->n_rk == 4) c.acc4.assign((size_t)c.ncell * NP, 0.0);
   Thermo& t = c.th;

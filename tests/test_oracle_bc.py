@@ -1,8 +1,11 @@
 """The oracle's wall, inlet and RK4 paths against known answers (no GPU): a gas at rest in a closed
 curvilinear box stays at rest (walls balance the pressure exactly), a uniform supersonic stream entering
 through a 405 inlet whose state is the stream's own leaves a zero residual, outward flow closes a 405
-face (no mass through it), the no-slip wall drags a tangential stream, and classical RK4 converges at
-fourth order in time (SSP-RK3 at third) on a smooth periodic problem."""
+face (no mass through it), the no-slip wall drags a tangential stream, an isothermal wall conducts the
+heat k (T_wall - T) / (dy / 2) into a gas at rest, symmetry faces act as the extrapolated faces of a
+transversely uniform tube, a 406 outlet at the stream's pressure passes a subsonic stream unchanged and
+one below it draws more mass out, inward flow closes a 406 face, and classical RK4 converges at fourth
+order in time (SSP-RK3 at third) on a smooth periodic problem."""
 import math
 
 import numpy as np
@@ -80,6 +83,75 @@ def test_no_slip_wall_drags_a_tangential_stream():
     A = c.blocks[0]["fm2"][3::4].max()
     # tau = mu du/dy with du/dy = u / (dy/2) between the wall and the first cell centre
     assert np.allclose(I[1, :, 0], mu * 100.0 / (0.5 * dy) * A, rtol=1e-10)
+
+
+SYM = abi.BC_SYMMETRY
+
+
+def test_isothermal_wall_conducts_heat_into_a_gas_at_rest():
+    Tw, T = 330.0, 300.0
+    bc = {1: SYM, 2: SYM, 3: (abi.BC_WALL_T, (Tw,)), 4: (abi.BC_WALL_T, (Tw,)), 5: SYM, 6: SYM}
+    c = cs.multiblock_2d(cols=1, rows=1, lo=8, hi=8, seed=4, amp=0.0, bc=bc, visc=1, velocity=0.0, T=T)
+    _, P, R = _residual(c)
+    I = c.interior(R, 0)
+    mu, cp, prandtl = c.meta["mu"], c.thermo["cp"][0], 0.71
+    kl = mu * cp / prandtl                        # constant viscosity and cp: k at the wall = k of the gas
+    dy = 1.0 / c.blocks[0]["n"][1]
+    A = c.blocks[0]["fm2"][3::4].max()
+    q = kl * (Tw - T) / (0.5 * dy) * A            # heat conducted in through each wall face
+    assert np.allclose(I[4, :, 0], -q, rtol=1e-9) and np.allclose(I[4, :, -1], -q, rtol=1e-9)
+    assert np.abs(I[4, :, 1:-1]).max() <= 1e-9 * q
+    assert np.abs(I[0]).max() == 0.0              # no mass through walls or symmetry faces, gas at rest
+
+
+def test_symmetry_faces_act_as_extrapolated_faces_of_a_uniform_tube():
+    a = cs.riemann_1d(n=100)
+    b = cs.riemann_1d(n=100)
+    b.rec["type"][b.rec["face"] >= 3] = SYM
+    Pa, Pb = a.P0.copy(), b.P0.copy()
+    oa, ob = oracle.Oracle(a), oracle.Oracle(b)
+    assert oa.step(Pa, 40) == 0 and ob.step(Pb, 40) == 0
+    e = H.rel_err(H.conserved(b, Pb), H.conserved(a, Pa))
+    assert np.all(e[[0, 1, 4]] <= 1e-12), e
+    assert np.abs(b.interior(Pb, 0)[2:4]).max() == 0.0   # no transverse motion
+
+
+def _outlet_stream(p_exit_ratio, velocity=None):
+    bc = {1: abi.BC_INFLOW, 2: (abi.BC_OUTLET, (p_exit_ratio * 1.0e5, 1.0)), 3: SYM, 4: SYM, 5: SYM, 6: SYM}
+    c = cs.multiblock_2d(cols=2, rows=1, lo=6, hi=9, seed=4, amp=0.0, bc=bc, visc=0, mach=0.5, velocity=velocity)
+    return c
+
+
+def test_outlet_at_the_stream_pressure_passes_a_subsonic_stream():
+    c = _outlet_stream(1.0)
+    _, P, R = _residual(c)
+    Ri = H.interior_rows(c, R)
+    rho, V = c.meta["rho"], c.meta["V"]
+    A = c.blocks[0]["fm1"][3::4].max()
+    scale = np.array([rho * V, rho * V * V, rho * V * V, rho * V * V, rho * V ** 3]) * A
+    assert (np.abs(Ri).max(axis=1) <= 1e-9 * scale).all(), np.abs(Ri).max(axis=1) / scale
+
+
+def test_outlet_below_the_stream_pressure_draws_more_mass_out():
+    c = _outlet_stream(0.8)
+    _, P, R = _residual(c)
+    last = c.interior(R, 1)                       # the block at the outlet
+    rho, V = c.meta["rho"], c.meta["V"]
+    A = c.blocks[1]["fm1"][3::4].max()
+    assert (last[0, -1] > 1e-3 * rho * V * A).all()          # net mass out of the outlet cells
+    assert np.abs(last[0, :-1]).max() <= 1e-9 * rho * V * A  # the stream elsewhere untouched
+
+
+def test_inward_flow_closes_a_406_face():
+    bc = {1: abi.BC_EXTRAPOLATION, 2: (abi.BC_OUTLET, (1.0e5, 0.5)), 3: SYM, 4: SYM, 5: SYM, 6: SYM}
+    c = cs.multiblock_2d(cols=1, rows=1, lo=8, hi=8, seed=4, amp=0.0, bc=bc, visc=0, velocity=-300.0)
+    _, P, R = _residual(c)
+    I = c.interior(R, 0)
+    rho = c.meta["rho"]
+    A = c.blocks[0]["fm1"][3::4].max()
+    # cells at i = max: only the interior face i - 1/2 carries mass (u < 0); cells inside: zero
+    assert np.allclose(I[0, -1], rho * 300.0 * A, rtol=1e-12)
+    assert np.abs(I[0, 1:-1]).max() <= 1e-12 * rho * 300.0 * A
 
 
 def _entropy_wave(n, cfl, n_rk, t_end=0.05):
