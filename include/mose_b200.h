@@ -187,6 +187,10 @@ typedef struct mb_status {
   double dt;           /* dt of the last step */
   int32_t done;        /* the case reached its stop time (t_end) and no longer advances */
   int32_t pad0;
+  double res[5];       /* residual diagnostic of the last step taken by mb_step / mb_stage (Compute_Residual_blk,
+                          Mod_Diagnostic.f90:64-104, as the L2 norm of Mod_Explicit.f90:325-358): sqrt of the sum
+                          over the case's interior cells of (new - old)^2 of rho, u, v, w, p; in the mixed form the
+                          partial sums of a warp are FP32 */
 } mb_status;
 
 /* The stop rule of one case of a batch (mb_group_reset): the reference's time loop stops at time >= timemax

@@ -642,6 +642,7 @@ static void to_status(const DevState& h, int state_check, mb_status* st) {
   st->time = h.time;
   st->dt = h.dt;
   st->done = h.done;
+  for (int v = 0; v < MB_NPRIM; ++v) st->res[v] = sqrt(h.res2[v]);
   st->code = MB_OK;
   if (h.n_bad_thermo > 0) st->code = MB_E_THERMO;
   else if (h.n_bad_state > 0 && state_check) st->code = MB_E_STATE;

@@ -1011,7 +1011,7 @@ __device__ __forceinline__ void stage_plane(const Params& p, const DBlk& b, cons
 template <typename R, int TY, bool VISC, int MODE, int RS, int LIM, bool KM>
 __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const double* __restrict__ Pin,
                                            const double* Pold, double* Pout, double* Rout, double rkc, int last,
-                                           unsigned char* smem_raw, double* sred) {
+                                           unsigned char* smem_raw, double* sred, double* s_res) {
   constexpr int NF = VISC ? 2 * MB_NP : MB_NP;  // values a face task computes (convective, viscous)
   // values a face keeps in shared memory: both fluxes in the FP64 form (pass 2 sums them in the reference's
   // order); the net flux (convective - viscous) in the mixed form
@@ -1034,6 +1034,7 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
   const bool own = (i <= b.n1) && (j <= b.n2);
   const double dt = (MODE == MODE_UPDATE) ? st->dt : 0.0;
   double dtloc = 1e300;
+  if (MODE == MODE_UPDATE && last && tid < 8 * MB_NP) s_res[tid] = 0.0;  // used after the prologue's barrier
   int kb = 0;  // buffer of the k-face above the current plane
   // ghost layers the stencils read: 2 along an axis with faces; for a block one cell deep along j or k (2-D,
   // 1-D) no face of that axis exists and only the viscous transverse gradient reads one ghost layer
@@ -1086,6 +1087,11 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
       for (int q = 0; q < NS; ++q) dst[q] = NET ? out[q] - out[MB_NP + q] : out[q];
     }
     __syncthreads();
+    // the residual diagnostic of the last stage: (new - old)^2 of this thread's cell, in the flux type (the warps'
+    // partial sums in FP32 in the mixed form: the diagnostic to FP32 accuracy there)
+    R rsq[MB_NP];
+#pragma unroll
+    for (int v = 0; v < MB_NP; ++v) rsq[v] = (R)0;
     if (own) {
       // ---- pass 2 (pass2_body.inc): convective i +,-, j +,-, k +,-, then viscous i -,+, j -,+, k -,+
       double acc[MB_NP];
@@ -1161,6 +1167,11 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
 #pragma unroll
         for (int s = 0; s < MB_NP; ++s) Pout[r + s * p.nc] = pn[s];
         if (last) {  // the new state's local dt, in the flux type (FP64 in the parity form)
+#pragma unroll
+          for (int v = 0; v < MB_NP; ++v) {
+            const R dv = (R)(pn[v] - po[v]);
+            rsq[v] = dv * dv;
+          }
           R pr[MB_NP];
 #pragma unroll
           for (int s = 0; s < MB_NP; ++s) pr[s] = cvt<R>(pn[s]);
@@ -1168,9 +1179,25 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
         }
       }
     }
+    if (MODE == MODE_UPDATE && last) {  // uniform over the CTA: each warp adds its plane sums into its own slots
+#pragma unroll
+      for (int v = 0; v < MB_NP; ++v) {
+        R x = rsq[v];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((tid & 31) == 0) s_res[8 * v + (tid >> 5)] += (double)x;
+      }
+    }
     kb ^= 1;
   }
-  if (MODE == MODE_UPDATE && last) cta_min_dt(st, dtloc, sred);
+  if (MODE == MODE_UPDATE && last) {
+    cta_min_dt(st, dtloc, sred);  // its barrier also orders the warps' sums before their reads below
+    if (tid < MB_NP) {
+      double x = 0.0;
+      for (int w = 0; w < (TY < 8 ? TY : 8); ++w) x += s_res[8 * tid + w];
+      atomicAdd(&st->res2[tid], x);
+    }
+  }
 }
 
 // The fused stage over a tile list (KM: the tiles of mirrored one-plane blocks, a separate instantiation so that
@@ -1185,9 +1212,12 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
         double* Rout, double rkc, int last) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double sred[32];
+  __shared__ double s_res[8 * MB_NP];  // per warp (at most 8) and variable: the tile's residual sums
   __shared__ int s_next;
+  static_assert(TY <= 8, "one residual slot per warp");
   if (!p.queue) {
-    sweep_tile<R, TY, VISC, MODE, RS, LIM, KM>(p, tiles[blockIdx.x], Pin, Pold, Pout, Rout, rkc, last, smem_raw, sred);
+    sweep_tile<R, TY, VISC, MODE, RS, LIM, KM>(p, tiles[blockIdx.x], Pin, Pold, Pout, Rout, rkc, last, smem_raw, sred,
+                                                s_res);
     return;
   }
   for (;;) {
@@ -1195,7 +1225,8 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
     __syncthreads();
     const int tix = s_next;
     if (tix >= p.ntiles_run) break;
-    sweep_tile<R, TY, VISC, MODE, RS, LIM, KM>(p, tiles[tix], Pin, Pold, Pout, Rout, rkc, last, smem_raw, sred);
+    sweep_tile<R, TY, VISC, MODE, RS, LIM, KM>(p, tiles[tix], Pin, Pold, Pout, Rout, rkc, last, smem_raw, sred,
+                                                s_res);
     __syncthreads();  // the tile's shared memory is free and s_next may be overwritten
   }
 }

@@ -152,6 +152,7 @@ __global__ void k_clock(Params p) {
     st->time = st->time + dtg;
     st->steps = st->steps + 1;
     st->dtmin_bits = (unsigned long long)__double_as_longlong(1e300);
+    for (int v = 0; v < MB_NP; ++v) st->res2[v] = 0.0;
   }
 }
 
@@ -163,6 +164,7 @@ __global__ void k_group_reset(Params p, int g, int time_clip, double t_end) {
   st->n_bad_state = 0; st->n_bad_thermo = 0;
   st->bad_blk = 0; st->bad_i = 0; st->bad_j = 0; st->bad_k = 0; st->first_bad_claimed = 0;
   st->time_clip = time_clip; st->done = 0; st->t_end = t_end;
+  for (int v = 0; v < MB_NP; ++v) st->res2[v] = 0.0;
 }
 
 // ---- launchers ----

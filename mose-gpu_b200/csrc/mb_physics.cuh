@@ -84,6 +84,8 @@ struct DevState {
   int time_clip;                  // the case's stop rule: clip the last step onto t_end
   int done;                       // the case reached t_end: its tiles are skipped
   double t_end;                   // 0: no stop
+  double res2[MB_NP];             // sum over the case's interior cells of (new - old)^2 of the step's primitive state
+                                  // (the fused last stage accumulates it; zeroed at the step's start)
 };
 
 struct Params {

@@ -86,7 +86,7 @@ class MBStatus(C.Structure):
     _fields_ = [("code", C.c_int32), ("n_bad_state", C.c_int32), ("n_bad_thermo", C.c_int32),
                 ("bad_blk", C.c_int32), ("bad_i", C.c_int32), ("bad_j", C.c_int32), ("bad_k", C.c_int32),
                 ("steps", C.c_int32), ("time", C.c_double), ("dt", C.c_double), ("done", C.c_int32),
-                ("pad0", C.c_int32)]
+                ("pad0", C.c_int32), ("res", C.c_double * 5)]
 
 
 class MBGroup(C.Structure):

@@ -35,6 +35,7 @@
 //   local dt                src/lib/gpu/dt_blk.inc:11-222, numerics/time/Mod_dt.f90:15-106
 //   thermo leaves           lib/FLINT/src/lib/Lib_ThermoTransport_dev.f90:54-300
 //   the step                explicit/Mod_Explicit.f90:52-279
+//   residual diagnostic     src/lib/diagnostic/Mod_Diagnostic.f90:64-104, Mod_Explicit.f90:325-358
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
@@ -1811,6 +1812,20 @@ int orc_step(orc_ctx* o, double* P, double* PO, double* R, int nsteps) {
       residual(c, P, R);
       update(c, P, PO, R, irk, dt);
     }
+    // the residual diagnostic of the step (Compute_Residual_blk, Mod_Diagnostic.f90:64-104; the L2 norm of
+    // Mod_Explicit.f90:325-358): sqrt of the sum over the interior cells of (new - old)^2 per primitive variable
+    double r2[NP] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (const Blk& b : c.blk)
+      for (int k = 1; k <= b.n3; ++k)
+        for (int j = 1; j <= b.n2; ++j)
+          for (int i = 1; i <= b.n1; ++i) {
+            const int64_t r = row(b, i, j, k);
+            for (int v = 0; v < NP; ++v) {
+              const double d = P[r + v * c.ncell] - PO[r + v * c.ncell];
+              r2[v] = r2[v] + d * d;
+            }
+          }
+    for (int v = 0; v < NP; ++v) c.st.res[v] = std::sqrt(r2[v]);
     c.st.steps += 1;
     if (c.st.code != MB_OK) return c.st.code;
   }

@@ -210,3 +210,28 @@ def test_multiblock_2d_many_steps_fp64_and_mixed(torch_cuda):
     assert np.all(e <= TOL_MANY), e
     l1, l2, li = H.norms(H.conserved(case, b.state()), H.conserved(case, a.state()))
     assert l2[0] < 1e-5, l2
+
+
+@pytest.mark.parametrize("cid", ["sod_hllc_minmod", "tgv_hllc_minmod_8blk", "mb2d_ausm_vanleer_rk4",
+                                 "duct3d_hllc_vanleer"])
+def test_residual_diagnostic_matches_the_oracle(torch_cuda, cid):
+    """The residual diagnostic accumulated in the fused last stage (sum of (new - old)^2, reduced per tile) equals
+    the oracle's after one and after several steps in the FP64 form; the mixed form's agrees to its accuracy."""
+    import oracle
+    from mosegpu.engine import Engine
+    case = dict(H.small_cases())[cid]()
+    orc = oracle.Oracle(case)
+    eng = Engine(case)
+    mix = Engine(case, precision=abi.PREC_MIXED)
+    P = case.P0.copy()
+    for n in (1, 6):
+        assert orc.step(P, n) == 0
+        eng.step(n, graph=(n > 1))
+        mix.step(n, graph=(n > 1))
+        want = np.array(orc.status().res[:])
+        got = np.array(eng.status().res[:])
+        scale = want.max()
+        assert scale > 0
+        assert np.all(np.abs(got - want) <= 1e-10 * scale), (got, want)
+        gm = np.array(mix.status().res[:])
+        assert np.all(np.abs(gm - want) <= 1e-3 * scale), (gm, want)

@@ -130,3 +130,24 @@ def test_golden_vectors():
         np.testing.assert_array_equal(R, ref["R"])
         np.testing.assert_array_equal(P, ref["P"])
         assert dt == float(ref["dt"])
+
+
+def test_residual_diagnostic_is_the_l2_norm_of_the_step_change():
+    """status.res = sqrt(sum over interior cells of (new - old)^2) per primitive variable (Compute_Residual_blk,
+    the L2 norm of Explicit_Step), zero for a state that does not change."""
+    c = cs.riemann_1d(n=100)
+    o = oracle.Oracle(c)
+    P = c.P0.copy()
+    assert o.step(P, 3) == 0
+    P0 = P.copy()
+    assert o.step(P, 1) == 0
+    m = c.interior_mask()
+    want = np.sqrt(((P[:, m] - P0[:, m]) ** 2).sum(axis=1))
+    got = np.array(o.status().res[:])
+    assert np.allclose(got, want, rtol=1e-12, atol=0.0), (got, want)
+    assert got[0] > 0 and got[2] == 0.0 and got[3] == 0.0
+    u = cs.riemann_1d(n=50, left=(1.0, 0.0, 1.0), right=(1.0, 0.0, 1.0))   # no jump: nothing moves
+    ou = oracle.Oracle(u)
+    Pu = u.P0.copy()
+    assert ou.step(Pu, 2) == 0
+    assert max(ou.status().res[:]) == 0.0
