@@ -175,6 +175,9 @@ typedef struct mb_scheme {
   double schmidt;     /* laminar Schmidt (Lib_RANS.f90:25), 0.7 */
   double mco;         /* riemann-options-Mco (LMRoe low-Mach floor; 1 = plain Roe) */
   double time_threshold;
+  double res_stop;    /* [MOSE-parameters] res-threshold (MOSE_Types_m.f90:247-250, default 1e-10 there): the case
+                         stops once the residual diagnostic of rho (mb_status.res[0]) of a step is <= res_stop, as
+                         Explicit_Step's end test (Mod_Explicit.f90:363-370); 0 = no residual stop */
 } mb_scheme;
 
 typedef struct mb_status {
@@ -185,7 +188,7 @@ typedef struct mb_status {
   int32_t steps;       /* steps taken by mb_step since mb_init (or the case's mb_group_reset) */
   double time;         /* simulated time (sum of dt) */
   double dt;           /* dt of the last step */
-  int32_t done;        /* the case reached its stop time (t_end) and no longer advances */
+  int32_t done;        /* the case reached its stop time (t_end) or residual (res_stop) and no longer advances */
   int32_t pad0;
   double res[5];       /* residual diagnostic of the last step taken by mb_step / mb_stage (Compute_Residual_blk,
                           Mod_Diagnostic.f90:64-104, as the L2 norm of Mod_Explicit.f90:325-358): sqrt of the sum
@@ -199,6 +202,7 @@ typedef struct mb_group {
   int32_t time_clip;  /* clip the last step onto t_end */
   int32_t pad0;
   double t_end;       /* the case stops advancing once its time reaches t_end (0: never) */
+  double res_stop;    /* ... or once a step's residual of rho (mb_status.res[0]) is <= res_stop (0: never) */
 } mb_group;
 
 typedef struct mb_ctx mb_ctx;

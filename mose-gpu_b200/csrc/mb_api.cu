@@ -500,6 +500,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
     return MB_E_UNSUPPORTED;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
   if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
+  if (!(sc->res_stop >= 0.0)) return MB_E_ARG;
   if (sc->precision != MB_PREC_FP64 && sc->precision != MB_PREC_MIXED) return MB_E_UNSUPPORTED;
   if (sc->ndir < 1 || sc->ndir > 3) return MB_E_ARG;
   if (th->tmax - th->tmin < 2 || !th->cp || !th->h || !th->mu || !th->k) return MB_E_ARG;
@@ -544,6 +545,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
       memcpy(&h.dtmin_bits, &big, sizeof(double));
       h.time_clip = sc->time_clip;
       h.t_end = sc->time_clip ? sc->time_threshold : 0.0;
+      h.res_stop = sc->res_stop;
     }
     if (cudaMemcpy(c->d_st, hs.data(), ngroups * sizeof(DevState), cudaMemcpyHostToDevice) != cudaSuccess) {
       free_ctx(c);
@@ -623,10 +625,10 @@ int mb_reconfigure(mb_ctx* ctx, const mb_mesh* mesh) {
 }
 
 int mb_group_reset(mb_ctx* ctx, int g, const mb_group* spec, const double* P, void* stream) {
-  if (!ctx || !spec || !P || g < 0 || g >= ctx->ngroups || spec->t_end < 0.0) return MB_E_ARG;
+  if (!ctx || !spec || !P || g < 0 || g >= ctx->ngroups || spec->t_end < 0.0 || spec->res_stop < 0.0) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
   cudaStream_t s = (cudaStream_t)stream;
-  CK(group_reset(ctx->p, g, spec->time_clip, spec->t_end, s));
+  CK(group_reset(ctx->p, g, spec->time_clip, spec->t_end, spec->res_stop, s));
   CK(ctx->sc.precision == MB_PREC_MIXED ? sweep_f32_rs1_dt(ctx->p, ctx->d_tiles_aux, ctx->ntiles_aux, P, g, s)
                                          : dt_cells(ctx->p, ctx->d_tiles_aux, ctx->ntiles_aux, P, s, g));
   ctx->launches += 2;

@@ -141,6 +141,11 @@ __global__ void k_clock(Params p) {
       st->done = 1;
       continue;
     }
+    // the residual end test of the step just taken (Mod_Explicit.f90:363-370: residuotot(1) <= restop)
+    if (st->res_stop > 0.0 && st->steps > 0 && sqrt(st->res2[0]) <= st->res_stop) {
+      st->done = 1;
+      continue;
+    }
     double dtg = 1e5;
     double dm = __longlong_as_double((long long)st->dtmin_bits);
     dtg = mn(dm, dtg);
@@ -157,13 +162,13 @@ __global__ void k_clock(Params p) {
 }
 
 // mb_group_reset: case g starts afresh with its stop rule
-__global__ void k_group_reset(Params p, int g, int time_clip, double t_end) {
+__global__ void k_group_reset(Params p, int g, int time_clip, double t_end, double res_stop) {
   DevState* st = p.st + g;
   st->dtmin_bits = (unsigned long long)__double_as_longlong(1e300);
   st->dt = 0.0; st->time = 0.0; st->steps = 0; st->code = 0;
   st->n_bad_state = 0; st->n_bad_thermo = 0;
   st->bad_blk = 0; st->bad_i = 0; st->bad_j = 0; st->bad_k = 0; st->first_bad_claimed = 0;
-  st->time_clip = time_clip; st->done = 0; st->t_end = t_end;
+  st->time_clip = time_clip; st->done = 0; st->t_end = t_end; st->res_stop = res_stop;
   for (int v = 0; v < MB_NP; ++v) st->res2[v] = 0.0;
 }
 
@@ -218,8 +223,8 @@ cudaError_t clock_step(const Params& p, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t group_reset(const Params& p, int g, int time_clip, double t_end, cudaStream_t s) {
-  k_group_reset<<<1, 1, 0, s>>>(p, g, time_clip, t_end);
+cudaError_t group_reset(const Params& p, int g, int time_clip, double t_end, double res_stop, cudaStream_t s) {
+  k_group_reset<<<1, 1, 0, s>>>(p, g, time_clip, t_end, res_stop);
   return cudaGetLastError();
 }
 

@@ -74,6 +74,6 @@ cudaError_t update_cells(const Params& p, const DTile* tiles, int ntiles, double
 cudaError_t reset_dt(const Params& p, cudaStream_t s, int only_group = -1);
 cudaError_t to_float(const double* src, float* dst, long long n, cudaStream_t s);
 cudaError_t clock_step(const Params& p, cudaStream_t s);
-cudaError_t group_reset(const Params& p, int g, int time_clip, double t_end, cudaStream_t s);
+cudaError_t group_reset(const Params& p, int g, int time_clip, double t_end, double res_stop, cudaStream_t s);
 
 }  // namespace mb

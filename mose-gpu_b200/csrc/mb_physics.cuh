@@ -86,6 +86,7 @@ struct DevState {
   double t_end;                   // 0: no stop
   double res2[MB_NP];             // sum over the case's interior cells of (new - old)^2 of the step's primitive state
                                   // (the fused last stage accumulates it; zeroed at the step's start)
+  double res_stop;                // the case stops once sqrt(res2[0]) of a step is <= res_stop (0: never)
 };
 
 struct Params {

@@ -79,7 +79,7 @@ class MBScheme(C.Structure):
                 ("state_check", C.c_int32), ("dt_additive", C.c_int32), ("pad0", C.c_int32),
                 ("cfl", C.c_double), ("vnn", C.c_double),
                 ("prandtl", C.c_double), ("schmidt", C.c_double), ("mco", C.c_double),
-                ("time_threshold", C.c_double)]
+                ("time_threshold", C.c_double), ("res_stop", C.c_double)]
 
 
 class MBStatus(C.Structure):
@@ -90,7 +90,7 @@ class MBStatus(C.Structure):
 
 
 class MBGroup(C.Structure):
-    _fields_ = [("time_clip", C.c_int32), ("pad0", C.c_int32), ("t_end", C.c_double)]
+    _fields_ = [("time_clip", C.c_int32), ("pad0", C.c_int32), ("t_end", C.c_double), ("res_stop", C.c_double)]
 
 
 BC_DTYPE = np.dtype([("blk", "<i4"), ("i", "<i4"), ("j", "<i4"), ("k", "<i4"), ("face", "<i4"),

@@ -178,6 +178,7 @@ class Case:
         s.cfl = d["cfl"]; s.vnn = d.get("vnn", 0.3); s.prandtl = d.get("prandtl", 0.0)
         s.schmidt = d.get("schmidt", 0.7); s.mco = d.get("mco", 1.0)
         s.time_threshold = d.get("time_threshold", 0.0)
+        s.res_stop = d.get("res_stop", 0.0)
         return s
 
 

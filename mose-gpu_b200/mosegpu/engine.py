@@ -202,9 +202,10 @@ class Engine:
         return st
 
     def run_to(self, t_end, max_steps=10 ** 7, chunk=1):
-        """Steps until the simulated time reaches t_end (the reference's `time >= timemax` stop)."""
+        """Steps until the simulated time reaches t_end (the reference's `time >= timemax` stop) or the case's
+        residual stop (scheme res_stop) ends it."""
         n = 0
-        while self.status().time < t_end and n < max_steps:
+        while self.status().time < t_end and not self.status().done and n < max_steps:
             self.step(chunk, graph=False)
             n += chunk
         return n

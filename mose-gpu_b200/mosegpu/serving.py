@@ -28,12 +28,14 @@ GEO_BYTES_PER_CELL = (3 * 4 + 3 + 9 + 1) * 8
 
 
 class Request:
-    """One case to solve: a Case (cs.layout_case) with its stop time, arriving at `arrival` seconds."""
+    """One case to solve: a Case (cs.layout_case) with its stop time (and, for a steady case, the residual of rho
+    at which it stops: res_stop, 0 = none), arriving at `arrival` seconds."""
 
-    def __init__(self, rid, case, t_end, arrival=0.0, geo_key=None):
+    def __init__(self, rid, case, t_end, arrival=0.0, geo_key=None, res_stop=0.0):
         self.rid = rid
         self.case = case
         self.t_end = float(t_end)
+        self.res_stop = float(res_stop)
         self.arrival = float(arrival)
         self.geo_key = geo_key
         self.npad = int(case.ncell)
@@ -240,6 +242,7 @@ class Server:
             spec = abi.MBGroup()
             spec.time_clip = 1
             spec.t_end = req.t_end
+            spec.res_stop = req.res_stop
             _check(self.L.mb_group_reset(self.ctx, grp, C.byref(spec), self.P.data_ptr(), self._s()), "mb_group_reset")
 
     def poll(self, now_fn):

@@ -1799,6 +1799,7 @@ int orc_step(orc_ctx* o, double* P, double* PO, double* R, int nsteps) {
   Ctx& c = o->c;
   const int64_t n = c.ncell * NP;
   for (int st = 0; st < nsteps; ++st) {
+    if (c.st.done) return MB_OK;  // the residual end test stopped the case (Mod_Explicit.f90:363-370)
     double dt = compute_dt(c, P);
     if (c.sc.time_clip) {  // Clip_dt_To_Timemax (Mod_dt.f90:283-296)
       double rem = c.sc.time_threshold - c.st.time;
@@ -1827,6 +1828,7 @@ int orc_step(orc_ctx* o, double* P, double* PO, double* R, int nsteps) {
           }
     for (int v = 0; v < NP; ++v) c.st.res[v] = std::sqrt(r2[v]);
     c.st.steps += 1;
+    if (c.sc.res_stop > 0.0 && c.st.res[0] <= c.sc.res_stop) c.st.done = 1;
     if (c.st.code != MB_OK) return c.st.code;
   }
   return MB_OK;

@@ -122,7 +122,7 @@ class Oracle:
     def run_to(self, P, t_end, max_steps=1000000):
         """Steps until the simulated time reaches t_end (the reference's `time >= timemax` stop)."""
         n = 0
-        while self.status().time < t_end and n < max_steps:
+        while self.status().time < t_end and not self.status().done and n < max_steps:
             rc = self.step(P, 1)
             if rc != 0:
                 raise abi.MoseError(rc, "orc_step")

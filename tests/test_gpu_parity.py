@@ -235,3 +235,30 @@ def test_residual_diagnostic_matches_the_oracle(torch_cuda, cid):
         assert np.all(np.abs(got - want) <= 1e-10 * scale), (got, want)
         gm = np.array(mix.status().res[:])
         assert np.all(np.abs(gm - want) <= 1e-3 * scale), (gm, want)
+
+
+def test_residual_stop_matches_the_oracle(torch_cuda):
+    """A case with a residual stop (res_stop between two steps' residuals) stops at the oracle's step, in the same
+    state, and further steps leave it alone (the device clock marks it done)."""
+    import oracle
+    from mosegpu.engine import Engine
+    case = dict(H.small_cases())["mb2d_ausm_vanleer_rk4"]()
+    orc = oracle.Oracle(case)
+    P = case.P0.copy()
+    res = []
+    for _ in range(10):
+        assert orc.step(P, 1) == 0
+        res.append(orc.status().res[0])
+    thr = res[5] * (1.0 + 1e-8)
+    assert all(abs(r - thr) > 1e-6 * thr for i, r in enumerate(res) if i != 5)   # no other residual near it
+    k = next(i for i, r in enumerate(res) if r <= thr) + 1
+    case.scheme["res_stop"] = thr
+    eng = Engine(case)
+    eng.step(12, graph=True)
+    st = eng.status()
+    assert st.done == 1 and st.steps == k, (st.steps, k, res)
+    ref = oracle.Oracle(case)
+    Pk = case.P0.copy()
+    assert ref.step(Pk, 12) == 0 and ref.status().steps == k
+    e = H.rel_err(H.conserved(case, eng.state()), H.conserved(case, Pk))
+    assert np.all(e <= TOL_ONE), e

@@ -151,3 +151,20 @@ def test_residual_diagnostic_is_the_l2_norm_of_the_step_change():
     Pu = u.P0.copy()
     assert ou.step(Pu, 2) == 0
     assert max(ou.status().res[:]) == 0.0
+
+
+def test_residual_stop_ends_a_converged_case():
+    """res_stop (the reference's res-threshold): a state that does not change stops after its first step, and
+    further steps leave it alone; a moving one runs on."""
+    u = cs.riemann_1d(n=50, left=(1.0, 0.0, 1.0), right=(1.0, 0.0, 1.0))
+    u.scheme["res_stop"] = 1e-10
+    o = oracle.Oracle(u)
+    P = u.P0.copy()
+    assert o.step(P, 5) == 0
+    st = o.status()
+    assert st.done == 1 and st.steps == 1
+    c = cs.riemann_1d(n=50)
+    c.scheme["res_stop"] = 1e-10
+    oc = oracle.Oracle(c)
+    Pc = c.P0.copy()
+    assert oc.step(Pc, 5) == 0 and oc.status().steps == 5 and oc.status().done == 0
