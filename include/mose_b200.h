@@ -88,7 +88,9 @@ extern "C" {
 #define MB_RS_AUSMP 4
 #define MB_RS_LLF 8
 #define MB_RS_SLAU2 9
+#define MB_RS_EXACT 11
 #define MB_RS_LMROE 12
+#define MB_RS_MICZEKROE 13
 
 #define MB_PREC_FP64 0
 #define MB_PREC_MIXED 1 /* reconstruction + Riemann + viscous flux arithmetic in FP32; state,

@@ -496,7 +496,8 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   if (!mesh || !sc || !th || !out) return MB_E_ARG;
   *out = nullptr;
   if (sc->riemann != MB_RS_HLLC && sc->riemann != MB_RS_HLLE && sc->riemann != MB_RS_SLAU && sc->riemann != MB_RS_AUSMP &&
-      sc->riemann != MB_RS_LLF && sc->riemann != MB_RS_SLAU2 && sc->riemann != MB_RS_LMROE)
+      sc->riemann != MB_RS_LLF && sc->riemann != MB_RS_SLAU2 && sc->riemann != MB_RS_LMROE && sc->riemann != MB_RS_EXACT &&
+      sc->riemann != MB_RS_MICZEKROE)
     return MB_E_UNSUPPORTED;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
   if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;

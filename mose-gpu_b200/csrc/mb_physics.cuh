@@ -322,6 +322,25 @@ MB_HD R h_static(const Params& p, R rhoi, R pr) {
   return (R)0 + hs * rhoi / rho_;
 }
 
+template <typename R> MB_HD R powr(R x, R y);
+template <> MB_HD double powr(double x, double y) { return pow(x, y); }
+template <> MB_HD float powr(float x, float y) { return powf(x, y); }
+
+// gamma of a state as riemann_open_body.inc writes f_gamma out (:349-366): T from p / (R rho_tot), the table row
+// int(T) with both rows held to the table
+template <typename R>
+MB_HD R gam_state(const Params& p, R d, R pr, R dtot) {
+  const R* CP = Tab<R>::cp(p);
+  R rho_ = (R)0 + d;
+  R rg_ = (R)0 + (R)p.ri * d / rho_;
+  R T_ = pr / (rg_ * dtot);
+  int Ti = (int)T_;
+  R Td = T_ - (R)Ti;
+  int t1 = max(p.tmin, min(Ti, p.tmax)), t2 = max(p.tmin, min(Ti + 1, p.tmax));
+  R cp_ = (R)0 + d / dtot * (CP[t1] + (CP[t2] - CP[t1]) * Td);
+  return cp_ / (cp_ - rg_);
+}
+
 template <typename R>
 MB_HD void riemann_open(const Params& p, int rs, R dl, R ul, R vl, R wl, R pl, R al, R dltot,
                                              R dr, R ur, R vr, R wr, R pr, R ar, R drtot, R nx, R ny, R nz,
@@ -360,6 +379,174 @@ MB_HD void riemann_open(const Params& p, int rs, R dl, R ul, R vl, R wl, R pl, R
     F_v = mdotp * vl + mdotm * vr + ny * phalf;
     F_w = mdotp * wl + mdotm * wr + nz * phalf;
     F_E = mdotp * H_L + mdotm * H_R;
+    return;
+  }
+  if (rs == 11) {  // exact Godunov (riemann_open_body.inc:348-516): Newton on the star velocity, gamma of each state
+    R gam_L = gam_state(p, dl, pl, dltot), gam_R = gam_state(p, dr, pr, drtot);
+    R gm1 = gam_L - (R)1.0, gm4 = gam_R - (R)1.0;
+    R d1 = (R)0.5 * gm1, d4 = (R)0.5 * gm4;
+    R e1 = gam_L / d1, e4 = gam_R / d4;
+    R un1 = ul * nx + vl * ny + wl * nz;
+    R ut1 = ul - un1 * nx, vt1 = vl - un1 * ny, wt1 = wl - un1 * nz;
+    R un4 = ur * nx + vr * ny + wr * nz;
+    R ut4 = ur - un4 * nx, vt4 = vr - un4 * ny, wt4 = wr - un4 * nz;
+    R r2i = un1 + ((R)2.0 / gm1) * al;
+    R r1iv = un4 - ((R)2.0 / gm4) * ar;
+    R dum = (pl < pr) ? gm4 / ((R)2.0 * gam_R) : gm1 / ((R)2.0 * gam_L);
+    R z = (gm1 / gm4) * (ar / al) * powr(pl / pr, dum);
+    R vel = (z * r2i + r1iv) / ((R)1.0 + z);
+    R p3 = (R)1.0, p2 = (R)2.0 * p3, dpr = (R)0.0, dpl = (R)0.0;
+    int iter = 0;
+    R swl = (R)0.0, swr = (R)0.0, vw1 = (R)0.0, vw2 = (R)0.0, vw3 = (R)0.0, vw4 = (R)0.0, a2 = al, a3 = ar;
+    while (fabs((R)1.0 - (p2 / p3)) >= (R)1e-5 && iter <= 1000) {
+      if (vel < un1) {  // shock on the left
+        R x = (gam_L + (R)1.0) * (vel - un1) / ((R)4.0 * al);
+        R mrel = x - rsqrt_((R)1.0 + x * x);
+        R c = gam_L * pl / al;
+        p2 = pl + c * (vel - un1) * mrel;
+        dpr = (R)2.0 * c * powr(mrel, (R)3.0) / ((R)1.0 + mrel * mrel);
+        R rp = p2 / pl;
+        swl = un1 + al * mrel;
+        a2 = al * rsqrt_((gam_L + (R)1.0 + (gam_L - (R)1.0) * rp) / (gam_L + (R)1.0 + (gam_L - (R)1.0) / rp));
+      } else {  // rarefaction on the left
+        R delta = (R)0.5 * (gam_L - (R)1.0);
+        R dum1 = (R)2.0 * gam_L / (gam_L - (R)1.0);
+        a2 = al - delta * (vel - un1);
+        p2 = pl * powr(a2 / al, dum1);
+        dpr = -gam_L * p2 / a2;
+        vw1 = un1 - al;
+        vw2 = vel - a2;
+      }
+      if (vel > un4) {  // shock on the right
+        R x = (gam_R + (R)1.0) * (vel - un4) / ((R)4.0 * ar);
+        R mrel = x + rsqrt_((R)1.0 + x * x);
+        R c = gam_R * pr / ar;
+        p3 = pr + c * (vel - un4) * mrel;
+        dpl = (R)2.0 * c * powr(mrel, (R)3.0) / ((R)1.0 + mrel * mrel);
+        R rp = p3 / pr;
+        swr = un4 + ar * mrel;
+        a3 = ar * rsqrt_((gam_R + (R)1.0 + (gam_R - (R)1.0) * rp) / (gam_R + (R)1.0 + (gam_R - (R)1.0) / rp));
+      } else {  // rarefaction on the right
+        R delta = (R)0.5 * (gam_R - (R)1.0);
+        R dum1 = (R)2.0 * gam_R / (gam_R - (R)1.0);
+        a3 = ar + delta * (vel - un4);
+        p3 = pr * powr(a3 / ar, dum1);
+        dpl = gam_R * p3 / a3;
+        vw3 = vel + a3;
+        vw4 = un4 + ar;
+      }
+      vel = vel - ((p2 - p3) / (dpr - dpl));
+      iter = iter + 1;
+    }
+    R af, pf, rhof, uf, vf, wf, Hs;
+    if (vel > (R)0.0) {
+      af = a2; pf = p2;
+      if (vel <= un1) {
+        if (swl > (R)0.0) { af = al; vel = un1; pf = pl; }
+      } else if (vw1 > (R)0.0) {
+        vel = un1; af = al; pf = pl;
+      } else if (vw2 > (R)0.0) {
+        af = (un1 + al / d1) / ((R)1.0 + (R)1.0 / d1);
+        vel = af;
+        pf = pl * powr(af / al, e1);
+      }
+      rhof = gam_L * pf / (af * af);
+      uf = vel * nx + ut1; vf = vel * ny + vt1; wf = vel * nz + wt1;
+      Hs = h_static(p, dl / dltot * rhof, pf);
+    } else {
+      af = a3; pf = p3;
+      if (vel >= un4) {
+        if (swr < (R)0.0) { af = ar; vel = un4; pf = pr; }
+      } else if (vw4 < (R)0.0) {
+        af = ar; vel = un4; pf = pr;
+      } else if (vw3 < (R)0.0) {
+        af = -(un4 - ar / d4) / ((R)1.0 + (R)1.0 / d4);
+        vel = -af;
+        pf = pr * powr(af / ar, e4);
+      }
+      rhof = gam_R * pf / (af * af);
+      uf = vel * nx + ut4; vf = vel * ny + vt4; wf = vel * nz + wt4;
+      Hs = h_static(p, dr / drtot * rhof, pf);
+    }
+    F_r = rhof * vel;
+    F_u = F_r * uf + pf * nx;
+    F_v = F_r * vf + pf * ny;
+    F_w = F_r * wf + pf * nz;
+    R uu = rsqrt_(vel * vel);
+    F_E = F_r * (Hs + (R)0.5 * uu * uu);
+    return;
+  }
+  if (rs == 13) {  // MiczekRoe (riemann_open_body.inc:518-676): the Miczek et al. 2015 preconditioned Roe flux
+    R nmag = rsqrt_(nx * nx + ny * ny + nz * nz);
+    if (nmag <= (R)0.0) { F_r = (R)0.0; F_u = (R)0.0; F_v = (R)0.0; F_w = (R)0.0; F_E = (R)0.0; return; }
+    R n1 = nx / nmag, n2 = ny / nmag, n3 = nz / nmag;
+    R tx = (R)1.0, ty = (R)0.0, tz = (R)0.0;
+    if (!(fabs(n1) < (R)0.9)) { tx = (R)0.0; ty = (R)1.0; }
+    R dot = tx * n1 + ty * n2 + tz * n3;
+    R t1x = tx - dot * n1, t1y = ty - dot * n2, t1z = tz - dot * n3;
+    R tmag = rsqrt_(t1x * t1x + t1y * t1y + t1z * t1z);
+    if (tmag <= (R)0.0) {
+      t1x = -n2; t1y = n1; t1z = (R)0.0;
+      tmag = rsqrt_(t1x * t1x + t1y * t1y + t1z * t1z);
+    }
+    t1x = t1x / tmag; t1y = t1y / tmag; t1z = t1z / tmag;
+    R t2x = n2 * t1z - n3 * t1y, t2y = n3 * t1x - n1 * t1z, t2z = n1 * t1y - n2 * t1x;
+    R unL = ul * n1 + vl * n2 + wl * n3, unR = ur * n1 + vr * n2 + wr * n3;
+    R ut1L = ul * t1x + vl * t1y + wl * t1z, ut1R = ur * t1x + vr * t1y + wr * t1z;
+    R ut2L = ul * t2x + vl * t2y + wl * t2z, ut2R = ur * t2x + vr * t2y + wr * t2z;
+    R hL = h_static(p, dl, pl), hR = h_static(p, dr, pr);
+    R H0L = hL + (R)0.5 * (ul * ul + vl * vl + wl * wl);
+    R H0R = hR + (R)0.5 * (ur * ur + vr * vr + wr * wr);
+    R FL1 = dltot * unL, FL2 = dltot * unL * ul + pl * n1, FL3 = dltot * unL * vl + pl * n2,
+           FL4 = dltot * unL * wl + pl * n3, FL5 = dltot * unL * H0L;
+    R FR1 = drtot * unR, FR2 = drtot * unR * ur + pr * n1, FR3 = drtot * unR * vr + pr * n2,
+           FR4 = drtot * unR * wr + pr * n3, FR5 = drtot * unR * H0R;
+    R sRL = rsqrt_(dltot), sRR = rsqrt_(drtot), den = sRL + sRR;
+    R u = (sRL * ul + sRR * ur) / den, v = (sRL * vl + sRR * vr) / den, w = (sRL * wl + sRR * wr) / den;
+    R H = (sRL * H0L + sRR * H0R) / den;
+    R un = u * n1 + v * n2 + w * n3;
+    R rho = sRL * sRR;
+    R u2 = u * u + v * v + w * w;
+    R gam_L = gam_state(p, dl, pl, dltot), gam_R = gam_state(p, dr, pr, drtot);
+    R kL = gam_L - (R)1.0, kR = gam_R - (R)1.0;
+    R chiL = al * al - kL * hL, chiR = ar * ar - kR * hR;
+    R kRoe = (sRL * kL + sRR * kR) / den, chiRoe = (sRL * chiL + sRR * chiR) / den;
+    R cc = rsqrt_(mx((R)1e-30, chiRoe + kRoe * (H - (R)0.5 * u2)));
+    R Mcut = mx((R)1e-6, (R)p.mco);
+    R Mloc = rsqrt_(u2) / cc;
+    R mu = mn((R)1.0, mx(Mloc, Mcut));
+    R del = (R)1.0 / mu - (R)1.0, del2 = del * del, om = (R)1.0 / ((R)1.0 + del2);
+    R drho = drtot - dltot, dp = pr - pl, dun = unR - unL, dut1 = ut1R - ut1L, dut2 = ut2R - ut2L;
+    R p11 = un, p12 = rho * ((R)1.0 + del * un / cc), p13 = del / cc, p22 = un - del * cc;
+    R p23 = ((R)1.0 - del * un / cc) / rho, p32 = rho * cc * (cc + del * un), p33 = un + cc * del;
+    R s2 = ((R)1.0 + del2) * cc * cc - del2 * un * un;
+    R s = rsqrt_(mx((R)1e-30, s2));
+    s2 = s * s;
+    R le = un, lp = un + s, lm = un - s;
+    R va1 = (p11 - lm) * drho + p12 * dun + p13 * dp, va2 = (p22 - lm) * dun + p23 * dp,
+           va3 = p32 * dun + (p33 - lm) * dp;
+    R vb1 = (p11 - lp) * drho + p12 * dun + p13 * dp, vb2 = (p22 - lp) * dun + p23 * dp,
+           vb3 = p32 * dun + (p33 - lp) * dp;
+    R w1 = (p11 - lp) * va1 + p12 * va2 + p13 * va3, w2 = (p22 - lp) * va2 + p23 * va3,
+           w3 = p32 * va2 + (p33 - lp) * va3;
+    R x1 = (p11 - le) * va1 + p12 * va2 + p13 * va3, x2 = (p22 - le) * va2 + p23 * va3,
+           x3 = p32 * va2 + (p33 - le) * va3;
+    R z1 = (p11 - le) * vb1 + p12 * vb2 + p13 * vb3, z2 = (p22 - le) * vb2 + p23 * vb3,
+           z3 = p32 * vb2 + (p33 - le) * vb3;
+    R c1 = fabs(le) / (-s2), c2 = fabs(lp) / ((R)2.0 * s2), c3 = fabs(lm) / ((R)2.0 * s2);
+    R g1 = c1 * w1 + c2 * x1 + c3 * z1, g2 = c1 * w2 + c2 * x2 + c3 * z2, g3 = c1 * w3 + c2 * x3 + c3 * z3;
+    R ddrho = g1 - (rho * del / cc) * om * g2 - (del2 / (cc * cc)) * om * g3;
+    R ddun = om * (g2 + (del / (rho * cc)) * g3);
+    R ddp = om * (-rho * cc * del * g2 + g3);
+    R ddut1 = fabs(un) * dut1, ddut2 = fabs(un) * dut2;
+    R ddux = ddun * n1 + ddut1 * t1x + ddut2 * t2x;
+    R dduy = ddun * n2 + ddut1 * t1y + ddut2 * t2y;
+    R dduz = ddun * n3 + ddut1 * t1z + ddut2 * t2z;
+    F_r = (R)0.5 * (FL1 + FR1) - (R)0.5 * (ddrho);
+    F_u = (R)0.5 * (FL2 + FR2) - (R)0.5 * (u * ddrho + rho * ddux);
+    F_v = (R)0.5 * (FL3 + FR3) - (R)0.5 * (v * ddrho + rho * dduy);
+    F_w = (R)0.5 * (FL4 + FR4) - (R)0.5 * (w * ddrho + rho * dduz);
+    F_E = (R)0.5 * (FL5 + FR5) - (R)0.5 * ((R)0.5 * u2 * ddrho + rho * (u * ddux + v * dduy + w * dduz) + ddp / kRoe);
     return;
   }
   if (rs == 8) {  // LLF / Rusanov (riemann_open_body.inc:244-278)

@@ -1,5 +1,5 @@
 // Fused sweep of the FP64 form, the Riemann solver id read at run time (HLLE, SLAU, LLF,
-// SLAU2: the solvers of no benchmarked case).
+// SLAU2, exact, MiczekRoe: the solvers of no benchmarked case).
 #define MB_R double
 #define MB_RS 0
 #define MB_TY TY_F64

@@ -41,6 +41,7 @@ BC_OUTLET = 24      # q = (exit pressure, relaxation factor)
 
 LIM_MINMOD, LIM_VANLEER, LIM_VANALBADA, LIM_MC, LIM_SUPERBEE, LIM_FIRST = 1, 2, 3, 4, 5, 6
 RS_HLLC, RS_HLLE, RS_SLAU, RS_AUSMP, RS_LLF, RS_SLAU2, RS_LMROE = 1, 2, 3, 4, 8, 9, 12
+RS_EXACT, RS_MICZEKROE = 11, 13
 PREC_FP64, PREC_MIXED = 0, 1
 
 

@@ -14,7 +14,8 @@
 //   convective face         src/lib/gpu/conv_physics.inc:1-179, Mod_Convective.f90:288-412
 //   limiter                 src/lib/numerics/space/Lib_Limiters.f90:65-97 (Mod_Convective.f90:161-191)
 //   AUSM+, LMRoe            src/lib/numerics/fluxes/riemann_open_body.inc:100-150, 679-730, 965-1091
-//   LLF, SLAU2              src/lib/numerics/fluxes/riemann_open_body.inc:244-347
+//   LLF, SLAU2, exact,      src/lib/numerics/fluxes/riemann_open_body.inc:244-347, 348-516, 518-676
+//   MiczekRoe
 //   HLLC, HLLE at records   src/lib/numerics/fluxes/Lib_Riemann_HLL.f90:21-198, 209-310
 //   HLLE, SLAU interior     src/lib/gpu/conv_physics.inc:116-159
 //   SLAU at records         src/lib/numerics/fluxes/Lib_Riemann.f90:138-197
@@ -259,6 +260,19 @@ inline double h_static(const Thermo& th, double rhoi, double p) {
   return 0.0 + hs * rhoi / rho_;
 }
 
+// gamma of a state as riemann_open_body.inc writes f_gamma out (:349-366): T from p / (R rho_tot), the table row
+// int(T) with both rows held to the table
+inline double gam_state(const Thermo& th, double d, double p, double dtot) {
+  double rho_ = 0.0 + d;
+  double rg_ = 0.0 + th.ri * d / rho_;
+  double T_ = p / (rg_ * dtot);
+  int Ti = (int)T_;
+  double Td = T_ - Ti;
+  int t1 = std::max(th.tmin, std::min(Ti, th.tmax)), t2 = std::max(th.tmin, std::min(Ti + 1, th.tmax));
+  double cp_ = 0.0 + d / dtot * (th.cp[t1] + (th.cp[t2] - th.cp[t1]) * Td);
+  return cp_ / (cp_ - rg_);
+}
+
 void riemann_open(const Thermo& th, int rs, double mco, double dl, double ul, double vl, double wl,
                   double pl, double al, double dltot, double dr, double ur, double vr, double wr, double pr,
                   double ar, double drtot, double nx, double ny, double nz, double& F_r, double& F_u,
@@ -297,6 +311,174 @@ void riemann_open(const Thermo& th, int rs, double mco, double dl, double ul, do
     F_v = mdotp * vl + mdotm * vr + ny * phalf;
     F_w = mdotp * wl + mdotm * wr + nz * phalf;
     F_E = mdotp * H_L + mdotm * H_R;
+    return;
+  }
+  if (rs == 11) {  // exact Godunov (riemann_open_body.inc:348-516): Newton on the star velocity, gamma of each state
+    double gam_L = gam_state(th, dl, pl, dltot), gam_R = gam_state(th, dr, pr, drtot);
+    double gm1 = gam_L - 1.0, gm4 = gam_R - 1.0;
+    double d1 = 0.5 * gm1, d4 = 0.5 * gm4;
+    double e1 = gam_L / d1, e4 = gam_R / d4;
+    double un1 = ul * nx + vl * ny + wl * nz;
+    double ut1 = ul - un1 * nx, vt1 = vl - un1 * ny, wt1 = wl - un1 * nz;
+    double un4 = ur * nx + vr * ny + wr * nz;
+    double ut4 = ur - un4 * nx, vt4 = vr - un4 * ny, wt4 = wr - un4 * nz;
+    double r2i = un1 + (2.0 / gm1) * al;
+    double r1iv = un4 - (2.0 / gm4) * ar;
+    double dum = (pl < pr) ? gm4 / (2.0 * gam_R) : gm1 / (2.0 * gam_L);
+    double z = (gm1 / gm4) * (ar / al) * std::pow(pl / pr, dum);
+    double vel = (z * r2i + r1iv) / (1.0 + z);
+    double p3 = 1.0, p2 = 2.0 * p3, dpr = 0.0, dpl = 0.0;
+    int iter = 0;
+    double swl = 0.0, swr = 0.0, vw1 = 0.0, vw2 = 0.0, vw3 = 0.0, vw4 = 0.0, a2 = al, a3 = ar;
+    while (std::fabs(1.0 - (p2 / p3)) >= 1e-5 && iter <= 1000) {
+      if (vel < un1) {  // shock on the left
+        double x = (gam_L + 1.0) * (vel - un1) / (4.0 * al);
+        double mrel = x - std::sqrt(1.0 + x * x);
+        double c = gam_L * pl / al;
+        p2 = pl + c * (vel - un1) * mrel;
+        dpr = 2.0 * c * std::pow(mrel, 3.0) / (1.0 + mrel * mrel);
+        double rp = p2 / pl;
+        swl = un1 + al * mrel;
+        a2 = al * std::sqrt((gam_L + 1.0 + (gam_L - 1.0) * rp) / (gam_L + 1.0 + (gam_L - 1.0) / rp));
+      } else {  // rarefaction on the left
+        double delta = 0.5 * (gam_L - 1.0);
+        double dum1 = 2.0 * gam_L / (gam_L - 1.0);
+        a2 = al - delta * (vel - un1);
+        p2 = pl * std::pow(a2 / al, dum1);
+        dpr = -gam_L * p2 / a2;
+        vw1 = un1 - al;
+        vw2 = vel - a2;
+      }
+      if (vel > un4) {  // shock on the right
+        double x = (gam_R + 1.0) * (vel - un4) / (4.0 * ar);
+        double mrel = x + std::sqrt(1.0 + x * x);
+        double c = gam_R * pr / ar;
+        p3 = pr + c * (vel - un4) * mrel;
+        dpl = 2.0 * c * std::pow(mrel, 3.0) / (1.0 + mrel * mrel);
+        double rp = p3 / pr;
+        swr = un4 + ar * mrel;
+        a3 = ar * std::sqrt((gam_R + 1.0 + (gam_R - 1.0) * rp) / (gam_R + 1.0 + (gam_R - 1.0) / rp));
+      } else {  // rarefaction on the right
+        double delta = 0.5 * (gam_R - 1.0);
+        double dum1 = 2.0 * gam_R / (gam_R - 1.0);
+        a3 = ar + delta * (vel - un4);
+        p3 = pr * std::pow(a3 / ar, dum1);
+        dpl = gam_R * p3 / a3;
+        vw3 = vel + a3;
+        vw4 = un4 + ar;
+      }
+      vel = vel - ((p2 - p3) / (dpr - dpl));
+      iter = iter + 1;
+    }
+    double af, pf, rhof, uf, vf, wf, Hs;
+    if (vel > 0.0) {
+      af = a2; pf = p2;
+      if (vel <= un1) {
+        if (swl > 0.0) { af = al; vel = un1; pf = pl; }
+      } else if (vw1 > 0.0) {
+        vel = un1; af = al; pf = pl;
+      } else if (vw2 > 0.0) {
+        af = (un1 + al / d1) / (1.0 + 1.0 / d1);
+        vel = af;
+        pf = pl * std::pow(af / al, e1);
+      }
+      rhof = gam_L * pf / (af * af);
+      uf = vel * nx + ut1; vf = vel * ny + vt1; wf = vel * nz + wt1;
+      Hs = h_static(th, dl / dltot * rhof, pf);
+    } else {
+      af = a3; pf = p3;
+      if (vel >= un4) {
+        if (swr < 0.0) { af = ar; vel = un4; pf = pr; }
+      } else if (vw4 < 0.0) {
+        af = ar; vel = un4; pf = pr;
+      } else if (vw3 < 0.0) {
+        af = -(un4 - ar / d4) / (1.0 + 1.0 / d4);
+        vel = -af;
+        pf = pr * std::pow(af / ar, e4);
+      }
+      rhof = gam_R * pf / (af * af);
+      uf = vel * nx + ut4; vf = vel * ny + vt4; wf = vel * nz + wt4;
+      Hs = h_static(th, dr / drtot * rhof, pf);
+    }
+    F_r = rhof * vel;
+    F_u = F_r * uf + pf * nx;
+    F_v = F_r * vf + pf * ny;
+    F_w = F_r * wf + pf * nz;
+    double uu = std::sqrt(vel * vel);
+    F_E = F_r * (Hs + 0.5 * uu * uu);
+    return;
+  }
+  if (rs == 13) {  // MiczekRoe (riemann_open_body.inc:518-676): the Miczek et al. 2015 preconditioned Roe flux
+    double nmag = std::sqrt(nx * nx + ny * ny + nz * nz);
+    if (nmag <= 0.0) { F_r = 0.0; F_u = 0.0; F_v = 0.0; F_w = 0.0; F_E = 0.0; return; }
+    double n1 = nx / nmag, n2 = ny / nmag, n3 = nz / nmag;
+    double tx = 1.0, ty = 0.0, tz = 0.0;
+    if (!(std::fabs(n1) < 0.9)) { tx = 0.0; ty = 1.0; }
+    double dot = tx * n1 + ty * n2 + tz * n3;
+    double t1x = tx - dot * n1, t1y = ty - dot * n2, t1z = tz - dot * n3;
+    double tmag = std::sqrt(t1x * t1x + t1y * t1y + t1z * t1z);
+    if (tmag <= 0.0) {
+      t1x = -n2; t1y = n1; t1z = 0.0;
+      tmag = std::sqrt(t1x * t1x + t1y * t1y + t1z * t1z);
+    }
+    t1x = t1x / tmag; t1y = t1y / tmag; t1z = t1z / tmag;
+    double t2x = n2 * t1z - n3 * t1y, t2y = n3 * t1x - n1 * t1z, t2z = n1 * t1y - n2 * t1x;
+    double unL = ul * n1 + vl * n2 + wl * n3, unR = ur * n1 + vr * n2 + wr * n3;
+    double ut1L = ul * t1x + vl * t1y + wl * t1z, ut1R = ur * t1x + vr * t1y + wr * t1z;
+    double ut2L = ul * t2x + vl * t2y + wl * t2z, ut2R = ur * t2x + vr * t2y + wr * t2z;
+    double hL = h_static(th, dl, pl), hR = h_static(th, dr, pr);
+    double H0L = hL + 0.5 * (ul * ul + vl * vl + wl * wl);
+    double H0R = hR + 0.5 * (ur * ur + vr * vr + wr * wr);
+    double FL1 = dltot * unL, FL2 = dltot * unL * ul + pl * n1, FL3 = dltot * unL * vl + pl * n2,
+           FL4 = dltot * unL * wl + pl * n3, FL5 = dltot * unL * H0L;
+    double FR1 = drtot * unR, FR2 = drtot * unR * ur + pr * n1, FR3 = drtot * unR * vr + pr * n2,
+           FR4 = drtot * unR * wr + pr * n3, FR5 = drtot * unR * H0R;
+    double sRL = std::sqrt(dltot), sRR = std::sqrt(drtot), den = sRL + sRR;
+    double u = (sRL * ul + sRR * ur) / den, v = (sRL * vl + sRR * vr) / den, w = (sRL * wl + sRR * wr) / den;
+    double H = (sRL * H0L + sRR * H0R) / den;
+    double un = u * n1 + v * n2 + w * n3;
+    double rho = sRL * sRR;
+    double u2 = u * u + v * v + w * w;
+    double gam_L = gam_state(th, dl, pl, dltot), gam_R = gam_state(th, dr, pr, drtot);
+    double kL = gam_L - 1.0, kR = gam_R - 1.0;
+    double chiL = al * al - kL * hL, chiR = ar * ar - kR * hR;
+    double kRoe = (sRL * kL + sRR * kR) / den, chiRoe = (sRL * chiL + sRR * chiR) / den;
+    double cc = std::sqrt(std::max(1e-30, chiRoe + kRoe * (H - 0.5 * u2)));
+    double Mcut = std::max(1e-6, mco);
+    double Mloc = std::sqrt(u2) / cc;
+    double mu = std::min(1.0, std::max(Mloc, Mcut));
+    double del = 1.0 / mu - 1.0, del2 = del * del, om = 1.0 / (1.0 + del2);
+    double drho = drtot - dltot, dp = pr - pl, dun = unR - unL, dut1 = ut1R - ut1L, dut2 = ut2R - ut2L;
+    double p11 = un, p12 = rho * (1.0 + del * un / cc), p13 = del / cc, p22 = un - del * cc;
+    double p23 = (1.0 - del * un / cc) / rho, p32 = rho * cc * (cc + del * un), p33 = un + cc * del;
+    double s2 = (1.0 + del2) * cc * cc - del2 * un * un;
+    double s = std::sqrt(std::max(1e-30, s2));
+    s2 = s * s;
+    double le = un, lp = un + s, lm = un - s;
+    double va1 = (p11 - lm) * drho + p12 * dun + p13 * dp, va2 = (p22 - lm) * dun + p23 * dp,
+           va3 = p32 * dun + (p33 - lm) * dp;
+    double vb1 = (p11 - lp) * drho + p12 * dun + p13 * dp, vb2 = (p22 - lp) * dun + p23 * dp,
+           vb3 = p32 * dun + (p33 - lp) * dp;
+    double w1 = (p11 - lp) * va1 + p12 * va2 + p13 * va3, w2 = (p22 - lp) * va2 + p23 * va3,
+           w3 = p32 * va2 + (p33 - lp) * va3;
+    double x1 = (p11 - le) * va1 + p12 * va2 + p13 * va3, x2 = (p22 - le) * va2 + p23 * va3,
+           x3 = p32 * va2 + (p33 - le) * va3;
+    double z1 = (p11 - le) * vb1 + p12 * vb2 + p13 * vb3, z2 = (p22 - le) * vb2 + p23 * vb3,
+           z3 = p32 * vb2 + (p33 - le) * vb3;
+    double c1 = std::fabs(le) / (-s2), c2 = std::fabs(lp) / (2.0 * s2), c3 = std::fabs(lm) / (2.0 * s2);
+    double g1 = c1 * w1 + c2 * x1 + c3 * z1, g2 = c1 * w2 + c2 * x2 + c3 * z2, g3 = c1 * w3 + c2 * x3 + c3 * z3;
+    double ddrho = g1 - (rho * del / cc) * om * g2 - (del2 / (cc * cc)) * om * g3;
+    double ddun = om * (g2 + (del / (rho * cc)) * g3);
+    double ddp = om * (-rho * cc * del * g2 + g3);
+    double ddut1 = std::fabs(un) * dut1, ddut2 = std::fabs(un) * dut2;
+    double ddux = ddun * n1 + ddut1 * t1x + ddut2 * t2x;
+    double dduy = ddun * n2 + ddut1 * t1y + ddut2 * t2y;
+    double dduz = ddun * n3 + ddut1 * t1z + ddut2 * t2z;
+    F_r = 0.5 * (FL1 + FR1) - 0.5 * (ddrho);
+    F_u = 0.5 * (FL2 + FR2) - 0.5 * (u * ddrho + rho * ddux);
+    F_v = 0.5 * (FL3 + FR3) - 0.5 * (v * ddrho + rho * dduy);
+    F_w = 0.5 * (FL4 + FR4) - 0.5 * (w * ddrho + rho * dduz);
+    F_E = 0.5 * (FL5 + FR5) - 0.5 * (0.5 * u2 * ddrho + rho * (u * ddux + v * dduy + w * dduz) + ddp / kRoe);
     return;
   }
   if (rs == 8) {  // LLF / Rusanov (riemann_open_body.inc:244-278)
@@ -1745,7 +1927,7 @@ struct orc_ctx { Ctx c; };
 int orc_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, orc_ctx** out) {
   if (!mesh || !sc || !th || !out) return MB_E_ARG;
   if (sc->riemann != 1 && sc->riemann != 2 && sc->riemann != 3 && sc->riemann != 4 && sc->riemann != 8 &&
-      sc->riemann != 9 && sc->riemann != 12)
+      sc->riemann != 9 && sc->riemann != 11 && sc->riemann != 12 && sc->riemann != 13)
     return MB_E_UNSUPPORTED;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
   if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;

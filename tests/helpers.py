@@ -57,6 +57,12 @@ def reversed_records(case):
     return case
 
 
+def with_scheme(case, **kw):
+    """The case with scheme entries replaced (e.g. mco)."""
+    case.scheme.update(kw)
+    return case
+
+
 def small_cases():
     """(id, builder) of the parity cases: every boundary type, Riemann solver and limiter served."""
     return [
@@ -90,6 +96,13 @@ def small_cases():
                                                          limiter=abi.LIM_MINMOD)),
         ("mb2d_hlle_mc_euler", lambda: cs.multiblock_2d(cols=2, rows=2, lo=5, hi=10, seed=4, riemann=abi.RS_HLLE,
                                                         limiter=abi.LIM_MC, visc=0)),
+        # the exact Godunov solver (Newton on the star state) and MiczekRoe (preconditioned below Mco)
+        ("sod_exact_minmod", lambda: cs.riemann_1d(n=64, riemann=abi.RS_EXACT)),
+        ("quad2d_exact_vanleer", lambda: cs.riemann_2d(n=20, riemann=abi.RS_EXACT, limiter=abi.LIM_VANLEER)),
+        ("mb2d_exact_minmod_rk3", lambda: cs.multiblock_2d(cols=2, rows=2, lo=5, hi=9, seed=21, riemann=abi.RS_EXACT,
+                                                           limiter=abi.LIM_MINMOD, n_rk=3)),
+        ("tgv_miczek_mco02", lambda: with_scheme(cs.taylor_green(n=12, riemann=abi.RS_MICZEKROE), mco=0.2)),
+        ("duct3d_miczek_mco03", lambda: with_scheme(cs.duct_3d(riemann=abi.RS_MICZEKROE), mco=0.3)),
         # symmetry (300), isothermal walls (302) and the back-pressure outlet (406)
         ("duct3d_hllc_vanleer", lambda: cs.duct_3d()),
         ("duct3d_roe_vanalbada_rk4", lambda: cs.duct_3d(widths=(5, 6), heights=(4, 3), depths=(4,),

@@ -58,7 +58,7 @@ def test_init_rejects_bad_arguments_without_a_device():
     mesh.nblk = 1
     mesh.ncell_total = 10
     sc = abi.MBScheme()
-    sc.riemann = 11   # the exact Godunov solver: not served
+    sc.riemann = 14   # HLLC-PC (preconditioned integration variables): not served
     sc.limiter = 1
     sc.n_rk = 3
     sc.ndir = 3

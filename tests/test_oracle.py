@@ -23,7 +23,8 @@ def test_exact_riemann_star_state():
     assert abs(r[0] - 0.42632) < 5e-5 and abs(r[1] - 0.26557) < 5e-5
 
 
-ALL_RS = [abi.RS_HLLC, abi.RS_HLLE, abi.RS_SLAU, abi.RS_AUSMP, abi.RS_LLF, abi.RS_SLAU2, abi.RS_LMROE]
+ALL_RS = [abi.RS_HLLC, abi.RS_HLLE, abi.RS_SLAU, abi.RS_AUSMP, abi.RS_LLF, abi.RS_SLAU2, abi.RS_EXACT, abi.RS_LMROE,
+          abi.RS_MICZEKROE]
 
 
 @pytest.mark.parametrize("riemann", ALL_RS)
