@@ -580,7 +580,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   p.ngroups = ngroups;
   p.nc = c->ncell;
   p.tmin = th->tmin; p.tmax = th->tmax;
-  p.wm = th->wm; p.ri = RUNIV / th->wm;
+  p.wm = th->wm; p.ri = RUNIV / th->wm; p.iri = th->wm / RUNIV;
   p.lim = sc->limiter; p.rs = sc->riemann; p.visc = sc->visc ? 1 : 0; p.ndir = sc->ndir; p.dt_additive = sc->dt_additive;
   p.guard = sc->visc ? 1 : 0; p.state_check = sc->state_check;
   p.cfl = sc->cfl; p.vnn = sc->vnn; p.prandtl = sc->prandtl; p.schmidt = sc->schmidt; p.mco = sc->mco;

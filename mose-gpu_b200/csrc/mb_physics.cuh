@@ -101,6 +101,7 @@ struct Params {
   long long nc;
   int tmin, tmax;
   double wm, ri;
+  double iri;              // 1 / ri (the mixed form's state update multiplies by it)
   int lim, rs, visc, ndir, dt_additive, guard, state_check;
   double cfl, vnn, prandtl, schmidt, mco;
   void* recflux;           // boundary-record contributions [record][10] in the flux type (k_records)
