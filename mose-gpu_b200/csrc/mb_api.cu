@@ -31,7 +31,6 @@ struct mb_ctx {
   long long* d_cdst = nullptr;
   long long* d_csrc = nullptr;
   long long* d_pgsrc = nullptr;
-  double* d_pg = nullptr;
   double* d_recflux = nullptr;  // boundary-record contributions [nrec][10] (flux type)
   int* d_brec = nullptr;        // records in type order (the record kernel's work list)
   int* d_bcell = nullptr;       // their blk, i, j, k, face
@@ -91,7 +90,7 @@ static void free_ctx(mb_ctx* c) {
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   if (c->graph) cudaGraphDestroy(c->graph);
   void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
-                  c->d_pgsrc, c->d_pg, c->d_tab, c->d_tabf, c->d_st, c->d_tiles_sweep, c->d_tiles_aux, c->d_scratch, c->d_acc4, c->d_queue, c->d_recflux, c->d_brec, c->d_bcell,
+                  c->d_pgsrc, c->d_tab, c->d_tabf, c->d_st, c->d_tiles_sweep, c->d_tiles_aux, c->d_scratch, c->d_acc4, c->d_queue, c->d_recflux, c->d_brec, c->d_bcell,
                   c->d_physf, c->d_cubicf, c->d_tiles_km};
   for (void* q : ptrs)
     if (q) cudaFree(q);
@@ -187,14 +186,14 @@ static int check_mesh(const mb_mesh* mesh, int ngroups) {
 // frees the mesh-dependent device tables (blocks, record maps, records, ghost lists, tiles, FP32 geometry)
 static void free_tables(mb_ctx* c) {
   void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
-                  c->d_pgsrc, c->d_pg, c->d_tiles_sweep, c->d_tiles_aux, c->d_recflux, c->d_brec, c->d_bcell,
+                  c->d_pgsrc, c->d_tiles_sweep, c->d_tiles_aux, c->d_recflux, c->d_brec, c->d_bcell,
                   c->d_physf, c->d_cubicf, c->d_tiles_km};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   c->d_physf = nullptr; c->d_cubicf = nullptr; c->d_tiles_km = nullptr; c->ntiles_km = 0;
   c->d_recflux = nullptr; c->d_brec = nullptr; c->d_bcell = nullptr; c->nrec = 0;
   c->d_blk = nullptr; c->d_recmap = nullptr; c->d_rec = nullptr; c->d_grec = nullptr; c->d_phys = nullptr;
-  c->d_cubic = nullptr; c->d_cdst = nullptr; c->d_csrc = nullptr; c->d_pgsrc = nullptr; c->d_pg = nullptr;
+  c->d_cubic = nullptr; c->d_cdst = nullptr; c->d_csrc = nullptr; c->d_pgsrc = nullptr;
   c->d_tiles_sweep = nullptr; c->d_tiles_aux = nullptr;
 }
 
@@ -475,15 +474,12 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
     return MB_E_NOMEM;
   c->ntiles_sweep = (int)ts.size();
   c->ntiles_aux = (int)ta.size();
-  if (mesh->nconn > 0 && cudaMalloc((void**)&c->d_pg, (size_t)mesh->nconn * 6 * MB_NPRIM * sizeof(double)) != cudaSuccess)
-    return MB_E_NOMEM;
   Params& p = c->p;
-  p.blk = c->d_blk; p.rec_map = c->d_recmap; p.rec = c->d_rec; p.pg = c->d_pg;
+  p.blk = c->d_blk; p.rec_map = c->d_recmap; p.rec = c->d_rec; p.pgsrc = c->d_pgsrc;
   p.recflux = c->d_recflux;
   GhostLists& g = c->g;
   g.rec = c->d_grec; g.phys = c->d_phys; g.nphys = (int)phys.size(); g.cubic = c->d_cubic; g.ncubic = (int)cubic.size();
   g.cdst = c->d_cdst; g.csrc = c->d_csrc; g.ncopy = (int)cdst.size(); g.pgsrc = c->d_pgsrc; g.nconn = mesh->nconn;
-  g.pg = c->d_pg;
   g.ordered = ordered;
   for (int f = 0; f < 3; ++f) { g.phys_off[f] = po[f]; g.cubic_off[f] = co[f]; }
   c->gf = g;

@@ -209,10 +209,13 @@ MB_HD void bc_conn_eul(const Params& p, const DBlk& b, const double* __restrict_
   A[MB_IPR] = sg * F_E * area;
 }
 
-// BC_Connection_Visc_lean (Lib_BC.f90:2113-2178); pg = bc_pg(:,1:6) of the record
+// BC_Connection_Visc_lean (Lib_BC.f90:2113-2178). The reference reads bc_pg(:,1:6), a copy of six donor cells taken
+// after the ghost fill (Ghost_Connection_pairs_B, Lib_Extrapolation.f90:1136-1191); the records run on the same
+// filled state, so this reads those cells of P in place: pgr = the six donor rows of the record (the same values,
+// without the copy pass and its nconn x 30 FP64 buffer).
 template <typename R>
 MB_HD void bc_conn_visc(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm,
-                                          int Km, int Fm, const double* __restrict__ pg, R* S) {
+                                          int Km, int Fm, const long long* __restrict__ pgr, R* S) {
   const long long nc = p.nc;
   int dir = (Fm + 1) / 2, modfm2 = 1 - 2 * (Fm % 2), gstep = 2 * (Fm % 2) - 1;
   int ia = dir - 1, ib, ic;
@@ -234,8 +237,8 @@ MB_HD void bc_conn_visc(const Params& p, const DBlk& b, const double* __restrict
   const long long scm = (b.kmirror && ic == 2) ? 0 : sc;  // a mirrored block's k ghosts are its k = 1 cells
   const long long rc[6] = {r1, 0, r1 + sb, r1 - sb, r1 + scm, r1 - scm};
   auto pv = [&](int q, int s) -> R {
-    if (q == 1) return cvt<R>(ld(pg + s));
-    if (q >= 6) return cvt<R>(ld(pg + s + MB_NP * (q - 4)));
+    if (q == 1) return cvt<R>(ld(P + pgr[0] + s * nc));
+    if (q >= 6) return cvt<R>(ld(P + pgr[q - 4] + s * nc));
     return cvt<R>(ld(P + rc[q] + s * nc));
   };
   R rh[10], rg[10];
@@ -725,7 +728,7 @@ MB_HD void bc_record(const Params& p, const DBlk& b, const double* __restrict__ 
     for (int s = 0; s < MB_NP; ++s) S[s] = (R)0;
   if (rc.type == 1) {
     bc_conn_eul<R, RS, LIM>(p, b, P, i, j, k, F, A);
-    if (VISC) bc_conn_visc<R>(p, b, P, i, j, k, F, p.pg + (long long)rc.pg * 6 * MB_NP, S);
+    if (VISC) bc_conn_visc<R>(p, b, P, i, j, k, F, p.pgsrc + (long long)rc.pg * 6, S);
   } else if (rc.type == 11) {
     bc_extrap<R>(p, b, P, i, j, k, F, A);
   } else if (rc.type == 5) {

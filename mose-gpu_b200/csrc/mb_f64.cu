@@ -75,15 +75,6 @@ __global__ void k_ghost_copy(const long long* __restrict__ dst, const long long*
   P[dst[e] + s * nc] = P[src[e] + s * nc];
 }
 
-// bc_pg(:,1:6) of every connection after all ghosts are written (Ghost_Connection_pairs_B, :1136-1191)
-__global__ void k_pg(const long long* __restrict__ src, int nconn, long long nc, const double* __restrict__ P,
-                     double* pg) {
-  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= (long long)nconn * 6 * MB_NP) return;
-  const long long e = q / MB_NP;  // (conn, slot)
-  const int s = (int)(q - e * MB_NP);
-  pg[q] = P[src[e] + s * nc];
-}
 
 // ---- Compute_dt alone: k_dt_t<double> of mb_engine.cuh ----
 
@@ -192,10 +183,6 @@ cudaError_t ghost_fill(const Params& p, const GhostLists& g, double* P, cudaStre
   }
   if (g.ncopy > 0) {
     k_ghost_copy<<<nblk_for((long long)g.ncopy * MB_NP, 256), 256, 0, s>>>(g.cdst, g.csrc, g.ncopy, p.nc, P);
-    ++*nl;
-  }
-  if (g.nconn > 0 && p.visc) {
-    k_pg<<<nblk_for((long long)g.nconn * 6 * MB_NP, 256), 256, 0, s>>>(g.pgsrc, g.nconn, p.nc, P, g.pg);
     ++*nl;
   }
   return cudaGetLastError();

@@ -24,7 +24,6 @@ struct GhostLists {
   int ncopy;
   const long long* pgsrc; // [nconn][6] source rows of bc_pg
   int nconn;
-  double* pg;             // [nconn][6][5]
   // ordered != 0: the phys and cubic lists are split in two halves, off[0]..off[1] and off[1]..off[2], the second
   // holding the records whose opposite-face partner on the same column comes earlier in record order; each pass then
   // runs as two launches (only on blocks with an axis of at most two cells does the order change values)

@@ -93,7 +93,7 @@ struct Params {
   const DBlk* blk;
   const int* rec_map;
   const DRec* rec;
-  const double* pg;        // [record][6][5]
+  const long long* pgsrc;  // [connection][6]: the rows of P that bc_pg(:,1:6) of the connection record copies
   const double *cp, *h, *mu, *k;      // FP64 tables, indexed by the table row (pointer shifted by -tmin)
   const float *cpf, *hf, *muf, *kf;   // FP32 copies for the mixed form
   DevState* st;            // one clock per case: st[DBlk::grp]
