@@ -72,7 +72,7 @@ extern "C" {
 #define MB_BC_WALL_T 6
 #define MB_BC_EXTRAPOLATION 11
 #define MB_BC_OUTLET 24
-#define MB_BC_NQ 6 /* parameters of a record (mb_bc.q) */
+#define MB_BC_NQ 12 /* parameters of a record (mb_bc.q) */
 
 /* limiter ids = lim_dev (numerics/space/Lib_Limiters.f90:21-61) */
 #define MB_LIM_MINMOD 1
@@ -118,8 +118,14 @@ typedef struct mb_bc {
   int32_t type;  /* MB_BC_* */
   int32_t conn;  /* type 1: index into mb_mesh.conn; -1 otherwise */
   int32_t pad0;
-  double q[MB_BC_NQ]; /* type 4 (405): mach, T0, p0 (static T and p), alpha, beta (flow angles, radians),
-                         rel_fac (bc%mach, bc%T0, bc%p0, bc%alpha, bc%beta, bc%rel_fac); unused otherwise */
+  double q[MB_BC_NQ]; /* type 4: q[0..5] = mach, T0, p0, alpha, beta (flow angles, radians), rel_fac (bc%mach, %T0,
+                         %p0, %alpha, %beta, %rel_fac); q[6] = the bc.txt code of the closure, as IO_BC_Open.f90:229-307
+                         maps it: 0 or 405 the static inlet (T0, p0 static; the supersonic closure at any Mach),
+                         401 the stagnation inlet (T0, p0 total), 403 the mass-flux inlet with total T (p0 = the mass
+                         flux), 404 the mass-flux inlet with static T (rel_fac 1), 407 the ambient boundary (stagnation
+                         inlet inwards, outflow to q[7] = pamb outwards); q[8..10] = the unit tangent of the face (the
+                         diagonal of its nodes, Mod_BC.f90:226-240; read by 401-404 and 407);
+                         type 6: q[0] = T_wall; type 24: q[0] = exit pressure, q[1] = rel_fac; unused otherwise */
 } mb_bc;
 
 /* One connection (domain%conn_*, Lib_Extrapolation.f90:1023-1134): the donor face cell of a

@@ -176,7 +176,16 @@ static int check_mesh(const mb_mesh* mesh, int ngroups) {
         r.type != MB_BC_INFLOW && r.type != MB_BC_SYMMETRY && r.type != MB_BC_WALL_T && r.type != MB_BC_OUTLET)
       return MB_E_UNSUPPORTED;
     if (r.blk < 0 || r.blk >= mesh->nblk || r.face < 1 || r.face > 6) return MB_E_ARG;
-    if (r.type == MB_BC_INFLOW && !(r.q[1] > 0.0 && r.q[2] > 0.0)) return MB_E_ARG;  // T0, p0
+    if (r.type == MB_BC_INFLOW) {
+      if (!(r.q[1] > 0.0 && r.q[2] > 0.0)) return MB_E_ARG;  // T0, p0 (or the mass flux)
+      const int code = (int)r.q[6];
+      if (code != 0 && code != 401 && code != 403 && code != 404 && code != 405 && code != 407) return MB_E_UNSUPPORTED;
+      if (code == 404 && r.q[5] != 1.0) return MB_E_UNSUPPORTED;  // IO_BC_Open.f90:276-281
+      if (code == 401 || code == 403 || code == 404 || code == 407) {  // the face tangent is read
+        const double tn = r.q[8] * r.q[8] + r.q[9] * r.q[9] + r.q[10] * r.q[10];
+        if (!(fabs(tn - 1.0) < 1e-6)) return MB_E_ARG;
+      }
+    }
     if (r.type == MB_BC_WALL_T && !(r.q[0] > 0.0)) return MB_E_ARG;                   // T_wall
     if (r.type == MB_BC_OUTLET && !(r.q[0] >= 0.0 && r.q[1] >= 0.0 && r.q[1] <= 1.0)) return MB_E_ARG;
   }
@@ -255,10 +264,12 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
     const mb_bc& r = mesh->rec[q];
     hr[q].type = r.type;
     hr[q].pg = r.conn;
-    for (int s = 0; s < 8; ++s) hr[q].q[s] = 0.0;
+    for (int s = 0; s < 16; ++s) hr[q].q[s] = 0.0;
     if (r.type == MB_BC_INFLOW) {  // mach, T0, p0, rel_fac, cos / sin of alpha and beta
       const double v[8] = {r.q[0], r.q[1], r.q[2], r.q[5], cos(r.q[3]), sin(r.q[3]), cos(r.q[4]), sin(r.q[4])};
       for (int s = 0; s < 8; ++s) hr[q].q[s] = v[s];
+      hr[q].q[8] = r.q[6]; hr[q].q[9] = r.q[7]; hr[q].q[10] = r.q[3]; hr[q].q[11] = r.q[4];
+      hr[q].q[12] = r.q[8]; hr[q].q[13] = r.q[9]; hr[q].q[14] = r.q[10];
     }
     if (r.type == MB_BC_WALL_T) hr[q].q[0] = r.q[0];                                  // T_wall
     if (r.type == MB_BC_OUTLET) { hr[q].q[0] = r.q[0]; hr[q].q[1] = r.q[1]; }        // exit pressure, relaxation

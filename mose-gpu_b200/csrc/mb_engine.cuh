@@ -561,8 +561,153 @@ MB_HD void bc_wall_temp(const Params& p, const DBlk& b, const double* __restrict
   S[MB_IPR] = (R)modfm2 * Flux_np;
 }
 
-// BC_Inflow_Outflow (Lib_BC.f90:1519-1597) of a 405 record: inward flow -> BC_Supersonic_Inflow (Lib_BC.f90:
-// 1247-1330), outward flow -> the face closes (BC_Symmetry_Eul).
+template <typename R> MB_HD R pw_(R x, R y);
+template <> MB_HD double pw_(double x, double y) { return pow(x, y); }
+template <> MB_HD float pw_(float x, float y) { return powf(x, y); }
+
+// BC_Outflow (Lib_BC.f90:1166-1240): the face state of an outflow to the pressure p_Amb (isentropic when the normal
+// Mach number is below 1 and p_Amb > 0, the boundary cell itself otherwise) and its flux Fl
+template <typename R>
+MB_HD void outflow_face(const Params& p, const R* Bp, R Brho, R BRgas, R BSound, R Un, R BGamma, R Riem,
+                        const R* nrm, R area, R p_Amb, R BC_Sign, R* Fl) {
+  R VT[3] = {Bp[MB_IU] - Un * nrm[0], Bp[MB_IV] - Un * nrm[1], Bp[MB_IW] - Un * nrm[2]};
+  R Mach_N = fabs(Un / BSound);
+  R pe = p_Amb;
+  R Fp[MB_NP], Fun, Frho, FRgas;
+  if (Mach_N < (R)1 && p_Amb > (R)0) {
+    R delta = (R)0.5 * (BGamma - (R)1);
+    R denom = (R)1 / pw_((R)1 + delta, BGamma / (BGamma - (R)1));
+    R pstar = Bp[MB_IPR] * denom * pw_((R)1 + delta * (Mach_N * Mach_N), BGamma / (BGamma - (R)1));
+    if (pstar >= p_Amb) pe = pstar;
+    R Isentropic = (BGamma - (R)1) / ((R)2 * BGamma);
+    R FSound = BSound * pw_(pe / Bp[MB_IPR], Isentropic);
+    Fun = (Riem - FSound) / (BC_Sign * (R)0.5 * (BGamma - (R)1));
+    Fp[MB_IPR] = pe;
+    Frho = BGamma * Fp[MB_IPR] / (FSound * FSound);
+    Fp[0] = Bp[0] / Brho * Frho;
+    Fp[MB_IU] = VT[0] + Fun * nrm[0];
+    Fp[MB_IV] = VT[1] + Fun * nrm[1];
+    Fp[MB_IW] = VT[2] + Fun * nrm[2];
+    FRgas = BRgas;
+  } else {
+#pragma unroll
+    for (int s = 0; s < MB_NP; ++s) Fp[s] = Bp[s];
+    Fun = Un; Frho = Brho; FRgas = BRgas;
+  }
+  R FT = Fp[MB_IPR] / (FRgas * Frho);
+  int Ti = tidx(p, FT);
+  R Td = FT - (R)Ti;
+  const R* H = Tab<R>::h(p);
+  R FEnth = (R)0 + Fp[0] / Frho * (H[Ti] + (H[Ti + 1] - H[Ti]) * Td);
+  Fl[0] = Fp[0] * area * Fun;
+  R Fmass = Frho * area * Fun;
+  Fl[MB_IU] = Fp[MB_IU] * Fmass + Fp[MB_IPR] * area * nrm[0];
+  Fl[MB_IV] = Fp[MB_IV] * Fmass + Fp[MB_IPR] * area * nrm[1];
+  Fl[MB_IW] = Fp[MB_IW] * Fmass + Fp[MB_IPR] * area * nrm[2];
+  R vt2 = Fp[MB_IU] * Fp[MB_IU] + Fp[MB_IV] * Fp[MB_IV] + Fp[MB_IW] * Fp[MB_IW];
+  Fl[MB_IPR] = Fmass * ((R)0.5 * vt2 + FEnth);
+}
+
+// BC_Subsonic_Inflow (Lib_BC.f90:1335-1512), one species: the face state from the outgoing Riemann invariant and the
+// stagnation (mach >= 0) or mass-flux (mach < 0: p0 = the mass flux; mach -10: T0 total) conditions, and its flux Fl
+template <typename R>
+MB_HD void subsonic_inflow_face(const Params& p, const R* Bp, R Un, R Sound, R Gamma, R Riem, R BC_alpha, R BC_beta,
+                                R BC_Mach, R BC_T0, R BC_p0, R rel, R BC_Sign, const R* t, const R* n, R area, R* Fl) {
+  R bv[3] = {n[1] * t[2] - n[2] * t[1], n[2] * t[0] - n[0] * t[2], n[0] * t[1] - n[1] * t[0]};
+  R bmod = rsqrt_(bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2]);
+  bv[0] = bv[0] / bmod; bv[1] = bv[1] / bmod; bv[2] = bv[2] / bmod;
+  R alpha, beta;
+  if (BC_alpha == (R)0 && BC_beta == (R)0) {
+    alpha = atan(n[1] / (n[0] + (R)1e-20));
+    beta = atan(n[2] / (n[0] + (R)1e-20));
+  } else {
+    alpha = BC_alpha; beta = BC_beta;
+  }
+  const R ta = tan(alpha), tb = tan(beta);
+  R XA = n[1] - n[0] * ta, XB = t[1] - t[0] * ta, XC = bv[1] - bv[0] * ta;
+  R XD = n[2] - n[0] * tb, XE = t[2] - t[0] * tb, XF = bv[2] - bv[0] * tb;
+  R check = (XC * XE - XF * XB);
+  R E1 = (XF * XA - XC * XD) / check;
+  R E2 = (XD * XB - XE * XA) / check;
+  const R ri = (R)p.ri;
+  R Fp[MB_NP], Frho, FRgas, Fun;
+  if (BC_Mach >= (R)0) {
+    R Discr = (R)-1, p0_try = BC_p0, Sound0 = (R)0, Coef_D = (R)0, YA = (R)1, YB = (R)0;
+    int iter = 0;
+    FRgas = (R)0 + (R)1 * ri;
+    while (Discr < (R)0) {  // at most 1001 passes
+      iter = iter + 1;
+      FRgas = (R)0 + (R)1 * ri;
+      Sound0 = rsqrt_(Gamma * FRgas * BC_T0);
+      Coef_D = ((R)1 + E1 * E1 + E2 * E2) * (Gamma - (R)1) / (R)2;
+      R Coef_C = powr(p0_try / Bp[MB_IPR], (Gamma - (R)1) / Gamma);
+      Coef_C = Coef_C * ((Sound / Sound0) * (Sound / Sound0));
+      const R g2 = (Gamma - (R)1) / (R)2;
+      YA = g2 * g2 + Coef_C * Coef_D;
+      YB = BC_Sign * Riem * ((Gamma - (R)1) / (R)2);
+      R YC = Riem * Riem - Coef_C * (Sound0 * Sound0);
+      Discr = YB * YB - YA * YC;
+      if (Discr < (R)0 && fabs(Discr) < (R)1e-2) Discr = (R)0;
+      if (Discr < (R)0 && fabs(Discr) > (R)1e-2) {
+        if (rel == (R)1) { Discr = (R)0; break; }
+        p0_try = rel * p0_try + ((R)1 - rel) * Bp[MB_IPR];
+      }
+      if (iter > 1000) { Discr = (R)0; break; }
+    }
+    R Un_Sign = copysign((R)1, Un);
+    R Un3 = (YB + Un_Sign * rsqrt_(Discr)) / YA;
+    R Sound3 = rsqrt_(Sound0 * Sound0 - Coef_D * (Un3 * Un3));
+    R p3 = p0_try * powr(Sound3 / Sound0, (R)2 * Gamma / (Gamma - (R)1));
+    R Ut3 = Un3 * E1, Ub3 = Un3 * E2;
+    Fp[MB_IPR] = p3;
+    Frho = Gamma * Fp[MB_IPR] / (Sound3 * Sound3);
+    Fp[0] = (R)1 * Frho;
+    Fp[MB_IU] = Un3 * n[0] + Ut3 * t[0] + Ub3 * bv[0];
+    Fp[MB_IV] = Un3 * n[1] + Ut3 * t[1] + Ub3 * bv[1];
+    Fp[MB_IW] = Un3 * n[2] + Ut3 * t[2] + Ub3 * bv[2];
+    Fun = Un3;
+  } else {
+    R mdot = BC_p0, p3 = Bp[MB_IPR];
+    int Ti = tidx(p, BC_T0);
+    R Td = BC_T0 - (R)Ti;
+    const R* CP = Tab<R>::cp(p);
+    R cp3 = (R)0 + (R)1 * (CP[Ti] + (CP[Ti + 1] - CP[Ti]) * Td);
+    R Rgas3 = (R)0 + (R)1 * ri;
+    R T3 = BC_T0;
+    if (BC_Mach == (R)-10) {
+      R x = mdot * Rgas3 / p3, y = p3 / (mdot * Rgas3);
+      T3 = (-cp3 + rsqrt_(cp3 * cp3 + (R)2 * cp3 * BC_T0 * (x * x))) * (y * y);
+    }
+    R rho3 = p3 / (Rgas3 * T3);
+    R Un3 = mdot / rho3;
+    R Ut3 = Un3 * E1, Ub3 = Un3 * E2;
+    FRgas = Rgas3;
+    Frho = rho3;
+    Fp[0] = Frho * (R)1;
+    Fp[MB_IU] = Un3 * n[0] + Ut3 * t[0] + Ub3 * bv[0];
+    Fp[MB_IV] = Un3 * n[1] + Ut3 * t[1] + Ub3 * bv[1];
+    Fp[MB_IW] = Un3 * n[2] + Ut3 * t[2] + Ub3 * bv[2];
+    Fp[MB_IPR] = p3;
+    Fun = Un3;
+  }
+  R FT = Fp[MB_IPR] / (FRgas * Frho);
+  int Ti = tidx(p, FT);
+  R Td = FT - (R)Ti;
+  const R* H = Tab<R>::h(p);
+  R FEnth = (R)0 + Fp[0] / Frho * (H[Ti] + (H[Ti + 1] - H[Ti]) * Td);
+  Fl[0] = Fp[0] * Fun * area;
+  R Fmass = Frho * Fun * area;
+  Fl[MB_IU] = Fmass * Fp[MB_IU] + Fp[MB_IPR] * area * n[0];
+  Fl[MB_IV] = Fmass * Fp[MB_IV] + Fp[MB_IPR] * area * n[1];
+  Fl[MB_IW] = Fmass * Fp[MB_IW] + Fp[MB_IPR] * area * n[2];
+  R vt2 = Fp[MB_IU] * Fp[MB_IU] + Fp[MB_IV] * Fp[MB_IV] + Fp[MB_IW] * Fp[MB_IW];
+  Fl[MB_IPR] = Fmass * ((R)0.5 * vt2 + FEnth);
+}
+
+// The inflow / outflow record (type 4), BC_Inflow_Outflow (Lib_BC.f90:1519-1597). The record's closure code (q[8]:
+// 0 / 405, 401, 403, 404, 407, as IO_BC_Open.f90:229-307 sets them up) gives mach and pamb: outward flow closes an
+// inlet face (BC_Symmetry_Eul) or leaves to pamb (BC_Outflow, 407); inward flow takes the supersonic static inlet
+// (405, or mach > 1: BC_Supersonic_Inflow, Lib_BC.f90:1247-1330) or the subsonic closure (BC_Subsonic_Inflow).
 template <typename R, int RS = 0, int LIM = 0>
 MB_HD void bc_inflow(const Params& p, const DBlk& b, const double* __restrict__ P, int Im, int Jm, int Km,
                               int Fm, const double* __restrict__ q, R* A) {
@@ -577,12 +722,49 @@ MB_HD void bc_inflow(const Params& p, const DBlk& b, const double* __restrict__ 
   double g[4];
   bc_face_geom(b, Im, Jm, Km, Fm, g);
   R nx = cvt<R>(g[0]), ny = cvt<R>(g[1]), nz = cvt<R>(g[2]), area = cvt<R>(g[3]);
-  const R BC_Mach = cvt<R>(ld(q + 0)), BC_T0 = cvt<R>(ld(q + 1)), BC_p0 = cvt<R>(ld(q + 2)), rel = cvt<R>(ld(q + 3));
+  const int code = (int)ld(q + 8);
+  R BC_Mach = cvt<R>(ld(q + 0));
+  R pamb = (R)-2.71;  // PAMB_FORCE_SUPERSONIC
+  if (code == 401) { BC_Mach = (R)0; pamb = (R)-3.14; }
+  else if (code == 403) { BC_Mach = (R)-10; pamb = (R)-3.14; }
+  else if (code == 404) { BC_Mach = (R)-1; pamb = (R)-3.14; }
+  else if (code == 407) { BC_Mach = (R)0; pamb = cvt<R>(ld(q + 9)); }
+  const R BC_T0 = cvt<R>(ld(q + 1)), BC_p0 = cvt<R>(ld(q + 2)), rel = cvt<R>(ld(q + 3));
+  const R BC_Sign = (R)modfm2;
   R Un = P2[MB_IU] * nx + P2[MB_IV] * ny + P2[MB_IW] * nz;
-  R InOut = (R)modfm2 * Un;
+  R Brho, BRgas;
+  rotot_rtot(p, P2[0], Brho, BRgas);
+  R BSound = f_ss(p, P2[0], P2[MB_IPR], Brho, BRgas);
+  R Tb = P2[MB_IPR] / (Brho * BRgas);
+  int tiB = tidx(p, Tb);
+  R cpB = f_cp(p, P2[0], tiB, Tb - (R)tiB, Brho);
+  R BGamma = cpB / (cpB - BRgas);
+  R Riem = BSound + BC_Sign * (R)0.5 * (BGamma - (R)1) * Un;
+  R InOut = BC_Sign * Un;
   if (BC_Mach < (R)0) InOut = (R)-1;
+  const R nrm[3] = {nx, ny, nz};
   if (InOut >= (R)0) {
-    bc_sym_eul<R, RS, LIM>(p, b, P, Im, Jm, Km, Fm, A);
+    if (pamb == (R)-3.14 || pamb == (R)-2.71) {  // an inlet: the face closes
+      bc_sym_eul<R, RS, LIM>(p, b, P, Im, Jm, Km, Fm, A);
+      return;
+    }
+    R Fo[MB_NP];
+    outflow_face<R>(p, P2, Brho, BRgas, BSound, Un, BGamma, Riem, nrm, area, pamb, BC_Sign, Fo);
+#pragma unroll
+    for (int s = 0; s < MB_NP; ++s) A[s] = (R)modfm2 * Fo[s];
+    return;
+  }
+  if (!(BC_Mach > (R)1 || pamb == (R)-2.71)) {
+    R Fo[MB_NP];
+#pragma unroll
+    for (int s = 0; s < MB_NP; ++s) Fo[s] = (R)0;
+    if (BC_Mach < (R)1) {
+      const R tv[3] = {cvt<R>(ld(q + 12)), cvt<R>(ld(q + 13)), cvt<R>(ld(q + 14))};
+      subsonic_inflow_face<R>(p, P2, Un, BSound, BGamma, Riem, cvt<R>(ld(q + 10)), cvt<R>(ld(q + 11)), BC_Mach, BC_T0,
+                              BC_p0, rel, BC_Sign, tv, nrm, area, Fo);
+    }
+#pragma unroll
+    for (int s = 0; s < MB_NP; ++s) A[s] = (R)modfm2 * Fo[s];
     return;
   }
   R frho, fR;
@@ -631,9 +813,6 @@ MB_HD void bc_inflow(const Params& p, const DBlk& b, const double* __restrict__ 
   for (int s = 0; s < MB_NP; ++s) A[s] = (R)modfm2 * Fl[s];
 }
 
-template <typename R> MB_HD R pw_(R x, R y);
-template <> MB_HD double pw_(double x, double y) { return pow(x, y); }
-template <> MB_HD float pw_(float x, float y) { return powf(x, y); }
 
 // BC_Outlet (Lib_BC.f90:1604-1658) of a 406 record (q = exit pressure, relaxation factor): inward flow closes the face
 // (BC_Symmetry_Eul); otherwise the face state of BC_Outflow (Lib_BC.f90:1166-1240) from the Riemann invariant towards
@@ -668,43 +847,8 @@ MB_HD void bc_outlet(const Params& p, const DBlk& b, const double* __restrict__ 
   R BGamma = cp / (cp - BRgas);
   R Riem = BSound + BC_Sign * (R)0.5 * (BGamma - (R)1) * Un;
   R p_Amb = rel * pExit + ((R)1 - rel) * Bp[MB_IPR];
-  R VT[3] = {Bp[MB_IU] - Un * nrm[0], Bp[MB_IV] - Un * nrm[1], Bp[MB_IW] - Un * nrm[2]};
-  R Mach_N = fabs(Un / BSound);
-  R pe = p_Amb;
-  R Fp[MB_NP], Fun, Frho, FRgas;
-  if (Mach_N < (R)1 && p_Amb > (R)0) {
-    R delta = (R)0.5 * (BGamma - (R)1);
-    R denom = (R)1 / pw_((R)1 + delta, BGamma / (BGamma - (R)1));
-    R pstar = Bp[MB_IPR] * denom * pw_((R)1 + delta * (Mach_N * Mach_N), BGamma / (BGamma - (R)1));
-    if (pstar >= p_Amb) pe = pstar;
-    R Isentropic = (BGamma - (R)1) / ((R)2 * BGamma);
-    R FSound = BSound * pw_(pe / Bp[MB_IPR], Isentropic);
-    Fun = (Riem - FSound) / (BC_Sign * (R)0.5 * (BGamma - (R)1));
-    Fp[MB_IPR] = pe;
-    Frho = BGamma * Fp[MB_IPR] / (FSound * FSound);
-    Fp[0] = Bp[0] / Brho * Frho;
-    Fp[MB_IU] = VT[0] + Fun * nrm[0];
-    Fp[MB_IV] = VT[1] + Fun * nrm[1];
-    Fp[MB_IW] = VT[2] + Fun * nrm[2];
-    FRgas = BRgas;
-  } else {
-#pragma unroll
-    for (int s = 0; s < MB_NP; ++s) Fp[s] = Bp[s];
-    Fun = Un; Frho = Brho; FRgas = BRgas;
-  }
-  R FT = Fp[MB_IPR] / (FRgas * Frho);
-  int Ti = tidx(p, FT);
-  R Td = FT - (R)Ti;
-  const R* H = Tab<R>::h(p);
-  R FEnth = (R)0 + Fp[0] / Frho * (H[Ti] + (H[Ti + 1] - H[Ti]) * Td);
   R Fl[MB_NP];
-  Fl[0] = Fp[0] * area * Fun;
-  R Fmass = Frho * area * Fun;
-  Fl[MB_IU] = Fp[MB_IU] * Fmass + Fp[MB_IPR] * area * nrm[0];
-  Fl[MB_IV] = Fp[MB_IV] * Fmass + Fp[MB_IPR] * area * nrm[1];
-  Fl[MB_IW] = Fp[MB_IW] * Fmass + Fp[MB_IPR] * area * nrm[2];
-  R vt2 = Fp[MB_IU] * Fp[MB_IU] + Fp[MB_IV] * Fp[MB_IV] + Fp[MB_IW] * Fp[MB_IW];
-  Fl[MB_IPR] = Fmass * ((R)0.5 * vt2 + FEnth);
+  outflow_face<R>(p, Bp, Brho, BRgas, BSound, Un, BGamma, Riem, nrm, area, p_Amb, BC_Sign, Fl);
 #pragma unroll
   for (int s = 0; s < MB_NP; ++s) A[s] = (R)modfm2 * Fl[s];
 }

@@ -64,10 +64,10 @@ template <> struct Geo<float> {
 struct DRec {
   int type;
   int pg;               // row of the record in the transverse-stencil table (connections), -1 otherwise
-  // type 4 (405 inlet): mach, T0, p0, rel_fac, cos alpha, sin alpha, cos beta, sin beta (the angles' cos / sin
-  // taken once on the host, so that every form uses the same values); type 6: T_wall; type 24: exit pressure,
-  // relaxation factor
-  double q[8];
+  // type 4: mach, T0, p0, rel_fac, cos alpha, sin alpha, cos beta, sin beta (the angles' cos / sin taken once on the
+  // host, so that every form uses the same values), the closure code (0 / 401 / 403 / 404 / 405 / 407), pamb, alpha,
+  // beta, the face's unit tangent (3); type 6: T_wall; type 24: exit pressure, relaxation factor
+  double q[16];
 };
 
 // device status + clock of the time loop (one per context)

@@ -10,7 +10,7 @@ import numpy as np
 GC = 2
 NSC = 1
 NPRIM = 5
-BC_NQ = 6
+BC_NQ = 12
 
 MB_OK = 0
 MB_E_ARG = -1

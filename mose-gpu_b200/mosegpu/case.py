@@ -295,6 +295,15 @@ def layout_case(name, cuts, node_fn, periodic, bc_faces, thermo, scheme, prim_fn
                     r["q"][:, :qv.size] = qv
                 else:
                     r["type"] = spec
+                if r["type"][0] == abi.BC_INFLOW:
+                    # the unit tangent of each face: the diagonal of its nodes (Mod_BC.f90:226-240)
+                    lo = b["lo"]
+                    Fi = [I.astype(np.float64), J.astype(np.float64), K.astype(np.float64)]
+                    Fi[ax] = Fi[ax] - (face % 2)
+                    A = [Fi[d] + lo[d] for d in range(3)]
+                    Bn = [A[d] - (0 if d == ax else 1) for d in range(3)]
+                    tv = node_fn(*A) - node_fn(*Bn)
+                    r["q"][:, 8:11] = tv / np.linalg.norm(tv, axis=-1, keepdims=True)
             recs.append(r)
             nrec += m
     case.rec = np.concatenate(recs) if recs else np.zeros(0, dtype=abi.BC_DTYPE)

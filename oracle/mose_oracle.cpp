@@ -1379,9 +1379,118 @@ void bc_wall_temperature(const Ctx& c, const Blk& b, const double* P, double* R,
   R[rb + IP * nc] = R[rb + IP * nc] - (double)modfm2 * Flux_np;
 }
 
-// BC_Inflow_Outflow (Lib_BC.f90:1519-1597) for a 405 record (pamb = PAMB_FORCE_SUPERSONIC): inward flow ->
-// BC_Supersonic_Inflow (Lib_BC.f90:1247-1330), outward flow -> the face closes (BC_Symmetry_Eul).
-// q = mach, T0, p0, alpha, beta, rel_fac; the angles enter through cos / sin taken on the host.
+// The inflow / outflow record (type 4), BC_Inflow_Outflow (Lib_BC.f90:1519-1597). q = mach, T0, p0, alpha, beta,
+// rel_fac, open code, pamb, t (3): the open code selects the closure as IO_BC_Open.f90:229-307 sets it up -- 0 or 405
+// the supersonic static inlet (any Mach; the face closes on outward flow), 401 the subsonic stagnation inlet (T0, p0),
+// 403 the mass-flux inlet with total T (p0 = the mass flux), 404 the mass-flux inlet with static T, 407 the ambient
+// boundary (stagnation inlet on inward flow, outflow to pamb = q[7] on outward flow). t is the unit tangent of the
+// face (Mod_BC.f90:226-240: the diagonal of its nodes). Outward flow at a 401-405 face closes it (BC_Symmetry_Eul).
+void outflow_flux(const Thermo& th, const double* Bp, double Brho, double BRgas, double BSound, double Un,
+                  double BGamma, double Riem, const double* nrm, double area, double p_Amb, double BC_Sign,
+                  double* Flux);
+void inflow_resolve(const double* q, double& mach, double& pamb) {
+  const int code = (int)q[6];
+  mach = q[0];
+  pamb = -2.71;  // PAMB_FORCE_SUPERSONIC
+  if (code == 401) { mach = 0.0; pamb = -3.14; }
+  else if (code == 403) { mach = -10.0; pamb = -3.14; }
+  else if (code == 404) { mach = -1.0; pamb = -3.14; }
+  else if (code == 407) { mach = 0.0; pamb = q[7]; }
+}
+
+// BC_Subsonic_Inflow (Lib_BC.f90:1335-1512), one species: the face state from the outgoing Riemann invariant and the
+// stagnation (mach >= 0) or mass-flux (mach < 0) conditions; its flux into Flux
+void subsonic_inflow_flux(const Thermo& th, const double* Bp, double Un, double Sound, double Gamma, double Riem,
+                          double BC_alpha, double BC_beta, double BC_Mach, double BC_T0, double BC_p0, double rel,
+                          double BC_Sign, const double* t, const double* n, double area, double* Flux) {
+  double bv[3] = {n[1] * t[2] - n[2] * t[1], n[2] * t[0] - n[0] * t[2], n[0] * t[1] - n[1] * t[0]};
+  double bmod = std::sqrt(bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2]);
+  bv[0] = bv[0] / bmod; bv[1] = bv[1] / bmod; bv[2] = bv[2] / bmod;
+  double alpha, beta;
+  if (BC_alpha == 0.0 && BC_beta == 0.0) {
+    alpha = std::atan(n[1] / (n[0] + 1e-20));
+    beta = std::atan(n[2] / (n[0] + 1e-20));
+  } else {
+    alpha = BC_alpha; beta = BC_beta;
+  }
+  const double ta = std::tan(alpha), tb = std::tan(beta);
+  double XA = n[1] - n[0] * ta, XB = t[1] - t[0] * ta, XC = bv[1] - bv[0] * ta;
+  double XD = n[2] - n[0] * tb, XE = t[2] - t[0] * tb, XF = bv[2] - bv[0] * tb;
+  double check = (XC * XE - XF * XB);
+  double E1 = (XF * XA - XC * XD) / check;
+  double E2 = (XD * XB - XE * XA) / check;
+  double Fp[NP], Frho, FRgas, Fun;
+  if (BC_Mach >= 0.0) {
+    double Discr = -1.0, p0_try = BC_p0, Sound0 = 0.0, Coef_D = 0.0, YA = 0.0, YB = 0.0;
+    int iter = 0;
+    while (Discr < 0.0) {
+      iter = iter + 1;
+      FRgas = 0.0 + 1.0 * th.ri;
+      Sound0 = std::sqrt(Gamma * FRgas * BC_T0);
+      Coef_D = (1.0 + E1 * E1 + E2 * E2) * (Gamma - 1.0) / 2.0;
+      double Coef_C = std::pow(p0_try / Bp[IP], (Gamma - 1.0) / Gamma);
+      Coef_C = Coef_C * ((Sound / Sound0) * (Sound / Sound0));
+      const double g2 = (Gamma - 1.0) / 2.0;
+      YA = g2 * g2 + Coef_C * Coef_D;
+      YB = BC_Sign * Riem * ((Gamma - 1.0) / 2.0);
+      double YC = Riem * Riem - Coef_C * (Sound0 * Sound0);
+      Discr = YB * YB - YA * YC;
+      if (Discr < 0.0 && std::fabs(Discr) < 1e-2) Discr = 0.0;
+      if (Discr < 0.0 && std::fabs(Discr) > 1e-2) {
+        if (rel == 1.0) { Discr = 0.0; break; }
+        p0_try = rel * p0_try + (1.0 - rel) * Bp[IP];
+      }
+      if (iter > 1000) { Discr = 0.0; break; }
+    }
+    double Un_Sign = std::copysign(1.0, Un);
+    double Un3 = (YB + Un_Sign * std::sqrt(Discr)) / YA;
+    double Sound3 = std::sqrt(Sound0 * Sound0 - Coef_D * (Un3 * Un3));
+    double p3 = p0_try * std::pow(Sound3 / Sound0, 2.0 * Gamma / (Gamma - 1.0));
+    double Ut3 = Un3 * E1, Ub3 = Un3 * E2;
+    Fp[IP] = p3;
+    Frho = Gamma * Fp[IP] / (Sound3 * Sound3);
+    Fp[0] = 1.0 * Frho;
+    Fp[IU] = Un3 * n[0] + Ut3 * t[0] + Ub3 * bv[0];
+    Fp[IV] = Un3 * n[1] + Ut3 * t[1] + Ub3 * bv[1];
+    Fp[IW] = Un3 * n[2] + Ut3 * t[2] + Ub3 * bv[2];
+    Fun = Un3;
+  } else {  // mass flux (p0 column) and temperature: total (mach -10) or static
+    double mdot = BC_p0, p3 = Bp[IP];
+    int Ti = tidx(th, BC_T0);
+    double Td = BC_T0 - Ti;
+    double cp3 = 0.0 + 1.0 * tabT(th.cp, Ti, Td);
+    double Rgas3 = 0.0 + 1.0 * th.ri;
+    double T3 = BC_T0;
+    if (BC_Mach == -10.0) {
+      double x = mdot * Rgas3 / p3, y = p3 / (mdot * Rgas3);
+      T3 = (-cp3 + std::sqrt(cp3 * cp3 + 2.0 * cp3 * BC_T0 * (x * x))) * (y * y);
+    }
+    double rho3 = p3 / (Rgas3 * T3);
+    double Un3 = mdot / rho3;
+    double Ut3 = Un3 * E1, Ub3 = Un3 * E2;
+    FRgas = Rgas3;
+    Frho = rho3;
+    Fp[0] = Frho * 1.0;
+    Fp[IU] = Un3 * n[0] + Ut3 * t[0] + Ub3 * bv[0];
+    Fp[IV] = Un3 * n[1] + Ut3 * t[1] + Ub3 * bv[1];
+    Fp[IW] = Un3 * n[2] + Ut3 * t[2] + Ub3 * bv[2];
+    Fp[IP] = p3;
+    Fun = Un3;
+  }
+  double FEnth = 0.0;
+  double FT = Fp[IP] / (FRgas * Frho);
+  int Ti = tidx(th, FT);
+  double Td = FT - Ti;
+  FEnth = FEnth + Fp[0] / Frho * tabT(th.h, Ti, Td);
+  Flux[0] = Fp[0] * Fun * area;
+  double Fmass = Frho * Fun * area;
+  Flux[IU] = Fmass * Fp[IU] + Fp[IP] * area * n[0];
+  Flux[IV] = Fmass * Fp[IV] + Fp[IP] * area * n[1];
+  Flux[IW] = Fmass * Fp[IW] + Fp[IP] * area * n[2];
+  double vt2 = Fp[IU] * Fp[IU] + Fp[IV] * Fp[IV] + Fp[IW] * Fp[IW];
+  Flux[IP] = Fmass * (0.5 * vt2 + FEnth);
+}
+
 void bc_inflow_405(const Ctx& c, const Blk& b, const double* P, double* R, int Im, int Jm, int Km, int Fm,
                    const double* q) {
   const int64_t nc = c.ncell;
@@ -1394,12 +1503,38 @@ void bc_inflow_405(const Ctx& c, const Blk& b, const double* P, double* R, int I
   for (int s = 0; s < NP; ++s) { P2[s] = P[rb + s * nc]; Ip[s] = P[ri + s * nc]; }
   double nrm[3], area;
   bc_face_geom(b, Im, Jm, Km, Fm, nrm, area);
-  const double BC_Mach = q[0], BC_T0 = q[1], BC_p0 = q[2], rel = q[5];
+  double BC_Mach, pamb;
+  inflow_resolve(q, BC_Mach, pamb);
+  const double BC_T0 = q[1], BC_p0 = q[2], rel = q[5];
+  const double BC_Sign = (double)modfm2;
   double Un = P2[IU] * nrm[0] + P2[IV] * nrm[1] + P2[IW] * nrm[2];
-  double InOut = (double)modfm2 * Un;
+  double Brho, BRgas;
+  rotot_rtot(th, P2[0], Brho, BRgas);
+  double BSound = f_ss(th, P2[0], P2[IP], Brho, BRgas);
+  double T = P2[IP] / (Brho * BRgas);
+  int tiB = tidx(th, T);
+  double cpB = f_cp(th, P2[0], tiB, T - tiB, Brho);
+  double BGamma = cpB / (cpB - BRgas);
+  double Riem = BSound + BC_Sign * 0.5 * (BGamma - 1.0) * Un;
+  double InOut = BC_Sign * Un;
   if (BC_Mach < 0.0) InOut = -1.0;
-  if (InOut >= 0.0) {  // error = 1: the caller applies the symmetry flux
-    bc_symmetry_eul(c, b, P, R, Im, Jm, Km, Fm);
+  if (InOut >= 0.0) {
+    if (pamb == -3.14 || pamb == -2.71) {  // an inlet: error = 1, the caller applies the symmetry flux
+      bc_symmetry_eul(c, b, P, R, Im, Jm, Km, Fm);
+      return;
+    }
+    double Flux[NP];
+    outflow_flux(th, P2, Brho, BRgas, BSound, Un, BGamma, Riem, nrm, area, pamb, BC_Sign, Flux);
+    for (int s = 0; s < NP; ++s) R[rb + s * nc] = R[rb + s * nc] + (double)modfm2 * Flux[s];
+    return;
+  }
+  if (!(BC_Mach > 1.0 || pamb == -2.71)) {
+    if (BC_Mach < 1.0) {
+      double Flux[NP];
+      subsonic_inflow_flux(th, P2, Un, BSound, BGamma, Riem, q[3], q[4], BC_Mach, BC_T0, BC_p0, rel, BC_Sign, q + 8,
+                           nrm, area, Flux);
+      for (int s = 0; s < NP; ++s) R[rb + s * nc] = R[rb + s * nc] + (double)modfm2 * Flux[s];
+    }
     return;
   }
   // BC_Supersonic_Inflow
@@ -1447,6 +1582,51 @@ void bc_inflow_405(const Ctx& c, const Blk& b, const double* P, double* R, int I
   for (int s = 0; s < NP; ++s) R[rb + s * nc] = R[rb + s * nc] + (double)modfm2 * Fl[s];
 }
 
+// BC_Outflow (Lib_BC.f90:1166-1240): the face state of an outflow to the pressure p_Amb (isentropic when the normal
+// Mach number is below 1 and p_Amb > 0, the boundary cell itself otherwise) and its flux
+void outflow_flux(const Thermo& th, const double* Bp, double Brho, double BRgas, double BSound, double Un,
+                  double BGamma, double Riem, const double* nrm, double area, double p_Amb, double BC_Sign,
+                  double* Flux) {
+  double vmag = std::sqrt(Bp[IU] * Bp[IU] + Bp[IV] * Bp[IV] + Bp[IW] * Bp[IW]);
+  double VT[3] = {Bp[IU] - Un * nrm[0], Bp[IV] - Un * nrm[1], Bp[IW] - Un * nrm[2]};
+  double Mach_abs = vmag / BSound;
+  (void)Mach_abs;
+  double Mach_N = std::fabs(Un / BSound);
+  double pe = p_Amb;
+  double Fp[NP], Fun, Frho, FRgas;
+  if (Mach_N < 1.0 && p_Amb > 0.0) {
+    double delta = 0.5 * (BGamma - 1.0);
+    double denom = 1.0 / std::pow(1.0 + delta, BGamma / (BGamma - 1.0));
+    double pstar = Bp[IP] * denom * std::pow(1.0 + delta * (Mach_N * Mach_N), BGamma / (BGamma - 1.0));
+    if (pstar >= p_Amb) pe = pstar;
+    double Isentropic = (BGamma - 1.0) / (2.0 * BGamma);
+    double FSound = BSound * std::pow(pe / Bp[IP], Isentropic);
+    Fun = (Riem - FSound) / (BC_Sign * 0.5 * (BGamma - 1.0));
+    Fp[IP] = pe;
+    Frho = BGamma * Fp[IP] / (FSound * FSound);
+    Fp[0] = Bp[0] / Brho * Frho;
+    Fp[IU] = VT[0] + Fun * nrm[0];
+    Fp[IV] = VT[1] + Fun * nrm[1];
+    Fp[IW] = VT[2] + Fun * nrm[2];
+    FRgas = BRgas;
+  } else {
+    for (int s = 0; s < NP; ++s) Fp[s] = Bp[s];
+    Fun = Un; Frho = Brho; FRgas = BRgas;
+  }
+  double FEnth = 0.0;
+  double FT = Fp[IP] / (FRgas * Frho);
+  int Ti = tidx(th, FT);
+  double Td = FT - Ti;
+  FEnth = FEnth + Fp[0] / Frho * tabT(th.h, Ti, Td);
+  Flux[0] = Fp[0] * area * Fun;
+  double Fmass = Frho * area * Fun;
+  Flux[IU] = Fp[IU] * Fmass + Fp[IP] * area * nrm[0];
+  Flux[IV] = Fp[IV] * Fmass + Fp[IP] * area * nrm[1];
+  Flux[IW] = Fp[IW] * Fmass + Fp[IP] * area * nrm[2];
+  double vt2 = Fp[IU] * Fp[IU] + Fp[IV] * Fp[IV] + Fp[IW] * Fp[IW];
+  Flux[IP] = Fmass * (0.5 * vt2 + FEnth);
+}
+
 // BC_Outlet (Lib_BC.f90:1604-1658) of a 406 record, q = exit pressure, relaxation factor: inward flow closes the
 // face (BC_Symmetry_Eul); otherwise the Riemann invariant towards the face and the relaxed exit pressure give the
 // face state of BC_Outflow (Lib_BC.f90:1166-1240): isentropic to p_exit when the normal Mach number is below 1 and
@@ -1478,47 +1658,8 @@ void bc_outlet(const Ctx& c, const Blk& b, const double* P, double* R, int Im, i
   double BGamma = cp / (cp - BRgas);
   double Riem = BSound + BC_Sign * 0.5 * (BGamma - 1.0) * Un;
   double p_exit = BC_rel_fac * BC_pExit + (1.0 - BC_rel_fac) * Bp[IP];
-  // BC_Outflow
-  const double p_Amb = p_exit;
-  double vmag = std::sqrt(Bp[IU] * Bp[IU] + Bp[IV] * Bp[IV] + Bp[IW] * Bp[IW]);
-  double VT[3] = {Bp[IU] - Un * nrm[0], Bp[IV] - Un * nrm[1], Bp[IW] - Un * nrm[2]};
-  double Mach_abs = vmag / BSound;
-  (void)Mach_abs;
-  double Mach_N = std::fabs(Un / BSound);
-  double pe = p_Amb;
-  double Fp[NP], Fun, Frho, FRgas;
-  if (Mach_N < 1.0 && p_Amb > 0.0) {
-    double delta = 0.5 * (BGamma - 1.0);
-    double denom = 1.0 / std::pow(1.0 + delta, BGamma / (BGamma - 1.0));
-    double pstar = Bp[IP] * denom * std::pow(1.0 + delta * (Mach_N * Mach_N), BGamma / (BGamma - 1.0));
-    if (pstar >= p_Amb) pe = pstar;
-    double Isentropic = (BGamma - 1.0) / (2.0 * BGamma);
-    double FSound = BSound * std::pow(pe / Bp[IP], Isentropic);
-    Fun = (Riem - FSound) / (BC_Sign * 0.5 * (BGamma - 1.0));
-    Fp[IP] = pe;
-    Frho = BGamma * Fp[IP] / (FSound * FSound);
-    Fp[0] = Bp[0] / Brho * Frho;
-    Fp[IU] = VT[0] + Fun * nrm[0];
-    Fp[IV] = VT[1] + Fun * nrm[1];
-    Fp[IW] = VT[2] + Fun * nrm[2];
-    FRgas = BRgas;
-  } else {
-    for (int s = 0; s < NP; ++s) Fp[s] = Bp[s];
-    Fun = Un; Frho = Brho; FRgas = BRgas;
-  }
-  double FEnth = 0.0;
-  double FT = Fp[IP] / (FRgas * Frho);
-  int Ti = tidx(th, FT);
-  double Td = FT - Ti;
   double Flux[NP];
-  FEnth = FEnth + Fp[0] / Frho * tabT(th.h, Ti, Td);
-  Flux[0] = Fp[0] * area * Fun;
-  double Fmass = Frho * area * Fun;
-  Flux[IU] = Fp[IU] * Fmass + Fp[IP] * area * nrm[0];
-  Flux[IV] = Fp[IV] * Fmass + Fp[IP] * area * nrm[1];
-  Flux[IW] = Fp[IW] * Fmass + Fp[IP] * area * nrm[2];
-  double vt2 = Fp[IU] * Fp[IU] + Fp[IV] * Fp[IV] + Fp[IW] * Fp[IW];
-  Flux[IP] = Fmass * (0.5 * vt2 + FEnth);
+  outflow_flux(th, Bp, Brho, BRgas, BSound, Un, BGamma, Riem, nrm, area, p_exit, BC_Sign, Flux);
   for (int s = 0; s < NP; ++s) R[rb + s * nc] = R[rb + s * nc] + (double)modfm2 * Flux[s];
 }
 

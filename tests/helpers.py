@@ -114,6 +114,14 @@ def small_cases():
             cols=2, rows=2, lo=5, hi=9, seed=13, mach=0.5,
             bc={1: abi.BC_INFLOW, 2: (abi.BC_OUTLET, (0.9e5, 1.0)), 3: (abi.BC_WALL_T, (350.0,)),
                 4: (abi.BC_WALL_T, (280.0,)), 5: abi.BC_SYMMETRY, 6: abi.BC_SYMMETRY})),
+        # the subsonic inlets (401 stagnation, 403 / 404 mass flux) and the 407 ambient boundary
+        ("duct3d_401_stagnation_inlet", lambda: cs.duct_3d(bc={1: (abi.BC_INFLOW, (0.0, 320.0, 1.25e5, 0.0, 0.0, 0.5, 401))})),
+        ("duct3d_404_massflux_407_euler", lambda: cs.duct_3d(visc=0, riemann=abi.RS_AUSMP, bc={
+            1: (abi.BC_INFLOW, (0.0, 300.0, 210.0, 0.0, 0.0, 1.0, 404)),
+            2: (abi.BC_INFLOW, (0.0, 315.0, 1.19e5, 0.0, 0.0, 1.0, 407, 0.97e5))})),
+        ("mb2d_403_massflux_inlet", lambda: cs.multiblock_2d(cols=2, rows=2, lo=5, hi=9, seed=17, mach=0.4, bc={
+            1: (abi.BC_INFLOW, (0.0, 310.0, 180.0, 0.1, 0.0, 1.0, 403)), 2: (abi.BC_OUTLET, (1.0e5, 0.5)),
+            3: abi.BC_WALL, 4: abi.BC_WALL, 5: abi.BC_EXTRAPOLATION, 6: abi.BC_EXTRAPOLATION})),
         # blocks two cells and one cell high between walls: a wall's cubic ghosts read the opposite face's ghosts,
         # so the fill must follow the record order
         # (Euler slip walls: no-slip walls two cells apart diverge in the oracle itself)

@@ -4,8 +4,9 @@ through a 405 inlet whose state is the stream's own leaves a zero residual, outw
 face (no mass through it), the no-slip wall drags a tangential stream, an isothermal wall conducts the
 heat k (T_wall - T) / (dy / 2) into a gas at rest, symmetry faces act as the extrapolated faces of a
 transversely uniform tube, a 406 outlet at the stream's pressure passes a subsonic stream unchanged and
-one below it draws more mass out, inward flow closes a 406 face, and classical RK4 converges at fourth
-order in time (SSP-RK3 at third) on a smooth periodic problem."""
+one below it draws more mass out, inward flow closes a 406 face, the 401 / 403 / 404 / 407 inlets fed with the
+stagnation or mass-flux state of a uniform subsonic stream pass it unchanged, and classical RK4 converges at
+fourth order in time (SSP-RK3 at third) on a smooth periodic problem."""
 import math
 
 import numpy as np
@@ -152,6 +153,51 @@ def test_inward_flow_closes_a_406_face():
     # cells at i = max: only the interior face i - 1/2 carries mass (u < 0); cells inside: zero
     assert np.allclose(I[0, -1], rho * 300.0 * A, rtol=1e-12)
     assert np.abs(I[0, 1:-1]).max() <= 1e-12 * rho * 300.0 * A
+
+
+def _inlet_stream(inlet, mach=0.5, outlet=None):
+    """A uniform subsonic stream along +x on a Cartesian 2-block channel: the given type-4 inlet at i = 1, the 406
+    outlet at the stream's pressure at i = max (or `outlet`), symmetry elsewhere."""
+    bc = {1: inlet, 2: outlet or (abi.BC_OUTLET, (1.0e5, 1.0)), 3: SYM, 4: SYM, 5: SYM, 6: SYM}
+    return cs.multiblock_2d(cols=2, rows=1, lo=6, hi=9, seed=4, amp=0.0, bc=bc, visc=0, mach=mach)
+
+
+def _stream_state(mach=0.5, T=300.0, p=1.0e5):
+    th = cs.ideal_gas_tables()
+    R, gam = th["R"], th["gamma"]
+    d = 0.5 * (gam - 1.0)
+    rho = p / (R * T)
+    U = mach * math.sqrt(gam * R * T)
+    T0 = T * (1.0 + d * mach * mach)
+    p0 = p * (1.0 + d * mach * mach) ** (gam / (gam - 1.0))
+    return rho, U, T0, p0
+
+
+@pytest.mark.parametrize("code", [401, 403, 404, 407])
+def test_subsonic_inlets_pass_a_matching_stream(code):
+    rho, U, T0, p0 = _stream_state()
+    if code in (401, 407):
+        q = (0.0, T0, p0, 0.0, 0.0, 1.0, code, 1.0e5)      # stagnation T0, p0 (407: ambient pressure p outwards)
+    elif code == 403:
+        q = (0.0, T0, rho * U, 0.0, 0.0, 1.0, code)        # mass flux, total temperature
+    else:
+        q = (0.0, 300.0, rho * U, 0.0, 0.0, 1.0, code)     # mass flux, static temperature
+    c = _inlet_stream((abi.BC_INFLOW, q))
+    _, P, R = _residual(c)
+    Ri = H.interior_rows(c, R)
+    A = c.blocks[0]["fm1"][3::4].max()
+    scale = np.array([rho * U, rho * U * U, rho * U * U, rho * U * U, rho * U ** 3]) * A
+    assert (np.abs(Ri).max(axis=1) <= 1e-8 * scale).all(), np.abs(Ri).max(axis=1) / scale
+
+
+def test_ambient_boundary_lets_a_stream_out_at_its_pressure():
+    rho, U, T0, p0 = _stream_state()
+    amb = (abi.BC_INFLOW, (0.0, T0, p0, 0.0, 0.0, 1.0, 407, 1.0e5))
+    c = _inlet_stream((abi.BC_INFLOW, (0.5, 300.0, 1.0e5, 0.0, 0.0, 1.0)), outlet=amb)   # 405 in, 407 out
+    _, P, R = _residual(c)
+    Ri = H.interior_rows(c, R)
+    A = c.blocks[0]["fm1"][3::4].max()
+    assert np.abs(Ri[0]).max() <= 1e-8 * rho * U * A
 
 
 def _entropy_wave(n, cfl, n_rk, t_end=0.05):
