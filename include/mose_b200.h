@@ -86,11 +86,24 @@ extern "C" {
 #define MB_RS_HLLE 2
 #define MB_RS_SLAU 3
 #define MB_RS_AUSMP 4
+#define MB_RS_AUSMPM 5
+#define MB_RS_HLLEPP 6
+#define MB_RS_HLLC_TRAMEL 7
 #define MB_RS_LLF 8
 #define MB_RS_SLAU2 9
+#define MB_RS_HLLC_CHEN 10
 #define MB_RS_EXACT 11
 #define MB_RS_LMROE 12
 #define MB_RS_MICZEKROE 13
+
+/* the sensor id in effect (sd_dev): 0 none, 1 Tramel, 2 Chen */
+static inline int mb_effective_sensor(int riemann, int sensor) {
+  if (sensor == 1 || sensor == 2) return sensor;
+  if (sensor == 3) return 0;
+  if (riemann == 6 || riemann == 7) return 1;
+  if (riemann == 5 || riemann == 10) return 2;
+  return 0;
+}
 
 #define MB_PREC_FP64 0
 #define MB_PREC_MIXED 1 /* reconstruction + Riemann + viscous flux arithmetic in FP32; state,
@@ -176,7 +189,10 @@ typedef struct mb_scheme {
   int32_t state_check;/* [MOSE-scheme] state-check (Lib_Newstate.f90:14) */
   int32_t dt_additive;/* dt-rule = additive (dt_blk.inc:79-155; 3-D): the convective and diffusive rates of
                          the three directions add up; 0 = the default min rule (dt_blk.inc:156-191) */
-  int32_t pad0;
+  int32_t sensor;     /* [MOSE-scheme] shock-detector (Assign_SD, Lib_Shock_Detector.f90:22-46): 0 the solver's own
+                         (Tramel for HLLE++ / HLLC+Tramel, Chen for AUSM+M / HLLC+Chen, none otherwise), 1 Tramel,
+                         2 Chen, 3 none. A limiter name with the SD suffix is the Tramel sensor. With a sensor the
+                         cell's beta scales the reconstruction slopes of its faces and goes to their Riemann solver */
   double cfl;
   double vnn;         /* default 0.3 (MOSE_Types_m.f90:268) */
   double prandtl;     /* > 0: kl = mu cp / Pr (Mod_Diffusive.f90:303) */

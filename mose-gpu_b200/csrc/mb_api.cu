@@ -206,6 +206,10 @@ static void free_tables(mb_ctx* c) {
   c->d_tiles_sweep = nullptr; c->d_tiles_aux = nullptr;
 }
 
+// the sweep unit of a scheme: the benchmarked solvers' own (the solver a compile-time constant) unless a shock sensor
+// is on, which only the run-time solver unit carries
+static int sweep_unit(const mb_scheme* sc) { return mb_effective_sensor(sc->riemann, sc->sensor) ? 0 : sc->riemann; }
+
 // record types with physical ghosts (Fill_Ghost_Cell_blk, Lib_Extrapolation.f90:643-730)
 static bool phys_type(int t) {
   return t == MB_BC_EXTRAPOLATION || t == MB_BC_INFLOW || t == MB_BC_WALL || t == MB_BC_SYMMETRY ||
@@ -307,7 +311,7 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
       const int nax = mesh->blk[r.blk].n[ax];
       int layers = 2;
       if (nax >= 2) layers = 1;
-      else if (!sc->visc && all11[3 * r.blk + ax]) layers = 0;
+      else if (!sc->visc && !mb_effective_sensor(sc->riemann, sc->sensor) && all11[3 * r.blk + ax]) layers = 0;
       if (layers == 0) continue;
       physf.push_back(q | (layers << 28));
       if (r.type == MB_BC_EXTRAPOLATION) cubicf.push_back(q | (layers << 28));
@@ -502,10 +506,8 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
 int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int device, mb_ctx** out) {
   if (!mesh || !sc || !th || !out) return MB_E_ARG;
   *out = nullptr;
-  if (sc->riemann != MB_RS_HLLC && sc->riemann != MB_RS_HLLE && sc->riemann != MB_RS_SLAU && sc->riemann != MB_RS_AUSMP &&
-      sc->riemann != MB_RS_LLF && sc->riemann != MB_RS_SLAU2 && sc->riemann != MB_RS_LMROE && sc->riemann != MB_RS_EXACT &&
-      sc->riemann != MB_RS_MICZEKROE)
-    return MB_E_UNSUPPORTED;
+  if (sc->riemann < MB_RS_HLLC || sc->riemann > MB_RS_MICZEKROE) return MB_E_UNSUPPORTED;  // 14 (HLLC-PC) needs prec
+  if (sc->sensor < 0 || sc->sensor > 3) return MB_E_UNSUPPORTED;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
   if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
   if (!(sc->res_stop >= 0.0)) return MB_E_ARG;
@@ -575,7 +577,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   }
   {
     cudaError_t e = (sc->precision == MB_PREC_MIXED)
-                        ? MB_BY_RS(f32, sc->riemann, _setup, ()) : MB_BY_RS(f64, sc->riemann, _setup, ());
+                        ? MB_BY_RS(f32, sweep_unit(sc), _setup, ()) : MB_BY_RS(f64, sweep_unit(sc), _setup, ());
     if (e != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
   }
   // ---- kernel parameters
@@ -588,6 +590,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   p.nc = c->ncell;
   p.tmin = th->tmin; p.tmax = th->tmax;
   p.wm = th->wm; p.ri = RUNIV / th->wm; p.iri = th->wm / RUNIV;
+  p.sd = mb_effective_sensor(sc->riemann, sc->sensor);
   p.lim = sc->limiter; p.rs = sc->riemann; p.visc = sc->visc ? 1 : 0; p.ndir = sc->ndir; p.dt_additive = sc->dt_additive;
   p.guard = sc->visc ? 1 : 0; p.state_check = sc->state_check;
   p.cfl = sc->cfl; p.vnn = sc->vnn; p.prandtl = sc->prandtl; p.schmidt = sc->schmidt; p.mco = sc->mco;
@@ -598,7 +601,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
     const int v = sc->visc ? 1 : 0;
     int occ = (sc->precision == MB_PREC_MIXED)
-                  ? MB_BY_RS(f32, sc->riemann, _occupancy, (v)) : MB_BY_RS(f64, sc->riemann, _occupancy, (v));
+                  ? MB_BY_RS(f32, sweep_unit(sc), _occupancy, (v)) : MB_BY_RS(f64, sweep_unit(sc), _occupancy, (v));
     p.pgrid = std::max(1, occ) * std::max(1, nsm);
   }
   p.queue = nullptr;
@@ -607,7 +610,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   if (getenv("MB_REPORT")) {
     const int v = sc->visc ? 1 : 0;
     int occ = (sc->precision == MB_PREC_MIXED)
-                  ? MB_BY_RS(f32, sc->riemann, _occupancy, (v)) : MB_BY_RS(f64, sc->riemann, _occupancy, (v));
+                  ? MB_BY_RS(f32, sweep_unit(sc), _occupancy, (v)) : MB_BY_RS(f64, sweep_unit(sc), _occupancy, (v));
     fprintf(stderr, "[mose_b200] sweep: %s, %d threads per CTA, %d CTAs per SM, %d tiles\n",
             sc->precision == MB_PREC_MIXED ? "mixed" : "fp64", 32 * c->ty_sweep, occ, c->ntiles_sweep);
   }
@@ -694,9 +697,9 @@ static int sweep_on(mb_ctx* c, const DTile* t, int n, int persistent, int mode, 
   const double rkc = irk > 0 ? rkc_of(c->sc.n_rk, irk) : 0.0;
   cudaError_t e;
   if (c->sc.precision == MB_PREC_MIXED) {
-    e = MB_BY_RS(f32, c->sc.riemann, , (p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s));
+    e = MB_BY_RS(f32, sweep_unit(&c->sc), , (p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s));
   } else {
-    e = MB_BY_RS(f64, c->sc.riemann, , (p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s));
+    e = MB_BY_RS(f64, sweep_unit(&c->sc), , (p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s));
   }
   c->launches += 1;
   CK(e);
@@ -709,9 +712,9 @@ static int records(mb_ctx* c, const double* Pin, cudaStream_t s) {
   const Params& p = c->p;
   cudaError_t e;
   if (c->sc.precision == MB_PREC_MIXED) {
-    e = MB_BY_RS(f32, c->sc.riemann, _records, (p, c->d_brec, c->d_bcell, c->nrec, Pin, s));
+    e = MB_BY_RS(f32, sweep_unit(&c->sc), _records, (p, c->d_brec, c->d_bcell, c->nrec, Pin, s));
   } else {
-    e = MB_BY_RS(f64, c->sc.riemann, _records, (p, c->d_brec, c->d_bcell, c->nrec, Pin, s));
+    e = MB_BY_RS(f64, sweep_unit(&c->sc), _records, (p, c->d_brec, c->d_bcell, c->nrec, Pin, s));
   }
   c->launches += 1;
   CK(e);

@@ -76,7 +76,14 @@ MB_HD void face_flux(const Params& p, const DBlk& b, const Tile<R, TY>& T, int d
   for (int q = 0; q < 4; ++q) dlc[q] = (R)ld(gdl + d + 3 * (l0 + (q - 1) * st));
   const auto* f = Geo<R>::fm(b, d) + fmi32(b, d, i, j, k);
   R nx = (R)ld(f), ny = (R)ld(f + 1), nz = (R)ld(f + 2), area = (R)ld(f + 3);
-  conv_face<R, RS, LIM>(p, pm1, p0, pp1, pp2, dlc, nx, ny, nz, area, out);
+  R bet = (R)1;
+  if (RS == 0 && p.sd) {  // the sensor of the face's left cell (Mod_Fluxes.f90:282-294; conv_cuf: bet = beta(i,j,k))
+    constexpr int VP = MB_IPR * Tile<R, TY>::VS;
+    bet = sd_beta<R>(p.sd, p0[MB_IPR], T.base[T.off(sk, jj, ii - 1) + VP], T.base[T.off(sk, jj, ii + 1) + VP],
+                     T.base[T.off(sk, jj - 1, ii) + VP], T.base[T.off(sk, jj + 1, ii) + VP],
+                     T.base[T.off(skm, jj, ii) + VP], T.base[T.off(sk1, jj, ii) + VP]);
+  }
+  conv_face<R, RS, LIM>(p, pm1, p0, pp1, pp2, dlc, nx, ny, nz, area, out, bet);
   if (!VISC) return;
   // ---- viscous face: cells 1,2 = (c, c+d); 3,4 = c -/+ b-axis; 5,6 = c+d -/+ b; 7,8 = c -/+ c-axis; 9,10 = c+d -/+ c
   int oc[10];
@@ -179,7 +186,15 @@ MB_HD void bc_conn_eul(const Params& p, const DBlk& b, const double* __restrict_
   double g[4];
   bc_face_geom(b, Im, Jm, Km, Fm, g);
   R nx = cvt<R>(g[0]), ny = cvt<R>(g[1]), nz = cvt<R>(g[2]), area = cvt<R>(g[3]);
-  const R beta_ = (R)1;
+  R beta_ = (R)1;
+  if (RS == 0 && p.sd) {  // the sensor of the record's cell (Lib_BC.f90:1811-1818); a mirrored block's k ghosts are
+                          // its k = 1 cells
+    const double* pp = P + MB_IPR * nc;
+    const long long sj = b.pi, sk = b.kmirror ? 0 : (long long)b.pi * b.pj;
+    beta_ = sd_beta<R>(p.sd, cvt<R>(ld(pp + rm)), cvt<R>(ld(pp + rm - 1)), cvt<R>(ld(pp + rm + 1)),
+                       cvt<R>(ld(pp + rm - sj)), cvt<R>(ld(pp + rm + sj)), cvt<R>(ld(pp + rm - sk)),
+                       cvt<R>(ld(pp + rm + sk)));
+  }
   R Dl1 = dlc4[0] * (R)0.5, Dl2 = dlc4[1] * (R)0.5, Dl3 = dlc4[2] * (R)0.5, Dl4 = dlc4[3] * (R)0.5;
   R D12 = Dl1 + Dl2, D23 = Dl2 + Dl3, D34 = Dl3 + Dl4;
   R PL[MB_NP], PR[MB_NP];
@@ -198,7 +213,7 @@ MB_HD void bc_conn_eul(const Params& p, const DBlk& b, const double* __restrict_
   R aR = f_ss(p, PR[0], PR[MB_IPR], rhoR, RRr);
   R F_r, F_u, F_v, F_w, F_E;
   riemann_rec<R, RS>(p, PL[0], PL[MB_IU], PL[MB_IV], PL[MB_IW], PL[MB_IPR], aL, rhoL, RL, PR[0], PR[MB_IU], PR[MB_IV],
-                     PR[MB_IW], PR[MB_IPR], aR, rhoR, RRr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
+                     PR[MB_IW], PR[MB_IPR], aR, rhoR, RRr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E, beta_);
   R su = copysign((R)0.5, F_r), selL = (R)0.5 + su, selR = su - (R)0.5;
   R Fmass = F_r * area;
   R sg = (R)modfm2;
@@ -1256,8 +1271,9 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
   int kb = 0;  // buffer of the k-face above the current plane
   // ghost layers the stencils read: 2 along an axis with faces; for a block one cell deep along j or k (2-D,
   // 1-D) no face of that axis exists and only the viscous transverse gradient reads one ghost layer
-  const int jext = (b.n2 > 1) ? GC : (VISC ? 1 : 0);
-  const int kext = (b.n3 > 1) ? GC : ((VISC && !KM) ? 1 : 0);
+  const bool sens = RS == 0 && p.sd;  // the shock sensor reads the six face neighbours of a cell
+  const int jext = (b.n2 > 1) ? GC : ((VISC || sens) ? 1 : 0);
+  const int kext = (b.n3 > 1) ? GC : (((VISC || sens) && !KM) ? 1 : 0);
   // prologue: planes k0-2 .. k0+1, and the k-face below the first plane
   for (int kk = t.k0 - 2; kk <= t.k0 + 1; ++kk)
     if (kk >= 1 - kext && kk <= b.n3 + kext) stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, kk, jext);

@@ -102,6 +102,7 @@ struct Params {
   int tmin, tmax;
   double wm, ri;
   double iri;              // 1 / ri (the mixed form's state update multiplies by it)
+  int sd;                  // the shock sensor in effect (sd_dev): 0 none, 1 Tramel, 2 Chen
   int lim, rs, visc, ndir, dt_additive, guard, state_check;
   double cfl, vnn, prandtl, schmidt, mco;
   void* recflux;           // boundary-record contributions [record][10] in the flux type (k_records)
@@ -343,7 +344,7 @@ MB_HD R gam_state(const Params& p, R d, R pr, R dtot) {
 }
 
 template <typename R>
-MB_HD void riemann_open(const Params& p, int rs, R dl, R ul, R vl, R wl, R pl, R al, R dltot,
+MB_HD void riemann_open(const Params& p, int rs, R bet, R dl, R ul, R vl, R wl, R pl, R al, R dltot,
                                              R dr, R ur, R vr, R wr, R pr, R ar, R drtot, R nx, R ny, R nz,
                                              R& F_r, R& F_u, R& F_v, R& F_w, R& F_E) {
   R unl = ul * nx + vl * ny + wl * nz;
@@ -380,6 +381,56 @@ MB_HD void riemann_open(const Params& p, int rs, R dl, R ul, R vl, R wl, R pl, R
     F_v = mdotp * vl + mdotm * vr + ny * phalf;
     F_w = mdotp * wl + mdotm * wr + nz * phalf;
     F_E = mdotp * H_L + mdotm * H_R;
+    return;
+  }
+  if (rs == 5) {  // AUSM+M (riemann_open_body.inc:152-242, Chen et al. 2020): the AUSMPW+ sound speed, Mach-number
+                  // function f and the shock gate g of the face sensor bet
+    const R ab = (R)0.125, aa = (R)0.1875, pi_ = (R)3.141592653589793;
+    R Vl2 = ul * ul + vl * vl + wl * wl, Vr2 = ur * ur + vr * vr + wr * wr;
+    R Hs_L = h_static(p, dl, pl);
+    R vel_ = rsqrt_(Vl2);
+    R H_L = Hs_L + (R)0.5 * vel_ * vel_;
+    R gam_L = gam_state(p, dl, pl, dltot);
+    R Hs_R = h_static(p, dr, pr);
+    vel_ = rsqrt_(Vr2);
+    R H_R = Hs_R + (R)0.5 * vel_ * vel_;
+    R gam_R = gam_state(p, dr, pr, drtot);
+    R gam = (R)0.5 * (gam_L + gam_R);
+    R hnorm = (R)0.5 * (Hs_L + Hs_R);
+    R cs = rsqrt_((R)2.0 * (gam - (R)1.0) / (gam + (R)1.0) * hnorm);
+    R c12 = (unl + unr >= (R)0.0) ? cs * cs / mx(fabs(unl), cs) : cs * cs / mx(fabs(unr), cs);
+    R ML = unl / c12, MR = unr / c12;
+    R MplusL, pplusL, MminusR, pminusR;
+    if (fabs(ML) < (R)1.0) {
+      MplusL = (R)0.25 * ((ML + (R)1.0) * (ML + (R)1.0)) + ab * ((ML * ML - (R)1.0) * (ML * ML - (R)1.0));
+      pplusL = (R)0.25 * ((ML + (R)1.0) * (ML + (R)1.0)) * ((R)2.0 - ML) + aa * ML * ((ML * ML - (R)1.0) * (ML * ML - (R)1.0));
+    } else {
+      MplusL = (R)0.5 * (ML + fabs(ML));
+      pplusL = (R)0.5 * ((R)1.0 + copysign((R)1.0, ML));
+    }
+    if (fabs(MR) < (R)1.0) {
+      MminusR = (R)-0.25 * ((MR - (R)1.0) * (MR - (R)1.0)) - ab * ((MR * MR - (R)1.0) * (MR * MR - (R)1.0));
+      pminusR = (R)0.25 * ((MR - (R)1.0) * (MR - (R)1.0)) * ((R)2.0 + MR) - aa * MR * ((MR * MR - (R)1.0) * (MR * MR - (R)1.0));
+    } else {
+      MminusR = (R)0.5 * (MR - fabs(MR));
+      pminusR = (R)0.5 * ((R)1.0 - copysign((R)1.0, MR));
+    }
+    R f_ = (R)0.5 * ((R)1.0 - cos(pi_ * mn((R)1.0, mx(fabs(ML), fabs(MR)))));
+    R g_ = (R)0.5 * ((R)1.0 + cos(pi_ * bet));
+    R rho12 = (R)0.5 * (dltot + drtot);
+    R Mp = (R)-0.5 * ((R)1.0 - f_) * (pr - pl) / (rho12 * c12 * c12) * ((R)1.0 - g_);
+    R M12 = MplusL + MminusR + Mp;
+    R mdot = M12 * c12 * ((M12 >= (R)0.0) ? dltot : drtot);
+    R fo = mn((R)1.0, mx(f_, (R)p.mco));
+    R ps = (R)0.5 * (pl + pr) + (R)0.5 * (pplusL - pminusR) * (pl - pr) + fo * (pplusL + pminusR - (R)1.0) * (R)0.5 * (pl + pr);
+    R gfac = g_ * gam * (pl + pr) / ((R)2.0 * c12) * pplusL * pminusR;
+    R pux = -gfac * (ur - ul), puy = -gfac * (vr - vl), puz = -gfac * (wr - wl);
+    F_r = mdot;
+    if (M12 >= (R)0.0) {
+      F_u = mdot * ul + ps * nx + pux; F_v = mdot * vl + ps * ny + puy; F_w = mdot * wl + ps * nz + puz; F_E = mdot * H_L;
+    } else {
+      F_u = mdot * ur + ps * nx + pux; F_v = mdot * vr + ps * ny + puy; F_w = mdot * wr + ps * nz + puz; F_E = mdot * H_R;
+    }
     return;
   }
   if (rs == 11) {  // exact Godunov (riemann_open_body.inc:348-516): Newton on the star velocity, gamma of each state
@@ -655,6 +706,152 @@ MB_HD void riemann_open(const Params& p, int rs, R dl, R ul, R vl, R wl, R pl, R
   R gam_roe = (R)1 + R_roe / cv_roe;
   R vel2 = u_roe * u_roe + v_roe * v_roe + w_roe * w_roe;
   R a_roe = rsqrt_((gam_roe - (R)1) * (h0_roe - (R)0.5 * vel2 + cv_roe * T_roe - sum_ei));
+  R un_roe = u_roe * nx + v_roe * ny + w_roe * nz;
+  if (rs == 6) {  // HLLE++ (riemann_open_body.inc:728-810): HLLE and Roe wave speeds blended by the face sensor
+    R S1 = mn(mn((R)0.0, unl - al), un_roe - a_roe);
+    R S4 = mx(mx((R)0.0, unr + ar), un_roe + a_roe);
+    R inv_denom = (R)1.0 / (S4 - S1);
+    R lam1_hlle = fabs((S4 + S1) * un_roe * inv_denom - (R)2.0 * S4 * S1 * inv_denom);
+    R lam2_hlle = fabs((S4 + S1) * (un_roe - a_roe) * inv_denom - (R)2.0 * S4 * S1 * inv_denom);
+    R lam3_hlle = fabs((S4 + S1) * (un_roe + a_roe) * inv_denom - (R)2.0 * S4 * S1 * inv_denom);
+    R eps_ = (R)0.3 * (fabs(un_roe) + a_roe);
+    R lam1_roe = fabs(un_roe);
+    R vv = un_roe - a_roe;
+    R lam2_roe = fabs(vv);
+    if (fabs(vv) <= eps_) lam2_roe = (vv * vv + eps_ * eps_) / ((R)2.0 * eps_);
+    vv = un_roe + a_roe;
+    R lam3_roe = fabs(vv);
+    if (fabs(vv) <= eps_) lam3_roe = (vv * vv + eps_ * eps_) / ((R)2.0 * eps_);
+    R lam1_pp = bet * lam1_roe + ((R)1.0 - bet) * lam1_hlle;
+    R lam2_pp = bet * lam2_roe + ((R)1.0 - bet) * lam2_hlle;
+    R lam3_pp = bet * lam3_roe + ((R)1.0 - bet) * lam3_hlle;
+    R rL = (R)0.0 + dl;
+    R FrL = rL * (ul * nx + vl * ny + wl * nz);
+    R Ful = FrL * ul + pl * nx, Fvl = FrL * vl + pl * ny, Fwl = FrL * wl + pl * nz;
+    R Hs_L = h_static(p, dl, pl);
+    R vel_ = rsqrt_(ul * ul + vl * vl + wl * wl);
+    R Fel = FrL * (Hs_L + (R)0.5 * vel_ * vel_);
+    R rR = (R)0.0 + dr;
+    R FrR = rR * (ur * nx + vr * ny + wr * nz);
+    R Fur = FrR * ur + pr * nx, Fvr = FrR * vr + pr * ny, Fwr = FrR * wr + pr * nz;
+    R Hs_R = h_static(p, dr, pr);
+    vel_ = rsqrt_(ur * ur + vr * vr + wr * wr);
+    R Fer = FrR * (Hs_R + (R)0.5 * vel_ * vel_);
+    F_r = (R)0.5 * (FrL + FrR); F_u = (R)0.5 * (Ful + Fur); F_v = (R)0.5 * (Fvl + Fvr); F_w = (R)0.5 * (Fwl + Fwr);
+    F_E = (R)0.5 * (Fel + Fer);
+    R drho = drtot - dltot, dp = pr - pl, du = ur - ul, dv = vr - vl, dw = wr - wl, dun = unr - unl;
+    R t1x, t1y, t1z;
+    if (fabs(nx) < (R)0.9) { t1x = (R)0.0; t1y = -nz; t1z = ny; } else { t1x = -nz; t1y = (R)0.0; t1z = nx; }
+    R normt = rsqrt_(t1x * t1x + t1y * t1y + t1z * t1z);
+    t1x = t1x / normt; t1y = t1y / normt; t1z = t1z / normt;
+    R t2x = ny * t1z - nz * t1y, t2y = nz * t1x - nx * t1z, t2z = nx * t1y - ny * t1x;
+    R alpha_m = (dp - rho_roe * a_roe * dun) / ((R)2.0 * a_roe * a_roe);
+    R alpha_c = drho - dp / (a_roe * a_roe);
+    R alpha_s1 = rho_roe * (du * t1x + dv * t1y + dw * t1z);
+    R alpha_s2 = rho_roe * (du * t2x + dv * t2y + dw * t2z);
+    R alpha_p = (dp + rho_roe * a_roe * dun) / ((R)2.0 * a_roe * a_roe);
+    F_r = F_r - (R)0.5 * (alpha_c * lam1_pp + alpha_m * lam2_pp + alpha_p * lam3_pp);
+    F_u = F_u - (R)0.5 * (alpha_c * lam1_pp * u_roe);
+    F_v = F_v - (R)0.5 * (alpha_c * lam1_pp * v_roe);
+    F_w = F_w - (R)0.5 * (alpha_c * lam1_pp * w_roe);
+    F_u = F_u - (R)0.5 * lam1_pp * (alpha_s1 * t1x + alpha_s2 * t2x);
+    F_v = F_v - (R)0.5 * lam1_pp * (alpha_s1 * t1y + alpha_s2 * t2y);
+    F_w = F_w - (R)0.5 * lam1_pp * (alpha_s1 * t1z + alpha_s2 * t2z);
+    F_u = F_u - (R)0.5 * (alpha_m * lam2_pp * (u_roe - a_roe * nx) + alpha_p * lam3_pp * (u_roe + a_roe * nx));
+    F_v = F_v - (R)0.5 * (alpha_m * lam2_pp * (v_roe - a_roe * ny) + alpha_p * lam3_pp * (v_roe + a_roe * ny));
+    F_w = F_w - (R)0.5 * (alpha_m * lam2_pp * (w_roe - a_roe * nz) + alpha_p * lam3_pp * (w_roe + a_roe * nz));
+    F_E = F_E - (R)0.5 * lam1_pp * (alpha_c * (R)0.5 * (u_roe * u_roe + v_roe * v_roe + w_roe * w_roe));
+    F_E = F_E - (R)0.5 * lam1_pp *
+                    (alpha_s1 * (u_roe * t1x + v_roe * t1y + w_roe * t1z) + alpha_s2 * (u_roe * t2x + v_roe * t2y + w_roe * t2z));
+    F_E = F_E - (R)0.5 * (alpha_m * lam2_pp * (h0_roe - a_roe * un_roe) + alpha_p * lam3_pp * (h0_roe + a_roe * un_roe));
+    return;
+  }
+  if (rs == 7 || rs == 10) {  // HLLC+Tramel (:811-880) and HLLC+Chen (:881-964): HLLC with the face sensor
+    R S1 = mn(mn((R)0.0, unl - al), un_roe - a_roe);
+    R S4 = mx(mx((R)0.0, unr + ar), un_roe + a_roe);
+    R FrE = (R)0.0, FuE = (R)0.0, FvE = (R)0.0, FwE = (R)0.0, FeE = (R)0.0;
+    if (rs == 7) {  // riemann_HLLE
+      R inv_denom = (R)1.0 / (S4 - S1);
+      R FrL = dltot * unl, FrR = drtot * unr;
+      FrE = (S4 * FrL - S1 * FrR + S1 * S4 * (drtot - dltot)) * inv_denom;
+      FuE = (S4 * (FrL * ul + pl * nx) - S1 * (FrR * ur + pr * nx) + S1 * S4 * (drtot * ur - dltot * ul)) * inv_denom;
+      FvE = (S4 * (FrL * vl + pl * ny) - S1 * (FrR * vr + pr * ny) + S1 * S4 * (drtot * vr - dltot * vl)) * inv_denom;
+      FwE = (S4 * (FrL * wl + pl * nz) - S1 * (FrR * wr + pr * nz) + S1 * S4 * (drtot * wr - dltot * wl)) * inv_denom;
+      FeE = (S4 * (FrL * h0l) - S1 * (FrR * h0r) + S1 * S4 * (drtot * (h0r - pr / drtot) - dltot * (h0l - pl / dltot))) *
+            inv_denom;
+    }
+    R e0l = h0l - pl / dltot, e0r = h0r - pr / drtot;
+    R inv_denom = (R)1.0 / (dltot * (S1 - unl) - drtot * (S4 - unr));
+    R Sstar = (pr - pl + dltot * unl * (S1 - unl) - drtot * unr * (S4 - unr)) * inv_denom;
+    R pstar = dltot * (unl - S1) * (unl - Sstar) + pl;
+    R ch_pref = (R)0.0, ch_fstar = (R)0.0, ch_g = (R)0.0, ch_dU = (R)0.0, ch_dutx = (R)0.0, ch_duty = (R)0.0, ch_dutz = (R)0.0;
+    if (rs == 10) {  // the Chen all-speed terms (the sensor h of the face is bet)
+      R ch_phiL = dltot * (S1 - unl), ch_phiR = drtot * (S4 - unr);
+      ch_pref = ch_phiL * ch_phiR / (ch_phiR - ch_phiL);
+      R ch_Mloc = mn((R)1.0, mx(rsqrt_(ul * ul + vl * vl + wl * wl) / al,
+                                              rsqrt_(ur * ur + vr * vr + wr * wr) / ar));
+      ch_Mloc = mx((R)p.mco, ch_Mloc);
+      R om = (R)1.0 - ch_Mloc * ch_Mloc;
+      R ch_fM = ch_Mloc * rsqrt_((R)4.0 + om * om) / ((R)1.0 + ch_Mloc * ch_Mloc);
+      ch_g = (R)1.0 - powr(bet, ch_Mloc);
+      ch_fstar = ch_fM + ch_g * ((R)1.0 - ch_fM);
+      ch_dU = unr - unl;
+      ch_dutx = (ur - ul) - ch_dU * nx; ch_duty = (vr - vl) - ch_dU * ny; ch_dutz = (wr - wl) - ch_dU * nz;
+    }
+    R FrC, FuC, FvC, FwC, FeC;
+    if (S1 >= (R)0.0) {
+      FrC = dltot * unl; FuC = FrC * ul + pl * nx; FvC = FrC * vl + pl * ny; FwC = FrC * wl + pl * nz; FeC = FrC * h0l;
+    } else if (Sstar >= (R)0.0) {
+      FrC = dltot * unl; FuC = FrC * ul + pl * nx; FvC = FrC * vl + pl * ny; FwC = FrC * wl + pl * nz; FeC = FrC * h0l;
+      R id = (R)1.0 / (S1 - Sstar);
+      R U1S = dltot * (S1 - unl) * id;
+      R U2S = ((S1 - unl) * dltot * ul + (pstar - pl) * nx) * id;
+      R U3S = ((S1 - unl) * dltot * vl + (pstar - pl) * ny) * id;
+      R U4S = ((S1 - unl) * dltot * wl + (pstar - pl) * nz) * id;
+      R U5S = ((S1 - unl) * dltot * e0l - pl * unl + pstar * Sstar) * id;
+      FrC = FrC + S1 * (U1S - dltot); FuC = FuC + S1 * (U2S - dltot * ul); FvC = FvC + S1 * (U3S - dltot * vl);
+      FwC = FwC + S1 * (U4S - dltot * wl); FeC = FeC + S1 * (U5S - dltot * e0l);
+      if (rs == 10) {
+        R ch_SK = S1;
+        R ch_lm = ch_pref * (ch_fstar - (R)1.0) * ch_dU;
+        R ch_sh = ch_pref * (ch_SK / (ch_SK - Sstar)) * ch_g;
+        FuC = FuC + ch_lm * nx + ch_sh * ch_dutx;
+        FvC = FvC + ch_lm * ny + ch_sh * ch_duty;
+        FwC = FwC + ch_lm * nz + ch_sh * ch_dutz;
+        FeC = FeC + ch_lm * Sstar;
+      }
+    } else if (S4 > (R)0.0) {
+      FrC = drtot * unr; FuC = FrC * ur + pr * nx; FvC = FrC * vr + pr * ny; FwC = FrC * wr + pr * nz; FeC = FrC * h0r;
+      R id = (R)1.0 / (S4 - Sstar);
+      R U1S = drtot * (S4 - unr) * id;
+      R U2S = ((S4 - unr) * drtot * ur + (pstar - pr) * nx) * id;
+      R U3S = ((S4 - unr) * drtot * vr + (pstar - pr) * ny) * id;
+      R U4S = ((S4 - unr) * drtot * wr + (pstar - pr) * nz) * id;
+      R U5S = ((S4 - unr) * drtot * e0r - pr * unr + pstar * Sstar) * id;
+      FrC = FrC + S4 * (U1S - drtot); FuC = FuC + S4 * (U2S - drtot * ur); FvC = FvC + S4 * (U3S - drtot * vr);
+      FwC = FwC + S4 * (U4S - drtot * wr); FeC = FeC + S4 * (U5S - drtot * e0r);
+      if (rs == 10) {
+        R ch_SK = S4;
+        R ch_lm = ch_pref * (ch_fstar - (R)1.0) * ch_dU;
+        R ch_sh = ch_pref * (ch_SK / (ch_SK - Sstar)) * ch_g;
+        FuC = FuC + ch_lm * nx + ch_sh * ch_dutx;
+        FvC = FvC + ch_lm * ny + ch_sh * ch_duty;
+        FwC = FwC + ch_lm * nz + ch_sh * ch_dutz;
+        FeC = FeC + ch_lm * Sstar;
+      }
+    } else {
+      FrC = drtot * unr; FuC = FrC * ur + pr * nx; FvC = FrC * vr + pr * ny; FwC = FrC * wr + pr * nz; FeC = FrC * h0r;
+    }
+    if (rs == 10 || bet >= (R)1.0) {
+      F_r = FrC; F_u = FuC; F_v = FvC; F_w = FwC; F_E = FeC;
+    } else if (bet == (R)0.0) {
+      F_r = FrE; F_u = FuE; F_v = FvE; F_w = FwE; F_E = FeE;
+    } else {
+      F_r = bet * FrC + ((R)1.0 - bet) * FrE; F_u = bet * FuC + ((R)1.0 - bet) * FuE; F_v = bet * FvC + ((R)1.0 - bet) * FvE;
+      F_w = bet * FwC + ((R)1.0 - bet) * FwE; F_E = bet * FeC + ((R)1.0 - bet) * FeE;
+    }
+    return;
+  }
   if (Fast<R>::on) {
     // The mixed form evaluates the same flux with fewer operations: the face normal is already a unit vector,
     // the two tangential waves together are the tangential part of the velocity jump, (du - dun n), and the
@@ -956,16 +1153,45 @@ MB_HD void hllc(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R 
   }
 }
 
+// The shock sensor of a cell from its pressure and its six face neighbours' (SD_beta, Lib_Shock_Detector.f90:51-81):
+// 1 Tramel (1 smooth, 0 at a shock), 2 Chen (the smallest neighbour pressure ratio), 1 otherwise
+template <typename R>
+MB_HD R sd_beta(int id, R pc, R p1, R p2, R p3, R p4, R p5, R p6) {
+  if (id == 1) {
+    const R DELTA = (R)20;
+    R kp1 = fabs((p2 - (R)2 * pc + p1) / (p2 + (R)2 * pc + p1));
+    R kp2 = fabs((p4 - (R)2 * pc + p3) / (p4 + (R)2 * pc + p3));
+    R kp3 = fabs((p6 - (R)2 * pc + p5) / (p6 + (R)2 * pc + p5));
+    R sw = mx(mx(kp1, kp2), kp3);
+    if (sw < (R)1 / DELTA) {
+      R phi = mx(sw / DELTA, (R)0);
+      return (R)1 - tanh((R)10 * phi * phi * phi);
+    }
+    return (R)0;
+  }
+  if (id == 2) {
+    R beta = (R)1;
+    beta = mn(beta, mn(pc, p1) / mx(pc, p1));
+    beta = mn(beta, mn(pc, p2) / mx(pc, p2));
+    beta = mn(beta, mn(pc, p3) / mx(pc, p3));
+    beta = mn(beta, mn(pc, p4) / mx(pc, p4));
+    beta = mn(beta, mn(pc, p5) / mx(pc, p5));
+    beta = mn(beta, mn(pc, p6) / mx(pc, p6));
+    return beta;
+  }
+  return (R)1;
+}
+
 // ---- interior convective face from the 4-cell stencil (conv_physics.inc) ----
 // RS / LIM: the Riemann solver and limiter ids fixed at compile time (0: read p.rs / p.lim at run time)
 template <typename R, int RS = 0, int LIM = 0>
 MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, const R* pp2,
-                                          const R* dlc, R nx, R ny, R nz, R area, R* res0) {
+                                          const R* dlc, R nx, R ny, R nz, R area, R* res0, R bet = (R)1) {
   const int rs = RS ? RS : p.rs;
   const int lim = LIM ? LIM : p.lim;
   R l0 = (R)0.5 * (dlc[0] + dlc[1]), l1 = (R)0.5 * (dlc[1] + dlc[2]), l2 = (R)0.5 * (dlc[2] + dlc[3]);
   R lm = (R)0.5 * dlc[1], lp = (R)0.5 * dlc[2];
-  const R beta_order = (R)1;
+  const R beta_order = (RS == 0 && p.sd) ? bet : (R)1;  // SD_space_order: the slopes scaled by the face sensor
   R idl0 = (R)1 / l0, idl1 = (R)1 / l1, idl2 = (R)1 / l2;
   R P1[MB_NP], P4[MB_NP];
 #pragma unroll
@@ -1011,7 +1237,7 @@ MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, c
          Fast<R>::on ? th1 : nullptr, Fast<R>::on ? th4 : nullptr, Ti1, Ti4, rs);
   }
   else
-    riemann_open(p, rs, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], a1, rotot1, P4[0], P4[MB_IU],
+    riemann_open(p, rs, bet, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], a1, rotot1, P4[0], P4[MB_IU],
                  P4[MB_IV], P4[MB_IW], P4[MB_IPR], a4, rotot4, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
   if (Fast<R>::on) {
     res0[0] = F_r * area;  // one species: the upwinded mass fraction is 1
@@ -1027,7 +1253,8 @@ MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, c
 // 2 (both after roe_averages), SLAU for 3, the MOSE_open solvers otherwise
 template <typename R, int RS = 0>
 MB_HD void riemann_rec(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R Rl, R dr, R ur, R vr, R wr,
-                       R pr, R ar, R drtot, R Rr, R nx, R ny, R nz, R& F_r, R& F_u, R& F_v, R& F_w, R& F_E) {
+                       R pr, R ar, R drtot, R Rr, R nx, R ny, R nz, R& F_r, R& F_u, R& F_v, R& F_w, R& F_E,
+                       R bet = (R)1) {
   const int rs = RS ? RS : p.rs;
   if (rs == 1 || rs == 2)
     hllc(p, dl, ul, vl, wl, pl, al, dltot, Rl, dr, ur, vr, wr, pr, ar, drtot, Rr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E,
@@ -1035,7 +1262,7 @@ MB_HD void riemann_rec(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dl
   else if (rs == 3)
     slau_rec(p, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
   else
-    riemann_open(p, rs, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r, F_u, F_v, F_w,
+    riemann_open(p, rs, bet, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r, F_u, F_v, F_w,
                  F_E);
 }
 

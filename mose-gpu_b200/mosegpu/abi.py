@@ -42,6 +42,8 @@ BC_OUTLET = 24      # q = (exit pressure, relaxation factor)
 LIM_MINMOD, LIM_VANLEER, LIM_VANALBADA, LIM_MC, LIM_SUPERBEE, LIM_FIRST = 1, 2, 3, 4, 5, 6
 RS_HLLC, RS_HLLE, RS_SLAU, RS_AUSMP, RS_LLF, RS_SLAU2, RS_LMROE = 1, 2, 3, 4, 8, 9, 12
 RS_EXACT, RS_MICZEKROE = 11, 13
+RS_AUSMPM, RS_HLLEPP, RS_HLLC_TRAMEL, RS_HLLC_CHEN = 5, 6, 7, 10
+SENSOR_DEFAULT, SENSOR_TRAMEL, SENSOR_CHEN, SENSOR_NONE = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 
 
@@ -77,7 +79,7 @@ class MBThermo(C.Structure):
 class MBScheme(C.Structure):
     _fields_ = [("limiter", C.c_int32), ("riemann", C.c_int32), ("visc", C.c_int32), ("n_rk", C.c_int32),
                 ("precision", C.c_int32), ("ndir", C.c_int32), ("time_clip", C.c_int32),
-                ("state_check", C.c_int32), ("dt_additive", C.c_int32), ("pad0", C.c_int32),
+                ("state_check", C.c_int32), ("dt_additive", C.c_int32), ("sensor", C.c_int32),
                 ("cfl", C.c_double), ("vnn", C.c_double),
                 ("prandtl", C.c_double), ("schmidt", C.c_double), ("mco", C.c_double),
                 ("time_threshold", C.c_double), ("res_stop", C.c_double)]

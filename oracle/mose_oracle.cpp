@@ -74,6 +74,7 @@ struct Ctx {
   std::vector<mb_conn> conn;
   int64_t ncell;
   mb_scheme sc;
+  int sd = 0;               // the shock sensor (sd_dev): 0 none, 1 Tramel, 2 Chen
   Thermo th;
   std::vector<double> pg;  // bc_pg(nprim, 6, nrec) of the connection records
   std::vector<double> acc4; // RK4: the conserved accumulator Un + dt (k1/6 + k2/3 + ...), (ncell, nprim)
@@ -273,7 +274,7 @@ inline double gam_state(const Thermo& th, double d, double p, double dtot) {
   return cp_ / (cp_ - rg_);
 }
 
-void riemann_open(const Thermo& th, int rs, double mco, double dl, double ul, double vl, double wl,
+void riemann_open(const Thermo& th, int rs, double mco, double bet, double dl, double ul, double vl, double wl,
                   double pl, double al, double dltot, double dr, double ur, double vr, double wr, double pr,
                   double ar, double drtot, double nx, double ny, double nz, double& F_r, double& F_u,
                   double& F_v, double& F_w, double& F_E) {
@@ -311,6 +312,56 @@ void riemann_open(const Thermo& th, int rs, double mco, double dl, double ul, do
     F_v = mdotp * vl + mdotm * vr + ny * phalf;
     F_w = mdotp * wl + mdotm * wr + nz * phalf;
     F_E = mdotp * H_L + mdotm * H_R;
+    return;
+  }
+  if (rs == 5) {  // AUSM+M (riemann_open_body.inc:152-242, Chen et al. 2020): the AUSMPW+ sound speed, Mach-number
+                  // function f and the shock gate g of the face sensor bet
+    const double ab = 0.125, aa = 0.1875, pi_ = 3.141592653589793;
+    double Vl2 = ul * ul + vl * vl + wl * wl, Vr2 = ur * ur + vr * vr + wr * wr;
+    double Hs_L = h_static(th, dl, pl);
+    double vel_ = std::sqrt(Vl2);
+    double H_L = Hs_L + 0.5 * vel_ * vel_;
+    double gam_L = gam_state(th, dl, pl, dltot);
+    double Hs_R = h_static(th, dr, pr);
+    vel_ = std::sqrt(Vr2);
+    double H_R = Hs_R + 0.5 * vel_ * vel_;
+    double gam_R = gam_state(th, dr, pr, drtot);
+    double gam = 0.5 * (gam_L + gam_R);
+    double hnorm = 0.5 * (Hs_L + Hs_R);
+    double cs = std::sqrt(2.0 * (gam - 1.0) / (gam + 1.0) * hnorm);
+    double c12 = (unl + unr >= 0.0) ? cs * cs / std::max(std::fabs(unl), cs) : cs * cs / std::max(std::fabs(unr), cs);
+    double ML = unl / c12, MR = unr / c12;
+    double MplusL, pplusL, MminusR, pminusR;
+    if (std::fabs(ML) < 1.0) {
+      MplusL = 0.25 * ((ML + 1.0) * (ML + 1.0)) + ab * ((ML * ML - 1.0) * (ML * ML - 1.0));
+      pplusL = 0.25 * ((ML + 1.0) * (ML + 1.0)) * (2.0 - ML) + aa * ML * ((ML * ML - 1.0) * (ML * ML - 1.0));
+    } else {
+      MplusL = 0.5 * (ML + std::fabs(ML));
+      pplusL = 0.5 * (1.0 + std::copysign(1.0, ML));
+    }
+    if (std::fabs(MR) < 1.0) {
+      MminusR = -0.25 * ((MR - 1.0) * (MR - 1.0)) - ab * ((MR * MR - 1.0) * (MR * MR - 1.0));
+      pminusR = 0.25 * ((MR - 1.0) * (MR - 1.0)) * (2.0 + MR) - aa * MR * ((MR * MR - 1.0) * (MR * MR - 1.0));
+    } else {
+      MminusR = 0.5 * (MR - std::fabs(MR));
+      pminusR = 0.5 * (1.0 - std::copysign(1.0, MR));
+    }
+    double f_ = 0.5 * (1.0 - std::cos(pi_ * std::min(1.0, std::max(std::fabs(ML), std::fabs(MR)))));
+    double g_ = 0.5 * (1.0 + std::cos(pi_ * bet));
+    double rho12 = 0.5 * (dltot + drtot);
+    double Mp = -0.5 * (1.0 - f_) * (pr - pl) / (rho12 * c12 * c12) * (1.0 - g_);
+    double M12 = MplusL + MminusR + Mp;
+    double mdot = M12 * c12 * ((M12 >= 0.0) ? dltot : drtot);
+    double fo = std::min(1.0, std::max(f_, mco));
+    double ps = 0.5 * (pl + pr) + 0.5 * (pplusL - pminusR) * (pl - pr) + fo * (pplusL + pminusR - 1.0) * 0.5 * (pl + pr);
+    double gfac = g_ * gam * (pl + pr) / (2.0 * c12) * pplusL * pminusR;
+    double pux = -gfac * (ur - ul), puy = -gfac * (vr - vl), puz = -gfac * (wr - wl);
+    F_r = mdot;
+    if (M12 >= 0.0) {
+      F_u = mdot * ul + ps * nx + pux; F_v = mdot * vl + ps * ny + puy; F_w = mdot * wl + ps * nz + puz; F_E = mdot * H_L;
+    } else {
+      F_u = mdot * ur + ps * nx + pux; F_v = mdot * vr + ps * ny + puy; F_w = mdot * wr + ps * nz + puz; F_E = mdot * H_R;
+    }
     return;
   }
   if (rs == 11) {  // exact Godunov (riemann_open_body.inc:348-516): Newton on the star velocity, gamma of each state
@@ -541,7 +592,7 @@ void riemann_open(const Thermo& th, int rs, double mco, double dl, double ul, do
     }
     return;
   }
-  // rs == 12: Roe averages (riemann_open_body.inc:679-730) then LMRoe (:965-1091)
+  // rs 6, 7, 10, 12: Roe averages (riemann_open_body.inc:679-730), then HLLE++, HLLC+Tramel, HLLC+Chen or LMRoe
   double rho_ = 0.0 + dl;
   double Rl = 0.0 + th.ri * dl / rho_;
   rho_ = 0.0 + dr;
@@ -578,6 +629,152 @@ void riemann_open(const Thermo& th, int rs, double mco, double dl, double ul, do
   double gam_roe = 1.0 + R_roe / cv_roe;
   double vel2 = u_roe * u_roe + v_roe * v_roe + w_roe * w_roe;
   double a_roe = std::sqrt((gam_roe - 1.0) * (h0_roe - 0.5 * vel2 + cv_roe * T_roe - sum_ei));
+  double un_roe = u_roe * nx + v_roe * ny + w_roe * nz;
+  if (rs == 6) {  // HLLE++ (riemann_open_body.inc:728-810): HLLE and Roe wave speeds blended by the face sensor
+    double S1 = std::min(std::min(0.0, unl - al), un_roe - a_roe);
+    double S4 = std::max(std::max(0.0, unr + ar), un_roe + a_roe);
+    double inv_denom = 1.0 / (S4 - S1);
+    double lam1_hlle = std::fabs((S4 + S1) * un_roe * inv_denom - 2.0 * S4 * S1 * inv_denom);
+    double lam2_hlle = std::fabs((S4 + S1) * (un_roe - a_roe) * inv_denom - 2.0 * S4 * S1 * inv_denom);
+    double lam3_hlle = std::fabs((S4 + S1) * (un_roe + a_roe) * inv_denom - 2.0 * S4 * S1 * inv_denom);
+    double eps_ = 0.3 * (std::fabs(un_roe) + a_roe);
+    double lam1_roe = std::fabs(un_roe);
+    double vv = un_roe - a_roe;
+    double lam2_roe = std::fabs(vv);
+    if (std::fabs(vv) <= eps_) lam2_roe = (vv * vv + eps_ * eps_) / (2.0 * eps_);
+    vv = un_roe + a_roe;
+    double lam3_roe = std::fabs(vv);
+    if (std::fabs(vv) <= eps_) lam3_roe = (vv * vv + eps_ * eps_) / (2.0 * eps_);
+    double lam1_pp = bet * lam1_roe + (1.0 - bet) * lam1_hlle;
+    double lam2_pp = bet * lam2_roe + (1.0 - bet) * lam2_hlle;
+    double lam3_pp = bet * lam3_roe + (1.0 - bet) * lam3_hlle;
+    double rL = 0.0 + dl;
+    double FrL = rL * (ul * nx + vl * ny + wl * nz);
+    double Ful = FrL * ul + pl * nx, Fvl = FrL * vl + pl * ny, Fwl = FrL * wl + pl * nz;
+    double Hs_L = h_static(th, dl, pl);
+    double vel_ = std::sqrt(ul * ul + vl * vl + wl * wl);
+    double Fel = FrL * (Hs_L + 0.5 * vel_ * vel_);
+    double rR = 0.0 + dr;
+    double FrR = rR * (ur * nx + vr * ny + wr * nz);
+    double Fur = FrR * ur + pr * nx, Fvr = FrR * vr + pr * ny, Fwr = FrR * wr + pr * nz;
+    double Hs_R = h_static(th, dr, pr);
+    vel_ = std::sqrt(ur * ur + vr * vr + wr * wr);
+    double Fer = FrR * (Hs_R + 0.5 * vel_ * vel_);
+    F_r = 0.5 * (FrL + FrR); F_u = 0.5 * (Ful + Fur); F_v = 0.5 * (Fvl + Fvr); F_w = 0.5 * (Fwl + Fwr);
+    F_E = 0.5 * (Fel + Fer);
+    double drho = drtot - dltot, dp = pr - pl, du = ur - ul, dv = vr - vl, dw = wr - wl, dun = unr - unl;
+    double t1x, t1y, t1z;
+    if (std::fabs(nx) < 0.9) { t1x = 0.0; t1y = -nz; t1z = ny; } else { t1x = -nz; t1y = 0.0; t1z = nx; }
+    double normt = std::sqrt(t1x * t1x + t1y * t1y + t1z * t1z);
+    t1x = t1x / normt; t1y = t1y / normt; t1z = t1z / normt;
+    double t2x = ny * t1z - nz * t1y, t2y = nz * t1x - nx * t1z, t2z = nx * t1y - ny * t1x;
+    double alpha_m = (dp - rho_roe * a_roe * dun) / (2.0 * a_roe * a_roe);
+    double alpha_c = drho - dp / (a_roe * a_roe);
+    double alpha_s1 = rho_roe * (du * t1x + dv * t1y + dw * t1z);
+    double alpha_s2 = rho_roe * (du * t2x + dv * t2y + dw * t2z);
+    double alpha_p = (dp + rho_roe * a_roe * dun) / (2.0 * a_roe * a_roe);
+    F_r = F_r - 0.5 * (alpha_c * lam1_pp + alpha_m * lam2_pp + alpha_p * lam3_pp);
+    F_u = F_u - 0.5 * (alpha_c * lam1_pp * u_roe);
+    F_v = F_v - 0.5 * (alpha_c * lam1_pp * v_roe);
+    F_w = F_w - 0.5 * (alpha_c * lam1_pp * w_roe);
+    F_u = F_u - 0.5 * lam1_pp * (alpha_s1 * t1x + alpha_s2 * t2x);
+    F_v = F_v - 0.5 * lam1_pp * (alpha_s1 * t1y + alpha_s2 * t2y);
+    F_w = F_w - 0.5 * lam1_pp * (alpha_s1 * t1z + alpha_s2 * t2z);
+    F_u = F_u - 0.5 * (alpha_m * lam2_pp * (u_roe - a_roe * nx) + alpha_p * lam3_pp * (u_roe + a_roe * nx));
+    F_v = F_v - 0.5 * (alpha_m * lam2_pp * (v_roe - a_roe * ny) + alpha_p * lam3_pp * (v_roe + a_roe * ny));
+    F_w = F_w - 0.5 * (alpha_m * lam2_pp * (w_roe - a_roe * nz) + alpha_p * lam3_pp * (w_roe + a_roe * nz));
+    F_E = F_E - 0.5 * lam1_pp * (alpha_c * 0.5 * (u_roe * u_roe + v_roe * v_roe + w_roe * w_roe));
+    F_E = F_E - 0.5 * lam1_pp *
+                    (alpha_s1 * (u_roe * t1x + v_roe * t1y + w_roe * t1z) + alpha_s2 * (u_roe * t2x + v_roe * t2y + w_roe * t2z));
+    F_E = F_E - 0.5 * (alpha_m * lam2_pp * (h0_roe - a_roe * un_roe) + alpha_p * lam3_pp * (h0_roe + a_roe * un_roe));
+    return;
+  }
+  if (rs == 7 || rs == 10) {  // HLLC+Tramel (:811-880) and HLLC+Chen (:881-964): HLLC with the face sensor
+    double S1 = std::min(std::min(0.0, unl - al), un_roe - a_roe);
+    double S4 = std::max(std::max(0.0, unr + ar), un_roe + a_roe);
+    double FrE = 0.0, FuE = 0.0, FvE = 0.0, FwE = 0.0, FeE = 0.0;
+    if (rs == 7) {  // riemann_HLLE
+      double inv_denom = 1.0 / (S4 - S1);
+      double FrL = dltot * unl, FrR = drtot * unr;
+      FrE = (S4 * FrL - S1 * FrR + S1 * S4 * (drtot - dltot)) * inv_denom;
+      FuE = (S4 * (FrL * ul + pl * nx) - S1 * (FrR * ur + pr * nx) + S1 * S4 * (drtot * ur - dltot * ul)) * inv_denom;
+      FvE = (S4 * (FrL * vl + pl * ny) - S1 * (FrR * vr + pr * ny) + S1 * S4 * (drtot * vr - dltot * vl)) * inv_denom;
+      FwE = (S4 * (FrL * wl + pl * nz) - S1 * (FrR * wr + pr * nz) + S1 * S4 * (drtot * wr - dltot * wl)) * inv_denom;
+      FeE = (S4 * (FrL * h0l) - S1 * (FrR * h0r) + S1 * S4 * (drtot * (h0r - pr / drtot) - dltot * (h0l - pl / dltot))) *
+            inv_denom;
+    }
+    double e0l = h0l - pl / dltot, e0r = h0r - pr / drtot;
+    double inv_denom = 1.0 / (dltot * (S1 - unl) - drtot * (S4 - unr));
+    double Sstar = (pr - pl + dltot * unl * (S1 - unl) - drtot * unr * (S4 - unr)) * inv_denom;
+    double pstar = dltot * (unl - S1) * (unl - Sstar) + pl;
+    double ch_pref = 0.0, ch_fstar = 0.0, ch_g = 0.0, ch_dU = 0.0, ch_dutx = 0.0, ch_duty = 0.0, ch_dutz = 0.0;
+    if (rs == 10) {  // the Chen all-speed terms (the sensor h of the face is bet)
+      double ch_phiL = dltot * (S1 - unl), ch_phiR = drtot * (S4 - unr);
+      ch_pref = ch_phiL * ch_phiR / (ch_phiR - ch_phiL);
+      double ch_Mloc = std::min(1.0, std::max(std::sqrt(ul * ul + vl * vl + wl * wl) / al,
+                                              std::sqrt(ur * ur + vr * vr + wr * wr) / ar));
+      ch_Mloc = std::max(mco, ch_Mloc);
+      double om = 1.0 - ch_Mloc * ch_Mloc;
+      double ch_fM = ch_Mloc * std::sqrt(4.0 + om * om) / (1.0 + ch_Mloc * ch_Mloc);
+      ch_g = 1.0 - std::pow(bet, ch_Mloc);
+      ch_fstar = ch_fM + ch_g * (1.0 - ch_fM);
+      ch_dU = unr - unl;
+      ch_dutx = (ur - ul) - ch_dU * nx; ch_duty = (vr - vl) - ch_dU * ny; ch_dutz = (wr - wl) - ch_dU * nz;
+    }
+    double FrC, FuC, FvC, FwC, FeC;
+    if (S1 >= 0.0) {
+      FrC = dltot * unl; FuC = FrC * ul + pl * nx; FvC = FrC * vl + pl * ny; FwC = FrC * wl + pl * nz; FeC = FrC * h0l;
+    } else if (Sstar >= 0.0) {
+      FrC = dltot * unl; FuC = FrC * ul + pl * nx; FvC = FrC * vl + pl * ny; FwC = FrC * wl + pl * nz; FeC = FrC * h0l;
+      double id = 1.0 / (S1 - Sstar);
+      double U1S = dltot * (S1 - unl) * id;
+      double U2S = ((S1 - unl) * dltot * ul + (pstar - pl) * nx) * id;
+      double U3S = ((S1 - unl) * dltot * vl + (pstar - pl) * ny) * id;
+      double U4S = ((S1 - unl) * dltot * wl + (pstar - pl) * nz) * id;
+      double U5S = ((S1 - unl) * dltot * e0l - pl * unl + pstar * Sstar) * id;
+      FrC = FrC + S1 * (U1S - dltot); FuC = FuC + S1 * (U2S - dltot * ul); FvC = FvC + S1 * (U3S - dltot * vl);
+      FwC = FwC + S1 * (U4S - dltot * wl); FeC = FeC + S1 * (U5S - dltot * e0l);
+      if (rs == 10) {
+        double ch_SK = S1;
+        double ch_lm = ch_pref * (ch_fstar - 1.0) * ch_dU;
+        double ch_sh = ch_pref * (ch_SK / (ch_SK - Sstar)) * ch_g;
+        FuC = FuC + ch_lm * nx + ch_sh * ch_dutx;
+        FvC = FvC + ch_lm * ny + ch_sh * ch_duty;
+        FwC = FwC + ch_lm * nz + ch_sh * ch_dutz;
+        FeC = FeC + ch_lm * Sstar;
+      }
+    } else if (S4 > 0.0) {
+      FrC = drtot * unr; FuC = FrC * ur + pr * nx; FvC = FrC * vr + pr * ny; FwC = FrC * wr + pr * nz; FeC = FrC * h0r;
+      double id = 1.0 / (S4 - Sstar);
+      double U1S = drtot * (S4 - unr) * id;
+      double U2S = ((S4 - unr) * drtot * ur + (pstar - pr) * nx) * id;
+      double U3S = ((S4 - unr) * drtot * vr + (pstar - pr) * ny) * id;
+      double U4S = ((S4 - unr) * drtot * wr + (pstar - pr) * nz) * id;
+      double U5S = ((S4 - unr) * drtot * e0r - pr * unr + pstar * Sstar) * id;
+      FrC = FrC + S4 * (U1S - drtot); FuC = FuC + S4 * (U2S - drtot * ur); FvC = FvC + S4 * (U3S - drtot * vr);
+      FwC = FwC + S4 * (U4S - drtot * wr); FeC = FeC + S4 * (U5S - drtot * e0r);
+      if (rs == 10) {
+        double ch_SK = S4;
+        double ch_lm = ch_pref * (ch_fstar - 1.0) * ch_dU;
+        double ch_sh = ch_pref * (ch_SK / (ch_SK - Sstar)) * ch_g;
+        FuC = FuC + ch_lm * nx + ch_sh * ch_dutx;
+        FvC = FvC + ch_lm * ny + ch_sh * ch_duty;
+        FwC = FwC + ch_lm * nz + ch_sh * ch_dutz;
+        FeC = FeC + ch_lm * Sstar;
+      }
+    } else {
+      FrC = drtot * unr; FuC = FrC * ur + pr * nx; FvC = FrC * vr + pr * ny; FwC = FrC * wr + pr * nz; FeC = FrC * h0r;
+    }
+    if (rs == 10 || bet >= 1.0) {
+      F_r = FrC; F_u = FuC; F_v = FvC; F_w = FwC; F_E = FeC;
+    } else if (bet == 0.0) {
+      F_r = FrE; F_u = FuE; F_v = FvE; F_w = FwE; F_E = FeE;
+    } else {
+      F_r = bet * FrC + (1.0 - bet) * FrE; F_u = bet * FuC + (1.0 - bet) * FuE; F_v = bet * FvC + (1.0 - bet) * FvE;
+      F_w = bet * FwC + (1.0 - bet) * FwE; F_E = bet * FeC + (1.0 - bet) * FeE;
+    }
+    return;
+  }
   double nmag = std::sqrt(nx * nx + ny * ny + nz * nz);
   if (nmag <= 0.0) { F_r = F_u = F_v = F_w = F_E = 0.0; return; }
   double n1 = nx / nmag, n2 = ny / nmag, n3 = nz / nmag;
@@ -731,14 +928,51 @@ void riemann_slau_bc(const Thermo& th, double dl, double ul, double vl, double w
             F_E);
 }
 
+// The shock sensor of a cell from its pressure and its six face neighbours' (SD_beta, Lib_Shock_Detector.f90:51-81):
+// 1 Tramel (1 smooth, 0 at a shock), 2 Chen (the smallest neighbour pressure ratio)
+double sd_beta(int id, double p, double p1, double p2, double p3, double p4, double p5, double p6) {
+  const double DELTA = 20.0;
+  if (id == 1) {
+    double kp1 = std::fabs((p2 - 2.0 * p + p1) / (p2 + 2.0 * p + p1));
+    double kp2 = std::fabs((p4 - 2.0 * p + p3) / (p4 + 2.0 * p + p3));
+    double kp3 = std::fabs((p6 - 2.0 * p + p5) / (p6 + 2.0 * p + p5));
+    double sw = std::max(std::max(kp1, kp2), kp3);
+    if (sw < 1.0 / DELTA) {
+      double phi = std::max(sw / DELTA, 0.0);
+      return 1.0 - std::tanh(10.0 * phi * phi * phi);
+    }
+    return 0.0;
+  }
+  if (id == 2) {
+    double beta = 1.0;
+    beta = std::min(beta, std::min(p, p1) / std::max(p, p1));
+    beta = std::min(beta, std::min(p, p2) / std::max(p, p2));
+    beta = std::min(beta, std::min(p, p3) / std::max(p, p3));
+    beta = std::min(beta, std::min(p, p4) / std::max(p, p4));
+    beta = std::min(beta, std::min(p, p5) / std::max(p, p5));
+    beta = std::min(beta, std::min(p, p6) / std::max(p, p6));
+    return beta;
+  }
+  return 1.0;
+}
+
+// beta of the cell (i,j,k) from the filled state (Fluxes_blk, Mod_Fluxes.f90:282-294), 1 without a sensor
+double cell_beta(const Ctx& c, const Blk& b, const double* P, int i, int j, int k) {
+  if (!c.sd) return 1.0;
+  const int64_t o = IP * c.ncell;
+  return sd_beta(c.sd, P[row(b, i, j, k) + o], P[row(b, i - 1, j, k) + o], P[row(b, i + 1, j, k) + o],
+                 P[row(b, i, j - 1, k) + o], P[row(b, i, j + 1, k) + o], P[row(b, i, j, k - 1) + o],
+                 P[row(b, i, j, k + 1) + o]);
+}
+
 // ---- one interior convective face: conv_physics.inc:1-179 ----
 void conv_face(const Ctx& c, const double* pm1, const double* p0, const double* pp1, const double* pp2,
-               const double* dlc, const double* nrm, double area, double* res0) {
+               const double* dlc, const double* nrm, double area, double* res0, double bet) {
   const Thermo& th = c.th;
   const int limv = c.sc.limiter, rsv = c.sc.riemann;
   double l0 = 0.5 * (dlc[0] + dlc[1]), l1 = 0.5 * (dlc[1] + dlc[2]), l2 = 0.5 * (dlc[2] + dlc[3]);
   double lm = 0.5 * dlc[1], lp = 0.5 * dlc[2];
-  const double beta_order = 1.0;
+  const double beta_order = c.sd ? bet : 1.0;  // SD_space_order: the slopes scaled by the face sensor
   double idl0 = 1.0 / l0, idl1 = 1.0 / l1, idl2 = 1.0 / l2;
   double P1[NP], P4[NP];
   for (int s = 0; s < NP; ++s) {
@@ -844,7 +1078,7 @@ void conv_face(const Ctx& c, const double* pm1, const double* p0, const double* 
       F_r = drtot * unr; F_u = F_r * ur + pr * nx; F_v = F_r * vr + pr * ny; F_w = F_r * wr + pr * nz; F_E = F_r * h0r;
     }
   } else {
-    riemann_open(th, rsv, c.sc.mco, P1[0], ul, vl, wl, pl, al, dltot, P4[0], ur, vr, wr, pr, ar, drtot, nx, ny, nz,
+    riemann_open(th, rsv, c.sc.mco, bet, P1[0], ul, vl, wl, pl, al, dltot, P4[0], ur, vr, wr, pr, ar, drtot, nx, ny, nz,
                  F_r, F_u, F_v, F_w, F_E);
   }
   double su = fsign_half(F_r), sp = 0.5 + su, sm = su - 0.5;
@@ -1014,7 +1248,7 @@ void bc_face_geom(const Blk& b, int Im, int Jm, int Km, int Fm, double* nrm, dou
 
 void riemann_rec(const Ctx& c, double dl, double ul, double vl, double wl, double pl, double al, double dltot,
                  double dr, double ur, double vr, double wr, double pr, double ar, double drtot, double nx, double ny,
-                 double nz, double& F_r, double& F_u, double& F_v, double& F_w, double& F_E);
+                 double nz, double& F_r, double& F_u, double& F_v, double& F_w, double& F_E, double bet = 1.0);
 
 // BC_Connection_Eul_lean (Lib_BC.f90:1770-1867)
 void bc_connection_eul(const Ctx& c, const Blk& b, const double* P, double* R, int Im, int Jm, int Km, int Fm) {
@@ -1036,7 +1270,7 @@ void bc_connection_eul(const Ctx& c, const Blk& b, const double* P, double* R, i
   dlc4[3] = dlv(b, dir - 1, Im + o4 * e[0], Jm + o4 * e[1], Km + o4 * e[2]);
   double nrm[3], area;
   bc_face_geom(b, Im, Jm, Km, Fm, nrm, area);
-  const double beta_ = 1.0;
+  const double beta_ = cell_beta(c, b, P, Im, Jm, Km);  // Lib_BC.f90:1811-1818
   double Dl1 = dlc4[0] * 0.5, Dl2 = dlc4[1] * 0.5, Dl3 = dlc4[2] * 0.5, Dl4 = dlc4[3] * 0.5;
   double D12 = Dl1 + Dl2, D23 = Dl2 + Dl3, D34 = Dl3 + Dl4;
   double PL[NP], PR[NP];
@@ -1053,7 +1287,7 @@ void bc_connection_eul(const Ctx& c, const Blk& b, const double* P, double* R, i
   double aR = f_ss(th, PR[0], PR[IP], rhoR, RR);
   double F_r, F_u, F_v, F_w, F_E;
   riemann_rec(c, PL[0], PL[IU], PL[IV], PL[IW], PL[IP], aL, rhoL, PR[0], PR[IU], PR[IV], PR[IW], PR[IP], aR, rhoR,
-              nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E);
+              nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E, beta_);
   double su = fsign_half(F_r), selL = 0.5 + su, selR = su - 0.5;
   double Fmass = F_r * area;
   int64_t rm = row(b, Im, Jm, Km);
@@ -1154,7 +1388,7 @@ void bc_extrapolation(const Ctx& c, const Blk& b, const double* P, double* R, in
 // 2, SLAU for 3, the MOSE_open solvers for rs 4..14 (the face sensor argument is 1 at these records)
 void riemann_rec(const Ctx& c, double dl, double ul, double vl, double wl, double pl, double al, double dltot,
                  double dr, double ur, double vr, double wr, double pr, double ar, double drtot, double nx, double ny,
-                 double nz, double& F_r, double& F_u, double& F_v, double& F_w, double& F_E) {
+                 double nz, double& F_r, double& F_u, double& F_v, double& F_w, double& F_E, double bet) {
   if (c.sc.riemann == 1 || c.sc.riemann == 2)
     riemann_hllc_bc(c.th, c.sc.riemann, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r,
                     F_u, F_v, F_w, F_E);
@@ -1162,7 +1396,7 @@ void riemann_rec(const Ctx& c, double dl, double ul, double vl, double wl, doubl
     riemann_slau_bc(c.th, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r, F_u, F_v, F_w,
                     F_E);
   else
-    riemann_open(c.th, c.sc.riemann, c.sc.mco, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz,
+    riemann_open(c.th, c.sc.riemann, c.sc.mco, bet, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz,
                  F_r, F_u, F_v, F_w, F_E);
 }
 
@@ -1790,7 +2024,7 @@ void residual(Ctx& c, const double* P, double* R) {
             }
             for (int q = -1; q <= 2; ++q) dlc[q + 1] = dlv(b, d, i + q * e[0], j + q * e[1], k + q * e[2]);
             const double* f = (d == 0) ? fm1p(b, i, j, k) : (d == 1) ? fm2p(b, i, j, k) : fm3p(b, i, j, k);
-            conv_face(c, pm1, p0, pp1, pp2, dlc, f, f[3], res0);
+            conv_face(c, pm1, p0, pp1, pp2, dlc, f, f[3], res0, cell_beta(c, b, P, i, j, k));
             int64_t fi;
             if (d == 0) fi = (i - 1) + (int64_t)(j - 1) * (n1 - 1) + (int64_t)(k - 1) * (n1 - 1) * n2;
             else if (d == 1) fi = (i - 1) + (int64_t)(j - 1) * n1 + (int64_t)(k - 1) * n1 * (n2 - 1);
@@ -2067,14 +2301,14 @@ struct orc_ctx { Ctx c; };
 
 int orc_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, orc_ctx** out) {
   if (!mesh || !sc || !th || !out) return MB_E_ARG;
-  if (sc->riemann != 1 && sc->riemann != 2 && sc->riemann != 3 && sc->riemann != 4 && sc->riemann != 8 &&
-      sc->riemann != 9 && sc->riemann != 11 && sc->riemann != 12 && sc->riemann != 13)
+  if (sc->riemann < 1 || sc->riemann > 13 || sc->sensor < 0 || sc->sensor > 3)
     return MB_E_UNSUPPORTED;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
   if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
   orc_ctx* o = new orc_ctx();
   Ctx& c = o->c;
   c.sc = *sc;
+  c.sd = mb_effective_sensor(sc->riemann, sc->sensor);
   c.ncell = mesh->ncell_total;
   for (int b = 0; b < mesh->nblk; ++b) {
     const mb_block& q = mesh->blk[b];

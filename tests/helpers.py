@@ -103,6 +103,18 @@ def small_cases():
                                                            limiter=abi.LIM_MINMOD, n_rk=3)),
         ("tgv_miczek_mco02", lambda: with_scheme(cs.taylor_green(n=12, riemann=abi.RS_MICZEKROE), mco=0.2)),
         ("duct3d_miczek_mco03", lambda: with_scheme(cs.duct_3d(riemann=abi.RS_MICZEKROE), mco=0.3)),
+        # the solvers that read the shock sensor (beta of the face's left cell; connection records: their own cell's)
+        # and a base solver with a sensor (the slopes scaled by beta)
+        ("sod_ausmpm_chen_mco02", lambda: with_scheme(cs.riemann_1d(n=64, riemann=abi.RS_AUSMPM), mco=0.2)),
+        ("sod_hllepp_tramel", lambda: cs.riemann_1d(n=64, riemann=abi.RS_HLLEPP, limiter=abi.LIM_VANLEER)),
+        ("quad2d_hllc_tramel_mc", lambda: cs.riemann_2d(n=20, riemann=abi.RS_HLLC_TRAMEL, limiter=abi.LIM_MC)),
+        ("tgv_hllc_chen_8blk", lambda: with_scheme(cs.taylor_green(n=12, blocks=2, riemann=abi.RS_HLLC_CHEN,
+                                                                   noise=1e-3), mco=0.2)),
+        ("mb2d_hllc_sensor_tramel", lambda: with_scheme(cs.multiblock_2d(cols=2, rows=2, lo=5, hi=9, seed=23,
+                                                                         riemann=abi.RS_HLLC), sensor=abi.SENSOR_TRAMEL)),
+        ("mb2d_ausmpm_chen_euler", lambda: with_scheme(cs.multiblock_2d(cols=2, rows=1, lo=6, hi=9, seed=29, visc=0,
+                                                                        riemann=abi.RS_AUSMPM), mco=0.3)),
+        ("duct3d_hllepp_tramel", lambda: cs.duct_3d(riemann=abi.RS_HLLEPP)),
         # symmetry (300), isothermal walls (302) and the back-pressure outlet (406)
         ("duct3d_hllc_vanleer", lambda: cs.duct_3d()),
         ("duct3d_roe_vanalbada_rk4", lambda: cs.duct_3d(widths=(5, 6), heights=(4, 3), depths=(4,),

@@ -125,7 +125,8 @@ def test_sod_to_t_end(torch_cuda):
 
 
 @pytest.mark.parametrize("riemann", [abi.RS_LMROE, abi.RS_HLLC, abi.RS_HLLE, abi.RS_SLAU, abi.RS_AUSMP, abi.RS_LLF,
-                                     abi.RS_SLAU2, abi.RS_EXACT, abi.RS_MICZEKROE])
+                                     abi.RS_SLAU2, abi.RS_EXACT, abi.RS_MICZEKROE, abi.RS_AUSMPM, abi.RS_HLLEPP,
+                                     abi.RS_HLLC_TRAMEL, abi.RS_HLLC_CHEN])
 def test_mixed_precision_error(torch_cuda, riemann):
     """The mixed form (FP32 flux arithmetic, FP64 state) against the FP64 form on a small TGV, every solver."""
     from mosegpu import case as cs
