@@ -193,6 +193,11 @@ typedef struct mb_scheme {
                          (Tramel for HLLE++ / HLLC+Tramel, Chen for AUSM+M / HLLC+Chen, none otherwise), 1 Tramel,
                          2 Chen, 3 none. A limiter name with the SD suffix is the Tramel sensor. With a sensor the
                          cell's beta scales the reconstruction slopes of its faces and goes to their Riemann solver */
+  int32_t intvar;     /* integration-variables (Assign_Integration_Variables, Lib_Newstate.f90:43-60): 0 cons
+                         (Newstate_Conservative), 1 prim (Newstate_Primitive: the residual taken to the primitive
+                         variables through the inverse of the prim -> cons Jacobian, Lib_Newstate.f90:348-531; with
+                         n_rk <= 3) */
+  int32_t pad1;
   double cfl;
   double vnn;         /* default 0.3 (MOSE_Types_m.f90:268) */
   double prandtl;     /* > 0: kl = mu cp / Pr (Mod_Diffusive.f90:303) */

@@ -207,8 +207,10 @@ static void free_tables(mb_ctx* c) {
 }
 
 // the sweep unit of a scheme: the benchmarked solvers' own (the solver a compile-time constant) unless a shock sensor
-// is on, which only the run-time solver unit carries
-static int sweep_unit(const mb_scheme* sc) { return mb_effective_sensor(sc->riemann, sc->sensor) ? 0 : sc->riemann; }
+// or the primitive update is on, which only the run-time solver unit carries
+static int sweep_unit(const mb_scheme* sc) {
+  return (mb_effective_sensor(sc->riemann, sc->sensor) || sc->intvar) ? 0 : sc->riemann;
+}
 
 // record types with physical ghosts (Fill_Ghost_Cell_blk, Lib_Extrapolation.f90:643-730)
 static bool phys_type(int t) {
@@ -508,6 +510,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   *out = nullptr;
   if (sc->riemann < MB_RS_HLLC || sc->riemann > MB_RS_MICZEKROE) return MB_E_UNSUPPORTED;  // 14 (HLLC-PC) needs prec
   if (sc->sensor < 0 || sc->sensor > 3) return MB_E_UNSUPPORTED;
+  if (sc->intvar < 0 || sc->intvar > 1 || (sc->intvar == 1 && sc->n_rk == 4)) return MB_E_UNSUPPORTED;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
   if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
   if (!(sc->res_stop >= 0.0)) return MB_E_ARG;
@@ -591,6 +594,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   p.tmin = th->tmin; p.tmax = th->tmax;
   p.wm = th->wm; p.ri = RUNIV / th->wm; p.iri = th->wm / RUNIV;
   p.sd = mb_effective_sensor(sc->riemann, sc->sensor);
+  p.intvar = sc->intvar;
   p.lim = sc->limiter; p.rs = sc->riemann; p.visc = sc->visc ? 1 : 0; p.ndir = sc->ndir; p.dt_additive = sc->dt_additive;
   p.guard = sc->visc ? 1 : 0; p.state_check = sc->state_check;
   p.cfl = sc->cfl; p.vnn = sc->vnn; p.prandtl = sc->prandtl; p.schmidt = sc->schmidt; p.mco = sc->mco;

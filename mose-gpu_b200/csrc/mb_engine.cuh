@@ -1018,6 +1018,60 @@ MB_HD void cons_update(const Params& p, const double* pc, const double* po, cons
   if (pn[0] < 1e-20) pn[0] = 1e-20;
 }
 
+// Newstate_Primitive_blk (Lib_Newstate.f90:348-531), one species, FP64 in both forms: the conservative residual taken
+// to the primitive variables by the inverse of the prim -> cons Jacobian (Theta = rho_p), then the RK stage on the
+// primitive state, rho floored at 1e-20
+MB_HD void prim_update(const Params& p, const double* pc, const double* po, const double* res, double vol, double dt,
+                       double rkc, double* pn) {
+  const double strang = 1.0;
+  double rho, Rgas;
+  rotot_rtot(p, pc[0], rho, Rgas);
+  const double temperature = pc[MB_IPR] / (rho * Rgas);
+  const int T_i = tidx(p, temperature);
+  const double Tdiff = temperature - (double)T_i;
+  const double inv_rho = 1.0 / rho;
+  const double vel[3] = {pc[MB_IU], pc[MB_IV], pc[MB_IW]};
+  const double modvel = sqrt(vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
+  const double q2 = modvel * modvel;
+  const double cp = f_cp(p, pc[0], T_i, Tdiff, rho);
+  const double rho_T = -rho / temperature;
+  const double rho_p = 1.0 / (Rgas * temperature);
+  const double enthalpy = H0(p, pc[MB_IPR], pc[0], modvel);
+  const double Theta = rho_p;
+  const double Denom = 1.0 / (rho * cp * Theta + rho_T);
+  double G[5][5];
+  G[0][0] = (rho_T * (enthalpy - q2) + rho * cp) * Denom;
+  G[0][1] = rho_T * vel[0] * Denom; G[0][2] = rho_T * vel[1] * Denom; G[0][3] = rho_T * vel[2] * Denom;
+  G[0][4] = -rho_T * Denom;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    G[1 + a][0] = -vel[a] * inv_rho;
+#pragma unroll
+    for (int q = 1; q < 5; ++q) G[1 + a][q] = 0.0;
+    G[1 + a][1 + a] = inv_rho;
+  }
+  G[4][0] = -(Theta * (enthalpy - q2) - 1.0) * Denom;
+  G[4][1] = -vel[0] * Theta * Denom; G[4][2] = -vel[1] * Theta * Denom; G[4][3] = -vel[2] * Theta * Denom;
+  G[4][4] = Theta * Denom;
+  const double cres[5] = {-res[0], -res[MB_IU], -res[MB_IV], -res[MB_IW], -res[MB_IPR]};
+  double pres[5];
+#pragma unroll
+  for (int r_ = 0; r_ < 5; ++r_) {
+    pres[r_] = 0.0;
+#pragma unroll
+    for (int c_ = 0; c_ < 5; ++c_) pres[r_] = pres[r_] + G[r_][c_] * cres[c_];
+  }
+  double rl[MB_NP];
+  rl[MB_IU] = pres[1]; rl[MB_IV] = pres[2]; rl[MB_IW] = pres[3];
+  rl[MB_IPR] = pres[0];
+  rl[0] = rho_p * pres[0] + rho_T * pres[4];
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) rl[s] = rl[s] * dt / vol * strang;
+#pragma unroll
+  for (int s = 0; s < MB_NP; ++s) pn[s] = po[s] + (pc[s] - po[s] + rl[s]) * rkc;
+  if (pn[0] < 1e-20) pn[0] = 1e-20;
+}
+
 // The state update of the mixed form: the arithmetic of cons_update, in FP64, with the single-species identities
 // (rho = rho_s, R_mix = R, h_mix = h(T)) applied exactly and each division by rho, vol or R taken once as a
 // reciprocal: p / rho = R T in the Newton iteration for T, its stop test |de| < 1e-6 |e| without a division. About
@@ -1394,7 +1448,8 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
           Tc = mn(mx(Tc, 1.0), 9990.0);
         }
         const double vol = ld(b.vol + (r - b.boff));
-        if (Fast<R>::on) cons_update_fast(p, pc, po, acc, vol, dt, rkc, Tc, pn, r);
+        if (RS == 0 && p.intvar) prim_update(p, pc, po, acc, vol, dt, rkc, pn);
+        else if (Fast<R>::on) cons_update_fast(p, pc, po, acc, vol, dt, rkc, Tc, pn, r);
         else cons_update(p, pc, po, acc, vol, dt, rkc, Tc, pn, r);
         bool bad = !(pn[MB_IPR] >= 0.0);
 #pragma unroll

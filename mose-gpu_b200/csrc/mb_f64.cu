@@ -97,7 +97,8 @@ __global__ void __launch_bounds__(32 * TY_AUX) k_update(Params p, const DTile* _
       if (T != T) T = 300.0;
       T = mn(mx(T, 1.0), 9990.0);
     }
-    cons_update(p, pc, po, res, ld(b.vol + (r - b.boff)), dt, rkc, T, pn, r);
+    if (p.intvar) prim_update(p, pc, po, res, ld(b.vol + (r - b.boff)), dt, rkc, pn);
+    else cons_update(p, pc, po, res, ld(b.vol + (r - b.boff)), dt, rkc, T, pn, r);
     bool bad = !(pn[MB_IPR] >= 0.0);
     for (int s = 0; s < MB_NP; ++s) bad = bad || !isfinite(pn[s]);
     if (bad) report_bad_state(st, t.blk, i, j, k);

@@ -103,6 +103,7 @@ struct Params {
   double wm, ri;
   double iri;              // 1 / ri (the mixed form's state update multiplies by it)
   int sd;                  // the shock sensor in effect (sd_dev): 0 none, 1 Tramel, 2 Chen
+  int intvar;              // integration variables: 0 conservative, 1 primitive
   int lim, rs, visc, ndir, dt_additive, guard, state_check;
   double cfl, vnn, prandtl, schmidt, mco;
   void* recflux;           // boundary-record contributions [record][10] in the flux type (k_records)

@@ -44,6 +44,7 @@ RS_HLLC, RS_HLLE, RS_SLAU, RS_AUSMP, RS_LLF, RS_SLAU2, RS_LMROE = 1, 2, 3, 4, 8,
 RS_EXACT, RS_MICZEKROE = 11, 13
 RS_AUSMPM, RS_HLLEPP, RS_HLLC_TRAMEL, RS_HLLC_CHEN = 5, 6, 7, 10
 SENSOR_DEFAULT, SENSOR_TRAMEL, SENSOR_CHEN, SENSOR_NONE = 0, 1, 2, 3
+INTVAR_CONS, INTVAR_PRIM = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 
 
@@ -80,6 +81,7 @@ class MBScheme(C.Structure):
     _fields_ = [("limiter", C.c_int32), ("riemann", C.c_int32), ("visc", C.c_int32), ("n_rk", C.c_int32),
                 ("precision", C.c_int32), ("ndir", C.c_int32), ("time_clip", C.c_int32),
                 ("state_check", C.c_int32), ("dt_additive", C.c_int32), ("sensor", C.c_int32),
+                ("intvar", C.c_int32), ("pad1", C.c_int32),
                 ("cfl", C.c_double), ("vnn", C.c_double),
                 ("prandtl", C.c_double), ("schmidt", C.c_double), ("mco", C.c_double),
                 ("time_threshold", C.c_double), ("res_stop", C.c_double)]

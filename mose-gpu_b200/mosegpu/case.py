@@ -176,6 +176,7 @@ class Case:
         s.time_clip = d.get("time_clip", 0); s.state_check = d.get("state_check", 1)
         s.dt_additive = d.get("dt_additive", 0)
         s.sensor = d.get("sensor", 0)
+        s.intvar = d.get("intvar", 0)
         s.cfl = d["cfl"]; s.vnn = d.get("vnn", 0.3); s.prandtl = d.get("prandtl", 0.0)
         s.schmidt = d.get("schmidt", 0.7); s.mco = d.get("mco", 1.0)
         s.time_threshold = d.get("time_threshold", 0.0)

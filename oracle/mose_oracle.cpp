@@ -31,7 +31,8 @@
 //                           physics/turbulence/Mod_Fluid.f90:20-44 (wall stress)
 //   ghost fill              bc/Lib_Extrapolation.f90:558-641 (symmetry, ZG, cubic), 643-730, 859-879, 1023-1191
 //   thermo cache            src/lib/physics/Mod_Thermo_Cache.f90:291-425
-//   state update            src/lib/gpu/newstate_cons_body.inc:1-89, explicit/Lib_Newstate.f90:257-307
+//   state update            src/lib/gpu/newstate_cons_body.inc:1-89, explicit/Lib_Newstate.f90:257-307,
+//                           348-531 (primitive)
 //   RK coefficients         explicit/Lib_RK.f90:6-9; classical RK4 with a conserved accumulator (no reference)
 //   local dt                src/lib/gpu/dt_blk.inc:11-222, numerics/time/Mod_dt.f90:15-106
 //   thermo leaves           lib/FLINT/src/lib/Lib_ThermoTransport_dev.f90:54-300
@@ -2170,6 +2171,53 @@ void update_cell(const Ctx& c, const double* po, double* p, const double* res, d
   if (p[0] < 1e-20) p[0] = 1e-20;
 }
 
+// Newstate_Primitive_blk (Lib_Newstate.f90:348-531), one species: the conservative residual taken to the primitive
+// variables by the inverse of the prim -> cons Jacobian (Theta = rho_p: no preconditioning), then the RK stage on the
+// primitive state: new = old + (state - old + res dt / vol) rkc, rho floored at 1e-20
+void update_cell_prim(const Ctx& c, const double* po, double* p, const double* res, double vol, double dt, double rkc) {
+  const Thermo& th = c.th;
+  const double strang = 1.0;
+  double rho, Rgas;
+  rotot_rtot(th, p[0], rho, Rgas);
+  double temperature = p[IP] / (rho * Rgas);
+  int T_i = tidx(th, temperature);
+  double Tdiff = temperature - T_i;
+  double inv_rho = 1.0 / rho;
+  double vel[3] = {p[IU], p[IV], p[IW]};
+  double modvel = std::sqrt(vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
+  double q2 = modvel * modvel;
+  double cp = f_cp(th, p[0], T_i, Tdiff, rho);
+  double rho_T = -rho / temperature;
+  double rho_p = 1.0 / (Rgas * temperature);
+  double enthalpy = H0(th, p[IP], p[0], modvel);
+  double Theta = rho_p;
+  double Denom = 1.0 / (rho * cp * Theta + rho_T);
+  double G[5][5];
+  G[0][0] = (rho_T * (enthalpy - q2) + rho * cp) * Denom;
+  G[0][1] = rho_T * vel[0] * Denom; G[0][2] = rho_T * vel[1] * Denom; G[0][3] = rho_T * vel[2] * Denom;
+  G[0][4] = -rho_T * Denom;
+  for (int a = 0; a < 3; ++a) {
+    G[1 + a][0] = -vel[a] * inv_rho;
+    for (int q = 1; q < 5; ++q) G[1 + a][q] = 0.0;
+    G[1 + a][1 + a] = inv_rho;
+  }
+  G[4][0] = -(Theta * (enthalpy - q2) - 1.0) * Denom;
+  G[4][1] = -vel[0] * Theta * Denom; G[4][2] = -vel[1] * Theta * Denom; G[4][3] = -vel[2] * Theta * Denom;
+  G[4][4] = Theta * Denom;
+  double cres[5] = {-res[0], -res[IU], -res[IV], -res[IW], -res[IP]}, pres[5];
+  for (int r_ = 0; r_ < 5; ++r_) {
+    pres[r_] = 0.0;
+    for (int c_ = 0; c_ < 5; ++c_) pres[r_] = pres[r_] + G[r_][c_] * cres[c_];
+  }
+  double rl[NP];
+  rl[IU] = pres[1]; rl[IV] = pres[2]; rl[IW] = pres[3];
+  rl[IP] = pres[0];
+  rl[0] = rho_p * pres[0] + rho_T * pres[4];
+  for (int s = 0; s < NP; ++s) rl[s] = rl[s] * dt / vol * strang;
+  for (int s = 0; s < NP; ++s) p[s] = po[s] + (p[s] - po[s] + rl[s]) * rkc;
+  if (p[0] < 1e-20) p[0] = 1e-20;
+}
+
 void update(Ctx& c, double* P, const double* PO, const double* R, int irk, double dt) {
   const int64_t nc = c.ncell;
   const double rkc = c.sc.n_rk == 4 ? 0.0 : RKC[c.sc.n_rk - 1][irk - 1];
@@ -2191,7 +2239,9 @@ void update(Ctx& c, double* P, const double* PO, const double* R, int irk, doubl
             if (T != T) T = 300.0;
             T = std::min(std::max(T, 1.0), 9990.0);
           }
-          if (c.sc.n_rk == 4)
+          if (c.sc.intvar == 1)
+            update_cell_prim(c, po, p, res, b.vol[lin(b, i, j, k)], dt, rkc);
+          else if (c.sc.n_rk == 4)
             update_cell(c, po, p, res, b.vol[lin(b, i, j, k)], dt, rkc, T, irk, &c.acc4[(size_t)r * NP]);
           else
             update_cell(c, po, p, res, b.vol[lin(b, i, j, k)], dt, rkc, T);
@@ -2301,7 +2351,8 @@ struct orc_ctx { Ctx c; };
 
 int orc_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, orc_ctx** out) {
   if (!mesh || !sc || !th || !out) return MB_E_ARG;
-  if (sc->riemann < 1 || sc->riemann > 13 || sc->sensor < 0 || sc->sensor > 3)
+  if (sc->riemann < 1 || sc->riemann > 13 || sc->sensor < 0 || sc->sensor > 3 || sc->intvar < 0 || sc->intvar > 1 ||
+      (sc->intvar == 1 && sc->n_rk == 4))
     return MB_E_UNSUPPORTED;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
   if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;

@@ -115,6 +115,11 @@ def small_cases():
         ("mb2d_ausmpm_chen_euler", lambda: with_scheme(cs.multiblock_2d(cols=2, rows=1, lo=6, hi=9, seed=29, visc=0,
                                                                         riemann=abi.RS_AUSMPM), mco=0.3)),
         ("duct3d_hllepp_tramel", lambda: cs.duct_3d(riemann=abi.RS_HLLEPP)),
+        # the primitive-variable update (integration-variables = prim)
+        ("sod_prim_hllc", lambda: with_scheme(cs.riemann_1d(n=64), intvar=abi.INTVAR_PRIM)),
+        ("tgv_prim_roe_8blk", lambda: with_scheme(cs.taylor_green(n=12, blocks=2), intvar=abi.INTVAR_PRIM)),
+        ("mb2d_prim_ausm_rk3", lambda: with_scheme(cs.multiblock_2d(cols=2, rows=2, lo=5, hi=9, seed=31, n_rk=3),
+                                                   intvar=abi.INTVAR_PRIM)),
         # symmetry (300), isothermal walls (302) and the back-pressure outlet (406)
         ("duct3d_hllc_vanleer", lambda: cs.duct_3d()),
         ("duct3d_roe_vanalbada_rk4", lambda: cs.duct_3d(widths=(5, 6), heights=(4, 3), depths=(4,),
