@@ -314,6 +314,10 @@ int mb_reconfigure(mb_ctx* ctx, const mb_mesh* mesh);
 
 /* Starts case g afresh: time 0, no steps, cleared status, its stop rule, and its first dt from the cells of P
  * that belong to it (the other cases' clocks are untouched). */
+/* Replaces the parameters (mb_bc.q, same meaning as at mb_init) of record `rec` from the next stage on, ordered on
+ * `stream`: a time-dependent boundary driven by the host, as the reference's 402 inlet interpolates p0(t) from its file
+ * table each step (Mod_BC_Time.f90) and hands the value to the record. Validated as at mb_init. */
+int mb_set_record_params(mb_ctx* ctx, int rec, const double* q, void* stream);
 int mb_group_reset(mb_ctx* ctx, int g, const mb_group* spec, const double* P, void* stream);
 
 /* Status of cases g0 .. g0+n-1 (one device read). Synchronises. */

@@ -22,6 +22,8 @@ struct mb_ctx {
   DBlk* d_blk = nullptr;
   int* d_recmap = nullptr;
   DRec* d_rec = nullptr;
+  std::vector<mb_bc> hrec;      // the host records of the current mesh (mb_set_record_params)
+  std::vector<DRec> hdrec;      // their device form (the source of single-record updates)
   GRec* d_grec = nullptr;
   int* d_phys = nullptr;
   int* d_cubic = nullptr;
@@ -155,7 +157,40 @@ const char* mb_version(void) { return "mose_b200 0.1 (sm_100a)"; }
 int64_t mb_launch_count(const mb_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 // the checks of a mesh description that mb_init and mb_reconfigure share
+// the parameters of one record (mb_bc.q) for its type
+static int check_record_params(const mb_bc& r) {
+  if (r.type == MB_BC_INFLOW) {
+    if (!(r.q[1] > 0.0 && r.q[2] > 0.0)) return MB_E_ARG;  // T0, p0 (or the mass flux)
+    const int code = (int)r.q[6];
+    if (code != 0 && code != 401 && code != 403 && code != 404 && code != 405 && code != 407) return MB_E_UNSUPPORTED;
+    if (code == 404 && r.q[5] != 1.0) return MB_E_UNSUPPORTED;  // IO_BC_Open.f90:276-281
+    if (code == 401 || code == 403 || code == 404 || code == 407) {  // the face tangent is read
+      const double tn = r.q[8] * r.q[8] + r.q[9] * r.q[9] + r.q[10] * r.q[10];
+      if (!(fabs(tn - 1.0) < 1e-6)) return MB_E_ARG;
+    }
+  }
+  if (r.type == MB_BC_WALL_T && !(r.q[0] > 0.0)) return MB_E_ARG;                   // T_wall
+  if (r.type == MB_BC_OUTLET && !(r.q[0] >= 0.0 && r.q[1] >= 0.0 && r.q[1] <= 1.0)) return MB_E_ARG;
+  return MB_OK;
+}
+
+// the device record of one mb_bc: the type, the connection row and the parameters in the form the kernels read
+static void fill_drec(const mb_bc& r, DRec* d) {
+  d->type = r.type;
+  d->pg = r.conn;
+  for (int s = 0; s < 16; ++s) d->q[s] = 0.0;
+  if (r.type == MB_BC_INFLOW) {  // mach, T0, p0, rel_fac, cos / sin of alpha and beta, code, pamb, alpha, beta, t
+    const double v[8] = {r.q[0], r.q[1], r.q[2], r.q[5], cos(r.q[3]), sin(r.q[3]), cos(r.q[4]), sin(r.q[4])};
+    for (int s = 0; s < 8; ++s) d->q[s] = v[s];
+    d->q[8] = r.q[6]; d->q[9] = r.q[7]; d->q[10] = r.q[3]; d->q[11] = r.q[4];
+    d->q[12] = r.q[8]; d->q[13] = r.q[9]; d->q[14] = r.q[10];
+  }
+  if (r.type == MB_BC_WALL_T) d->q[0] = r.q[0];                                 // T_wall
+  if (r.type == MB_BC_OUTLET) { d->q[0] = r.q[0]; d->q[1] = r.q[1]; }         // exit pressure, relaxation
+}
+
 static int check_mesh(const mb_mesh* mesh, int ngroups) {
+  int rc;
   if (!mesh || mesh->nblk <= 0 || mesh->ncell_total <= 0 || !mesh->blk) return MB_E_ARG;
   if (mesh->nrec > 0 && !mesh->rec) return MB_E_ARG;
   if (mesh->nrec >= (1 << 28)) return MB_E_ARG;  // record ids share a 32-bit word with a layer count
@@ -176,18 +211,7 @@ static int check_mesh(const mb_mesh* mesh, int ngroups) {
         r.type != MB_BC_INFLOW && r.type != MB_BC_SYMMETRY && r.type != MB_BC_WALL_T && r.type != MB_BC_OUTLET)
       return MB_E_UNSUPPORTED;
     if (r.blk < 0 || r.blk >= mesh->nblk || r.face < 1 || r.face > 6) return MB_E_ARG;
-    if (r.type == MB_BC_INFLOW) {
-      if (!(r.q[1] > 0.0 && r.q[2] > 0.0)) return MB_E_ARG;  // T0, p0 (or the mass flux)
-      const int code = (int)r.q[6];
-      if (code != 0 && code != 401 && code != 403 && code != 404 && code != 405 && code != 407) return MB_E_UNSUPPORTED;
-      if (code == 404 && r.q[5] != 1.0) return MB_E_UNSUPPORTED;  // IO_BC_Open.f90:276-281
-      if (code == 401 || code == 403 || code == 404 || code == 407) {  // the face tangent is read
-        const double tn = r.q[8] * r.q[8] + r.q[9] * r.q[9] + r.q[10] * r.q[10];
-        if (!(fabs(tn - 1.0) < 1e-6)) return MB_E_ARG;
-      }
-    }
-    if (r.type == MB_BC_WALL_T && !(r.q[0] > 0.0)) return MB_E_ARG;                   // T_wall
-    if (r.type == MB_BC_OUTLET && !(r.q[0] >= 0.0 && r.q[1] >= 0.0 && r.q[1] <= 1.0)) return MB_E_ARG;
+    if ((rc = check_record_params(r)) != MB_OK) return rc;
   }
   return MB_OK;
 }
@@ -268,17 +292,7 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   std::vector<int> phys, cubic;
   for (int q = 0; q < mesh->nrec; ++q) {
     const mb_bc& r = mesh->rec[q];
-    hr[q].type = r.type;
-    hr[q].pg = r.conn;
-    for (int s = 0; s < 16; ++s) hr[q].q[s] = 0.0;
-    if (r.type == MB_BC_INFLOW) {  // mach, T0, p0, rel_fac, cos / sin of alpha and beta
-      const double v[8] = {r.q[0], r.q[1], r.q[2], r.q[5], cos(r.q[3]), sin(r.q[3]), cos(r.q[4]), sin(r.q[4])};
-      for (int s = 0; s < 8; ++s) hr[q].q[s] = v[s];
-      hr[q].q[8] = r.q[6]; hr[q].q[9] = r.q[7]; hr[q].q[10] = r.q[3]; hr[q].q[11] = r.q[4];
-      hr[q].q[12] = r.q[8]; hr[q].q[13] = r.q[9]; hr[q].q[14] = r.q[10];
-    }
-    if (r.type == MB_BC_WALL_T) hr[q].q[0] = r.q[0];                                  // T_wall
-    if (r.type == MB_BC_OUTLET) { hr[q].q[0] = r.q[0]; hr[q].q[1] = r.q[1]; }        // exit pressure, relaxation
+    fill_drec(r, &hr[q]);
     hg[q] = GRec{r.blk, r.i, r.j, r.k, r.face, r.type};
     if (phys_type(r.type)) phys.push_back(q);
     if (r.type == MB_BC_EXTRAPOLATION) cubic.push_back(q);
@@ -423,6 +437,8 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   if ((rc = upload(&c->d_blk, hb.data(), hb.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_recmap, recmap.data(), recmap.size())) != MB_OK) return rc;
   if ((rc = upload(&c->d_rec, hr.data(), hr.size())) != MB_OK) return rc;
+  c->hrec.assign(mesh->rec, mesh->rec + mesh->nrec);
+  c->hdrec = hr;
   if ((rc = upload(&c->d_grec, hg.data(), hg.size())) != MB_OK) return rc;
   // Ghost passes in two halves where the record order changes values. The extrapolating ghosts of a face (walls in
   // the first pass, type 11 in the second) read the opposite face's ghost layers when the axis has at most two
@@ -637,6 +653,20 @@ int mb_reconfigure(mb_ctx* ctx, const mb_mesh* mesh) {
   ctx->gP = nullptr;
   ctx->gPO = nullptr;
   return build_tables(ctx, mesh);
+}
+
+int mb_set_record_params(mb_ctx* ctx, int rec, const double* q, void* stream) {
+  if (!ctx || !q || rec < 0 || rec >= (int)ctx->hrec.size()) return MB_E_ARG;
+  mb_bc r = ctx->hrec[rec];
+  for (int s = 0; s < MB_BC_NQ; ++s) r.q[s] = q[s];
+  int rc = check_record_params(r);
+  if (rc != MB_OK) return rc;
+  CK(cudaSetDevice(ctx->device));
+  ctx->hrec[rec] = r;
+  fill_drec(r, &ctx->hdrec[rec]);
+  CK(cudaMemcpyAsync(ctx->d_rec + rec, &ctx->hdrec[rec], sizeof(DRec), cudaMemcpyHostToDevice,
+                     (cudaStream_t)stream));
+  return MB_OK;
 }
 
 int mb_group_reset(mb_ctx* ctx, int g, const mb_group* spec, const double* P, void* stream) {

@@ -47,6 +47,7 @@ def load_library():
     L.mb_profile_stage.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), vp]
     L.mb_reconfigure.argtypes = [vp, C.POINTER(abi.MBMesh)]
     L.mb_group_reset.argtypes = [vp, C.c_int, C.POINTER(abi.MBGroup), vp, vp]
+    L.mb_set_record_params.argtypes = [vp, C.c_int, C.POINTER(C.c_double), vp]
     L.mb_get_group_status.argtypes = [vp, C.c_int, C.c_int, C.POINTER(abi.MBStatus)]
     L.mb_read_group_status.argtypes = [vp, C.c_int, C.c_int, C.POINTER(abi.MBStatus), vp]
     L.mb_autotune.argtypes = [vp, vp, vp]
@@ -200,6 +201,11 @@ class Engine:
         st = abi.MBStatus()
         _check(self.lib.mb_get_status(self.ctx, C.byref(st)), "mb_get_status")
         return st
+
+    def set_record_params(self, rec, q):
+        """New parameters (mb_bc.q) of record `rec` from the next stage on (a host-driven time-dependent boundary)."""
+        qa = (C.c_double * abi.BC_NQ)(*[float(x) for x in q])
+        _check(self.lib.mb_set_record_params(self.ctx, int(rec), qa, self._s()), "mb_set_record_params")
 
     def run_to(self, t_end, max_steps=10 ** 7, chunk=1):
         """Steps until the simulated time reaches t_end (the reference's `time >= timemax` stop) or the case's

@@ -2444,4 +2444,10 @@ int orc_step(orc_ctx* o, double* P, double* PO, double* R, int nsteps) {
 
 int orc_get_status(orc_ctx* o, mb_status* st) { *st = o->c.st; return MB_OK; }
 
+int orc_set_record_params(orc_ctx* o, int rec, const double* q) {
+  if (rec < 0 || rec >= (int)o->c.rec.size()) return MB_E_ARG;
+  for (int s = 0; s < MB_BC_NQ; ++s) o->c.rec[rec].q[s] = q[s];
+  return MB_OK;
+}
+
 }  // extern "C"

@@ -42,6 +42,7 @@ def lib():
         L.orc_dt.argtypes = [vp, vp, C.POINTER(C.c_double)]
         L.orc_step.argtypes = [vp, vp, vp, vp, C.c_int]
         L.orc_get_status.argtypes = [vp, C.POINTER(abi.MBStatus)]
+        L.orc_set_record_params.argtypes = [vp, C.c_int, C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -118,6 +119,12 @@ class Oracle:
         st = abi.MBStatus()
         lib().orc_get_status(self.h, C.byref(st))
         return st
+
+    def set_record_params(self, rec, q):
+        qa = (C.c_double * abi.BC_NQ)(*[float(x) for x in q])
+        rc = lib().orc_set_record_params(self.h, int(rec), qa)
+        if rc != 0:
+            raise abi.MoseError(rc, "orc_set_record_params")
 
     def run_to(self, P, t_end, max_steps=1000000):
         """Steps until the simulated time reaches t_end (the reference's `time >= timemax` stop)."""

@@ -267,3 +267,30 @@ def test_residual_stop_matches_the_oracle(torch_cuda):
     assert ref.step(Pk, 12) == 0 and ref.status().steps == k
     e = H.rel_err(H.conserved(case, eng.state()), H.conserved(case, Pk))
     assert np.all(e <= TOL_ONE), e
+
+
+def test_record_params_changed_between_steps_match_the_oracle(torch_cuda):
+    """A host-driven time-dependent inlet (the reference's 402: p0(t) handed to the records each step): the inlet
+    records' stagnation pressure raised between steps through mb_set_record_params, the same on the oracle's
+    records; the states stay equal."""
+    import oracle
+    from mosegpu.engine import Engine
+    case = dict(H.small_cases())["duct3d_401_stagnation_inlet"]()
+    eng, orc = Engine(case), oracle.Oracle(case)
+    P = case.P0.copy()
+    inlet = [q for q in range(len(case.rec)) if case.rec["type"][q] == abi.BC_INFLOW]
+    assert inlet
+    for n, p0 in ((3, 1.25e5), (3, 1.32e5), (3, 1.28e5)):
+        for q in inlet:
+            qv = np.array(case.rec["q"][q])
+            qv[2] = p0
+            eng.set_record_params(q, qv)
+            orc.set_record_params(q, qv)
+        assert orc.step(P, n) == 0
+        eng.step(n, graph=True)
+    e = H.rel_err(H.conserved(case, eng.state()), H.conserved(case, P))
+    assert np.all(e <= TOL_MANY), e
+    with pytest.raises(abi.MoseError):
+        bad = np.array(case.rec["q"][inlet[0]])
+        bad[1] = -1.0                                     # T0 <= 0 is rejected as at mb_init
+        eng.set_record_params(inlet[0], bad)
