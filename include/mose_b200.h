@@ -197,7 +197,10 @@ typedef struct mb_scheme {
                          (Newstate_Conservative), 1 prim (Newstate_Primitive: the residual taken to the primitive
                          variables through the inverse of the prim -> cons Jacobian, Lib_Newstate.f90:348-531; with
                          n_rk <= 3) */
-  int32_t pad1;
+  int32_t irs;        /* implicit residual smoothing (IRS = t of [MOSE-scheme], Lib_IRS.f90:57-105): the number of Jacobi
+                         sweeps of R* = R + beta d2(R*) along each direction (the reference runs 2); 0 = off, at most
+                         4, with n_rk <= 3. Conservative variables: the residual is scaled to -dt R / vol first and
+                         the update takes it as it is; primitive variables: the raw residual is smoothed */
   double cfl;
   double vnn;         /* default 0.3 (MOSE_Types_m.f90:268) */
   double prandtl;     /* > 0: kl = mu cp / Pr (Mod_Diffusive.f90:303) */
@@ -207,6 +210,7 @@ typedef struct mb_scheme {
   double res_stop;    /* [MOSE-parameters] res-threshold (MOSE_Types_m.f90:247-250, default 1e-10 there): the case
                          stops once the residual diagnostic of rho (mb_status.res[0]) of a step is <= res_stop, as
                          Explicit_Step's end test (Mod_Explicit.f90:363-370); 0 = no residual stop */
+  double irs_beta;    /* [MOSE-scheme] beta of the smoothing (Lib_IRS.f90:41-42, default 0.5), >= 0 */
 } mb_scheme;
 
 typedef struct mb_status {
@@ -254,7 +258,9 @@ int mb_fill_ghosts(mb_ctx* ctx, double* P, void* stream);
 int mb_residual(mb_ctx* ctx, const double* P, double* R, void* stream);
 
 /* RK_Newstate (conservative form) of stage irk (1-based) with residual R and time step dt:
- * P <- update(P, PO, R) at every interior cell (Lib_Newstate.f90:77-143, newstate_cons_body.inc). */
+ * P <- update(P, PO, R) at every interior cell (Lib_Newstate.f90:77-143, newstate_cons_body.inc).
+ * With implicit residual smoothing (mb_scheme.irs > 0) the smoothing of IRS_apply runs first on a copy
+ * of R in the engine's own buffers (Lib_IRS.f90:57-105); R itself is not written. */
 int mb_update(mb_ctx* ctx, double* P, const double* PO, const double* R, int irk, double dt,
               void* stream);
 

@@ -55,6 +55,10 @@ struct mb_ctx {
   int ntiles_aux = 0;
   double* d_scratch = nullptr;  // the engine's own stage buffer (ncell x 5)
   double* d_acc4 = nullptr;     // RK4: conserved accumulator (ncell x 5)
+  double* d_irs = nullptr;      // residual smoothing: two residual buffers (2 x ncell x 5)
+  long long* d_idst = nullptr;  // its first-ghost-layer copies, direction by direction: row idst[e] <- row isrc[e]
+  long long* d_isrc = nullptr;
+  int irs_off[4] = {0, 0, 0, 0};
   struct Geo32 { const double* src; float* buf; long long n; };
   std::vector<Geo32> geo32;     // FP32 geometry copies of the mixed form (source array, copy, elements)
   int ngroups = 1;              // case clocks
@@ -93,7 +97,7 @@ static void free_ctx(mb_ctx* c) {
   if (c->graph) cudaGraphDestroy(c->graph);
   void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
                   c->d_pgsrc, c->d_tab, c->d_tabf, c->d_st, c->d_tiles_sweep, c->d_tiles_aux, c->d_scratch, c->d_acc4, c->d_queue, c->d_recflux, c->d_brec, c->d_bcell,
-                  c->d_physf, c->d_cubicf, c->d_tiles_km};
+                  c->d_physf, c->d_cubicf, c->d_tiles_km, c->d_irs, c->d_idst, c->d_isrc};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& q : c->geo32)
@@ -220,9 +224,11 @@ static int check_mesh(const mb_mesh* mesh, int ngroups) {
 static void free_tables(mb_ctx* c) {
   void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
                   c->d_pgsrc, c->d_tiles_sweep, c->d_tiles_aux, c->d_recflux, c->d_brec, c->d_bcell,
-                  c->d_physf, c->d_cubicf, c->d_tiles_km};
+                  c->d_physf, c->d_cubicf, c->d_tiles_km, c->d_idst, c->d_isrc};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  c->d_idst = nullptr; c->d_isrc = nullptr;
+  for (int d = 0; d < 4; ++d) c->irs_off[d] = 0;
   c->d_physf = nullptr; c->d_cubicf = nullptr; c->d_tiles_km = nullptr; c->ntiles_km = 0;
   c->d_recflux = nullptr; c->d_brec = nullptr; c->d_bcell = nullptr; c->nrec = 0;
   c->d_blk = nullptr; c->d_recmap = nullptr; c->d_rec = nullptr; c->d_grec = nullptr; c->d_phys = nullptr;
@@ -518,6 +524,50 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   c->gf = g;
   c->gf.phys = c->d_physf; c->gf.nphys = (int)physf.size(); c->gf.cubic = c->d_cubicf; c->gf.ncubic = (int)cubicf.size();
   for (int f = 0; f < 3; ++f) { c->gf.phys_off[f] = pof[f]; c->gf.cubic_off[f] = cof[f]; }
+  // ---- residual smoothing: the first ghost layer of the faces of each direction (Ghost_Residual_Extrapolation,
+  // Lib_IRS.f90:119-177): every face cell's ghost from the cell itself, a connection record's from its donor face
+  // cell instead; blocks of a case with fewer directions are left out
+  if (sc->irs > 0) {
+    std::vector<long long> idst, isrc;
+    for (int d = 1; d <= 3; ++d) {
+      c->irs_off[d - 1] = (int)idst.size();
+      std::vector<size_t> fbase(2 * (size_t)mesh->nblk, 0);  // first entry of (block, side) in this direction
+      for (int b = 0; b < mesh->nblk; ++b) {
+        const DBlk& q = hb[b];
+        if (q.ndir < d) continue;
+        const int n[3] = {q.n1, q.n2, q.n3};
+        const int a = (d == 1) ? 1 : 0, bb = (d == 3) ? 1 : 2;  // the two transverse axes
+        for (int side = 0; side < 2; ++side) {
+          fbase[2 * b + side] = idst.size();
+          for (int v = 1; v <= n[bb]; ++v)
+            for (int u = 1; u <= n[a]; ++u) {
+              int cc[3];
+              cc[d - 1] = side ? n[d - 1] : 1;
+              cc[a] = u; cc[bb] = v;
+              int gg[3] = {cc[0], cc[1], cc[2]};
+              gg[d - 1] += side ? 1 : -1;
+              idst.push_back(row(q, gg[0], gg[1], gg[2]));
+              isrc.push_back(row(q, cc[0], cc[1], cc[2]));
+            }
+        }
+      }
+      for (int e = 0; e < mesh->nconn; ++e) {
+        const mb_conn& cn = mesh->conn[e];
+        const mb_bc& r = mesh->rec[cn.rec];
+        if ((r.face + 1) / 2 != d || hb[r.blk].ndir < d) continue;
+        const DBlk& q = hb[r.blk];
+        const int n[3] = {q.n1, q.n2, q.n3};
+        const int a = (d == 1) ? 1 : 0, bb = (d == 3) ? 1 : 2;
+        const int cc[3] = {r.i, r.j, r.k};
+        const size_t pos = fbase[2 * r.blk + ((r.face & 1) ? 0 : 1)] + (size_t)(cc[a] - 1) +
+                           (size_t)(cc[bb] - 1) * n[a];
+        isrc[pos] = row(hb[cn.bs], cn.is, cn.js, cn.ks);
+      }
+    }
+    c->irs_off[3] = (int)idst.size();
+    if ((rc = upload(&c->d_idst, idst.data(), idst.size())) != MB_OK) return rc;
+    if ((rc = upload(&c->d_isrc, isrc.data(), isrc.size())) != MB_OK) return rc;
+  }
   return MB_OK;
 }
 
@@ -527,6 +577,8 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   if (sc->riemann < MB_RS_HLLC || sc->riemann > MB_RS_MICZEKROE) return MB_E_UNSUPPORTED;  // 14 (HLLC-PC) needs prec
   if (sc->sensor < 0 || sc->sensor > 3) return MB_E_UNSUPPORTED;
   if (sc->intvar < 0 || sc->intvar > 1 || (sc->intvar == 1 && sc->n_rk == 4)) return MB_E_UNSUPPORTED;
+  if (sc->irs < 0 || sc->irs > 4 || (sc->irs > 0 && sc->n_rk == 4)) return MB_E_UNSUPPORTED;
+  if (sc->irs > 0 && !(sc->irs_beta >= 0.0 && std::isfinite(sc->irs_beta))) return MB_E_ARG;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
   if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
   if (!(sc->res_stop >= 0.0)) return MB_E_ARG;
@@ -587,6 +639,11 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
     return MB_E_NOMEM;
   }
   if (cudaMemset(c->d_scratch, 0, (size_t)c->ncell * MB_NPRIM * sizeof(double)) != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+  if (sc->irs > 0) {
+    const size_t nb = 2 * (size_t)c->ncell * MB_NPRIM * sizeof(double);
+    if (cudaMalloc((void**)&c->d_irs, nb) != cudaSuccess) { free_ctx(c); return MB_E_NOMEM; }
+    if (cudaMemset(c->d_irs, 0, nb) != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+  }
   if (sc->n_rk == 4) {
     if (cudaMalloc((void**)&c->d_acc4, (size_t)c->ncell * MB_NPRIM * sizeof(double)) != cudaSuccess) {
       free_ctx(c);
@@ -797,6 +854,28 @@ static int fill(mb_ctx* c, double* P, cudaStream_t s, bool fused = true) {
   return MB_OK;
 }
 
+// IRS_apply (Lib_IRS.f90:57-105) on R, the first of the engine's two residual buffers: on the conservative path the
+// scaling -R / vol * dt (dt < 0: each case's clock dt), then per direction the first ghost layer and the Jacobi
+// sweeps, alternating between the two buffers; *out receives the buffer that holds the result
+static int smooth_residual(mb_ctx* c, double* R, double dt, cudaStream_t s, const double** out) {
+  double* cur = R;
+  double* alt = (cur == c->d_irs) ? c->d_irs + (size_t)c->ncell * MB_NPRIM : c->d_irs;
+  if (c->sc.intvar == 0) {
+    CK(irs_scale(c->p, c->d_tiles_aux, c->ntiles_aux, cur, dt, s));
+    c->launches += 1;
+  }
+  for (int d = 1; d <= 3; ++d) {
+    const int n = c->irs_off[d] - c->irs_off[d - 1];
+    if (n <= 0) continue;  // no block of the mesh has this direction
+    CK(irs_ghosts(c->p, c->d_idst + c->irs_off[d - 1], c->d_isrc + c->irs_off[d - 1], n, cur, s));
+    CK(irs_smooth(c->p, c->d_tiles_aux, c->ntiles_aux, cur, alt, d, c->sc.irs, c->sc.irs_beta, s));
+    c->launches += 2;
+    std::swap(cur, alt);
+  }
+  *out = cur;
+  return MB_OK;
+}
+
 int mb_fill_ghosts(mb_ctx* ctx, double* P, void* stream) {
   if (!ctx || !P) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
@@ -816,8 +895,17 @@ int mb_update(mb_ctx* ctx, double* P, const double* PO, const double* R, int irk
   CK(cudaSetDevice(ctx->device));
   Params p = ctx->p;
   p.irk = irk;
-  cudaError_t e = update_cells(p, ctx->d_tiles_aux, ctx->ntiles_aux, P, PO, R, rkc_of(ctx->sc.n_rk, irk), dt,
-                               (cudaStream_t)stream);
+  cudaStream_t s = (cudaStream_t)stream;
+  int prescaled = 0;
+  if (ctx->sc.irs > 0) {  // IRS_apply on the engine's copy of R, then the update takes the smoothed residual
+    double* R0 = ctx->d_irs;
+    CK(cudaMemcpyAsync(R0, R, (size_t)ctx->ncell * MB_NPRIM * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    int rc = smooth_residual(ctx, R0, dt, s, &R);
+    if (rc != MB_OK) return rc;
+    prescaled = ctx->sc.intvar == 0;
+  }
+  cudaError_t e = update_cells(p, ctx->d_tiles_aux, ctx->ntiles_aux, P, PO, R, rkc_of(ctx->sc.n_rk, irk), dt, s,
+                               prescaled);
   ctx->launches += 1;
   CK(e);
   return MB_OK;
@@ -858,6 +946,23 @@ int mb_begin_step(mb_ctx* ctx, const double* P, void* stream) {
   return MB_OK;
 }
 
+// the stage's computation after its ghost fill and boundary records: the fused sweep, or with residual smoothing the
+// sweep's residual, IRS_apply and the update on the smoothed residual (old state in P)
+static int stage_compute(mb_ctx* c, const double* in, const double* P, double* outp, int irk, int last,
+                         cudaStream_t s) {
+  if (c->sc.irs <= 0) return sweep(c, MODE_UPDATE, in, P, outp, nullptr, irk, last, s);
+  int rc = sweep(c, MODE_RESIDUAL, in, nullptr, nullptr, c->d_irs, irk, 0, s);
+  if (rc != MB_OK) return rc;
+  const double* R = nullptr;
+  rc = smooth_residual(c, c->d_irs, -1.0, s, &R);
+  if (rc != MB_OK) return rc;
+  Params p = c->p;
+  p.irk = irk;
+  CK(irs_stage_update(p, c->d_tiles_aux, c->ntiles_aux, in, P, outp, R, rkc_of(c->sc.n_rk, irk), last, s));
+  c->launches += 1;
+  return MB_OK;
+}
+
 static int stage(mb_ctx* c, double* P, double* PO, int irk, cudaStream_t s) {
   const int n = c->sc.n_rk;
   double* S = c->d_scratch;
@@ -869,7 +974,7 @@ static int stage(mb_ctx* c, double* P, double* PO, int irk, cudaStream_t s) {
   rc = records(c, in, s);
   if (rc != MB_OK) return rc;
   const int last = (irk == n) ? 1 : 0;
-  rc = sweep(c, MODE_UPDATE, in, P, outp, nullptr, irk, last, s);
+  rc = stage_compute(c, in, P, outp, irk, last, s);
   if (rc != MB_OK) return rc;
   if (n == 1) {
     CK(cudaMemcpyAsync(P, S, (size_t)c->ncell * MB_NPRIM * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -958,7 +1063,7 @@ int mb_profile_stage(mb_ctx* ctx, double* P, double* PO, int irk, int nrep, floa
     rc = fill(ctx, const_cast<double*>(in), s);
     if (rc == MB_OK) rc = records(ctx, in, s);
     cudaEventRecord(e1, s);
-    if (rc == MB_OK) rc = sweep(ctx, MODE_UPDATE, in, P, outp, nullptr, irk, irk == n ? 1 : 0, s);
+    if (rc == MB_OK) rc = stage_compute(ctx, in, P, outp, irk, irk == n ? 1 : 0, s);
     cudaEventRecord(e2, s);
     cudaEventSynchronize(e2);
     float a = 0.f, b = 0.f;

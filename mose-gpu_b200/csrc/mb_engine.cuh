@@ -946,7 +946,7 @@ MB_HD void bc_apply(const R* v, double* acc) {
 
 MB_HD void cons_update(const Params& p, const double* pc, const double* po, const double* res,
                                             double vol, double dt, double rkc, double tc, double* pn,
-                                            long long row_ = -1) {
+                                            long long row_ = -1, bool prescaled = false) {
   const double strang = 1.0;
   double cons[MB_NP], cold[MB_NP], rl[MB_NP];
   auto prim2cons = [&](const double* q, double* u) {
@@ -969,7 +969,7 @@ MB_HD void cons_update(const Params& p, const double* pc, const double* po, cons
   prim2cons(po, cold);
   prim2cons(pc, cons);
 #pragma unroll
-  for (int s = 0; s < MB_NP; ++s) rl[s] = -res[s] / vol * dt * strang;
+  for (int s = 0; s < MB_NP; ++s) rl[s] = prescaled ? res[s] : -res[s] / vol * dt * strang;  // IRS: prescaled
   if (p.n_rk != 4) {
 #pragma unroll
     for (int s = 0; s < MB_NP; ++s) cons[s] = cold[s] + (cons[s] - cold[s] + rl[s]) * rkc;

@@ -80,7 +80,8 @@ __global__ void k_ghost_copy(const long long* __restrict__ dst, const long long*
 
 // ---- RK_Newstate alone: the conservative update of every interior cell from a given residual ----
 __global__ void __launch_bounds__(32 * TY_AUX) k_update(Params p, const DTile* __restrict__ tiles, double* P,
-                                                        const double* PO, const double* R, double rkc, double dt) {
+                                                        const double* PO, const double* R, double rkc, double dt,
+                                                        int prescaled) {
   const DTile t = tiles[blockIdx.x];
   const DBlk b = p.blk[t.blk];
   DevState* st = p.st + b.grp;
@@ -98,7 +99,7 @@ __global__ void __launch_bounds__(32 * TY_AUX) k_update(Params p, const DTile* _
       T = mn(mx(T, 1.0), 9990.0);
     }
     if (p.intvar) prim_update(p, pc, po, res, ld(b.vol + (r - b.boff)), dt, rkc, pn);
-    else cons_update(p, pc, po, res, ld(b.vol + (r - b.boff)), dt, rkc, T, pn, r);
+    else cons_update(p, pc, po, res, ld(b.vol + (r - b.boff)), dt, rkc, T, pn, r, prescaled != 0);
     bool bad = !(pn[MB_IPR] >= 0.0);
     for (int s = 0; s < MB_NP; ++s) bad = bad || !isfinite(pn[s]);
     if (bad) report_bad_state(st, t.blk, i, j, k);
@@ -196,8 +197,8 @@ cudaError_t dt_cells(const Params& p, const DTile* tiles, int ntiles, const doub
 }
 
 cudaError_t update_cells(const Params& p, const DTile* tiles, int ntiles, double* P, const double* PO, const double* R,
-                         double rkc, double dt, cudaStream_t s) {
-  k_update<<<ntiles, 32 * TY_AUX, 0, s>>>(p, tiles, P, PO, R, rkc, dt);
+                         double rkc, double dt, cudaStream_t s, int prescaled) {
+  k_update<<<ntiles, 32 * TY_AUX, 0, s>>>(p, tiles, P, PO, R, rkc, dt, prescaled);
   return cudaGetLastError();
 }
 

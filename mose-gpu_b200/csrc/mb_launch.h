@@ -69,8 +69,15 @@ cudaError_t ghost_fill(const Params& p, const GhostLists& g, double* P, cudaStre
 cudaError_t dt_cells(const Params& p, const DTile* tiles, int ntiles, const double* P, cudaStream_t s,
                      int only_group = -1);
 cudaError_t update_cells(const Params& p, const DTile* tiles, int ntiles, double* P, const double* PO,
-                         const double* R, double rkc, double dt, cudaStream_t s);
+                         const double* R, double rkc, double dt, cudaStream_t s, int prescaled = 0);
 cudaError_t reset_dt(const Params& p, cudaStream_t s, int only_group = -1);
+// implicit residual smoothing (mb_irs.cu)
+cudaError_t irs_scale(const Params& p, const DTile* tiles, int ntiles, double* R, double dt, cudaStream_t s);
+cudaError_t irs_ghosts(const Params& p, const long long* dst, const long long* src, int n, double* R, cudaStream_t s);
+cudaError_t irs_smooth(const Params& p, const DTile* tiles, int ntiles, const double* Rin, double* Rout, int d,
+                       int njacobi, double beta, cudaStream_t s);
+cudaError_t irs_stage_update(const Params& p, const DTile* tiles, int ntiles, const double* Pin, const double* Pold,
+                             double* Pout, const double* R, double rkc, int last, cudaStream_t s);
 cudaError_t to_float(const double* src, float* dst, long long n, cudaStream_t s);
 cudaError_t clock_step(const Params& p, cudaStream_t s);
 cudaError_t group_reset(const Params& p, int g, int time_clip, double t_end, double res_stop, cudaStream_t s);

@@ -81,10 +81,10 @@ class MBScheme(C.Structure):
     _fields_ = [("limiter", C.c_int32), ("riemann", C.c_int32), ("visc", C.c_int32), ("n_rk", C.c_int32),
                 ("precision", C.c_int32), ("ndir", C.c_int32), ("time_clip", C.c_int32),
                 ("state_check", C.c_int32), ("dt_additive", C.c_int32), ("sensor", C.c_int32),
-                ("intvar", C.c_int32), ("pad1", C.c_int32),
+                ("intvar", C.c_int32), ("irs", C.c_int32),
                 ("cfl", C.c_double), ("vnn", C.c_double),
                 ("prandtl", C.c_double), ("schmidt", C.c_double), ("mco", C.c_double),
-                ("time_threshold", C.c_double), ("res_stop", C.c_double)]
+                ("time_threshold", C.c_double), ("res_stop", C.c_double), ("irs_beta", C.c_double)]
 
 
 class MBStatus(C.Structure):

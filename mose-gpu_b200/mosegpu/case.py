@@ -181,6 +181,8 @@ class Case:
         s.schmidt = d.get("schmidt", 0.7); s.mco = d.get("mco", 1.0)
         s.time_threshold = d.get("time_threshold", 0.0)
         s.res_stop = d.get("res_stop", 0.0)
+        s.irs = d.get("irs", 0)                         # Jacobi sweeps of the residual smoothing (0: off)
+        s.irs_beta = d.get("irs_beta", 0.5)
         return s
 
 

@@ -33,6 +33,7 @@
 //   thermo cache            src/lib/physics/Mod_Thermo_Cache.f90:291-425
 //   state update            src/lib/gpu/newstate_cons_body.inc:1-89, explicit/Lib_Newstate.f90:257-307,
 //                           348-531 (primitive)
+//   residual smoothing      explicit/Lib_IRS.f90:57-236
 //   RK coefficients         explicit/Lib_RK.f90:6-9; classical RK4 with a conserved accumulator (no reference)
 //   local dt                src/lib/gpu/dt_blk.inc:11-222, numerics/time/Mod_dt.f90:15-106
 //   thermo leaves           lib/FLINT/src/lib/Lib_ThermoTransport_dev.f90:54-300
@@ -2113,7 +2114,7 @@ static const double RK4_W[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
 // the cell's accumulator a4: stage 1 a4 = cold + rl/6, stages 2-3 a4 += rl/3, new = cold + C rl; stage 4
 // new = a4 + rl/6 (rl = -R / vol * dt).
 void update_cell(const Ctx& c, const double* po, double* p, const double* res, double vol, double dt, double rkc,
-                 double tc, int rk4 = 0, double* a4 = nullptr) {
+                 double tc, int rk4 = 0, double* a4 = nullptr, bool prescaled = false) {
   const Thermo& th = c.th;
   const double strang = 1.0;
   double cons[NP], cold[NP], rl[NP];
@@ -2134,7 +2135,8 @@ void update_cell(const Ctx& c, const double* po, double* p, const double* res, d
   };
   prim2cons(po, cold);
   prim2cons(p, cons);
-  for (int s = 0; s < NP; ++s) rl[s] = -res[s] / vol * dt * strang;
+  // IRS: the residual arrives scaled (-R / vol * dt * strang) and smoothed (newstate_cons_body.inc, ps_)
+  for (int s = 0; s < NP; ++s) rl[s] = prescaled ? res[s] : -res[s] / vol * dt * strang;
   if (rk4 == 0) {
     for (int s = 0; s < NP; ++s) cons[s] = cold[s] + (cons[s] - cold[s] + rl[s]) * rkc;
   } else if (rk4 < 4) {
@@ -2218,7 +2220,7 @@ void update_cell_prim(const Ctx& c, const double* po, double* p, const double* r
   if (p[0] < 1e-20) p[0] = 1e-20;
 }
 
-void update(Ctx& c, double* P, const double* PO, const double* R, int irk, double dt) {
+void update(Ctx& c, double* P, const double* PO, const double* R, int irk, double dt, bool prescaled = false) {
   const int64_t nc = c.ncell;
   const double rkc = c.sc.n_rk == 4 ? 0.0 : RKC[c.sc.n_rk - 1][irk - 1];
   const bool guard = c.sc.visc != 0;
@@ -2244,7 +2246,7 @@ void update(Ctx& c, double* P, const double* PO, const double* R, int irk, doubl
           else if (c.sc.n_rk == 4)
             update_cell(c, po, p, res, b.vol[lin(b, i, j, k)], dt, rkc, T, irk, &c.acc4[(size_t)r * NP]);
           else
-            update_cell(c, po, p, res, b.vol[lin(b, i, j, k)], dt, rkc, T);
+            update_cell(c, po, p, res, b.vol[lin(b, i, j, k)], dt, rkc, T, 0, nullptr, prescaled);
           bool bad = !(p[IP] >= 0.0);
           for (int s = 0; s < NP; ++s) if (!std::isfinite(p[s])) bad = true;
           if (bad) ++nbad;
@@ -2255,6 +2257,93 @@ void update(Ctx& c, double* P, const double* PO, const double* R, int irk, doubl
   c.st.n_bad_thermo += nth;
   if (nth && c.st.code == MB_OK) c.st.code = MB_E_THERMO;
   if (nbad && c.sc.state_check && c.st.code == MB_OK) c.st.code = MB_E_STATE;
+}
+
+// ---- implicit residual smoothing: IRS_apply (Lib_IRS.f90:57-105) ----
+
+// Ghost_Residual_Extrapolation (irs_ghost_residual, :119-177): the first ghost layer of every face of every block
+// takes the adjacent cell's residual, then every connection record's ghost takes its donor face cell's
+void irs_ghost_residual(const Ctx& c, double* R) {
+  const int64_t nc = c.ncell;
+  for (const Blk& b : c.blk) {
+    auto cp = [&](int64_t g, int64_t m) { for (int s = 0; s < NP; ++s) R[g + s * nc] = R[m + s * nc]; };
+    for (int k = 1; k <= b.n3; ++k)
+      for (int j = 1; j <= b.n2; ++j) {
+        cp(row(b, 0, j, k), row(b, 1, j, k));
+        cp(row(b, b.n1 + 1, j, k), row(b, b.n1, j, k));
+      }
+    for (int k = 1; k <= b.n3; ++k)
+      for (int i = 1; i <= b.n1; ++i) {
+        cp(row(b, i, 0, k), row(b, i, 1, k));
+        cp(row(b, i, b.n2 + 1, k), row(b, i, b.n2, k));
+      }
+    for (int j = 1; j <= b.n2; ++j)
+      for (int i = 1; i <= b.n1; ++i) {
+        cp(row(b, i, j, 0), row(b, i, j, 1));
+        cp(row(b, i, j, b.n3 + 1), row(b, i, j, b.n3));
+      }
+  }
+  // irs_ghost_conn (:180-200): r(receiver ghost behind its face cell) = r(donor face cell)
+  for (const mb_conn& q : c.conn) {
+    const mb_bc& r = c.rec[q.rec];
+    const Blk& bm = c.blk[r.blk];
+    const int gstep = 2 * (r.face % 2) - 1;
+    int ig = r.i, jg = r.j, kg = r.k;
+    if (r.face <= 2) ig -= gstep; else if (r.face <= 4) jg -= gstep; else kg -= gstep;
+    const int64_t cg = row(bm, ig, jg, kg), cd = row(c.blk[q.bs], q.is, q.js, q.ks);
+    for (int s = 0; s < NP; ++s) R[cg + s * nc] = R[cd + s * nc];
+  }
+}
+
+// IRS_apply: scale (Scale_Residual_Cons, irs_scale_blk :108-116: R = -R / vol * dt * strang on the interior, the
+// conservative path only), then per direction the ghost residual and njacobi Jacobi sweeps of
+// R* = (R + beta (R*(c - off) + R*(c + off))) / (1 + 2 beta) over the interior (irs_smooth_blk, :204-236)
+void irs_apply(Ctx& c, double* R, double dt, bool scale) {
+  const int64_t nc = c.ncell;
+  const double strang = 1.0, beta = c.sc.irs_beta;
+  const int njacobi = c.sc.irs;
+  if (scale)
+    for (const Blk& b : c.blk)
+      for (int k = 1; k <= b.n3; ++k)
+        for (int j = 1; j <= b.n2; ++j)
+          for (int i = 1; i <= b.n1; ++i) {
+            const int64_t r = row(b, i, j, k);
+            const double vol_ = b.vol[lin(b, i, j, k)];
+            for (int s = 0; s < NP; ++s) R[r + s * nc] = -R[r + s * nc] / vol_ * dt * strang;
+          }
+  std::vector<double> rs1((size_t)nc * NP), rs2((size_t)nc * NP);
+  for (int d = 1; d <= c.sc.ndir; ++d) {
+    irs_ghost_residual(c, R);
+    for (const Blk& b : c.blk) {
+      const int64_t off = (d == 1) ? 1 : (d == 2 ? (int64_t)b.pi : (int64_t)b.pi * b.pj);
+      const int64_t nflat = (int64_t)b.pi * b.pj * (b.n3 + 2 * GC);
+      for (int s = 0; s < NP; ++s)
+        for (int64_t q = 0; q < nflat; ++q) rs1[b.boff + q + s * nc] = R[b.boff + q + s * nc];
+      for (int jac = 0; jac < njacobi; ++jac) {
+        for (int k = 1; k <= b.n3; ++k)
+          for (int j = 1; j <= b.n2; ++j)
+            for (int i = 1; i <= b.n1; ++i) {
+              const int64_t c0 = row(b, i, j, k);
+              for (int s = 0; s < NP; ++s) {
+                const int64_t x = c0 + s * nc;
+                rs2[x] = (R[x] + beta * (rs1[x - off] + rs1[x + off])) / (1.0 + 2.0 * beta);
+              }
+            }
+        for (int k = 1; k <= b.n3; ++k)
+          for (int j = 1; j <= b.n2; ++j)
+            for (int i = 1; i <= b.n1; ++i) {
+              const int64_t c0 = row(b, i, j, k);
+              for (int s = 0; s < NP; ++s) rs1[c0 + s * nc] = rs2[c0 + s * nc];
+            }
+      }
+      for (int k = 1; k <= b.n3; ++k)
+        for (int j = 1; j <= b.n2; ++j)
+          for (int i = 1; i <= b.n1; ++i) {
+            const int64_t c0 = row(b, i, j, k);
+            for (int s = 0; s < NP; ++s) R[c0 + s * nc] = rs1[c0 + s * nc];
+          }
+    }
+  }
 }
 
 // ---- local dt: dt_blk.inc (min rule) + Thermo_Cache_rrt_blk / _visc_blk ----
@@ -2352,8 +2441,9 @@ struct orc_ctx { Ctx c; };
 int orc_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, orc_ctx** out) {
   if (!mesh || !sc || !th || !out) return MB_E_ARG;
   if (sc->riemann < 1 || sc->riemann > 13 || sc->sensor < 0 || sc->sensor > 3 || sc->intvar < 0 || sc->intvar > 1 ||
-      (sc->intvar == 1 && sc->n_rk == 4))
+      (sc->intvar == 1 && sc->n_rk == 4) || sc->irs < 0 || sc->irs > 4 || (sc->irs > 0 && sc->n_rk == 4))
     return MB_E_UNSUPPORTED;
+  if (sc->irs > 0 && !(sc->irs_beta >= 0.0 && std::isfinite(sc->irs_beta))) return MB_E_ARG;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
   if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
   orc_ctx* o = new orc_ctx();
@@ -2397,8 +2487,15 @@ void orc_destroy(orc_ctx* o) { delete o; }
 int orc_fill_ghosts(orc_ctx* o, double* P) { fill_ghosts(o->c, P); return MB_OK; }
 int orc_residual(orc_ctx* o, const double* P, double* R) { residual(o->c, P, R); return MB_OK; }
 int orc_update(orc_ctx* o, double* P, const double* PO, const double* R, int irk, double dt) {
-  update(o->c, P, PO, R, irk, dt);
-  return o->c.st.code;
+  Ctx& c = o->c;
+  if (c.sc.irs > 0) {  // RK_Newstate with IRS: the smoothing on a copy of R (Newstate_Conservative / _Primitive)
+    std::vector<double> Rs(R, R + c.ncell * NP);
+    irs_apply(c, Rs.data(), dt, c.sc.intvar == 0);
+    update(c, P, PO, Rs.data(), irk, dt, c.sc.intvar == 0);
+  } else {
+    update(c, P, PO, R, irk, dt);
+  }
+  return c.st.code;
 }
 int orc_dt(orc_ctx* o, const double* P, double* dt) { *dt = compute_dt(o->c, P); return MB_OK; }
 
@@ -2419,7 +2516,8 @@ int orc_step(orc_ctx* o, double* P, double* PO, double* R, int nsteps) {
     for (int irk = 1; irk <= c.sc.n_rk; ++irk) {
       fill_ghosts(c, P);
       residual(c, P, R);
-      update(c, P, PO, R, irk, dt);
+      if (c.sc.irs > 0) irs_apply(c, R, dt, c.sc.intvar == 0);
+      update(c, P, PO, R, irk, dt, c.sc.irs > 0 && c.sc.intvar == 0);
     }
     // the residual diagnostic of the step (Compute_Residual_blk, Mod_Diagnostic.f90:64-104; the L2 norm of
     // Mod_Explicit.f90:325-358): sqrt of the sum over the interior cells of (new - old)^2 per primitive variable

@@ -120,6 +120,14 @@ def small_cases():
         ("tgv_prim_roe_8blk", lambda: with_scheme(cs.taylor_green(n=12, blocks=2), intvar=abi.INTVAR_PRIM)),
         ("mb2d_prim_ausm_rk3", lambda: with_scheme(cs.multiblock_2d(cols=2, rows=2, lo=5, hi=9, seed=31, n_rk=3),
                                                    intvar=abi.INTVAR_PRIM)),
+        # implicit residual smoothing (IRS = t): the Jacobi sweeps along every direction, the ghost residual from the
+        # face cell or a connection's donor, on the conservative (scaled) and the primitive (raw) residual
+        ("sod_irs2_hllc", lambda: with_scheme(cs.riemann_1d(n=64), irs=2, cfl=0.8)),
+        ("tgv_irs2_roe_8blk", lambda: with_scheme(cs.taylor_green(n=12, blocks=2, noise=1e-3), irs=2)),
+        ("mb2d_irs3_ausm_rk2_beta07", lambda: with_scheme(cs.multiblock_2d(cols=2, rows=2, lo=5, hi=9, seed=37,
+                                                                           n_rk=2), irs=3, irs_beta=0.7)),
+        ("duct3d_irs1_hllc_beta03", lambda: with_scheme(cs.duct_3d(), irs=1, irs_beta=0.3)),
+        ("sod_prim_irs4_hllc", lambda: with_scheme(cs.riemann_1d(n=64), intvar=abi.INTVAR_PRIM, irs=4)),
         # symmetry (300), isothermal walls (302) and the back-pressure outlet (406)
         ("duct3d_hllc_vanleer", lambda: cs.duct_3d()),
         ("duct3d_roe_vanalbada_rk4", lambda: cs.duct_3d(widths=(5, 6), heights=(4, 3), depths=(4,),

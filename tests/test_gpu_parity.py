@@ -218,7 +218,7 @@ def test_multiblock_2d_many_steps_fp64_and_mixed(torch_cuda):
 
 
 @pytest.mark.parametrize("cid", ["sod_hllc_minmod", "tgv_hllc_minmod_8blk", "mb2d_ausm_vanleer_rk4",
-                                 "duct3d_hllc_vanleer"])
+                                 "duct3d_hllc_vanleer", "tgv_irs2_roe_8blk"])
 def test_residual_diagnostic_matches_the_oracle(torch_cuda, cid):
     """The residual diagnostic accumulated in the fused last stage (sum of (new - old)^2, reduced per tile) equals
     the oracle's after one and after several steps in the FP64 form; the mixed form's agrees to its accuracy."""
@@ -294,3 +294,27 @@ def test_record_params_changed_between_steps_match_the_oracle(torch_cuda):
         bad = np.array(case.rec["q"][inlet[0]])
         bad[1] = -1.0                                     # T0 <= 0 is rejected as at mb_init
         eng.set_record_params(inlet[0], bad)
+
+
+@pytest.mark.parametrize("cid", ["tgv_irs2_roe_8blk", "mb2d_irs3_ausm_rk2_beta07", "duct3d_irs1_hllc_beta03"])
+def test_irs_mixed_within_gate_and_stages_match_fused(torch_cuda, cid):
+    """With residual smoothing: the mixed form (FP32 fluxes, the smoothing and the update in FP64) stays within
+    L2(rho) 1e-5 of the FP64 form after 20 steps, and the reference's call sequence (begin_step + stage 1..n)
+    equals mb_step bit for bit."""
+    from mosegpu.engine import Engine
+    case = dict(H.small_cases())[cid]()
+    a = Engine(case, precision=abi.PREC_FP64)
+    b = Engine(case, precision=abi.PREC_MIXED)
+    a.step(20, graph=True)
+    b.step(20, graph=True)
+    assert a.status().code == 0 and b.status().code == 0
+    l1, l2, li = H.norms(H.conserved(case, b.state()), H.conserved(case, a.state()))
+    assert l2[0] < 1e-5, l2
+    c, d = Engine(case), Engine(case)
+    for _ in range(3):
+        c.begin_step()
+        for irk in range(1, case.scheme["n_rk"] + 1):
+            c.stage(irk)
+    d.step(3, graph=False)
+    m = case.interior_mask()
+    assert np.array_equal(c.state()[:, m], d.state()[:, m])
