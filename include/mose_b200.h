@@ -211,6 +211,13 @@ typedef struct mb_scheme {
                          stops once the residual diagnostic of rho (mb_status.res[0]) of a step is <= res_stop, as
                          Explicit_Step's end test (Mod_Explicit.f90:363-370); 0 = no residual stop */
   double irs_beta;    /* [MOSE-scheme] beta of the smoothing (Lib_IRS.f90:41-42, default 0.5), >= 0 */
+  int32_t local_dt;   /* time-accurate = false (Mod_Explicit.f90:122-128): every cell advances with its own local step
+                         (dtlocal of Compute_dt, taken from the state at the start of the step), the simulated time
+                         does not advance (a steady run ends by res_stop or by the step count); 0 = time-accurate, the
+                         global minimum step */
+  int32_t cfl_rise;   /* [MOSE-parameters] cfl-rise-threshold (rampa_iter, Mod_dt.f90:57-58): the local steps are scaled
+                         by iter / cfl_rise while the step count iter (1 for the first step of mb_init or
+                         mb_group_reset) is below it; 0 = no ramp */
 } mb_scheme;
 
 typedef struct mb_status {
@@ -265,7 +272,9 @@ int mb_update(mb_ctx* ctx, double* P, const double* PO, const double* R, int irk
               void* stream);
 
 /* Compute_dt: the global minimum local step of P (interior cells), written to *dt_host
- * (Mod_dt.f90:15-243, dt_blk.inc:11-222). Synchronises the stream. */
+ * (Mod_dt.f90:15-243, dt_blk.inc:11-222), with the cfl-rise factor of case 0's next step. Synchronises
+ * the stream. With local time stepping (mb_scheme.local_dt) mb_update takes each cell's own step from PO
+ * and ignores its dt argument. */
 int mb_dt(mb_ctx* ctx, const double* P, double* dt_host, void* stream);
 
 /* One fused stage: ghost fill of the stage input, then ONE sweep that computes every face flux once,

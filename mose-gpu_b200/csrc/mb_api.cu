@@ -236,10 +236,10 @@ static void free_tables(mb_ctx* c) {
   c->d_tiles_sweep = nullptr; c->d_tiles_aux = nullptr;
 }
 
-// the sweep unit of a scheme: the benchmarked solvers' own (the solver a compile-time constant) unless a shock sensor
-// or the primitive update is on, which only the run-time solver unit carries
+// the sweep unit of a scheme: the benchmarked solvers' own (the solver a compile-time constant) unless a shock sensor,
+// the primitive update or local time stepping is on, which only the run-time solver unit carries
 static int sweep_unit(const mb_scheme* sc) {
-  return (mb_effective_sensor(sc->riemann, sc->sensor) || sc->intvar) ? 0 : sc->riemann;
+  return (mb_effective_sensor(sc->riemann, sc->sensor) || sc->intvar || sc->local_dt) ? 0 : sc->riemann;
 }
 
 // record types with physical ghosts (Fill_Ghost_Cell_blk, Lib_Extrapolation.f90:643-730)
@@ -579,6 +579,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   if (sc->intvar < 0 || sc->intvar > 1 || (sc->intvar == 1 && sc->n_rk == 4)) return MB_E_UNSUPPORTED;
   if (sc->irs < 0 || sc->irs > 4 || (sc->irs > 0 && sc->n_rk == 4)) return MB_E_UNSUPPORTED;
   if (sc->irs > 0 && !(sc->irs_beta >= 0.0 && std::isfinite(sc->irs_beta))) return MB_E_ARG;
+  if (sc->local_dt < 0 || sc->local_dt > 1 || sc->cfl_rise < 0) return MB_E_ARG;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
   if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
   if (!(sc->res_stop >= 0.0)) return MB_E_ARG;
@@ -627,6 +628,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
       h.time_clip = sc->time_clip;
       h.t_end = sc->time_clip ? sc->time_threshold : 0.0;
       h.res_stop = sc->res_stop;
+      h.rampf = (1 < sc->cfl_rise) ? 1.0 / sc->cfl_rise : 1.0;  // the factor of step 1
     }
     if (cudaMemcpy(c->d_st, hs.data(), ngroups * sizeof(DevState), cudaMemcpyHostToDevice) != cudaSuccess) {
       free_ctx(c);
@@ -668,6 +670,8 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   p.wm = th->wm; p.ri = RUNIV / th->wm; p.iri = th->wm / RUNIV;
   p.sd = mb_effective_sensor(sc->riemann, sc->sensor);
   p.intvar = sc->intvar;
+  p.local_dt = sc->local_dt;
+  p.cfl_rise = sc->cfl_rise;
   p.lim = sc->limiter; p.rs = sc->riemann; p.visc = sc->visc ? 1 : 0; p.ndir = sc->ndir; p.dt_additive = sc->dt_additive;
   p.guard = sc->visc ? 1 : 0; p.state_check = sc->state_check;
   p.cfl = sc->cfl; p.vnn = sc->vnn; p.prandtl = sc->prandtl; p.schmidt = sc->schmidt; p.mco = sc->mco;
@@ -857,11 +861,11 @@ static int fill(mb_ctx* c, double* P, cudaStream_t s, bool fused = true) {
 // IRS_apply (Lib_IRS.f90:57-105) on R, the first of the engine's two residual buffers: on the conservative path the
 // scaling -R / vol * dt (dt < 0: each case's clock dt), then per direction the first ghost layer and the Jacobi
 // sweeps, alternating between the two buffers; *out receives the buffer that holds the result
-static int smooth_residual(mb_ctx* c, double* R, double dt, cudaStream_t s, const double** out) {
+static int smooth_residual(mb_ctx* c, double* R, double dt, const double* Pold, cudaStream_t s, const double** out) {
   double* cur = R;
   double* alt = (cur == c->d_irs) ? c->d_irs + (size_t)c->ncell * MB_NPRIM : c->d_irs;
   if (c->sc.intvar == 0) {
-    CK(irs_scale(c->p, c->d_tiles_aux, c->ntiles_aux, cur, dt, s));
+    CK(irs_scale(c->p, c->d_tiles_aux, c->ntiles_aux, cur, dt, Pold, s));
     c->launches += 1;
   }
   for (int d = 1; d <= 3; ++d) {
@@ -900,7 +904,7 @@ int mb_update(mb_ctx* ctx, double* P, const double* PO, const double* R, int irk
   if (ctx->sc.irs > 0) {  // IRS_apply on the engine's copy of R, then the update takes the smoothed residual
     double* R0 = ctx->d_irs;
     CK(cudaMemcpyAsync(R0, R, (size_t)ctx->ncell * MB_NPRIM * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    int rc = smooth_residual(ctx, R0, dt, s, &R);
+    int rc = smooth_residual(ctx, R0, dt, PO, s, &R);
     if (rc != MB_OK) return rc;
     prescaled = ctx->sc.intvar == 0;
   }
@@ -926,11 +930,15 @@ int mb_dt(mb_ctx* ctx, const double* P, double* dt_host, void* stream) {
   int rc = dt_min(ctx, P, s);
   if (rc != MB_OK) return rc;
   unsigned long long bits;
+  int steps = 0;
   CK(cudaMemcpyAsync(&bits, &ctx->d_st->dtmin_bits, sizeof(bits), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&steps, &ctx->d_st->steps, sizeof(steps), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   double dm;
   memcpy(&dm, &bits, sizeof(dm));
-  *dt_host = std::min(dm, 1e5);
+  const int iter = steps + 1;  // the ramp factor of the case's next step (cfl-rise-threshold)
+  const double f = (iter < ctx->sc.cfl_rise) ? (double)iter / ctx->sc.cfl_rise : 1.0;
+  *dt_host = std::min(dm * f, 1e5);
   ctx->dt_valid = true;  // the device minimum now belongs to P
   return MB_OK;
 }
@@ -954,7 +962,7 @@ static int stage_compute(mb_ctx* c, const double* in, const double* P, double* o
   int rc = sweep(c, MODE_RESIDUAL, in, nullptr, nullptr, c->d_irs, irk, 0, s);
   if (rc != MB_OK) return rc;
   const double* R = nullptr;
-  rc = smooth_residual(c, c->d_irs, -1.0, s, &R);
+  rc = smooth_residual(c, c->d_irs, -1.0, P, s, &R);
   if (rc != MB_OK) return rc;
   Params p = c->p;
   p.irk = irk;

@@ -1221,6 +1221,14 @@ MB_HD double cell_dt(const Params& p, const DBlk& b, long long l, const double* 
   return cell_dt_t<double>(p, b, l, pl);
 }
 
+// the step of a cell in the state update: the case's dt, or with local time stepping (time-accurate = false) the
+// cell's own dtlocal, from its state at the start of the step, times the step's ramp factor (dt_blk.inc: dtlocal =
+// dtc * rampa_fac)
+__device__ __forceinline__ double step_dt(const Params& p, const DBlk& b, const DevState* st, long long l,
+                                          const double* po, double dt) {
+  return p.local_dt ? cell_dt(p, b, l, po) * st->rampf : dt;
+}
+
 // min over the CTA of a positive double, then one atomic into the device clock
 __device__ __forceinline__ void cta_min_dt(DevState* st, double v, double* sred) {
   const unsigned full = 0xffffffffu;
@@ -1448,9 +1456,16 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
           Tc = mn(mx(Tc, 1.0), 9990.0);
         }
         const double vol = ld(b.vol + (r - b.boff));
-        if (RS == 0 && p.intvar) prim_update(p, pc, po, acc, vol, dt, rkc, pn);
-        else if (Fast<R>::on) cons_update_fast(p, pc, po, acc, vol, dt, rkc, Tc, pn, r);
-        else cons_update(p, pc, po, acc, vol, dt, rkc, Tc, pn, r);
+        double dtc = dt;
+        if (RS == 0 && p.local_dt) {  // the cell's own step in the flux type (FP64 in the parity form)
+          R pr[MB_NP];
+#pragma unroll
+          for (int s = 0; s < MB_NP; ++s) pr[s] = cvt<R>(po[s]);
+          dtc = (double)cell_dt_t<R>(p, b, r - b.boff, pr) * st->rampf;
+        }
+        if (RS == 0 && p.intvar) prim_update(p, pc, po, acc, vol, dtc, rkc, pn);
+        else if (Fast<R>::on) cons_update_fast(p, pc, po, acc, vol, dtc, rkc, Tc, pn, r);
+        else cons_update(p, pc, po, acc, vol, dtc, rkc, Tc, pn, r);
         bool bad = !(pn[MB_IPR] >= 0.0);
 #pragma unroll
         for (int s = 0; s < MB_NP; ++s) bad = bad || !isfinite(pn[s]);

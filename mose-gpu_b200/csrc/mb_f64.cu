@@ -98,8 +98,9 @@ __global__ void __launch_bounds__(32 * TY_AUX) k_update(Params p, const DTile* _
       if (T != T) T = 300.0;
       T = mn(mx(T, 1.0), 9990.0);
     }
-    if (p.intvar) prim_update(p, pc, po, res, ld(b.vol + (r - b.boff)), dt, rkc, pn);
-    else cons_update(p, pc, po, res, ld(b.vol + (r - b.boff)), dt, rkc, T, pn, r, prescaled != 0);
+    const double dtc = step_dt(p, b, st, r - b.boff, po, dt);
+    if (p.intvar) prim_update(p, pc, po, res, ld(b.vol + (r - b.boff)), dtc, rkc, pn);
+    else cons_update(p, pc, po, res, ld(b.vol + (r - b.boff)), dtc, rkc, T, pn, r, prescaled != 0);
     bool bad = !(pn[MB_IPR] >= 0.0);
     for (int s = 0; s < MB_NP; ++s) bad = bad || !isfinite(pn[s]);
     if (bad) report_bad_state(st, t.blk, i, j, k);
@@ -139,15 +140,19 @@ __global__ void k_clock(Params p) {
       st->done = 1;
       continue;
     }
+    // cfl-rise-threshold: the factor of step iter (Mod_dt.f90:57-58); the minimum of the scaled local steps is the
+    // scaled minimum (a product with a positive factor rounds monotonically)
+    const int iter = st->steps + 1;
+    st->rampf = (iter < p.cfl_rise) ? (double)iter / p.cfl_rise : 1.0;
     double dtg = 1e5;
     double dm = __longlong_as_double((long long)st->dtmin_bits);
-    dtg = mn(dm, dtg);
-    if (st->time_clip) {
+    dtg = mn(dm * st->rampf, dtg);
+    if (st->time_clip && !p.local_dt) {
       double rem = st->t_end - st->time;
       if (rem > 0.0 && dtg > rem) dtg = rem * (1.0 + 1e-12);
     }
     st->dt = dtg;
-    st->time = st->time + dtg;
+    if (!p.local_dt) st->time = st->time + dtg;  // time-accurate = false: no simulated time (Mod_Explicit.f90:124-128)
     st->steps = st->steps + 1;
     st->dtmin_bits = (unsigned long long)__double_as_longlong(1e300);
     for (int v = 0; v < MB_NP; ++v) st->res2[v] = 0.0;
@@ -162,6 +167,7 @@ __global__ void k_group_reset(Params p, int g, int time_clip, double t_end, doub
   st->n_bad_state = 0; st->n_bad_thermo = 0;
   st->bad_blk = 0; st->bad_i = 0; st->bad_j = 0; st->bad_k = 0; st->first_bad_claimed = 0;
   st->time_clip = time_clip; st->done = 0; st->t_end = t_end; st->res_stop = res_stop;
+  st->rampf = (1 < p.cfl_rise) ? 1.0 / p.cfl_rise : 1.0;  // the factor of step 1 (the update hook before any step)
   for (int v = 0; v < MB_NP; ++v) st->res2[v] = 0.0;
 }
 

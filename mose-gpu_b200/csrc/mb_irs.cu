@@ -11,21 +11,30 @@
 
 namespace mb {
 
-// Scale_Residual_Cons (irs_scale_blk, Lib_IRS.f90:108-116): R = -R / vol * dt * strang on the interior cells;
-// dt < 0: the case's clock dt (the stage path), else the given dt (mb_update)
+// Scale_Residual_Cons (irs_scale_blk, Lib_IRS.f90:108-116): R = -R / vol * dtlocal * strang on the interior cells;
+// dt < 0: the case's clock dt (the stage path), else the given dt (mb_update); with local time stepping each cell's
+// own step from Pold, the state at the start of the step
 __global__ void __launch_bounds__(32 * TY_AUX) k_irs_scale(Params p, const DTile* __restrict__ tiles, double* R,
-                                                           double dt_arg) {
+                                                           double dt_arg, const double* __restrict__ Pold) {
   const DTile t = tiles[blockIdx.x];
   const DBlk b = p.blk[t.blk];
   const int i = t.i0 + (threadIdx.x & 31), j = t.j0 + (threadIdx.x >> 5);
   if (i > b.n1 || j > b.n2) return;
   const double strang = 1.0;
-  const double dt = dt_arg >= 0.0 ? dt_arg : p.st[b.grp].dt;
+  const DevState* st = p.st + b.grp;
+  const double dt = dt_arg >= 0.0 ? dt_arg : st->dt;
   for (int k = t.k0; k < t.k1; ++k) {
     const long long r = row(b, i, j, k);
     const double vol = ld(b.vol + (r - b.boff));
+    double dtc = dt;
+    if (p.local_dt) {
+      double po[MB_NP];
 #pragma unroll
-    for (int s = 0; s < MB_NP; ++s) R[r + s * p.nc] = -R[r + s * p.nc] / vol * dt * strang;
+      for (int s = 0; s < MB_NP; ++s) po[s] = Pold[r + s * p.nc];
+      dtc = step_dt(p, b, st, r - b.boff, po, dt);
+    }
+#pragma unroll
+    for (int s = 0; s < MB_NP; ++s) R[r + s * p.nc] = -R[r + s * p.nc] / vol * dtc * strang;
   }
 }
 
@@ -113,8 +122,9 @@ __global__ void __launch_bounds__(32 * TY_AUX) k_irs_stage_update(Params p, cons
         T = mn(mx(T, 1.0), 9990.0);
       }
       const double vol = ld(b.vol + (r - b.boff));
-      if (p.intvar) prim_update(p, pc, po, res, vol, dt, rkc, pn);
-      else cons_update(p, pc, po, res, vol, dt, rkc, T, pn, r, true);
+      const double dtc = step_dt(p, b, st, r - b.boff, po, dt);
+      if (p.intvar) prim_update(p, pc, po, res, vol, dtc, rkc, pn);
+      else cons_update(p, pc, po, res, vol, dtc, rkc, T, pn, r, true);
       bool bad = !(pn[MB_IPR] >= 0.0);
 #pragma unroll
       for (int s = 0; s < MB_NP; ++s) bad = bad || !isfinite(pn[s]);
@@ -154,8 +164,9 @@ __global__ void k_irs_ghost(const long long* __restrict__ dst, const long long* 
 }
 
 // ---- launchers ----
-cudaError_t irs_scale(const Params& p, const DTile* tiles, int ntiles, double* R, double dt, cudaStream_t s) {
-  k_irs_scale<<<ntiles, 32 * TY_AUX, 0, s>>>(p, tiles, R, dt);
+cudaError_t irs_scale(const Params& p, const DTile* tiles, int ntiles, double* R, double dt, const double* Pold,
+                      cudaStream_t s) {
+  k_irs_scale<<<ntiles, 32 * TY_AUX, 0, s>>>(p, tiles, R, dt, Pold);
   return cudaGetLastError();
 }
 

@@ -72,7 +72,8 @@ cudaError_t update_cells(const Params& p, const DTile* tiles, int ntiles, double
                          const double* R, double rkc, double dt, cudaStream_t s, int prescaled = 0);
 cudaError_t reset_dt(const Params& p, cudaStream_t s, int only_group = -1);
 // implicit residual smoothing (mb_irs.cu)
-cudaError_t irs_scale(const Params& p, const DTile* tiles, int ntiles, double* R, double dt, cudaStream_t s);
+cudaError_t irs_scale(const Params& p, const DTile* tiles, int ntiles, double* R, double dt, const double* Pold,
+                      cudaStream_t s);
 cudaError_t irs_ghosts(const Params& p, const long long* dst, const long long* src, int n, double* R, cudaStream_t s);
 cudaError_t irs_smooth(const Params& p, const DTile* tiles, int ntiles, const double* Rin, double* Rout, int d,
                        int njacobi, double beta, cudaStream_t s);

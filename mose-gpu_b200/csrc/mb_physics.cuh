@@ -87,6 +87,7 @@ struct DevState {
   double res2[MB_NP];             // sum over the case's interior cells of (new - old)^2 of the step's primitive state
                                   // (the fused last stage accumulates it; zeroed at the step's start)
   double res_stop;                // the case stops once sqrt(res2[0]) of a step is <= res_stop (0: never)
+  double rampf;                   // cfl-rise-threshold factor of the current step (1 without a ramp)
 };
 
 struct Params {
@@ -104,6 +105,8 @@ struct Params {
   double iri;              // 1 / ri (the mixed form's state update multiplies by it)
   int sd;                  // the shock sensor in effect (sd_dev): 0 none, 1 Tramel, 2 Chen
   int intvar;              // integration variables: 0 conservative, 1 primitive
+  int local_dt;            // time-accurate = false: each cell's own step (from the state at the start of the step)
+  int cfl_rise;            // cfl-rise-threshold (0: no ramp)
   int lim, rs, visc, ndir, dt_additive, guard, state_check;
   double cfl, vnn, prandtl, schmidt, mco;
   void* recflux;           // boundary-record contributions [record][10] in the flux type (k_records)

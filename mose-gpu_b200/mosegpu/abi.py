@@ -84,7 +84,8 @@ class MBScheme(C.Structure):
                 ("intvar", C.c_int32), ("irs", C.c_int32),
                 ("cfl", C.c_double), ("vnn", C.c_double),
                 ("prandtl", C.c_double), ("schmidt", C.c_double), ("mco", C.c_double),
-                ("time_threshold", C.c_double), ("res_stop", C.c_double), ("irs_beta", C.c_double)]
+                ("time_threshold", C.c_double), ("res_stop", C.c_double), ("irs_beta", C.c_double),
+                ("local_dt", C.c_int32), ("cfl_rise", C.c_int32)]
 
 
 class MBStatus(C.Structure):

@@ -183,6 +183,8 @@ class Case:
         s.res_stop = d.get("res_stop", 0.0)
         s.irs = d.get("irs", 0)                         # Jacobi sweeps of the residual smoothing (0: off)
         s.irs_beta = d.get("irs_beta", 0.5)
+        s.local_dt = d.get("local_dt", 0)               # time-accurate = false: each cell its own step
+        s.cfl_rise = d.get("cfl_rise", 0)               # cfl-rise-threshold
         return s
 
 

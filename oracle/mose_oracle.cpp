@@ -2220,7 +2220,8 @@ void update_cell_prim(const Ctx& c, const double* po, double* p, const double* r
   if (p[0] < 1e-20) p[0] = 1e-20;
 }
 
-void update(Ctx& c, double* P, const double* PO, const double* R, int irk, double dt, bool prescaled = false) {
+void update(Ctx& c, double* P, const double* PO, const double* R, int irk, double dt, bool prescaled = false,
+            const double* dtl = nullptr) {
   const int64_t nc = c.ncell;
   const double rkc = c.sc.n_rk == 4 ? 0.0 : RKC[c.sc.n_rk - 1][irk - 1];
   const bool guard = c.sc.visc != 0;
@@ -2241,12 +2242,13 @@ void update(Ctx& c, double* P, const double* PO, const double* R, int irk, doubl
             if (T != T) T = 300.0;
             T = std::min(std::max(T, 1.0), 9990.0);
           }
+          const double dtc = dtl ? dtl[r] : dt;  // time-accurate = false: the cell's own dtlocal
           if (c.sc.intvar == 1)
-            update_cell_prim(c, po, p, res, b.vol[lin(b, i, j, k)], dt, rkc);
+            update_cell_prim(c, po, p, res, b.vol[lin(b, i, j, k)], dtc, rkc);
           else if (c.sc.n_rk == 4)
-            update_cell(c, po, p, res, b.vol[lin(b, i, j, k)], dt, rkc, T, irk, &c.acc4[(size_t)r * NP]);
+            update_cell(c, po, p, res, b.vol[lin(b, i, j, k)], dtc, rkc, T, irk, &c.acc4[(size_t)r * NP]);
           else
-            update_cell(c, po, p, res, b.vol[lin(b, i, j, k)], dt, rkc, T, 0, nullptr, prescaled);
+            update_cell(c, po, p, res, b.vol[lin(b, i, j, k)], dtc, rkc, T, 0, nullptr, prescaled);
           bool bad = !(p[IP] >= 0.0);
           for (int s = 0; s < NP; ++s) if (!std::isfinite(p[s])) bad = true;
           if (bad) ++nbad;
@@ -2298,7 +2300,7 @@ void irs_ghost_residual(const Ctx& c, double* R) {
 // IRS_apply: scale (Scale_Residual_Cons, irs_scale_blk :108-116: R = -R / vol * dt * strang on the interior, the
 // conservative path only), then per direction the ghost residual and njacobi Jacobi sweeps of
 // R* = (R + beta (R*(c - off) + R*(c + off))) / (1 + 2 beta) over the interior (irs_smooth_blk, :204-236)
-void irs_apply(Ctx& c, double* R, double dt, bool scale) {
+void irs_apply(Ctx& c, double* R, double dt, bool scale, const double* dtl = nullptr) {
   const int64_t nc = c.ncell;
   const double strang = 1.0, beta = c.sc.irs_beta;
   const int njacobi = c.sc.irs;
@@ -2308,8 +2310,8 @@ void irs_apply(Ctx& c, double* R, double dt, bool scale) {
         for (int j = 1; j <= b.n2; ++j)
           for (int i = 1; i <= b.n1; ++i) {
             const int64_t r = row(b, i, j, k);
-            const double vol_ = b.vol[lin(b, i, j, k)];
-            for (int s = 0; s < NP; ++s) R[r + s * nc] = -R[r + s * nc] / vol_ * dt * strang;
+            const double vol_ = b.vol[lin(b, i, j, k)], dtl_ = dtl ? dtl[r] : dt;
+            for (int s = 0; s < NP; ++s) R[r + s * nc] = -R[r + s * nc] / vol_ * dtl_ * strang;
           }
   std::vector<double> rs1((size_t)nc * NP), rs2((size_t)nc * NP);
   for (int d = 1; d <= c.sc.ndir; ++d) {
@@ -2347,85 +2349,101 @@ void irs_apply(Ctx& c, double* R, double dt, bool scale) {
 }
 
 // ---- local dt: dt_blk.inc (min rule) + Thermo_Cache_rrt_blk / _visc_blk ----
-double compute_dt(Ctx& c, const double* P) {
+// the local step of one interior cell of P (Compute_dt_blk, dt_blk.inc:11-191), before the ramp factor
+double cell_dt(const Ctx& c, const Blk& b, const double* P, int i, int j, int k) {
   const int64_t nc = c.ncell;
   const Thermo& th = c.th;
+  int64_t r = row(b, i, j, k);
+  double pl[NP];
+  for (int s = 0; s < NP; ++s) pl[s] = P[r + s * nc];
+  double rho, Rg;
+  rotot_rtot(th, pl[0], rho, Rg);
+  double Tc = pl[IP] / (rho * Rg);
+  double Sound = f_ss(th, pl[0], pl[IP], rho, Rg);
+  double dtc = 1e8;
+  if (c.sc.dt_additive) {  // dt-rule = additive (dt_blk.inc:79-155)
+    double ra_c = 0.0, ra_v = 0.0;
+    for (int d = 0; d < c.sc.ndir; ++d) {
+      double m0 = mv(b, d, 0, i, j, k), m1 = mv(b, d, 1, i, j, k), m2 = mv(b, d, 2, i, j, k);
+      double gn = std::sqrt(m0 * m0 + m1 * m1 + m2 * m2);
+      double vel_ = std::fabs(pl[IU] * m0 + pl[IV] * m1 + pl[IW] * m2) / gn;
+      double lambda = vel_ + Sound;
+      ra_c = ra_c + lambda * gn;
+      ra_v = ra_v + gn * gn;
+    }
+    if (c.sc.visc) {
+      if (c.sc.ndir == 3) {
+        double g[3][3];
+        for (int d = 0; d < 3; ++d) for (int a = 0; a < 3; ++a) g[d][a] = mv(b, d, a, i, j, k);
+        auto dot = [&](int p, int q) { return g[p][0] * g[q][0] + g[p][1] * g[q][1] + g[p][2] * g[q][2]; };
+        auto nr = [&](int p) { return std::sqrt(g[p][0] * g[p][0] + g[p][1] * g[p][1] + g[p][2] * g[p][2]); };
+        double c12 = dot(0, 1) / (nr(0) * nr(1)), c13 = dot(0, 2) / (nr(0) * nr(2)), c23 = dot(1, 2) / (nr(1) * nr(2));
+        double ss = c12 * c12 + c13 * c13 + c23 * c23;
+        double qp = c12 * c13 * c23;
+        if (ss + 2.0 * qp > 1.0) {
+          double mr = 2.0 * std::sqrt(ss / 3.0) *
+                      std::cos(std::acos(std::max(-1.0, std::min(1.0, 3.0 * std::sqrt(3.0) * qp / std::pow(ss, 1.5)))) / 3.0);
+          ra_v = ra_v * 0.25 * (2.0 + mr + 1.0 / mr);
+        }
+      }
+      double Ta = pl[IP] / (rho * Rg);
+      int ta = tidx(th, Ta);
+      double tda = Ta - ta;
+      double cpa = f_cp(th, pl[0], ta, tda, rho);
+      double cva = cpa - Rg;
+      double mila, kla;
+      wilke(th, pl[0], rho, ta, tda, mila, kla);
+      if (c.sc.prandtl > 0.0) kla = mila * cpa / c.sc.prandtl;
+      const double mie = 0.0, prt = 0.85;
+      double Dmx = std::max(4.0 / 3.0 * (mila + mie) / rho, (kla + mie * cpa / prt) / (rho * cva));
+      dtc = 1.0 / (ra_c / c.sc.cfl + Dmx * ra_v / c.sc.vnn);
+    } else {
+      dtc = c.sc.cfl / ra_c;
+    }
+  } else {
+  for (int d = 0; d < c.sc.ndir; ++d) {
+    double m0 = mv(b, d, 0, i, j, k), m1 = mv(b, d, 1, i, j, k), m2 = mv(b, d, 2, i, j, k);
+    double nrm = std::sqrt(m0 * m0 + m1 * m1 + m2 * m2);
+    double v0 = m0 / nrm, v1 = m1 / nrm, v2 = m2 / nrm;
+    double vel_ = std::fabs(pl[IU] * v0 + pl[IV] * v1 + pl[IW] * v2);
+    double lambda = vel_ + Sound;
+    double dtd = dlv(b, d, i, j, k) / lambda * c.sc.cfl;
+    dtc = std::min(dtd, dtc);
+  }
+  if (c.sc.visc) {
+    int ti = tidx(th, Tc);
+    double td = Tc - ti, mil, kl;
+    wilke(th, pl[0], rho, ti, td, mil, kl);
+    double mi = 0.0 + mil;
+    for (int d = 0; d < c.sc.ndir; ++d) {
+      double dl = dlv(b, d, i, j, k);
+      double dtd = (rho * (dl * dl) * c.sc.vnn) / mi;
+      dtc = std::min(dtd, dtc);
+    }
+  }
+  }
+  return dtc;
+}
+
+// cfl-rise-threshold (rampa_iter, Mod_dt.f90:57-58): the step's dt factor iter / rampa_iter while iter < rampa_iter, iter
+// counting this step
+double ramp_factor(const Ctx& c) {
+  const int iter = c.st.steps + 1;
+  return (iter < c.sc.cfl_rise) ? (double)iter / c.sc.cfl_rise : 1.0;
+}
+
+// Compute_dt: dtglobal = min(1e5, the cells' local steps times the ramp factor); with local time stepping (time-accurate
+// = false) the cells' own steps, in dtl (per row of P, interior cells), are the step of each cell
+double compute_dt(Ctx& c, const double* P, std::vector<double>* dtl = nullptr) {
   double dtglobal = 1e5;  // Mod_Explicit.f90:122
+  const double rampa = ramp_factor(c);
   for (const Blk& b : c.blk) {
 #pragma omp parallel for collapse(2) schedule(static) reduction(min : dtglobal)
     for (int k = 1; k <= b.n3; ++k)
       for (int j = 1; j <= b.n2; ++j)
         for (int i = 1; i <= b.n1; ++i) {
-          int64_t r = row(b, i, j, k);
-          double pl[NP];
-          for (int s = 0; s < NP; ++s) pl[s] = P[r + s * nc];
-          double rho, Rg;
-          rotot_rtot(th, pl[0], rho, Rg);
-          double Tc = pl[IP] / (rho * Rg);
-          double Sound = f_ss(th, pl[0], pl[IP], rho, Rg);
-          double dtc = 1e8;
-          if (c.sc.dt_additive) {  // dt-rule = additive (dt_blk.inc:79-155)
-            double ra_c = 0.0, ra_v = 0.0;
-            for (int d = 0; d < c.sc.ndir; ++d) {
-              double m0 = mv(b, d, 0, i, j, k), m1 = mv(b, d, 1, i, j, k), m2 = mv(b, d, 2, i, j, k);
-              double gn = std::sqrt(m0 * m0 + m1 * m1 + m2 * m2);
-              double vel_ = std::fabs(pl[IU] * m0 + pl[IV] * m1 + pl[IW] * m2) / gn;
-              double lambda = vel_ + Sound;
-              ra_c = ra_c + lambda * gn;
-              ra_v = ra_v + gn * gn;
-            }
-            if (c.sc.visc) {
-              if (c.sc.ndir == 3) {
-                double g[3][3];
-                for (int d = 0; d < 3; ++d) for (int a = 0; a < 3; ++a) g[d][a] = mv(b, d, a, i, j, k);
-                auto dot = [&](int p, int q) { return g[p][0] * g[q][0] + g[p][1] * g[q][1] + g[p][2] * g[q][2]; };
-                auto nr = [&](int p) { return std::sqrt(g[p][0] * g[p][0] + g[p][1] * g[p][1] + g[p][2] * g[p][2]); };
-                double c12 = dot(0, 1) / (nr(0) * nr(1)), c13 = dot(0, 2) / (nr(0) * nr(2)), c23 = dot(1, 2) / (nr(1) * nr(2));
-                double ss = c12 * c12 + c13 * c13 + c23 * c23;
-                double qp = c12 * c13 * c23;
-                if (ss + 2.0 * qp > 1.0) {
-                  double mr = 2.0 * std::sqrt(ss / 3.0) *
-                              std::cos(std::acos(std::max(-1.0, std::min(1.0, 3.0 * std::sqrt(3.0) * qp / std::pow(ss, 1.5)))) / 3.0);
-                  ra_v = ra_v * 0.25 * (2.0 + mr + 1.0 / mr);
-                }
-              }
-              double Ta = pl[IP] / (rho * Rg);
-              int ta = tidx(th, Ta);
-              double tda = Ta - ta;
-              double cpa = f_cp(th, pl[0], ta, tda, rho);
-              double cva = cpa - Rg;
-              double mila, kla;
-              wilke(th, pl[0], rho, ta, tda, mila, kla);
-              if (c.sc.prandtl > 0.0) kla = mila * cpa / c.sc.prandtl;
-              const double mie = 0.0, prt = 0.85;
-              double Dmx = std::max(4.0 / 3.0 * (mila + mie) / rho, (kla + mie * cpa / prt) / (rho * cva));
-              dtc = 1.0 / (ra_c / c.sc.cfl + Dmx * ra_v / c.sc.vnn);
-            } else {
-              dtc = c.sc.cfl / ra_c;
-            }
-          } else {
-          for (int d = 0; d < c.sc.ndir; ++d) {
-            double m0 = mv(b, d, 0, i, j, k), m1 = mv(b, d, 1, i, j, k), m2 = mv(b, d, 2, i, j, k);
-            double nrm = std::sqrt(m0 * m0 + m1 * m1 + m2 * m2);
-            double v0 = m0 / nrm, v1 = m1 / nrm, v2 = m2 / nrm;
-            double vel_ = std::fabs(pl[IU] * v0 + pl[IV] * v1 + pl[IW] * v2);
-            double lambda = vel_ + Sound;
-            double dtd = dlv(b, d, i, j, k) / lambda * c.sc.cfl;
-            dtc = std::min(dtd, dtc);
-          }
-          if (c.sc.visc) {
-            int ti = tidx(th, Tc);
-            double td = Tc - ti, mil, kl;
-            wilke(th, pl[0], rho, ti, td, mil, kl);
-            double mi = 0.0 + mil;
-            for (int d = 0; d < c.sc.ndir; ++d) {
-              double dl = dlv(b, d, i, j, k);
-              double dtd = (rho * (dl * dl) * c.sc.vnn) / mi;
-              dtc = std::min(dtd, dtc);
-            }
-          }
-          }
-          dtc = dtc * 1.0;
+          double dtc = cell_dt(c, b, P, i, j, k) * rampa;
+          if (dtl) (*dtl)[row(b, i, j, k)] = dtc;
           dtglobal = std::min(dtc, dtglobal);
         }
   }
@@ -2444,6 +2462,7 @@ int orc_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, orc_
       (sc->intvar == 1 && sc->n_rk == 4) || sc->irs < 0 || sc->irs > 4 || (sc->irs > 0 && sc->n_rk == 4))
     return MB_E_UNSUPPORTED;
   if (sc->irs > 0 && !(sc->irs_beta >= 0.0 && std::isfinite(sc->irs_beta))) return MB_E_ARG;
+  if (sc->local_dt < 0 || sc->local_dt > 1 || sc->cfl_rise < 0) return MB_E_ARG;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
   if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
   orc_ctx* o = new orc_ctx();
@@ -2488,12 +2507,19 @@ int orc_fill_ghosts(orc_ctx* o, double* P) { fill_ghosts(o->c, P); return MB_OK;
 int orc_residual(orc_ctx* o, const double* P, double* R) { residual(o->c, P, R); return MB_OK; }
 int orc_update(orc_ctx* o, double* P, const double* PO, const double* R, int irk, double dt) {
   Ctx& c = o->c;
+  // time-accurate = false: each cell's dtlocal, from the state at the start of the step (PO)
+  std::vector<double> dtl;
+  if (c.sc.local_dt) {
+    dtl.assign((size_t)c.ncell, 0.0);
+    compute_dt(c, PO, &dtl);
+  }
+  const double* dl = c.sc.local_dt ? dtl.data() : nullptr;
   if (c.sc.irs > 0) {  // RK_Newstate with IRS: the smoothing on a copy of R (Newstate_Conservative / _Primitive)
     std::vector<double> Rs(R, R + c.ncell * NP);
-    irs_apply(c, Rs.data(), dt, c.sc.intvar == 0);
-    update(c, P, PO, Rs.data(), irk, dt, c.sc.intvar == 0);
+    irs_apply(c, Rs.data(), dt, c.sc.intvar == 0, dl);
+    update(c, P, PO, Rs.data(), irk, dt, c.sc.intvar == 0, dl);
   } else {
-    update(c, P, PO, R, irk, dt);
+    update(c, P, PO, R, irk, dt, false, dl);
   }
   return c.st.code;
 }
@@ -2505,19 +2531,24 @@ int orc_step(orc_ctx* o, double* P, double* PO, double* R, int nsteps) {
   const int64_t n = c.ncell * NP;
   for (int st = 0; st < nsteps; ++st) {
     if (c.st.done) return MB_OK;  // the residual end test stopped the case (Mod_Explicit.f90:363-370)
-    double dt = compute_dt(c, P);
-    if (c.sc.time_clip) {  // Clip_dt_To_Timemax (Mod_dt.f90:283-296)
-      double rem = c.sc.time_threshold - c.st.time;
-      if (rem > 0.0 && dt > rem) dt = rem * (1.0 + 1e-12);
+    std::vector<double> dtl;
+    if (c.sc.local_dt) dtl.assign((size_t)c.ncell, 0.0);
+    double dt = compute_dt(c, P, c.sc.local_dt ? &dtl : nullptr);
+    const double* dl = c.sc.local_dt ? dtl.data() : nullptr;
+    if (!c.sc.local_dt) {  // time-accurate: Set_Global_dt and the clock (Mod_Explicit.f90:124-128)
+      if (c.sc.time_clip) {  // Clip_dt_To_Timemax (Mod_dt.f90:283-296)
+        double rem = c.sc.time_threshold - c.st.time;
+        if (rem > 0.0 && dt > rem) dt = rem * (1.0 + 1e-12);
+      }
+      c.st.time += dt;
     }
-    c.st.time += dt;
     c.st.dt = dt;
     std::memcpy(PO, P, sizeof(double) * n);
     for (int irk = 1; irk <= c.sc.n_rk; ++irk) {
       fill_ghosts(c, P);
       residual(c, P, R);
-      if (c.sc.irs > 0) irs_apply(c, R, dt, c.sc.intvar == 0);
-      update(c, P, PO, R, irk, dt, c.sc.irs > 0 && c.sc.intvar == 0);
+      if (c.sc.irs > 0) irs_apply(c, R, dt, c.sc.intvar == 0, dl);
+      update(c, P, PO, R, irk, dt, c.sc.irs > 0 && c.sc.intvar == 0, dl);
     }
     // the residual diagnostic of the step (Compute_Residual_blk, Mod_Diagnostic.f90:64-104; the L2 norm of
     // Mod_Explicit.f90:325-358): sqrt of the sum over the interior cells of (new - old)^2 per primitive variable

@@ -128,6 +128,15 @@ def small_cases():
                                                                            n_rk=2), irs=3, irs_beta=0.7)),
         ("duct3d_irs1_hllc_beta03", lambda: with_scheme(cs.duct_3d(), irs=1, irs_beta=0.3)),
         ("sod_prim_irs4_hllc", lambda: with_scheme(cs.riemann_1d(n=64), intvar=abi.INTVAR_PRIM, irs=4)),
+        # local time stepping (time-accurate = false) and the cfl-rise ramp, alone and with the smoothing and the
+        # primitive update
+        ("mb2d_local_dt_ausm_rk3_rise10", lambda: with_scheme(cs.multiblock_2d(cols=2, rows=2, lo=5, hi=9, seed=43,
+                                                                               n_rk=3), local_dt=1, cfl_rise=10)),
+        ("tgv_local_dt_roe_8blk", lambda: with_scheme(cs.taylor_green(n=12, blocks=2, noise=1e-3), local_dt=1)),
+        ("sod_local_dt_irs2_hllc", lambda: with_scheme(cs.riemann_1d(n=64), local_dt=1, irs=2)),
+        ("duct3d_local_dt_prim_rise4", lambda: with_scheme(cs.duct_3d(), local_dt=1, intvar=abi.INTVAR_PRIM,
+                                                           cfl_rise=4)),
+        ("sod_rise5_hllc", lambda: with_scheme(cs.riemann_1d(n=64), cfl_rise=5)),
         # symmetry (300), isothermal walls (302) and the back-pressure outlet (406)
         ("duct3d_hllc_vanleer", lambda: cs.duct_3d()),
         ("duct3d_roe_vanalbada_rk4", lambda: cs.duct_3d(widths=(5, 6), heights=(4, 3), depths=(4,),

@@ -309,3 +309,42 @@ def test_irs_extends_the_stable_cfl_on_sod():
     x = c.blocks[0]["centres"][:, 0, 0, 0]
     r, u, p = cs.exact_riemann((1.0, 0.0, 1.0), (0.125, 0.0, 0.1), x, st.time)
     assert np.abs(c.interior(P, 0)[0, :, 0, 0] - r).mean() < 1e-2
+
+
+def test_local_time_stepping_reaches_the_same_steady_state():
+    """time-accurate = false: every cell advances with its own step, the simulated time stays 0, and a supersonic
+    channel (M 2, Euler, two blocks of different cell counts) converges by the residual stop to the steady state of the
+    time-accurate run, in no more steps."""
+    runs = {}
+    for local in (0, 1):
+        c = cs.multiblock_2d(cols=2, rows=1, widths=[6, 24], heights=[10], seed=41, visc=0, n_rk=3, mach=2.0, amp=0.02)
+        H.with_scheme(c, local_dt=local, res_stop=1e-10)
+        o = oracle.Oracle(c)
+        P = c.P0.copy()
+        for _ in range(30):
+            assert o.step(P, 50) == 0
+            if o.status().done:
+                break
+        st = o.status()
+        assert st.done and st.res[0] <= 1e-10
+        runs[local] = (c, P, st)
+    assert runs[1][2].time == 0.0 and runs[0][2].time > 0.0
+    assert runs[1][2].steps <= runs[0][2].steps
+    c = runs[0][0]
+    assert np.all(H.rel_err(H.conserved(c, runs[1][1]), H.conserved(c, runs[0][1])) < 1e-8)
+
+
+def test_cfl_rise_ramps_the_first_steps():
+    """cfl-rise-threshold = 10: the step of iteration n < 10 is n / 10 of the unramped minimum, from step 10 on the
+    full one (Mod_dt.f90:57-58); the local steps of time-accurate = false are ramped the same way."""
+    c = cs.riemann_1d(n=50)
+    d = cs.riemann_1d(n=50)
+    H.with_scheme(d, cfl_rise=10)
+    oc, od = oracle.Oracle(c), oracle.Oracle(d)
+    P = c.P0.copy()
+    assert abs(od.dt(P) - 0.1 * oc.dt(P)) <= 1e-15 * oc.dt(P)
+    Pd = d.P0.copy()
+    for n in range(1, 13):
+        want = oc.dt(Pd) * (min(n, 10) / 10.0)
+        assert od.step(Pd, 1) == 0
+        assert abs(od.status().dt - want) <= 1e-15 * want, n
