@@ -95,6 +95,7 @@ extern "C" {
 #define MB_RS_EXACT 11
 #define MB_RS_LMROE 12
 #define MB_RS_MICZEKROE 13
+#define MB_RS_HLLC_PC 14 /* with intvar = 2 (prec) only */
 
 /* the sensor id in effect (sd_dev): 0 none, 1 Tramel, 2 Chen */
 static inline int mb_effective_sensor(int riemann, int sensor) {
@@ -196,7 +197,9 @@ typedef struct mb_scheme {
   int32_t intvar;     /* integration-variables (Assign_Integration_Variables, Lib_Newstate.f90:43-60): 0 cons
                          (Newstate_Conservative), 1 prim (Newstate_Primitive: the residual taken to the primitive
                          variables through the inverse of the prim -> cons Jacobian, Lib_Newstate.f90:348-531; with
-                         n_rk <= 3) */
+                         n_rk <= 3), 2 prec (the primitive update with the Weiss-Smith low-Mach preconditioning of
+                         Lib_Preconditioning.f90: the reference velocity Ur of every cell sets Theta, the local step
+                         with the pseudo-acoustic speed and the HLLC-PC solver 14; steady runs only: local_dt = 1) */
   int32_t irs;        /* implicit residual smoothing (IRS = t of [MOSE-scheme], Lib_IRS.f90:57-105): the number of Jacobi
                          sweeps of R* = R + beta d2(R*) along each direction (the reference runs 2); 0 = off, at most
                          4, with n_rk <= 3. Conservative variables: the residual is scaled to -dt R / vol first and
@@ -218,6 +221,14 @@ typedef struct mb_scheme {
   int32_t cfl_rise;   /* [MOSE-parameters] cfl-rise-threshold (rampa_iter, Mod_dt.f90:57-58): the local steps are scaled
                          by iter / cfl_rise while the step count iter (1 for the first step of mb_init or
                          mb_group_reset) is below it; 0 = no ramp */
+  int32_t prec_smooth;    /* integration-variables = prec (intvar 2): preconditioning-Ur-smooth, passes of max over the
+                             six face neighbours (Lib_Preconditioning.f90:269-295) */
+  int32_t pad2;
+  double prec_eps_min;    /* preconditioning-eps-min, in (0, 1) (default 0.05) */
+  double prec_uref;       /* preconditioning-Uref (> 0: mode 1, a uniform reference velocity) */
+  double prec_mach;       /* preconditioning-Mach (> 0: mode 2, the target preconditioned Mach number) */
+  double prec_ur_factor;  /* preconditioning-Ur-factor (mode 3, Weiss-Smith; default 1) */
+  double prec_ur_min;     /* preconditioning-Ur-min (> 0: a floor of Ur) */
 } mb_scheme;
 
 typedef struct mb_status {

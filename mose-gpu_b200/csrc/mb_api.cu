@@ -59,6 +59,9 @@ struct mb_ctx {
   long long* d_idst = nullptr;  // its first-ghost-layer copies, direction by direction: row idst[e] <- row isrc[e]
   long long* d_isrc = nullptr;
   int irs_off[4] = {0, 0, 0, 0};
+  double* d_ur = nullptr;       // prec: Ur of every row (ghost rows 0), its smoothing buffer, the step's local steps
+  double* d_urb = nullptr;
+  double* d_dtl = nullptr;
   struct Geo32 { const double* src; float* buf; long long n; };
   std::vector<Geo32> geo32;     // FP32 geometry copies of the mixed form (source array, copy, elements)
   int ngroups = 1;              // case clocks
@@ -97,7 +100,7 @@ static void free_ctx(mb_ctx* c) {
   if (c->graph) cudaGraphDestroy(c->graph);
   void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
                   c->d_pgsrc, c->d_tab, c->d_tabf, c->d_st, c->d_tiles_sweep, c->d_tiles_aux, c->d_scratch, c->d_acc4, c->d_queue, c->d_recflux, c->d_brec, c->d_bcell,
-                  c->d_physf, c->d_cubicf, c->d_tiles_km, c->d_irs, c->d_idst, c->d_isrc};
+                  c->d_physf, c->d_cubicf, c->d_tiles_km, c->d_irs, c->d_idst, c->d_isrc, c->d_ur, c->d_urb, c->d_dtl};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& q : c->geo32)
@@ -239,7 +242,8 @@ static void free_tables(mb_ctx* c) {
 // the sweep unit of a scheme: the benchmarked solvers' own (the solver a compile-time constant) unless a shock sensor,
 // the primitive update or local time stepping is on, which only the run-time solver unit carries
 static int sweep_unit(const mb_scheme* sc) {
-  return (mb_effective_sensor(sc->riemann, sc->sensor) || sc->intvar || sc->local_dt) ? 0 : sc->riemann;
+  return (mb_effective_sensor(sc->riemann, sc->sensor) || sc->intvar || sc->local_dt || sc->riemann > 13) ? 0
+                                                                                                          : sc->riemann;
 }
 
 // record types with physical ghosts (Fill_Ghost_Cell_blk, Lib_Extrapolation.f90:643-730)
@@ -574,9 +578,14 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
 int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int device, mb_ctx** out) {
   if (!mesh || !sc || !th || !out) return MB_E_ARG;
   *out = nullptr;
-  if (sc->riemann < MB_RS_HLLC || sc->riemann > MB_RS_MICZEKROE) return MB_E_UNSUPPORTED;  // 14 (HLLC-PC) needs prec
+  if (sc->riemann < MB_RS_HLLC || sc->riemann > MB_RS_HLLC_PC) return MB_E_UNSUPPORTED;
   if (sc->sensor < 0 || sc->sensor > 3) return MB_E_UNSUPPORTED;
-  if (sc->intvar < 0 || sc->intvar > 1 || (sc->intvar == 1 && sc->n_rk == 4)) return MB_E_UNSUPPORTED;
+  if (sc->intvar < 0 || sc->intvar > 2 || (sc->intvar >= 1 && sc->n_rk == 4)) return MB_E_UNSUPPORTED;
+  // HLLC-PC only with preconditioning (Assign_RS, Lib_Riemann.f90:88-89), preconditioning only for steady runs
+  // (IO_Ini_Open.f90:125-127)
+  if ((sc->riemann == MB_RS_HLLC_PC) != (sc->intvar == 2) || (sc->intvar == 2 && sc->local_dt != 1))
+    return MB_E_UNSUPPORTED;
+  if (sc->intvar == 2 && !(sc->prec_eps_min > 0.0 && sc->prec_eps_min < 1.0 && sc->prec_smooth >= 0)) return MB_E_ARG;
   if (sc->irs < 0 || sc->irs > 4 || (sc->irs > 0 && sc->n_rk == 4)) return MB_E_UNSUPPORTED;
   if (sc->irs > 0 && !(sc->irs_beta >= 0.0 && std::isfinite(sc->irs_beta))) return MB_E_ARG;
   if (sc->local_dt < 0 || sc->local_dt > 1 || sc->cfl_rise < 0) return MB_E_ARG;
@@ -641,6 +650,14 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
     return MB_E_NOMEM;
   }
   if (cudaMemset(c->d_scratch, 0, (size_t)c->ncell * MB_NPRIM * sizeof(double)) != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+  if (sc->intvar == 2) {
+    const size_t nb = (size_t)c->ncell * sizeof(double);
+    double** bufs[3] = {&c->d_ur, &c->d_urb, &c->d_dtl};
+    for (double** q : bufs) {
+      if (cudaMalloc((void**)q, nb) != cudaSuccess) { free_ctx(c); return MB_E_NOMEM; }
+      if (cudaMemset(*q, 0, nb) != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
+    }
+  }
   if (sc->irs > 0) {
     const size_t nb = 2 * (size_t)c->ncell * MB_NPRIM * sizeof(double);
     if (cudaMalloc((void**)&c->d_irs, nb) != cudaSuccess) { free_ctx(c); return MB_E_NOMEM; }
@@ -672,6 +689,11 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   p.intvar = sc->intvar;
   p.local_dt = sc->local_dt;
   p.cfl_rise = sc->cfl_rise;
+  p.prec = sc->intvar == 2 ? 1 : 0;
+  p.ur = c->d_ur;
+  p.dtl = c->d_dtl;
+  p.prec_eps_min = sc->prec_eps_min; p.prec_uref = sc->prec_uref; p.prec_mach = sc->prec_mach;
+  p.prec_ur_factor = sc->prec_ur_factor; p.prec_ur_min = sc->prec_ur_min;
   p.lim = sc->limiter; p.rs = sc->riemann; p.visc = sc->visc ? 1 : 0; p.ndir = sc->ndir; p.dt_additive = sc->dt_additive;
   p.guard = sc->visc ? 1 : 0; p.state_check = sc->state_check;
   p.cfl = sc->cfl; p.vnn = sc->vnn; p.prandtl = sc->prandtl; p.schmidt = sc->schmidt; p.mco = sc->mco;
@@ -880,6 +902,17 @@ static int smooth_residual(mb_ctx* c, double* R, double dt, const double* Pold, 
   return MB_OK;
 }
 
+// prec: Ur of the state P (Update_Derived_Variables). Every entry point that reads Ur computes it from the state it is
+// given, and the time loop from each stage's input: the reference refreshes it after every update, so it is always the
+// Ur of the current state
+static int ur_pass(mb_ctx* c, const double* P, cudaStream_t s) {
+  if (!c->p.prec) return MB_OK;
+  int nl = 0;
+  CK(prec_ur(c->p, c->d_tiles_aux, c->ntiles_aux, P, c->d_ur, c->d_urb, c->sc.prec_smooth, s, &nl));
+  c->launches += nl;
+  return MB_OK;
+}
+
 int mb_fill_ghosts(mb_ctx* ctx, double* P, void* stream) {
   if (!ctx || !P) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
@@ -889,7 +922,9 @@ int mb_fill_ghosts(mb_ctx* ctx, double* P, void* stream) {
 int mb_residual(mb_ctx* ctx, const double* P, double* R, void* stream) {
   if (!ctx || !P || !R) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
-  int rc = records(ctx, P, (cudaStream_t)stream);
+  int rc = ur_pass(ctx, P, (cudaStream_t)stream);
+  if (rc != MB_OK) return rc;
+  rc = records(ctx, P, (cudaStream_t)stream);
   if (rc != MB_OK) return rc;
   return sweep(ctx, MODE_RESIDUAL, P, nullptr, nullptr, R, 0, 0, (cudaStream_t)stream);
 }
@@ -901,6 +936,12 @@ int mb_update(mb_ctx* ctx, double* P, const double* PO, const double* R, int irk
   p.irk = irk;
   cudaStream_t s = (cudaStream_t)stream;
   int prescaled = 0;
+  if (p.prec) {  // Ur of the stage input, then each cell's local step from PO (not reduced into the clock)
+    int rc = ur_pass(ctx, P, s);
+    if (rc != MB_OK) return rc;
+    CK(prec_dt(p, ctx->d_tiles_aux, ctx->ntiles_aux, PO, ctx->d_dtl, 0, s));
+    ctx->launches += 1;
+  }
   if (ctx->sc.irs > 0) {  // IRS_apply on the engine's copy of R, then the update takes the smoothed residual
     double* R0 = ctx->d_irs;
     CK(cudaMemcpyAsync(R0, R, (size_t)ctx->ncell * MB_NPRIM * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -916,6 +957,14 @@ int mb_update(mb_ctx* ctx, double* P, const double* PO, const double* R, int irk
 }
 
 static int dt_min(mb_ctx* c, const double* P, cudaStream_t s) {
+  if (c->p.prec) {  // Ur of P, then the preconditioned local steps of the step into dtl and their minimum
+    int rc = ur_pass(c, P, s);
+    if (rc != MB_OK) return rc;
+    CK(reset_dt(c->p, s));
+    CK(prec_dt(c->p, c->d_tiles_aux, c->ntiles_aux, P, c->d_dtl, 1, s));
+    c->launches += 2;
+    return MB_OK;
+  }
   CK(reset_dt(c->p, s));
   CK(c->sc.precision == MB_PREC_MIXED ? sweep_f32_rs1_dt(c->p, c->d_tiles_aux, c->ntiles_aux, P, -1, s)
                                        : dt_cells(c->p, c->d_tiles_aux, c->ntiles_aux, P, s));
@@ -977,7 +1026,9 @@ static int stage(mb_ctx* c, double* P, double* PO, int irk, cudaStream_t s) {
   const double* in;
   double* outp;
   stage_buffers(n, irk, P, PO, S, &in, &outp);
-  int rc = fill(c, const_cast<double*>(in), s);
+  int rc = ur_pass(c, in, s);  // prec: Ur of the stage input
+  if (rc != MB_OK) return rc;
+  rc = fill(c, const_cast<double*>(in), s);
   if (rc != MB_OK) return rc;
   rc = records(c, in, s);
   if (rc != MB_OK) return rc;
@@ -997,6 +1048,10 @@ int mb_stage(mb_ctx* ctx, double* P, double* PO, int irk, void* stream) {
 }
 
 static int one_step(mb_ctx* c, double* P, double* PO, cudaStream_t s) {
+  if (c->p.prec) {  // the preconditioned local steps need the Ur of the step's state: their own pass, not the fused one
+    int rc = dt_min(c, P, s);
+    if (rc != MB_OK) return rc;
+  }
   CK(clock_step(c->p, s));
   c->launches += 1;
   for (int irk = 1; irk <= c->sc.n_rk; ++irk) {

@@ -83,7 +83,12 @@ MB_HD void face_flux(const Params& p, const DBlk& b, const Tile<R, TY>& T, int d
                      T.base[T.off(sk, jj - 1, ii) + VP], T.base[T.off(sk, jj + 1, ii) + VP],
                      T.base[T.off(skm, jj, ii) + VP], T.base[T.off(sk1, jj, ii) + VP]);
   }
-  conv_face<R, RS, LIM>(p, pm1, p0, pp1, pp2, dlc, nx, ny, nz, area, out, bet);
+  R urL = (R)0, urR = (R)0;
+  if (RS == 0 && p.prec) {  // HLLC-PC: the Ur of the face's two cells (conv_physics.inc:159-163)
+    urL = (R)ld(p.ur + b.boff + l0);
+    urR = (R)ld(p.ur + b.boff + l0 + st);
+  }
+  conv_face<R, RS, LIM>(p, pm1, p0, pp1, pp2, dlc, nx, ny, nz, area, out, bet, urL, urR);
   if (!VISC) return;
   // ---- viscous face: cells 1,2 = (c, c+d); 3,4 = c -/+ b-axis; 5,6 = c+d -/+ b; 7,8 = c -/+ c-axis; 9,10 = c+d -/+ c
   int oc[10];
@@ -212,8 +217,10 @@ MB_HD void bc_conn_eul(const Params& p, const DBlk& b, const double* __restrict_
   rotot_rtot(p, PR[0], rhoR, RRr);
   R aR = f_ss(p, PR[0], PR[MB_IPR], rhoR, RRr);
   R F_r, F_u, F_v, F_w, F_E;
+  // HLLC-PC: the Ur of cells 2 and 3, the ghost's 0 (never filled, Lib_BC.f90:1739-1742)
+  const R urL = (RS == 0 && p.prec) ? (R)ld(p.ur + rr[1]) : (R)0, urR = (RS == 0 && p.prec) ? (R)ld(p.ur + rr[2]) : (R)0;
   riemann_rec<R, RS>(p, PL[0], PL[MB_IU], PL[MB_IV], PL[MB_IW], PL[MB_IPR], aL, rhoL, RL, PR[0], PR[MB_IU], PR[MB_IV],
-                     PR[MB_IW], PR[MB_IPR], aR, rhoR, RRr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E, beta_);
+                     PR[MB_IW], PR[MB_IPR], aR, rhoR, RRr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E, beta_, urL, urR);
   R su = copysign((R)0.5, F_r), selL = (R)0.5 + su, selR = su - (R)0.5;
   R Fmass = F_r * area;
   R sg = (R)modfm2;
@@ -372,8 +379,9 @@ MB_HD void bc_sym_eul(const Params& p, const DBlk& b, const double* __restrict__
 #pragma unroll
   for (int a = 0; a < 3; ++a) { U1[a] = Un1 * nrm[a] + Vt[a]; U4[a] = -Un1 * nrm[a] + Vt[a]; }
   R F_r, F_u, F_v, F_w, F_E;
+  const R urc = (RS == 0 && p.prec) ? (R)ld(p.ur + rb) : (R)0;  // HLLC-PC: the cell's Ur on both sides (:720-723)
   riemann_rec<R, RS>(p, F[0], U1[0], U1[1], U1[2], F[MB_IPR], Sound, rotot, Rtot, F[0], U4[0], U4[1], U4[2],
-                     F[MB_IPR], Sound, rotot, Rtot, nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E);
+                     F[MB_IPR], Sound, rotot, Rtot, nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E, (R)1, urc, urc);
   A[0] = (R)-0.0;  // an exact no-op when added: only the momentum rows change
   A[MB_IU] = (R)modfm2 * F_u * area;
   A[MB_IV] = (R)modfm2 * F_v * area;
@@ -816,8 +824,9 @@ MB_HD void bc_inflow(const Params& p, const DBlk& b, const double* __restrict__ 
   rotot_rtot(p, PR[0], rR, RRr);
   R aR = f_ss(p, PR[0], PR[MB_IPR], rR, RRr);
   R F_r, F_u, F_v, F_w, F_E;
+  // Ur = a on both sides: no preconditioning at the inlet (Lib_BC.f90:1308-1310)
   riemann_rec<R, RS>(p, PL[0], PL[MB_IU], PL[MB_IV], PL[MB_IW], PL[MB_IPR], aL, rL, RL, PR[0], PR[MB_IU], PR[MB_IV],
-                     PR[MB_IW], PR[MB_IPR], aR, rR, RRr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
+                     PR[MB_IW], PR[MB_IPR], aR, rR, RRr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E, (R)1, aL, aR);
   R su = copysign((R)1, F_r);
   R selL = ((R)1 + su) / (R)2, selR = (su - (R)1) / (R)2;
   R Fmass = F_r * area;
@@ -1022,7 +1031,7 @@ MB_HD void cons_update(const Params& p, const double* pc, const double* po, cons
 // to the primitive variables by the inverse of the prim -> cons Jacobian (Theta = rho_p), then the RK stage on the
 // primitive state, rho floored at 1e-20
 MB_HD void prim_update(const Params& p, const double* pc, const double* po, const double* res, double vol, double dt,
-                       double rkc, double* pn) {
+                       double rkc, double* pn, double urc = 0.0) {
   const double strang = 1.0;
   double rho, Rgas;
   rotot_rtot(p, pc[0], rho, Rgas);
@@ -1037,7 +1046,14 @@ MB_HD void prim_update(const Params& p, const double* pc, const double* po, cons
   const double rho_T = -rho / temperature;
   const double rho_p = 1.0 / (Rgas * temperature);
   const double enthalpy = H0(p, pc[MB_IPR], pc[0], modvel);
-  const double Theta = rho_p;
+  double Theta = rho_p;
+  if (p.prec) {  // Weiss-Smith: Theta from the cell's Ur (Lib_Newstate.f90:399-402)
+    const double gam = cp / (cp - Rgas);
+    const double sound = sqrt(gam * Rgas * temperature);
+    const double a2 = sound * sound;
+    const double beta2 = mx(urc * urc / a2, 1.0e-6);
+    Theta = 1.0 / (beta2 * a2) + 1.0 / (cp * temperature);
+  }
   const double Denom = 1.0 / (rho * cp * Theta + rho_T);
   double G[5][5];
   G[0][0] = (rho_T * (enthalpy - q2) + rho * cp) * Denom;
@@ -1144,9 +1160,11 @@ MB_HD void cons_update_fast(const Params& p, const double* pc, const double* po,
 }
 
 // local dt of one cell (dt_blk.inc: min rule :156-191, additive rule :79-155) in the arithmetic type R: FP64 for the
-// parity form and the standalone Compute_dt, FP32 (geometry and tables in FP32) for the fused dt of the mixed form
-template <typename R>
-MB_HD R cell_dt_t(const Params& p, const DBlk& b, long long l, const R* pl) {
+// parity form and the standalone Compute_dt, FP32 (geometry and tables in FP32) for the fused dt of the mixed form.
+// PREC: integration-variables = prec, the pseudo-acoustic speed c* = sqrt(alpha^2 u^2 + Ur^2) of the preconditioned
+// system with the cell's Ur (urc) in place of the sound speed (dt_blk.inc:72-75, 89-92, 138-142)
+template <typename R, bool PREC = false>
+MB_HD R cell_dt_t(const Params& p, const DBlk& b, long long l, const R* pl, R urc = (R)0) {
   R rho, Rg;
   rotot_rtot(p, pl[0], rho, Rg);
   R Tc = pl[MB_IPR] / (rho * Rg);
@@ -1154,6 +1172,11 @@ MB_HD R cell_dt_t(const Params& p, const DBlk& b, long long l, const R* pl) {
   const auto* m = Geo<R>::m(b) + 9 * l;
   const auto* dl = Geo<R>::dl(b) + 3 * l;
   R dtc = (R)1e8;
+  R Alpha_ = (R)0;
+  if (PREC) {
+    const R Beta_ = (R)1 / (Sound * Sound);
+    Alpha_ = (R)0.5 * ((R)1 - Beta_ * (urc * urc));
+  }
   if (p.dt_additive) {
     R ra_c = (R)0, ra_v = (R)0;
     for (int d = 0; d < b.ndir; ++d) {
@@ -1161,6 +1184,7 @@ MB_HD R cell_dt_t(const Params& p, const DBlk& b, long long l, const R* pl) {
       R gn = rsqrt_(m0 * m0 + m1 * m1 + m2 * m2);
       R vel_ = fabs(pl[MB_IU] * m0 + pl[MB_IV] * m1 + pl[MB_IW] * m2) / gn;
       R lambda = vel_ + Sound;
+      if (PREC) lambda = vel_ * ((R)1 - Alpha_) + rsqrt_(Alpha_ * Alpha_ * (vel_ * vel_) + urc * urc);
       ra_c = ra_c + lambda * gn;
       ra_v = ra_v + gn * gn;
     }
@@ -1200,6 +1224,11 @@ MB_HD R cell_dt_t(const Params& p, const DBlk& b, long long l, const R* pl) {
       R v0 = m0 / nrm, v1 = m1 / nrm, v2 = m2 / nrm;
       R vel_ = fabs(pl[MB_IU] * v0 + pl[MB_IV] * v1 + pl[MB_IW] * v2);
       R lambda = vel_ + Sound;
+      if (PREC) {
+        const R cst_ = rsqrt_(Alpha_ * Alpha_ * (vel_ * vel_) + urc * urc);
+        vel_ = vel_ * ((R)1 - Alpha_);
+        lambda = vel_ + cst_;
+      }
       R dtd = cvt<R>(ld(dl + d)) / lambda * (R)p.cfl;
       dtc = mn(dtd, dtc);
     }
@@ -1226,6 +1255,7 @@ MB_HD double cell_dt(const Params& p, const DBlk& b, long long l, const double* 
 // dtc * rampa_fac)
 __device__ __forceinline__ double step_dt(const Params& p, const DBlk& b, const DevState* st, long long l,
                                           const double* po, double dt) {
+  if (p.prec) return p.dtl[b.boff + l] * st->rampf;  // prec: the steps of the start of the step, with its Ur
   return p.local_dt ? cell_dt(p, b, l, po) * st->rampf : dt;
 }
 
@@ -1457,13 +1487,15 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
         }
         const double vol = ld(b.vol + (r - b.boff));
         double dtc = dt;
-        if (RS == 0 && p.local_dt) {  // the cell's own step in the flux type (FP64 in the parity form)
+        if (RS == 0 && p.prec) {
+          dtc = ld(p.dtl + r) * st->rampf;  // the steps of the start of the step (Ur of that state)
+        } else if (RS == 0 && p.local_dt) {  // the cell's own step in the flux type (FP64 in the parity form)
           R pr[MB_NP];
 #pragma unroll
           for (int s = 0; s < MB_NP; ++s) pr[s] = cvt<R>(po[s]);
           dtc = (double)cell_dt_t<R>(p, b, r - b.boff, pr) * st->rampf;
         }
-        if (RS == 0 && p.intvar) prim_update(p, pc, po, acc, vol, dtc, rkc, pn);
+        if (RS == 0 && p.intvar) prim_update(p, pc, po, acc, vol, dtc, rkc, pn, p.prec ? ld(p.ur + r) : 0.0);
         else if (Fast<R>::on) cons_update_fast(p, pc, po, acc, vol, dtc, rkc, Tc, pn, r);
         else cons_update(p, pc, po, acc, vol, dtc, rkc, Tc, pn, r);
         bool bad = !(pn[MB_IPR] >= 0.0);

@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(32 * TY_AUX) k_update(Params p, const DTile* _
       T = mn(mx(T, 1.0), 9990.0);
     }
     const double dtc = step_dt(p, b, st, r - b.boff, po, dt);
-    if (p.intvar) prim_update(p, pc, po, res, ld(b.vol + (r - b.boff)), dtc, rkc, pn);
+    if (p.intvar) prim_update(p, pc, po, res, ld(b.vol + (r - b.boff)), dtc, rkc, pn, p.prec ? p.ur[r] : 0.0);
     else cons_update(p, pc, po, res, ld(b.vol + (r - b.boff)), dtc, rkc, T, pn, r, prescaled != 0);
     bool bad = !(pn[MB_IPR] >= 0.0);
     for (int s = 0; s < MB_NP; ++s) bad = bad || !isfinite(pn[s]);

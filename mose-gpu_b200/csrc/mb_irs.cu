@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(32 * TY_AUX) k_irs_stage_update(Params p, cons
       }
       const double vol = ld(b.vol + (r - b.boff));
       const double dtc = step_dt(p, b, st, r - b.boff, po, dt);
-      if (p.intvar) prim_update(p, pc, po, res, vol, dtc, rkc, pn);
+      if (p.intvar) prim_update(p, pc, po, res, vol, dtc, rkc, pn, p.prec ? p.ur[r] : 0.0);
       else cons_update(p, pc, po, res, vol, dtc, rkc, T, pn, r, true);
       bool bad = !(pn[MB_IPR] >= 0.0);
 #pragma unroll

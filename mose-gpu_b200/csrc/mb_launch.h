@@ -71,6 +71,12 @@ cudaError_t dt_cells(const Params& p, const DTile* tiles, int ntiles, const doub
 cudaError_t update_cells(const Params& p, const DTile* tiles, int ntiles, double* P, const double* PO,
                          const double* R, double rkc, double dt, cudaStream_t s, int prescaled = 0);
 cudaError_t reset_dt(const Params& p, cudaStream_t s, int only_group = -1);
+// integration-variables = prec (mb_prec.cu): Ur of the interior cells of P with nsmooth smoothing passes (urb: the
+// second buffer; *nl: kernels launched), and the local steps of P into dtl (reduce: their minimum into the clocks)
+cudaError_t prec_ur(const Params& p, const DTile* tiles, int ntiles, const double* P, double* ur, double* urb,
+                    int nsmooth, cudaStream_t s, int* nl);
+cudaError_t prec_dt(const Params& p, const DTile* tiles, int ntiles, const double* P, double* dtl, int reduce,
+                    cudaStream_t s);
 // implicit residual smoothing (mb_irs.cu)
 cudaError_t irs_scale(const Params& p, const DTile* tiles, int ntiles, double* R, double dt, const double* Pold,
                       cudaStream_t s);

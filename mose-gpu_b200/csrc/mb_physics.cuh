@@ -106,6 +106,11 @@ struct Params {
   int sd;                  // the shock sensor in effect (sd_dev): 0 none, 1 Tramel, 2 Chen
   int intvar;              // integration variables: 0 conservative, 1 primitive
   int local_dt;            // time-accurate = false: each cell's own step (from the state at the start of the step)
+  int prec;                // integration-variables = prec: Ur of every row in ur (ghost rows 0), the local steps of
+                           // the step in dtl (rows; fixed at the start of the step), HLLC-PC (14) reads ur
+  const double* ur;
+  const double* dtl;
+  double prec_eps_min, prec_uref, prec_mach, prec_ur_factor, prec_ur_min;  // the preconditioning keys (comp_Ur)
   int cfl_rise;            // cfl-rise-threshold (0: no ramp)
   int lim, rs, visc, ndir, dt_additive, guard, state_check;
   double cfl, vnn, prandtl, schmidt, mco;
@@ -350,9 +355,60 @@ MB_HD R gam_state(const Params& p, R d, R pr, R dtot) {
 template <typename R>
 MB_HD void riemann_open(const Params& p, int rs, R bet, R dl, R ul, R vl, R wl, R pl, R al, R dltot,
                                              R dr, R ur, R vr, R wr, R pr, R ar, R drtot, R nx, R ny, R nz,
-                                             R& F_r, R& F_u, R& F_v, R& F_w, R& F_E) {
+                                             R& F_r, R& F_u, R& F_v, R& F_w, R& F_E, R urL = (R)0, R urR = (R)0) {
   R unl = ul * nx + vl * ny + wl * nz;
   R unr = ur * nx + vr * ny + wr * nz;
+  if (rs == 14) {  // HLLC-PC (riemann_open_body.inc:1092-1175, Riemann_HLLCprec): HLLC Batten with the signal speeds of
+                   // the preconditioned system, Vr = min(Ur, a) of each side (urL, urR) and of the sqrt(rho) average
+    const R hL = h_static(p, dl, pl), hR = h_static(p, dr, pr);
+    const R eL = hL - pl / dltot, eR = hR - pr / drtot;
+    const R kL = (R)0.5 * (ul * ul + vl * vl + wl * wl), kR = (R)0.5 * (ur * ur + vr * vr + wr * wr);
+    const R h0l = hL + kL, h0r = hR + kR, EtL = eL + kL, EtR = eR + kR;
+    const R FrL = dltot * unl;
+    const R Ful = FrL * ul + pl * nx, Fvl = FrL * vl + pl * ny, Fwl = FrL * wl + pl * nz, Fel = FrL * h0l;
+    const R FrR = drtot * unr;
+    const R Fur = FrR * ur + pr * nx, Fvr = FrR * vr + pr * ny, Fwr = FrR * wr + pr * nz, Fer = FrR * h0r;
+    const R srL = rsqrt_(dltot), srR = rsqrt_(drtot), den = srL + srR;
+    const R u_roe = (srL * ul + srR * ur) / den, v_roe = (srL * vl + srR * vr) / den;
+    const R w_roe = (srL * wl + srR * wr) / den, a_roe = (srL * al + srR * ar) / den;
+    const R un_roe = u_roe * nx + v_roe * ny + w_roe * nz;
+    const R VrL = mn(urL, al), VrR = mn(urR, ar), VrRoe = (srL * VrL + srR * VrR) / den;
+    const R alL = ((R)1 - (VrL * VrL) / (al * al)) / (R)2, alR = ((R)1 - (VrR * VrR) / (ar * ar)) / (R)2;
+    const R alRoe = ((R)1 - (VrRoe * VrRoe) / (a_roe * a_roe)) / (R)2;
+    const R vLs = unl * ((R)1 - alL), vRs = unr * ((R)1 - alR), vRoes = un_roe * ((R)1 - alRoe);
+    const R cLs = rsqrt_(mx(alL * alL * (unl * unl) + VrL * VrL, (R)0));
+    const R cRs = rsqrt_(mx(alR * alR * (unr * unr) + VrR * VrR, (R)0));
+    const R cRoes = rsqrt_(mx(alRoe * alRoe * (un_roe * un_roe) + VrRoe * VrRoe, (R)0));
+    const R S1 = mn(mn((R)0, vLs - cLs), vRoes - cRoes);
+    const R S4 = mx(mx((R)0, vRs + cRs), vRoes + cRoes);
+    const R Sstar = (pr - pl + dltot * unl * (S1 - unl) - drtot * unr * (S4 - unr)) /
+                    (dltot * (S1 - unl) - drtot * (S4 - unr));
+    const R pstar = dltot * (unl - S1) * (unl - Sstar) + pl;
+    if (S1 >= (R)0) {
+      F_r = FrL; F_u = Ful; F_v = Fvl; F_w = Fwl; F_E = Fel;
+    } else if (S4 <= (R)0) {
+      F_r = FrR; F_u = Fur; F_v = Fvr; F_w = Fwr; F_E = Fer;
+    } else if (Sstar >= (R)0) {
+      const R q = S1 - Sstar;
+      const R U1S = dltot * (S1 - unl) / q;
+      const R U2S = ((S1 - unl) * dltot * ul + (pstar - pl) * nx) / q;
+      const R U3S = ((S1 - unl) * dltot * vl + (pstar - pl) * ny) / q;
+      const R U4S = ((S1 - unl) * dltot * wl + (pstar - pl) * nz) / q;
+      const R U5S = ((S1 - unl) * dltot * EtL - pl * unl + pstar * Sstar) / q;
+      F_r = FrL + S1 * (U1S - dltot); F_u = Ful + S1 * (U2S - dltot * ul); F_v = Fvl + S1 * (U3S - dltot * vl);
+      F_w = Fwl + S1 * (U4S - dltot * wl); F_E = Fel + S1 * (U5S - dltot * EtL);
+    } else {
+      const R q = S4 - Sstar;
+      const R U1S = drtot * (S4 - unr) / q;
+      const R U2S = ((S4 - unr) * drtot * ur + (pstar - pr) * nx) / q;
+      const R U3S = ((S4 - unr) * drtot * vr + (pstar - pr) * ny) / q;
+      const R U4S = ((S4 - unr) * drtot * wr + (pstar - pr) * nz) / q;
+      const R U5S = ((S4 - unr) * drtot * EtR - pr * unr + pstar * Sstar) / q;
+      F_r = FrR + S4 * (U1S - drtot); F_u = Fur + S4 * (U2S - drtot * ur); F_v = Fvr + S4 * (U3S - drtot * vr);
+      F_w = Fwr + S4 * (U4S - drtot * wr); F_E = Fer + S4 * (U5S - drtot * EtR);
+    }
+    return;
+  }
   if (rs == 4) {
     const R ab = (R)0.125, aa = (R)0.1875;
     R vel = rsqrt_(ul * ul + vl * vl + wl * wl);
@@ -1190,7 +1246,8 @@ MB_HD R sd_beta(int id, R pc, R p1, R p2, R p3, R p4, R p5, R p6) {
 // RS / LIM: the Riemann solver and limiter ids fixed at compile time (0: read p.rs / p.lim at run time)
 template <typename R, int RS = 0, int LIM = 0>
 MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, const R* pp2,
-                                          const R* dlc, R nx, R ny, R nz, R area, R* res0, R bet = (R)1) {
+                                          const R* dlc, R nx, R ny, R nz, R area, R* res0, R bet = (R)1,
+                                          R urL = (R)0, R urR = (R)0) {
   const int rs = RS ? RS : p.rs;
   const int lim = LIM ? LIM : p.lim;
   R l0 = (R)0.5 * (dlc[0] + dlc[1]), l1 = (R)0.5 * (dlc[1] + dlc[2]), l2 = (R)0.5 * (dlc[2] + dlc[3]);
@@ -1242,7 +1299,7 @@ MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, c
   }
   else
     riemann_open(p, rs, bet, P1[0], P1[MB_IU], P1[MB_IV], P1[MB_IW], P1[MB_IPR], a1, rotot1, P4[0], P4[MB_IU],
-                 P4[MB_IV], P4[MB_IW], P4[MB_IPR], a4, rotot4, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
+                 P4[MB_IV], P4[MB_IW], P4[MB_IPR], a4, rotot4, nx, ny, nz, F_r, F_u, F_v, F_w, F_E, urL, urR);
   if (Fast<R>::on) {
     res0[0] = F_r * area;  // one species: the upwinded mass fraction is 1
   } else {
@@ -1258,7 +1315,7 @@ MB_HD void conv_face(const Params& p, const R* pm1, const R* p0, const R* pp1, c
 template <typename R, int RS = 0>
 MB_HD void riemann_rec(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dltot, R Rl, R dr, R ur, R vr, R wr,
                        R pr, R ar, R drtot, R Rr, R nx, R ny, R nz, R& F_r, R& F_u, R& F_v, R& F_w, R& F_E,
-                       R bet = (R)1) {
+                       R bet = (R)1, R urL = (R)0, R urR = (R)0) {
   const int rs = RS ? RS : p.rs;
   if (rs == 1 || rs == 2)
     hllc(p, dl, ul, vl, wl, pl, al, dltot, Rl, dr, ur, vr, wr, pr, ar, drtot, Rr, nx, ny, nz, F_r, F_u, F_v, F_w, F_E,
@@ -1267,7 +1324,7 @@ MB_HD void riemann_rec(const Params& p, R dl, R ul, R vl, R wl, R pl, R al, R dl
     slau_rec(p, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r, F_u, F_v, F_w, F_E);
   else
     riemann_open(p, rs, bet, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r, F_u, F_v, F_w,
-                 F_E);
+                 F_E, urL, urR);
 }
 
 // face thermo (Diffusive_Face_Thermo_Fill, Mod_Diffusive.f90:311-325 = Diffusive_Face_State :748-776)

@@ -41,10 +41,10 @@ BC_OUTLET = 24      # q = (exit pressure, relaxation factor)
 
 LIM_MINMOD, LIM_VANLEER, LIM_VANALBADA, LIM_MC, LIM_SUPERBEE, LIM_FIRST = 1, 2, 3, 4, 5, 6
 RS_HLLC, RS_HLLE, RS_SLAU, RS_AUSMP, RS_LLF, RS_SLAU2, RS_LMROE = 1, 2, 3, 4, 8, 9, 12
-RS_EXACT, RS_MICZEKROE = 11, 13
+RS_EXACT, RS_MICZEKROE, RS_HLLC_PC = 11, 13, 14
 RS_AUSMPM, RS_HLLEPP, RS_HLLC_TRAMEL, RS_HLLC_CHEN = 5, 6, 7, 10
 SENSOR_DEFAULT, SENSOR_TRAMEL, SENSOR_CHEN, SENSOR_NONE = 0, 1, 2, 3
-INTVAR_CONS, INTVAR_PRIM = 0, 1
+INTVAR_CONS, INTVAR_PRIM, INTVAR_PREC = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 
 
@@ -85,7 +85,9 @@ class MBScheme(C.Structure):
                 ("cfl", C.c_double), ("vnn", C.c_double),
                 ("prandtl", C.c_double), ("schmidt", C.c_double), ("mco", C.c_double),
                 ("time_threshold", C.c_double), ("res_stop", C.c_double), ("irs_beta", C.c_double),
-                ("local_dt", C.c_int32), ("cfl_rise", C.c_int32)]
+                ("local_dt", C.c_int32), ("cfl_rise", C.c_int32), ("prec_smooth", C.c_int32), ("pad2", C.c_int32),
+                ("prec_eps_min", C.c_double), ("prec_uref", C.c_double), ("prec_mach", C.c_double),
+                ("prec_ur_factor", C.c_double), ("prec_ur_min", C.c_double)]
 
 
 class MBStatus(C.Structure):

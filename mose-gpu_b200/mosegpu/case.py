@@ -185,6 +185,12 @@ class Case:
         s.irs_beta = d.get("irs_beta", 0.5)
         s.local_dt = d.get("local_dt", 0)               # time-accurate = false: each cell its own step
         s.cfl_rise = d.get("cfl_rise", 0)               # cfl-rise-threshold
+        s.prec_smooth = d.get("prec_smooth", 0)         # integration-variables = prec: the preconditioning keys
+        s.prec_eps_min = d.get("prec_eps_min", 0.05)
+        s.prec_uref = d.get("prec_uref", 0.0)
+        s.prec_mach = d.get("prec_mach", 0.0)
+        s.prec_ur_factor = d.get("prec_ur_factor", 1.0)
+        s.prec_ur_min = d.get("prec_ur_min", 0.0)
         return s
 
 

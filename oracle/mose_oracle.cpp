@@ -80,8 +80,13 @@ struct Ctx {
   Thermo th;
   std::vector<double> pg;  // bc_pg(nprim, 6, nrec) of the connection records
   std::vector<double> acc4; // RK4: the conserved accumulator Un + dt (k1/6 + k2/3 + ...), (ncell, nprim)
+  std::vector<double> ur;   // prec: Ur of every row (ur_f; the ghost rows stay 0, Lib_Preconditioning.f90:146-153)
+  bool ur_ready = false;    // Ur computed (the first Compute_dt, then after every stage's update)
   mb_status st;
 };
+
+inline bool prec_on(const Ctx& c) { return c.sc.intvar == 2; }
+inline double ur_at(const Ctx& c, int64_t r) { return prec_on(c) ? c.ur[r] : 0.0; }
 
 // ---- indexing (MOSE_Field_m.f90:78-109; geometry shapes Mod_Convective.f90:594-596) ----
 inline int64_t row(const Blk& b, int i, int j, int k) {
@@ -279,9 +284,60 @@ inline double gam_state(const Thermo& th, double d, double p, double dtot) {
 void riemann_open(const Thermo& th, int rs, double mco, double bet, double dl, double ul, double vl, double wl,
                   double pl, double al, double dltot, double dr, double ur, double vr, double wr, double pr,
                   double ar, double drtot, double nx, double ny, double nz, double& F_r, double& F_u,
-                  double& F_v, double& F_w, double& F_E) {
+                  double& F_v, double& F_w, double& F_E, double urL_ = 0.0, double urR_ = 0.0) {
   double unl = ul * nx + vl * ny + wl * nz;
   double unr = ur * nx + vr * ny + wr * nz;
+  if (rs == 14) {  // HLLC-PC (riemann_open_body.inc:1092-1175, Riemann_HLLCprec): HLLC Batten with the signal speeds of
+                   // the preconditioned system, Vr = min(Ur, a) of each side and of the sqrt(rho) average
+    const double hL = h_static(th, dl, pl), hR = h_static(th, dr, pr);
+    const double eL = hL - pl / dltot, eR = hR - pr / drtot;
+    const double h0l = hL + 0.5 * (ul * ul + vl * vl + wl * wl), h0r = hR + 0.5 * (ur * ur + vr * vr + wr * wr);
+    const double EtL = eL + 0.5 * (ul * ul + vl * vl + wl * wl), EtR = eR + 0.5 * (ur * ur + vr * vr + wr * wr);
+    const double FrL = dltot * unl;
+    const double Ful = FrL * ul + pl * nx, Fvl = FrL * vl + pl * ny, Fwl = FrL * wl + pl * nz, Fel = FrL * h0l;
+    const double FrR = drtot * unr;
+    const double Fur = FrR * ur + pr * nx, Fvr = FrR * vr + pr * ny, Fwr = FrR * wr + pr * nz, Fer = FrR * h0r;
+    const double srL = std::sqrt(dltot), srR = std::sqrt(drtot), den = srL + srR;
+    const double u_roe = (srL * ul + srR * ur) / den, v_roe = (srL * vl + srR * vr) / den;
+    const double w_roe = (srL * wl + srR * wr) / den, a_roe = (srL * al + srR * ar) / den;
+    const double un_roe = u_roe * nx + v_roe * ny + w_roe * nz;
+    const double VrL = std::min(urL_, al), VrR = std::min(urR_, ar), VrRoe = (srL * VrL + srR * VrR) / den;
+    const double alL = (1.0 - (VrL * VrL) / (al * al)) / 2.0, alR = (1.0 - (VrR * VrR) / (ar * ar)) / 2.0;
+    const double alRoe = (1.0 - (VrRoe * VrRoe) / (a_roe * a_roe)) / 2.0;
+    const double vLs = unl * (1.0 - alL), vRs = unr * (1.0 - alR), vRoes = un_roe * (1.0 - alRoe);
+    const double cLs = std::sqrt(std::max(alL * alL * (unl * unl) + VrL * VrL, 0.0));
+    const double cRs = std::sqrt(std::max(alR * alR * (unr * unr) + VrR * VrR, 0.0));
+    const double cRoes = std::sqrt(std::max(alRoe * alRoe * (un_roe * un_roe) + VrRoe * VrRoe, 0.0));
+    const double S1 = std::min(std::min(0.0, vLs - cLs), vRoes - cRoes);
+    const double S4 = std::max(std::max(0.0, vRs + cRs), vRoes + cRoes);
+    const double Sstar = (pr - pl + dltot * unl * (S1 - unl) - drtot * unr * (S4 - unr)) /
+                         (dltot * (S1 - unl) - drtot * (S4 - unr));
+    const double pstar = dltot * (unl - S1) * (unl - Sstar) + pl;
+    if (S1 >= 0.0) {
+      F_r = FrL; F_u = Ful; F_v = Fvl; F_w = Fwl; F_E = Fel;
+    } else if (S4 <= 0.0) {
+      F_r = FrR; F_u = Fur; F_v = Fvr; F_w = Fwr; F_E = Fer;
+    } else if (Sstar >= 0.0) {
+      const double q = S1 - Sstar;
+      const double U1S = dltot * (S1 - unl) / q;
+      const double U2S = ((S1 - unl) * dltot * ul + (pstar - pl) * nx) / q;
+      const double U3S = ((S1 - unl) * dltot * vl + (pstar - pl) * ny) / q;
+      const double U4S = ((S1 - unl) * dltot * wl + (pstar - pl) * nz) / q;
+      const double U5S = ((S1 - unl) * dltot * EtL - pl * unl + pstar * Sstar) / q;
+      F_r = FrL + S1 * (U1S - dltot); F_u = Ful + S1 * (U2S - dltot * ul); F_v = Fvl + S1 * (U3S - dltot * vl);
+      F_w = Fwl + S1 * (U4S - dltot * wl); F_E = Fel + S1 * (U5S - dltot * EtL);
+    } else {
+      const double q = S4 - Sstar;
+      const double U1S = drtot * (S4 - unr) / q;
+      const double U2S = ((S4 - unr) * drtot * ur + (pstar - pr) * nx) / q;
+      const double U3S = ((S4 - unr) * drtot * vr + (pstar - pr) * ny) / q;
+      const double U4S = ((S4 - unr) * drtot * wr + (pstar - pr) * nz) / q;
+      const double U5S = ((S4 - unr) * drtot * EtR - pr * unr + pstar * Sstar) / q;
+      F_r = FrR + S4 * (U1S - drtot); F_u = Fur + S4 * (U2S - drtot * ur); F_v = Fvr + S4 * (U3S - drtot * vr);
+      F_w = Fwr + S4 * (U4S - drtot * wr); F_E = Fer + S4 * (U5S - drtot * EtR);
+    }
+    return;
+  }
   if (rs == 4) {  // riemann_open_body.inc:100-150
     const double ab = 0.125, aa = 0.1875;
     double vel = std::sqrt(ul * ul + vl * vl + wl * wl);
@@ -969,7 +1025,8 @@ double cell_beta(const Ctx& c, const Blk& b, const double* P, int i, int j, int 
 
 // ---- one interior convective face: conv_physics.inc:1-179 ----
 void conv_face(const Ctx& c, const double* pm1, const double* p0, const double* pp1, const double* pp2,
-               const double* dlc, const double* nrm, double area, double* res0, double bet) {
+               const double* dlc, const double* nrm, double area, double* res0, double bet, double urL = 0.0,
+               double urR = 0.0) {
   const Thermo& th = c.th;
   const int limv = c.sc.limiter, rsv = c.sc.riemann;
   double l0 = 0.5 * (dlc[0] + dlc[1]), l1 = 0.5 * (dlc[1] + dlc[2]), l2 = 0.5 * (dlc[2] + dlc[3]);
@@ -1080,8 +1137,9 @@ void conv_face(const Ctx& c, const double* pm1, const double* p0, const double* 
       F_r = drtot * unr; F_u = F_r * ur + pr * nx; F_v = F_r * vr + pr * ny; F_w = F_r * wr + pr * nz; F_E = F_r * h0r;
     }
   } else {
+    // HLLC-PC takes the Ur of the face's two cells (conv_physics.inc:159-163)
     riemann_open(th, rsv, c.sc.mco, bet, P1[0], ul, vl, wl, pl, al, dltot, P4[0], ur, vr, wr, pr, ar, drtot, nx, ny, nz,
-                 F_r, F_u, F_v, F_w, F_E);
+                 F_r, F_u, F_v, F_w, F_E, urL, urR);
   }
   double su = fsign_half(F_r), sp = 0.5 + su, sm = su - 0.5;
   double irotot1 = 1.0 / rotot1, irotot4 = 1.0 / rotot4;
@@ -1250,7 +1308,8 @@ void bc_face_geom(const Blk& b, int Im, int Jm, int Km, int Fm, double* nrm, dou
 
 void riemann_rec(const Ctx& c, double dl, double ul, double vl, double wl, double pl, double al, double dltot,
                  double dr, double ur, double vr, double wr, double pr, double ar, double drtot, double nx, double ny,
-                 double nz, double& F_r, double& F_u, double& F_v, double& F_w, double& F_E, double bet = 1.0);
+                 double nz, double& F_r, double& F_u, double& F_v, double& F_w, double& F_E, double bet = 1.0,
+                 double urL = 0.0, double urR = 0.0);
 
 // BC_Connection_Eul_lean (Lib_BC.f90:1770-1867)
 void bc_connection_eul(const Ctx& c, const Blk& b, const double* P, double* R, int Im, int Jm, int Km, int Fm) {
@@ -1288,8 +1347,9 @@ void bc_connection_eul(const Ctx& c, const Blk& b, const double* P, double* R, i
   rotot_rtot(th, PR[0], rhoR, RR);
   double aR = f_ss(th, PR[0], PR[IP], rhoR, RR);
   double F_r, F_u, F_v, F_w, F_E;
+  // HLLC-PC: the Ur of the two cells of the face, the ghost's 0 (never filled, Lib_BC.f90:1739-1742)
   riemann_rec(c, PL[0], PL[IU], PL[IV], PL[IW], PL[IP], aL, rhoL, PR[0], PR[IU], PR[IV], PR[IW], PR[IP], aR, rhoR,
-              nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E, beta_);
+              nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E, beta_, ur_at(c, r2), ur_at(c, r3));
   double su = fsign_half(F_r), selL = 0.5 + su, selR = su - 0.5;
   double Fmass = F_r * area;
   int64_t rm = row(b, Im, Jm, Km);
@@ -1390,7 +1450,8 @@ void bc_extrapolation(const Ctx& c, const Blk& b, const double* P, double* R, in
 // 2, SLAU for 3, the MOSE_open solvers for rs 4..14 (the face sensor argument is 1 at these records)
 void riemann_rec(const Ctx& c, double dl, double ul, double vl, double wl, double pl, double al, double dltot,
                  double dr, double ur, double vr, double wr, double pr, double ar, double drtot, double nx, double ny,
-                 double nz, double& F_r, double& F_u, double& F_v, double& F_w, double& F_E, double bet) {
+                 double nz, double& F_r, double& F_u, double& F_v, double& F_w, double& F_E, double bet, double urL,
+                 double urR) {
   if (c.sc.riemann == 1 || c.sc.riemann == 2)
     riemann_hllc_bc(c.th, c.sc.riemann, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz, F_r,
                     F_u, F_v, F_w, F_E);
@@ -1399,7 +1460,7 @@ void riemann_rec(const Ctx& c, double dl, double ul, double vl, double wl, doubl
                     F_E);
   else
     riemann_open(c.th, c.sc.riemann, c.sc.mco, bet, dl, ul, vl, wl, pl, al, dltot, dr, ur, vr, wr, pr, ar, drtot, nx, ny, nz,
-                 F_r, F_u, F_v, F_w, F_E);
+                 F_r, F_u, F_v, F_w, F_E, urL, urR);
 }
 
 // BC_Symmetry_Eul (Lib_BC.f90:640-737): the boundary cell mirrored about the face (Un_wall = 0), a limited
@@ -1445,8 +1506,9 @@ void bc_symmetry_eul(const Ctx& c, const Blk& b, const double* P, double* R, int
   double U1[3], U4[3];
   for (int a = 0; a < 3; ++a) { U1[a] = Un1 * nrm[a] + Vt[a]; U4[a] = -Un1 * nrm[a] + Vt[a]; }
   double F_r, F_u, F_v, F_w, F_E;
+  // HLLC-PC: the Ur of the cell on both sides (Lib_BC.f90:720-723)
   riemann_rec(c, F[0], U1[0], U1[1], U1[2], F[IP], Sound, rotot, F[0], U4[0], U4[1], U4[2], F[IP], Sound, rotot,
-              nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E);
+              nrm[0], nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E, 1.0, ur_at(c, rb), ur_at(c, rb));
   R[rb + IU * nc] = R[rb + IU * nc] + (double)modfm2 * F_u * area;
   R[rb + IV * nc] = R[rb + IV * nc] + (double)modfm2 * F_v * area;
   R[rb + IW * nc] = R[rb + IW * nc] + (double)modfm2 * F_w * area;
@@ -1807,8 +1869,9 @@ void bc_inflow_405(const Ctx& c, const Blk& b, const double* P, double* R, int I
   rotot_rtot(th, PR[0], rR, RR);
   double aR = f_ss(th, PR[0], PR[IP], rR, RR);
   double F_r, F_u, F_v, F_w, F_E;
+  // Ur = a on both sides: no preconditioning at the inlet (Lib_BC.f90:1308-1310)
   riemann_rec(c, PL[0], PL[IU], PL[IV], PL[IW], PL[IP], aL, rL, PR[0], PR[IU], PR[IV], PR[IW], PR[IP], aR, rR, nrm[0],
-              nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E);
+              nrm[1], nrm[2], F_r, F_u, F_v, F_w, F_E, 1.0, aL, aR);
   double su = std::copysign(1.0, F_r);
   double selL = (1.0 + su) / 2.0, selR = (su - 1.0) / 2.0;
   double Fmass = F_r * area;
@@ -2026,7 +2089,8 @@ void residual(Ctx& c, const double* P, double* R) {
             }
             for (int q = -1; q <= 2; ++q) dlc[q + 1] = dlv(b, d, i + q * e[0], j + q * e[1], k + q * e[2]);
             const double* f = (d == 0) ? fm1p(b, i, j, k) : (d == 1) ? fm2p(b, i, j, k) : fm3p(b, i, j, k);
-            conv_face(c, pm1, p0, pp1, pp2, dlc, f, f[3], res0, cell_beta(c, b, P, i, j, k));
+            conv_face(c, pm1, p0, pp1, pp2, dlc, f, f[3], res0, cell_beta(c, b, P, i, j, k), ur_at(c, r0),
+                      ur_at(c, r0 + st));
             int64_t fi;
             if (d == 0) fi = (i - 1) + (int64_t)(j - 1) * (n1 - 1) + (int64_t)(k - 1) * (n1 - 1) * n2;
             else if (d == 1) fi = (i - 1) + (int64_t)(j - 1) * n1 + (int64_t)(k - 1) * n1 * (n2 - 1);
@@ -2176,7 +2240,8 @@ void update_cell(const Ctx& c, const double* po, double* p, const double* res, d
 // Newstate_Primitive_blk (Lib_Newstate.f90:348-531), one species: the conservative residual taken to the primitive
 // variables by the inverse of the prim -> cons Jacobian (Theta = rho_p: no preconditioning), then the RK stage on the
 // primitive state: new = old + (state - old + res dt / vol) rkc, rho floored at 1e-20
-void update_cell_prim(const Ctx& c, const double* po, double* p, const double* res, double vol, double dt, double rkc) {
+void update_cell_prim(const Ctx& c, const double* po, double* p, const double* res, double vol, double dt, double rkc,
+                      double urc = 0.0) {
   const Thermo& th = c.th;
   const double strang = 1.0;
   double rho, Rgas;
@@ -2193,6 +2258,13 @@ void update_cell_prim(const Ctx& c, const double* po, double* p, const double* r
   double rho_p = 1.0 / (Rgas * temperature);
   double enthalpy = H0(th, p[IP], p[0], modvel);
   double Theta = rho_p;
+  if (prec_on(c)) {  // Weiss-Smith: Theta from the cell's Ur (Lib_Newstate.f90:399-402)
+    const double gam = cp / (cp - Rgas);
+    const double sound = std::sqrt(gam * Rgas * temperature);
+    const double a2 = sound * sound;
+    const double beta2 = std::max(urc * urc / a2, 1.0e-6);
+    Theta = 1.0 / (beta2 * a2) + 1.0 / (cp * temperature);
+  }
   double Denom = 1.0 / (rho * cp * Theta + rho_T);
   double G[5][5];
   G[0][0] = (rho_T * (enthalpy - q2) + rho * cp) * Denom;
@@ -2243,8 +2315,8 @@ void update(Ctx& c, double* P, const double* PO, const double* R, int irk, doubl
             T = std::min(std::max(T, 1.0), 9990.0);
           }
           const double dtc = dtl ? dtl[r] : dt;  // time-accurate = false: the cell's own dtlocal
-          if (c.sc.intvar == 1)
-            update_cell_prim(c, po, p, res, b.vol[lin(b, i, j, k)], dtc, rkc);
+          if (c.sc.intvar >= 1)
+            update_cell_prim(c, po, p, res, b.vol[lin(b, i, j, k)], dtc, rkc, ur_at(c, r));
           else if (c.sc.n_rk == 4)
             update_cell(c, po, p, res, b.vol[lin(b, i, j, k)], dtc, rkc, T, irk, &c.acc4[(size_t)r * NP]);
           else
@@ -2349,6 +2421,94 @@ void irs_apply(Ctx& c, double* R, double dt, bool scale, const double* dtl = nul
 }
 
 // ---- local dt: dt_blk.inc (min rule) + Thermo_Cache_rrt_blk / _visc_blk ----
+// ---- integration-variables = prec: the reference velocity Ur (Lib_Preconditioning.f90) ----
+
+// comp_Ur (:84-142): mode 1 a uniform Uref (the sound speed above it), mode 2 the target preconditioned Mach number
+// (the root w < 1 of A w^2 + B w + A = 0, w = (Ur / a)^2), mode 3 Weiss-Smith (|u| Ur-factor between eps_min a and a);
+// the viscous floor in modes 2 and 3, then Ur-min
+double comp_ur(const mb_scheme& sc, double vel, double sound, double ur_visc) {
+  double Ur;
+  const double eps = sc.prec_eps_min;
+  if (sc.prec_uref > 0.0) {
+    Ur = (vel > sc.prec_uref) ? sound : sc.prec_uref;
+  } else if (sc.prec_mach > 0.0) {
+    const double Mt = sc.prec_mach, m = vel / sound;
+    const double A_q = 0.25 * m * m * (Mt * Mt - 1.0);
+    const double B_q = Mt * Mt - 0.5 * m * m * (Mt * Mt + 1.0);
+    if (std::fabs(A_q) > 1.0e-30) {
+      const double S_q = -B_q / A_q, disc = S_q * S_q - 4.0;
+      if (disc > 0.0 && S_q > 2.0) Ur = sound * std::sqrt(2.0 / (S_q + std::sqrt(disc)));
+      else Ur = sound;
+    } else {
+      Ur = sound * eps;
+    }
+    Ur = std::max(Ur, eps * sound);
+    Ur = std::min(Ur, sound);
+    Ur = std::max(Ur, ur_visc);
+  } else {
+    if (vel < eps * sound) Ur = sound * eps;
+    else if (vel >= sound) Ur = sound;
+    else Ur = vel * sc.prec_ur_factor;
+    Ur = std::max(Ur, ur_visc);
+  }
+  if (sc.prec_ur_min > 0.0) Ur = std::max(Ur, sc.prec_ur_min);
+  return Ur;
+}
+
+// Update_Derived_Variables (:158-184): Ur_Blk (:187-264) of every interior cell of P, the viscous floor
+// max(mu / (rho dx_min), k / (rho cp dx_min)) with mu and k of the Wilke rule, then Smooth_Ur_Blk (:269-295): passes of
+// the max over the cell and its six face neighbours, the ghost neighbours 0
+void update_ur(Ctx& c, const double* P) {
+  const int64_t nc = c.ncell;
+  const Thermo& th = c.th;
+  for (const Blk& b : c.blk) {
+    for (int k = 1; k <= b.n3; ++k)
+      for (int j = 1; j <= b.n2; ++j)
+        for (int i = 1; i <= b.n1; ++i) {
+          const int64_t r = row(b, i, j, k);
+          double pl[NP];
+          for (int s = 0; s < NP; ++s) pl[s] = P[r + s * nc];
+          double rho, R;
+          rotot_rtot(th, pl[0], rho, R);
+          const double T = pl[IP] / (rho * R);
+          const double vel_mag = std::sqrt(pl[IU] * pl[IU] + pl[IV] * pl[IV] + pl[IW] * pl[IW]);
+          double ur_visc = 0.0;
+          if (c.sc.visc) {
+            double dx_min = dlv(b, 0, i, j, k);
+            for (int d = 1; d < c.sc.ndir; ++d) dx_min = std::min(dx_min, dlv(b, d, i, j, k));
+            const int ti = tidx(th, T);
+            const double td = T - ti;
+            const double cp = f_cp(th, pl[0], ti, td, rho);
+            double mu, lambda;
+            wilke(th, pl[0], rho, ti, td, mu, lambda);
+            ur_visc = std::max(mu / (rho * dx_min), lambda / (rho * cp * dx_min));
+          }
+          const double sound = f_ss(th, pl[0], pl[IP], rho, R);
+          c.ur[r] = comp_ur(c.sc, vel_mag, sound, ur_visc);
+        }
+    std::vector<double> urb((size_t)b.n1 * b.n2 * b.n3);
+    for (int pass = 0; pass < c.sc.prec_smooth; ++pass) {
+      const int64_t si = 1, sj = b.pi, sk = (int64_t)b.pi * b.pj;
+      size_t q = 0;
+      for (int k = 1; k <= b.n3; ++k)
+        for (int j = 1; j <= b.n2; ++j)
+          for (int i = 1; i <= b.n1; ++i, ++q) {
+            const int64_t r = row(b, i, j, k);
+            double m = c.ur[r];
+            m = std::max(m, c.ur[r - si]); m = std::max(m, c.ur[r + si]);
+            m = std::max(m, c.ur[r - sj]); m = std::max(m, c.ur[r + sj]);
+            m = std::max(m, c.ur[r - sk]); m = std::max(m, c.ur[r + sk]);
+            urb[q] = m;
+          }
+      q = 0;
+      for (int k = 1; k <= b.n3; ++k)
+        for (int j = 1; j <= b.n2; ++j)
+          for (int i = 1; i <= b.n1; ++i, ++q) c.ur[row(b, i, j, k)] = urb[q];
+    }
+  }
+  c.ur_ready = true;
+}
+
 // the local step of one interior cell of P (Compute_dt_blk, dt_blk.inc:11-191), before the ramp factor
 double cell_dt(const Ctx& c, const Blk& b, const double* P, int i, int j, int k) {
   const int64_t nc = c.ncell;
@@ -2361,13 +2521,22 @@ double cell_dt(const Ctx& c, const Blk& b, const double* P, int i, int j, int k)
   double Tc = pl[IP] / (rho * Rg);
   double Sound = f_ss(th, pl[0], pl[IP], rho, Rg);
   double dtc = 1e8;
+  const bool prec = prec_on(c);
+  double Alpha_ = 0.0, urc = 0.0;
+  if (prec) {  // the pseudo-acoustic speed of the preconditioned system (dt_blk.inc:72-75)
+    urc = c.ur[r];
+    const double Beta_ = 1.0 / (Sound * Sound);
+    Alpha_ = 0.5 * (1.0 - Beta_ * (urc * urc));
+  }
   if (c.sc.dt_additive) {  // dt-rule = additive (dt_blk.inc:79-155)
     double ra_c = 0.0, ra_v = 0.0;
     for (int d = 0; d < c.sc.ndir; ++d) {
       double m0 = mv(b, d, 0, i, j, k), m1 = mv(b, d, 1, i, j, k), m2 = mv(b, d, 2, i, j, k);
       double gn = std::sqrt(m0 * m0 + m1 * m1 + m2 * m2);
       double vel_ = std::fabs(pl[IU] * m0 + pl[IV] * m1 + pl[IW] * m2) / gn;
-      double lambda = vel_ + Sound;
+      double lambda;
+      if (prec) lambda = vel_ * (1.0 - Alpha_) + std::sqrt(Alpha_ * Alpha_ * (vel_ * vel_) + urc * urc);
+      else lambda = vel_ + Sound;
       ra_c = ra_c + lambda * gn;
       ra_v = ra_v + gn * gn;
     }
@@ -2406,7 +2575,14 @@ double cell_dt(const Ctx& c, const Blk& b, const double* P, int i, int j, int k)
     double nrm = std::sqrt(m0 * m0 + m1 * m1 + m2 * m2);
     double v0 = m0 / nrm, v1 = m1 / nrm, v2 = m2 / nrm;
     double vel_ = std::fabs(pl[IU] * v0 + pl[IV] * v1 + pl[IW] * v2);
-    double lambda = vel_ + Sound;
+    double lambda;
+    if (prec) {
+      const double cst_ = std::sqrt(Alpha_ * Alpha_ * (vel_ * vel_) + urc * urc);
+      vel_ = vel_ * (1.0 - Alpha_);
+      lambda = vel_ + cst_;
+    } else {
+      lambda = vel_ + Sound;
+    }
     double dtd = dlv(b, d, i, j, k) / lambda * c.sc.cfl;
     dtc = std::min(dtd, dtc);
   }
@@ -2458,11 +2634,13 @@ struct orc_ctx { Ctx c; };
 
 int orc_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, orc_ctx** out) {
   if (!mesh || !sc || !th || !out) return MB_E_ARG;
-  if (sc->riemann < 1 || sc->riemann > 13 || sc->sensor < 0 || sc->sensor > 3 || sc->intvar < 0 || sc->intvar > 1 ||
-      (sc->intvar == 1 && sc->n_rk == 4) || sc->irs < 0 || sc->irs > 4 || (sc->irs > 0 && sc->n_rk == 4))
+  if (sc->riemann < 1 || sc->riemann > 14 || sc->sensor < 0 || sc->sensor > 3 || sc->intvar < 0 || sc->intvar > 2 ||
+      (sc->intvar >= 1 && sc->n_rk == 4) || (sc->riemann == 14) != (sc->intvar == 2) ||
+      (sc->intvar == 2 && sc->local_dt != 1) || sc->irs < 0 || sc->irs > 4 || (sc->irs > 0 && sc->n_rk == 4))
     return MB_E_UNSUPPORTED;
   if (sc->irs > 0 && !(sc->irs_beta >= 0.0 && std::isfinite(sc->irs_beta))) return MB_E_ARG;
   if (sc->local_dt < 0 || sc->local_dt > 1 || sc->cfl_rise < 0) return MB_E_ARG;
+  if (sc->intvar == 2 && !(sc->prec_eps_min > 0.0 && sc->prec_eps_min < 1.0 && sc->prec_smooth >= 0)) return MB_E_ARG;
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
   if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
   orc_ctx* o = new orc_ctx();
@@ -2489,6 +2667,7 @@ int orc_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, orc_
     }
   c.pg.assign((size_t)c.rec.size() * 6 * NP, 0.0);
   if (sc->n_rk == 4) c.acc4.assign((size_t)c.ncell * NP, 0.0);
+  if (sc->intvar == 2) c.ur.assign((size_t)c.ncell, 0.0);
   Thermo& t = c.th;
   t.tmin = th->tmin; t.tmax = th->tmax; t.wm = th->wm; t.ri = RUNIV / th->wm;
   size_t nt = (size_t)(th->tmax - th->tmin + 1);
@@ -2504,9 +2683,20 @@ int orc_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, orc_
 void orc_destroy(orc_ctx* o) { delete o; }
 
 int orc_fill_ghosts(orc_ctx* o, double* P) { fill_ghosts(o->c, P); return MB_OK; }
-int orc_residual(orc_ctx* o, const double* P, double* R) { residual(o->c, P, R); return MB_OK; }
+// prec: an entry point that reads Ur computes it from the state it is given when nothing has yet (the reference's first
+// Compute_dt); the time loop refreshes it after every stage's update (Mod_Explicit.f90:273-277)
+static void ur_first(Ctx& c, const double* P) {
+  if (prec_on(c) && !c.ur_ready) update_ur(c, P);
+}
+
+int orc_residual(orc_ctx* o, const double* P, double* R) {
+  ur_first(o->c, P);
+  residual(o->c, P, R);
+  return MB_OK;
+}
 int orc_update(orc_ctx* o, double* P, const double* PO, const double* R, int irk, double dt) {
   Ctx& c = o->c;
+  ur_first(c, P);
   // time-accurate = false: each cell's dtlocal, from the state at the start of the step (PO)
   std::vector<double> dtl;
   if (c.sc.local_dt) {
@@ -2523,7 +2713,11 @@ int orc_update(orc_ctx* o, double* P, const double* PO, const double* R, int irk
   }
   return c.st.code;
 }
-int orc_dt(orc_ctx* o, const double* P, double* dt) { *dt = compute_dt(o->c, P); return MB_OK; }
+int orc_dt(orc_ctx* o, const double* P, double* dt) {
+  ur_first(o->c, P);
+  *dt = compute_dt(o->c, P);
+  return MB_OK;
+}
 
 // nsteps explicit steps (Mod_Explicit.f90:52-279): dt, PO <- P, then per stage ghost fill, residual, update.
 int orc_step(orc_ctx* o, double* P, double* PO, double* R, int nsteps) {
@@ -2531,6 +2725,7 @@ int orc_step(orc_ctx* o, double* P, double* PO, double* R, int nsteps) {
   const int64_t n = c.ncell * NP;
   for (int st = 0; st < nsteps; ++st) {
     if (c.st.done) return MB_OK;  // the residual end test stopped the case (Mod_Explicit.f90:363-370)
+    ur_first(c, P);
     std::vector<double> dtl;
     if (c.sc.local_dt) dtl.assign((size_t)c.ncell, 0.0);
     double dt = compute_dt(c, P, c.sc.local_dt ? &dtl : nullptr);
@@ -2549,6 +2744,7 @@ int orc_step(orc_ctx* o, double* P, double* PO, double* R, int nsteps) {
       residual(c, P, R);
       if (c.sc.irs > 0) irs_apply(c, R, dt, c.sc.intvar == 0, dl);
       update(c, P, PO, R, irk, dt, c.sc.irs > 0 && c.sc.intvar == 0, dl);
+      if (prec_on(c)) update_ur(c, P);  // Ur of the updated state
     }
     // the residual diagnostic of the step (Compute_Residual_blk, Mod_Diagnostic.f90:64-104; the L2 norm of
     // Mod_Explicit.f90:325-358): sqrt of the sum over the interior cells of (new - old)^2 per primitive variable

@@ -63,6 +63,12 @@ def with_scheme(case, **kw):
     return case
 
 
+def prec_case(case, **kw):
+    """The case with integration-variables = prec (HLLC-PC, local steps) and the given preconditioning keys."""
+    case.scheme["riemann"] = abi.RS_HLLC_PC
+    return with_scheme(case, intvar=abi.INTVAR_PREC, local_dt=1, **kw)
+
+
 def small_cases():
     """(id, builder) of the parity cases: every boundary type, Riemann solver and limiter served."""
     return [
@@ -137,6 +143,14 @@ def small_cases():
         ("duct3d_local_dt_prim_rise4", lambda: with_scheme(cs.duct_3d(), local_dt=1, intvar=abi.INTVAR_PRIM,
                                                            cfl_rise=4)),
         ("sod_rise5_hllc", lambda: with_scheme(cs.riemann_1d(n=64), cfl_rise=5)),
+        # integration-variables = prec: Ur (the three modes, smoothing), the preconditioned local steps, Theta of the
+        # primitive update and HLLC-PC at interior faces, connections (the ghost's Ur 0), symmetry faces and walls
+        ("mb2d_prec_hllcpc_ns", lambda: prec_case(cs.multiblock_2d(cols=2, rows=2, lo=5, hi=9, seed=47, n_rk=3,
+                                                                    mach=0.2, cfl=0.3))),
+        ("duct3d_prec_mach03_smooth2", lambda: prec_case(cs.duct_3d(cfl=0.3), prec_mach=0.3, prec_smooth=2)),
+        ("tgv_prec_uref_8blk", lambda: prec_case(with_scheme(cs.taylor_green(n=12, blocks=2, noise=1e-3), cfl=0.3),
+                                                 prec_uref=200.0)),
+        ("sod_prec_irs2_rk2", lambda: prec_case(cs.riemann_1d(n=64, n_rk=2, cfl=0.3), irs=2, prec_eps_min=0.9)),
         # symmetry (300), isothermal walls (302) and the back-pressure outlet (406)
         ("duct3d_hllc_vanleer", lambda: cs.duct_3d()),
         ("duct3d_roe_vanalbada_rk4", lambda: cs.duct_3d(widths=(5, 6), heights=(4, 3), depths=(4,),

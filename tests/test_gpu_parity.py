@@ -297,11 +297,13 @@ def test_record_params_changed_between_steps_match_the_oracle(torch_cuda):
 
 
 @pytest.mark.parametrize("cid", ["tgv_irs2_roe_8blk", "mb2d_irs3_ausm_rk2_beta07", "duct3d_irs1_hllc_beta03",
-                                 "mb2d_local_dt_ausm_rk3_rise10", "tgv_local_dt_roe_8blk", "sod_local_dt_irs2_hllc"])
+                                 "mb2d_local_dt_ausm_rk3_rise10", "tgv_local_dt_roe_8blk", "sod_local_dt_irs2_hllc",
+                                 "mb2d_prec_hllcpc_ns", "duct3d_prec_mach03_smooth2"])
 def test_irs_mixed_within_gate_and_stages_match_fused(torch_cuda, cid):
-    """With residual smoothing or local time stepping: the mixed form (FP32 fluxes; the smoothing and the update in
-    FP64; the local steps of the fused sweep in FP32) stays within L2(rho) 1e-5 of the FP64 form after 20 steps, and
-    the reference's call sequence (begin_step + stage 1..n) equals mb_step bit for bit."""
+    """With residual smoothing, local time stepping or preconditioning: the mixed form (FP32 fluxes; the smoothing,
+    Ur, the preconditioned steps and the update in FP64; the local steps of the fused sweep in FP32) stays within
+    L2(rho) 1e-5 of the FP64 form after 20 steps, and the reference's call sequence (begin_step + stage 1..n) equals
+    mb_step bit for bit."""
     from mosegpu.engine import Engine
     case = dict(H.small_cases())[cid]()
     a = Engine(case, precision=abi.PREC_FP64)

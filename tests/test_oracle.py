@@ -348,3 +348,68 @@ def test_cfl_rise_ramps_the_first_steps():
         want = oc.dt(Pd) * (min(n, 10) / 10.0)
         assert od.step(Pd, 1) == 0
         assert abs(od.status().dt - want) <= 1e-15 * want, n
+
+
+def _prec(case, **kw):
+    case.scheme["riemann"] = abi.RS_HLLC_PC
+    return H.with_scheme(case, intvar=abi.INTVAR_PREC, local_dt=1, **kw)
+
+
+@pytest.mark.parametrize("mode", ["weiss_smith", "uref", "mach"])
+def test_prec_local_step_is_that_of_the_pseudo_acoustic_speed(mode):
+    """integration-variables = prec on a uniform 1-D stream at M 0.1: Ur of each mode of comp_Ur
+    (Lib_Preconditioning.f90:84-142) and the local step dl / (|u| (1 - alpha) + sqrt(alpha^2 u^2 + Ur^2)) cfl,
+    alpha = (1 - Ur^2 / a^2) / 2 (dt_blk.inc:72-75, 176-182), against this closed-form restatement."""
+    kw = {"weiss_smith": {}, "uref": {"prec_uref": 0.3}, "mach": {"prec_mach": 0.5}}[mode]
+    st = (1.0, 0.1 * np.sqrt(1.4), 1.0)                     # rho, u, p: a = sqrt(1.4), M = 0.1
+    c = _prec(cs.riemann_1d(n=40, left=st, right=st), **kw)
+    o = oracle.Oracle(c)
+    a = np.sqrt(1.4)
+    u = st[1]
+    if mode == "weiss_smith":
+        Ur = u                                               # eps_min a < |u| < a: |u| Ur-factor
+    elif mode == "uref":
+        Ur = 0.3                                             # |u| <= Uref
+    else:
+        Mt, m = 0.5, u / a
+        A, B = 0.25 * m * m * (Mt * Mt - 1.0), Mt * Mt - 0.5 * m * m * (Mt * Mt + 1.0)
+        S = -B / A
+        Ur = min(max(a * np.sqrt(2.0 / (S + np.sqrt(S * S - 4.0))), 0.05 * a), a)
+    alpha = 0.5 * (1.0 - Ur * Ur / (a * a))
+    dl = c.blocks[0]["dl"].reshape((3,) + c.padded(0), order="F")[0, 2, 2, 2]
+    want = dl / (u * (1.0 - alpha) + np.sqrt(alpha * alpha * u * u + Ur * Ur)) * c.scheme["cfl"]
+    assert abs(o.dt(c.P0.copy()) - want) <= 1e-13 * want
+    plain = cs.riemann_1d(n=40, left=st, right=st)
+    assert o.dt(c.P0.copy()) > 3.0 * oracle.Oracle(plain).dt(plain.P0.copy())
+
+
+def test_prec_with_ur_equal_to_the_sound_speed_is_the_plain_step_and_keeps_a_uniform_stream():
+    """Ur = a (a Uref below |u|): alpha = 0 and c* = a, so the preconditioned step is the plain one; and the
+    preconditioned update with HLLC-PC keeps a uniform stream uniform (the fluxes of equal states are the physical
+    flux) with and without the Ur smoothing."""
+    st = (1.0, 0.5, 1.0)
+    c = _prec(cs.riemann_1d(n=40, left=st, right=st), prec_uref=1e-3)
+    plain = cs.riemann_1d(n=40, left=st, right=st)
+    d0, d1 = oracle.Oracle(plain).dt(plain.P0.copy()), oracle.Oracle(c).dt(c.P0.copy())
+    assert abs(d1 - d0) <= 1e-15 * d0
+    for kw in ({}, {"prec_smooth": 2}):
+        u = _prec(cs.riemann_1d(n=40, left=st, right=st), **kw)
+        P = u.P0.copy()
+        assert oracle.Oracle(u).step(P, 5) == 0
+        m = u.interior_mask()
+        assert np.abs(P[:, m] - u.P0[:, m]).max() <= 1e-13
+
+
+def test_prec_runs_a_low_mach_channel_with_larger_steps():
+    """The purpose of the preconditioning: on a 2-D channel at M 0.05 the preconditioned local steps are several
+    times the plain ones and the run stays physical (CFL 0.2, HLLC-PC, RK3)."""
+    def make(prec):
+        c = cs.multiblock_2d(cols=2, rows=1, widths=[10, 10], heights=[8], seed=41, visc=0, n_rk=3, mach=0.05,
+                             amp=0.02, cfl=0.2)
+        return _prec(c) if prec else H.with_scheme(c, local_dt=1)
+    a, b = make(False), make(True)
+    da, db = oracle.Oracle(a).dt(a.P0.copy()), oracle.Oracle(b).dt(b.P0.copy())
+    assert db > 4.0 * da
+    P = b.P0.copy()
+    o = oracle.Oracle(b)
+    assert o.step(P, 300) == 0 and o.status().code == 0
