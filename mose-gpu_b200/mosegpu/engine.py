@@ -207,6 +207,24 @@ class Engine:
         qa = (C.c_double * abi.BC_NQ)(*[float(x) for x in q])
         _check(self.lib.mb_set_record_params(self.ctx, int(rec), qa, self._s()), "mb_set_record_params")
 
+    def save_native(self, path):
+        """Backup of the case in the reference's native field file (write_native, IO_Solution.f90:450-496): the
+        interior of every block and the simulated time, -1 for a steady run (local_dt) as Wrap_Setup.f90:152-166."""
+        from .native_io import write_native
+        t = -1.0 if self.case.scheme.get("local_dt", 0) else self.status().time
+        write_native(path, self.case, self.state(), t)
+
+    def load_native(self, path):
+        """Restart from a native field file (read_native, IO_Solution.f90:223-292): replaces the interior of every
+        block of the device state (the ghost rows are refilled by the next stage) and returns the stored time. The
+        case clock is not moved: a time-accurate restart that must stop at t_end gives mb_group_reset the time
+        still to run."""
+        from .native_io import read_native
+        P, t = read_native(path, self.case, self.state())
+        self.set_state(P)
+        self.dt()        # the device minimum of the local steps now belongs to the loaded state (mb_step reuses it)
+        return t
+
     def run_to(self, t_end, max_steps=10 ** 7, chunk=1):
         """Steps until the simulated time reaches t_end (the reference's `time >= timemax` stop) or the case's
         residual stop (scheme res_stop) ends it."""
