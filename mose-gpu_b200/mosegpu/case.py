@@ -139,6 +139,16 @@ class Case:
         self.P0 = None
         self.steps = 1
         self.meta = {}
+        self.node_fn = None  # (iu, iv, iw) global node indices -> (..., 3) coordinates
+
+    def nodes(self, b):
+        """Node coordinates (n1+1, n2+1, n3+1, 3) of the interior of block b, from the mapping the case was built
+        with (the mesh file's nodes of the reference)."""
+        blk = self.blocks[b]
+        n, lo = blk["n"], blk["lo"]
+        ax = [np.arange(lo[d], lo[d] + n[d] + 1, dtype=np.float64) for d in range(3)]
+        IU, IV, IW = np.meshgrid(ax[0], ax[1], ax[2], indexing="ij")
+        return self.node_fn(IU, IV, IW)
 
     # --- indexing helpers (MOSE_Field_m.f90:78-109)
     def padded(self, b):
@@ -219,6 +229,7 @@ def layout_case(name, cuts, node_fn, periodic, bc_faces, thermo, scheme, prim_fn
     case = Case(name)
     case.thermo = thermo
     case.scheme = dict(scheme)
+    case.node_fn = node_fn
     nb = [len(c) - 1 for c in cuts]
     Ntot = [c[-1] for c in cuts]
     blocks = []

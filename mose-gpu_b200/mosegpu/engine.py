@@ -214,6 +214,13 @@ class Engine:
         t = -1.0 if self.case.scheme.get("local_dt", 0) else self.status().time
         write_native(path, self.case, self.state(), t)
 
+    def save_tecplot(self, path):
+        """The solution file in Tecplot ASCII (write_vtk_tec, IO_Solution.f90:499-587, through ORION's ASCII
+        writer): nodes, the interior primitive variables and T of every block."""
+        from .tecplot import write_tecplot_ascii
+        t = -1.0 if self.case.scheme.get("local_dt", 0) else self.status().time
+        write_tecplot_ascii(path, self.case, self.state(), t)
+
     def load_native(self, path):
         """Restart from a native field file (read_native, IO_Solution.f90:223-292): replaces the interior of every
         block of the device state (the ghost rows are refilled by the next stage) and returns the stored time. The
