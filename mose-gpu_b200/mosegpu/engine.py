@@ -221,6 +221,15 @@ class Engine:
         t = -1.0 if self.case.scheme.get("local_dt", 0) else self.status().time
         write_tecplot_ascii(path, self.case, self.state(), t)
 
+    def load_tecplot(self, path):
+        """Start or restart from a Tecplot ASCII field in ORION's layout (read_vtk_tec, IO_Solution.f90:294-328):
+        replaces the interior of every block of the device state; returns (time, steady) of the file."""
+        from .tecplot import read_tecplot_ascii
+        P, t, steady = read_tecplot_ascii(path, self.case, self.state())
+        self.set_state(P)
+        self.dt()        # the device minimum of the local steps now belongs to the loaded state (mb_step reuses it)
+        return t, steady
+
     def load_native(self, path):
         """Restart from a native field file (read_native, IO_Solution.f90:223-292): replaces the interior of every
         block of the device state (the ghost rows are refilled by the next stage) and returns the stored time. The

@@ -22,6 +22,7 @@ value rounded to 15 significant digits (nearest), a 3-digit signed exponent, rig
 `Infinity`, `-Infinity` right-justified, as gfortran writes them.
 """
 import math
+import re
 
 import numpy as np
 
@@ -88,3 +89,74 @@ def write_tecplot_ascii(path, case, P, time):
             for s in range(5):
                 f.write(_lines(v[s].ravel(order="F")))
             f.write(_lines(temperature(case, v[0], v[4]).ravel(order="F")))
+
+
+def _zone_fields(text):
+    """KEY=value pairs of zone header text (T, I, J, K, DATAPACKING, VARLOCATION, SOLUTIONTIME, STRANDID ...)."""
+    out = {}
+    for m in re.finditer(r"([A-Za-z]+)\s*=\s*(\([^)]*\)\)?|\"[^\"]*\"|[^,\s]+)", text):
+        out[m.group(1).upper()] = m.group(2)
+    return out
+
+
+def _is_number_line(line):
+    try:
+        [float(x.replace("D", "E").replace("d", "e")) for x in line.split()]
+        return bool(line.split())
+    except ValueError:
+        return False
+
+
+def read_tecplot_ascii(path, case, P=None):
+    """Reads a Tecplot ASCII field in ORION's structured block layout (tec_read_structured_multiblock, ascii branch,
+    Lib_Tecplot.f90:452-600: one zone per block, nodal x, y, z, then cell-centred variables; the reader of an
+    `ini-format` / `rst-format = tecplot ascii` start, read_vtk_tec, IO_Solution.f90:294-328). Returns
+    `(P, time, steady)`: the first five variables of every zone (rho, u, v, w, p; further ones such as T are skipped,
+    as the reference keeps only its nprim) written into the interior of a copy of `P` (or of `case.P0`), the zone's
+    SOLUTIONTIME and whether the zone carries a STRANDID (a steady run's file). The zone count and I, J, K must match
+    the case's blocks (nodes = cells + 1); nodal variables are not served (ORION writes MOSE's fields cell-centred)."""
+    base = case.P0 if P is None else P
+    out = np.array(base, dtype=np.float64, copy=True)
+    with open(path) as f:
+        lines = f.read().splitlines()
+    names = None
+    q = 0
+    while q < len(lines) and "ZONE" not in lines[q].upper():
+        if "VARIABLES" in lines[q].upper():
+            names = re.findall(r"\"([^\"]*)\"", lines[q])
+        q += 1
+    if not names or len(names) < 8:
+        raise ValueError("no VARIABLES line with x, y, z and five field variables")
+    nvar = len(names) - 3
+    time, steady = 0.0, False
+    for b in range(len(case.blocks)):
+        if q >= len(lines):
+            raise ValueError(f"the file holds {b} zones, the case has {len(case.blocks)} blocks")
+        head = []
+        while q < len(lines) and not _is_number_line(lines[q]):
+            head.append(lines[q])
+            q += 1
+        z = _zone_fields(" ".join(head))
+        n1, n2, n3 = case.blocks[b]["n"]
+        dims = tuple(int(z.get(k, "0")) for k in ("I", "J", "K"))
+        if dims != (n1 + 1, n2 + 1, n3 + 1):
+            raise ValueError(f"zone {b + 1}: I, J, K = {dims}, the block has {(n1 + 1, n2 + 1, n3 + 1)} nodes")
+        if "CELLCENTERED" not in z.get("VARLOCATION", "").upper():
+            raise ValueError(f"zone {b + 1}: the variables are not cell-centred")
+        if "SOLUTIONTIME" in z:
+            time = float(z["SOLUTIONTIME"].replace("D", "E"))
+        steady = "STRANDID" in z
+        nn, nc = (n1 + 1) * (n2 + 1) * (n3 + 1), n1 * n2 * n3
+        need = 3 * nn + nvar * nc
+        vals = []
+        while len(vals) < need:
+            if q >= len(lines):
+                raise ValueError(f"zone {b + 1}: the file ends after {len(vals)} of {need} values")
+            vals += [float(x.replace("D", "E").replace("d", "e")) for x in lines[q].split()]
+            q += 1
+        if len(vals) != need:
+            raise ValueError(f"zone {b + 1}: {len(vals)} values, expected {need}")
+        v = np.asarray(vals[3 * nn:], dtype=np.float64)
+        for s in range(5):
+            case.interior(out, b)[s] = v[s * nc:(s + 1) * nc].reshape(n3, n2, n1).transpose(2, 1, 0)
+    return out, time, steady

@@ -5,6 +5,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from mosegpu import case as cs
 from mosegpu.tecplot import fortran_e23_15e3, temperature, write_tecplot_ascii
@@ -88,3 +89,62 @@ def test_steady_run_zone_and_temperature(tmp_path):
     v = c.interior(c.P0, 0)
     R = 8314.46261815324 / c.thermo["wm"]
     assert np.allclose(temperature(c, v[0], v[4]), v[4] / (v[0] * R), rtol=1e-15)
+
+
+def test_reader_round_trip_of_the_writer(tmp_path):
+    from mosegpu.tecplot import read_tecplot_ascii
+    c = cs.multiblock_2d(cols=2, rows=2, lo=5, hi=8, seed=5)
+    rng = np.random.default_rng(4)
+    P = c.P0 * (1.0 + 1e-3 * rng.standard_normal(c.P0.shape))
+    path = tmp_path / "field.tec"
+    write_tecplot_ascii(path, c, P, 0.5)
+    Q, t, steady = read_tecplot_ascii(path, c)
+    assert t == 0.5 and not steady
+    m = c.interior_mask()
+    assert np.allclose(Q[:, m], P[:, m], rtol=1e-14, atol=0)      # 15 significant digits
+    assert np.array_equal(Q[:, ~m], c.P0[:, ~m])
+    write_tecplot_ascii(path, c, P, -1.0)
+    _, t, steady = read_tecplot_ascii(path, c)
+    assert t == 1.0 and steady
+
+
+def test_reader_takes_orion_zone_headers_and_skips_extra_variables(tmp_path):
+    """A one-cell-deep block written in the two header styles of the reference's test inputs (one ZONE line with
+    DATAPACKING / VARLOCATION / SOLUTIONTIME, as ORION writes; and a multi-line header), values several per line
+    and with D exponents, a sixth variable that the reader skips."""
+    from mosegpu.tecplot import read_tecplot_ascii
+    c = cs.riemann_1d(n=3)
+    n1, n2, n3 = c.blocks[0]["n"]
+    nn, nc = (n1 + 1) * (n2 + 1) * (n3 + 1), n1 * n2 * n3
+    xyz = list(np.arange(3 * nn, dtype=float))
+    fields = [[10.0 * s + i + 0.5 for i in range(nc)] for s in range(6)]
+    zone_line = [ln[1:] for ln in _golden() if ln.startswith("H ZONE") and "CELLCENTERED" in ln][0]
+    zone_line = re.sub(r"I=\d+, J=\d+, K=\d+", f"I={n1 + 1}, J={n2 + 1}, K={n3 + 1}", zone_line)
+    zone_line = zone_line.replace("[4-8]", "[4-9]")
+    body = " ".join("%.17g" % v for v in xyz) + "\n" + "\n".join(
+        " ".join(("%.17e" % v).replace("e", "D") for v in f) for f in fields) + "\n"
+    times = []
+    for header in (zone_line + "\n",
+                   f' ZONE T="BLOCCO 1"\n I= {n1 + 1}, J= {n2 + 1}, K= {n3 + 1}, DATAPACKING=BLOCK, '
+                   f'VARLOCATION=([1-3]=NODAL,[4-9]=CELLCENTERED)\n'):
+        path = tmp_path / "ic.tec"
+        path.write_text(' VARIABLES ="x" "y" "z" "rho1" "u" "v" "w" "p" "T"\n' + header + body)
+        Q, t, _ = read_tecplot_ascii(path, c)
+        v = c.interior(Q, 0)
+        for s in range(5):
+            assert np.array_equal(v[s].ravel(order="F"), np.array(fields[s]))
+        times.append(t)
+    assert times == [float("0.695304987880493E-309"), 0.0]     # the subnormal SOLUTIONTIME; no SOLUTIONTIME key
+
+
+def test_reader_rejects_a_file_that_does_not_fit(tmp_path):
+    from mosegpu.tecplot import read_tecplot_ascii
+    c = cs.riemann_1d(n=8)
+    path = tmp_path / "field.tec"
+    write_tecplot_ascii(path, c, c.P0, 0.0)
+    with pytest.raises(ValueError, match="nodes"):
+        read_tecplot_ascii(path, cs.riemann_1d(n=9))
+    text = path.read_text().splitlines()
+    (tmp_path / "cut.tec").write_text("\n".join(text[:-3]) + "\n")
+    with pytest.raises(ValueError, match="ends"):
+        read_tecplot_ascii(tmp_path / "cut.tec", c)
