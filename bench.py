@@ -245,15 +245,39 @@ def run_c5(args, dev, stream):
     return r
 
 
-def run_serving(args, dev):
+def partition_requests(reqs, world, rank):
+    """Serving cases are independent (no exchange between them): rank r of `world` serves requests r, r + world,
+    r + 2 world, ... of the one seeded stream every rank builds."""
+    return reqs[rank::world]
+
+
+def merge_serving(parts):
+    """One serving summary from every rank's part: (latencies, first arrival, last finish, cell-updates, cases
+    completed, failed request ids); the ranks started their request loops together (after a barrier)."""
+    lat = np.array(sorted(x for p in parts for x in p[0]))
+    done = int(sum(p[4] for p in parts))
+    firsts = [p[1] for p in parts if p[1] is not None]
+    lasts = [p[2] for p in parts if p[2] is not None]
+    span = (max(lasts) - min(firsts)) if (done and firsts and lasts) else float("nan")
+    work = float(sum(p[3] for p in parts))
+    return {"cases_completed": done, "failed": sorted(x for p in parts for x in p[5]),
+            "cases_per_s": done / span if done else 0.0,
+            "p50_s": float(np.percentile(lat, 50)) if done else None,
+            "p99_s": float(np.percentile(lat, 99)) if done else None,
+            "cell_updates_per_s": work / span if done else 0.0, "makespan_s": span}
+
+
+def run_serving(args, dev, world=1, rank=0, pg=None):
     """A bounded sample of the seeded serving stream (1-D and 2-D Riemann cases, HLLC + minmod, SSP-RK3,
     CFL 0.5, mixed precision) through the continuous-batching server: p50 / p99 time-to-solution (arrival to
-    result on the host), cases/s over the run, and the cell-updates/s the batch sustained."""
+    result on the host), cases/s over the run, and the cell-updates/s the batch sustained. Under torchrun the
+    cases are partitioned over the ranks (partition_requests) and the summary merges every rank's cases."""
     from mosegpu import abi
     from mosegpu import serving as sv
     t0 = time.time()
     stream = sv.request_stream(n_cases=args.serve_cases, rate=args.serve_rate, seed=20261203)
-    reqs = [sv.riemann_request(q, d, n, st, te, arrival=t) for q, (t, d, n, st, te) in enumerate(stream)]
+    reqs_all = [sv.riemann_request(q, d, n, st, te, arrival=t) for q, (t, d, n, st, te) in enumerate(stream)]
+    reqs = partition_requests(reqs_all, world, rank)
     setup = time.time() - t0
     # two lanes: 1-D cases (cheap steps, many of them) and 2-D cases, each its own context and stream
     budget = int(args.serve_budget_gb * 2 ** 30)
@@ -261,22 +285,26 @@ def run_serving(args, dev):
                        max_cases=128, precision=abi.PREC_MIXED, device=dev.index, poll_steps=args.serve_poll),
              sv.Server(reqs[0].case.scheme, reqs[0].case.thermo, budget_bytes=budget - min(2 << 30, budget // 4),
                        max_cases=128, precision=abi.PREC_MIXED, device=dev.index, poll_steps=args.serve_poll)]
+    if pg is not None:
+        barrier(pg, dev)
     done = sv.serve_lanes(lanes, lambda r: 0 if r.case.blocks[0]["n"][1] == 1 else 1, reqs, max_wall=args.serve_max_s)
     for lane in lanes:
         lane.close()
-    lat = np.array(sorted(r.finish - r.arrival for r in done))
-    span = max(r.finish for r in done) - min(r.arrival for r in reqs) if done else float("nan")
-    work = sum(r.case.n_interior * r.steps for r in done)
-    bad = [r.rid for r in done if r.error is not None or r.status.code != abi.MB_OK]
-    return {"cases_submitted": len(reqs), "cases_completed": len(done), "failed": bad,
-            "arrival_rate_per_s": args.serve_rate, "cases_per_s": len(done) / span if done else 0.0,
-            "p50_s": float(np.percentile(lat, 50)) if done else None,
-            "p99_s": float(np.percentile(lat, 99)) if done else None,
-            "cell_updates_per_s": work / span if done else 0.0, "makespan_s": span, "poll_steps": args.serve_poll,
-            "lanes": "2 (1-D cases | 2-D cases), one context and stream each",
-            "budget_gb": args.serve_budget_gb, "precision": "mixed", "setup_s": round(setup, 1),
-            "sample": "the first %d cases of the seeded 4096-case stream (half 1-D N in [256, 8192], half 2-D N^2 "
-                      "with N in [128, 1024], log-uniform), Poisson arrivals" % len(reqs)}
+    part = ([r.finish - r.arrival for r in done], min(r.arrival for r in reqs) if reqs else None,
+            max(r.finish for r in done) if done else None, sum(r.case.n_interior * r.steps for r in done), len(done),
+            [r.rid for r in done if r.error is not None or r.status.code != abi.MB_OK])
+    parts = [part]
+    if pg is not None:
+        parts = [None] * world
+        pg.all_gather_object(parts, part)
+    out = {"cases_submitted": len(reqs_all), **merge_serving(parts), "arrival_rate_per_s": args.serve_rate,
+           "poll_steps": args.serve_poll, "lanes": "2 (1-D cases | 2-D cases), one context and stream each",
+           "budget_gb": args.serve_budget_gb, "precision": "mixed", "setup_s": round(setup, 1),
+           "sample": "the first %d cases of the seeded 4096-case stream (half 1-D N in [256, 8192], half 2-D N^2 "
+                     "with N in [128, 1024], log-uniform), Poisson arrivals" % len(reqs_all)}
+    if world > 1:
+        out["partition"] = "request q on rank q mod %d, no exchange" % world
+    return out
 
 
 def run_reference(args):
@@ -347,7 +375,7 @@ def main():
     if args.workload in ("c3", "c5", "serving"):
         stream = torch.cuda.Stream(dev)
         r = {"c3": lambda: run_c3(args, dev, stream), "c5": lambda: run_c5(args, dev, stream),
-             "serving": lambda: run_serving(args, dev)}[args.workload]()
+             "serving": lambda: run_serving(args, dev, world, rank, pg)}[args.workload]()
         if rank == 0:
             print(json.dumps({"workload": args.workload, "n_gpus": world, **r}), flush=True)
         if pg is not None:
@@ -462,7 +490,7 @@ def main():
     forms.clear()
     torch.cuda.empty_cache()
     if args.workload == "default":
-        line["workloads"] = {"serving": run_serving(args, dev), "mb2d": run_c3(args, dev, torch.cuda.Stream(dev))}
+        line["workloads"] = {"serving": run_serving(args, dev, world, rank, pg), "mb2d": run_c3(args, dev, torch.cuda.Stream(dev))}
     if rank == 0 and world == 1 and not args.no_cpu:
         v, n, t = cpu_sample(case, min_seconds=10.0, max_steps=2)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",

@@ -1,6 +1,7 @@
 """The N > 1 path of bench.py on the CPU: two gloo ranks (the GPU run uses NCCL the same way). The replicas share
-nothing but the timing reductions: the job's time is the maximum over ranks, every rank passes the same barriers, and
-in the reference arm rank 0 alone works and prints while the other ranks exit 0 without work."""
+nothing but the timing reductions: the job's time is the maximum over ranks, every rank passes the same barriers, the
+serving cases are partitioned over the ranks and their summaries merged, and in the reference arm rank 0 alone works
+and prints while the other ranks exit 0 without work."""
 import io
 import os
 import socket
@@ -30,6 +31,12 @@ def _rank_main(rank, world, port, q):
     bench.barrier(pg, dev)
     out["max"] = bench.max_over_ranks(pg, 1.5 + rank, dev)            # per-rank times 1.5, 2.5 -> 2.5
     bench.barrier(pg, dev)
+    # serving: the cases partitioned over the ranks, every rank's part gathered and merged as bench does
+    mine = bench.partition_requests(list(range(10)), world, rank)
+    part = ([0.5 * (x + 1) for x in mine], 0.0 + rank, 10.0 + rank, 100 * len(mine), len(mine), [])
+    parts = [None] * world
+    pg.all_gather_object(parts, part)
+    out["mine"], out["merged"] = mine, bench.merge_serving(parts)
     # the reference arm: ranks other than 0 return at once without work or output
     if rank != 0:
         buf = io.StringIO()
@@ -57,6 +64,11 @@ def test_two_gloo_ranks_time_as_the_max_over_ranks():
     assert [d["world"] for d in res] == [2, 2]
     assert [d["max"] for d in res] == [2.5, 2.5]
     assert res[1]["ref_rc"] == 0 and res[1]["ref_out"] == ""
+    assert sorted(res[0]["mine"] + res[1]["mine"]) == list(range(10)) and not set(res[0]["mine"]) & set(res[1]["mine"])
+    m = res[0]["merged"]
+    assert m == res[1]["merged"]
+    assert m["cases_completed"] == 10 and m["makespan_s"] == 11.0 and m["p50_s"] == 2.75
+    assert m["cell_updates_per_s"] == 1000 / 11.0 and m["failed"] == []
 
 
 def test_single_process_needs_no_process_group():
