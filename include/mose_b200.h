@@ -319,15 +319,26 @@ int mb_get_status(mb_ctx* ctx, mb_status* st);
  * allowed during capture). Everything is caller-owned: P (the arena, ncell_total rows), the block's
  * padded dl and m, the FP64 cp, mu and k tables (rows tmin..tmax) on the device, the scheme (host
  * struct: cfl, vnn, prandtl, ndir, visc, dt_additive) and dt_out, one device double that receives
- * min(1e5, min of the local dt) as mb_dt computes it. The only scratch is a file-scope device array of
- * 65536 doubles (512 KB) of per-CTA partial minima, held by every GPU that loads the library until exit;
- * a block whose 32 x 8-cell (i, j) tiles exceed 65536 is rejected with MB_E_ARG. The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress), so make that first call before
- * any stream capture. Calls share the array: calls that overlap on the GPU (different streams, no
- * ordering between them) race and must not be issued. */
+ * min(1e5, min over the block's interior cells of the local dt).
+ * What it computes differs from mb_dt in two stated ways: the local dt is always the FP64 rule of the parity
+ * form (mb_dt of a mixed-precision context takes it in FP32), and the cfl-rise ramp is NOT applied (during the
+ * ramp, iteration iter < cfl_rise, the caller multiplies dt_out by iter / cfl_rise as mb_dt does).
+ * integration-variables = prec (intvar 2) takes its steps from the context's Ur field: MB_E_UNSUPPORTED.
+ * The only scratch is a file-scope device array of 65536 doubles (512 KB) of per-CTA partial minima, held by
+ * every GPU that loads the library until exit; a block whose 32 x 8-cell (i, j) tiles exceed 65536 is rejected
+ * with MB_E_ARG. The first call on a device looks up the array's device address (cudaGetSymbolAddress), so make
+ * that first call before any stream capture (a first call on a capturing stream returns MB_E_ARG). Calls share
+ * the array: calls that overlap on the GPU (different streams, no ordering between them) race and must not be
+ * issued. */
 int mb_dt_block_noalloc(const double* P, int64_t ncell_total, int64_t boff, const int32_t n[3], const double* dl,
                         const double* m, const double* cp, const double* mu, const double* k, int32_t tmin,
                         int32_t tmax, double wm, const mb_scheme* sc, double* dt_out, void* stream);
+
+/* The launch shape mb_dt_block_noalloc uses for a block of n[3] interior cells, without launching anything (a
+ * host-only query): the k chunk *kc (16 planes, doubled until one partial minimum per tile fits the 65536 of the
+ * static array) and the tile count *ntiles = ceil(n1/32) ceil(n2/8) ceil(n3/kc). MB_E_ARG when even one plane
+ * needs more than 65536 tiles. No counterpart in the reference. */
+int mb_dt_block_noalloc_tiles(const int32_t n[3], int32_t* kc, int32_t* ntiles);
 
 /* Batched cases (no counterpart in the reference, whose process runs one case): mb_init with
  * mesh->ngroups = G reserves G case clocks; the blocks of every case sit in one arena of ncell_total rows and

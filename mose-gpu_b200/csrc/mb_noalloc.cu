@@ -14,7 +14,9 @@
 // written by the same call first, so nothing needs clearing); pass 2, one CTA, folds the slots in a
 // fixed order and writes min(1e5, minimum) to the caller's output, as Compute_dt's dtglobal
 // (numerics/time/Mod_dt.f90:15-106; Mod_Explicit.f90:122). The local dt of a cell is cell_dt of
-// mb_engine.cuh, the same arithmetic as mb_dt. Built with --fmad=false like the FP64 form.
+// mb_engine.cuh, the FP64 arithmetic of mb_dt's parity form, whatever the scheme's precision (the mixed form's mb_dt
+// takes it in FP32), and the cfl-rise ramp is not applied: the caller multiplies by iter / cfl_rise during the ramp.
+// Built with --fmad=false like the FP64 form.
 #include <cstdio>
 #include <cstring>
 #include "../../include/mose_b200.h"
@@ -77,6 +79,29 @@ __global__ void __launch_bounds__(1024) k_dt_fold(const double* __restrict__ par
 
 }  // namespace
 
+// the tile decomposition of a block: 32 x 8 cells per (i, j) tile; the k chunk starts at 16 planes and doubles until
+// the partial minima (one per tile) fit the static array. Tile t covers i-tile t % ti, j-tile (t / ti) % tj and the
+// planes 1 + kc * (t / (ti * tj)) .. min(that + kc, n3 + 1) - 1.
+static int dt_tiles(const int32_t n[3], long long* ti, long long* tj, long long* kc, long long* ntiles) {
+  if (!n || n[0] < 1 || n[1] < 1 || n[2] < 1) return MB_E_ARG;
+  *ti = (n[0] + 31) / 32;
+  *tj = (n[1] + kTY - 1) / kTY;
+  if (*ti * *tj > kMaxPartials) return MB_E_ARG;
+  *kc = 16;
+  while (*ti * *tj * ((n[2] + *kc - 1) / *kc) > kMaxPartials) *kc *= 2;
+  *ntiles = *ti * *tj * ((n[2] + *kc - 1) / *kc);
+  return MB_OK;
+}
+
+extern "C" int mb_dt_block_noalloc_tiles(const int32_t n[3], int32_t* kc, int32_t* ntiles) {
+  long long ti, tj, k, nt;
+  const int rc = dt_tiles(n, &ti, &tj, &k, &nt);
+  if (rc != MB_OK) return rc;
+  if (kc) *kc = (int32_t)k;
+  if (ntiles) *ntiles = (int32_t)nt;
+  return MB_OK;
+}
+
 extern "C" int mb_dt_block_noalloc(const double* P, int64_t ncell_total, int64_t boff, const int32_t n[3],
                                    const double* dl, const double* m, const double* cp, const double* mu,
                                    const double* k, int32_t tmin, int32_t tmax, double wm, const mb_scheme* sc,
@@ -84,22 +109,34 @@ extern "C" int mb_dt_block_noalloc(const double* P, int64_t ncell_total, int64_t
   if (!P || !n || !dl || !m || !cp || !mu || !k || !sc || !dt_out) return MB_E_ARG;
   if (n[0] < 1 || n[1] < 1 || n[2] < 1 || tmax - tmin < 2 || ncell_total < 1 || boff < 0) return MB_E_ARG;
   if (sc->ndir < 1 || sc->ndir > 3) return MB_E_ARG;
+  // preconditioning takes its steps from the Ur field of the context (pseudo-acoustic speed): not served here
+  if (sc->intvar == 2) {
+    fprintf(stderr, "[mose_b200] mb_dt_block_noalloc: integration-variables = prec needs the Ur field of a context "
+                    "(mb_dt)\n");
+    return MB_E_UNSUPPORTED;
+  }
   const long long pi = n[0] + 2 * MB_GC, pj = n[1] + 2 * MB_GC, pk = n[2] + 2 * MB_GC;
   if (boff + pi * pj * pk > ncell_total) return MB_E_ARG;
-  // tiles: 32 x 8 cells per (i, j) tile; the k chunk grows so that the partial minima fit the array
-  const long long ti = (n[0] + 31) / 32, tj = (n[1] + kTY - 1) / kTY;
-  if (ti * tj > kMaxPartials) {
+  long long ti, tj, kc, nt;
+  if (dt_tiles(n, &ti, &tj, &kc, &nt) != MB_OK) {
     fprintf(stderr, "[mose_b200] mb_dt_block_noalloc: a %d x %d plane needs %lld partial minima, more than the "
                     "%d of its static scratch\n", n[0], n[1], ti * tj, kMaxPartials);
     return MB_E_ARG;
   }
-  long long kc = 16;
-  while (ti * tj * ((n[2] + kc - 1) / kc) > kMaxPartials) kc *= 2;
-  const int ntiles = (int)(ti * tj * ((n[2] + kc - 1) / kc));
+  const int ntiles = (int)nt;
+  cudaStream_t s = (cudaStream_t)stream;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MB_E_CUDA;
   if (!g_partials_addr[dev]) {
-    // set-up, once per device: the host name g_partials is only a stand-in for the device array
+    // set-up, once per device: the host name g_partials is only a stand-in for the device array. The look-up may
+    // not run inside a stream capture (it would fail or invalidate the capture), so a first call made while the
+    // stream is capturing is refused with a message
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+      fprintf(stderr, "[mose_b200] mb_dt_block_noalloc: the first call on a device sets up the device address of its "
+                      "scratch and cannot run while the stream is being captured; make one call before the capture\n");
+      return MB_E_ARG;
+    }
     void* a = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&a, g_partials);
     if (e != cudaSuccess || !a) {
@@ -134,7 +171,6 @@ extern "C" int mb_dt_block_noalloc(const double* P, int64_t ncell_total, int64_t
   b.dl = dl;
   b.m = m;
   for (int f = 0; f < 6; ++f) b.rmap[f] = -1;
-  cudaStream_t s = (cudaStream_t)stream;
   k_dt_partials<<<ntiles, 32 * kTY, 0, s>>>(p, b, P, (int)ti, (int)tj, (int)kc, g_partials_addr[dev]);
   k_dt_fold<<<1, 1024, 0, s>>>(g_partials_addr[dev], ntiles, dt_out);
   return cudaGetLastError() == cudaSuccess ? MB_OK : MB_E_CUDA;

@@ -36,11 +36,11 @@ def _bind():
 
 
 class Caller:
-    """The device inputs of one single-block case as a caller without an engine context would hold them."""
+    """The device inputs of one block of a case as a caller without an engine context would hold them."""
 
-    def __init__(self, torch, case):
+    def __init__(self, torch, case, blk=0):
         dev = torch.device("cuda", 0)
-        b = case.blocks[0]
+        b = case.blocks[blk]
         self.n = (C.c_int32 * 3)(*b["n"])
         self.boff = b["boff"]
         self.ncell = case.ncell
@@ -79,6 +79,36 @@ def test_dt_without_allocation_matches_mb_dt(torch_cuda):
     for got, want in calls:
         assert abs(got - want) <= TOL * want, (got, want)
     assert calls[0][0] != calls[2][0]
+
+
+def test_block_with_a_row_offset_in_a_multi_block_arena(torch_cuda):
+    """A block that does not start at row 0 (boff > 0) of an 8-block arena: the flow of the last block is made the
+    fastest, so the minimum step of the whole case lies there and mb_dt must equal that block's own minimum."""
+    f = _bind()
+    case = cs.taylor_green(n=16, blocks=2)            # 8 blocks of 8^3 cells in one arena
+    last = len(case.blocks) - 1
+    assert case.blocks[last]["boff"] > 0
+    P = np.array(case.P0, copy=True)
+    case.block_view(P, last)[1:4] *= 3.0              # Mach 0.3 in the last block, 0.1 elsewhere
+    e = engine.Engine(case)
+    e.set_state(P)
+    want = e.dt()
+    got = [Caller(torch_cuda, case, b).dt(f, e.P) for b in range(len(case.blocks))]
+    assert abs(got[last] - want) <= TOL * want, (got[last], want)
+    assert min(got) == got[last]
+    assert all(g > want * (1 + 1e-3) for g in got[:last])
+
+
+def test_cfl_rise_ramp_is_left_to_the_caller(torch_cuda):
+    """During the cfl-rise ramp mb_dt scales the minimum by iter / cfl_rise; this entry point returns the minimum
+    without the ramp (stated in the header), so the caller's product reproduces mb_dt."""
+    f = _bind()
+    sod = cs.riemann_1d(n=200)
+    sod.scheme["cfl_rise"] = 10
+    e = engine.Engine(sod)
+    c = Caller(torch_cuda, sod)
+    got, want = c.dt(f, e.P), e.dt()                  # first step: iter 1, factor 1 / 10
+    assert abs(got * (1.0 / 10.0) - want) <= TOL * want, (got, want)
 
 
 def test_oversized_block_is_rejected_before_any_launch(torch_cuda):
