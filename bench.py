@@ -183,6 +183,27 @@ def _err_norms(case, a, b):
     return err
 
 
+def accuracy_at_config_steps(case, dev, stream, local):
+    """The mixed form against both FP64 forms after the config's own step count (case.steps), each form on a fresh
+    engine from the initial field, graph-replayed steps."""
+    import torch
+    from mosegpu import abi
+    from mosegpu.engine import Engine
+    st = {}
+    for name, prec in (("fp64", abi.PREC_FP64), ("fp64_fast", abi.PREC_FP64_FAST), ("mixed", abi.PREC_MIXED)):
+        eng = Engine(case, precision=prec, device=local, stream=stream)
+        with torch.cuda.stream(stream):
+            eng.step(case.steps, graph=True)
+        torch.cuda.synchronize(dev)
+        if eng.status().code != 0 or eng.status().steps != case.steps:
+            raise RuntimeError("%s form did not complete %d steps" % (name, case.steps))
+        st[name] = eng.state()
+        eng.close()
+        del eng
+        torch.cuda.empty_cache()
+    return _err_norms(case, st["fp64"], st["mixed"]), _err_norms(case, st["fp64_fast"], st["mixed"])
+
+
 def run_fixed_steps(case, steps, warmup, dev, stream):
     """Both forms of one case for warmup + steps graph-replayed steps; device time of the timed steps
     (CUDA events on the launching stream), cell-updates/s, launches and the mixed-vs-FP64 error."""
@@ -387,7 +408,7 @@ def main():
     cells = case.n_interior
     stream = torch.cuda.Stream(dev)
     forms = {}
-    for name, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
+    for name, prec in (("fp64", abi.PREC_FP64), ("fp64_fast", abi.PREC_FP64_FAST), ("mixed", abi.PREC_MIXED)):
         eng = Engine(case, precision=prec, device=local, stream=stream)
         clk = Clocks(local)
         with torch.cuda.stream(stream):
@@ -415,29 +436,27 @@ def main():
             g_ms, s_ms = eng.profile_stage(2, 5)
         forms[name] = dict(eng=eng, ms=ms, launches=eng.launches - l0, clocks=clocks, sweep_ms=s_ms, ghost_ms=g_ms,
                            tuning={"k_chunk": tuning[0], "persistent": bool(tuning[1])})
-    # accuracy of the mixed form: both forms ran warmup + steps from the same initial field
-    torch.cuda.synchronize(dev)
-    a = forms["fp64"]["eng"].state()
-    b = forms["mixed"]["eng"].state()
-    m = case.interior_mask()
-    err = {}
-    for q, nm in enumerate(["rho", "u", "v", "w", "p"]):
-        x, y = b[q, m], a[q, m]
-        d = x - y
-        err[nm] = {"L1": float(np.abs(d).sum() / np.abs(y).sum()),
-                   "L2": float(np.sqrt((d * d).sum() / (y * y).sum())),
-                   "Linf": float(np.abs(d).max() / np.abs(y).max())}
+        if name != "mixed":                  # the mixed form's engine is kept for the e2e leg
+            eng.close()
+            forms[name]["eng"] = None
+            torch.cuda.empty_cache()
+    # accuracy of the mixed form at the config's step count (100), against the FP64 parity form (the oracle's
+    # arithmetic bit for bit, tests/test_gpu_fullsize_oracle.py) and the FP64 production form, from the same field
+    err, err_fast = accuracy_at_config_steps(case, dev, stream, local)
     l2_rho = err["rho"]["L2"]
     head = "mixed" if l2_rho <= 1e-5 else "fp64"
     f = forms[head]
     value = world * cells * args.steps / (f["ms"] * 1e-3)
     fp64_value = world * cells * args.steps / (forms["fp64"]["ms"] * 1e-3)
+    fast_value = world * cells * args.steps / (forms["fp64_fast"]["ms"] * 1e-3)
     mixed_value = world * cells * args.steps / (forms["mixed"]["ms"] * 1e-3)
 
     # e2e through the C ABI with host buffers: the initial field uploaded from pinned host memory, each step
     # driven by the reference-facing calls (begin_step, stage 1..3) with the status (dt, time, checks) read
     # back to the host, the final field downloaded to pinned host memory.
     eng = forms[head]["eng"]
+    if eng is None:
+        eng = forms[head]["eng"] = Engine(case, precision=abi.PREC_FP64, device=local, stream=stream)
     host_in = torch.from_numpy(case.P0).pin_memory()
     host_out = torch.empty_like(host_in).pin_memory()
     barrier(pg, dev)
@@ -472,21 +491,36 @@ def main():
                        (state_bytes / 1e6), "dt_rule": "additive", "setup_s": round(setup_s, 1)},
             "forms": {"fp64": {"value": fp64_value, "ms_per_step": forms["fp64"]["ms"] / args.steps,
                                "sweep_ms": forms["fp64"]["sweep_ms"], "ghost_ms": forms["fp64"]["ghost_ms"],
-                               "tuning": forms["fp64"]["tuning"], "clocks": forms["fp64"]["clocks"]},
+                               "tuning": forms["fp64"]["tuning"], "clocks": forms["fp64"]["clocks"],
+                               "build": "parity form: the reference's statements, no FMA (bit-identical to the oracle)"},
+                      "fp64_fast": {"value": fast_value, "ms_per_step": forms["fp64_fast"]["ms"] / args.steps,
+                                    "sweep_ms": forms["fp64_fast"]["sweep_ms"],
+                                    "ghost_ms": forms["fp64_fast"]["ghost_ms"], "tuning": forms["fp64_fast"]["tuning"],
+                                    "clocks": forms["fp64_fast"]["clocks"],
+                                    "build": "production form: FP64 values, simplified flux path, FMA (within the "
+                                             "1e-12 / 1e-9 gates of the oracle)"},
                       "mixed": {"value": mixed_value, "ms_per_step": forms["mixed"]["ms"] / args.steps,
                                 "sweep_ms": forms["mixed"]["sweep_ms"], "ghost_ms": forms["mixed"]["ghost_ms"],
-                                "tuning": forms["mixed"]["tuning"], "speedup_vs_fp64": mixed_value / fp64_value},
-                      "mixed_vs_fp64_error_after_%d_steps" % (args.steps + args.warmup): err},
+                                "tuning": forms["mixed"]["tuning"], "speedup_vs_fp64": mixed_value / fp64_value,
+                                "speedup_vs_fp64_fast": mixed_value / fast_value,
+                                "speedup_vs_faster_fp64": mixed_value / max(fp64_value, fast_value)},
+                      "mixed_vs_fp64_error_after_%d_steps" % case.steps: err,
+                      "mixed_vs_fp64_fast_error_after_%d_steps" % case.steps: err_fast},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": tr, "peak_source": peak_kind,
                          "kernel": "k_sweep<%s> (stage 2)" % ("float" if head == "mixed" else "double"),
                          "algorithmic_bytes_per_launch": bytes_launch},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
                     "d2h_bytes_per_step": state_bytes / args.steps + 48,
+                    "copies": "once per run: the state is uploaded before the first step and downloaded after the "
+                              "last (the per-step bytes are those copies divided by the steps), as the reference's "
+                              "host loop keeps the field on the device between output iterations "
+                              "(Mod_Explicit.f90:300-305); the status (dt, time, checks) is read every step",
                     "path": "C ABI: upload once, per step mb_begin_step + 3 x mb_stage + mb_get_status, download"},
             "gpu_launches": f["launches"], "clocks": f["clocks"]}
     for fm in forms.values():
-        fm["eng"].close()
+        if fm["eng"] is not None:
+            fm["eng"].close()
     forms.clear()
     torch.cuda.empty_cache()
     if args.workload == "default":

@@ -109,6 +109,11 @@ static inline int mb_effective_sensor(int riemann, int sensor) {
 #define MB_PREC_FP64 0
 #define MB_PREC_MIXED 1 /* reconstruction + Riemann + viscous flux arithmetic in FP32; state,
                            RK accumulation, T/p recovery and dt in FP64 */
+#define MB_PREC_FP64_FAST 2 /* the FP64 production form: every value FP64 as in MB_PREC_FP64, but the flux path of the
+                               mixed form (single-species identities applied exactly, van Albada as one quotient, net
+                               face fluxes, reciprocals in the state update) built with FMA contraction. It meets the
+                               parity gates against the reference's statement order (1e-12 relative after one step,
+                               1e-9 after many) without being bit-identical to it; MB_PREC_FP64 is the bit-parity form */
 
 /* One block: interior extents, row offset in the arena, geometry (device pointers). */
 typedef struct mb_block {

@@ -2,6 +2,8 @@
 
   mb_f64.cu, mb_irs.cu, mb_prec.cu, mb_api.cu, mb_noalloc.cu, mb_sweep_f64_*.cu   --fmad=false
       (the FP64 form rounds statement by statement as written)
+  mb_sweep_f64f_*.cu  --fmad=true
+      (the FP64 production form: FMA contraction; FP64 division and square root stay IEEE)
   mb_sweep_f32_*.cu   --fmad=true -prec-div=false -prec-sqrt=false -ftz=true
       (the mixed form: FP32 flux arithmetic with FMA and the fast FP32 divide / square root; the FP64 state
        arithmetic in those units is unaffected by these single-precision options)
@@ -21,9 +23,11 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-lineinfo", "-Xptxas", "-v"]
 F64 = ["--fmad=false"]
+F64F = ["--fmad=true"]
 F32 = ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
 UNITS = [("mb_f64.cu", F64), ("mb_irs.cu", F64), ("mb_prec.cu", F64), ("mb_api.cu", F64), ("mb_noalloc.cu", F64)] + \
         [("mb_sweep_f64_rs%d.cu" % r, F64) for r in (0, 1, 4, 12)] + \
+        [("mb_sweep_f64f_rs%d.cu" % r, F64F) for r in (0, 1, 4, 12)] + \
         [("mb_sweep_f32_rs%d.cu" % r, F32) for r in (0, 1, 4, 12)]
 DEPS = ["mb_physics.cuh", "mb_engine.cuh", "mb_launch.h", "mb_sweep_inst.inc",
         os.path.join("..", "..", "include", "mose_b200.h")]

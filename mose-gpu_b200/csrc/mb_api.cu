@@ -592,7 +592,8 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   if (sc->limiter < 1 || sc->limiter > 6) return MB_E_UNSUPPORTED;
   if (sc->n_rk < 1 || sc->n_rk > 4) return MB_E_UNSUPPORTED;
   if (!(sc->res_stop >= 0.0)) return MB_E_ARG;
-  if (sc->precision != MB_PREC_FP64 && sc->precision != MB_PREC_MIXED) return MB_E_UNSUPPORTED;
+  if (sc->precision != MB_PREC_FP64 && sc->precision != MB_PREC_MIXED && sc->precision != MB_PREC_FP64_FAST)
+    return MB_E_UNSUPPORTED;
   if (sc->ndir < 1 || sc->ndir > 3) return MB_E_ARG;
   if (th->tmax - th->tmin < 2 || !th->cp || !th->h || !th->mu || !th->k) return MB_E_ARG;
   const int ngroups = mesh->ngroups > 0 ? mesh->ngroups : 1;
@@ -671,8 +672,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
     if (cudaMemset(c->d_acc4, 0, (size_t)c->ncell * MB_NPRIM * sizeof(double)) != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
   }
   {
-    cudaError_t e = (sc->precision == MB_PREC_MIXED)
-                        ? MB_BY_RS(f32, sweep_unit(sc), _setup, ()) : MB_BY_RS(f64, sweep_unit(sc), _setup, ());
+    cudaError_t e = MB_BY_FORM(sc->precision, sweep_unit(sc), _setup, ());
     if (e != cudaSuccess) { free_ctx(c); return MB_E_CUDA; }
   }
   // ---- kernel parameters
@@ -703,8 +703,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
     const int v = sc->visc ? 1 : 0;
-    int occ = (sc->precision == MB_PREC_MIXED)
-                  ? MB_BY_RS(f32, sweep_unit(sc), _occupancy, (v)) : MB_BY_RS(f64, sweep_unit(sc), _occupancy, (v));
+    int occ = MB_BY_FORM(sc->precision, sweep_unit(sc), _occupancy, (v));
     p.pgrid = std::max(1, occ) * std::max(1, nsm);
   }
   p.queue = nullptr;
@@ -712,10 +711,10 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   TRY(build_tables(c, mesh));
   if (getenv("MB_REPORT")) {
     const int v = sc->visc ? 1 : 0;
-    int occ = (sc->precision == MB_PREC_MIXED)
-                  ? MB_BY_RS(f32, sweep_unit(sc), _occupancy, (v)) : MB_BY_RS(f64, sweep_unit(sc), _occupancy, (v));
+    int occ = MB_BY_FORM(sc->precision, sweep_unit(sc), _occupancy, (v));
     fprintf(stderr, "[mose_b200] sweep: %s, %d threads per CTA, %d CTAs per SM, %d tiles\n",
-            sc->precision == MB_PREC_MIXED ? "mixed" : "fp64", 32 * c->ty_sweep, occ, c->ntiles_sweep);
+            sc->precision == MB_PREC_MIXED ? "mixed" : (sc->precision == MB_PREC_FP64_FAST ? "fp64 fast" : "fp64"),
+            32 * c->ty_sweep, occ, c->ntiles_sweep);
   }
 #undef TRY
   *out = c;
@@ -757,8 +756,9 @@ int mb_group_reset(mb_ctx* ctx, int g, const mb_group* spec, const double* P, vo
   CK(cudaSetDevice(ctx->device));
   cudaStream_t s = (cudaStream_t)stream;
   CK(group_reset(ctx->p, g, spec->time_clip, spec->t_end, spec->res_stop, s));
-  CK(ctx->sc.precision == MB_PREC_MIXED ? sweep_f32_rs1_dt(ctx->p, ctx->d_tiles_aux, ctx->ntiles_aux, P, g, s)
-                                         : dt_cells(ctx->p, ctx->d_tiles_aux, ctx->ntiles_aux, P, s, g));
+  CK(ctx->sc.precision == MB_PREC_MIXED       ? sweep_f32_rs1_dt(ctx->p, ctx->d_tiles_aux, ctx->ntiles_aux, P, g, s)
+     : ctx->sc.precision == MB_PREC_FP64_FAST ? sweep_f64f_rs1_dt(ctx->p, ctx->d_tiles_aux, ctx->ntiles_aux, P, g, s)
+                                              : dt_cells(ctx->p, ctx->d_tiles_aux, ctx->ntiles_aux, P, s, g));
   ctx->launches += 2;
   return MB_OK;
 }
@@ -813,11 +813,7 @@ static int sweep_on(mb_ctx* c, const DTile* t, int n, int persistent, int mode, 
   p.queue = persistent ? c->d_queue : nullptr;
   const double rkc = irk > 0 ? rkc_of(c->sc.n_rk, irk) : 0.0;
   cudaError_t e;
-  if (c->sc.precision == MB_PREC_MIXED) {
-    e = MB_BY_RS(f32, sweep_unit(&c->sc), , (p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s));
-  } else {
-    e = MB_BY_RS(f64, sweep_unit(&c->sc), , (p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s));
-  }
+  e = MB_BY_FORM(c->sc.precision, sweep_unit(&c->sc), , (p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s));
   c->launches += 1;
   CK(e);
   return MB_OK;
@@ -828,11 +824,7 @@ static int records(mb_ctx* c, const double* Pin, cudaStream_t s) {
   if (c->nrec <= 0) return MB_OK;
   const Params& p = c->p;
   cudaError_t e;
-  if (c->sc.precision == MB_PREC_MIXED) {
-    e = MB_BY_RS(f32, sweep_unit(&c->sc), _records, (p, c->d_brec, c->d_bcell, c->nrec, Pin, s));
-  } else {
-    e = MB_BY_RS(f64, sweep_unit(&c->sc), _records, (p, c->d_brec, c->d_bcell, c->nrec, Pin, s));
-  }
+  e = MB_BY_FORM(c->sc.precision, sweep_unit(&c->sc), _records, (p, c->d_brec, c->d_bcell, c->nrec, Pin, s));
   c->launches += 1;
   CK(e);
   return MB_OK;
@@ -966,8 +958,9 @@ static int dt_min(mb_ctx* c, const double* P, cudaStream_t s) {
     return MB_OK;
   }
   CK(reset_dt(c->p, s));
-  CK(c->sc.precision == MB_PREC_MIXED ? sweep_f32_rs1_dt(c->p, c->d_tiles_aux, c->ntiles_aux, P, -1, s)
-                                       : dt_cells(c->p, c->d_tiles_aux, c->ntiles_aux, P, s));
+  CK(c->sc.precision == MB_PREC_MIXED       ? sweep_f32_rs1_dt(c->p, c->d_tiles_aux, c->ntiles_aux, P, -1, s)
+     : c->sc.precision == MB_PREC_FP64_FAST ? sweep_f64f_rs1_dt(c->p, c->d_tiles_aux, c->ntiles_aux, P, -1, s)
+                                            : dt_cells(c->p, c->d_tiles_aux, c->ntiles_aux, P, s));
   c->launches += 2;
   return MB_OK;
 }

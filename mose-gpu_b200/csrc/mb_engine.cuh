@@ -920,7 +920,8 @@ MB_HD void bc_record(const Params& p, const DBlk& b, const double* __restrict__ 
 // Every boundary record of the mesh, one thread each, from the stage input P (ghosts filled): the contributions
 // (A, S) of record q go to recflux[q][0..9] in the flux type; the sweep adds them in face order after the interior
 // sum (BC_Fluxes after Fluxes, Mod_Explicit.f90:187-189).
-template <typename R, bool VISC, int RS, int LIM>
+// VAR tells apart the instantiations of the same types built with different flags (the FP64 production form's units)
+template <typename R, bool VISC, int RS, int LIM, int VAR = 0>
 __global__ void __launch_bounds__(128) k_records(Params p, const int* __restrict__ brec, const int* __restrict__ bcell,
                                                int nrec, const double* __restrict__ P) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1278,7 +1279,7 @@ __device__ __forceinline__ void cta_min_dt(DevState* st, double v, double* sred)
 // ---- Compute_dt alone: the local dt of every interior cell in the form's arithmetic (FP64; FP32 for the mixed
 // form, as its fused dt), reduced into the case's clock. only_group >= 0: the cells of that case only (its first
 // dt after mb_group_reset). Tiles of 32 x TY_AUX cells (8 rows).
-template <typename R>
+template <typename R, int VAR = 0>
 __global__ void __launch_bounds__(256) k_dt_t(Params p, const DTile* __restrict__ tiles, const double* P,
                                              int only_group) {
   __shared__ double sred[32];
@@ -1544,7 +1545,7 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
 // work queue: a grid of about one wave of CTAs, each taking the next tile from the counter p.queue (zeroed
 // before the launch) until the list is exhausted. MINB: resident CTAs per SM the register allocation must
 // allow (launch bounds).
-template <typename R, int TY, bool VISC, int MODE, int RS, int LIM, int MINB, bool KM = false>
+template <typename R, int TY, bool VISC, int MODE, int RS, int LIM, int MINB, bool KM = false, int VAR = 0>
 __global__ void __launch_bounds__(32 * TY, MINB)
 k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pin, const double* Pold, double* Pout,
         double* Rout, double rkc, int last) {

@@ -58,8 +58,17 @@ MB_DECLARE_SWEEP(sweep_f32_rs4)
 MB_DECLARE_SWEEP(sweep_f32_rs12)
 MB_DECLARE_SWEEP(sweep_f64_rs0)
 MB_DECLARE_SWEEP(sweep_f32_rs0)
+// the FP64 production form: the simplified flux path in FP64, built with FMA contraction
+MB_DECLARE_SWEEP(sweep_f64f_rs1)
+MB_DECLARE_SWEEP(sweep_f64f_rs4)
+MB_DECLARE_SWEEP(sweep_f64f_rs12)
+MB_DECLARE_SWEEP(sweep_f64f_rs0)
 // the sweep unit of a Riemann solver id: one unit per benchmarked solver (the id a compile-time constant there), the
 // rs0 units (the id read at run time) for the others
+// the unit of the scheme's precision form (MB_PREC_MIXED: f32, MB_PREC_FP64_FAST: f64f, MB_PREC_FP64: f64)
+#define MB_BY_FORM(prec, rs, fn, args)                                                                     \
+  ((prec) == MB_PREC_MIXED ? MB_BY_RS(f32, rs, fn, args)                                                  \
+                           : (prec) == MB_PREC_FP64_FAST ? MB_BY_RS(f64f, rs, fn, args) : MB_BY_RS(f64, rs, fn, args))
 #define MB_BY_RS(form, rs, fn, args)                                                                        \
   ((rs) == 1 ? sweep_##form##_rs1##fn args                                                                  \
              : (rs) == 4 ? sweep_##form##_rs4##fn args : (rs) == 12 ? sweep_##form##_rs12##fn args : sweep_##form##_rs0##fn args)

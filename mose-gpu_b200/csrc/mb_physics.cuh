@@ -127,7 +127,13 @@ struct Params {
 // exactly: rho = rho_s, Y = rho_s / rho = 1, R_mix = Ri, cp_mix = cp(T), h_mix = h(T), the Wilke mixture
 // viscosity / conductivity = the table values, and a zero species-diffusion flux. The FP64 form keeps the
 // literal statements (their rounding is what the parity gate compares).
-template <typename R> struct Fast { static constexpr bool on = sizeof(R) == 4; };
+// The algebraically simplified flux path (single-species identities, one-quotient van Albada, net face fluxes, the
+// reciprocal state update): the mixed form's FP32 arithmetic, and the FP64 production form's (its translation units
+// define MB_FAST64 = 1 and are built with FMA contraction). The FP64 parity form keeps the reference's statements.
+#ifndef MB_FAST64
+#define MB_FAST64 0
+#endif
+template <typename R> struct Fast { static constexpr bool on = sizeof(R) == 4 || MB_FAST64; };
 
 template <typename R> struct Tab;
 template <> struct Tab<double> {

@@ -46,6 +46,7 @@ RS_AUSMPM, RS_HLLEPP, RS_HLLC_TRAMEL, RS_HLLC_CHEN = 5, 6, 7, 10
 SENSOR_DEFAULT, SENSOR_TRAMEL, SENSOR_CHEN, SENSOR_NONE = 0, 1, 2, 3
 INTVAR_CONS, INTVAR_PRIM, INTVAR_PREC = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64_FAST = 2   # FP64 values, the simplified flux path with FMA (the gates, not bit parity)
 
 
 class MBBlock(C.Structure):

@@ -90,6 +90,28 @@ def test_one_step_and_many(torch_cuda, cid, builder, graph):
     assert abs(sg.time - so.time) <= 1e-12 * so.time
 
 
+@pytest.mark.parametrize("cid,builder", H.small_cases(), ids=[c[0] for c in H.small_cases()])
+def test_fp64_production_form_within_the_gates(torch_cuda, cid, builder):
+    """The FP64 production form (FP64 values, the simplified flux path with FMA contraction) against the oracle at
+    the north-star gates: 1e-12 after one step, 1e-9 after 16 (not bit for bit: FMA and the reordered formulas)."""
+    import oracle
+    from mosegpu.engine import Engine
+    case = builder()
+    eng, orc = Engine(case, precision=abi.PREC_FP64_FAST), oracle.Oracle(case)
+    P = case.P0.copy()
+    assert orc.step(P, 1) == 0
+    eng.step(1, graph=True)
+    e1 = H.rel_err(H.conserved(case, eng.state()), H.conserved(case, P))
+    assert np.all(e1 <= TOL_ONE), ("one step", e1)
+    assert orc.step(P, 15) == 0
+    eng.step(15, graph=True)
+    en = H.rel_err(H.conserved(case, eng.state()), H.conserved(case, P))
+    assert np.all(en <= TOL_MANY), ("16 steps", en)
+    so, sg = orc.status(), eng.status()
+    assert sg.code == 0 and sg.steps == so.steps
+    assert abs(sg.time - so.time) <= 1e-11 * so.time
+
+
 def test_stage_by_stage_matches_fused(torch_cuda):
     """begin_step + stage(1..n) (the reference's call sequence) equals the fused mb_step."""
     from mosegpu import case as cs
