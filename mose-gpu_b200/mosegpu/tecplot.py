@@ -14,7 +14,10 @@ variables of its interior cells and the temperature `T = EOS(p, rho, Rtot) = p /
   so every value starts a new record)
 
 Cell-centred variables and no ghost layer are MOSE's settings (`IOfield%tec%node = .false.`, `%bc = .false.`,
-IO_Solution.f90:409-418). The optional "thermo" and "transport" variables are not written.
+IO_Solution.f90:409-418). The "thermo" variables are MOSE's default (`sol-variables = thermo`, IO_Solution.f90:128):
+after T come "g" = f_gamma = cp / (cp - Rtot), cp from the 1 K table at T (f_cp, Lib_ThermoTransport.f90:273-293,
+329-339; the row idint(T), no clamp), and "R" = Rtot (IO_Solution.f90:384-389,536-539); `variables=""` writes T only
+(`sol-variables` without "thermo"). The optional "transport" variables are not written.
 
 `fortran_e23_15e3(x)` restates Fortran's Ew.dEe editing for w = 23, d = 15, e = 3: the mantissa 0.d1...d15 with the
 value rounded to 15 significant digits (nearest), a 3-digit signed exponent, right-justified in 23 characters
@@ -62,9 +65,25 @@ def temperature(case, rho, p):
     return p / (rho * rtot)
 
 
-def write_tecplot_ascii(path, case, P, time):
+def gamma_rtot(case, rho, p):
+    """g and R of write_vtk_tec's "thermo" variables: Rtot = 0 + Ri rho / rho, T = p / (Rtot rho), cp = 0 + rho / rho
+    (cp(int T) + (cp(int T + 1) - cp(int T)) (T - int T)), g = cp / (cp - Rtot), in that order (one species)."""
+    th = case.thermo
+    ri = RUNIV / th["wm"]
+    rtot = 0.0 + (ri * rho) / rho
+    T = p / (rtot * rho)
+    ti = np.trunc(T).astype(np.int64)
+    td = T - ti
+    cpt = th["cp"]
+    c1, c2 = cpt[ti - th["tmin"]], cpt[ti + 1 - th["tmin"]]
+    cp = 0.0 + (rho / rho) * (c1 + (c2 - c1) * td)
+    return cp / (cp - rtot), rtot
+
+
+def write_tecplot_ascii(path, case, P, time, variables="thermo"):
     """Writes the Tecplot ASCII solution file of `case` from the state `P (5, ncell)` (host, float64) at `time`
-    (negative for a steady run: the zone then carries |time| and STRANDID = 0, Lib_Tecplot.f90:127-131,318-319)."""
+    (negative for a steady run: the zone then carries |time| and STRANDID = 0, Lib_Tecplot.f90:127-131,318-319).
+    variables: "thermo" (MOSE's default: T, g, R after the primitives) or "" (T only)."""
     P = np.asarray(P, dtype=np.float64)
     if P.shape != (5, case.ncell):
         raise ValueError(f"state of shape {P.shape}, expected {(5, case.ncell)}")
@@ -73,12 +92,14 @@ def write_tecplot_ascii(path, case, P, time):
     time_accurate = time >= 0
     t = abs(float(time))
     tstr = fortran_e23_15e3(t)[1:]            # str(no_sign=.true.): drop the sign position
+    thermo = "thermo" in variables
+    nvt = 3 + 6 + (2 if thermo else 0)
     with open(path, "w") as f:
-        f.write(' VARIABLES ="x" "y" "z" "rho(1)" "u" "v" "w" "p" "T"\n')
+        f.write(' VARIABLES ="x" "y" "z" "rho(1)" "u" "v" "w" "p" "T"' + (' "g" "R"' if thermo else "") + "\n")
         for b in range(len(case.blocks)):
             n1, n2, n3 = case.blocks[b]["n"]
             zone = (f" ZONE  T = Block{b + 1}, I={_int(n1 + 1)}, J={_int(n2 + 1)}, K={_int(n3 + 1)}, DATAPACKING=BLOCK"
-                    f", VARLOCATION=([1-3]=NODAL,[4-9]=CELLCENTERED), SOLUTIONTIME={tstr}")
+                    f", VARLOCATION=([1-3]=NODAL,[4-{nvt}]=CELLCENTERED), SOLUTIONTIME={tstr}")
             if not time_accurate:
                 zone += ", STRANDID = 0"
             f.write(zone + "\n")
@@ -89,6 +110,10 @@ def write_tecplot_ascii(path, case, P, time):
             for s in range(5):
                 f.write(_lines(v[s].ravel(order="F")))
             f.write(_lines(temperature(case, v[0], v[4]).ravel(order="F")))
+            if thermo:
+                g, r = gamma_rtot(case, v[0], v[4])
+                f.write(_lines(g.ravel(order="F")))
+                f.write(_lines(r.ravel(order="F")))
 
 
 def _zone_fields(text):

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from mosegpu import case as cs
-from mosegpu.tecplot import fortran_e23_15e3, temperature, write_tecplot_ascii
+from mosegpu.tecplot import fortran_e23_15e3, gamma_rtot, temperature, write_tecplot_ascii
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "orion_tecplot_lines.txt")
 
@@ -57,12 +57,12 @@ def test_written_case_layout_and_values(tmp_path):
     path = tmp_path / "field.tec"
     write_tecplot_ascii(path, c, P, 0.0123)
     L = _read(path)
-    assert L[0] == ' VARIABLES ="x" "y" "z" "rho(1)" "u" "v" "w" "p" "T"'
+    assert L[0] == ' VARIABLES ="x" "y" "z" "rho(1)" "u" "v" "w" "p" "T" "g" "R"'
     q = 1
     for b in range(len(c.blocks)):
         n1, n2, n3 = c.blocks[b]["n"]
         assert L[q] == (f" ZONE  T = Block{b + 1}, I={n1 + 1}, J={n2 + 1}, K={n3 + 1}, DATAPACKING=BLOCK, "
-                        f"VARLOCATION=([1-3]=NODAL,[4-9]=CELLCENTERED), SOLUTIONTIME=0.123000000000000E-001")
+                        f"VARLOCATION=([1-3]=NODAL,[4-11]=CELLCENTERED), SOLUTIONTIME=0.123000000000000E-001")
         q += 1
         nn, nc = (n1 + 1) * (n2 + 1) * (n3 + 1), n1 * n2 * n3
         X = c.nodes(b)
@@ -71,7 +71,9 @@ def test_written_case_layout_and_values(tmp_path):
             assert np.allclose(got, X[..., d].ravel(order="F"), rtol=1e-14, atol=1e-300)
             q += nn
         v = c.interior(P, b)
-        want = [v[s] for s in range(5)] + [temperature(c, v[0], v[4])]
+        g, r = gamma_rtot(c, v[0], v[4])
+        want = [v[s] for s in range(5)] + [temperature(c, v[0], v[4]), g, r]
+        assert np.allclose(g, c.thermo["gamma"], rtol=1e-12) and np.allclose(r, c.thermo["R"], rtol=1e-15)
         for w in want:
             got = np.array([float(x) for x in L[q:q + nc]])
             assert np.allclose(got, w.ravel(order="F"), rtol=1e-14, atol=0)
