@@ -118,7 +118,11 @@ static inline int mb_effective_sensor(int riemann, int sensor) {
 /* One block: interior extents, row offset in the arena, geometry (device pointers). */
 typedef struct mb_block {
   int32_t n[3];      /* interior cells n1, n2, n3 (blk%dim) */
-  int32_t group;     /* the independent case (time step, clock, status) the block belongs to: 0 .. ngroups-1 */
+  int32_t group;     /* the independent case (time step, clock, status) the block belongs to: 0 .. ngroups-1;
+                        -1: an external block, the local copy of a block another rank owns when the blocks are
+                        partitioned over GPUs: its rows hold the donor cells the halo exchange writes (mb_unpack_rows),
+                        the connection records of the local blocks may name it as donor, and nothing is computed on
+                        it (no tiles, records, ghost fill, time step or status); it carries no records itself */
   int64_t boff;      /* 0-based first row of the padded block in P_flat (field_block_index_params) */
   const double* fm1; /* (4, 0:n1, n2, n3): nx, ny, nz, area of the i-faces */
   const double* fm2; /* (4, n1, 0:n2, n3) */
@@ -314,6 +318,40 @@ int mb_begin_step(mb_ctx* ctx, const double* P, void* stream);
 int mb_profile_stage(mb_ctx* ctx, double* P, double* PO, int irk, int nrep, float* ms_ghost, float* ms_sweep,
                      void* stream);
 
+/* ---- Blocks partitioned over several GPUs (one process and context per GPU; the reference's MPI decomposition by
+ * blocks, src/lib/parallel/Mod_MPI.f90:147-258 and the halo exchange of Mod_GhostExchange.f90:217-383,685-957).
+ * Each rank's mesh holds its own blocks and, as external blocks (group -1), copies of the remote donor blocks of its
+ * connection records. A step is then
+ *   mb_step_prepare -> MIN all-reduce of the clock's minimum local step (mb_copy_dtmin out, all-reduce, back in;
+ *   mpi_allreduce_min_r8 of Mod_MPI.f90:571-581) -> mb_step_start -> per stage:
+ *   halo rows of the donors' interior cells (mb_pack_rows on the owner, mb_unpack_rows into the external block)
+ *   -> mb_stage_begin (ghost fill of the stage input) -> for Navier-Stokes, the donor rows the viscous connection
+ *   records read, after the owners' own ghost fill -> mb_stage_end (records, sweep, update).
+ * mb_begin_step = mb_step_prepare + mb_step_start and mb_stage = mb_stage_begin + mb_stage_end on one rank. */
+
+/* Makes the minimum local step of P available in the case clocks (Compute_dt over this context's blocks; nothing
+ * to do when the last stage of the previous step computed it). No host synchronisation. */
+int mb_step_prepare(mb_ctx* ctx, const double* P, void* stream);
+
+/* Copies case g's minimum local step between its clock and a caller device buffer of 8 bytes, ordered on `stream`:
+ * to_clock = 0 clock -> buf, 1 buf -> clock. The value is the IEEE bit pattern of a positive double, so an integer
+ * MIN all-reduce of the 64-bit patterns (signed or unsigned) is the MIN of the steps. */
+int mb_copy_dtmin(mb_ctx* ctx, int g, void* buf, int to_clock, void* stream);
+
+/* Starts the step on every case clock from the minimum in the clock (the ramp, the clip onto t_end, time and step
+ * count, Set_Global_dt + Clip_dt_To_Timemax). */
+int mb_step_start(mb_ctx* ctx, void* stream);
+
+/* Stage irk split at the halo exchange point: mb_stage_begin fills the ghosts of the stage input (Fill_Ghost_Cell),
+ * mb_stage_end computes the boundary records and runs the fused sweep and update. */
+int mb_stage_begin(mb_ctx* ctx, double* P, double* PO, int irk, void* stream);
+int mb_stage_end(mb_ctx* ctx, double* P, double* PO, int irk, void* stream);
+
+/* Halo rows of a partitioned mesh: buf[v * n + q] = P[rows[q] + v * ncell] (pack) and its inverse (unpack), for the
+ * five primitive variables v; rows (int64) and buf are device arrays. Ordered on `stream`; no context needed. */
+int mb_pack_rows(const double* P, int64_t ncell, const int64_t* rows, int32_t n, double* buf, void* stream);
+int mb_unpack_rows(double* P, int64_t ncell, const int64_t* rows, int32_t n, const double* buf, void* stream);
+
 /* Status of case 0 (state check, thermo guard, first offender, simulated time, last dt). Synchronises. */
 int mb_get_status(mb_ctx* ctx, mb_status* st);
 
@@ -381,6 +419,14 @@ int mb_set_tuning(mb_ctx* ctx, int kchunk, int persistent);
 
 /* The configuration chosen by mb_autotune (k-chunk 16 and the plain grid before any call) and its sweep time. */
 int mb_get_tuning(const mb_ctx* ctx, int* kchunk, int* persistent, float* ms);
+
+/* How the mixed form's sweep launches of this context staged their state tiles (no counterpart in the reference):
+ * *tma_sweeps by TMA (cp.async.bulk.tensor boxes of 38 rows x 5 variables of the state arena into shared memory,
+ * completing on an mbarrier), *plain_sweeps by per-thread loads (the state buffer not 16-byte aligned, an odd
+ * ncell_total, no tensor map made yet during a capture, or MB_NO_TMA set in the environment at mb_init). Both
+ * paths give the same tile values, so the results do not depend on it. Launches recorded into a CUDA graph count
+ * once, at capture. */
+int mb_get_staging(const mb_ctx* ctx, int64_t* tma_sweeps, int64_t* plain_sweeps);
 
 /* Number of kernel launches this context has issued (for launch accounting). */
 int64_t mb_launch_count(const mb_ctx* ctx);

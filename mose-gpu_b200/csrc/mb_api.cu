@@ -9,6 +9,7 @@
 #include <unordered_map>
 #include <algorithm>
 #include "../../include/mose_b200.h"
+#include <cudaTypedefs.h>  // CUtensorMap and the driver's tensor-map encoder type (taken at run time, no -lcuda)
 #include "mb_launch.h"
 
 using namespace mb;
@@ -54,6 +55,12 @@ struct mb_ctx {
   DTile* d_tiles_aux = nullptr;
   int ntiles_aux = 0;
   double* d_scratch = nullptr;  // the engine's own stage buffer (ncell x 5)
+  // TMA tensor maps of the state buffers the mixed sweep stages from: (buffer, its row count) -> a CUtensorMap in
+  // device memory; made outside any capture, never rewritten (a captured step keeps pointing at its maps)
+  struct Tmap { const double* ptr; long long nc; void* dev; };
+  std::vector<Tmap> tmaps;
+  bool no_tma = false;          // MB_NO_TMA set at mb_init: the scalar staging path (same tile values)
+  long long sweeps_tma = 0, sweeps_plain = 0;  // sweep launches of the mixed form by staging path
   double* d_acc4 = nullptr;     // RK4: conserved accumulator (ncell x 5)
   double* d_irs = nullptr;      // residual smoothing: two residual buffers (2 x ncell x 5)
   long long* d_idst = nullptr;  // its first-ghost-layer copies, direction by direction: row idst[e] <- row isrc[e]
@@ -96,6 +103,8 @@ static int upload(T** dst, const T* src, size_t n) {
 
 static void free_ctx(mb_ctx* c) {
   if (!c) return;
+  for (auto& m : c->tmaps) cudaFree(m.dev);
+  c->tmaps.clear();
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   if (c->graph) cudaGraphDestroy(c->graph);
   void* ptrs[] = {c->d_blk, c->d_recmap, c->d_rec, c->d_grec, c->d_phys, c->d_cubic, c->d_cdst, c->d_csrc,
@@ -119,6 +128,7 @@ static std::vector<DTile> make_tiles(const std::vector<int>& dims, int ty, int k
     const int* n = &dims[3 * b];
     const int cls = n[2] > 1 ? 3 : (n[1] > 1 ? 2 : 1);
     if (!(mask & (1 << cls))) continue;
+    if (km && (*km)[b] < 0) continue;  // an external block: nothing is computed on it
     if (km && km_sel >= 0 && (*km)[b] != km_sel) continue;
     for (int k0 = 1; k0 <= n[2]; k0 += kc)
       for (int j0 = 1; j0 <= n[1]; j0 += ty)
@@ -160,6 +170,13 @@ static void stage_buffers(int n, int irk, double* P, double* PO, double* S, cons
 extern "C" {
 
 const char* mb_version(void) { return "mose_b200 0.1 (sm_100a)"; }
+
+int mb_get_staging(const mb_ctx* ctx, int64_t* tma_sweeps, int64_t* plain_sweeps) {
+  if (!ctx || !tma_sweeps || !plain_sweeps) return MB_E_ARG;
+  *tma_sweeps = ctx->sweeps_tma;
+  *plain_sweeps = ctx->sweeps_plain;
+  return MB_OK;
+}
 
 int64_t mb_launch_count(const mb_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
@@ -205,7 +222,7 @@ static int check_mesh(const mb_mesh* mesh, int ngroups) {
   for (int b = 0; b < mesh->nblk; ++b) {
     const mb_block& q = mesh->blk[b];
     if (q.n[0] < 1 || q.n[1] < 1 || q.n[2] < 1 || !q.fm1 || !q.fm2 || !q.fm3 || !q.dl || !q.m || !q.vol) return MB_E_ARG;
-    if (q.group < 0 || q.group >= ngroups) return MB_E_ARG;
+    if (q.group < -1 || q.group >= ngroups) return MB_E_ARG;  // -1: an external block (a halo copy)
     // intra-block offsets of the sweep are 32-bit: 9 metric values per padded cell, 4 per face
     const long long npad = (long long)(q.n[0] + 2 * MB_GC) * (q.n[1] + 2 * MB_GC) * (q.n[2] + 2 * MB_GC);
     if (9 * npad >= (1LL << 31)) return MB_E_ARG;
@@ -218,6 +235,7 @@ static int check_mesh(const mb_mesh* mesh, int ngroups) {
         r.type != MB_BC_INFLOW && r.type != MB_BC_SYMMETRY && r.type != MB_BC_WALL_T && r.type != MB_BC_OUTLET)
       return MB_E_UNSUPPORTED;
     if (r.blk < 0 || r.blk >= mesh->nblk || r.face < 1 || r.face > 6) return MB_E_ARG;
+    if (mesh->blk[r.blk].group < 0) return MB_E_ARG;  // an external block carries no records
     if ((rc = check_record_params(r)) != MB_OK) return rc;
   }
   return MB_OK;
@@ -265,6 +283,7 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   std::vector<int> gndir(c->ngroups, 0);
   for (int b = 0; b < mesh->nblk; ++b) {
     const mb_block& q = mesh->blk[b];
+    if (q.group < 0) continue;
     if (gndir[q.group] == 0) gndir[q.group] = (q.n[2] > 1) ? 3 : ((q.n[1] == 1 && q.n[2] == 1) ? 1 : 2);
   }
   for (int b = 0; b < mesh->nblk; ++b) {
@@ -274,7 +293,7 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
     d.n1 = q.n[0]; d.n2 = q.n[1]; d.n3 = q.n[2];
     d.pi = q.n[0] + 2 * MB_GC; d.pj = q.n[1] + 2 * MB_GC;
     d.grp = q.group;
-    d.ndir = (c->ngroups > 1) ? gndir[q.group] : sc->ndir;
+    d.ndir = (c->ngroups > 1 && q.group >= 0) ? gndir[q.group] : sc->ndir;
     d.boff = q.boff;
     d.fm1 = q.fm1; d.fm2 = q.fm2; d.fm3 = q.fm3; d.dl = q.dl; d.m = q.m; d.vol = q.vol;
     for (int f = 0; f < 6; ++f) d.rmap[f] = -1;
@@ -398,11 +417,11 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   for (int b = 0; b < mesh->nblk; ++b)
     for (int a = 0; a < 3; ++a) c->hdims[3 * b + a] = mesh->blk[b].n[a];
   c->hkm.assign(mesh->nblk, 0);
-  for (int b = 0; b < mesh->nblk; ++b) c->hkm[b] = hb[b].kmirror;
+  for (int b = 0; b < mesh->nblk; ++b) c->hkm[b] = mesh->blk[b].group < 0 ? -1 : hb[b].kmirror;
   std::vector<DTile> ts = make_tiles(c->hdims, c->ty_sweep, c->kc3, 0xe, &c->hkm, 0);
   std::vector<DTile> tk = make_tiles(c->hdims, c->ty_sweep, c->kc3, 0xe, &c->hkm, 1);
   if (c->persistent) sort_by_work(ts, c->hdims, c->ty_sweep);
-  std::vector<DTile> ta = make_tiles(c->hdims, TY_AUX, 16);
+  std::vector<DTile> ta = make_tiles(c->hdims, TY_AUX, 16, 0xe, &c->hkm, -1);
   // ---- the mixed form reads its geometry in FP32: one conversion per distinct array of this mesh (blocks may
   // share arrays). Every copy is converted afresh (a caller may have replaced an array at the same address);
   // the buffers of the previous mesh are reused where the size matches.
@@ -609,6 +628,7 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   c->ncell = mesh->ncell_total;
   c->ngroups = ngroups;
   c->ty_sweep = sc->precision == MB_PREC_MIXED ? TY_F32 : TY_F64;
+  c->no_tma = getenv("MB_NO_TMA") != nullptr;
 #define TRY(x)                 \
   do {                         \
     rc = (x);                  \
@@ -774,7 +794,8 @@ static void to_status(const DevState& h, int state_check, mb_status* st) {
   st->done = h.done;
   for (int v = 0; v < MB_NPRIM; ++v) st->res[v] = sqrt(h.res2[v]);
   st->code = MB_OK;
-  if (h.n_bad_thermo > 0) st->code = MB_E_THERMO;
+  if (h.code == MB_E_TIMEOUT) st->code = MB_E_TIMEOUT;  // a bounded wait of the sweep's TMA staging gave up
+  else if (h.n_bad_thermo > 0) st->code = MB_E_THERMO;
   else if (h.n_bad_state > 0 && state_check) st->code = MB_E_STATE;
 }
 
@@ -805,12 +826,69 @@ void mb_destroy(mb_ctx* ctx) {
   free_ctx(ctx);
 }
 
+// ---- TMA staging of the mixed sweep: the state buffer P viewed as a 2-D tensor of ncell rows x 5 FP64 variables
+// (var-last, the variable stride ncell x 8 bytes), boxes of 38 rows x 5 variables (one staged j-row of a tile plane)
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)f;
+  }
+  return fn;
+}
+
+// the tensor map of P for the current row count, or null: the form does not stage by TMA, P is not 16-byte aligned,
+// ncell is odd (the variable stride must be a multiple of 16 bytes), or (create) the stream is capturing and the map
+// does not exist yet. Without a map the sweep stages with plain loads; both paths give the same tile values.
+static const void* tmap_of(mb_ctx* c, const double* P, cudaStream_t s, bool create) {
+  if (c->sc.precision != MB_PREC_MIXED || !P || c->no_tma) return nullptr;
+  for (const auto& m : c->tmaps)
+    if (m.ptr == P && m.nc == c->ncell) return m.dev;
+  if (!create || ((uintptr_t)P & 15u) || (c->ncell & 1) || c->tmaps.size() >= 64) return nullptr;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return nullptr;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+  if (!enc) return nullptr;
+  CUtensorMap m;
+  cuuint64_t dims[2] = {(cuuint64_t)c->ncell, (cuuint64_t)MB_NPRIM};
+  cuuint64_t strides[1] = {(cuuint64_t)c->ncell * sizeof(double)};
+  cuuint32_t box[2] = {(cuuint32_t)TMA_BOX_ROWS, (cuuint32_t)MB_NPRIM};
+  cuuint32_t es[2] = {1, 1};
+  if (enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void*)P, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+      CUDA_SUCCESS)
+    return nullptr;
+  void* d = nullptr;
+  if (cudaMalloc(&d, sizeof(CUtensorMap)) != cudaSuccess) return nullptr;
+  if (cudaMemcpyAsync(d, &m, sizeof(CUtensorMap), cudaMemcpyHostToDevice, s) != cudaSuccess) {
+    cudaFree(d);
+    return nullptr;
+  }
+  c->tmaps.push_back({P, c->ncell, d});
+  return d;
+}
+
+// the maps of the buffers a stage or step may read (before any capture)
+static void prepare_tmaps(mb_ctx* c, const double* P, const double* PO, cudaStream_t s) {
+  tmap_of(c, P, s, true);
+  tmap_of(c, PO, s, true);
+  tmap_of(c, c->d_scratch, s, true);
+}
+
 static int sweep_on(mb_ctx* c, const DTile* t, int n, int persistent, int mode, const double* Pin,
                     const double* Pold, double* Pout, double* Rout, int irk, int last, cudaStream_t s, int km = 0) {
   if (n <= 0) return MB_OK;
   Params p = c->p;
   p.irk = irk;
   p.queue = persistent ? c->d_queue : nullptr;
+  p.tmap = tmap_of(c, Pin, s, false);
+  p.tmap_old = (mode == MODE_UPDATE) ? tmap_of(c, Pold, s, false) : nullptr;
+  if (c->sc.precision == MB_PREC_MIXED) ((p.tmap || p.tmap_old) ? c->sweeps_tma : c->sweeps_plain) += 1;
   const double rkc = irk > 0 ? rkc_of(c->sc.n_rk, irk) : 0.0;
   cudaError_t e;
   e = MB_BY_FORM(c->sc.precision, sweep_unit(&c->sc), , (p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s));
@@ -914,6 +992,7 @@ int mb_fill_ghosts(mb_ctx* ctx, double* P, void* stream) {
 int mb_residual(mb_ctx* ctx, const double* P, double* R, void* stream) {
   if (!ctx || !P || !R) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
+  tmap_of(ctx, P, (cudaStream_t)stream, true);
   int rc = ur_pass(ctx, P, (cudaStream_t)stream);
   if (rc != MB_OK) return rc;
   rc = records(ctx, P, (cudaStream_t)stream);
@@ -996,6 +1075,37 @@ int mb_begin_step(mb_ctx* ctx, const double* P, void* stream) {
   return MB_OK;
 }
 
+// ---- the step start and the stage split into its exchange points, for a host that partitions the blocks over
+// several GPUs (one context per GPU, external blocks holding the halo copies; mosegpu/partition.py): the minimum
+// local step of each rank is all-reduced (MIN) between mb_step_prepare and mb_step_start, and the halo rows are
+// exchanged before mb_stage_begin (the donor cells the ghost copies read) and between mb_stage_begin and
+// mb_stage_end (the donor ghost cells the viscous connection records read after the donors' own ghost fill)
+int mb_step_prepare(mb_ctx* ctx, const double* P, void* stream) {
+  if (!ctx || !P) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  if (ctx->dt_valid) return MB_OK;  // the last stage of the previous step left the minimum of P in the clocks
+  int rc = dt_min(ctx, P, (cudaStream_t)stream);
+  if (rc == MB_OK) ctx->dt_valid = true;
+  return rc;
+}
+
+int mb_copy_dtmin(mb_ctx* ctx, int g, void* buf, int to_clock, void* stream) {
+  if (!ctx || !buf || g < 0 || g >= ctx->ngroups) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  void* clk = (void*)&ctx->d_st[g].dtmin_bits;
+  CK(cudaMemcpyAsync(to_clock ? clk : buf, to_clock ? buf : clk, sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                     (cudaStream_t)stream));
+  return MB_OK;
+}
+
+int mb_step_start(mb_ctx* ctx, void* stream) {
+  if (!ctx) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(clock_step(ctx->p, (cudaStream_t)stream));
+  ctx->launches += 1;
+  return MB_OK;
+}
+
 // the stage's computation after its ghost fill and boundary records: the fused sweep, or with residual smoothing the
 // sweep's residual, IRS_apply and the update on the smoothed residual (old state in P)
 static int stage_compute(mb_ctx* c, const double* in, const double* P, double* outp, int irk, int last,
@@ -1034,9 +1144,54 @@ static int stage(mb_ctx* c, double* P, double* PO, int irk, cudaStream_t s) {
   return MB_OK;
 }
 
+int mb_stage_begin(mb_ctx* ctx, double* P, double* PO, int irk, void* stream) {
+  if (!ctx || !P || !PO || irk < 1 || irk > ctx->sc.n_rk) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  prepare_tmaps(ctx, P, PO, s);
+  const double* in;
+  double* outp;
+  stage_buffers(ctx->sc.n_rk, irk, P, PO, ctx->d_scratch, &in, &outp);
+  int rc = ur_pass(ctx, in, s);
+  if (rc != MB_OK) return rc;
+  return fill(ctx, const_cast<double*>(in), s);
+}
+
+int mb_stage_end(mb_ctx* ctx, double* P, double* PO, int irk, void* stream) {
+  if (!ctx || !P || !PO || irk < 1 || irk > ctx->sc.n_rk) return MB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int n = ctx->sc.n_rk;
+  const double* in;
+  double* outp;
+  stage_buffers(n, irk, P, PO, ctx->d_scratch, &in, &outp);
+  int rc = records(ctx, in, s);
+  if (rc != MB_OK) return rc;
+  rc = stage_compute(ctx, in, P, outp, irk, irk == n ? 1 : 0, s);
+  if (rc != MB_OK) return rc;
+  if (n == 1) CK(cudaMemcpyAsync(P, ctx->d_scratch, (size_t)ctx->ncell * MB_NPRIM * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, s));
+  return MB_OK;
+}
+
+int mb_pack_rows(const double* P, int64_t ncell, const int64_t* rows, int32_t n, double* buf, void* stream) {
+  if (!P || ncell < 1 || n < 0 || (n > 0 && (!rows || !buf))) return MB_E_ARG;
+  if (n == 0) return MB_OK;
+  CK(pack_rows(P, ncell, (const long long*)rows, n, buf, (cudaStream_t)stream));
+  return MB_OK;
+}
+
+int mb_unpack_rows(double* P, int64_t ncell, const int64_t* rows, int32_t n, const double* buf, void* stream) {
+  if (!P || ncell < 1 || n < 0 || (n > 0 && (!rows || !buf))) return MB_E_ARG;
+  if (n == 0) return MB_OK;
+  CK(unpack_rows(P, ncell, (const long long*)rows, n, buf, (cudaStream_t)stream));
+  return MB_OK;
+}
+
 int mb_stage(mb_ctx* ctx, double* P, double* PO, int irk, void* stream) {
   if (!ctx || !P || !PO || irk < 1 || irk > ctx->sc.n_rk) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
+  prepare_tmaps(ctx, P, PO, (cudaStream_t)stream);
   return stage(ctx, P, PO, irk, (cudaStream_t)stream);
 }
 
@@ -1058,6 +1213,7 @@ int mb_step(mb_ctx* ctx, double* P, double* PO, int nsteps, int use_graph, void*
   if (!ctx || !P || !PO || nsteps < 0) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
   cudaStream_t s = (cudaStream_t)stream;
+  prepare_tmaps(ctx, P, PO, s);
   if (!ctx->dt_valid) {
     int rc = dt_min(ctx, P, s);
     if (rc != MB_OK) return rc;
@@ -1103,6 +1259,7 @@ int mb_profile_stage(mb_ctx* ctx, double* P, double* PO, int irk, int nrep, floa
   if (!ctx || !P || !PO || irk < 1 || irk > ctx->sc.n_rk || nrep < 1 || !ms_ghost || !ms_sweep) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
   cudaStream_t s = (cudaStream_t)stream;
+  prepare_tmaps(ctx, P, PO, s);
   const int n = ctx->sc.n_rk;
   double* S = ctx->d_scratch;
   const double* in;
@@ -1146,6 +1303,7 @@ int mb_autotune(mb_ctx* ctx, const double* P, void* stream) {
   if (!ctx || !P) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
   cudaStream_t s = (cudaStream_t)stream;
+  prepare_tmaps(ctx, P, P, s);
   const int ty = ctx->ty_sweep;
   int maxk = 1;
   for (size_t b = 0; b < ctx->hdims.size() / 3; ++b) maxk = std::max(maxk, ctx->hdims[3 * b + 2]);

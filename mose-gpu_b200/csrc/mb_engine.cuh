@@ -31,18 +31,47 @@ template <typename R> MB_HD R cvt(double x) { return (R)x; }
 
 // ---------------------------------------------------------------------------------------------
 // The state tile of a CTA in shared memory: 4 k-planes (a rolling window), each (32+4) x (TY+4) cells
-// (two halo cells on each side in i and j), NV values per cell: rho_s, u, v, w, p of P and the thermo-cache
-// temperature T = p / (rho Rg) (Mod_Thermo_Cache.f90:327-330), converted to the flux arithmetic type once
-// per cell. Layout [slot][value][jj][ii], ii fastest.
+// (two halo cells on each side in i and j), converted to the flux arithmetic type once per cell, with the
+// thermo-cache temperature T = p / (rho Rg) (Mod_Thermo_Cache.f90:327-330). The FP64 forms keep 6 values per cell:
+// rho_s, u, v, w, p, T. The mixed form keeps 5: rho_s, u, v, w, T, and takes p = rho Rg T where it reads it (one
+// value less per cell leaves room in shared memory for the TMA staging buffer at 3 CTAs per SM).
+// Layout [slot][value][jj][ii], ii fastest.
 constexpr int TXH = 36;
-constexpr int NV = 6;
+#ifndef MB_TILE5
+#define MB_TILE5 0
+#endif
+template <typename R> struct TileNV { static constexpr int v = (sizeof(R) == 4 && MB_TILE5) ? 5 : 6; };
+// TMA staging in the mixed form: of the halo tile of the sweep's input (MB_TMA_HALO) and of the old state the update
+// reads at the tile's own cells (MB_TMA_OLD)
+#ifndef MB_TMA_HALO
+#define MB_TMA_HALO 0
+#endif
+#ifndef MB_TMA_OLD
+#define MB_TMA_OLD 1
+#endif
+template <typename R> struct TmaOn {
+  static constexpr bool halo = sizeof(R) == 4 && MB_TMA_HALO;
+  static constexpr bool old = sizeof(R) == 4 && MB_TMA_OLD;
+};
+// the k-face fluxes of the mixed form live in registers (sweep_tile)
+#ifndef MB_KFACE_REG
+#define MB_KFACE_REG 1
+#endif
+template <typename R> struct KfaceReg { static constexpr bool on = sizeof(R) == 4 && MB_KFACE_REG; };
 
 template <typename R, int TY>
 struct Tile {
   R* base;
+  R rg;                                              // the gas constant of the single species (5-value tile)
+  static constexpr int NVT = TileNV<R>::v;
   static constexpr int VS = (TY + 4) * TXH;          // stride between the values of one cell
-  MB_HD int off(int slot, int jj, int ii) const { return slot * NV * VS + jj * TXH + ii; }
-  MB_HD R v(int o, int var) const { return base[o + var * VS]; }
+  MB_HD int off(int slot, int jj, int ii) const { return slot * NVT * VS + jj * TXH + ii; }
+  // value var (0..4: rho_s, u, v, w, p; 5: T) of the cell at offset o
+  MB_HD R v(int o, int var) const {
+    if (NVT == 6 || var < 4) return base[o + var * VS];
+    if (var == 5) return base[o + 4 * VS];
+    return base[o] * rg * base[o + 4 * VS];
+  }
 };
 
 // the plane slot of plane kk (kk >= -1)
@@ -78,10 +107,9 @@ MB_HD void face_flux(const Params& p, const DBlk& b, const Tile<R, TY>& T, int d
   R nx = (R)ld(f), ny = (R)ld(f + 1), nz = (R)ld(f + 2), area = (R)ld(f + 3);
   R bet = (R)1;
   if (RS == 0 && p.sd) {  // the sensor of the face's left cell (Mod_Fluxes.f90:282-294; conv_cuf: bet = beta(i,j,k))
-    constexpr int VP = MB_IPR * Tile<R, TY>::VS;
-    bet = sd_beta<R>(p.sd, p0[MB_IPR], T.base[T.off(sk, jj, ii - 1) + VP], T.base[T.off(sk, jj, ii + 1) + VP],
-                     T.base[T.off(sk, jj - 1, ii) + VP], T.base[T.off(sk, jj + 1, ii) + VP],
-                     T.base[T.off(skm, jj, ii) + VP], T.base[T.off(sk1, jj, ii) + VP]);
+    bet = sd_beta<R>(p.sd, p0[MB_IPR], T.v(T.off(sk, jj, ii - 1), MB_IPR), T.v(T.off(sk, jj, ii + 1), MB_IPR),
+                     T.v(T.off(sk, jj - 1, ii), MB_IPR), T.v(T.off(sk, jj + 1, ii), MB_IPR),
+                     T.v(T.off(skm, jj, ii), MB_IPR), T.v(T.off(sk1, jj, ii), MB_IPR));
   }
   R urL = (R)0, urR = (R)0;
   if (RS == 0 && p.prec) {  // HLLC-PC: the Ur of the face's two cells (conv_physics.inc:159-163)
@@ -1309,7 +1337,22 @@ __device__ __forceinline__ void report_bad_state(DevState* st, int blk, int i, i
 // ---------------------------------------------------------------------------------------------
 // Stage plane kk of the tile window: cells (i0-2 .. i0+33) x (j0-2 .. j0+TY+1), those inside the padded block and
 // within jext rows of the interior (jext < 2 for a block one cell deep in j: no j-faces, so only the viscous
-// transverse stencil reads the ghost rows).
+// transverse stencil reads the ghost rows); the others hold zeros.
+template <typename R, int TY>
+__device__ __forceinline__ void put_cell(const Params& p, const Tile<R, TY>& T, int o, R* vals) {
+  R rho, Tc;
+  cell_rho_T<R>(p, vals[0], vals[MB_IPR], rho, Tc);
+  constexpr int VS = Tile<R, TY>::VS;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) T.base[o + v * VS] = vals[v];
+  if (Tile<R, TY>::NVT == 6) {
+    T.base[o + 4 * VS] = vals[MB_IPR];
+    T.base[o + 5 * VS] = Tc;
+  } else {
+    T.base[o + 4 * VS] = Tc;
+  }
+}
+
 template <typename R, int TY>
 __device__ __forceinline__ void stage_plane(const Params& p, const DBlk& b, const double* __restrict__ P,
                                             const Tile<R, TY>& T, int i0, int j0, int kk, int jext) {
@@ -1318,26 +1361,137 @@ __device__ __forceinline__ void stage_plane(const Params& p, const DBlk& b, cons
   for (int c = threadIdx.x; c < TXH * (TY + 4); c += blockDim.x) {
     const int jj = c / TXH, ii = c - jj * TXH;
     const int i = i0 - 2 + ii, j = j0 - 2 + jj;
-    R vals[NV] = {(R)0, (R)0, (R)0, (R)0, (R)0, (R)0};
+    const int o = T.off(sl, jj, ii);
+    R vals[MB_NP] = {(R)0, (R)0, (R)0, (R)0, (R)0};
     if (i >= 1 - GC && i <= b.n1 + GC && j >= 1 - jext && j <= b.n2 + jext) {
       const long long r = row(b, i, j, kk);
 #pragma unroll
       for (int s = 0; s < MB_NP; ++s) vals[s] = cvt<R>(ld(P + r + s * nc));
-      R rho, Tc;
-      cell_rho_T<R>(p, vals[0], vals[MB_IPR], rho, Tc);
-      vals[5] = Tc;
-    }
-    const int o = T.off(sl, jj, ii);
+      put_cell<R, TY>(p, T, o, vals);
+    } else {
 #pragma unroll
-    for (int v = 0; v < NV; ++v) T.base[o + v * Tile<R, TY>::VS] = vals[v];
+      for (int v = 0; v < Tile<R, TY>::NVT; ++v) T.base[o + v * Tile<R, TY>::VS] = (R)0;
+    }
+  }
+}
+
+// ---- TMA staging of the mixed form (sm_100a). The state arena is a 2-D tensor of ncell_total rows x 5 variables
+// (var-last, the reference's P_flat); one staged j-row of a plane is one box of 38 consecutive rows x 5 variables,
+// its first row rounded down to an even row (the 16-byte rule of the innermost coordinate), so the 36 cells of the
+// row sit at offset (row & 1). The TY+4 boxes of a plane land in the raw buffer ([jj][var][38] FP64, one 1536-byte
+// slot per j-row) and complete one phase of a shared-memory mbarrier; stage_plane_raw then converts them to the tile.
+constexpr int TMA_BOX_ROWS = 38;
+constexpr int TMA_ROW_BYTES = 1536;                  // 5 x 38 x 8 = 1520, padded to a multiple of 128
+constexpr unsigned TMA_WAIT_LIMIT = 1u << 22;        // try_wait rounds before a wait gives up (seconds)
+
+__device__ __forceinline__ unsigned smem_addr(const void* q) { return (unsigned)__cvta_generic_to_shared(q); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred q;\n mbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\n selp.u32 %0, 1, 0, q;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait of every thread for the phase `parity` of bar; false if it gave up (the caller's threads then agree
+// through a barrier and leave)
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  for (unsigned q = 0; q < TMA_WAIT_LIMIT; ++q)
+    if (mbar_test(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(smem_addr(dst)), "l"(tmap), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// warp 0 issues the TY+4 row boxes of plane kk into raw (lane 0 arms the barrier first)
+template <int TY>
+__device__ __forceinline__ void tma_issue_plane(const Params& p, const DBlk& b, unsigned char* raw,
+                                                unsigned long long* bar, int i0, int j0, int kk) {
+  if (threadIdx.x >= 32) return;
+  if (threadIdx.x == 0) mbar_expect(bar, (unsigned)((TY + 4) * MB_NP * TMA_BOX_ROWS * sizeof(double)));
+  __syncwarp();
+  const int jj = threadIdx.x;
+  if (jj < TY + 4) {
+    const long long r = row(b, i0 - 2, j0 - 2 + jj, kk);
+    tma_load_2d(raw + jj * TMA_ROW_BYTES, p.tmap, (int)(r & ~1LL), 0, bar);
+  }
+}
+
+// the TMA staging state of a CTA: the halo-plane buffer and the old-state buffer, their mbarriers and the parity
+// each is waited for next
+struct TmaStage {
+  unsigned char* halo;
+  unsigned char* old;
+  unsigned long long* bar_halo;
+  unsigned long long* bar_old;
+  unsigned ph_halo, ph_old;
+};
+
+// warp 0 issues the TY row boxes of the old state at the tile's own cells of plane k (one box per j-row: 38 rows
+// from the even row at or below the row of cell i0, so the 32 cells sit at offset row & 1)
+template <int TY>
+__device__ __forceinline__ void tma_issue_old(const Params& p, const DBlk& b, unsigned char* buf,
+                                              unsigned long long* bar, int i0, int j0, int k) {
+  if (threadIdx.x >= 32) return;
+  if (threadIdx.x == 0) mbar_expect(bar, (unsigned)(TY * MB_NP * TMA_BOX_ROWS * sizeof(double)));
+  __syncwarp();
+  const int jj = threadIdx.x;
+  if (jj < TY) {
+    const long long r = row(b, i0, j0 + jj, k);
+    tma_load_2d(buf + jj * TMA_ROW_BYTES, p.tmap_old, (int)(r & ~1LL), 0, bar);
+  }
+}
+
+// convert the landed raw plane into the tile slot of plane kk (the same cells and values as stage_plane)
+template <typename R, int TY>
+__device__ __forceinline__ void stage_plane_raw(const Params& p, const DBlk& b, const unsigned char* raw,
+                                                const Tile<R, TY>& T, int i0, int j0, int kk, int jext) {
+  const int sl = slot_of(kk);
+  for (int c = threadIdx.x; c < TXH * (TY + 4); c += blockDim.x) {
+    const int jj = c / TXH, ii = c - jj * TXH;
+    const int i = i0 - 2 + ii, j = j0 - 2 + jj;
+    const int o = T.off(sl, jj, ii);
+    R vals[MB_NP] = {(R)0, (R)0, (R)0, (R)0, (R)0};
+    if (i >= 1 - GC && i <= b.n1 + GC && j >= 1 - jext && j <= b.n2 + jext) {
+      const int sh = (int)(row(b, i0 - 2, j, kk) & 1);
+      const double* src = reinterpret_cast<const double*>(raw + jj * TMA_ROW_BYTES) + sh + ii;
+#pragma unroll
+      for (int s = 0; s < MB_NP; ++s) vals[s] = cvt<R>(src[s * TMA_BOX_ROWS]);
+      put_cell<R, TY>(p, T, o, vals);
+    } else {
+#pragma unroll
+      for (int v = 0; v < Tile<R, TY>::NVT; ++v) T.base[o + v * Tile<R, TY>::VS] = (R)0;
+    }
   }
 }
 
 // One tile of the fused stage (the body of k_sweep).
+// With TMA staging (the mixed form, p.tmap set) raw is the staging buffer and bar its mbarrier, phase the parity the
+// CTA waits for next; false: a bounded wait gave up (the clock's code is set to MB_E_TIMEOUT) and the CTA must stop.
 template <typename R, int TY, bool VISC, int MODE, int RS, int LIM, bool KM>
-__device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const double* __restrict__ Pin,
+__device__ __forceinline__ bool sweep_tile(const Params& p, const DTile t, const double* __restrict__ Pin,
                                            const double* Pold, double* Pout, double* Rout, double rkc, int last,
-                                           unsigned char* smem_raw, double* sred, double* s_res) {
+                                           unsigned char* smem_raw, double* sred, double* s_res, TmaStage& ts) {
+  unsigned char* raw = ts.halo;
+  unsigned long long* bar = ts.bar_halo;
+  unsigned& phase = ts.ph_halo;
   constexpr int NF = VISC ? 2 * MB_NP : MB_NP;  // values a face task computes (convective, viscous)
   // values a face keeps in shared memory: both fluxes in the FP64 form (pass 2 sums them in the reference's
   // order); the net flux (convective - viscous) in the mixed form
@@ -1346,14 +1500,25 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
   typedef R RowI[33][NS];
   typedef R RowJ[32][NS];
   Tile<R, TY> T;
-  T.base = reinterpret_cast<R*>(smem_raw);                                       // [4][NV][TY+4][36]
-  unsigned char* fbase = smem_raw + sizeof(R) * 4 * NV * (TY + 4) * TXH;
+  T.base = reinterpret_cast<R*>(smem_raw);                                       // [4][NVT][TY+4][36]
+  T.rg = (R)p.ri;
+  unsigned char* fbase = smem_raw + sizeof(R) * 4 * Tile<R, TY>::NVT * (TY + 4) * TXH;
   RowI* sFi = reinterpret_cast<RowI*>(fbase);                                     // [TY][33][NS]
   RowJ* sFj = reinterpret_cast<RowJ*>(fbase + sizeof(R) * TY * 33 * NS);          // [TY+1][32][NS]
+  // the k-faces: the face above a cell is computed by the thread of that cell and is the face below it on the next
+  // plane, so the mixed form carries both in that thread's registers (kup, kdn: no shared buffer, which leaves room
+  // for the TMA staging buffer at 3 CTAs per SM); the FP64 forms keep them in shared memory (two planes)
+  constexpr bool KREG = KfaceReg<R>::on;
   RowJ* sFk0 = reinterpret_cast<RowJ*>(fbase + sizeof(R) * (TY * 33 + (TY + 1) * 32) * NS);  // [2][TY][32][NS]
+  R kup[NS], kdn[NS];
+#pragma unroll
+  for (int q = 0; q < NS; ++q) kup[q] = kdn[q] = (R)0;
   const DBlk b = p.blk[t.blk];
   DevState* st = p.st + b.grp;
-  if (MODE == MODE_UPDATE && st->done) return;  // the case has reached its stop time (uniform over the CTA)
+  if (MODE == MODE_UPDATE && st->done) return true;  // the case has reached its stop time (uniform over the CTA)
+  const bool tma = TmaOn<R>::halo && p.tmap != nullptr;  // TMA staging of the halo tile (uniform over the CTA)
+  // TMA staging of the old state at the tile's own cells, one plane per loop iteration (uniform over the CTA)
+  const bool tmo = TmaOn<R>::old && MODE == MODE_UPDATE && p.tmap_old != nullptr;
   const int tid = threadIdx.x;
   const int tx = tid & 31, ty = tid >> 5;
   const int i = t.i0 + tx, j = t.j0 + ty;
@@ -1367,22 +1532,59 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
   const bool sens = RS == 0 && p.sd;  // the shock sensor reads the six face neighbours of a cell
   const int jext = (b.n2 > 1) ? GC : ((VISC || sens) ? 1 : 0);
   const int kext = (b.n3 > 1) ? GC : (((VISC || sens) && !KM) ? 1 : 0);
+  // a TMA wait that gave up: every thread learns it at the same barrier, the clock records it, the CTA stops
+  auto gave_up = [&](bool ok) -> bool {
+    if (!__syncthreads_or(!ok)) return false;
+    if (tid == 0) atomicCAS(&st->code, 0, MB_E_TIMEOUT_DEV);
+    return true;
+  };
   // prologue: planes k0-2 .. k0+1, and the k-face below the first plane
-  for (int kk = t.k0 - 2; kk <= t.k0 + 1; ++kk)
-    if (kk >= 1 - kext && kk <= b.n3 + kext) stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, kk, jext);
+  for (int kk = t.k0 - 2; kk <= t.k0 + 1; ++kk) {
+    if (kk < 1 - kext || kk > b.n3 + kext) continue;
+    if (tma) {
+      tma_issue_plane<TY>(p, b, raw, bar, t.i0, t.j0, kk);
+      const bool ok = mbar_wait(bar, phase);
+      phase ^= 1u;
+      if (gave_up(ok)) return false;
+      stage_plane_raw<R, TY>(p, b, raw, T, t.i0, t.j0, kk, jext);
+      __syncthreads();  // the staging buffer is free again
+    } else {
+      stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, kk, jext);
+    }
+  }
+  // the first plane of the loop in flight while the k-face below is computed
+  if (tma && t.k0 + 2 <= b.n3 + kext) tma_issue_plane<TY>(p, b, raw, bar, t.i0, t.j0, t.k0 + 2);
   __syncthreads();
   if (own && t.k0 > 1) {
     R out[NF];
     face_flux<R, TY, VISC, RS, LIM, KM>(p, b, T, 2, i, j, t.k0 - 1, tx + 2, ty + 2, out);
-    R* dst = &sFk0[(kb ^ 1) * TY + ty][tx][0];
+    if (KREG) {
 #pragma unroll
-    for (int q = 0; q < NS; ++q) dst[q] = NET ? out[q] - out[MB_NP + q] : out[q];
+      for (int q = 0; q < NS; ++q) kdn[q] = NET ? out[q] - out[MB_NP + q] : out[q];
+    } else {
+      R* dst = &sFk0[(kb ^ 1) * TY + ty][tx][0];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) dst[q] = NET ? out[q] - out[MB_NP + q] : out[q];
+    }
   }
   for (int k = t.k0; k < t.k1; ++k) {
     // the slot of plane k-2 is free: its last readers, the faces of plane k-1, finished before the barrier that
     // preceded pass 2 of plane k-1; so a thread stages plane k+2 as soon as its own pass 2 of plane k-1 is done
-    if (k + 2 <= b.n3 + kext) stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, k + 2, jext);
+    if (k + 2 <= b.n3 + kext) {
+      if (tma) {
+        const bool ok = mbar_wait(bar, phase);
+        phase ^= 1u;
+        if (gave_up(ok)) return false;
+        stage_plane_raw<R, TY>(p, b, raw, T, t.i0, t.j0, k + 2, jext);
+      } else {
+        stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, k + 2, jext);
+      }
+    }
     __syncthreads();  // plane k+2 staged, and every pass 2 of plane k-1 done (the flux buffers are free)
+    // the next plane's boxes fly under this plane's faces and pass 2 (the staging buffer was read before the barrier)
+    if (tma && k + 3 <= b.n3 + kext && k + 1 < t.k1) tma_issue_plane<TY>(p, b, raw, bar, t.i0, t.j0, k + 3);
+    // the old state of this plane's cells flies under the face work (its buffer was last read by pass 2 of k-1)
+    if (tmo) tma_issue_old<TY>(p, b, ts.old, ts.bar_old, t.i0, t.j0, k);
     // ---- face tasks of this plane through one call site: 0 = i-face #tid, 1 = extra i-faces (last warp,
     // lanes < TY), 2 = j-face #tid, 3 = extra j-face row (warp 0), 4 = the k-face above
 #pragma unroll 1
@@ -1405,15 +1607,25 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
         if (fj >= 1 && fj <= b.n2 - 1 && fi <= b.n1) { d = 1; dst = &sFj[rw][cl][0]; }
       } else {
         if (!own || k >= b.n3) continue;
-        fi = i; fj = j; ii = tx + 2; jj = ty + 2; d = 2; dst = &sFk0[kb * TY + ty][tx][0];
+        fi = i; fj = j; ii = tx + 2; jj = ty + 2; d = 2; dst = KREG ? nullptr : &sFk0[kb * TY + ty][tx][0];
       }
       if (d < 0) continue;
       R out[NF];
       face_flux<R, TY, VISC, RS, LIM, KM>(p, b, T, d, fi, fj, k, ii, jj, out);
+      if (KREG && task == 4) {
 #pragma unroll
-      for (int q = 0; q < NS; ++q) dst[q] = NET ? out[q] - out[MB_NP + q] : out[q];
+        for (int q = 0; q < NS; ++q) kup[q] = NET ? out[q] - out[MB_NP + q] : out[q];
+      } else {
+#pragma unroll
+        for (int q = 0; q < NS; ++q) dst[q] = NET ? out[q] - out[MB_NP + q] : out[q];
+      }
     }
     __syncthreads();
+    if (tmo) {
+      const bool ok = mbar_wait(ts.bar_old, ts.ph_old);
+      ts.ph_old ^= 1u;
+      if (gave_up(ok)) return false;
+    }
     // the residual diagnostic of the last stage: (new - old)^2 of this thread's cell, in the flux type (the warps'
     // partial sums in FP32 in the mixed form: the diagnostic to FP32 accuracy there)
     R rsq[MB_NP];
@@ -1426,8 +1638,9 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
       const R* fl = (i > 1) ? &sFi[ty][tx][0] : nullptr;
       const R* gr = (j < b.n2) ? &sFj[ty + 1][tx][0] : nullptr;
       const R* gl = (j > 1) ? &sFj[ty][tx][0] : nullptr;
-      const R* hr = (k < b.n3) ? &sFk0[kb * TY + ty][tx][0] : nullptr;
-      const R* hl = (k > 1) ? &sFk0[(kb ^ 1) * TY + ty][tx][0] : nullptr;
+      const bool hr_on = k < b.n3, hl_on = k > 1;
+      const R* hr = (!KREG && hr_on) ? &sFk0[kb * TY + ty][tx][0] : nullptr;
+      const R* hl = (!KREG && hl_on) ? &sFk0[(kb ^ 1) * TY + ty][tx][0] : nullptr;
       // the sum runs in the flux type (the FP64 form: FP64 in the reference's order; the mixed form: the six FP32
       // net face fluxes summed in FP32 and converted once), the boundary records and the update in FP64
 #pragma unroll
@@ -1437,8 +1650,13 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
         if (fl) a = a - fl[s];
         if (gr) a = a + gr[s];
         if (gl) a = a - gl[s];
-        if (hr) a = a + hr[s];
-        if (hl) a = a - hl[s];
+        if (KREG) {
+          if (hr_on) a = a + kup[s];
+          if (hl_on) a = a - kdn[s];
+        } else {
+          if (hr) a = a + hr[s];
+          if (hl) a = a - hl[s];
+        }
         if (VISC && !NET) {
           if (fr) a = a - fr[MB_NP + s];
           if (fl) a = a + fl[MB_NP + s];
@@ -1477,7 +1695,14 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
       } else {
         double pc[MB_NP], po[MB_NP], pn[MB_NP];
 #pragma unroll
-        for (int s = 0; s < MB_NP; ++s) { pc[s] = ld(Pin + r + s * p.nc); po[s] = Pold[r + s * p.nc]; }
+        if (tmo) {
+          const double* src = reinterpret_cast<const double*>(ts.old + ty * TMA_ROW_BYTES) + (int)(row(b, t.i0, j, k) & 1) + tx;
+#pragma unroll
+          for (int s = 0; s < MB_NP; ++s) { pc[s] = ld(Pin + r + s * p.nc); po[s] = src[s * TMA_BOX_ROWS]; }
+        } else {
+#pragma unroll
+          for (int s = 0; s < MB_NP; ++s) { pc[s] = ld(Pin + r + s * p.nc); po[s] = Pold[r + s * p.nc]; }
+        }
         double rho, Tc;
         if (Fast<R>::on) Tc = pc[MB_IPR] / pc[0] * p.iri;  // one species: R_mix = R
         else cell_rho_T(p, pc[0], pc[MB_IPR], rho, Tc);
@@ -1528,6 +1753,10 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
       }
     }
     kb ^= 1;
+    if (KREG) {
+#pragma unroll
+      for (int q = 0; q < NS; ++q) kdn[q] = kup[q];
+    }
   }
   if (MODE == MODE_UPDATE && last) {
     cta_min_dt(st, dtloc, sred);  // its barrier also orders the warps' sums before their reads below
@@ -1537,6 +1766,21 @@ __device__ __forceinline__ void sweep_tile(const Params& p, const DTile t, const
       atomicAdd(&st->res2[tid], x);
     }
   }
+  return true;
+}
+
+// shared memory of the sweep: the state tile and the face-flux buffers (sweep_smem_core), and in the mixed form the
+// TMA staging buffer of one plane (TY+4 row slots) with its 128-byte alignment slack
+template <typename R, int TY, bool VISC>
+MB_HD constexpr size_t sweep_smem_core() {
+  return sizeof(R) * ((size_t)4 * TileNV<R>::v * (TY + 4) * TXH +
+                      (size_t)(TY * 33 + (TY + 1) * 32 + (KfaceReg<R>::on ? 0 : 2 * TY * 32)) *
+                          ((VISC && !Fast<R>::on) ? 2 * MB_NP : MB_NP));
+}
+template <typename R, int TY, bool VISC>
+MB_HD constexpr size_t sweep_smem() {
+  return sweep_smem_core<R, TY, VISC>() + (TmaOn<R>::halo ? (size_t)128 + (size_t)(TY + 4) * TMA_ROW_BYTES : 0) +
+         (TmaOn<R>::old ? (size_t)128 + (size_t)TY * TMA_ROW_BYTES : 0);
 }
 
 // The fused stage over a tile list (KM: the tiles of mirrored one-plane blocks, a separate instantiation so that
@@ -1553,10 +1797,34 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
   __shared__ double sred[32];
   __shared__ double s_res[8 * MB_NP];  // per warp (at most 8) and variable: the tile's residual sums
   __shared__ int s_next;
+  __shared__ __align__(8) unsigned long long s_bar[2];  // TMA staging: the mbarriers of the halo plane, the old state
   static_assert(TY <= 8, "one residual slot per warp");
+  TmaStage ts{nullptr, nullptr, &s_bar[0], &s_bar[1], 0u, 0u};
+  if (TmaOn<R>::halo || TmaOn<R>::old) {  // the staging buffers after the tile and the flux buffers, 128-byte aligned
+    unsigned char* q = smem_raw + sweep_smem_core<R, TY, VISC>();
+    if (TmaOn<R>::halo) {
+      ts.halo = q + ((128u - (smem_addr(q) & 127u)) & 127u);
+      q += 128 + (TY + 4) * TMA_ROW_BYTES;
+    }
+    if (TmaOn<R>::old) ts.old = q + ((128u - (smem_addr(q) & 127u)) & 127u);
+    const void* maps[2] = {TmaOn<R>::halo ? p.tmap : nullptr,
+                           (TmaOn<R>::old && MODE == MODE_UPDATE) ? p.tmap_old : nullptr};
+    if (maps[0] || maps[1]) {
+      if (threadIdx.x == 0) {
+        if (maps[0]) mbar_init(&s_bar[0]);
+        if (maps[1]) mbar_init(&s_bar[1]);
+      }
+      // the maps were written to device memory by a host copy: the lanes that issue copies order them into the
+      // tensor-map proxy before their first use
+      for (int m = 0; m < 2; ++m)
+        if (maps[m] && threadIdx.x < 32)
+          asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(maps[m]) : "memory");
+      __syncthreads();
+    }
+  }
   if (!p.queue) {
     sweep_tile<R, TY, VISC, MODE, RS, LIM, KM>(p, tiles[blockIdx.x], Pin, Pold, Pout, Rout, rkc, last, smem_raw, sred,
-                                                s_res);
+                                                s_res, ts);
     return;
   }
   for (;;) {
@@ -1564,16 +1832,11 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
     __syncthreads();
     const int tix = s_next;
     if (tix >= p.ntiles_run) break;
-    sweep_tile<R, TY, VISC, MODE, RS, LIM, KM>(p, tiles[tix], Pin, Pold, Pout, Rout, rkc, last, smem_raw, sred,
-                                                s_res);
+    if (!sweep_tile<R, TY, VISC, MODE, RS, LIM, KM>(p, tiles[tix], Pin, Pold, Pout, Rout, rkc, last, smem_raw, sred,
+                                                     s_res, ts))
+      break;
     __syncthreads();  // the tile's shared memory is free and s_next may be overwritten
   }
-}
-
-template <typename R, int TY, bool VISC>
-constexpr size_t sweep_smem() {
-  return sizeof(R) * ((size_t)4 * NV * (TY + 4) * TXH +
-                      (size_t)(TY * 33 + (TY + 1) * 32 + 2 * TY * 32) * ((VISC && !Fast<R>::on) ? 2 * MB_NP : MB_NP));
 }
 
 }  // namespace mb

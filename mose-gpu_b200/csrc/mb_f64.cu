@@ -213,6 +213,36 @@ cudaError_t reset_dt(const Params& p, cudaStream_t s, int only_group) {
   return cudaGetLastError();
 }
 
+// the halo rows of a partitioned mesh, gathered into / scattered from a contiguous buffer [variable][row] (one
+// thread per row and variable, coalesced on the buffer side)
+__global__ void k_pack_rows(const double* __restrict__ P, long long nc, const long long* __restrict__ rows, int n,
+                            double* __restrict__ buf) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long long)n * MB_NP) return;
+  const int v = (int)(q / n), e = (int)(q - (long long)v * n);
+  buf[q] = P[rows[e] + v * nc];
+}
+
+__global__ void k_unpack_rows(double* __restrict__ P, long long nc, const long long* __restrict__ rows, int n,
+                              const double* __restrict__ buf) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long long)n * MB_NP) return;
+  const int v = (int)(q / n), e = (int)(q - (long long)v * n);
+  P[rows[e] + v * nc] = buf[q];
+}
+
+cudaError_t pack_rows(const double* P, long long ncell, const long long* rows, int n, double* buf, cudaStream_t s) {
+  const long long tot = (long long)n * MB_NP;
+  k_pack_rows<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(P, ncell, rows, n, buf);
+  return cudaGetLastError();
+}
+
+cudaError_t unpack_rows(double* P, long long ncell, const long long* rows, int n, const double* buf, cudaStream_t s) {
+  const long long tot = (long long)n * MB_NP;
+  k_unpack_rows<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(P, ncell, rows, n, buf);
+  return cudaGetLastError();
+}
+
 cudaError_t clock_step(const Params& p, cudaStream_t s) {
   k_clock<<<1, 256, 0, s>>>(p);
   return cudaGetLastError();

@@ -95,6 +95,9 @@ cudaError_t irs_smooth(const Params& p, const DTile* tiles, int ntiles, const do
 cudaError_t irs_stage_update(const Params& p, const DTile* tiles, int ntiles, const double* Pin, const double* Pold,
                              double* Pout, const double* R, double rkc, int last, cudaStream_t s);
 cudaError_t to_float(const double* src, float* dst, long long n, cudaStream_t s);
+// halo rows of a partitioned mesh: buf[v * n + q] <-> P[rows[q] + v * ncell] (mb_pack_rows / mb_unpack_rows)
+cudaError_t pack_rows(const double* P, long long ncell, const long long* rows, int n, double* buf, cudaStream_t s);
+cudaError_t unpack_rows(double* P, long long ncell, const long long* rows, int n, const double* buf, cudaStream_t s);
 cudaError_t clock_step(const Params& p, cudaStream_t s);
 cudaError_t group_reset(const Params& p, int g, int time_clip, double t_end, double res_stop, cudaStream_t s);
 

@@ -33,6 +33,7 @@ namespace mb {
 
 constexpr int GC = 2;
 constexpr double RUNIV = 8314.46261815324;  // lib/FLINT/src/lib/Lib_ThermoTransport.f90:13
+constexpr int MB_E_TIMEOUT_DEV = -7;  // MB_E_TIMEOUT of the C ABI: a bounded device wait gave up
 
 struct DBlk {
   int n1, n2, n3, pi, pj;
@@ -115,6 +116,9 @@ struct Params {
   int lim, rs, visc, ndir, dt_additive, guard, state_check;
   double cfl, vnn, prandtl, schmidt, mco;
   void* recflux;           // boundary-record contributions [record][10] in the flux type (k_records)
+  const void* tmap;        // mixed form: the TMA tensor map (CUtensorMap, device memory) of the sweep's input state as
+                           // a 2-D tensor of (ncell_total rows, 5 variables), or null (the scalar staging path)
+  const void* tmap_old;    // the same for the old state of the update (Pold), or null
   int* queue;              // persistent sweep: the tile counter (null: one CTA per tile)
   int ntiles_run;          // tiles of the launch (persistent sweep)
   int pgrid;               // CTAs of a persistent launch (resident CTAs per SM x SMs)

@@ -53,6 +53,18 @@ def load_library():
     L.mb_autotune.argtypes = [vp, vp, vp]
     L.mb_set_tuning.argtypes = [vp, C.c_int, C.c_int]
     L.mb_get_tuning.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)]
+    L.mb_step_prepare.argtypes = [vp, vp, vp]
+    L.mb_copy_dtmin.argtypes = [vp, C.c_int, vp, C.c_int, vp]
+    L.mb_step_start.argtypes = [vp, vp]
+    L.mb_stage_begin.argtypes = [vp, vp, vp, C.c_int, vp]
+    L.mb_stage_end.argtypes = [vp, vp, vp, C.c_int, vp]
+    L.mb_pack_rows.argtypes = [vp, C.c_int64, vp, C.c_int32, vp, vp]
+    L.mb_unpack_rows.argtypes = [vp, C.c_int64, vp, C.c_int32, vp, vp]
+    for f in ("mb_step_prepare", "mb_copy_dtmin", "mb_step_start", "mb_stage_begin", "mb_stage_end", "mb_pack_rows",
+              "mb_unpack_rows"):
+        getattr(L, f).restype = C.c_int
+    L.mb_get_staging.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.mb_get_staging.restype = C.c_int
     L.mb_launch_count.argtypes = [vp]
     L.mb_launch_count.restype = C.c_int64
     L.mb_version.restype = C.c_char_p
@@ -88,6 +100,7 @@ class Engine:
             B = self._blk[q]
             B.n[0], B.n[1], B.n[2] = b["n"]
             B.boff = b["boff"]
+            B.group = b.get("group", 0)          # -1: an external block (a halo copy, partition.py)
             for f in ("fm1", "fm2", "fm3", "dl", "m", "vol"):
                 key = id(b[f])
                 if key not in self._geo:
@@ -141,6 +154,12 @@ class Engine:
 
     def state(self):
         return self.P.cpu().numpy()
+
+    def staging(self):
+        """(sweep launches staged by TMA, by plain loads) of the mixed form so far (mb_get_staging)."""
+        a, b = C.c_int64(), C.c_int64()
+        _check(self.lib.mb_get_staging(self.ctx, C.byref(a), C.byref(b)), "mb_get_staging")
+        return a.value, b.value
 
     @property
     def launches(self):

@@ -68,6 +68,8 @@ struct Blk {
   int n1, n2, n3, pi, pj;
   int64_t boff;
   const double *fm1, *fm2, *fm3, *dl, *m, *vol;
+  bool ext = false;  // mb_block.group < 0: a copy of a block another rank owns (its rows are donor values the halo
+                     // exchange writes); nothing is computed on it
 };
 
 struct Ctx {
@@ -2062,6 +2064,7 @@ void residual(Ctx& c, const double* P, double* R) {
   const int64_t nc = c.ncell;
   const bool visc = c.sc.visc != 0;
   for (const Blk& b : c.blk) {
+    if (b.ext) continue;
     const int n1 = b.n1, n2 = b.n2, n3 = b.n3;
     const int64_t nf1 = (int64_t)(n1 - 1) * n2 * n3, nf2 = (int64_t)n1 * (n2 - 1) * n3, nf3 = (int64_t)n1 * n2 * (n3 - 1);
     std::vector<double> fh[3], dfh[3];
@@ -2300,6 +2303,7 @@ void update(Ctx& c, double* P, const double* PO, const double* R, int irk, doubl
   int nbad = 0, nth = 0;
   for (size_t bi = 0; bi < c.blk.size(); ++bi) {
     const Blk& b = c.blk[bi];
+    if (b.ext) continue;
 #pragma omp parallel for collapse(2) schedule(static) reduction(+ : nbad, nth)
     for (int k = 1; k <= b.n3; ++k)
       for (int j = 1; j <= b.n2; ++j)
@@ -2340,6 +2344,7 @@ void update(Ctx& c, double* P, const double* PO, const double* R, int irk, doubl
 void irs_ghost_residual(const Ctx& c, double* R) {
   const int64_t nc = c.ncell;
   for (const Blk& b : c.blk) {
+    if (b.ext) continue;
     auto cp = [&](int64_t g, int64_t m) { for (int s = 0; s < NP; ++s) R[g + s * nc] = R[m + s * nc]; };
     for (int k = 1; k <= b.n3; ++k)
       for (int j = 1; j <= b.n2; ++j) {
@@ -2378,6 +2383,7 @@ void irs_apply(Ctx& c, double* R, double dt, bool scale, const double* dtl = nul
   const int njacobi = c.sc.irs;
   if (scale)
     for (const Blk& b : c.blk)
+      if (!b.ext)
       for (int k = 1; k <= b.n3; ++k)
         for (int j = 1; j <= b.n2; ++j)
           for (int i = 1; i <= b.n1; ++i) {
@@ -2389,6 +2395,7 @@ void irs_apply(Ctx& c, double* R, double dt, bool scale, const double* dtl = nul
   for (int d = 1; d <= c.sc.ndir; ++d) {
     irs_ghost_residual(c, R);
     for (const Blk& b : c.blk) {
+    if (b.ext) continue;
       const int64_t off = (d == 1) ? 1 : (d == 2 ? (int64_t)b.pi : (int64_t)b.pi * b.pj);
       const int64_t nflat = (int64_t)b.pi * b.pj * (b.n3 + 2 * GC);
       for (int s = 0; s < NP; ++s)
@@ -2462,6 +2469,7 @@ void update_ur(Ctx& c, const double* P) {
   const int64_t nc = c.ncell;
   const Thermo& th = c.th;
   for (const Blk& b : c.blk) {
+    if (b.ext) continue;
     for (int k = 1; k <= b.n3; ++k)
       for (int j = 1; j <= b.n2; ++j)
         for (int i = 1; i <= b.n1; ++i) {
@@ -2614,6 +2622,7 @@ double compute_dt(Ctx& c, const double* P, std::vector<double>* dtl = nullptr) {
   double dtglobal = 1e5;  // Mod_Explicit.f90:122
   const double rampa = ramp_factor(c);
   for (const Blk& b : c.blk) {
+    if (b.ext) continue;
 #pragma omp parallel for collapse(2) schedule(static) reduction(min : dtglobal)
     for (int k = 1; k <= b.n3; ++k)
       for (int j = 1; j <= b.n2; ++j)
@@ -2655,6 +2664,7 @@ int orc_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, orc_
     k.pi = q.n[0] + 2 * GC; k.pj = q.n[1] + 2 * GC;
     k.boff = q.boff;
     k.fm1 = q.fm1; k.fm2 = q.fm2; k.fm3 = q.fm3; k.dl = q.dl; k.m = q.m; k.vol = q.vol;
+    k.ext = q.group < 0;
     c.blk.push_back(k);
   }
   c.rec.assign(mesh->rec, mesh->rec + mesh->nrec);
@@ -2750,6 +2760,7 @@ int orc_step(orc_ctx* o, double* P, double* PO, double* R, int nsteps) {
     // Mod_Explicit.f90:325-358): sqrt of the sum over the interior cells of (new - old)^2 per primitive variable
     double r2[NP] = {0.0, 0.0, 0.0, 0.0, 0.0};
     for (const Blk& b : c.blk)
+      if (!b.ext)
       for (int k = 1; k <= b.n3; ++k)
         for (int j = 1; j <= b.n2; ++j)
           for (int i = 1; i <= b.n1; ++i) {

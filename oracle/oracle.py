@@ -64,6 +64,7 @@ class Oracle:
             B = self._blk[q]
             B.n[0], B.n[1], B.n[2] = b["n"]
             B.boff = b["boff"]
+            B.group = b.get("group", 0)          # -1: an external block (a halo copy, partition.py)
             for f in ("fm1", "fm2", "fm3", "dl", "m", "vol"):
                 a = np.ascontiguousarray(b[f], dtype=np.float64)
                 self._keep.append(a)

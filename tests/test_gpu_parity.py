@@ -112,6 +112,38 @@ def test_fp64_production_form_within_the_gates(torch_cuda, cid, builder):
     assert abs(sg.time - so.time) <= 1e-11 * so.time
 
 
+TMA_CASES = {"tgv24_2x2x2": lambda cs: cs.taylor_green(n=24, blocks=2),
+             "mb2d_3x2": lambda cs: cs.multiblock_2d(cols=3, rows=2, lo=9, hi=40, seed=11),
+             "sod300": lambda cs: cs.riemann_1d(n=300)}
+
+
+@pytest.mark.parametrize("cid", sorted(TMA_CASES))
+def test_tma_staging_matches_plain_staging(torch_cuda, cid, monkeypatch):
+    """The mixed sweep stages its tiles by TMA (boxes of the state arena landing on an mbarrier) or, without a tensor
+    map, by plain loads: the tile values, and so every result, are the same bit for bit."""
+    from mosegpu import case as cs
+    from mosegpu.engine import Engine
+    case = TMA_CASES[cid](cs)
+    if case.ncell % 2:                                   # the variable stride must be a multiple of 16 bytes
+        pad = 1
+        case.ncell += pad
+        case.P0 = np.concatenate([case.P0, np.zeros((5, pad))], axis=1)
+    a = Engine(case, precision=abi.PREC_MIXED)
+    monkeypatch.setenv("MB_NO_TMA", "1")
+    b = Engine(case, precision=abi.PREC_MIXED)
+    monkeypatch.delenv("MB_NO_TMA")
+    a.step(6, graph=True)
+    b.step(6, graph=True)
+    ta, pa = a.staging()
+    tb, pb = b.staging()
+    assert ta > 0 and pa == 0, (ta, pa)
+    assert tb == 0 and pb > 0, (tb, pb)
+    m = case.interior_mask()
+    assert np.array_equal(a.state()[:, m], b.state()[:, m])
+    sa, sb = a.status(), b.status()
+    assert sa.code == 0 and sb.code == 0 and sa.time == sb.time
+
+
 def test_stage_by_stage_matches_fused(torch_cuda):
     """begin_step + stage(1..n) (the reference's call sequence) equals the fused mb_step."""
     from mosegpu import case as cs

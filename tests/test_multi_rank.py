@@ -8,6 +8,7 @@ import socket
 import sys
 from contextlib import redirect_stdout
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -79,3 +80,147 @@ def test_single_process_needs_no_process_group():
     w, r, local, pg = bench.dist_setup()
     assert (w, r, local, pg) == (1, 0, 0, None)
     assert bench.max_over_ranks(None, 3.25, None) == 3.25
+
+
+# ---------------------------------------------------------------------------------------------------------------------
+# Blocks partitioned over ranks (mosegpu/partition.py): the 2 x 2 x 2-block Taylor-Green field split over two gloo
+# ranks, each rank stepping its own blocks with the oracle and exchanging its halo rows through the partition's
+# schedule; the result must equal the one-rank oracle bit for bit.
+
+class OracleRank:
+    """One rank's blocks on the CPU restatement, with the rank-driver interface of partition.EngineRank."""
+
+    def __init__(self, rank_case):
+        import oracle
+        self.rc = rank_case
+        self.o = oracle.Oracle(rank_case.case)
+        self.P = rank_case.case.P0.copy()
+        self.PO = np.zeros_like(self.P)
+        self.dt = None
+
+    def pack(self, rows, rnd, tag):
+        import torch
+        return torch.from_numpy(np.ascontiguousarray(self.P[:, rows]).ravel())
+
+    def unpack(self, rows, buf):
+        self.P[:, rows] = np.asarray(buf).reshape(5, len(rows))
+
+    def local_dtmin(self):
+        return self.o.dt(self.P)
+
+    def start(self, dt):
+        self.dt = dt
+        self.PO[...] = self.P
+
+    def stage(self, irk, part):
+        if part == 0:
+            self.o.fill_ghosts(self.P)
+        else:
+            # the oracle copies bc_pg at its ghost fill (Ghost_Connection_pairs_B), the engine's records read those
+            # rows in place: after the round-2 rows have landed the fill runs again (the ghost values are the same,
+            # the copied donor rows now current)
+            self.o.fill_ghosts(self.P)
+            R = self.o.residual(self.P)
+            assert self.o.update(self.P, self.PO, R, irk, self.dt) == 0
+
+    def state(self):
+        return self.P
+
+
+def _tgv_case():
+    from mosegpu import case as cs
+    return cs.taylor_green(n=12, blocks=2)
+
+
+def _partition_rank_main(rank, world, port, q, steps):
+    try:
+        _partition_rank(rank, world, port, q, steps)
+    except Exception:
+        import traceback
+        q.put({"rank": rank, "error": traceback.format_exc()})
+        raise
+
+
+def _partition_rank(rank, world, port, q, steps):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    sys.path.insert(0, os.path.join(ROOT, "mose-gpu_b200"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from mosegpu import partition as pt
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    case = _tgv_case()
+    owner = pt.partition_blocks(case, world)
+    ranks = [pt.split_case(case, owner, r) for r in range(world)]
+    plan = pt.halo_plan(case, owner, ranks, visc=True)
+    drv = OracleRank(ranks[rank])
+    ex = pt.DistExchange(drv, plan, rank, world, torch.device("cpu"))
+    pt.step_rank(drv, ex, True, case.scheme["n_rk"], nsteps=steps)
+    out = {"rank": rank, "own": ranks[rank].own, "ext": ranks[rank].ext,
+           "interior": {g: ranks[rank].case.interior(drv.state(), q).copy() for q, g in enumerate(ranks[rank].own)},
+           "pairs": sorted(plan)}
+    dist.destroy_process_group()
+    q.put(out)
+
+
+def test_partitioned_blocks_match_one_rank_bit_for_bit():
+    import torch.multiprocessing as mp
+    sys.path.insert(0, os.path.join(ROOT, "mose-gpu_b200"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    steps = 3
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_partition_rank_main, args=(r, 2, port, q, steps)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    res.sort(key=lambda d: d["rank"])
+    assert not any("error" in d for d in res), [d.get("error") for d in res]
+    case = _tgv_case()
+    assert sorted(res[0]["own"] + res[1]["own"]) == list(range(8)) and len(res[0]["own"]) == 4
+    assert res[0]["ext"] and res[1]["ext"] and res[0]["pairs"] == [(0, 1), (1, 0)]
+    P = case.P0.copy()
+    assert oracle.Oracle(case).step(P, steps) == 0
+    for d in res:
+        for g, v in d["interior"].items():
+            assert np.array_equal(v, case.interior(P, g)), g
+
+
+def test_partition_and_halo_plan_on_one_process():
+    """The partition balances the cells, every remote donor block of a rank is one of its external copies, and the
+    halo rows of each pair are rows of the owner's own blocks (round 1) or of its padded blocks (round 2)."""
+    sys.path.insert(0, os.path.join(ROOT, "mose-gpu_b200"))
+    from mosegpu import case as cs
+    from mosegpu import partition as pt
+    case = cs.taylor_green(n=24, blocks=3)                   # 27 blocks of 8^3
+    for world in (2, 3, 4):
+        owner = pt.partition_blocks(case, world)
+        loads = [sum(int(np.prod(case.blocks[b]["n"])) for b in range(27) if owner[b] == r) for r in range(world)]
+        assert max(loads) - min(loads) <= 512
+        ranks = [pt.split_case(case, owner, r) for r in range(world)]
+        plan = pt.halo_plan(case, owner, ranks, visc=True)
+        for (src, dst), (s1, d1, s2, d2) in plan.items():
+            assert src != dst and len(s1) == len(d1) and len(s2) == len(d2) and len(s1) > 0
+            own_rows = np.zeros(ranks[src].case.ncell, dtype=bool)
+            for q in range(len(ranks[src].own)):
+                own_rows[ranks[src].case.blocks[q]["boff"] + np.arange(pt._padded(ranks[src].case.blocks[q]["n"]))] = True
+            assert own_rows[s1].all() and own_rows[s2].all()
+            ext_rows = np.zeros(ranks[dst].case.ncell, dtype=bool)
+            n_own = len(ranks[dst].own)
+            for q in range(n_own, n_own + len(ranks[dst].ext)):
+                b = ranks[dst].case.blocks[q]
+                ext_rows[b["boff"] + np.arange(pt._padded(b["n"]))] = True
+            assert ext_rows[d1].all() and ext_rows[d2].all()
+        for rc in ranks:
+            for b in rc.case.blocks[len(rc.own):]:
+                assert b["group"] == -1
+            assert all(int(rc.case.rec[q]["blk"]) < len(rc.own) for q in range(len(rc.case.rec)))
