@@ -215,7 +215,9 @@ def run_fixed_steps(case, steps, warmup, dev, stream):
     for name, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
         eng = Engine(case, precision=prec, device=dev.index, stream=stream)
         with torch.cuda.stream(stream):
-            eng.step(warmup, graph=True)
+            eng.step(1, graph=True)
+            tuning = eng.autotune()          # k-chunk, queue and (mixed) staging, timed on this state
+            eng.step(warmup - 1, graph=True)
         torch.cuda.synchronize(dev)
         l0 = eng.launches
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -229,7 +231,11 @@ def run_fixed_steps(case, steps, warmup, dev, stream):
         if st.code != 0:
             raise RuntimeError("%s %s form: %s" % (case.name, name, abi.status_message(st.code)))
         out[name] = {"value": case.n_interior * steps / (ms * 1e-3), "ms_per_step": ms / steps,
-                     "gpu_launches": eng.launches - l0, "time": st.time}
+                     "gpu_launches": eng.launches - l0, "time": st.time,
+                     "tuning": {"k_chunk": tuning[0], "persistent": bool(tuning[1])}}
+        if prec == abi.PREC_MIXED:
+            t, pl = eng.staging()
+            out[name]["staging"] = "TMA" if t > pl else "plain loads"
         states[name] = eng.state()
         eng.close()
         del eng
@@ -328,6 +334,26 @@ def run_serving(args, dev, world=1, rank=0, pg=None):
     return out
 
 
+def run_serving_sweep(args, dev, world=1, rank=0, pg=None):
+    """The serving sample at each offered rate of --serve-rates: cases/s served, p50 / p99 time-to-solution. The
+    sustained rate is the highest offered rate the server keeps up with (served >= 0.9 x offered, the p99 not
+    growing by more than half over the previous rate's)."""
+    out = {"rates": []}
+    sustained, prev_p99 = None, None
+    for rate in [float(x) for x in args.serve_rates.split(",")]:
+        args.serve_rate = rate
+        r = run_serving(args, dev, world, rank, pg)
+        out["rates"].append({k: r[k] for k in ("arrival_rate_per_s", "cases_per_s", "p50_s", "p99_s",
+                                                "cell_updates_per_s", "cases_completed", "makespan_s")})
+        keeps = r["cases_per_s"] >= 0.9 * rate and (prev_p99 is None or r["p99_s"] <= 1.5 * prev_p99)
+        if keeps:
+            sustained = rate
+        prev_p99 = r["p99_s"]
+    out["sustained_rate_per_s"] = sustained
+    out["sample"] = r["sample"]
+    return out
+
+
 def run_reference(args):
     world, rank, local, pg = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0, None
     if rank != 0:
@@ -373,7 +399,9 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="default", choices=["default", "c2", "c3", "c5", "serving"],
+    ap.add_argument("--serve-rates", default="1.0,1.5,2.0,2.5,3.0",
+                    help="serving-sweep: the offered rates (cases/s), each served with --serve-cases cases")
+    ap.add_argument("--workload", default="default", choices=["default", "c2", "c3", "c5", "serving", "serving-sweep"],
                     help="default: the 256^3 Taylor-Green headline plus the serving sample and the 2-D batch; "
                          "c2 / c3 / c5 / serving: that workload alone")
     ap.add_argument("--serve-cases", type=int, default=48)
@@ -393,10 +421,11 @@ def main():
     world, rank, local, pg = dist_setup()
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    if args.workload in ("c3", "c5", "serving"):
+    if args.workload in ("c3", "c5", "serving", "serving-sweep"):
         stream = torch.cuda.Stream(dev)
         r = {"c3": lambda: run_c3(args, dev, stream), "c5": lambda: run_c5(args, dev, stream),
-             "serving": lambda: run_serving(args, dev, world, rank, pg)}[args.workload]()
+             "serving": lambda: run_serving(args, dev, world, rank, pg),
+             "serving-sweep": lambda: run_serving_sweep(args, dev, world, rank, pg)}[args.workload]()
         if rank == 0:
             print(json.dumps({"workload": args.workload, "n_gpus": world, **r}), flush=True)
         if pg is not None:

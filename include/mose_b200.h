@@ -65,6 +65,8 @@ extern "C" {
  * whatever the Mach, the face closed to a symmetry face on outward flow), 5 = adiabatic no-slip wall
  * (301 with q = 0), 11 = extrapolation (400), 3 = symmetry (300), 6 = no-slip wall at a prescribed temperature
  * (302; q[0] = T_wall), 24 = back-pressure outlet (406; q[0] = exit pressure, q[1] = relaxation factor) */
+#define MB_BC_NONE 0 /* no boundary condition (bc.txt 0 / 100, IO_BC_Open.f90:155-156): the degenerate faces of a 1-D or
+                        2-D mesh; zero-gradient ghosts and no face flux (Mod_BC.f90:55-59, Lib_Extrapolation.f90:692) */
 #define MB_BC_CONNECTION 1
 #define MB_BC_SYMMETRY 3
 #define MB_BC_INFLOW 4
@@ -345,6 +347,9 @@ int mb_step_start(mb_ctx* ctx, void* stream);
 /* Stage irk split at the halo exchange point: mb_stage_begin fills the ghosts of the stage input (Fill_Ghost_Cell),
  * mb_stage_end computes the boundary records and runs the fused sweep and update. */
 int mb_stage_begin(mb_ctx* ctx, double* P, double* PO, int irk, void* stream);
+/* The device buffer stage irk reads (P, PO or the engine's own stage buffer: the engine rotates three buffers through
+ * the stages): the buffer whose halo rows the exchange of that stage packs and unpacks. */
+int mb_stage_input(mb_ctx* ctx, double* P, double* PO, int irk, double** in);
 int mb_stage_end(mb_ctx* ctx, double* P, double* PO, int irk, void* stream);
 
 /* Halo rows of a partitioned mesh: buf[v * n + q] = P[rows[q] + v * ncell] (pack) and its inverse (unpack), for the
@@ -392,6 +397,12 @@ int mb_dt_block_noalloc_tiles(const int32_t n[3], int32_t* kc, int32_t* ntiles);
  * Synchronises the device; invalidates the captured step graph. */
 int mb_reconfigure(mb_ctx* ctx, const mb_mesh* mesh);
 
+/* The same, ordered on `stream` (the stream every call of this context runs on) without synchronising the device:
+ * the new tables are allocated and copied in stream order (the stream-ordered allocator) and the old ones released
+ * after the work already queued on the stream, so other contexts (other serving lanes) keep running. Invalidates
+ * the captured step graph (a replay in flight completes on the old tables). No counterpart in the reference. */
+int mb_reconfigure_async(mb_ctx* ctx, const mb_mesh* mesh, void* stream);
+
 /* Starts case g afresh: time 0, no steps, cleared status, its stop rule, and its first dt from the cells of P
  * that belong to it (the other cases' clocks are untouched). */
 /* Replaces the parameters (mb_bc.q, same meaning as at mb_init) of record `rec` from the next stage on, ordered on
@@ -420,12 +431,19 @@ int mb_set_tuning(mb_ctx* ctx, int kchunk, int persistent);
 /* The configuration chosen by mb_autotune (k-chunk 16 and the plain grid before any call) and its sweep time. */
 int mb_get_tuning(const mb_ctx* ctx, int* kchunk, int* persistent, float* ms);
 
-/* How the mixed form's sweep launches of this context staged their state tiles (no counterpart in the reference):
- * *tma_sweeps by TMA (cp.async.bulk.tensor boxes of 38 rows x 5 variables of the state arena into shared memory,
- * completing on an mbarrier), *plain_sweeps by per-thread loads (the state buffer not 16-byte aligned, an odd
- * ncell_total, no tensor map made yet during a capture, or MB_NO_TMA set in the environment at mb_init). Both
- * paths give the same tile values, so the results do not depend on it. Launches recorded into a CUDA graph count
- * once, at capture. */
+/* The tile staging of the mixed form's sweep (no counterpart in the reference): tma = 1 (the default) stages each
+ * plane of a tile by TMA, cp.async.bulk.tensor boxes of 38 rows x 5 variables of the state arena landing on an
+ * mbarrier (bounded waits; a wait that gives up sets MB_E_TIMEOUT in the case status), converted into a 5-value
+ * FP32 tile (rho, u, v, w, T; p = rho R T where it is read) with the k-face fluxes carried in registers; tma = 0
+ * stages by per-thread coalesced loads into a 6-value tile (rho, u, v, w, p, T). The two differ in the FP32
+ * rounding of p (within the mixed form's accuracy); mb_autotune keeps the faster. TMA is used where a tensor map of
+ * the state buffer can be made: the buffer 16-byte aligned, ncell_total even, the map made outside any stream
+ * capture (at the first mb_stage / mb_step / mb_residual / mb_autotune on that buffer), MB_NO_TMA unset at
+ * mb_init. Invalidates the captured step graph when it changes the staging. */
+int mb_set_staging(mb_ctx* ctx, int tma);
+
+/* The mixed form's sweep launches of this context so far by staging: *tma_sweeps by TMA, *plain_sweeps by plain
+ * loads (launches recorded into a CUDA graph count once, at capture). */
 int mb_get_staging(const mb_ctx* ctx, int64_t* tma_sweeps, int64_t* plain_sweeps);
 
 /* Number of kernel launches this context has issued (for launch accounting). */

@@ -59,7 +59,9 @@ struct mb_ctx {
   // device memory; made outside any capture, never rewritten (a captured step keeps pointing at its maps)
   struct Tmap { const double* ptr; long long nc; void* dev; };
   std::vector<Tmap> tmaps;
-  bool no_tma = false;          // MB_NO_TMA set at mb_init: the scalar staging path (same tile values)
+  bool no_tma = false;          // MB_NO_TMA set at mb_init: no tensor maps (the TMA staging is never used)
+  bool stage_tma = true;        // the mixed sweep stages by TMA where a map exists (mb_set_staging, mb_autotune)
+  cudaStream_t tstream = 0;     // the stream the mesh tables are (re)built in the order of (build_tables)
   long long sweeps_tma = 0, sweeps_plain = 0;  // sweep launches of the mixed form by staging path
   double* d_acc4 = nullptr;     // RK4: conserved accumulator (ncell x 5)
   double* d_irs = nullptr;      // residual smoothing: two residual buffers (2 x ncell x 5)
@@ -93,11 +95,13 @@ struct mb_ctx {
     }                                            \
   } while (0)
 
+// a device copy of a host array, allocated and copied in the order of stream s (the stream-ordered allocator: a
+// table rebuilt while the previous tables are still read by queued work on s is released after that work)
 template <typename T>
-static int upload(T** dst, const T* src, size_t n) {
+static int upload(T** dst, const T* src, size_t n, cudaStream_t s = 0) {
   if (n == 0) { *dst = nullptr; return MB_OK; }
-  if (cudaMalloc((void**)dst, n * sizeof(T)) != cudaSuccess) return MB_E_NOMEM;
-  CK(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  if (cudaMallocAsync((void**)dst, n * sizeof(T), s) != cudaSuccess) return MB_E_NOMEM;
+  CK(cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, s));
   return MB_OK;
 }
 
@@ -171,6 +175,18 @@ extern "C" {
 
 const char* mb_version(void) { return "mose_b200 0.1 (sm_100a)"; }
 
+int mb_set_staging(mb_ctx* ctx, int tma) {
+  if (!ctx || tma < 0 || tma > 1) return MB_E_ARG;
+  if (ctx->stage_tma != (tma == 1)) {
+    ctx->stage_tma = tma == 1;
+    if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }  // a replay in flight completes
+    if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+    ctx->gP = nullptr;
+    ctx->gPO = nullptr;
+  }
+  return MB_OK;
+}
+
 int mb_get_staging(const mb_ctx* ctx, int64_t* tma_sweeps, int64_t* plain_sweeps) {
   if (!ctx || !tma_sweeps || !plain_sweeps) return MB_E_ARG;
   *tma_sweeps = ctx->sweeps_tma;
@@ -232,7 +248,8 @@ static int check_mesh(const mb_mesh* mesh, int ngroups) {
   for (int q = 0; q < mesh->nrec; ++q) {
     const mb_bc& r = mesh->rec[q];
     if (r.type != MB_BC_CONNECTION && r.type != MB_BC_EXTRAPOLATION && r.type != MB_BC_WALL &&
-        r.type != MB_BC_INFLOW && r.type != MB_BC_SYMMETRY && r.type != MB_BC_WALL_T && r.type != MB_BC_OUTLET)
+        r.type != MB_BC_INFLOW && r.type != MB_BC_SYMMETRY && r.type != MB_BC_WALL_T && r.type != MB_BC_OUTLET &&
+        r.type != MB_BC_NONE)
       return MB_E_UNSUPPORTED;
     if (r.blk < 0 || r.blk >= mesh->nblk || r.face < 1 || r.face > 6) return MB_E_ARG;
     if (mesh->blk[r.blk].group < 0) return MB_E_ARG;  // an external block carries no records
@@ -247,7 +264,7 @@ static void free_tables(mb_ctx* c) {
                   c->d_pgsrc, c->d_tiles_sweep, c->d_tiles_aux, c->d_recflux, c->d_brec, c->d_bcell,
                   c->d_physf, c->d_cubicf, c->d_tiles_km, c->d_idst, c->d_isrc};
   for (void* q : ptrs)
-    if (q) cudaFree(q);
+    if (q) cudaFreeAsync(q, c->tstream);  // after the work queued on the table stream that may still read them
   c->d_idst = nullptr; c->d_isrc = nullptr;
   for (int d = 0; d < 4; ++d) c->irs_off[d] = 0;
   c->d_physf = nullptr; c->d_cubicf = nullptr; c->d_tiles_km = nullptr; c->ntiles_km = 0;
@@ -267,7 +284,7 @@ static int sweep_unit(const mb_scheme* sc) {
 // record types with physical ghosts (Fill_Ghost_Cell_blk, Lib_Extrapolation.f90:643-730)
 static bool phys_type(int t) {
   return t == MB_BC_EXTRAPOLATION || t == MB_BC_INFLOW || t == MB_BC_WALL || t == MB_BC_SYMMETRY ||
-         t == MB_BC_WALL_T || t == MB_BC_OUTLET;
+         t == MB_BC_WALL_T || t == MB_BC_OUTLET || t == MB_BC_NONE;
 }
 
 // builds the mesh-dependent device tables from the host description (Setup_BC_Device, Mod_BC.f90:99-338) and
@@ -300,6 +317,7 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   }
   for (int q = 0; q < mesh->nrec; ++q) {
     const mb_bc& r = mesh->rec[q];
+    if (r.type == MB_BC_NONE) continue;  // no face flux: the sweep finds no record on that face
     DBlk& d = hb[r.blk];
     const int ax = (r.face - 1) / 2;
     const int nt = (ax == 0) ? d.n2 * d.n3 : (ax == 1 ? d.n1 * d.n3 : d.n1 * d.n2);
@@ -366,7 +384,7 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   // k-face records of mirrored blocks (their sweep computes those)
   std::vector<int> brec;
   for (int q = 0; q < mesh->nrec; ++q)
-    if (!(hb[mesh->rec[q].blk].kmirror && mesh->rec[q].face >= 5)) brec.push_back(q);
+    if (!(hb[mesh->rec[q].blk].kmirror && mesh->rec[q].face >= 5) && mesh->rec[q].type != MB_BC_NONE) brec.push_back(q);
   std::stable_sort(brec.begin(), brec.end(), [&](int a, int b) { return mesh->rec[a].type < mesh->rec[b].type; });
   std::vector<int> bcell(5 * brec.size());
   for (size_t q = 0; q < brec.size(); ++q) {
@@ -441,14 +459,14 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
         if (dst[q]) continue;
         for (auto& m : pool)
           if (m.buf && m.n == n[q]) { dst[q] = m.buf; m.buf = nullptr; break; }
-        if (!dst[q] && cudaMalloc((void**)&dst[q], n[q] * sizeof(float)) != cudaSuccess) {
-          for (auto& m : keep) cudaFree(m.buf);
-          for (auto& m : pool) if (m.buf) cudaFree(m.buf);
+        if (!dst[q] && cudaMallocAsync((void**)&dst[q], n[q] * sizeof(float), c->tstream) != cudaSuccess) {
+          for (auto& m : keep) cudaFreeAsync(m.buf, c->tstream);
+          for (auto& m : pool) if (m.buf) cudaFreeAsync(m.buf, c->tstream);
           c->geo32.clear();
           return MB_E_NOMEM;
         }
         keep.push_back({src[q], dst[q], n[q]});
-        if (to_float(src[q], dst[q], n[q], 0) != cudaSuccess) {
+        if (to_float(src[q], dst[q], n[q], c->tstream) != cudaSuccess) {
           c->geo32 = keep;  // every buffer stays owned by the context
           for (auto& m : pool)
             if (m.buf) c->geo32.push_back(m);
@@ -458,17 +476,16 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
       d.fm1f = dst[0]; d.fm2f = dst[1]; d.fm3f = dst[2]; d.dlf = dst[3]; d.mf = dst[4];
     }
     for (auto& m : pool)
-      if (m.buf) cudaFree(m.buf);
+      if (m.buf) cudaFreeAsync(m.buf, c->tstream);
     c->geo32 = keep;
-    CK(cudaDeviceSynchronize());
   }
   free_tables(c);
-  if ((rc = upload(&c->d_blk, hb.data(), hb.size())) != MB_OK) return rc;
-  if ((rc = upload(&c->d_recmap, recmap.data(), recmap.size())) != MB_OK) return rc;
-  if ((rc = upload(&c->d_rec, hr.data(), hr.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_blk, hb.data(), hb.size(), c->tstream)) != MB_OK) return rc;
+  if ((rc = upload(&c->d_recmap, recmap.data(), recmap.size(), c->tstream)) != MB_OK) return rc;
+  if ((rc = upload(&c->d_rec, hr.data(), hr.size(), c->tstream)) != MB_OK) return rc;
   c->hrec.assign(mesh->rec, mesh->rec + mesh->nrec);
   c->hdrec = hr;
-  if ((rc = upload(&c->d_grec, hg.data(), hg.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_grec, hg.data(), hg.size(), c->tstream)) != MB_OK) return rc;
   // Ghost passes in two halves where the record order changes values. The extrapolating ghosts of a face (walls in
   // the first pass, type 11 in the second) read the opposite face's ghost layers when the axis has at most two
   // cells, so of two records on opposite faces of one column the later one in record order must see the earlier
@@ -517,22 +534,23 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
   split(cubic, late_cubic, co);
   split(physf, late_phys, pof);
   split(cubicf, late_cubic, cof);
-  if ((rc = upload(&c->d_phys, phys.data(), phys.size())) != MB_OK) return rc;
-  if ((rc = upload(&c->d_cubic, cubic.data(), cubic.size())) != MB_OK) return rc;
-  if ((rc = upload(&c->d_physf, physf.data(), physf.size())) != MB_OK) return rc;
-  if ((rc = upload(&c->d_cubicf, cubicf.data(), cubicf.size())) != MB_OK) return rc;
-  if ((rc = upload(&c->d_cdst, cdst.data(), cdst.size())) != MB_OK) return rc;
-  if ((rc = upload(&c->d_csrc, csrc.data(), csrc.size())) != MB_OK) return rc;
-  if ((rc = upload(&c->d_pgsrc, pgsrc.data(), pgsrc.size())) != MB_OK) return rc;
-  if ((rc = upload(&c->d_tiles_sweep, ts.data(), ts.size())) != MB_OK) return rc;
-  if ((rc = upload(&c->d_tiles_aux, ta.data(), ta.size())) != MB_OK) return rc;
-  if ((rc = upload(&c->d_tiles_km, tk.data(), tk.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_phys, phys.data(), phys.size(), c->tstream)) != MB_OK) return rc;
+  if ((rc = upload(&c->d_cubic, cubic.data(), cubic.size(), c->tstream)) != MB_OK) return rc;
+  if ((rc = upload(&c->d_physf, physf.data(), physf.size(), c->tstream)) != MB_OK) return rc;
+  if ((rc = upload(&c->d_cubicf, cubicf.data(), cubicf.size(), c->tstream)) != MB_OK) return rc;
+  if ((rc = upload(&c->d_cdst, cdst.data(), cdst.size(), c->tstream)) != MB_OK) return rc;
+  if ((rc = upload(&c->d_csrc, csrc.data(), csrc.size(), c->tstream)) != MB_OK) return rc;
+  if ((rc = upload(&c->d_pgsrc, pgsrc.data(), pgsrc.size(), c->tstream)) != MB_OK) return rc;
+  if ((rc = upload(&c->d_tiles_sweep, ts.data(), ts.size(), c->tstream)) != MB_OK) return rc;
+  if ((rc = upload(&c->d_tiles_aux, ta.data(), ta.size(), c->tstream)) != MB_OK) return rc;
+  if ((rc = upload(&c->d_tiles_km, tk.data(), tk.size(), c->tstream)) != MB_OK) return rc;
   c->ntiles_km = (int)tk.size();
-  if ((rc = upload(&c->d_brec, brec.data(), brec.size())) != MB_OK) return rc;
-  if ((rc = upload(&c->d_bcell, bcell.data(), bcell.size())) != MB_OK) return rc;
+  if ((rc = upload(&c->d_brec, brec.data(), brec.size(), c->tstream)) != MB_OK) return rc;
+  if ((rc = upload(&c->d_bcell, bcell.data(), bcell.size(), c->tstream)) != MB_OK) return rc;
   c->nrec = (int)brec.size();
   if (mesh->nrec > 0 &&
-      cudaMalloc((void**)&c->d_recflux, (size_t)mesh->nrec * 2 * MB_NPRIM * sizeof(double)) != cudaSuccess)
+      cudaMallocAsync((void**)&c->d_recflux, (size_t)mesh->nrec * 2 * MB_NPRIM * sizeof(double), c->tstream) !=
+          cudaSuccess)
     return MB_E_NOMEM;
   c->ntiles_sweep = (int)ts.size();
   c->ntiles_aux = (int)ta.size();
@@ -588,8 +606,8 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
       }
     }
     c->irs_off[3] = (int)idst.size();
-    if ((rc = upload(&c->d_idst, idst.data(), idst.size())) != MB_OK) return rc;
-    if ((rc = upload(&c->d_isrc, isrc.data(), isrc.size())) != MB_OK) return rc;
+    if ((rc = upload(&c->d_idst, idst.data(), idst.size(), c->tstream)) != MB_OK) return rc;
+    if ((rc = upload(&c->d_isrc, isrc.data(), isrc.size(), c->tstream)) != MB_OK) return rc;
   }
   return MB_OK;
 }
@@ -737,11 +755,12 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
             32 * c->ty_sweep, occ, c->ntiles_sweep);
   }
 #undef TRY
+  CK(cudaStreamSynchronize(0));  // the tables were built in the order of the legacy stream: ready for any stream
   *out = c;
   return MB_OK;
 }
 
-int mb_reconfigure(mb_ctx* ctx, const mb_mesh* mesh) {
+static int reconfigure(mb_ctx* ctx, const mb_mesh* mesh, cudaStream_t s, bool device_sync) {
   if (!ctx || !mesh) return MB_E_ARG;
   if (mesh->ncell_total > ctx->ncell) return MB_E_ARG;
   const int ng = mesh->ngroups > 0 ? mesh->ngroups : 1;
@@ -749,12 +768,23 @@ int mb_reconfigure(mb_ctx* ctx, const mb_mesh* mesh) {
   int rc = check_mesh(mesh, ctx->ngroups);
   if (rc != MB_OK) return rc;
   CK(cudaSetDevice(ctx->device));
-  CK(cudaDeviceSynchronize());  // the old tables may still be read by queued work
+  if (device_sync) CK(cudaDeviceSynchronize());  // the old tables may still be read by queued work on any stream
+  // a step graph in flight is freed when it completes; the next mb_step captures one over the new tables
   if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
   if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
   ctx->gP = nullptr;
   ctx->gPO = nullptr;
-  return build_tables(ctx, mesh);
+  ctx->tstream = s;
+  rc = build_tables(ctx, mesh);
+  ctx->tstream = 0;
+  if (device_sync) CK(cudaStreamSynchronize(s));
+  return rc;
+}
+
+int mb_reconfigure(mb_ctx* ctx, const mb_mesh* mesh) { return reconfigure(ctx, mesh, 0, true); }
+
+int mb_reconfigure_async(mb_ctx* ctx, const mb_mesh* mesh, void* stream) {
+  return reconfigure(ctx, mesh, (cudaStream_t)stream, false);
 }
 
 int mb_set_record_params(mb_ctx* ctx, int rec, const double* q, void* stream) {
@@ -886,9 +916,9 @@ static int sweep_on(mb_ctx* c, const DTile* t, int n, int persistent, int mode, 
   Params p = c->p;
   p.irk = irk;
   p.queue = persistent ? c->d_queue : nullptr;
-  p.tmap = tmap_of(c, Pin, s, false);
-  p.tmap_old = (mode == MODE_UPDATE) ? tmap_of(c, Pold, s, false) : nullptr;
-  if (c->sc.precision == MB_PREC_MIXED) ((p.tmap || p.tmap_old) ? c->sweeps_tma : c->sweeps_plain) += 1;
+  p.stg = (c->sc.precision == MB_PREC_MIXED && c->stage_tma) ? STG_TMA : STG_PLAIN;
+  p.tmap = p.stg == STG_TMA ? tmap_of(c, Pin, s, false) : nullptr;
+  if (c->sc.precision == MB_PREC_MIXED) (p.tmap ? c->sweeps_tma : c->sweeps_plain) += 1;
   const double rkc = irk > 0 ? rkc_of(c->sc.n_rk, irk) : 0.0;
   cudaError_t e;
   e = MB_BY_FORM(c->sc.precision, sweep_unit(&c->sc), , (p, t, n, mode, Pin, Pold, Pout, Rout, rkc, last, km, s));
@@ -1144,6 +1174,15 @@ static int stage(mb_ctx* c, double* P, double* PO, int irk, cudaStream_t s) {
   return MB_OK;
 }
 
+int mb_stage_input(mb_ctx* ctx, double* P, double* PO, int irk, double** in) {
+  if (!ctx || !P || !PO || !in || irk < 1 || irk > ctx->sc.n_rk) return MB_E_ARG;
+  const double* i;
+  double* o;
+  stage_buffers(ctx->sc.n_rk, irk, P, PO, ctx->d_scratch, &i, &o);
+  *in = const_cast<double*>(i);
+  return MB_OK;
+}
+
 int mb_stage_begin(mb_ctx* ctx, double* P, double* PO, int irk, void* stream) {
   if (!ctx || !P || !PO || irk < 1 || irk > ctx->sc.n_rk) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
@@ -1329,6 +1368,18 @@ int mb_autotune(mb_ctx* ctx, const double* P, void* stream) {
   ctx->persistent = ms_pers < ms_plain ? 1 : 0;
   ctx->tuned_ms = std::min(ms_plain, ms_pers);
   const std::vector<DTile>& use = ctx->persistent ? sorted : all;
+  // the mixed form: the tile staging (TMA boxes into a 5-value tile, or plain loads into a 6-value tile) that is
+  // faster on this state and mesh
+  float ms_stage[2] = {0.f, 0.f};
+  if (ctx->sc.precision == MB_PREC_MIXED && tmap_of(ctx, P, s, true)) {
+    const bool keep = ctx->stage_tma;
+    for (int m = 0; m < 2; ++m) {
+      ctx->stage_tma = m == 1;
+      if ((rc = time_sweep(ctx, use, ctx->persistent, P, 3, s, &ms_stage[m])) != MB_OK) { ctx->stage_tma = keep; return rc; }
+    }
+    ctx->stage_tma = ms_stage[1] < ms_stage[0];
+    ctx->tuned_ms = std::min(ms_stage[0], ms_stage[1]);
+  }
   if (ctx->d_tiles_sweep) cudaFree(ctx->d_tiles_sweep);
   ctx->d_tiles_sweep = nullptr;
   if ((rc = upload(&ctx->d_tiles_sweep, use.data(), use.size())) != MB_OK) return rc;
@@ -1338,8 +1389,10 @@ int mb_autotune(mb_ctx* ctx, const double* P, void* stream) {
   ctx->gP = nullptr;
   ctx->gPO = nullptr;
   if (getenv("MB_REPORT"))
-    fprintf(stderr, "[mose_b200] autotune: k-chunk %d, %s sweep (plain %.3f ms, persistent %.3f ms), %d tiles\n",
-            ctx->kc3, ctx->persistent ? "persistent" : "plain", ms_plain, ms_pers, ctx->ntiles_sweep);
+    fprintf(stderr, "[mose_b200] autotune: k-chunk %d, %s sweep (plain %.3f ms, persistent %.3f ms), %d tiles, "
+                    "staging %s (plain loads %.3f ms, TMA %.3f ms)\n",
+            ctx->kc3, ctx->persistent ? "persistent" : "plain", ms_plain, ms_pers, ctx->ntiles_sweep,
+            ctx->stage_tma ? "TMA" : "plain loads", ms_stage[0], ms_stage[1]);
   return MB_OK;
 }
 

@@ -37,33 +37,23 @@ template <typename R> MB_HD R cvt(double x) { return (R)x; }
 // value less per cell leaves room in shared memory for the TMA staging buffer at 3 CTAs per SM).
 // Layout [slot][value][jj][ii], ii fastest.
 constexpr int TXH = 36;
-#ifndef MB_TILE5
-#define MB_TILE5 0
-#endif
-template <typename R> struct TileNV { static constexpr int v = (sizeof(R) == 4 && MB_TILE5) ? 5 : 6; };
-// TMA staging in the mixed form: of the halo tile of the sweep's input (MB_TMA_HALO) and of the old state the update
-// reads at the tile's own cells (MB_TMA_OLD)
-#ifndef MB_TMA_HALO
-#define MB_TMA_HALO 0
-#endif
-#ifndef MB_TMA_OLD
-#define MB_TMA_OLD 1
-#endif
-template <typename R> struct TmaOn {
-  static constexpr bool halo = sizeof(R) == 4 && MB_TMA_HALO;
-  static constexpr bool old = sizeof(R) == 4 && MB_TMA_OLD;
+// The staging of a sweep's state tile, a template parameter of the sweep (STG) chosen per context (mb_autotune,
+// mb_set_staging): STG_PLAIN, per-thread coalesced loads into a 6-value tile (rho_s, u, v, w, p, T) with the k-face
+// fluxes of two planes in shared memory; STG_TMA (the mixed form), TMA boxes of the state arena landing on an mbarrier
+// in a staging buffer, converted into a 5-value tile (rho_s, u, v, w, T; p = rho Rg T where it is read) with the
+// k-face fluxes carried in registers, which together leave room for the staging buffer at 3 CTAs per SM.
+enum { STG_PLAIN = 0, STG_TMA = 1 };
+template <typename R, int STG> struct Stg {
+  static constexpr bool tma = STG == STG_TMA && sizeof(R) == 4;
+  static constexpr int nv = tma ? 5 : 6;   // values per staged cell
+  static constexpr bool kreg = tma;        // k-face fluxes in registers
 };
-// the k-face fluxes of the mixed form live in registers (sweep_tile)
-#ifndef MB_KFACE_REG
-#define MB_KFACE_REG 1
-#endif
-template <typename R> struct KfaceReg { static constexpr bool on = sizeof(R) == 4 && MB_KFACE_REG; };
 
-template <typename R, int TY>
+template <typename R, int TY, int NV_ = 6>
 struct Tile {
   R* base;
   R rg;                                              // the gas constant of the single species (5-value tile)
-  static constexpr int NVT = TileNV<R>::v;
+  static constexpr int NVT = NV_;
   static constexpr int VS = (TY + 4) * TXH;          // stride between the values of one cell
   MB_HD int off(int slot, int jj, int ii) const { return slot * NVT * VS + jj * TXH + ii; }
   // value var (0..4: rho_s, u, v, w, p; 5: T) of the cell at offset o
@@ -82,8 +72,8 @@ MB_HD int slot_of(int kk) { return (kk + 8) & 3; }
 // (diff_cuf_kernels.inc:11-87 + diff_physics.inc) into out[5..9]. (ii, jj) are the tile coordinates of the
 // cell, sk the slot of plane k. The gradients are built per variable in registers and placed on the
 // axes by d (ia = d; the two tangential axes in increasing order), as the reference's Grad(:, ia/ib/ic).
-template <typename R, int TY, bool VISC, int RS = 0, int LIM = 0, bool KM = false>
-MB_HD void face_flux(const Params& p, const DBlk& b, const Tile<R, TY>& T, int d, int i, int j, int k, int ii,
+template <typename R, int TY, bool VISC, int RS = 0, int LIM = 0, bool KM = false, int NVT = 6>
+MB_HD void face_flux(const Params& p, const DBlk& b, const Tile<R, TY, NVT>& T, int d, int i, int j, int k, int ii,
                      int jj, R* out) {
   // a mirrored block (one cell deep in k, extrapolated k faces) reads its k = 1 plane for the k ghosts
   const int skm = slot_of(KM ? k : k - 1), sk = slot_of(k), sk1 = slot_of(KM ? k : k + 1),
@@ -1338,14 +1328,14 @@ __device__ __forceinline__ void report_bad_state(DevState* st, int blk, int i, i
 // Stage plane kk of the tile window: cells (i0-2 .. i0+33) x (j0-2 .. j0+TY+1), those inside the padded block and
 // within jext rows of the interior (jext < 2 for a block one cell deep in j: no j-faces, so only the viscous
 // transverse stencil reads the ghost rows); the others hold zeros.
-template <typename R, int TY>
-__device__ __forceinline__ void put_cell(const Params& p, const Tile<R, TY>& T, int o, R* vals) {
+template <typename R, int TY, int NVT>
+__device__ __forceinline__ void put_cell(const Params& p, const Tile<R, TY, NVT>& T, int o, R* vals) {
   R rho, Tc;
   cell_rho_T<R>(p, vals[0], vals[MB_IPR], rho, Tc);
-  constexpr int VS = Tile<R, TY>::VS;
+  constexpr int VS = Tile<R, TY, NVT>::VS;
 #pragma unroll
   for (int v = 0; v < 4; ++v) T.base[o + v * VS] = vals[v];
-  if (Tile<R, TY>::NVT == 6) {
+  if (NVT == 6) {
     T.base[o + 4 * VS] = vals[MB_IPR];
     T.base[o + 5 * VS] = Tc;
   } else {
@@ -1353,9 +1343,9 @@ __device__ __forceinline__ void put_cell(const Params& p, const Tile<R, TY>& T, 
   }
 }
 
-template <typename R, int TY>
+template <typename R, int TY, int NVT>
 __device__ __forceinline__ void stage_plane(const Params& p, const DBlk& b, const double* __restrict__ P,
-                                            const Tile<R, TY>& T, int i0, int j0, int kk, int jext) {
+                                            const Tile<R, TY, NVT>& T, int i0, int j0, int kk, int jext) {
   const int sl = slot_of(kk);
   const long long nc = p.nc;
   for (int c = threadIdx.x; c < TXH * (TY + 4); c += blockDim.x) {
@@ -1367,10 +1357,10 @@ __device__ __forceinline__ void stage_plane(const Params& p, const DBlk& b, cons
       const long long r = row(b, i, j, kk);
 #pragma unroll
       for (int s = 0; s < MB_NP; ++s) vals[s] = cvt<R>(ld(P + r + s * nc));
-      put_cell<R, TY>(p, T, o, vals);
+      put_cell<R, TY, NVT>(p, T, o, vals);
     } else {
 #pragma unroll
-      for (int v = 0; v < Tile<R, TY>::NVT; ++v) T.base[o + v * Tile<R, TY>::VS] = (R)0;
+      for (int v = 0; v < NVT; ++v) T.base[o + v * Tile<R, TY, NVT>::VS] = (R)0;
     }
   }
 }
@@ -1434,35 +1424,18 @@ __device__ __forceinline__ void tma_issue_plane(const Params& p, const DBlk& b, 
   }
 }
 
-// the TMA staging state of a CTA: the halo-plane buffer and the old-state buffer, their mbarriers and the parity
-// each is waited for next
+// the TMA staging state of a CTA: the staging buffer of the landing plane, its mbarrier and the parity it is waited
+// for next
 struct TmaStage {
   unsigned char* halo;
-  unsigned char* old;
   unsigned long long* bar_halo;
-  unsigned long long* bar_old;
-  unsigned ph_halo, ph_old;
+  unsigned ph_halo;
 };
 
-// warp 0 issues the TY row boxes of the old state at the tile's own cells of plane k (one box per j-row: 38 rows
-// from the even row at or below the row of cell i0, so the 32 cells sit at offset row & 1)
-template <int TY>
-__device__ __forceinline__ void tma_issue_old(const Params& p, const DBlk& b, unsigned char* buf,
-                                              unsigned long long* bar, int i0, int j0, int k) {
-  if (threadIdx.x >= 32) return;
-  if (threadIdx.x == 0) mbar_expect(bar, (unsigned)(TY * MB_NP * TMA_BOX_ROWS * sizeof(double)));
-  __syncwarp();
-  const int jj = threadIdx.x;
-  if (jj < TY) {
-    const long long r = row(b, i0, j0 + jj, k);
-    tma_load_2d(buf + jj * TMA_ROW_BYTES, p.tmap_old, (int)(r & ~1LL), 0, bar);
-  }
-}
-
 // convert the landed raw plane into the tile slot of plane kk (the same cells and values as stage_plane)
-template <typename R, int TY>
+template <typename R, int TY, int NVT>
 __device__ __forceinline__ void stage_plane_raw(const Params& p, const DBlk& b, const unsigned char* raw,
-                                                const Tile<R, TY>& T, int i0, int j0, int kk, int jext) {
+                                                const Tile<R, TY, NVT>& T, int i0, int j0, int kk, int jext) {
   const int sl = slot_of(kk);
   for (int c = threadIdx.x; c < TXH * (TY + 4); c += blockDim.x) {
     const int jj = c / TXH, ii = c - jj * TXH;
@@ -1474,10 +1447,10 @@ __device__ __forceinline__ void stage_plane_raw(const Params& p, const DBlk& b, 
       const double* src = reinterpret_cast<const double*>(raw + jj * TMA_ROW_BYTES) + sh + ii;
 #pragma unroll
       for (int s = 0; s < MB_NP; ++s) vals[s] = cvt<R>(src[s * TMA_BOX_ROWS]);
-      put_cell<R, TY>(p, T, o, vals);
+      put_cell<R, TY, NVT>(p, T, o, vals);
     } else {
 #pragma unroll
-      for (int v = 0; v < Tile<R, TY>::NVT; ++v) T.base[o + v * Tile<R, TY>::VS] = (R)0;
+      for (int v = 0; v < NVT; ++v) T.base[o + v * Tile<R, TY, NVT>::VS] = (R)0;
     }
   }
 }
@@ -1485,7 +1458,7 @@ __device__ __forceinline__ void stage_plane_raw(const Params& p, const DBlk& b, 
 // One tile of the fused stage (the body of k_sweep).
 // With TMA staging (the mixed form, p.tmap set) raw is the staging buffer and bar its mbarrier, phase the parity the
 // CTA waits for next; false: a bounded wait gave up (the clock's code is set to MB_E_TIMEOUT) and the CTA must stop.
-template <typename R, int TY, bool VISC, int MODE, int RS, int LIM, bool KM>
+template <typename R, int TY, bool VISC, int MODE, int RS, int LIM, bool KM, int STG>
 __device__ __forceinline__ bool sweep_tile(const Params& p, const DTile t, const double* __restrict__ Pin,
                                            const double* Pold, double* Pout, double* Rout, double rkc, int last,
                                            unsigned char* smem_raw, double* sred, double* s_res, TmaStage& ts) {
@@ -1499,16 +1472,17 @@ __device__ __forceinline__ bool sweep_tile(const Params& p, const DTile t, const
   constexpr int NS = NET ? MB_NP : NF;
   typedef R RowI[33][NS];
   typedef R RowJ[32][NS];
-  Tile<R, TY> T;
+  constexpr int NVT = Stg<R, STG>::nv;
+  Tile<R, TY, NVT> T;
   T.base = reinterpret_cast<R*>(smem_raw);                                       // [4][NVT][TY+4][36]
   T.rg = (R)p.ri;
-  unsigned char* fbase = smem_raw + sizeof(R) * 4 * Tile<R, TY>::NVT * (TY + 4) * TXH;
+  unsigned char* fbase = smem_raw + sizeof(R) * 4 * NVT * (TY + 4) * TXH;
   RowI* sFi = reinterpret_cast<RowI*>(fbase);                                     // [TY][33][NS]
   RowJ* sFj = reinterpret_cast<RowJ*>(fbase + sizeof(R) * TY * 33 * NS);          // [TY+1][32][NS]
   // the k-faces: the face above a cell is computed by the thread of that cell and is the face below it on the next
   // plane, so the mixed form carries both in that thread's registers (kup, kdn: no shared buffer, which leaves room
   // for the TMA staging buffer at 3 CTAs per SM); the FP64 forms keep them in shared memory (two planes)
-  constexpr bool KREG = KfaceReg<R>::on;
+  constexpr bool KREG = Stg<R, STG>::kreg;
   RowJ* sFk0 = reinterpret_cast<RowJ*>(fbase + sizeof(R) * (TY * 33 + (TY + 1) * 32) * NS);  // [2][TY][32][NS]
   R kup[NS], kdn[NS];
 #pragma unroll
@@ -1516,9 +1490,8 @@ __device__ __forceinline__ bool sweep_tile(const Params& p, const DTile t, const
   const DBlk b = p.blk[t.blk];
   DevState* st = p.st + b.grp;
   if (MODE == MODE_UPDATE && st->done) return true;  // the case has reached its stop time (uniform over the CTA)
-  const bool tma = TmaOn<R>::halo && p.tmap != nullptr;  // TMA staging of the halo tile (uniform over the CTA)
-  // TMA staging of the old state at the tile's own cells, one plane per loop iteration (uniform over the CTA)
-  const bool tmo = TmaOn<R>::old && MODE == MODE_UPDATE && p.tmap_old != nullptr;
+  // TMA staging (uniform over the CTA; without a map the TMA form stages the same tile values by plain loads)
+  const bool tma = Stg<R, STG>::tma && p.tmap != nullptr;
   const int tid = threadIdx.x;
   const int tx = tid & 31, ty = tid >> 5;
   const int i = t.i0 + tx, j = t.j0 + ty;
@@ -1546,10 +1519,10 @@ __device__ __forceinline__ bool sweep_tile(const Params& p, const DTile t, const
       const bool ok = mbar_wait(bar, phase);
       phase ^= 1u;
       if (gave_up(ok)) return false;
-      stage_plane_raw<R, TY>(p, b, raw, T, t.i0, t.j0, kk, jext);
+      stage_plane_raw<R, TY, NVT>(p, b, raw, T, t.i0, t.j0, kk, jext);
       __syncthreads();  // the staging buffer is free again
     } else {
-      stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, kk, jext);
+      stage_plane<R, TY, NVT>(p, b, Pin, T, t.i0, t.j0, kk, jext);
     }
   }
   // the first plane of the loop in flight while the k-face below is computed
@@ -1557,7 +1530,7 @@ __device__ __forceinline__ bool sweep_tile(const Params& p, const DTile t, const
   __syncthreads();
   if (own && t.k0 > 1) {
     R out[NF];
-    face_flux<R, TY, VISC, RS, LIM, KM>(p, b, T, 2, i, j, t.k0 - 1, tx + 2, ty + 2, out);
+    face_flux<R, TY, VISC, RS, LIM, KM, NVT>(p, b, T, 2, i, j, t.k0 - 1, tx + 2, ty + 2, out);
     if (KREG) {
 #pragma unroll
       for (int q = 0; q < NS; ++q) kdn[q] = NET ? out[q] - out[MB_NP + q] : out[q];
@@ -1575,16 +1548,14 @@ __device__ __forceinline__ bool sweep_tile(const Params& p, const DTile t, const
         const bool ok = mbar_wait(bar, phase);
         phase ^= 1u;
         if (gave_up(ok)) return false;
-        stage_plane_raw<R, TY>(p, b, raw, T, t.i0, t.j0, k + 2, jext);
+        stage_plane_raw<R, TY, NVT>(p, b, raw, T, t.i0, t.j0, k + 2, jext);
       } else {
-        stage_plane<R, TY>(p, b, Pin, T, t.i0, t.j0, k + 2, jext);
+        stage_plane<R, TY, NVT>(p, b, Pin, T, t.i0, t.j0, k + 2, jext);
       }
     }
     __syncthreads();  // plane k+2 staged, and every pass 2 of plane k-1 done (the flux buffers are free)
     // the next plane's boxes fly under this plane's faces and pass 2 (the staging buffer was read before the barrier)
     if (tma && k + 3 <= b.n3 + kext && k + 1 < t.k1) tma_issue_plane<TY>(p, b, raw, bar, t.i0, t.j0, k + 3);
-    // the old state of this plane's cells flies under the face work (its buffer was last read by pass 2 of k-1)
-    if (tmo) tma_issue_old<TY>(p, b, ts.old, ts.bar_old, t.i0, t.j0, k);
     // ---- face tasks of this plane through one call site: 0 = i-face #tid, 1 = extra i-faces (last warp,
     // lanes < TY), 2 = j-face #tid, 3 = extra j-face row (warp 0), 4 = the k-face above
 #pragma unroll 1
@@ -1611,7 +1582,7 @@ __device__ __forceinline__ bool sweep_tile(const Params& p, const DTile t, const
       }
       if (d < 0) continue;
       R out[NF];
-      face_flux<R, TY, VISC, RS, LIM, KM>(p, b, T, d, fi, fj, k, ii, jj, out);
+      face_flux<R, TY, VISC, RS, LIM, KM, NVT>(p, b, T, d, fi, fj, k, ii, jj, out);
       if (KREG && task == 4) {
 #pragma unroll
         for (int q = 0; q < NS; ++q) kup[q] = NET ? out[q] - out[MB_NP + q] : out[q];
@@ -1621,11 +1592,6 @@ __device__ __forceinline__ bool sweep_tile(const Params& p, const DTile t, const
       }
     }
     __syncthreads();
-    if (tmo) {
-      const bool ok = mbar_wait(ts.bar_old, ts.ph_old);
-      ts.ph_old ^= 1u;
-      if (gave_up(ok)) return false;
-    }
     // the residual diagnostic of the last stage: (new - old)^2 of this thread's cell, in the flux type (the warps'
     // partial sums in FP32 in the mixed form: the diagnostic to FP32 accuracy there)
     R rsq[MB_NP];
@@ -1695,14 +1661,8 @@ __device__ __forceinline__ bool sweep_tile(const Params& p, const DTile t, const
       } else {
         double pc[MB_NP], po[MB_NP], pn[MB_NP];
 #pragma unroll
-        if (tmo) {
-          const double* src = reinterpret_cast<const double*>(ts.old + ty * TMA_ROW_BYTES) + (int)(row(b, t.i0, j, k) & 1) + tx;
 #pragma unroll
-          for (int s = 0; s < MB_NP; ++s) { pc[s] = ld(Pin + r + s * p.nc); po[s] = src[s * TMA_BOX_ROWS]; }
-        } else {
-#pragma unroll
-          for (int s = 0; s < MB_NP; ++s) { pc[s] = ld(Pin + r + s * p.nc); po[s] = Pold[r + s * p.nc]; }
-        }
+        for (int s = 0; s < MB_NP; ++s) { pc[s] = ld(Pin + r + s * p.nc); po[s] = Pold[r + s * p.nc]; }
         double rho, Tc;
         if (Fast<R>::on) Tc = pc[MB_IPR] / pc[0] * p.iri;  // one species: R_mix = R
         else cell_rho_T(p, pc[0], pc[MB_IPR], rho, Tc);
@@ -1771,16 +1731,16 @@ __device__ __forceinline__ bool sweep_tile(const Params& p, const DTile t, const
 
 // shared memory of the sweep: the state tile and the face-flux buffers (sweep_smem_core), and in the mixed form the
 // TMA staging buffer of one plane (TY+4 row slots) with its 128-byte alignment slack
-template <typename R, int TY, bool VISC>
+template <typename R, int TY, bool VISC, int STG = STG_PLAIN>
 MB_HD constexpr size_t sweep_smem_core() {
-  return sizeof(R) * ((size_t)4 * TileNV<R>::v * (TY + 4) * TXH +
-                      (size_t)(TY * 33 + (TY + 1) * 32 + (KfaceReg<R>::on ? 0 : 2 * TY * 32)) *
+  return sizeof(R) * ((size_t)4 * Stg<R, STG>::nv * (TY + 4) * TXH +
+                      (size_t)(TY * 33 + (TY + 1) * 32 + (Stg<R, STG>::kreg ? 0 : 2 * TY * 32)) *
                           ((VISC && !Fast<R>::on) ? 2 * MB_NP : MB_NP));
 }
-template <typename R, int TY, bool VISC>
+template <typename R, int TY, bool VISC, int STG = STG_PLAIN>
 MB_HD constexpr size_t sweep_smem() {
-  return sweep_smem_core<R, TY, VISC>() + (TmaOn<R>::halo ? (size_t)128 + (size_t)(TY + 4) * TMA_ROW_BYTES : 0) +
-         (TmaOn<R>::old ? (size_t)128 + (size_t)TY * TMA_ROW_BYTES : 0);
+  return sweep_smem_core<R, TY, VISC, STG>() +
+         (Stg<R, STG>::tma ? (size_t)128 + (size_t)(TY + 4) * TMA_ROW_BYTES : 0);
 }
 
 // The fused stage over a tile list (KM: the tiles of mirrored one-plane blocks, a separate instantiation so that
@@ -1789,7 +1749,8 @@ MB_HD constexpr size_t sweep_smem() {
 // work queue: a grid of about one wave of CTAs, each taking the next tile from the counter p.queue (zeroed
 // before the launch) until the list is exhausted. MINB: resident CTAs per SM the register allocation must
 // allow (launch bounds).
-template <typename R, int TY, bool VISC, int MODE, int RS, int LIM, int MINB, bool KM = false, int VAR = 0>
+template <typename R, int TY, bool VISC, int MODE, int RS, int LIM, int MINB, bool KM = false, int VAR = 0,
+          int STG = STG_PLAIN>
 __global__ void __launch_bounds__(32 * TY, MINB)
 k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pin, const double* Pold, double* Pout,
         double* Rout, double rkc, int last) {
@@ -1797,34 +1758,24 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
   __shared__ double sred[32];
   __shared__ double s_res[8 * MB_NP];  // per warp (at most 8) and variable: the tile's residual sums
   __shared__ int s_next;
-  __shared__ __align__(8) unsigned long long s_bar[2];  // TMA staging: the mbarriers of the halo plane, the old state
+  __shared__ __align__(8) unsigned long long s_bar;  // TMA staging: the mbarrier of the landing plane
   static_assert(TY <= 8, "one residual slot per warp");
-  TmaStage ts{nullptr, nullptr, &s_bar[0], &s_bar[1], 0u, 0u};
-  if (TmaOn<R>::halo || TmaOn<R>::old) {  // the staging buffers after the tile and the flux buffers, 128-byte aligned
-    unsigned char* q = smem_raw + sweep_smem_core<R, TY, VISC>();
-    if (TmaOn<R>::halo) {
-      ts.halo = q + ((128u - (smem_addr(q) & 127u)) & 127u);
-      q += 128 + (TY + 4) * TMA_ROW_BYTES;
-    }
-    if (TmaOn<R>::old) ts.old = q + ((128u - (smem_addr(q) & 127u)) & 127u);
-    const void* maps[2] = {TmaOn<R>::halo ? p.tmap : nullptr,
-                           (TmaOn<R>::old && MODE == MODE_UPDATE) ? p.tmap_old : nullptr};
-    if (maps[0] || maps[1]) {
-      if (threadIdx.x == 0) {
-        if (maps[0]) mbar_init(&s_bar[0]);
-        if (maps[1]) mbar_init(&s_bar[1]);
-      }
-      // the maps were written to device memory by a host copy: the lanes that issue copies order them into the
+  TmaStage ts{nullptr, &s_bar, 0u};
+  if (Stg<R, STG>::tma) {  // the staging buffer after the tile and the flux buffers, 128-byte aligned
+    unsigned char* q = smem_raw + sweep_smem_core<R, TY, VISC, STG>();
+    ts.halo = q + ((128u - (smem_addr(q) & 127u)) & 127u);
+    if (p.tmap) {
+      if (threadIdx.x == 0) mbar_init(&s_bar);
+      // the map was written to device memory by a host copy: the lanes that issue copies order it into the
       // tensor-map proxy before their first use
-      for (int m = 0; m < 2; ++m)
-        if (maps[m] && threadIdx.x < 32)
-          asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(maps[m]) : "memory");
+      if (threadIdx.x < 32)
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(p.tmap) : "memory");
       __syncthreads();
     }
   }
   if (!p.queue) {
-    sweep_tile<R, TY, VISC, MODE, RS, LIM, KM>(p, tiles[blockIdx.x], Pin, Pold, Pout, Rout, rkc, last, smem_raw, sred,
-                                                s_res, ts);
+    sweep_tile<R, TY, VISC, MODE, RS, LIM, KM, STG>(p, tiles[blockIdx.x], Pin, Pold, Pout, Rout, rkc, last, smem_raw,
+                                                     sred, s_res, ts);
     return;
   }
   for (;;) {
@@ -1832,8 +1783,8 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
     __syncthreads();
     const int tix = s_next;
     if (tix >= p.ntiles_run) break;
-    if (!sweep_tile<R, TY, VISC, MODE, RS, LIM, KM>(p, tiles[tix], Pin, Pold, Pout, Rout, rkc, last, smem_raw, sred,
-                                                     s_res, ts))
+    if (!sweep_tile<R, TY, VISC, MODE, RS, LIM, KM, STG>(p, tiles[tix], Pin, Pold, Pout, Rout, rkc, last, smem_raw,
+                                                          sred, s_res, ts))
       break;
     __syncthreads();  // the tile's shared memory is free and s_next may be overwritten
   }

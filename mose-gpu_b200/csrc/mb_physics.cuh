@@ -116,9 +116,9 @@ struct Params {
   int lim, rs, visc, ndir, dt_additive, guard, state_check;
   double cfl, vnn, prandtl, schmidt, mco;
   void* recflux;           // boundary-record contributions [record][10] in the flux type (k_records)
-  const void* tmap;        // mixed form: the TMA tensor map (CUtensorMap, device memory) of the sweep's input state as
-                           // a 2-D tensor of (ncell_total rows, 5 variables), or null (the scalar staging path)
-  const void* tmap_old;    // the same for the old state of the update (Pold), or null
+  int stg;                 // mixed form: the tile staging of the sweep (STG_PLAIN 0, STG_TMA 1 of mb_engine.cuh)
+  const void* tmap;        // STG_TMA: the TMA tensor map (CUtensorMap, device memory) of the sweep's input state as a
+                           // 2-D tensor of (ncell_total rows, 5 variables), or null (the same tile by plain loads)
   int* queue;              // persistent sweep: the tile counter (null: one CTA per tile)
   int ntiles_run;          // tiles of the launch (persistent sweep)
   int pgrid;               // CTAs of a persistent launch (resident CTAs per SM x SMs)

@@ -31,6 +31,7 @@ STATUS_NAMES = {
     MB_E_NODEV: "no CUDA device",
 }
 
+BC_NONE = 0          # no condition (bc.txt 0): zero-gradient ghosts, no face flux
 BC_CONNECTION = 1
 BC_INFLOW = 4
 BC_WALL = 5

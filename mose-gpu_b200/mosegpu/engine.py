@@ -46,6 +46,8 @@ def load_library():
     L.mb_get_status.argtypes = [vp, C.POINTER(abi.MBStatus)]
     L.mb_profile_stage.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), vp]
     L.mb_reconfigure.argtypes = [vp, C.POINTER(abi.MBMesh)]
+    L.mb_reconfigure_async.argtypes = [vp, C.POINTER(abi.MBMesh), vp]
+    L.mb_reconfigure_async.restype = C.c_int
     L.mb_group_reset.argtypes = [vp, C.c_int, C.POINTER(abi.MBGroup), vp, vp]
     L.mb_set_record_params.argtypes = [vp, C.c_int, C.POINTER(C.c_double), vp]
     L.mb_get_group_status.argtypes = [vp, C.c_int, C.c_int, C.POINTER(abi.MBStatus)]
@@ -57,12 +59,16 @@ def load_library():
     L.mb_copy_dtmin.argtypes = [vp, C.c_int, vp, C.c_int, vp]
     L.mb_step_start.argtypes = [vp, vp]
     L.mb_stage_begin.argtypes = [vp, vp, vp, C.c_int, vp]
+    L.mb_stage_input.argtypes = [vp, vp, vp, C.c_int, C.POINTER(vp)]
+    L.mb_stage_input.restype = C.c_int
     L.mb_stage_end.argtypes = [vp, vp, vp, C.c_int, vp]
     L.mb_pack_rows.argtypes = [vp, C.c_int64, vp, C.c_int32, vp, vp]
     L.mb_unpack_rows.argtypes = [vp, C.c_int64, vp, C.c_int32, vp, vp]
     for f in ("mb_step_prepare", "mb_copy_dtmin", "mb_step_start", "mb_stage_begin", "mb_stage_end", "mb_pack_rows",
               "mb_unpack_rows"):
         getattr(L, f).restype = C.c_int
+    L.mb_set_staging.argtypes = [vp, C.c_int]
+    L.mb_set_staging.restype = C.c_int
     L.mb_get_staging.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.mb_get_staging.restype = C.c_int
     L.mb_launch_count.argtypes = [vp]
@@ -154,6 +160,10 @@ class Engine:
 
     def state(self):
         return self.P.cpu().numpy()
+
+    def set_staging(self, tma):
+        """The mixed sweep's tile staging: 1 TMA (5-value tile), 0 plain loads (6-value tile) (mb_set_staging)."""
+        _check(self.lib.mb_set_staging(self.ctx, int(tma)), "mb_set_staging")
 
     def staging(self):
         """(sweep launches staged by TMA, by plain loads) of the mixed form so far (mb_get_staging)."""

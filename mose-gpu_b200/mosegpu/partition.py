@@ -19,7 +19,9 @@ step (mpi_allreduce_min_r8, Mod_MPI.f90:571-581). Here:
                     owner's arena; the receiver writes it at the same offset inside its external copy.
   EngineRank        one rank's blocks on its GPU: mb_step_prepare, MIN all-reduce of the clock minimum
                     (mb_copy_dtmin), mb_step_start, then per stage round 1 -> mb_stage_begin -> round 2 ->
-                    mb_stage_end; the halo rows move through mb_pack_rows / mb_unpack_rows and an exchange object.
+                    mb_stage_end; the halo rows of the stage's input buffer (mb_stage_input: the engine rotates
+                    three buffers through the stages) move through mb_pack_rows / mb_unpack_rows and an exchange
+                    object.
   DistExchange      the exchange between processes over torch.distributed (NCCL on GPUs: grouped send / recv
                     of each pair's packed rows; gloo on the CPU).
   LocalExchange     the exchange between rank drivers of one process (device copies; ranks emulated on one GPU).
@@ -252,6 +254,17 @@ class EngineRank:
         self._rows = {}
         self._bufs = {}
         self.dtbuf = torch.zeros(1, dtype=torch.int64, device=self.dev)
+        self.cur_in = self.eng.P.data_ptr()     # the device buffer the current stage reads (set_stage)
+
+    def set_stage(self, irk):
+        """The stage about to run: its input buffer (P, PO or the engine's own) is where the halo rows go."""
+        import ctypes as C
+        ptr = C.c_void_p()
+        e = self.eng
+        rc = e.lib.mb_stage_input(e.ctx, e.P.data_ptr(), e.PO.data_ptr(), irk, C.byref(ptr))
+        if rc != abi.MB_OK:
+            raise abi.MoseError(rc, "mb_stage_input")
+        self.cur_in = ptr.value
 
     def _s(self):
         return self.eng._s()
@@ -268,8 +281,8 @@ class EngineRank:
         if key not in self._bufs or self._bufs[key].numel() != NP * len(rows):
             self._bufs[key] = self.torch.empty(NP * len(rows), dtype=self.torch.float64, device=self.dev)
         buf = self._bufs[key]
-        rc = self.eng.lib.mb_pack_rows(self.eng.P.data_ptr(), self.rc.case.ncell, d.data_ptr(), len(rows),
-                                       buf.data_ptr(), self._s())
+        rc = self.eng.lib.mb_pack_rows(self.cur_in, self.rc.case.ncell, d.data_ptr(), len(rows), buf.data_ptr(),
+                                       self._s())
         if rc != abi.MB_OK:
             raise abi.MoseError(rc, "mb_pack_rows")
         return buf
@@ -278,8 +291,8 @@ class EngineRank:
         d = self._dev_rows(rows)
         if buf.device != self.dev:
             buf = buf.to(self.dev)
-        rc = self.eng.lib.mb_unpack_rows(self.eng.P.data_ptr(), self.rc.case.ncell, d.data_ptr(), len(rows),
-                                         buf.data_ptr(), self._s())
+        rc = self.eng.lib.mb_unpack_rows(self.cur_in, self.rc.case.ncell, d.data_ptr(), len(rows), buf.data_ptr(),
+                                         self._s())
         if rc != abi.MB_OK:
             raise abi.MoseError(rc, "mb_unpack_rows")
 
@@ -321,6 +334,8 @@ def step_ranks(drivers, exchange, visc, n_rk, nsteps=1):
         for d in drivers:
             d.start(dt)
         for irk in range(1, n_rk + 1):
+            for d in drivers:
+                d.set_stage(irk)
             exchange(0)
             for d in drivers:
                 d.stage(irk, 0)
@@ -335,6 +350,7 @@ def step_rank(driver, exchange, visc, n_rk, nsteps=1):
     for _ in range(nsteps):
         driver.start(exchange.min_all(driver.local_dtmin()))
         for irk in range(1, n_rk + 1):
+            driver.set_stage(irk)
             exchange(0)
             driver.stage(irk, 0)
             if visc:

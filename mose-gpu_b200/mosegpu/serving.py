@@ -7,7 +7,8 @@ would alone. Every step of the batch is one replay of the captured step graph: p
 ONE sweep over the tiles of all running cases. Between bursts of `poll_steps` steps the host reads the case
 clocks (one device read), downloads finished cases, frees their rows and clock, and admits arrived requests
 while the HBM budget, a contiguous range of arena rows and a clock are free; admitting rebuilds the context's
-tables (mb_reconfigure) without touching the state of the running cases.
+tables (mb_reconfigure_async, ordered on the lane's stream: the other lanes keep running) without touching the state
+of the running cases.
 
 Cases of one server share the scheme (limiter, Riemann solver, RK, precision, CFL) and the thermo table; each
 brings its own mesh, initial state and stop time. Cases with equal meshes share one device copy of the
@@ -207,7 +208,8 @@ class Server:
                 _check(self.L.mb_init(C.byref(mesh), C.byref(sc), C.byref(T), self.dev.index, C.byref(h)), "mb_init")
             self.ctx = h
         else:
-            _check(self.L.mb_reconfigure(self.ctx, C.byref(mesh)), "mb_reconfigure")
+            # stream-ordered: the other lanes' work is not drained
+            _check(self.L.mb_reconfigure_async(self.ctx, C.byref(mesh), self._s()), "mb_reconfigure_async")
 
     # ------------------------------------------------------------------ admission / retirement
     def fits(self, req):

@@ -1987,7 +1987,8 @@ void fill_ghosts(Ctx& c, double* P) {
       P[dst] = P[src];
       P[dst + IU * nc] = vel[0]; P[dst + IV * nc] = vel[1]; P[dst + IW * nc] = vel[2];
       P[dst + IP * nc] = P[src + IP * nc];
-    } else if (r.type == MB_BC_EXTRAPOLATION || r.type == MB_BC_INFLOW || r.type == MB_BC_OUTLET) {
+    } else if (r.type == MB_BC_EXTRAPOLATION || r.type == MB_BC_INFLOW || r.type == MB_BC_OUTLET ||
+               r.type == MB_BC_NONE) {  // type 0 (no condition): zero-gradient ghost (Lib_Extrapolation.f90:692)
       int64_t src = row(b, r.i, r.j, r.k);
       for (int g = 1; g <= GC; ++g) {
         int64_t dst = row(b, r.i - gstep * g * e[0], r.j - gstep * g * e[1], r.k - gstep * g * e[2]);
@@ -2671,7 +2672,8 @@ int orc_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, orc_
   c.conn.assign(mesh->conn, mesh->conn + mesh->nconn);
   for (const mb_bc& r : c.rec)
     if (r.type != MB_BC_CONNECTION && r.type != MB_BC_EXTRAPOLATION && r.type != MB_BC_WALL &&
-        r.type != MB_BC_INFLOW && r.type != MB_BC_SYMMETRY && r.type != MB_BC_WALL_T && r.type != MB_BC_OUTLET) {
+        r.type != MB_BC_INFLOW && r.type != MB_BC_SYMMETRY && r.type != MB_BC_WALL_T && r.type != MB_BC_OUTLET &&
+        r.type != MB_BC_NONE) {
       delete o;
       return MB_E_UNSUPPORTED;
     }

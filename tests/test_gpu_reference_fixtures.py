@@ -11,7 +11,7 @@ import pytest
 import helpers as H
 import refcases
 from mosegpu import abi
-from test_reference_fixtures import CASES, ORACLE_MD5, field_md5
+from test_reference_fixtures import CASES, ORACLE_MD5, REFERENCE_STEPS, field_md5
 
 pytestmark = pytest.mark.gpu
 
@@ -57,3 +57,21 @@ def test_contraction_changes_the_printed_field(torch_cuda, tmp_path):
         changed[name] = sum(x != y for x, y in zip(la, lb))
     print("printed lines that differ between the two FP64 builds after one iteration:", changed)
     assert sum(changed.values()) > 0, changed
+
+
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_FP64_FAST, abi.PREC_MIXED])
+def test_engine_runs_take_the_reference_steps(torch_cuda, precision):
+    """Each reference case run to its time-threshold on the GPU: the FP64 forms take the reference's own number of
+    steps (docs/vv/mose-comparison.md), the mixed form (dt in FP32) the same within one step."""
+    from mosegpu.engine import Engine
+    for name in CASES:
+        case = refcases.load(name)
+        e = Engine(case, precision=precision)
+        n = e.run_to(case.scheme["time_threshold"])
+        st = e.status()
+        e.close()
+        assert st.code == 0
+        if precision == abi.PREC_MIXED:
+            assert abs(n - REFERENCE_STEPS[name]) <= 1, (name, n)
+        else:
+            assert n == REFERENCE_STEPS[name], (name, n)

@@ -98,6 +98,9 @@ class OracleRank:
         self.PO = np.zeros_like(self.P)
         self.dt = None
 
+    def set_stage(self, irk):
+        pass                                   # the oracle updates P in place: every stage reads P
+
     def pack(self, rows, rnd, tag):
         import torch
         return torch.from_numpy(np.ascontiguousarray(self.P[:, rows]).ravel())

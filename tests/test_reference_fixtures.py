@@ -1,13 +1,15 @@
-"""The reference's own 1-D regression cases (test/1D/{Sod79, Ein91, Noh87, Shu-Osher, Tor99}: their input.ini, ic.tec,
-bc.txt, thermo.dat and phase.txt, packed in tests/golden/reference_1d_cases.npz) through the oracle, against what the
-reference ships for them:
+"""The reference's own 1-D regression cases (test/1D/{Sod79, Ein91, Noh87, Shu-Osher, Tor99}) and its 2-D isentropic
+vortex (test/2D/euler/isentropic-vortex): their input.ini, ic.tec, bc.txt, thermo.dat and phase.txt, packed in
+tests/golden/reference_1d_cases.npz, through the oracle, against what the reference ships for them:
 
   - the solution writer's E23.15E3 formatter reproduces every value line of the four ic.tec files that ORION wrote
     (md5 of the whole value text; Shu-Osher's ic.tec was written by another tool, with E-format mantissas of the form
     -5.000000000000000E+00, and is not a writer pin);
   - the tables are the reference's (gamma = cp / (cp - R) = 1.3999968 at these cp and wm, not 1.4);
   - one iteration (iter-threshold = 1, as run_mose_tests.py stages the regression table) writes OUTPUT/field.tec in
-    ORION's layout with MOSE's default variables (T, g, R), whose md5 the reference pins in test/reference_1it.md5.
+    ORION's layout with MOSE's default variables (T, g, R), whose md5 the reference pins in test/reference_1it.md5;
+  - the whole run of each case to its time-threshold takes the reference's own number of steps (the step counts of
+    docs/vv/mose-comparison.md), and the isentropic vortex returns after one period.
 
 The md5 of a 15-significant-digit ASCII field pins the arithmetic to the last bit of every value it prints, so it pins
 the compiler's choices along with the algorithm: the reference's pins were made by nvfortran on V100 GPUs
@@ -28,12 +30,18 @@ import pytest
 import refcases
 from mosegpu.tecplot import fortran_e23_15e3, write_tecplot_ascii
 
-CASES = ["Sod79", "Ein91", "Noh87", "Shu-Osher", "Tor99"]
+CASES = ["Sod79", "Ein91", "Noh87", "Shu-Osher", "Tor99", "isentropic-vortex"]
 ORION_WRITTEN = ["Sod79", "Ein91", "Noh87", "Tor99"]
 # md5 (first 8 hex digits) of the oracle's field.tec after one iteration of each case (regression values of this
 # repository; the reference's own pins are in the fixture)
 ORACLE_MD5 = {"Sod79": "e0e50956", "Ein91": "b38f75cc", "Noh87": "d896210c", "Shu-Osher": "8cfdfc7b",
-              "Tor99": "4243ab39"}
+              "Tor99": "e572c215", "isentropic-vortex": "175b1e26"}
+# time steps the reference takes to reach each case's time-threshold (docs/vv/mose-comparison.md, column "Steps",
+# MOSE-GPU's: 1-D Sod 195, Einfeldt 184, Noh 821, Shu-Osher 336, Toro 244 (MOSE's own 241 comes from its
+# one-cell-direction ghost defect, docs/vv/known-differences.md item 1), 2-D isentropic vortex 369): every step's dt is
+# the minimum over the cells of the current state, so the count pins the whole evolution, not one step
+REFERENCE_STEPS = {"Sod79": 195, "Ein91": 184, "Noh87": 821, "Shu-Osher": 336, "Tor99": 244,
+                   "isentropic-vortex": 369}
 
 
 def field_md5(case, P, time, path):
@@ -67,7 +75,7 @@ def test_cases_are_the_reference_inputs(name):
     th = case.thermo
     assert abs(th["gamma"] - 1.3999968) < 5e-7 and th["gamma"] != 1.4
     n = case.blocks[0]["n"]
-    assert n[1] == 1 and n[2] == 1 and n[0] in (200, 400)
+    assert tuple(n) in ((200, 1, 1), (400, 1, 1), (64, 64, 1))
     # the state is ic.tec's, and the nodes written back are ic.tec's nodes bit for bit
     d, _ = refcases._data()
     assert np.array_equal(case.interior(case.P0, 0), d[name + "/cells"])
@@ -89,3 +97,34 @@ def test_reference_md5(name, tmp_path):
     case = refcases.load(name)
     P, t = one_iteration(case)
     assert field_md5(case, P, t, tmp_path / "field.tec") == case.meta["md5_1it"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_steps_to_the_time_threshold_match_the_reference_runs(name):
+    """The oracle run of each reference case to its time-threshold (CFL of input.ini, the last step clipped onto the
+    threshold) takes the reference's own number of steps."""
+    import oracle
+    case = refcases.load(name)
+    o = oracle.Oracle(case)
+    P = case.P0.copy()
+    n = o.run_to(P, case.scheme["time_threshold"])
+    st = o.status()
+    assert st.code == 0 and n == REFERENCE_STEPS[name], (name, n)
+    assert abs(st.time - case.scheme["time_threshold"]) <= 1e-12 * case.scheme["time_threshold"]
+
+
+def test_isentropic_vortex_returns_after_one_period():
+    """The vortex of the reference's test (64 x 64 periodic box of side 10, unit mean flow, HLLC + van Leer, SSP-RK3,
+    CFL 0.5) after one period (t = 10): back at its start within the scheme's dissipation (L2 of rho within 1 % of
+    the initial field), mass, momentum and energy conserved to round-off on the periodic mesh."""
+    import helpers as H
+    import oracle
+    case = refcases.load("isentropic-vortex")
+    o = oracle.Oracle(case)
+    P = case.P0.copy()
+    o.run_to(P, case.scheme["time_threshold"])
+    q0, q1 = H.conserved(case, case.P0), H.conserved(case, P)
+    l1, l2, li = H.norms(q1, q0)
+    assert l2[0] < 1e-2 and l2[4] < 1e-2, l2
+    drift = np.abs(q1.sum(axis=1) - q0.sum(axis=1)) / np.abs(q0).sum(axis=1).clip(1e-300)
+    assert np.all(drift[[0, 1, 2, 4]] < 1e-12), drift
