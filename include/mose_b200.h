@@ -442,6 +442,12 @@ int mb_get_tuning(const mb_ctx* ctx, int* kchunk, int* persistent, float* ms);
  * mb_init. Invalidates the captured step graph when it changes the staging. */
 int mb_set_staging(mb_ctx* ctx, int tma);
 
+/* Failure-detection check of the staging's bounded waits (no counterpart in the reference): one CTA on `device` waits
+ * for an mbarrier phase that nothing completes, with a limit of `tries` rounds of mbarrier.try_wait, and the kernel
+ * returns; *gave_up = 1 when the wait ran out (as a sweep's would, which then sets MB_E_TIMEOUT in the case status
+ * and stops), the device staying usable. Synchronises. */
+int mb_selftest_bounded_wait(int device, int tries, int* gave_up);
+
 /* The mixed form's sweep launches of this context so far by staging: *tma_sweeps by TMA, *plain_sweeps by plain
  * loads (launches recorded into a CUDA graph count once, at capture). */
 int mb_get_staging(const mb_ctx* ctx, int64_t* tma_sweeps, int64_t* plain_sweeps);

@@ -47,8 +47,11 @@ struct mb_ctx {
   int ntiles_km = 0;
   std::vector<int> hkm;         // mirrored-block flag per block
   std::vector<int> hdims;       // 3 per block of the current mesh (interior extents)
-  int kc3 = 16;                 // k-chunk of the sweep tiles of blocks deeper than one cell (autotuned)
-  int persistent = 0;           // persistent work-queue sweep (autotuned)
+  int kc3 = 16;                 // k-chunk of the sweep tiles of blocks deeper than one cell (mb_set_tuning; the value
+                                // reported by mb_get_tuning: the chunk of the class with the most cells)
+  int kcls[4] = {16, 16, 16, 16};  // the k-chunk per depth class of 3-D blocks (kclass_of), autotuned per class
+  int persistent = 0;           // persistent work-queue sweep of the main tile list (autotuned)
+  int persistent_km = 0;        // the same for the tiles of mirrored one-plane blocks (autotuned)
   float tuned_ms = 0.f;         // sweep time of the chosen configuration
   int* d_queue = nullptr;       // tile counter of the persistent sweep
   int ty_sweep = 4;
@@ -97,11 +100,13 @@ struct mb_ctx {
 
 // a device copy of a host array, allocated and copied in the order of stream s (the stream-ordered allocator: a
 // table rebuilt while the previous tables are still read by queued work on s is released after that work)
+// (s = 0, the legacy stream: the copy is complete on return, ready for work on any stream)
 template <typename T>
 static int upload(T** dst, const T* src, size_t n, cudaStream_t s = 0) {
   if (n == 0) { *dst = nullptr; return MB_OK; }
   if (cudaMallocAsync((void**)dst, n * sizeof(T), s) != cudaSuccess) return MB_E_NOMEM;
   CK(cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, s));
+  if (s == 0) CK(cudaStreamSynchronize(0));
   return MB_OK;
 }
 
@@ -124,19 +129,26 @@ static void free_ctx(mb_ctx* c) {
 // the tiles (32 x ty cells, kc planes) of the blocks whose class (3: deeper than one cell in k, 2: one k plane,
 // 1: one cell deep in j and k) is in mask (bit cls), block-major
 // km: the mirrored-block flag per block; km_sel 0 / 1 keeps only the blocks with that flag (-1: all)
+// the depth class of a 3-D block for the k-chunk autotuning: n3 <= 16, <= 64, <= 256, more
+static int kclass_of(int n3) { return n3 <= 16 ? 0 : (n3 <= 64 ? 1 : (n3 <= 256 ? 2 : 3)); }
+
+// kcls: the k-chunk per depth class (null: kc for every block); dsel >= 0 keeps only the 3-D blocks of that class
 static std::vector<DTile> make_tiles(const std::vector<int>& dims, int ty, int kc, int mask = 0xe,
-                                     const std::vector<int>* km = nullptr, int km_sel = -1) {
+                                     const std::vector<int>* km = nullptr, int km_sel = -1, const int* kcls = nullptr,
+                                     int dsel = -1) {
   std::vector<DTile> t;
   const int nb = (int)dims.size() / 3;
   for (int b = 0; b < nb; ++b) {
     const int* n = &dims[3 * b];
     const int cls = n[2] > 1 ? 3 : (n[1] > 1 ? 2 : 1);
     if (!(mask & (1 << cls))) continue;
+    if (dsel >= 0 && (cls != 3 || kclass_of(n[2]) != dsel)) continue;
+    const int kcb = (kcls && n[2] > 1) ? kcls[kclass_of(n[2])] : kc;
     if (km && (*km)[b] < 0) continue;  // an external block: nothing is computed on it
     if (km && km_sel >= 0 && (*km)[b] != km_sel) continue;
-    for (int k0 = 1; k0 <= n[2]; k0 += kc)
+    for (int k0 = 1; k0 <= n[2]; k0 += kcb)
       for (int j0 = 1; j0 <= n[1]; j0 += ty)
-        for (int i0 = 1; i0 <= n[0]; i0 += 32) t.push_back(DTile{b, i0, j0, k0, std::min(k0 + kc, n[2] + 1)});
+        for (int i0 = 1; i0 <= n[0]; i0 += 32) t.push_back(DTile{b, i0, j0, k0, std::min(k0 + kcb, n[2] + 1)});
   }
   return t;
 }
@@ -174,6 +186,18 @@ static void stage_buffers(int n, int irk, double* P, double* PO, double* S, cons
 extern "C" {
 
 const char* mb_version(void) { return "mose_b200 0.1 (sm_100a)"; }
+
+int mb_selftest_bounded_wait(int device, int tries, int* gave_up) {
+  if (!gave_up || tries < 1) return MB_E_ARG;
+  CK(cudaSetDevice(device));
+  int* d = nullptr;
+  CK(cudaMalloc((void**)&d, sizeof(int)));
+  cudaError_t e = wait_selftest((unsigned)tries, d, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(gave_up, d, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  CK(e);
+  return MB_OK;
+}
 
 int mb_set_staging(mb_ctx* ctx, int tma) {
   if (!ctx || tma < 0 || tma > 1) return MB_E_ARG;
@@ -436,9 +460,10 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
     for (int a = 0; a < 3; ++a) c->hdims[3 * b + a] = mesh->blk[b].n[a];
   c->hkm.assign(mesh->nblk, 0);
   for (int b = 0; b < mesh->nblk; ++b) c->hkm[b] = mesh->blk[b].group < 0 ? -1 : hb[b].kmirror;
-  std::vector<DTile> ts = make_tiles(c->hdims, c->ty_sweep, c->kc3, 0xe, &c->hkm, 0);
+  std::vector<DTile> ts = make_tiles(c->hdims, c->ty_sweep, c->kc3, 0xe, &c->hkm, 0, c->kcls);
   std::vector<DTile> tk = make_tiles(c->hdims, c->ty_sweep, c->kc3, 0xe, &c->hkm, 1);
   if (c->persistent) sort_by_work(ts, c->hdims, c->ty_sweep);
+  if (c->persistent_km) sort_by_work(tk, c->hdims, c->ty_sweep);
   std::vector<DTile> ta = make_tiles(c->hdims, TY_AUX, 16, 0xe, &c->hkm, -1);
   // ---- the mixed form reads its geometry in FP32: one conversion per distinct array of this mesh (blocks may
   // share arrays). Every copy is converted afresh (a caller may have replaced an array at the same address);
@@ -941,14 +966,15 @@ static int records(mb_ctx* c, const double* Pin, cudaStream_t s) {
 static int sweep(mb_ctx* c, int mode, const double* Pin, const double* Pold, double* Pout, double* Rout, int irk,
                  int last, cudaStream_t s) {
   int rc = sweep_on(c, c->d_tiles_sweep, c->ntiles_sweep, c->persistent, mode, Pin, Pold, Pout, Rout, irk, last, s);
-  if (rc == MB_OK) rc = sweep_on(c, c->d_tiles_km, c->ntiles_km, 0, mode, Pin, Pold, Pout, Rout, irk, last, s, 1);
+  if (rc == MB_OK)
+    rc = sweep_on(c, c->d_tiles_km, c->ntiles_km, c->persistent_km, mode, Pin, Pold, Pout, Rout, irk, last, s, 1);
   return rc;
 }
 
 // average device time of nrep sweeps (MODE_UPDATE of stage 1 from P into the stage buffer, no dt) over a tile
 // list, after one untimed sweep; the state P and the clocks are not changed
 static int time_sweep(mb_ctx* c, const std::vector<DTile>& tl, int persistent, const double* P, int nrep,
-                      cudaStream_t s, float* ms) {
+                      cudaStream_t s, float* ms, int km = 0) {
   DTile* d = nullptr;
   int rc = upload(&d, tl.data(), tl.size());
   if (rc != MB_OK) return rc;
@@ -956,10 +982,11 @@ static int time_sweep(mb_ctx* c, const std::vector<DTile>& tl, int persistent, c
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   rc = records(c, P, s);
-  if (rc == MB_OK) rc = sweep_on(c, d, (int)tl.size(), persistent, MODE_UPDATE, P, P, c->d_scratch, nullptr, 1, 0, s);
+  if (rc == MB_OK)
+    rc = sweep_on(c, d, (int)tl.size(), persistent, MODE_UPDATE, P, P, c->d_scratch, nullptr, 1, 0, s, km);
   cudaEventRecord(e0, s);
   for (int q = 0; q < nrep && rc == MB_OK; ++q)
-    rc = sweep_on(c, d, (int)tl.size(), persistent, MODE_UPDATE, P, P, c->d_scratch, nullptr, 1, 0, s);
+    rc = sweep_on(c, d, (int)tl.size(), persistent, MODE_UPDATE, P, P, c->d_scratch, nullptr, 1, 0, s, km);
   cudaEventRecord(e1, s);
   cudaEventSynchronize(e1);
   float t = 0.f;
@@ -1334,65 +1361,107 @@ int mb_profile_stage(mb_ctx* ctx, double* P, double* PO, int irk, int nrep, floa
 
 int mb_get_status(mb_ctx* ctx, mb_status* st) { return mb_get_group_status(ctx, 0, 1, st); }
 
-// The sweep's project-written autotuner: per block-size class, the k-chunk of the tiles of blocks deeper than
-// one cell (8, 16, 32 or 64 planes; blocks one plane deep have one chunk), then a plain grid of one CTA per tile
-// against the persistent work queue (about one wave of CTAs taking tiles, largest first, from a counter), each
-// candidate timed on the caller's state over the current mesh. Call between steps (it uses the stage buffer).
+// The sweep's project-written autotuner, timed on the caller's state over the current mesh (call between steps: it
+// uses the stage buffer):
+//  - per depth class of the 3-D blocks (n3 <= 16, <= 64, <= 256, more; kclass_of), the k-chunk of their tiles
+//    (8, 16, 32 or 64 planes), each class timed over its own tiles;
+//  - for the main tile list and, separately, for the tiles of the mirrored one-plane blocks (2-D meshes): a plain
+//    grid of one CTA per tile against the persistent work queue (about one wave of CTAs taking tiles, largest first,
+//    from a counter);
+//  - the mixed form: the tile staging (TMA boxes into a 5-value tile, or plain loads into a 6-value tile).
+// The k-chunk and the queue never change a result; the staging changes the FP32 rounding of p in the mixed form.
 int mb_autotune(mb_ctx* ctx, const double* P, void* stream) {
   if (!ctx || !P) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));
   cudaStream_t s = (cudaStream_t)stream;
   prepare_tmaps(ctx, P, P, s);
   const int ty = ctx->ty_sweep;
-  int maxk = 1;
-  for (size_t b = 0; b < ctx->hdims.size() / 3; ++b) maxk = std::max(maxk, ctx->hdims[3 * b + 2]);
   int rc;
-  float best = 1e30f;
-  int kbest = ctx->kc3;
-  if (maxk > 1) {
+  long long ccells[4] = {0, 0, 0, 0};
+  int cmaxk[4] = {0, 0, 0, 0};
+  for (size_t b = 0; b < ctx->hdims.size() / 3; ++b) {
+    const int* n = &ctx->hdims[3 * b];
+    if (n[2] <= 1 || ctx->hkm[b] < 0) continue;
+    const int c = kclass_of(n[2]);
+    ccells[c] += (long long)n[0] * n[1] * n[2];
+    cmaxk[c] = std::max(cmaxk[c], n[2]);
+  }
+  int big = -1;
+  for (int c = 0; c < 4; ++c) {
+    if (!ccells[c]) continue;
+    float best = 1e30f;
+    int kbest = ctx->kcls[c];
     for (int kc : {8, 16, 32, 64}) {
-      if (kc > 16 && kc / 2 >= maxk) break;
-      std::vector<DTile> tl = make_tiles(ctx->hdims, ty, kc, 1 << 3, &ctx->hkm, 0);
+      if (kc > 16 && kc / 2 >= cmaxk[c]) break;
+      std::vector<DTile> tl = make_tiles(ctx->hdims, ty, kc, 1 << 3, &ctx->hkm, 0, nullptr, c);
       float ms = 0.f;
       if ((rc = time_sweep(ctx, tl, 0, P, 3, s, &ms)) != MB_OK) return rc;
       if (ms < best) { best = ms; kbest = kc; }
     }
+    ctx->kcls[c] = kbest;
+    if (big < 0 || ccells[c] > ccells[big]) big = c;
   }
-  ctx->kc3 = kbest;
-  std::vector<DTile> all = make_tiles(ctx->hdims, ty, kbest, 0xe, &ctx->hkm, 0);
+  if (big >= 0) ctx->kc3 = ctx->kcls[big];
+  std::vector<DTile> all = make_tiles(ctx->hdims, ty, ctx->kc3, 0xe, &ctx->hkm, 0, ctx->kcls);
   std::vector<DTile> sorted = all;
   sort_by_work(sorted, ctx->hdims, ty);
   float ms_plain = 0.f, ms_pers = 0.f;
-  if ((rc = time_sweep(ctx, all, 0, P, 3, s, &ms_plain)) != MB_OK) return rc;
-  if ((rc = time_sweep(ctx, sorted, 1, P, 3, s, &ms_pers)) != MB_OK) return rc;
+  if (!all.empty()) {
+    if ((rc = time_sweep(ctx, all, 0, P, 3, s, &ms_plain)) != MB_OK) return rc;
+    if ((rc = time_sweep(ctx, sorted, 1, P, 3, s, &ms_pers)) != MB_OK) return rc;
+  }
   ctx->persistent = ms_pers < ms_plain ? 1 : 0;
   ctx->tuned_ms = std::min(ms_plain, ms_pers);
   const std::vector<DTile>& use = ctx->persistent ? sorted : all;
-  // the mixed form: the tile staging (TMA boxes into a 5-value tile, or plain loads into a 6-value tile) that is
-  // faster on this state and mesh
+  // the one-plane (mirrored) blocks' list: its own queue mode
+  std::vector<DTile> km = make_tiles(ctx->hdims, ty, ctx->kc3, 0xe, &ctx->hkm, 1);
+  std::vector<DTile> km_sorted = km;
+  sort_by_work(km_sorted, ctx->hdims, ty);
+  float km_plain = 0.f, km_pers = 0.f;
+  if (!km.empty()) {
+    if ((rc = time_sweep(ctx, km, 0, P, 3, s, &km_plain, 1)) != MB_OK) return rc;
+    if ((rc = time_sweep(ctx, km_sorted, 1, P, 3, s, &km_pers, 1)) != MB_OK) return rc;
+    ctx->persistent_km = km_pers < km_plain ? 1 : 0;
+    ctx->tuned_ms += std::min(km_plain, km_pers);
+  }
+  const std::vector<DTile>& use_km = ctx->persistent_km ? km_sorted : km;
+  // the mixed form: the tile staging that is faster on this state and mesh (both lists together)
   float ms_stage[2] = {0.f, 0.f};
   if (ctx->sc.precision == MB_PREC_MIXED && tmap_of(ctx, P, s, true)) {
     const bool keep = ctx->stage_tma;
     for (int m = 0; m < 2; ++m) {
       ctx->stage_tma = m == 1;
-      if ((rc = time_sweep(ctx, use, ctx->persistent, P, 3, s, &ms_stage[m])) != MB_OK) { ctx->stage_tma = keep; return rc; }
+      float a = 0.f, b = 0.f;
+      if (!use.empty() && (rc = time_sweep(ctx, use, ctx->persistent, P, 3, s, &a)) != MB_OK) { ctx->stage_tma = keep; return rc; }
+      if (!use_km.empty() && (rc = time_sweep(ctx, use_km, ctx->persistent_km, P, 3, s, &b, 1)) != MB_OK) {
+        ctx->stage_tma = keep;
+        return rc;
+      }
+      ms_stage[m] = a + b;
     }
     ctx->stage_tma = ms_stage[1] < ms_stage[0];
     ctx->tuned_ms = std::min(ms_stage[0], ms_stage[1]);
   }
-  if (ctx->d_tiles_sweep) cudaFree(ctx->d_tiles_sweep);
-  ctx->d_tiles_sweep = nullptr;
+  for (auto* d : {&ctx->d_tiles_sweep, &ctx->d_tiles_km}) {
+    if (*d) cudaFree(*d);
+    *d = nullptr;
+  }
   if ((rc = upload(&ctx->d_tiles_sweep, use.data(), use.size())) != MB_OK) return rc;
+  if ((rc = upload(&ctx->d_tiles_km, use_km.data(), use_km.size())) != MB_OK) return rc;
   ctx->ntiles_sweep = (int)use.size();
+  ctx->ntiles_km = (int)use_km.size();
+  CK(cudaStreamSynchronize(0));
   if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
   if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
   ctx->gP = nullptr;
   ctx->gPO = nullptr;
   if (getenv("MB_REPORT"))
-    fprintf(stderr, "[mose_b200] autotune: k-chunk %d, %s sweep (plain %.3f ms, persistent %.3f ms), %d tiles, "
+    fprintf(stderr, "[mose_b200] autotune: k-chunks %d %d %d %d (depth classes), main list %s (plain %.3f ms, "
+                    "persistent %.3f ms, %d tiles), one-plane list %s (plain %.3f ms, persistent %.3f ms, %d tiles), "
                     "staging %s (plain loads %.3f ms, TMA %.3f ms)\n",
-            ctx->kc3, ctx->persistent ? "persistent" : "plain", ms_plain, ms_pers, ctx->ntiles_sweep,
-            ctx->stage_tma ? "TMA" : "plain loads", ms_stage[0], ms_stage[1]);
+            ctx->kcls[0], ctx->kcls[1], ctx->kcls[2], ctx->kcls[3], ctx->persistent ? "persistent" : "plain", ms_plain,
+            ms_pers, ctx->ntiles_sweep, ctx->persistent_km ? "persistent" : "plain", km_plain, km_pers,
+            ctx->ntiles_km, ctx->stage_tma ? "TMA" : "plain loads", ms_stage[0], ms_stage[1]);
   return MB_OK;
 }
 
@@ -1401,6 +1470,7 @@ int mb_set_tuning(mb_ctx* ctx, int kchunk, int persistent) {
   CK(cudaSetDevice(ctx->device));
   CK(cudaDeviceSynchronize());
   ctx->kc3 = kchunk;
+  for (int c = 0; c < 4; ++c) ctx->kcls[c] = kchunk;
   ctx->persistent = persistent;
   std::vector<DTile> use = make_tiles(ctx->hdims, ctx->ty_sweep, kchunk, 0xe, &ctx->hkm, 0);
   if (persistent) sort_by_work(use, ctx->hdims, ctx->ty_sweep);

@@ -243,6 +243,23 @@ cudaError_t unpack_rows(double* P, long long ncell, const long long* rows, int n
   return cudaGetLastError();
 }
 
+// the bounded wait of the TMA staging run out on purpose: one CTA waits for phase 0 of an mbarrier that nothing
+// arrives at, with a limit of `tries` rounds, and writes 1 once it gave up (a sweep then records MB_E_TIMEOUT and
+// returns); the kernel ends either way
+__global__ void k_wait_selftest(unsigned tries, int* gave_up) {
+  __shared__ __align__(8) unsigned long long bar;
+  if (threadIdx.x == 0) mbar_init(&bar);
+  __syncthreads();
+  bool ok = false;
+  for (unsigned q = 0; q < tries && !ok; ++q) ok = mbar_test(&bar, 0);
+  if (threadIdx.x == 0) *gave_up = ok ? 0 : 1;
+}
+
+cudaError_t wait_selftest(unsigned tries, int* gave_up, cudaStream_t s) {
+  k_wait_selftest<<<1, 32, 0, s>>>(tries, gave_up);
+  return cudaGetLastError();
+}
+
 cudaError_t clock_step(const Params& p, cudaStream_t s) {
   k_clock<<<1, 256, 0, s>>>(p);
   return cudaGetLastError();

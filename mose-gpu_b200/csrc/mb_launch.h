@@ -99,6 +99,8 @@ cudaError_t to_float(const double* src, float* dst, long long n, cudaStream_t s)
 cudaError_t pack_rows(const double* P, long long ncell, const long long* rows, int n, double* buf, cudaStream_t s);
 cudaError_t unpack_rows(double* P, long long ncell, const long long* rows, int n, const double* buf, cudaStream_t s);
 cudaError_t clock_step(const Params& p, cudaStream_t s);
+// the TMA staging's bounded mbarrier wait, made to run out (mb_selftest_bounded_wait)
+cudaError_t wait_selftest(unsigned tries, int* gave_up, cudaStream_t s);
 cudaError_t group_reset(const Params& p, int g, int time_clip, double t_end, double res_stop, cudaStream_t s);
 
 }  // namespace mb

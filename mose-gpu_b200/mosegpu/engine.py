@@ -67,6 +67,8 @@ def load_library():
     for f in ("mb_step_prepare", "mb_copy_dtmin", "mb_step_start", "mb_stage_begin", "mb_stage_end", "mb_pack_rows",
               "mb_unpack_rows"):
         getattr(L, f).restype = C.c_int
+    L.mb_selftest_bounded_wait.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int)]
+    L.mb_selftest_bounded_wait.restype = C.c_int
     L.mb_set_staging.argtypes = [vp, C.c_int]
     L.mb_set_staging.restype = C.c_int
     L.mb_get_staging.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
