@@ -180,6 +180,13 @@ def _err_norms(case, a, b):
         err[nm] = {"L1": float(np.abs(d).sum() / ny) if ny > 0 else float(np.abs(d).sum()),
                    "L2": float(np.sqrt((d * d).sum() / max((y * y).sum(), 1e-300))) if ny > 0 else float(np.sqrt((d * d).sum())),
                    "Linf": float(np.abs(d).max() / max(np.abs(y).max(), 1e-300)) if ny > 0 else float(np.abs(d).max())}
+    # the velocity vector against its own magnitude: a component that is near zero everywhere (w of a Taylor-Green
+    # field) has a large error relative to its own norm even when the velocity error is small
+    dv = np.sqrt(sum((b[q, m] - a[q, m]) ** 2 for q in (1, 2, 3)))
+    vm = np.sqrt(sum(a[q, m] ** 2 for q in (1, 2, 3)))
+    err["velocity"] = {"L1": float(dv.sum() / max(vm.sum(), 1e-300)),
+                       "L2": float(np.sqrt((dv * dv).sum() / max((vm * vm).sum(), 1e-300))),
+                       "Linf": float(dv.max() / max(vm.max(), 1e-300))}
     return err
 
 
@@ -399,6 +406,10 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--forms", default="fp64,fp64_fast,mixed",
+                    help="c2: the forms to time (the headline needs mixed; profiling runs take one form)")
+    ap.add_argument("--staging", default="auto", choices=["auto", "tma", "plain"],
+                    help="the mixed sweep's tile staging: auto = the autotuner's choice")
     ap.add_argument("--serve-rates", default="1.0,1.5,2.0,2.5,3.0",
                     help="serving-sweep: the offered rates (cases/s), each served with --serve-cases cases")
     ap.add_argument("--workload", default="default", choices=["default", "c2", "c3", "c5", "serving", "serving-sweep"],
@@ -437,12 +448,16 @@ def main():
     cells = case.n_interior
     stream = torch.cuda.Stream(dev)
     forms = {}
-    for name, prec in (("fp64", abi.PREC_FP64), ("fp64_fast", abi.PREC_FP64_FAST), ("mixed", abi.PREC_MIXED)):
+    forms_run = [f for f in (("fp64", abi.PREC_FP64), ("fp64_fast", abi.PREC_FP64_FAST), ("mixed", abi.PREC_MIXED))
+                 if f[0] in args.forms.split(",")]
+    for name, prec in forms_run:
         eng = Engine(case, precision=prec, device=local, stream=stream)
         clk = Clocks(local)
         with torch.cuda.stream(stream):
             eng.step(1, graph=True)
             tuning = eng.autotune()          # the sweep's tile configuration, timed on this state
+            if prec == abi.PREC_MIXED and args.staging != "auto":
+                eng.set_staging(1 if args.staging == "tma" else 0)
             eng.step(args.warmup - 1, graph=True)
         barrier(pg, dev)
         l0 = eng.launches
@@ -469,6 +484,21 @@ def main():
             eng.close()
             forms[name]["eng"] = None
             torch.cuda.empty_cache()
+    if len(forms) < 3:  # a profiling run of some forms: their times only, no headline line
+        out = {"workload": "c2 (%s)" % ",".join(forms), "cells": cells, "steps": args.steps,
+               "forms": {k: {"ms_per_step": v["ms"] / args.steps, "sweep_ms": v["sweep_ms"], "tuning": v["tuning"]}
+                         for k, v in forms.items()}}
+        if "mixed" in forms:
+            t, pl = forms["mixed"]["eng"].staging()
+            out["forms"]["mixed"]["staging"] = "TMA" if t > pl else "plain loads"
+        for fm in forms.values():
+            if fm["eng"] is not None:
+                fm["eng"].close()
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        if pg is not None:
+            pg.destroy_process_group()
+        return 0
     # accuracy of the mixed form at the config's step count (100), against the FP64 parity form (the oracle's
     # arithmetic bit for bit, tests/test_gpu_fullsize_oracle.py) and the FP64 production form, from the same field
     err, err_fast = accuracy_at_config_steps(case, dev, stream, local)
