@@ -241,8 +241,7 @@ def run_fixed_steps(case, steps, warmup, dev, stream):
                      "gpu_launches": eng.launches - l0, "time": st.time,
                      "tuning": {"k_chunk": tuning[0], "persistent": bool(tuning[1])}}
         if prec == abi.PREC_MIXED:
-            t, pl = eng.staging()
-            out[name]["staging"] = "TMA" if t > pl else "plain loads"
+            out[name]["staging"] = eng.staging_label()
         states[name] = eng.state()
         eng.close()
         del eng
@@ -408,6 +407,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--forms", default="fp64,fp64_fast,mixed",
                     help="c2: the forms to time (the headline needs mixed; profiling runs take one form)")
+    ap.add_argument("--tuning", default="", help="K,P: k-chunk K and persistent queue P (0/1) instead of the "
+                                                  "autotuner (profiling runs)")
     ap.add_argument("--staging", default="auto", choices=["auto", "tma", "plain"],
                     help="the mixed sweep's tile staging: auto = the autotuner's choice")
     ap.add_argument("--serve-rates", default="1.0,1.5,2.0,2.5,3.0",
@@ -455,7 +456,12 @@ def main():
         clk = Clocks(local)
         with torch.cuda.stream(stream):
             eng.step(1, graph=True)
-            tuning = eng.autotune()          # the sweep's tile configuration, timed on this state
+            if args.tuning:                  # a fixed tile configuration (profiling runs: no autotuner launches)
+                kc, pers = (int(x) for x in args.tuning.split(","))
+                eng.set_tuning(kc, pers)
+                tuning = (kc, pers)
+            else:
+                tuning = eng.autotune()      # the sweep's tile configuration, timed on this state
             if prec == abi.PREC_MIXED and args.staging != "auto":
                 eng.set_staging(1 if args.staging == "tma" else 0)
             eng.step(args.warmup - 1, graph=True)
@@ -489,8 +495,7 @@ def main():
                "forms": {k: {"ms_per_step": v["ms"] / args.steps, "sweep_ms": v["sweep_ms"], "tuning": v["tuning"]}
                          for k, v in forms.items()}}
         if "mixed" in forms:
-            t, pl = forms["mixed"]["eng"].staging()
-            out["forms"]["mixed"]["staging"] = "TMA" if t > pl else "plain loads"
+            out["forms"]["mixed"]["staging"] = forms["mixed"]["eng"].staging_label()
         for fm in forms.values():
             if fm["eng"] is not None:
                 fm["eng"].close()

@@ -452,6 +452,11 @@ int mb_selftest_bounded_wait(int device, int tries, int* gave_up);
  * loads (launches recorded into a CUDA graph count once, at capture). */
 int mb_get_staging(const mb_ctx* ctx, int64_t* tma_sweeps, int64_t* plain_sweeps);
 
+/* The mixed sweep's configured staging (mb_set_staging, or mb_autotune's choice): *tma = 1 for the 5-value tile
+ * (staged by TMA where the state buffer has a tensor map, by plain loads where it has none), 0 for the 6-value tile by
+ * plain loads. */
+int mb_get_staging_mode(const mb_ctx* ctx, int* tma);
+
 /* Number of kernel launches this context has issued (for launch accounting). */
 int64_t mb_launch_count(const mb_ctx* ctx);
 

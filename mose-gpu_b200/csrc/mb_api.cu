@@ -218,6 +218,12 @@ int mb_get_staging(const mb_ctx* ctx, int64_t* tma_sweeps, int64_t* plain_sweeps
   return MB_OK;
 }
 
+int mb_get_staging_mode(const mb_ctx* ctx, int* tma) {
+  if (!ctx || !tma) return MB_E_ARG;
+  *tma = ctx->stage_tma ? 1 : 0;
+  return MB_OK;
+}
+
 int64_t mb_launch_count(const mb_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 // the checks of a mesh description that mb_init and mb_reconfigure share
@@ -1425,9 +1431,12 @@ int mb_autotune(mb_ctx* ctx, const double* P, void* stream) {
     ctx->tuned_ms += std::min(km_plain, km_pers);
   }
   const std::vector<DTile>& use_km = ctx->persistent_km ? km_sorted : km;
-  // the mixed form: the tile staging that is faster on this state and mesh (both lists together)
+  // the mixed form: the tile staging that is faster on this state and mesh (both lists together): the 6-value tile
+  // by plain loads against the 5-value tile, staged by TMA where the state buffer has a tensor map (by plain loads
+  // into the same 5-value tile where it has none)
   float ms_stage[2] = {0.f, 0.f};
-  if (ctx->sc.precision == MB_PREC_MIXED && tmap_of(ctx, P, s, true)) {
+  if (ctx->sc.precision == MB_PREC_MIXED) {
+    tmap_of(ctx, P, s, true);
     const bool keep = ctx->stage_tma;
     for (int m = 0; m < 2; ++m) {
       ctx->stage_tma = m == 1;
@@ -1458,10 +1467,15 @@ int mb_autotune(mb_ctx* ctx, const double* P, void* stream) {
   if (getenv("MB_REPORT"))
     fprintf(stderr, "[mose_b200] autotune: k-chunks %d %d %d %d (depth classes), main list %s (plain %.3f ms, "
                     "persistent %.3f ms, %d tiles), one-plane list %s (plain %.3f ms, persistent %.3f ms, %d tiles), "
-                    "staging %s (plain loads %.3f ms, TMA %.3f ms)\n",
+                    "staging %s (6-value %.3f ms, 5-value %.3f ms)\n",
             ctx->kcls[0], ctx->kcls[1], ctx->kcls[2], ctx->kcls[3], ctx->persistent ? "persistent" : "plain", ms_plain,
             ms_pers, ctx->ntiles_sweep, ctx->persistent_km ? "persistent" : "plain", km_plain, km_pers,
-            ctx->ntiles_km, ctx->stage_tma ? "TMA" : "plain loads", ms_stage[0], ms_stage[1]);
+            ctx->ntiles_km,
+            ctx->sc.precision != MB_PREC_MIXED ? "none (FP64 form)"
+            : !ctx->stage_tma                  ? "6-value tile, plain loads"
+            : tmap_of(ctx, P, s, false)        ? "5-value tile, TMA"
+                                               : "5-value tile, plain loads (no tensor map)",
+            ms_stage[0], ms_stage[1]);
   return MB_OK;
 }
 

@@ -73,6 +73,8 @@ def load_library():
     L.mb_set_staging.restype = C.c_int
     L.mb_get_staging.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.mb_get_staging.restype = C.c_int
+    L.mb_get_staging_mode.argtypes = [vp, C.POINTER(C.c_int)]
+    L.mb_get_staging_mode.restype = C.c_int
     L.mb_launch_count.argtypes = [vp]
     L.mb_launch_count.restype = C.c_int64
     L.mb_version.restype = C.c_char_p
@@ -172,6 +174,19 @@ class Engine:
         a, b = C.c_int64(), C.c_int64()
         _check(self.lib.mb_get_staging(self.ctx, C.byref(a), C.byref(b)), "mb_get_staging")
         return a.value, b.value
+
+    def staging_mode(self):
+        """The configured staging of the mixed sweep: 1 = the 5-value tile (TMA where a tensor map exists), 0 = the
+        6-value tile by plain loads (mb_get_staging_mode)."""
+        m = C.c_int()
+        _check(self.lib.mb_get_staging_mode(self.ctx, C.byref(m)), "mb_get_staging_mode")
+        return m.value
+
+    def staging_label(self):
+        """A description of the staging the mixed sweep uses now."""
+        if not self.staging_mode():
+            return "6-value tile, plain loads"
+        return "5-value tile, TMA" if self.staging()[0] > 0 else "5-value tile, plain loads (no tensor map)"
 
     @property
     def launches(self):
