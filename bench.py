@@ -40,6 +40,17 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def instructions_per_cell(form):
+    """Warp instructions per cell of one sweep launch from the committed ncu summary (None without one)."""
+    p = os.path.join(ROOT, "profiles", "sweep_traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p)).get(form)
+    if not d or "warp_instructions" not in d:
+        return None
+    return float(d["warp_instructions"]) / float(d["cells"])
+
+
 def traffic_per_launch(n, form):
     """DRAM bytes (read + write) of one sweep launch of `form` from the committed ncu summary, scaled from the
     captured case by the cells processed (the sweep's traffic grows in proportion to them)."""
@@ -416,8 +427,8 @@ def main():
     ap.add_argument("--workload", default="default", choices=["default", "c2", "c3", "c5", "serving", "serving-sweep"],
                     help="default: the 256^3 Taylor-Green headline plus the serving sample and the 2-D batch; "
                          "c2 / c3 / c5 / serving: that workload alone")
-    ap.add_argument("--serve-cases", type=int, default=48)
-    ap.add_argument("--serve-rate", type=float, default=1.0, help="Poisson arrivals per second")
+    ap.add_argument("--serve-cases", type=int, default=256)
+    ap.add_argument("--serve-rate", type=float, default=3.0, help="Poisson arrivals per second")
     ap.add_argument("--serve-budget-gb", type=float, default=32.0)
     ap.add_argument("--serve-poll", type=int, default=16, help="steps between reads of the case clocks")
     ap.add_argument("--serve-max-s", type=float, default=240.0)
@@ -544,7 +555,21 @@ def main():
     peak, peak_kind = peaks()
     bytes_launch = cells * B_STAGE
     achieved = bytes_launch / (f["sweep_ms"] * 1e-3) / 1e9
-    tr = traffic_per_launch(args.n, head)
+    tkey = head
+    if head == "mixed" and f["eng"] is not None and f["eng"].staging_mode() == 1 and f["eng"].staging()[0] > 0:
+        tkey = "mixed_tma"               # the capture of the staging the timed sweep used
+    tr = traffic_per_launch(args.n, tkey)
+    # the bound that holds: instruction issue (ncu warp instructions per cell of the same kernel x cells / the sweep's
+    # CUDA-event time, against 4 schedulers x 148 SMs x the SM clock sampled during the timed steps)
+    ipc = instructions_per_cell(tkey)
+    sm_mhz = (f["clocks"] or {}).get("sm_mhz") if isinstance(f.get("clocks"), dict) else None
+    issue = None
+    if ipc and sm_mhz:
+        nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+        rate = ipc * cells / (f["sweep_ms"] * 1e-3)
+        issue = {"warp_instructions_per_cell": ipc, "achieved_per_s": rate,
+                 "peak_per_s": 4.0 * nsm * sm_mhz * 1e6, "frac": rate / (4.0 * nsm * sm_mhz * 1e6),
+                 "source": "ncu smsp__inst_executed.sum at 160^3 (profiles/k_sweep_mixed_tgv160_ncu.md)"}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": f["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 flux / f64 state" if head == "mixed" else "f64",
@@ -573,7 +598,8 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": tr, "peak_source": peak_kind,
                          "kernel": "k_sweep<%s> (stage 2)" % ("float" if head == "mixed" else "double"),
-                         "algorithmic_bytes_per_launch": bytes_launch},
+                         "staging": f["eng"].staging_label() if head == "mixed" and f["eng"] is not None else None,
+                         "algorithmic_bytes_per_launch": bytes_launch, "issue": issue},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
                     "d2h_bytes_per_step": state_bytes / args.steps + 48,
                     "copies": "once per run: the state is uploaded before the first step and downloaded after the "

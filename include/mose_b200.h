@@ -171,7 +171,11 @@ typedef struct mb_mesh {
                             mb_reconfigure calls */
   int64_t ncell_total;   /* rows of P_flat */
   const mb_block* blk;   /* host array [nblk] (the geometry pointers in it are device pointers) */
-  const mb_bc* rec;      /* host array [nrec], grouped per block and ordered by face within it */
+  const mb_bc* rec;      /* host array [nrec], grouped per block and ordered by face within it. A block one cell
+                            deep in k (n[2] = 1) with no record on faces 5 and 6 is taken as having extrapolation
+                            (type 11) records on every cell of both (the reference's 2-D meshes): the results are
+                            the same, with 2 n1 n2 records fewer; its k ghost rows are then never filled (nothing
+                            reads them) */
   const mb_conn* conn;   /* host array [nconn] */
 } mb_mesh;
 

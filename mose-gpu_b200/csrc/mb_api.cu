@@ -394,7 +394,11 @@ static int build_tables(mb_ctx* c, const mb_mesh* mesh) {
     for (int b = 0; b < mesh->nblk; ++b) {
       DBlk& d = hb[b];
       const long long nk = (long long)d.n1 * d.n2;
-      d.kmirror = (d.n3 == 1 && all11[3 * b + 2] && nface[6 * b + 4] == nk && nface[6 * b + 5] == nk) ? 1 : 0;
+      // extrapolation records on every cell of both k faces, or no k-face record at all (a one-plane block
+      // without k-face records is taken as extrapolated there: the reference's 2-D meshes, 2 n1 n2 records fewer)
+      const bool kfull = nface[6 * b + 4] == nk && nface[6 * b + 5] == nk;
+      const bool knone = nface[6 * b + 4] == 0 && nface[6 * b + 5] == 0;
+      d.kmirror = (d.n3 == 1 && all11[3 * b + 2] && (kfull || knone)) ? 1 : 0;
     }
     for (int q = 0; q < mesh->nrec; ++q) {
       const mb_bc& r = mesh->rec[q];

@@ -39,8 +39,9 @@ struct DBlk {
   int n1, n2, n3, pi, pj;
   int grp;              // the case of the block (its clock: Params::st[grp])
   int ndir;             // computational directions of the case (the dt rule)
-  int kmirror;          // one cell deep in k with extrapolation (type 11) records on every cell of both k faces:
-                        // its k ghosts equal the k = 1 values exactly (zero-gradient then cubic: 3a - 3a + a = a),
+  int kmirror;          // one cell deep in k with extrapolation (type 11) records on every cell of both k faces,
+                        // or with no k-face record at all (taken as the same): its k ghosts equal the k = 1 values
+                        // exactly (zero-gradient then cubic: 3a - 3a + a = a),
                         // so readers take the k = 1 cell and the fused stage does not fill them
   int rmap[6];          // offset of each face's record map in Params::rec_map (-1: none)
   long long boff;

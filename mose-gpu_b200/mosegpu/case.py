@@ -210,7 +210,29 @@ def _axis_nodes(N, L, x0=0.0):
     return x0 + nu * (L / N)
 
 
-def layout_case(name, cuts, node_fn, periodic, bc_faces, thermo, scheme, prim_fn, share_geometry=False):
+def uniform_geometry(n, h):
+    """The metric arrays of a block of n cells on a uniform Cartesian grid of spacings h = (hx, hy, hz), in the
+    layouts of cell_metrics / face_metrics (padded cells, interior faces): M = diag(1 / h), dl = h, vol = hx hy hz,
+    unit face normals along the axes with the face areas. The values of cell_metrics / face_metrics on such a grid up
+    to the rounding of the node coordinates, without evaluating them cell by cell."""
+    hx, hy, hz = (float(x) for x in h)
+    npad = (n[0] + 2 * GC) * (n[1] + 2 * GC) * (n[2] + 2 * GC)
+    m = np.zeros((npad, 9))
+    m[:, 0], m[:, 4], m[:, 8] = 1.0 / hx, 1.0 / hy, 1.0 / hz
+    dl = np.empty((npad, 3))
+    dl[:] = (hx, hy, hz)
+    out = dict(m=m.ravel(), dl=dl.ravel(), vol=np.full(npad, hx * hy * hz))
+    for q, (nf, nrm, area) in enumerate((((n[0] + 1) * n[1] * n[2], (1.0, 0.0, 0.0), hy * hz),
+                                         (n[0] * (n[1] + 1) * n[2], (0.0, 1.0, 0.0), hx * hz),
+                                         (n[0] * n[1] * (n[2] + 1), (0.0, 0.0, 1.0), hx * hy))):
+        f = np.empty((nf, 4))
+        f[:] = nrm + (area,)
+        out["fm%d" % (q + 1)] = f.ravel()
+    return out
+
+
+def layout_case(name, cuts, node_fn, periodic, bc_faces, thermo, scheme, prim_fn, share_geometry=False,
+                uniform=None, implicit_k=False):
     """A structured layout of blocks.
 
     cuts      : per axis, the cell-index cut points of the blocks, e.g. [[0, 128, 256], [0, 256], [0, 256]]
@@ -223,6 +245,10 @@ def layout_case(name, cuts, node_fn, periodic, bc_faces, thermo, scheme, prim_fn
     share_geometry : blocks of equal extents reuse the metric arrays of the first such block (exact for a
                 node_fn that is a translation from block to block, e.g. a uniform Cartesian grid; the
                 engine then holds one copy of the geometry on the device)
+    uniform   : (hx, hy, hz) when node_fn is a uniform Cartesian grid of those spacings: the metric arrays from
+                uniform_geometry instead of cell by cell (large serving cases)
+    implicit_k: blocks one cell deep in k get no records on their extrapolated k faces (5, 6): the engine and the
+                oracle take a one-plane block without k-face records as extrapolated there (2 n1 n2 records fewer)
     Blocks are numbered i fastest over the layout; faces between blocks are 1:1 connections with
     identity orientation; periodic axes wrap onto the first / last block.
     """
@@ -248,7 +274,12 @@ def layout_case(name, cuts, node_fn, periodic, bc_faces, thermo, scheme, prim_fn
     shared = {}
     for b in blocks:
         n, lo = b["n"], b["lo"]
-        if share_geometry and tuple(n) in shared:
+        if uniform is not None:
+            b.update(uniform_geometry(n, uniform))
+            ax = [np.arange(lo[d], lo[d] + n[d] + 1, dtype=np.float64) for d in range(3)]
+            IU, IV, IW = np.meshgrid(ax[0], ax[1], ax[2], indexing="ij")
+            Xi = node_fn(IU, IV, IW)
+        elif share_geometry and tuple(n) in shared:
             b.update(shared[tuple(n)])
             ax = [np.arange(lo[d], lo[d] + n[d] + 1, dtype=np.float64) for d in range(3)]
             IU, IV, IW = np.meshgrid(ax[0], ax[1], ax[2], indexing="ij")
@@ -312,6 +343,8 @@ def layout_case(name, cuts, node_fn, periodic, bc_faces, thermo, scheme, prim_fn
                 conns.append(cn)
             else:
                 spec = bc_faces[face]
+                if implicit_k and face >= 5 and n[2] == 1 and spec == abi.BC_EXTRAPOLATION:
+                    continue
                 if isinstance(spec, tuple):
                     r["type"] = spec[0]
                     qv = np.asarray(spec[1], dtype=np.float64)
@@ -500,10 +533,11 @@ def duct_3d(widths=(6, 5), heights=(5,), depths=(3, 4), mach=0.5, T=300.0, p=1.0
 
 
 def riemann_1d(n=1000, left=(1.0, 0.0, 1.0), right=(0.125, 0.0, 0.1), x0=0.5, t_end=0.2, cfl=0.5,
-               riemann=abi.RS_HLLC, limiter=abi.LIM_MINMOD, n_rk=3):
+               riemann=abi.RS_HLLC, limiter=abi.LIM_MINMOD, n_rk=3, compact=False):
     """1-D Euler Riemann problem on [0, 1] (non-dimensional: T < 1 K sits in table row 0, allowed
     for Euler), transmissive ends (400 -> extrapolation, type 11) and type-11 lateral faces as in
-    test/1D/Sod79/INPUT/bc.txt. left/right = (rho, u, p)."""
+    test/1D/Sod79/INPUT/bc.txt. left/right = (rho, u, p). compact: uniform-grid geometry and implicit k faces
+    (layout_case)."""
     th = ideal_gas_tables()
     h = 1.0 / n
 
@@ -521,15 +555,16 @@ def riemann_1d(n=1000, left=(1.0, 0.0, 1.0), right=(0.125, 0.0, 0.1), x0=0.5, t_
                   time_threshold=t_end)
     bc = {f: abi.BC_EXTRAPOLATION for f in range(1, 7)}
     case = layout_case("riemann1d_%d" % n, [[0, n], [0, 1], [0, 1]], nodes, (False, False, False), bc, th,
-                       scheme, prim)
+                       scheme, prim, uniform=(h, h, h) if compact else None, implicit_k=compact)
     case.meta = dict(left=left, right=right, x0=x0, t_end=t_end)
     case.steps = None
     return case
 
 
-def riemann_2d(n=128, states=None, t_end=0.25, cfl=0.5, riemann=abi.RS_HLLC, limiter=abi.LIM_MINMOD):
+def riemann_2d(n=128, states=None, t_end=0.25, cfl=0.5, riemann=abi.RS_HLLC, limiter=abi.LIM_MINMOD, compact=False):
     """2-D four-quadrant Riemann problem on [0,1]^2 (n x n cells, one k layer), extrapolation on every
-    face. states = [(rho,u,v,p)] for the quadrants (x>.5,y>.5), (x<.5,y>.5), (x<.5,y<.5), (x>.5,y<.5)."""
+    face. states = [(rho,u,v,p)] for the quadrants (x>.5,y>.5), (x<.5,y>.5), (x<.5,y<.5), (x>.5,y<.5).
+    compact: uniform-grid geometry and implicit k faces (layout_case)."""
     th = ideal_gas_tables()
     h = 1.0 / n
     if states is None:
@@ -552,7 +587,7 @@ def riemann_2d(n=128, states=None, t_end=0.25, cfl=0.5, riemann=abi.RS_HLLC, lim
                   time_threshold=t_end)
     bc = {f: abi.BC_EXTRAPOLATION for f in range(1, 7)}
     case = layout_case("riemann2d_%d" % n, [[0, n], [0, n], [0, 1]], nodes, (False, False, False), bc, th,
-                       scheme, prim)
+                       scheme, prim, uniform=(h, h, h) if compact else None, implicit_k=compact)
     case.meta = dict(t_end=t_end)
     return case
 

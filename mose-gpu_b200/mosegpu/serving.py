@@ -355,7 +355,7 @@ def riemann_request(rid, dim, n, states, t_end, arrival=0.0):
     key = (dim, n)
     base = _TEMPLATES.get(key)
     if base is None:
-        base = cs.riemann_1d(n=n, t_end=t_end) if dim == 1 else cs.riemann_2d(n=n, t_end=t_end)
+        base = cs.riemann_1d(n=n, t_end=t_end, compact=True) if dim == 1 else cs.riemann_2d(n=n, t_end=t_end, compact=True)
         _TEMPLATES[key] = base
     c = cs.Case(base.name)
     c.blocks, c.rec, c.conn, c.ncell, c.thermo = base.blocks, base.rec, base.conn, base.ncell, base.thermo

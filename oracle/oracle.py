@@ -51,8 +51,41 @@ def _ptr(a):
     return a.ctypes.data_as(C.c_void_p)
 
 
+def explicit_k_records(case):
+    """(records, connections) of the case with the implicit k faces made explicit: a block one cell deep in k with no
+    record on faces 5 and 6 gets type-11 (extrapolation) records on every cell of both, appended to its own records
+    (faces ordered within the block); the connections' record indices follow the renumbering. The reference's 2-D
+    meshes carry those records; the engine takes their absence as the same faces."""
+    rec, conn = case.rec, case.conn
+    need = [q for q, b in enumerate(case.blocks) if b["n"][2] == 1 and
+            not np.any((rec["blk"] == q) & (rec["face"] >= 5))]
+    if not need:
+        return rec, conn
+    parts, newidx, pos = [], np.empty(len(rec), dtype=np.int64), 0
+    for q in range(len(case.blocks)):
+        sel = np.nonzero(rec["blk"] == q)[0]
+        newidx[sel] = pos + np.arange(sel.size)
+        parts.append(rec[sel])
+        pos += sel.size
+        if q in need:
+            n1, n2 = case.blocks[q]["n"][:2]
+            I, J = [a.ravel(order="F") for a in np.meshgrid(np.arange(1, n1 + 1), np.arange(1, n2 + 1), indexing="ij")]
+            for face in (5, 6):
+                r = np.zeros(I.size, dtype=abi.BC_DTYPE)
+                r["blk"] = q; r["i"] = I; r["j"] = J; r["k"] = 1; r["face"] = face
+                r["type"] = abi.BC_EXTRAPOLATION; r["conn"] = -1
+                parts.append(r)
+                pos += I.size
+    rec2 = np.concatenate(parts)
+    conn2 = conn.copy()
+    if len(conn2):
+        conn2["rec"] = newidx[conn2["rec"]]
+    return rec2, conn2
+
+
 class Oracle:
-    """The CPU restatement bound to one case (host arrays)."""
+    """The CPU restatement bound to one case (host arrays). A one-plane block without k-face records is run with
+    explicit extrapolation records there (explicit_k_records)."""
 
     def __init__(self, case):
         self.case = case
@@ -69,8 +102,9 @@ class Oracle:
                 a = np.ascontiguousarray(b[f], dtype=np.float64)
                 self._keep.append(a)
                 setattr(B, f, _ptr(a).value)
-        self._rec = np.ascontiguousarray(case.rec)
-        self._conn = np.ascontiguousarray(case.conn)
+        rec, conn = explicit_k_records(case)
+        self._rec = np.ascontiguousarray(rec)
+        self._conn = np.ascontiguousarray(conn)
         mesh = abi.MBMesh()
         mesh.nblk = nb; mesh.nrec = len(self._rec); mesh.nconn = len(self._conn)
         mesh.ncell_total = case.ncell
