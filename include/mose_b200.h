@@ -440,7 +440,8 @@ int mb_get_tuning(const mb_ctx* ctx, int* kchunk, int* persistent, float* ms);
  * mbarrier (bounded waits; a wait that gives up sets MB_E_TIMEOUT in the case status), converted into a 5-value
  * FP32 tile (rho, u, v, w, T; p = rho R T where it is read) with the k-face fluxes carried in registers; tma = 0
  * stages by per-thread coalesced loads into a 6-value tile (rho, u, v, w, p, T). The two differ in the FP32
- * rounding of p (within the mixed form's accuracy); mb_autotune keeps the faster. TMA is used where a tensor map of
+ * rounding of p (within the mixed form's accuracy); mb_autotune keeps the faster for each tile list (this call sets
+ * both lists: the blocks with several k planes, and the mirrored one-plane blocks). TMA is used where a tensor map of
  * the state buffer can be made: the buffer 16-byte aligned, ncell_total even, the map made outside any stream
  * capture (at the first mb_stage / mb_step / mb_residual / mb_autotune on that buffer), MB_NO_TMA unset at
  * mb_init. Invalidates the captured step graph when it changes the staging. */
@@ -456,9 +457,10 @@ int mb_selftest_bounded_wait(int device, int tries, int* gave_up);
  * loads (launches recorded into a CUDA graph count once, at capture). */
 int mb_get_staging(const mb_ctx* ctx, int64_t* tma_sweeps, int64_t* plain_sweeps);
 
-/* The mixed sweep's configured staging (mb_set_staging, or mb_autotune's choice): *tma = 1 for the 5-value tile
- * (staged by TMA where the state buffer has a tensor map, by plain loads where it has none), 0 for the 6-value tile by
- * plain loads. */
+/* The mixed sweep's configured staging (mb_set_staging, or mb_autotune's choice, which tunes the tile list of
+ * mirrored one-plane blocks separately): *tma = 1 for the 5-value tile (staged by TMA where the state buffer has a
+ * tensor map, by plain loads where it has none), 0 for the 6-value tile by plain loads; of the main tile list, or of
+ * the one-plane list when the mesh has no other blocks. */
 int mb_get_staging_mode(const mb_ctx* ctx, int* tma);
 
 /* Number of kernel launches this context has issued (for launch accounting). */

@@ -64,6 +64,7 @@ struct mb_ctx {
   std::vector<Tmap> tmaps;
   bool no_tma = false;          // MB_NO_TMA set at mb_init: no tensor maps (the TMA staging is never used)
   bool stage_tma = true;        // the mixed sweep stages by TMA where a map exists (mb_set_staging, mb_autotune)
+  bool stage_tma_km = true;     // the same for the tile list of mirrored one-plane blocks (tuned separately)
   cudaStream_t tstream = 0;     // the stream the mesh tables are (re)built in the order of (build_tables)
   long long sweeps_tma = 0, sweeps_plain = 0;  // sweep launches of the mixed form by staging path
   double* d_acc4 = nullptr;     // RK4: conserved accumulator (ncell x 5)
@@ -201,8 +202,9 @@ int mb_selftest_bounded_wait(int device, int tries, int* gave_up) {
 
 int mb_set_staging(mb_ctx* ctx, int tma) {
   if (!ctx || tma < 0 || tma > 1) return MB_E_ARG;
-  if (ctx->stage_tma != (tma == 1)) {
+  if (ctx->stage_tma != (tma == 1) || ctx->stage_tma_km != (tma == 1)) {
     ctx->stage_tma = tma == 1;
+    ctx->stage_tma_km = tma == 1;
     if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }  // a replay in flight completes
     if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
     ctx->gP = nullptr;
@@ -220,7 +222,7 @@ int mb_get_staging(const mb_ctx* ctx, int64_t* tma_sweeps, int64_t* plain_sweeps
 
 int mb_get_staging_mode(const mb_ctx* ctx, int* tma) {
   if (!ctx || !tma) return MB_E_ARG;
-  *tma = ctx->stage_tma ? 1 : 0;
+  *tma = (ctx->ntiles_sweep > 0 ? ctx->stage_tma : ctx->stage_tma_km) ? 1 : 0;
   return MB_OK;
 }
 
@@ -778,6 +780,8 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
     const int v = sc->visc ? 1 : 0;
     int occ = MB_BY_FORM(sc->precision, sweep_unit(sc), _occupancy, (v));
     p.pgrid = std::max(1, occ) * std::max(1, nsm);
+    int occ_km = MB_BY_FORM(sc->precision, sweep_unit(sc), _occupancy_km, (v));
+    p.pgrid_km = std::max(1, occ_km) * std::max(1, nsm);
   }
   p.queue = nullptr;
   // ---- the mesh tables
@@ -785,9 +789,10 @@ int mb_init(const mb_mesh* mesh, const mb_scheme* sc, const mb_thermo* th, int d
   if (getenv("MB_REPORT")) {
     const int v = sc->visc ? 1 : 0;
     int occ = MB_BY_FORM(sc->precision, sweep_unit(sc), _occupancy, (v));
-    fprintf(stderr, "[mose_b200] sweep: %s, %d threads per CTA, %d CTAs per SM, %d tiles\n",
+    int occ_km = MB_BY_FORM(sc->precision, sweep_unit(sc), _occupancy_km, (v));
+    fprintf(stderr, "[mose_b200] sweep: %s, %d threads per CTA, %d CTAs per SM (%d for one-plane blocks), %d + %d tiles\n",
             sc->precision == MB_PREC_MIXED ? "mixed" : (sc->precision == MB_PREC_FP64_FAST ? "fp64 fast" : "fp64"),
-            32 * c->ty_sweep, occ, c->ntiles_sweep);
+            32 * c->ty_sweep, occ, occ_km, c->ntiles_sweep, c->ntiles_km);
   }
 #undef TRY
   CK(cudaStreamSynchronize(0));  // the tables were built in the order of the legacy stream: ready for any stream
@@ -951,7 +956,7 @@ static int sweep_on(mb_ctx* c, const DTile* t, int n, int persistent, int mode, 
   Params p = c->p;
   p.irk = irk;
   p.queue = persistent ? c->d_queue : nullptr;
-  p.stg = (c->sc.precision == MB_PREC_MIXED && c->stage_tma) ? STG_TMA : STG_PLAIN;
+  p.stg = (c->sc.precision == MB_PREC_MIXED && (km ? c->stage_tma_km : c->stage_tma)) ? STG_TMA : STG_PLAIN;
   p.tmap = p.stg == STG_TMA ? tmap_of(c, Pin, s, false) : nullptr;
   if (c->sc.precision == MB_PREC_MIXED) (p.tmap ? c->sweeps_tma : c->sweeps_plain) += 1;
   const double rkc = irk > 0 ? rkc_of(c->sc.n_rk, irk) : 0.0;
@@ -1435,25 +1440,25 @@ int mb_autotune(mb_ctx* ctx, const double* P, void* stream) {
     ctx->tuned_ms += std::min(km_plain, km_pers);
   }
   const std::vector<DTile>& use_km = ctx->persistent_km ? km_sorted : km;
-  // the mixed form: the tile staging that is faster on this state and mesh (both lists together): the 6-value tile
-  // by plain loads against the 5-value tile, staged by TMA where the state buffer has a tensor map (by plain loads
-  // into the same 5-value tile where it has none)
-  float ms_stage[2] = {0.f, 0.f};
+  // the mixed form: the tile staging that is faster on this state and mesh, per tile list: the 6-value tile by plain
+  // loads against the 5-value tile, staged by TMA where the state buffer has a tensor map (by plain loads into the
+  // same 5-value tile where it has none)
+  float ms_stage[2] = {0.f, 0.f}, ms_stage_km[2] = {0.f, 0.f};
   if (ctx->sc.precision == MB_PREC_MIXED) {
     tmap_of(ctx, P, s, true);
-    const bool keep = ctx->stage_tma;
+    const bool keep = ctx->stage_tma, keep_km = ctx->stage_tma_km;
     for (int m = 0; m < 2; ++m) {
-      ctx->stage_tma = m == 1;
-      float a = 0.f, b = 0.f;
-      if (!use.empty() && (rc = time_sweep(ctx, use, ctx->persistent, P, 3, s, &a)) != MB_OK) { ctx->stage_tma = keep; return rc; }
-      if (!use_km.empty() && (rc = time_sweep(ctx, use_km, ctx->persistent_km, P, 3, s, &b, 1)) != MB_OK) {
+      ctx->stage_tma = ctx->stage_tma_km = m == 1;
+      if ((!use.empty() && (rc = time_sweep(ctx, use, ctx->persistent, P, 3, s, &ms_stage[m])) != MB_OK) ||
+          (!use_km.empty() && (rc = time_sweep(ctx, use_km, ctx->persistent_km, P, 3, s, &ms_stage_km[m], 1)) != MB_OK)) {
         ctx->stage_tma = keep;
+        ctx->stage_tma_km = keep_km;
         return rc;
       }
-      ms_stage[m] = a + b;
     }
     ctx->stage_tma = ms_stage[1] < ms_stage[0];
-    ctx->tuned_ms = std::min(ms_stage[0], ms_stage[1]);
+    ctx->stage_tma_km = ms_stage_km[1] < ms_stage_km[0];
+    ctx->tuned_ms = std::min(ms_stage[0], ms_stage[1]) + std::min(ms_stage_km[0], ms_stage_km[1]);
   }
   for (auto* d : {&ctx->d_tiles_sweep, &ctx->d_tiles_km}) {
     if (*d) cudaFree(*d);
@@ -1468,18 +1473,20 @@ int mb_autotune(mb_ctx* ctx, const double* P, void* stream) {
   if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
   ctx->gP = nullptr;
   ctx->gPO = nullptr;
-  if (getenv("MB_REPORT"))
-    fprintf(stderr, "[mose_b200] autotune: k-chunks %d %d %d %d (depth classes), main list %s (plain %.3f ms, "
-                    "persistent %.3f ms, %d tiles), one-plane list %s (plain %.3f ms, persistent %.3f ms, %d tiles), "
-                    "staging %s (6-value %.3f ms, 5-value %.3f ms)\n",
+  if (getenv("MB_REPORT")) {
+    const bool mixed = ctx->sc.precision == MB_PREC_MIXED, mapped = mixed && tmap_of(ctx, P, s, false);
+    auto label = [&](bool tma) {
+      return !mixed ? "none (FP64 form)" : !tma ? "6-value tile, plain loads"
+                                       : mapped ? "5-value tile, TMA" : "5-value tile, plain loads (no tensor map)";
+    };
+    fprintf(stderr, "[mose_b200] autotune: k-chunks %d %d %d %d (depth classes); main list: %s (plain %.3f ms, "
+                    "persistent %.3f ms, %d tiles), staging %s (6-value %.3f ms, 5-value %.3f ms); one-plane list: %s "
+                    "(plain %.3f ms, persistent %.3f ms, %d tiles), staging %s (6-value %.3f ms, 5-value %.3f ms)\n",
             ctx->kcls[0], ctx->kcls[1], ctx->kcls[2], ctx->kcls[3], ctx->persistent ? "persistent" : "plain", ms_plain,
-            ms_pers, ctx->ntiles_sweep, ctx->persistent_km ? "persistent" : "plain", km_plain, km_pers,
-            ctx->ntiles_km,
-            ctx->sc.precision != MB_PREC_MIXED ? "none (FP64 form)"
-            : !ctx->stage_tma                  ? "6-value tile, plain loads"
-            : tmap_of(ctx, P, s, false)        ? "5-value tile, TMA"
-                                               : "5-value tile, plain loads (no tensor map)",
-            ms_stage[0], ms_stage[1]);
+            ms_pers, ctx->ntiles_sweep, label(ctx->stage_tma), ms_stage[0], ms_stage[1],
+            ctx->persistent_km ? "persistent" : "plain", km_plain, km_pers, ctx->ntiles_km, label(ctx->stage_tma_km),
+            ms_stage_km[0], ms_stage_km[1]);
+  }
   return MB_OK;
 }
 

@@ -64,8 +64,12 @@ struct Tile {
   }
 };
 
-// the plane slot of plane kk (kk >= -1)
-MB_HD int slot_of(int kk) { return (kk + 8) & 3; }
+// the plane slot of plane kk (kk >= -1); the tile of a mirrored one-plane block (KM) holds its one plane only
+template <bool KM = false>
+MB_HD int slot_of(int kk) { return KM ? 0 : (kk + 8) & 3; }
+// planes held by the state tile
+template <bool KM>
+MB_HD constexpr int tile_planes() { return KM ? 1 : 4; }
 
 // One interior face of direction d between cell (i,j,k) and its +d neighbour, from the state tile: the
 // convective flux (conv_physics.inc) into out[0..4] and, for Navier-Stokes, the viscous flux
@@ -76,8 +80,7 @@ template <typename R, int TY, bool VISC, int RS = 0, int LIM = 0, bool KM = fals
 MB_HD void face_flux(const Params& p, const DBlk& b, const Tile<R, TY, NVT>& T, int d, int i, int j, int k, int ii,
                      int jj, R* out) {
   // a mirrored block (one cell deep in k, extrapolated k faces) reads its k = 1 plane for the k ghosts
-  const int skm = slot_of(KM ? k : k - 1), sk = slot_of(k), sk1 = slot_of(KM ? k : k + 1),
-            sk2 = slot_of(k + 2);
+  const int skm = slot_of<KM>(k - 1), sk = slot_of<KM>(k), sk1 = slot_of<KM>(k + 1), sk2 = slot_of<KM>(k + 2);
   const int l0 = lin32(b, i, j, k);
   const int st = (d == 0) ? 1 : (d == 1 ? b.pi : b.pi * b.pj);
   // the 4-cell stencil along d
@@ -1343,10 +1346,10 @@ __device__ __forceinline__ void put_cell(const Params& p, const Tile<R, TY, NVT>
   }
 }
 
-template <typename R, int TY, int NVT>
+template <typename R, int TY, int NVT, bool KM>
 __device__ __forceinline__ void stage_plane(const Params& p, const DBlk& b, const double* __restrict__ P,
                                             const Tile<R, TY, NVT>& T, int i0, int j0, int kk, int jext) {
-  const int sl = slot_of(kk);
+  const int sl = slot_of<KM>(kk);
   const long long nc = p.nc;
   for (int c = threadIdx.x; c < TXH * (TY + 4); c += blockDim.x) {
     const int jj = c / TXH, ii = c - jj * TXH;
@@ -1433,10 +1436,10 @@ struct TmaStage {
 };
 
 // convert the landed raw plane into the tile slot of plane kk (the same cells and values as stage_plane)
-template <typename R, int TY, int NVT>
+template <typename R, int TY, int NVT, bool KM>
 __device__ __forceinline__ void stage_plane_raw(const Params& p, const DBlk& b, const unsigned char* raw,
                                                 const Tile<R, TY, NVT>& T, int i0, int j0, int kk, int jext) {
-  const int sl = slot_of(kk);
+  const int sl = slot_of<KM>(kk);
   for (int c = threadIdx.x; c < TXH * (TY + 4); c += blockDim.x) {
     const int jj = c / TXH, ii = c - jj * TXH;
     const int i = i0 - 2 + ii, j = j0 - 2 + jj;
@@ -1476,7 +1479,7 @@ __device__ __forceinline__ bool sweep_tile(const Params& p, const DTile t, const
   Tile<R, TY, NVT> T;
   T.base = reinterpret_cast<R*>(smem_raw);                                       // [4][NVT][TY+4][36]
   T.rg = (R)p.ri;
-  unsigned char* fbase = smem_raw + sizeof(R) * 4 * NVT * (TY + 4) * TXH;
+  unsigned char* fbase = smem_raw + sizeof(R) * tile_planes<KM>() * NVT * (TY + 4) * TXH;
   RowI* sFi = reinterpret_cast<RowI*>(fbase);                                     // [TY][33][NS]
   RowJ* sFj = reinterpret_cast<RowJ*>(fbase + sizeof(R) * TY * 33 * NS);          // [TY+1][32][NS]
   // the k-faces: the face above a cell is computed by the thread of that cell and is the face below it on the next
@@ -1519,10 +1522,10 @@ __device__ __forceinline__ bool sweep_tile(const Params& p, const DTile t, const
       const bool ok = mbar_wait(bar, phase);
       phase ^= 1u;
       if (gave_up(ok)) return false;
-      stage_plane_raw<R, TY, NVT>(p, b, raw, T, t.i0, t.j0, kk, jext);
+      stage_plane_raw<R, TY, NVT, KM>(p, b, raw, T, t.i0, t.j0, kk, jext);
       __syncthreads();  // the staging buffer is free again
     } else {
-      stage_plane<R, TY, NVT>(p, b, Pin, T, t.i0, t.j0, kk, jext);
+      stage_plane<R, TY, NVT, KM>(p, b, Pin, T, t.i0, t.j0, kk, jext);
     }
   }
   // the first plane of the loop in flight while the k-face below is computed
@@ -1548,9 +1551,9 @@ __device__ __forceinline__ bool sweep_tile(const Params& p, const DTile t, const
         const bool ok = mbar_wait(bar, phase);
         phase ^= 1u;
         if (gave_up(ok)) return false;
-        stage_plane_raw<R, TY, NVT>(p, b, raw, T, t.i0, t.j0, k + 2, jext);
+        stage_plane_raw<R, TY, NVT, KM>(p, b, raw, T, t.i0, t.j0, k + 2, jext);
       } else {
-        stage_plane<R, TY, NVT>(p, b, Pin, T, t.i0, t.j0, k + 2, jext);
+        stage_plane<R, TY, NVT, KM>(p, b, Pin, T, t.i0, t.j0, k + 2, jext);
       }
     }
     __syncthreads();  // plane k+2 staged, and every pass 2 of plane k-1 done (the flux buffers are free)
@@ -1730,16 +1733,17 @@ __device__ __forceinline__ bool sweep_tile(const Params& p, const DTile t, const
 }
 
 // shared memory of the sweep: the state tile and the face-flux buffers (sweep_smem_core), and in the mixed form the
-// TMA staging buffer of one plane (TY+4 row slots) with its 128-byte alignment slack
-template <typename R, int TY, bool VISC, int STG = STG_PLAIN>
+// TMA staging buffer of one plane (TY+4 row slots) with its 128-byte alignment slack. The tiles of mirrored one-plane
+// blocks (KM) hold one plane and have no k faces (no k-face buffers): a quarter of the tile, more CTAs per SM
+template <typename R, int TY, bool VISC, int STG = STG_PLAIN, bool KM = false>
 MB_HD constexpr size_t sweep_smem_core() {
-  return sizeof(R) * ((size_t)4 * Stg<R, STG>::nv * (TY + 4) * TXH +
-                      (size_t)(TY * 33 + (TY + 1) * 32 + (Stg<R, STG>::kreg ? 0 : 2 * TY * 32)) *
+  return sizeof(R) * ((size_t)tile_planes<KM>() * Stg<R, STG>::nv * (TY + 4) * TXH +
+                      (size_t)(TY * 33 + (TY + 1) * 32 + ((Stg<R, STG>::kreg || KM) ? 0 : 2 * TY * 32)) *
                           ((VISC && !Fast<R>::on) ? 2 * MB_NP : MB_NP));
 }
-template <typename R, int TY, bool VISC, int STG = STG_PLAIN>
+template <typename R, int TY, bool VISC, int STG = STG_PLAIN, bool KM = false>
 MB_HD constexpr size_t sweep_smem() {
-  return sweep_smem_core<R, TY, VISC, STG>() +
+  return sweep_smem_core<R, TY, VISC, STG, KM>() +
          (Stg<R, STG>::tma ? (size_t)128 + (size_t)(TY + 4) * TMA_ROW_BYTES : 0);
 }
 
@@ -1762,7 +1766,7 @@ k_sweep(Params p, const DTile* __restrict__ tiles, const double* __restrict__ Pi
   static_assert(TY <= 8, "one residual slot per warp");
   TmaStage ts{nullptr, &s_bar, 0u};
   if (Stg<R, STG>::tma) {  // the staging buffer after the tile and the flux buffers, 128-byte aligned
-    unsigned char* q = smem_raw + sweep_smem_core<R, TY, VISC, STG>();
+    unsigned char* q = smem_raw + sweep_smem_core<R, TY, VISC, STG, KM>();
     ts.halo = q + ((128u - (smem_addr(q) & 127u)) & 127u);
     if (p.tmap) {
       if (threadIdx.x == 0) mbar_init(&s_bar);

@@ -49,7 +49,8 @@ constexpr int TY_AUX = 8;    // tile rows of the per-cell kernels (dt, update)
                              cudaStream_t s);                                                                    \
   cudaError_t name##_dt(const Params& p, const DTile* tiles, int ntiles, const double* P, int only_group,       \
                         cudaStream_t s);                                                                         \
-  int name##_occupancy(int visc);
+  int name##_occupancy(int visc);                                                                            \
+  int name##_occupancy_km(int visc);
 MB_DECLARE_SWEEP(sweep_f64_rs1)
 MB_DECLARE_SWEEP(sweep_f64_rs4)
 MB_DECLARE_SWEEP(sweep_f64_rs12)

@@ -123,6 +123,7 @@ struct Params {
   int* queue;              // persistent sweep: the tile counter (null: one CTA per tile)
   int ntiles_run;          // tiles of the launch (persistent sweep)
   int pgrid;               // CTAs of a persistent launch (resident CTAs per SM x SMs)
+  int pgrid_km;            // the same for the tiles of mirrored one-plane blocks (their own occupancy)
   int n_rk;                // 4: classical RK4 through the accumulator acc4
   int irk;                 // stage of the launch (1-based; set per launch)
   double* acc4;            // RK4: conserved accumulator (nc, 5), null otherwise
