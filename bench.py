@@ -222,19 +222,32 @@ def accuracy_at_config_steps(case, dev, stream, local):
     return _err_norms(case, st["fp64"], st["mixed"]), _err_norms(case, st["fp64_fast"], st["mixed"])
 
 
-def run_fixed_steps(case, steps, warmup, dev, stream):
+def run_fixed_steps(case, steps, warmup, dev, stream, args=None):
     """Both forms of one case for warmup + steps graph-replayed steps; device time of the timed steps
-    (CUDA events on the launching stream), cell-updates/s, launches and the mixed-vs-FP64 error."""
+    (CUDA events on the launching stream), cell-updates/s, launches and the mixed-vs-FP64 error. A profiling run
+    (args.tuning set) takes args' forms, steps, warm-up, fixed tile configuration and staging instead."""
     import torch
     from mosegpu import abi
     from mosegpu.engine import Engine
     out = {}
     states = {}
-    for name, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
+    forms = (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED))
+    prof = args is not None and bool(args.tuning)
+    if prof:
+        forms = [f for f in forms if f[0] in args.forms.split(",")]
+        steps, warmup = args.steps, args.warmup
+    for name, prec in forms:
         eng = Engine(case, precision=prec, device=dev.index, stream=stream)
         with torch.cuda.stream(stream):
             eng.step(1, graph=True)
-            tuning = eng.autotune()          # k-chunk, queue and (mixed) staging, timed on this state
+            if prof:
+                kc, pers = (int(x) for x in args.tuning.split(","))
+                eng.set_tuning(kc, pers)
+                tuning = (kc, pers)
+                if prec == abi.PREC_MIXED and args.staging != "auto":
+                    eng.set_staging(1 if args.staging == "tma" else 0)
+            else:
+                tuning = eng.autotune()      # k-chunk, queue and (mixed) staging, timed on this state
             eng.step(warmup - 1, graph=True)
         torch.cuda.synchronize(dev)
         l0 = eng.launches
@@ -257,8 +270,9 @@ def run_fixed_steps(case, steps, warmup, dev, stream):
         eng.close()
         del eng
         torch.cuda.empty_cache()
-    out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
-    out["mixed_vs_fp64_error_after_%d_steps" % (steps + warmup)] = _err_norms(case, states["fp64"], states["mixed"])
+    if "fp64" in out and "mixed" in out:
+        out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+        out["mixed_vs_fp64_error_after_%d_steps" % (steps + warmup)] = _err_norms(case, states["fp64"], states["mixed"])
     return out
 
 
@@ -269,7 +283,7 @@ def run_c3(args, dev, stream):
     t0 = time.time()
     case = cs.multiblock_2d()
     setup = time.time() - t0
-    r = run_fixed_steps(case, case.steps - 3, 3, dev, stream)
+    r = run_fixed_steps(case, case.steps - 3, 3, dev, stream, args)
     r["config"] = {"workload": "mb2d_8x6_ns_ausm_vanleer_rk4", "cells": case.n_interior, "blocks": len(case.blocks),
                    "widths": case.meta["widths"], "heights": case.meta["heights"], "steps": case.steps,
                    "setup_s": round(setup, 1)}
@@ -283,7 +297,7 @@ def run_c5(args, dev, stream):
     t0 = time.time()
     case = cs.taylor_green_blocks(nb=4, nblk=128, steps=50)
     setup = time.time() - t0
-    r = run_fixed_steps(case, case.steps - 3, 3, dev, stream)
+    r = run_fixed_steps(case, case.steps - 3, 3, dev, stream, args)
     r["config"] = {"workload": "tgv_4x4x4_128_ns_hllc_vanalbada_ssprk3", "cells": case.n_interior,
                    "blocks": len(case.blocks), "steps": case.steps, "setup_s": round(setup, 1)}
     return r
