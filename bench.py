@@ -337,15 +337,24 @@ def run_serving(args, dev, world=1, rank=0, pg=None):
     reqs_all = [sv.riemann_request(q, d, n, st, te, arrival=t) for q, (t, d, n, st, te) in enumerate(stream)]
     reqs = partition_requests(reqs_all, world, rank)
     setup = time.time() - t0
-    # two lanes: 1-D cases (cheap steps, many of them) and 2-D cases, each its own context and stream
+    # lanes, each its own context and stream: 1-D cases (cheap steps, many of them) and 2-D cases; with three lanes
+    # the 2-D cases of N >= serve_split go to a lane of their own, so that a small 2-D case does not advance at the
+    # step time of the largest ones
     budget = int(args.serve_budget_gb * 2 ** 30)
-    lanes = [sv.Server(reqs[0].case.scheme, reqs[0].case.thermo, budget_bytes=min(2 << 30, budget // 4),
-                       max_cases=128, precision=abi.PREC_MIXED, device=dev.index, poll_steps=args.serve_poll),
-             sv.Server(reqs[0].case.scheme, reqs[0].case.thermo, budget_bytes=budget - min(2 << 30, budget // 4),
-                       max_cases=128, precision=abi.PREC_MIXED, device=dev.index, poll_steps=args.serve_poll)]
+    b1 = min(2 << 30, budget // 4)
+    nl = 3 if args.serve_lanes == 3 else 2
+    shares = [b1] + ([budget - b1] if nl == 2 else [(budget - b1) // 3, budget - b1 - (budget - b1) // 3])
+    lanes = [sv.Server(reqs[0].case.scheme, reqs[0].case.thermo, budget_bytes=bb, max_cases=128,
+                       precision=abi.PREC_MIXED, device=dev.index, poll_steps=args.serve_poll) for bb in shares]
+
+    def route(r):
+        n = r.case.blocks[0]["n"]
+        if n[1] == 1:
+            return 0
+        return 2 if (nl == 3 and n[0] >= args.serve_split) else 1
     if pg is not None:
         barrier(pg, dev)
-    done = sv.serve_lanes(lanes, lambda r: 0 if r.case.blocks[0]["n"][1] == 1 else 1, reqs, max_wall=args.serve_max_s)
+    done = sv.serve_lanes(lanes, route, reqs, max_wall=args.serve_max_s)
     for lane in lanes:
         lane.close()
     part = ([r.finish - r.arrival for r in done], min(r.arrival for r in reqs) if reqs else None,
@@ -356,7 +365,10 @@ def run_serving(args, dev, world=1, rank=0, pg=None):
         parts = [None] * world
         pg.all_gather_object(parts, part)
     out = {"cases_submitted": len(reqs_all), **merge_serving(parts), "arrival_rate_per_s": args.serve_rate,
-           "poll_steps": args.serve_poll, "lanes": "2 (1-D cases | 2-D cases), one context and stream each",
+           "poll_steps": args.serve_poll,
+           "lanes": ("2 (1-D cases | 2-D cases)" if nl == 2 else
+                     "3 (1-D cases | 2-D cases N < %d | 2-D cases N >= %d)" % (args.serve_split, args.serve_split))
+           + ", one context and stream each",
            "budget_gb": args.serve_budget_gb, "precision": "mixed", "setup_s": round(setup, 1),
            "sample": "the first %d cases of the seeded 4096-case stream (half 1-D N in [256, 8192], half 2-D N^2 "
                      "with N in [128, 1024], log-uniform), Poisson arrivals" % len(reqs_all)}
@@ -445,6 +457,9 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=3.0, help="Poisson arrivals per second")
     ap.add_argument("--serve-budget-gb", type=float, default=32.0)
     ap.add_argument("--serve-poll", type=int, default=16, help="steps between reads of the case clocks")
+    ap.add_argument("--serve-lanes", type=int, default=3, choices=[2, 3],
+                    help="2: 1-D | 2-D cases; 3: 1-D | small 2-D | large 2-D cases")
+    ap.add_argument("--serve-split", type=int, default=512, help="the N of the 2-D cases of the third lane")
     ap.add_argument("--serve-max-s", type=float, default=240.0)
     args = ap.parse_args()
     if args.impl == "reference":

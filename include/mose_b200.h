@@ -361,6 +361,15 @@ int mb_stage_end(mb_ctx* ctx, double* P, double* PO, int irk, void* stream);
 int mb_pack_rows(const double* P, int64_t ncell, const int64_t* rows, int32_t n, double* buf, void* stream);
 int mb_unpack_rows(double* P, int64_t ncell, const int64_t* rows, int32_t n, const double* buf, void* stream);
 
+/* The same halo rows moved in one kernel from the owner's stage input into the receiver's, without a buffer or a
+ * send / receive: dst[dst_rows[q] + v * ndst] = src[src_rows[q] + v * nsrc], launched on the owner's stream. dst is
+ * the receiver's arena: on the same GPU, or on a peer GPU of the same node with peer access enabled (the stores
+ * cross NVLink; a pointer from cudaIpcOpenMemHandle in a multi-process host). src_rows and dst_rows are device arrays
+ * on the owner's GPU. The receiver's next launch must be ordered after this one (an event, or a barrier between the
+ * processes). */
+int mb_push_rows(const double* src, int64_t nsrc, const int64_t* src_rows, double* dst, int64_t ndst,
+                 const int64_t* dst_rows, int32_t n, void* stream);
+
 /* Status of case 0 (state check, thermo guard, first offender, simulated time, last dt). Synchronises. */
 int mb_get_status(mb_ctx* ctx, mb_status* st);
 

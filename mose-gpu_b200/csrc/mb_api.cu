@@ -1269,6 +1269,14 @@ int mb_unpack_rows(double* P, int64_t ncell, const int64_t* rows, int32_t n, con
   return MB_OK;
 }
 
+int mb_push_rows(const double* src, int64_t nsrc, const int64_t* src_rows, double* dst, int64_t ndst,
+                 const int64_t* dst_rows, int32_t n, void* stream) {
+  if (!src || !dst || nsrc < 1 || ndst < 1 || n < 0 || (n > 0 && (!src_rows || !dst_rows))) return MB_E_ARG;
+  if (n == 0) return MB_OK;
+  CK(push_rows(src, nsrc, (const long long*)src_rows, dst, ndst, (const long long*)dst_rows, n, (cudaStream_t)stream));
+  return MB_OK;
+}
+
 int mb_stage(mb_ctx* ctx, double* P, double* PO, int irk, void* stream) {
   if (!ctx || !P || !PO || irk < 1 || irk > ctx->sc.n_rk) return MB_E_ARG;
   CK(cudaSetDevice(ctx->device));

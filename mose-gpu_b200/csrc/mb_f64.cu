@@ -231,6 +231,24 @@ __global__ void k_unpack_rows(double* __restrict__ P, long long nc, const long l
   P[rows[e] + v * nc] = buf[q];
 }
 
+// the halo rows moved straight from the owner's stage input into the receiver's (another arena, on this GPU or a
+// peer's: the stores cross NVLink, no staging buffer and no send / receive): one thread per row and variable, the
+// loads local, the stores posted to the receiver
+__global__ void k_push_rows(const double* __restrict__ src, long long nsrc, const long long* __restrict__ srows,
+                            double* __restrict__ dst, long long ndst, const long long* __restrict__ drows, int n) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long long)n * MB_NP) return;
+  const int v = (int)(q / n), e = (int)(q - (long long)v * n);
+  dst[drows[e] + v * ndst] = src[srows[e] + v * nsrc];
+}
+
+cudaError_t push_rows(const double* src, long long nsrc, const long long* srows, double* dst, long long ndst,
+                      const long long* drows, int n, cudaStream_t s) {
+  const long long tot = (long long)n * MB_NP;
+  k_push_rows<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(src, nsrc, srows, dst, ndst, drows, n);
+  return cudaGetLastError();
+}
+
 cudaError_t pack_rows(const double* P, long long ncell, const long long* rows, int n, double* buf, cudaStream_t s) {
   const long long tot = (long long)n * MB_NP;
   k_pack_rows<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(P, ncell, rows, n, buf);

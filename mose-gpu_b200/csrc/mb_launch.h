@@ -99,6 +99,9 @@ cudaError_t to_float(const double* src, float* dst, long long n, cudaStream_t s)
 // halo rows of a partitioned mesh: buf[v * n + q] <-> P[rows[q] + v * ncell] (mb_pack_rows / mb_unpack_rows)
 cudaError_t pack_rows(const double* P, long long ncell, const long long* rows, int n, double* buf, cudaStream_t s);
 cudaError_t unpack_rows(double* P, long long ncell, const long long* rows, int n, const double* buf, cudaStream_t s);
+// dst[drows[q] + v * ndst] = src[srows[q] + v * nsrc] (mb_push_rows; dst may be a peer GPU's memory)
+cudaError_t push_rows(const double* src, long long nsrc, const long long* srows, double* dst, long long ndst,
+                      const long long* drows, int n, cudaStream_t s);
 cudaError_t clock_step(const Params& p, cudaStream_t s);
 // the TMA staging's bounded mbarrier wait, made to run out (mb_selftest_bounded_wait)
 cudaError_t wait_selftest(unsigned tries, int* gave_up, cudaStream_t s);

@@ -25,6 +25,8 @@ step (mpi_allreduce_min_r8, Mod_MPI.f90:571-581). Here:
   DistExchange      the exchange between processes over torch.distributed (NCCL on GPUs: grouped send / recv
                     of each pair's packed rows; gloo on the CPU).
   LocalExchange     the exchange between rank drivers of one process (device copies; ranks emulated on one GPU).
+  PeerExchange      the same without buffers: one kernel per pair stores the owner's rows straight into the
+                    receiver's arena (mb_push_rows: same GPU, or a peer GPU over NVLink).
 
 Scope: 3-D blocks (n3 > 1) with 1:1 / periodic connections; donor blocks one cell deep (2-D meshes, whose k
 ghosts are mirrored) are refused. The oracle counterpart (tests/test_multi_rank.py) runs the same schedule on the
@@ -205,6 +207,49 @@ class LocalExchange:
         return min(values)
 
 
+class PeerExchange:
+    """Moves halo rows between rank drivers of one process by peer stores: per round and ordered pair, one
+    mb_push_rows on the owner's stream from its stage input straight into the receiver's (on the same GPU, or on a
+    peer GPU with peer access: the stores cross NVLink), no staging buffer and no send / receive; the receiver's
+    stream then waits for the owner's (a CUDA event). The reference's persistent exchange
+    (Mod_GhostExchange.f90:685-957) with the buffers and the messages taken out."""
+
+    def __init__(self, drivers, plan):
+        import torch
+        self.drivers = drivers
+        self.plan = plan
+        for (q, r) in plan:
+            dq, dr = drivers[q].dev, drivers[r].dev
+            if dq != dr and not torch.cuda.can_device_access_peer(dq.index, dr.index):
+                raise RuntimeError("no peer access from GPU %d to GPU %d" % (dq.index, dr.index))
+
+    def __call__(self, rnd):
+        import torch
+        waits = {}
+        for (q, r), rows in self.plan.items():
+            src, dst = rows[2 * rnd], rows[2 * rnd + 1]
+            if not len(src):
+                continue
+            a, b = self.drivers[q], self.drivers[r]
+            rc = a.eng.lib.mb_push_rows(a.cur_in, a.rc.case.ncell, a._dev_rows(src).data_ptr(), b.cur_in,
+                                        b.rc.case.ncell, a._dev_rows(dst).data_ptr(), len(src), a._s())
+            if rc != abi.MB_OK:
+                raise abi.MoseError(rc, "mb_push_rows")
+            waits.setdefault(r, set()).add(q)
+        for r, owners in waits.items():
+            b = self.drivers[r]
+            for q in owners:
+                a = self.drivers[q]
+                if a.ts.cuda_stream == b.ts.cuda_stream:
+                    continue
+                ev = torch.cuda.Event()
+                ev.record(a.ts)
+                b.ts.wait_event(ev)
+
+    def min_all(self, values):
+        return min(values)
+
+
 class DistExchange:
     """Moves halo rows between processes over torch.distributed: per round, every rank packs what each peer needs and
     the pairs exchange with one grouped send / receive (batch_isend_irecv), then every rank unpacks."""
@@ -244,16 +289,18 @@ class EngineRank:
     """One rank's blocks on its GPU, stepped through the split stage calls of the C ABI (mosegpu.engine.Engine for
     the context and the state buffers)."""
 
-    def __init__(self, rank_case, precision=abi.PREC_FP64, device=0):
+    def __init__(self, rank_case, precision=abi.PREC_FP64, device=0, stream=None):
         import torch
         from .engine import Engine
         self.torch = torch
         self.rc = rank_case
-        self.eng = Engine(rank_case.case, precision=precision, device=device)
+        self.eng = Engine(rank_case.case, precision=precision, device=device, stream=stream)
         self.dev = self.eng.dev
+        self.ts = stream if stream is not None else torch.cuda.current_stream(self.dev)   # the rank's stream
         self._rows = {}
         self._bufs = {}
-        self.dtbuf = torch.zeros(1, dtype=torch.int64, device=self.dev)
+        with torch.cuda.stream(self.ts):
+            self.dtbuf = torch.zeros(1, dtype=torch.int64, device=self.dev)
         self.cur_in = self.eng.P.data_ptr()     # the device buffer the current stage reads (set_stage)
 
     def set_stage(self, irk):
@@ -272,14 +319,16 @@ class EngineRank:
     def _dev_rows(self, rows):
         key = (rows.ctypes.data, len(rows))
         if key not in self._rows:
-            self._rows[key] = (rows, self.torch.from_numpy(rows).to(self.dev))
+            with self.torch.cuda.stream(self.ts):
+                self._rows[key] = (rows, self.torch.from_numpy(rows).to(self.dev))
         return self._rows[key][1]
 
     def pack(self, rows, rnd, tag):
         d = self._dev_rows(rows)
         key = (tag, rnd)
         if key not in self._bufs or self._bufs[key].numel() != NP * len(rows):
-            self._bufs[key] = self.torch.empty(NP * len(rows), dtype=self.torch.float64, device=self.dev)
+            with self.torch.cuda.stream(self.ts):
+                self._bufs[key] = self.torch.empty(NP * len(rows), dtype=self.torch.float64, device=self.dev)
         buf = self._bufs[key]
         rc = self.eng.lib.mb_pack_rows(self.cur_in, self.rc.case.ncell, d.data_ptr(), len(rows), buf.data_ptr(),
                                        self._s())
@@ -304,11 +353,13 @@ class EngineRank:
             rc = getattr(e.lib, f)(*a)
             if rc != abi.MB_OK:
                 raise abi.MoseError(rc, f)
+        self.ts.synchronize()
         return float(self.dtbuf.view(self.torch.float64).item())
 
     def start(self, dtmin):
         e = self.eng
-        self.dtbuf.view(self.torch.float64).fill_(dtmin)
+        with self.torch.cuda.stream(self.ts):
+            self.dtbuf.view(self.torch.float64).fill_(dtmin)
         for f, a in (("mb_copy_dtmin", (e.ctx, 0, self.dtbuf.data_ptr(), 1, self._s())),
                      ("mb_step_start", (e.ctx, self._s()))):
             rc = getattr(e.lib, f)(*a)
@@ -323,6 +374,7 @@ class EngineRank:
             raise abi.MoseError(rc, f)
 
     def state(self):
+        self.ts.synchronize()
         return self.eng.state()
 
 

@@ -160,6 +160,28 @@ def test_staging_modes_agree_within_the_mixed_form(torch_cuda):
     assert np.all(e < 1e-6), e
 
 
+def test_staging_mode_of_each_tile_list(torch_cuda):
+    """mb_set_staging sets the staging of both tile lists and mb_get_staging_mode reports it; mb_autotune chooses
+    each list's staging by time, and on a mesh of one-plane blocks only (the 2-D batch) reports the one-plane list's.
+    The two stagings of the one-plane tiles agree within the mixed form's rounding of p."""
+    from mosegpu import case as cs
+    from mosegpu.engine import Engine
+    case = cs.multiblock_2d(cols=3, rows=2, lo=9, hi=40, seed=11)
+    a, b = Engine(case, precision=abi.PREC_MIXED), Engine(case, precision=abi.PREC_MIXED)
+    a.set_staging(1)
+    b.set_staging(0)
+    assert a.staging_mode() == 1 and b.staging_mode() == 0
+    assert b.staging_label() == "6-value tile, plain loads"
+    a.step(8, graph=True)
+    b.step(8, graph=True)
+    e = H.rel_err(H.conserved(case, a.state()), H.conserved(case, b.state()))
+    assert np.all(e < 1e-6), e
+    a.autotune()
+    assert a.staging_mode() in (0, 1)
+    a.step(2, graph=True)
+    assert a.status().code == 0 and a.status().steps == 10
+
+
 def test_bounded_wait_runs_out_and_the_device_stays_usable(torch_cuda):
     """The TMA staging waits on its mbarrier with an iteration limit: a wait on a phase nothing completes gives up and
     the kernel returns (the device then runs the next work as usual)."""

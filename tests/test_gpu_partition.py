@@ -1,7 +1,8 @@
 """Blocks partitioned over ranks on the GPU path (mosegpu/partition.py through the C ABI): two ranks emulated as two
 engine contexts on one GPU (mb_step_prepare / mb_copy_dtmin / mb_step_start, the split stages, the halo rows moved
-by mb_pack_rows / mb_unpack_rows), stepped in the order a two-process run follows, against one context holding every
-block. No kernel of one rank waits on the other: the exchange is stream-ordered copies between the steps' calls."""
+by mb_pack_rows / mb_unpack_rows, or stored straight into the receiver's arena by mb_push_rows), stepped in the order a
+two-process run follows, against one context holding every block. No kernel of one rank waits on the other: the
+exchange is stream-ordered between the steps' calls."""
 import numpy as np
 import pytest
 
@@ -18,9 +19,10 @@ def torch_cuda():
     return torch
 
 
+@pytest.mark.parametrize("exchange", ["copies", "peer stores", "peer stores, own streams"])
 @pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED])
 @pytest.mark.parametrize("nranks", [2, 3])
-def test_partitioned_engine_matches_one_context(torch_cuda, precision, nranks):
+def test_partitioned_engine_matches_one_context(torch_cuda, precision, nranks, exchange):
     from mosegpu import case as cs
     from mosegpu import partition as pt
     from mosegpu.engine import Engine
@@ -29,8 +31,10 @@ def test_partitioned_engine_matches_one_context(torch_cuda, precision, nranks):
     owner = pt.partition_blocks(case, nranks)
     ranks = [pt.split_case(case, owner, r) for r in range(nranks)]
     plan = pt.halo_plan(case, owner, ranks, visc=True)
-    drivers = [pt.EngineRank(rc, precision=precision) for rc in ranks]
-    pt.step_ranks(drivers, pt.LocalExchange(drivers, plan), True, case.scheme["n_rk"], nsteps=steps)
+    streams = [torch_cuda.cuda.Stream() if "own streams" in exchange else None for _ in ranks]
+    drivers = [pt.EngineRank(rc, precision=precision, stream=st) for rc, st in zip(ranks, streams)]
+    ex = pt.LocalExchange(drivers, plan) if exchange == "copies" else pt.PeerExchange(drivers, plan)
+    pt.step_ranks(drivers, ex, True, case.scheme["n_rk"], nsteps=steps)
     one = Engine(case, precision=precision)
     one.step(steps, graph=False)
     P1 = one.state()
