@@ -370,6 +370,11 @@ int mb_unpack_rows(double* P, int64_t ncell, const int64_t* rows, int32_t n, con
 int mb_push_rows(const double* src, int64_t nsrc, const int64_t* src_rows, double* dst, int64_t ndst,
                  const int64_t* dst_rows, int32_t n, void* stream);
 
+/* Lets kernels running on `device` store into `peer`'s memory (cudaDeviceEnablePeerAccess, once per ordered pair of
+ * devices and process; already enabled is success, the same device is success): the precondition of mb_push_rows
+ * into a peer GPU's arena from one process. MB_E_UNSUPPORTED where the two GPUs have no peer path. */
+int mb_enable_peer(int device, int peer);
+
 /* Status of case 0 (state check, thermo guard, first offender, simulated time, last dt). Synchronises. */
 int mb_get_status(mb_ctx* ctx, mb_status* st);
 

@@ -1269,6 +1269,25 @@ int mb_unpack_rows(double* P, int64_t ncell, const int64_t* rows, int32_t n, con
   return MB_OK;
 }
 
+int mb_enable_peer(int device, int peer) {
+  if (device < 0 || peer < 0) return MB_E_ARG;
+  if (device == peer) return MB_OK;
+  int can = 0;
+  CK(cudaDeviceCanAccessPeer(&can, device, peer));
+  if (!can) return MB_E_UNSUPPORTED;
+  int cur = 0;
+  CK(cudaGetDevice(&cur));
+  CK(cudaSetDevice(device));
+  cudaError_t e = cudaDeviceEnablePeerAccess(peer, 0);
+  if (e == cudaErrorPeerAccessAlreadyEnabled) {
+    cudaGetLastError();  // the error of that call is not sticky: clear it
+    e = cudaSuccess;
+  }
+  cudaSetDevice(cur);
+  CK(e);
+  return MB_OK;
+}
+
 int mb_push_rows(const double* src, int64_t nsrc, const int64_t* src_rows, double* dst, int64_t ndst,
                  const int64_t* dst_rows, int32_t n, void* stream) {
   if (!src || !dst || nsrc < 1 || ndst < 1 || n < 0 || (n > 0 && (!src_rows || !dst_rows))) return MB_E_ARG;

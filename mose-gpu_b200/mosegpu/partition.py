@@ -215,13 +215,14 @@ class PeerExchange:
     (Mod_GhostExchange.f90:685-957) with the buffers and the messages taken out."""
 
     def __init__(self, drivers, plan):
-        import torch
         self.drivers = drivers
         self.plan = plan
         for (q, r) in plan:
             dq, dr = drivers[q].dev, drivers[r].dev
-            if dq != dr and not torch.cuda.can_device_access_peer(dq.index, dr.index):
-                raise RuntimeError("no peer access from GPU %d to GPU %d" % (dq.index, dr.index))
+            if dq != dr:                       # the owner's kernels store into the receiver's GPU
+                rc = drivers[q].eng.lib.mb_enable_peer(dq.index, dr.index)
+                if rc != abi.MB_OK:
+                    raise abi.MoseError(rc, "mb_enable_peer %d -> %d" % (dq.index, dr.index))
 
     def __call__(self, rnd):
         import torch

@@ -44,3 +44,17 @@ def test_partitioned_engine_matches_one_context(torch_cuda, precision, nranks, e
     st = [d.eng.status() for d in drivers]
     assert all(s.code == 0 and s.steps == steps for s in st)
     assert len({s.time for s in st}) == 1 and st[0].time == one.status().time
+
+
+def test_peer_access_entry_point(torch_cuda):
+    """mb_enable_peer: the same device is success; a device against every other GPU of the node either succeeds (twice:
+    already enabled is success) or reports that there is no peer path."""
+    from mosegpu.engine import load_library
+    L = load_library()
+    assert L.mb_enable_peer(0, 0) == abi.MB_OK
+    assert L.mb_enable_peer(-1, 0) == abi.MB_E_ARG
+    for peer in range(1, torch_cuda.cuda.device_count()):
+        rc = L.mb_enable_peer(0, peer)
+        assert rc in (abi.MB_OK, abi.MB_E_UNSUPPORTED)
+        if rc == abi.MB_OK:
+            assert L.mb_enable_peer(0, peer) == abi.MB_OK
