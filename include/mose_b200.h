@@ -375,6 +375,15 @@ int mb_push_rows(const double* src, int64_t nsrc, const int64_t* src_rows, doubl
  * into a peer GPU's arena from one process. MB_E_UNSUPPORTED where the two GPUs have no peer path. */
 int mb_enable_peer(int device, int peer);
 
+/* CUDA IPC of a stage buffer, for mb_push_rows between processes (one per GPU, or several on one GPU): mb_ipc_export
+ * writes the 64-byte handle of the allocation that ptr lies in, ptr's byte offset inside it and the allocation's size
+ * (a receiver checks that its arena fits); the owner's process maps it with mb_ipc_open (the base of the allocation,
+ * on `device`; add the offset) and unmaps it with mb_ipc_close. A handle cannot be opened in the process that exported
+ * it. */
+int mb_ipc_export(const void* ptr, void* handle, int64_t* offset, int64_t* size);
+int mb_ipc_open(const void* handle, int device, void** base);
+int mb_ipc_close(void* base);
+
 /* Status of case 0 (state check, thermo guard, first offender, simulated time, last dt). Synchronises. */
 int mb_get_status(mb_ctx* ctx, mb_status* st);
 

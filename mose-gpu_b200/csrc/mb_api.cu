@@ -1269,6 +1269,52 @@ int mb_unpack_rows(double* P, int64_t ncell, const int64_t* rows, int32_t n, con
   return MB_OK;
 }
 
+// ---- CUDA IPC of stage buffers (a peer-store exchange between processes)
+static PFN_cuMemGetAddressRange_v3020 addr_range_fn() {
+  static PFN_cuMemGetAddressRange_v3020 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuMemGetAddressRange_v3020)f;
+  }
+  return fn;
+}
+
+int mb_ipc_export(const void* ptr, void* handle, int64_t* offset, int64_t* size) {
+  if (!ptr || !handle || !offset || !size) return MB_E_ARG;
+  PFN_cuMemGetAddressRange_v3020 range = addr_range_fn();
+  if (!range) return MB_E_UNSUPPORTED;
+  CUdeviceptr base = 0;
+  size_t sz = 0;
+  if (range(&base, &sz, (CUdeviceptr)ptr) != CUDA_SUCCESS) return MB_E_ARG;  // not device memory
+  cudaIpcMemHandle_t h;
+  CK(cudaIpcGetMemHandle(&h, (void*)base));
+  static_assert(sizeof(h) == 64, "a CUDA IPC handle is 64 bytes");
+  memcpy(handle, &h, sizeof(h));
+  *offset = (int64_t)((const char*)ptr - (const char*)base);
+  *size = (int64_t)sz;
+  return MB_OK;
+}
+
+int mb_ipc_open(const void* handle, int device, void** base) {
+  if (!handle || !base || device < 0) return MB_E_ARG;
+  cudaIpcMemHandle_t h;
+  memcpy(&h, handle, sizeof(h));
+  CK(cudaSetDevice(device));
+  CK(cudaIpcOpenMemHandle(base, h, cudaIpcMemLazyEnablePeerAccess));
+  return MB_OK;
+}
+
+int mb_ipc_close(void* base) {
+  if (!base) return MB_E_ARG;
+  CK(cudaIpcCloseMemHandle(base));
+  return MB_OK;
+}
+
 int mb_enable_peer(int device, int peer) {
   if (device < 0 || peer < 0) return MB_E_ARG;
   if (device == peer) return MB_OK;

@@ -67,6 +67,11 @@ def load_library():
     L.mb_push_rows.argtypes = [vp, C.c_int64, vp, vp, C.c_int64, vp, C.c_int32, vp]
     L.mb_enable_peer.argtypes = [C.c_int, C.c_int]
     L.mb_enable_peer.restype = C.c_int
+    L.mb_ipc_export.argtypes = [vp, vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.mb_ipc_open.argtypes = [vp, C.c_int, C.POINTER(vp)]
+    L.mb_ipc_close.argtypes = [vp]
+    for f in ("mb_ipc_export", "mb_ipc_open", "mb_ipc_close"):
+        getattr(L, f).restype = C.c_int
     for f in ("mb_step_prepare", "mb_copy_dtmin", "mb_step_start", "mb_stage_begin", "mb_stage_end", "mb_pack_rows",
               "mb_unpack_rows", "mb_push_rows"):
         getattr(L, f).restype = C.c_int

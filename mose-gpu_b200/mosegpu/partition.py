@@ -27,6 +27,7 @@ step (mpi_allreduce_min_r8, Mod_MPI.f90:571-581). Here:
   LocalExchange     the exchange between rank drivers of one process (device copies; ranks emulated on one GPU).
   PeerExchange      the same without buffers: one kernel per pair stores the owner's rows straight into the
                     receiver's arena (mb_push_rows: same GPU, or a peer GPU over NVLink).
+  DistPeerExchange  the peer stores between processes: stage buffers mapped by CUDA IPC, a barrier per round.
 
 Scope: 3-D blocks (n3 > 1) with 1:1 / periodic connections; donor blocks one cell deep (2-D meshes, whose k
 ghosts are mirrored) are refused. The oracle counterpart (tests/test_multi_rank.py) runs the same schedule on the
@@ -251,6 +252,82 @@ class PeerExchange:
         return min(values)
 
 
+class DistPeerExchange:
+    """The peer-store exchange between processes (one per rank; on one node, one GPU each or several on one GPU): at
+    set-up every rank exports its stage buffers by CUDA IPC (mb_ipc_export) and maps those of the ranks it sends to
+    (mb_ipc_open), after checking on the host that every row it will write lies inside the receiver's arena and the
+    arena inside the mapped allocation. Per round each rank pushes its rows straight into the receivers' current
+    stage input (mb_push_rows), then all ranks meet: its stream drained, a barrier of the process group. No send /
+    receive, no staging buffer; no kernel waits on another rank."""
+
+    def __init__(self, driver, plan, rank, world, pg):
+        import ctypes as C
+        self.driver, self.plan, self.rank, self.world, self.pg = driver, plan, rank, world, pg
+        L = driver.eng.lib
+        self.bufs = driver.stage_buffers()
+        mine = []
+        for ptr in self.bufs:
+            h = (C.c_char * 64)()
+            off, size = C.c_int64(), C.c_int64()
+            rc = L.mb_ipc_export(ptr, h, C.byref(off), C.byref(size))
+            if rc != abi.MB_OK:
+                raise abi.MoseError(rc, "mb_ipc_export")
+            mine.append((bytes(h), off.value, size.value))
+        everyone = [None] * world
+        pg.all_gather_object(everyone, (mine, int(driver.rc.case.ncell)))
+        self.peer, self._bases, opened = {}, [], {}
+        for (q, r), rows in plan.items():
+            if q != rank or r in self.peer:
+                continue
+            theirs, nc = everyone[r]
+            if len(theirs) != len(self.bufs):
+                raise RuntimeError("rank %d has %d stage buffers, rank %d %d" % (r, len(theirs), rank, len(self.bufs)))
+            need = NP * nc * 8
+            for rr in (rows[1], rows[3]):
+                if len(rr) and (rr.min() < 0 or rr.max() >= nc):
+                    raise RuntimeError("halo row outside the arena of rank %d" % r)
+            ptrs = []
+            for h, off, size in theirs:
+                if off < 0 or off + need > size:
+                    raise RuntimeError("the arena of rank %d does not fit its allocation" % r)
+                if h not in opened:            # buffers in one allocation share its handle: map it once
+                    base = C.c_void_p()
+                    rc = L.mb_ipc_open(C.c_char_p(h), driver.dev.index, C.byref(base))
+                    if rc != abi.MB_OK:
+                        raise abi.MoseError(rc, "mb_ipc_open")
+                    opened[h] = base.value
+                    self._bases.append(base.value)
+                ptrs.append(opened[h] + off)
+            self.peer[r] = (ptrs, nc)
+
+    def __call__(self, rnd):
+        d = self.driver
+        k = self.bufs.index(d.cur_in)
+        for (q, r), rows in sorted(self.plan.items()):
+            src, dst = rows[2 * rnd], rows[2 * rnd + 1]
+            if q != self.rank or not len(src):
+                continue
+            ptrs, nc = self.peer[r]
+            rc = d.eng.lib.mb_push_rows(d.cur_in, d.rc.case.ncell, d._dev_rows(src).data_ptr(), ptrs[k], nc,
+                                        d._dev_rows(dst).data_ptr(), len(src), d._s())
+            if rc != abi.MB_OK:
+                raise abi.MoseError(rc, "mb_push_rows")
+        d.ts.synchronize()
+        self.pg.barrier()
+
+    def min_all(self, value):
+        import torch
+        t = torch.tensor([value], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MIN)
+        return float(t.item())
+
+    def close(self):
+        self.pg.barrier()                      # every rank's last push has landed before the mappings go
+        for b in self._bases:
+            self.driver.eng.lib.mb_ipc_close(b)
+        self._bases = []
+
+
 class DistExchange:
     """Moves halo rows between processes over torch.distributed: per round, every rank packs what each peer needs and
     the pairs exchange with one grouped send / receive (batch_isend_irecv), then every rank unpacks."""
@@ -316,6 +393,21 @@ class EngineRank:
 
     def _s(self):
         return self.eng._s()
+
+    def stage_buffers(self):
+        """The device buffers the stages read, in a fixed order: P, PO, then the engine's own (mb_stage_input over
+        the stages); a rank's stage irk reads the buffer of the same place in every rank's list."""
+        import ctypes as C
+        e = self.eng
+        out = [e.P.data_ptr(), e.PO.data_ptr()]
+        for irk in range(1, e.case.scheme["n_rk"] + 1):
+            ptr = C.c_void_p()
+            rc = e.lib.mb_stage_input(e.ctx, e.P.data_ptr(), e.PO.data_ptr(), irk, C.byref(ptr))
+            if rc != abi.MB_OK:
+                raise abi.MoseError(rc, "mb_stage_input")
+            if ptr.value not in out:
+                out.append(ptr.value)
+        return out
 
     def _dev_rows(self, rows):
         key = (rows.ctypes.data, len(rows))
