@@ -1,8 +1,8 @@
-"""Blocks partitioned over two processes, the halo rows stored straight into the other process's arena: each process
-holds one rank's engine context, exports its stage buffers by CUDA IPC and maps its peer's (mosegpu.partition.
-DistPeerExchange over a gloo process group for the barriers and the MIN all-reduce of dt). Both processes run on one
-GPU here; no kernel of one waits on the other (every round ends with the stream drained and a host barrier). The
-interiors after three steps equal one context holding every block, bit for bit."""
+"""Blocks partitioned over two or three processes, the halo rows stored straight into the other processes' arenas:
+each process holds one rank's engine context, exports its stage buffers by CUDA IPC and maps its receivers'
+(mosegpu.partition.DistPeerExchange over a gloo process group for the barriers and the MIN all-reduce of dt). The
+processes share one GPU here; no kernel of one waits on another (every round ends with the streams drained and a
+host barrier). The interiors after three steps equal one context holding every block, bit for bit."""
 import os
 import socket
 import sys
@@ -65,8 +65,9 @@ def _rank(rank, world, port, precision, steps, q):
     q.put(out)
 
 
+@pytest.mark.parametrize("nranks", [2, 3])
 @pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED])
-def test_two_processes_push_halo_rows_by_ipc(torch_cuda, precision):
+def test_processes_push_halo_rows_by_ipc(torch_cuda, precision, nranks):
     import torch.multiprocessing as mp
     from mosegpu import case as cs
     from mosegpu.engine import Engine
@@ -74,7 +75,7 @@ def test_two_processes_push_halo_rows_by_ipc(torch_cuda, precision):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, precision, steps, q)) for r in range(2)]
+    procs = [ctx.Process(target=_rank_main, args=(r, nranks, port, precision, steps, q)) for r in range(nranks)]
     for p in procs:
         p.start()
     try:
