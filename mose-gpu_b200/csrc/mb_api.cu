@@ -1304,8 +1304,12 @@ int mb_ipc_open(const void* handle, int device, void** base) {
   if (!handle || !base || device < 0) return MB_E_ARG;
   cudaIpcMemHandle_t h;
   memcpy(&h, handle, sizeof(h));
+  int cur = 0;
+  CK(cudaGetDevice(&cur));
   CK(cudaSetDevice(device));
-  CK(cudaIpcOpenMemHandle(base, h, cudaIpcMemLazyEnablePeerAccess));
+  const cudaError_t e = cudaIpcOpenMemHandle(base, h, cudaIpcMemLazyEnablePeerAccess);
+  cudaSetDevice(cur);  // the caller's current device is left as it was
+  CK(e);
   return MB_OK;
 }
 
